@@ -1,0 +1,123 @@
+// aak_common.hpp -- constants, 3PN rate formulas and the per-source record
+// shared by the host pipeline (C++) and the sm_100a kernels (CUDA).
+#pragma once
+
+#include <stdint.h>
+#include <math.h>
+
+#ifdef __CUDACC__
+#define AAK_HD __host__ __device__ __forceinline__
+#else
+#define AAK_HD inline
+#endif
+
+namespace aak {
+
+// Physical constants with the values of the reference's include/Constants.h.
+constexpr double kG = 6.67259e-11;
+constexpr double kC = 299792458.0;
+constexpr double kMsun = 1.98892e30;
+constexpr double kMsunSec = kG * kMsun / (kC * kC * kC);  // SOLARMASSINSEC
+constexpr double kGpc = 3.0856775807e16 * 1.e9 / kC;      // "Gpc" (seconds)
+constexpr double kYear = 31558149.8;                      // sidereal year
+constexpr double kAUsec = 1.4959787066e11 / kC;
+constexpr double kPi = 3.14159265358979323846;
+// Truncated constants the 3PN fits are written with (include/KSParMap.h:12-13).
+constexpr double kEulerGamma = 0.5772156649015329;
+constexpr double kPi2Trunc = 9.86960440109;
+
+// ---------------------------------------------------------------------------
+// Kerr-geodesic frequency ratios in the 3PN AK mapping (Sago & Fujita 2015),
+// as functions of v = 1/sqrt(p), e, Y = cos(iota), q = spin.  Same expressions
+// as src/suite/KSParMap.cc:146-209, grouped by powers of v.
+AAK_HD double pn_dtdm(double v, double e, double Y, double q) {
+  const double v2 = v * v, v3 = v2 * v, v4 = v2 * v2;
+  const double e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  double s = 2. * e4 *
+             (240. + v2 * (-120. + v * (42. * (-27. + 4. * q2) * v + (-6567. + 1996. * q2) * v3 +
+                                        48. * q * (8. + 77. * v2) * Y - 4. * q2 * v * (90. + 1577. * v2) * Y2)));
+  s += e4 * e2 *
+       (560. + v2 * (-360. + 960. * q * v * Y + 8816. * q * v3 * Y + v4 * (-15565. + 24. * q2 * (200. - 629. * Y2)) +
+                     v2 * (-2742. + 80. * q2 * (5. - 11. * Y2))));
+  s -= 8. * e2 *
+       (-48. + v2 * (8. - 64. * q * v * Y - 688. * q * v3 * Y + 2. * v2 * (99. + 16. * q2 * (-1. + 2. * Y2)) +
+                     v4 * (1233. + 8. * q2 * (-47. + 150. * Y2))));
+  s += 16. * (16. + v2 * (24. + v2 * (27. * (2. + 5. * v2) - 48. * q * v * Y +
+                                      4. * q2 * (2. - v2 + (-2. + 3. * v2) * Y2))));
+  return s / (256. * v4);
+}
+
+AAK_HD double pn_drdm(double v, double e, double Y, double q) {
+  const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  double s = 16. + 8. * (-3. + e2) * v2 - 16. * (-3. + e2) * q * v3 * Y + 8. * (33. + 4. * e2 - 3. * e4) * q * v3 * v2 * Y;
+  s += v3 * v3 *
+       (-351. + 132. * q2 + e2 * (-135. + 21. * e2 + 5. * e4 + 2. * (7. + e2) * q2) +
+        2. * (-204. + 13. * e2 * (-3. + e2)) * q2 * Y2);
+  s += 2. * v2 * v2 * (-45. + 3. * e4 + 4. * q2 * (1. - 4. * Y2) + 2. * e2 * q2 * (1. + Y2));
+  return s / (16. * v);
+}
+
+AAK_HD double pn_dthetadm(double v, double e, double Y, double q) {
+  const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  double s = 16. + 8. * (3. + e2) * v2 - 16. * (3. + e2) * q * v3 * Y - 8. * (3. + e2) * (5. + 3. * e2) * q * v3 * v2 * Y;
+  s += v3 * v3 *
+       (135. - 54. * q2 + e2 * (5. * (27. + 9. * e2 + e4) + 2. * (-38. + e2) * q2) +
+        2. * (57. + 90. * e2 + 13. * e4) * q2 * Y2);
+  s += 2. * v2 * v2 * (27. + 3. * e4 + 2. * q2 * (-1. + 7. * Y2) + 2. * e2 * (9. + q2 * (1. + Y2)));
+  return s / (16. * v);
+}
+
+AAK_HD double pn_dphidm(double v, double e, double Y, double q) {
+  const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  double s = 16. + 8. * (3. + e2) * v2 - 16. * q * v3 * (-2. + (3. + e2) * Y) -
+             8. * q * v3 * v2 * (-6. + 15. * Y + 3. * e4 * Y + 2. * e2 * (-4. + 7. * Y));
+  s += 2. * v2 * v2 * (27. + 3. * e4 + 2. * q2 * (-1. + Y) * (1. + 7. * Y) + 2. * e2 * (9. + q2 * (1. + Y2)));
+  s += v3 * v3 *
+       (5. * e4 * e2 + e4 * (45. + q2 * (2. + 26. * Y2)) + e2 * (135. + 4. * q2 * (-19. + 5. * Y * (-7. + 9. * Y))) +
+        3. * (45. + 2. * q2 * (-9. + Y * (-6. + 19. * Y))));
+  return s / (16. * v);
+}
+
+// Azimuthal frequency magnitude for pro/retrograde orbits (src/suite/AAK.cc:15-23).
+AAK_HD double omega_phi(double v, double e, double cosiota, double s, double M) {
+  if (cosiota > 0) return pn_dphidm(v, e, cosiota, s) / pn_dtdm(v, e, cosiota, s) / M;
+  return pn_dphidm(v, e, -cosiota, -s) / pn_dtdm(v, e, -cosiota, -s) / M;
+}
+
+// ---------------------------------------------------------------------------
+// Per-source record consumed by the dense kernels.  One per source, built by
+// the host pipeline (evolve.cpp) and copied to HBM as an array of structs.
+// All times are in seconds; masses M_sec in seconds.
+struct alignas(16) SourceDesc {
+  // orientation (reference waveform(), AAK.cc:323-338)
+  double lam, coslam, sinlam;
+  double qS, cosqS, sinqS, phiS;
+  double qK, cosqK, sinqK, phiK, cosphiK, sinphiK;
+  double zeta;       // mu_sec / (D Gpc)
+  double M_phys_sec; // M_phys * SOLARMASSINSEC
+  double dt;         // dense sample spacing
+  double t_first;    // time of dense sample 0 (first knot time)
+  double Phi0, gim0, alp0;
+  double rot_sign;   // unused padding slot (kept for alignment)
+  int64_t out_offset;   // first output sample of this source in the batch arrays
+  int64_t knot_offset;  // first knot of this source in the knot arrays
+  int64_t tile_offset;  // first tile of this source in the tile arrays
+  int32_t vlength;      // dense samples
+  int32_t n_knots;      // spline knots
+  int32_t i0;           // dense index of t = 0
+  int32_t i_plunge;
+  int32_t i_buffer;
+  int32_t nmodes;
+  int32_t mich;         // LISA response on/off
+  int32_t n_tiles;
+  int32_t bessel_offset; // first entry of this source in the Bessel start-order table
+  int32_t status;        // 0 = OK, else an aak_status code (source skipped by the kernels)
+};
+
+// Natural cubic spline piece on [t_k, t_{k+1}] for the four tracked
+// quantities (e, v, M, S): y + dx (b + dx (c + dx d)).
+struct alignas(16) KnotCoef {
+  double y, b, c, d;
+};
+
+}  // namespace aak

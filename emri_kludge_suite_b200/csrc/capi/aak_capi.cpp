@@ -1,0 +1,555 @@
+// aak_capi.cpp -- the extern "C" surface declared in include/aak.h: batch
+// planning on host threads, device buffers of a context, kernel launches.
+#include "aak.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../host/pipeline.hpp"
+#include "../kernels/aak_dense.cuh"
+
+using namespace aak;
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+  T *ptr = nullptr;
+  size_t cap = 0;
+  int reserve(size_t n) {
+    if (n <= cap && ptr) return AAK_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(n, 1);
+    want += want / 4;  // growth headroom
+    if (cudaMalloc(&ptr, want * sizeof(T)) != cudaSuccess) {
+      cudaGetLastError();
+      ptr = nullptr;
+      return AAK_ERR_NO_MEMORY;
+    }
+    cap = want;
+    return AAK_OK;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
+int cuda_ok(cudaError_t e) {
+  if (e == cudaSuccess) return AAK_OK;
+  cudaGetLastError();
+  return e == cudaErrorMemoryAllocation ? AAK_ERR_NO_MEMORY : AAK_ERR_CUDA;
+}
+
+}  // namespace
+
+struct aak_ctx {
+  int device = 0;
+  int num_sms = 148;
+  // host plan
+  int32_t nsrc = 0;
+  std::vector<SourcePlan> plans;
+  std::vector<int64_t> offsets;
+  std::vector<int32_t> status;
+  std::vector<SourceDesc> descs;
+  std::vector<int64_t> tile_start;
+  std::vector<double> knot_t;
+  std::vector<double4> knot_y, knot_c;
+  std::vector<int32_t> bessel;
+  int64_t total_samples = 0, total_tiles = 0, total_knots = 0;
+  bool uploaded = false;
+  // device buffers
+  DevBuf<SourceDesc> d_src;
+  DevBuf<int64_t> d_tile_start;
+  DevBuf<double> d_knot_t;
+  DevBuf<double4> d_knot_y, d_knot_c;
+  DevBuf<int32_t> d_bessel;
+  DevBuf<TileSummary> d_summ;
+  DevBuf<TileCarry> d_carry;
+  DevBuf<unsigned long long> d_counter;
+  DevBuf<double> d_out;  // outputs for the host-buffer entry points
+  int last_launches = 0;
+  std::mutex mu;
+};
+
+namespace {
+
+int select_device(int dev) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return AAK_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= n) return AAK_ERR_INVALID_PARAM;
+  return cuda_ok(cudaSetDevice(dev));
+}
+
+Params to_params(const aak_params &a) {
+  Params P;
+  P.length = a.length;
+  P.dt = a.dt;
+  P.p = a.p;
+  P.T = a.T;
+  P.f = a.f;
+  P.T_fit = a.T_fit;
+  P.mu = a.mu;
+  P.M = a.M;
+  P.s = a.s;
+  P.e = a.e;
+  P.iota = a.iota;
+  P.gamma = a.gamma;
+  P.psi = a.psi;
+  P.theta_S = a.theta_S;
+  P.phi_S = a.phi_S;
+  P.theta_K = a.theta_K;
+  P.phi_K = a.phi_K;
+  P.alpha = a.alpha;
+  P.D = a.D;
+  P.backint = a.backint;
+  P.LISA = a.LISA;
+  return P;
+}
+
+void to_mapped(const MappedTrajectory &m, aak_mapped *o) {
+  std::memset(o, 0, sizeof(*o));
+  o->steps = m.steps;
+  o->inspiral_flag = m.inspiral_flag;
+  o->newton_iterations = m.newton_iterations;
+  o->Phi0 = m.Phi0;
+  for (int i = 0; i < m.steps; ++i) {
+    o->e_traj[i] = m.e_traj[i];
+    o->v_map[i] = m.v_map[i];
+    o->M_map[i] = m.M_map[i];
+    o->s_map[i] = m.s_map[i];
+    o->dt_map[i] = m.dt_map[i];
+  }
+}
+
+void from_mapped(const aak_mapped &o, MappedTrajectory *m) {
+  m->steps = std::min<int>(o.steps, kMaxCoarseSteps);
+  m->inspiral_flag = o.inspiral_flag;
+  m->newton_iterations = o.newton_iterations;
+  m->Phi0 = o.Phi0;
+  for (int i = 0; i < m->steps; ++i) {
+    m->e_traj[i] = o.e_traj[i];
+    m->v_map[i] = o.v_map[i];
+    m->M_map[i] = o.M_map[i];
+    m->s_map[i] = o.s_map[i];
+    m->dt_map[i] = o.dt_map[i];
+  }
+}
+
+template <typename F>
+void parallel_for(int n, int nthreads, F &&fn) {
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  nthreads = std::min(nthreads, n);
+  if (nthreads <= 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<int> next(0);
+  std::vector<std::thread> pool;
+  pool.reserve(nthreads);
+  for (int t = 0; t < nthreads; ++t)
+    pool.emplace_back([&]() {
+      for (;;) {
+        const int i = next.fetch_add(1);
+        if (i >= n) break;
+        fn(i);
+      }
+    });
+  for (auto &th : pool) th.join();
+}
+
+// Pack per-source plans into the flat arrays the kernels read.
+void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
+  const int n = ctx->nsrc;
+  ctx->offsets.assign(n + 1, 0);
+  ctx->tile_start.assign(n + 1, 0);
+  ctx->descs.resize(n);
+  int64_t knots = 0, bes = 0;
+  for (int s = 0; s < n; ++s) {
+    const SourcePlan &pl = ctx->plans[s];
+    const int64_t len = P[s].length;
+    ctx->offsets[s + 1] = ctx->offsets[s] + len;
+    ctx->tile_start[s + 1] = ctx->tile_start[s] + (len + kTileSamples - 1) / kTileSamples;
+    if (ctx->status[s] == AAK_OK) {
+      knots += (int64_t)pl.knot_t.size();
+      bes += pl.nmodes;
+    }
+  }
+  ctx->total_samples = ctx->offsets[n];
+  ctx->total_tiles = ctx->tile_start[n];
+  ctx->total_knots = knots;
+  ctx->knot_t.resize(std::max<int64_t>(knots, 1));
+  ctx->knot_y.resize(std::max<int64_t>(knots, 1));
+  ctx->knot_c.resize(std::max<int64_t>(knots, 1));
+  ctx->bessel.resize(std::max<int64_t>(bes, 1));
+  int64_t ko = 0, bo = 0;
+  for (int s = 0; s < n; ++s) {
+    SourceDesc d;
+    const SourcePlan &pl = ctx->plans[s];
+    if (ctx->status[s] == AAK_OK) {
+      d = pl.desc;
+      const int64_t nk = (int64_t)pl.knot_t.size();
+      for (int64_t k = 0; k < nk; ++k) {
+        ctx->knot_t[ko + k] = pl.knot_t[k];
+        ctx->knot_y[ko + k] = make_double4(pl.knot_y[4 * k], pl.knot_y[4 * k + 1], pl.knot_y[4 * k + 2], pl.knot_y[4 * k + 3]);
+        ctx->knot_c[ko + k] = make_double4(pl.knot_c[4 * k], pl.knot_c[4 * k + 1], pl.knot_c[4 * k + 2], pl.knot_c[4 * k + 3]);
+      }
+      d.knot_offset = ko;
+      d.bessel_offset = (int32_t)bo;
+      for (int m = 1; m <= pl.nmodes; ++m) ctx->bessel[bo + m - 1] = bessel_start_order(m, pl.e_max);
+      ko += nk;
+      bo += pl.nmodes;
+    } else {
+      std::memset(&d, 0, sizeof(d));
+      d.status = ctx->status[s];
+      d.vlength = (int32_t)P[s].length;
+    }
+    d.out_offset = ctx->offsets[s];
+    d.tile_offset = ctx->tile_start[s];
+    d.n_tiles = (int32_t)(ctx->tile_start[s + 1] - ctx->tile_start[s]);
+    ctx->descs[s] = d;
+  }
+  ctx->uploaded = false;
+}
+
+int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32_t nsrc, const int32_t *nm,
+                int32_t nthreads) {
+  if (!ctx || !P || nsrc <= 0) return AAK_ERR_INVALID_PARAM;
+  std::vector<aak_params> Pv(P, P + nsrc);
+  for (auto &p : Pv)
+    if (p.length < 2 || p.length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
+  ctx->nsrc = nsrc;
+  ctx->plans.assign(nsrc, SourcePlan());
+  ctx->status.assign(nsrc, AAK_OK);
+  parallel_for(nsrc, nthreads, [&](int s) {
+    const Params Pp = to_params(Pv[s]);
+    int st = validate(Pp);
+    MappedTrajectory mt;
+    if (st == kOk) {
+      if (maps) from_mapped(maps[s], &mt);
+      else st = front_end(Pp, &mt, nullptr);
+    }
+    if (st == kOk) {
+      WaveInputs w;
+      genwave_inputs(Pp, mt, nm ? nm[s] : 0, &w);
+      if (w.nmodes > 4096) st = kErrCapacity;
+      else st = plan_source(w, &ctx->plans[s]);
+    }
+    ctx->status[s] = st;
+    if (st != kOk) {
+      ctx->plans[s].knot_t.clear();
+      ctx->plans[s].knot_y.clear();
+      ctx->plans[s].knot_c.clear();
+    }
+  });
+  pack(ctx, Pv);
+  return AAK_OK;
+}
+
+int upload(aak_ctx *ctx, cudaStream_t st) {
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  const int n = ctx->nsrc;
+  if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
+      (r = ctx->d_knot_t.reserve(ctx->knot_t.size())) || (r = ctx->d_knot_y.reserve(ctx->knot_y.size())) ||
+      (r = ctx->d_knot_c.reserve(ctx->knot_c.size())) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
+      (r = ctx->d_summ.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
+      (r = ctx->d_carry.reserve(std::max<int64_t>(ctx->total_tiles, 1))) || (r = ctx->d_counter.reserve(1)))
+    return r;
+  auto cp = [&](void *dst, const void *src, size_t bytes) {
+    return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+  };
+  if ((r = cp(ctx->d_src.ptr, ctx->descs.data(), n * sizeof(SourceDesc))) ||
+      (r = cp(ctx->d_tile_start.ptr, ctx->tile_start.data(), (n + 1) * sizeof(int64_t))) ||
+      (r = cp(ctx->d_knot_t.ptr, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
+      (r = cp(ctx->d_knot_y.ptr, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
+      (r = cp(ctx->d_knot_c.ptr, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
+      (r = cp(ctx->d_bessel.ptr, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
+    return r;
+  ctx->uploaded = true;
+  return AAK_OK;
+}
+
+int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride, int precision,
+        cudaStream_t st) {
+  if (!ctx->uploaded) return AAK_ERR_INVALID_PARAM;
+  if (!hI || !hII) return AAK_ERR_INVALID_PARAM;
+  if (traj && traj_stride < ctx->total_samples) return AAK_ERR_INVALID_PARAM;
+  if (precision != 0) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  BatchView bv;
+  bv.src = ctx->d_src.ptr;
+  bv.nsrc = ctx->nsrc;
+  bv.total_tiles = ctx->total_tiles;
+  bv.tile_start = ctx->d_tile_start.ptr;
+  bv.knot_t = ctx->d_knot_t.ptr;
+  bv.knot_y = ctx->d_knot_y.ptr;
+  bv.knot_c = ctx->d_knot_c.ptr;
+  bv.bessel_start = ctx->d_bessel.ptr;
+  bv.summ = ctx->d_summ.ptr;
+  bv.carry = ctx->d_carry.ptr;
+  bv.hI = hI;
+  bv.hII = hII;
+  bv.t_out = t;
+  bv.traj_out = traj;
+  bv.traj_stride = traj_stride;
+  bv.work_counter = ctx->d_counter.ptr;
+  launch_dense_fp64(bv, ctx->num_sms, st);
+  ctx->last_launches = 3;
+  return cuda_ok(cudaGetLastError());
+}
+
+std::mutex g_default_mu;
+aak_ctx *g_default[64] = {nullptr};
+
+int default_ctx(aak_ctx **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return AAK_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= 64) return AAK_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(g_default_mu);
+  if (!g_default[dev]) {
+    int r = aak_ctx_create(dev, &g_default[dev]);
+    if (r != AAK_OK) return r;
+  }
+  *out = g_default[dev];
+  return AAK_OK;
+}
+
+// Plan, upload and run one batch into ctx-owned device outputs, then copy to host.
+int host_roundtrip(aak_ctx *ctx, double *t, double *hI, double *hII) {
+  int r;
+  const int64_t N = ctx->total_samples;
+  if ((r = upload(ctx, 0)) != AAK_OK) return r;
+  if ((r = ctx->d_out.reserve((size_t)(t ? 3 : 2) * N)) != AAK_OK) return r;
+  double *dI = ctx->d_out.ptr, *dII = dI + N, *dt = t ? dII + N : nullptr;
+  if ((r = run(ctx, dI, dII, dt, nullptr, 0, 0, 0)) != AAK_OK) return r;
+  if ((r = cuda_ok(cudaMemcpyAsync(hI, dI, N * sizeof(double), cudaMemcpyDeviceToHost, 0))) ||
+      (r = cuda_ok(cudaMemcpyAsync(hII, dII, N * sizeof(double), cudaMemcpyDeviceToHost, 0))))
+    return r;
+  if (t && (r = cuda_ok(cudaMemcpyAsync(t, dt, N * sizeof(double), cudaMemcpyDeviceToHost, 0)))) return r;
+  return cuda_ok(cudaStreamSynchronize(0));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *aak_status_string(int s) {
+  switch (s) {
+    case AAK_OK: return "ok";
+    case AAK_ERR_INVALID_PARAM: return "invalid parameter";
+    case AAK_ERR_UNSTABLE_START: return "initial orbit inside the last stable orbit";
+    case AAK_ERR_FIT_TOO_CLOSE_TO_PLUNGE: return "fitting error: t_0 too close to plunge";
+    case AAK_ERR_SOLVER_NO_CONVERGE: return "Kerr-to-AK parameter map did not converge";
+    case AAK_ERR_CUDA: return "CUDA error or no CUDA device";
+    case AAK_ERR_NO_MEMORY: return "out of device memory";
+    case AAK_ERR_TOO_FEW_STEPS: return "coarse inspiral produced fewer than 3 points";
+    case AAK_ERR_CAPACITY: return "request exceeds a fixed-size buffer";
+    default: return "unknown status";
+  }
+}
+
+int aak_version(void) { return 10000; }
+
+int aak_front_end(const aak_params *p, const double *warm, aak_mapped *out) {
+  if (!p || !out) return AAK_ERR_INVALID_PARAM;
+  MappedTrajectory mt;
+  const int st = front_end(to_params(*p), &mt, warm);
+  if (st == kOk) to_mapped(mt, out);
+  else std::memset(out, 0, sizeof(*out));
+  return st;
+}
+
+int aak_coarse_kerr(const aak_params *p, int32_t *steps, double *t_rr, double *pp, double *e, double *cosi,
+                    double *Omega) {
+  if (!p || !steps) return AAK_ERR_INVALID_PARAM;
+  CoarseKerr ck;
+  const int st = coarse_kerr(to_params(*p), &ck);
+  *steps = ck.steps;
+  for (int i = 0; i < ck.steps; ++i) {
+    if (t_rr) t_rr[i] = ck.t_rr[i];
+    if (pp) pp[i] = ck.p[i];
+    if (e) e[i] = ck.e[i];
+    if (cosi) cosi[i] = ck.cosi[i];
+    if (Omega)
+      for (int k = 0; k < 3; ++k) Omega[3 * i + k] = ck.Omega[i][k];
+  }
+  return st;
+}
+
+int aak_parmap(const double Omega[3], double p, double M, double s, double e, double iota, const double *x0,
+               double map[3], int32_t *iterations) {
+  if (!Omega || !map) return AAK_ERR_INVALID_PARAM;
+  const int it = parmap(Omega, p, M, s, e, iota, x0, map);
+  if (iterations) *iterations = it < 0 ? -it - 1 : it;
+  return it < 0 ? AAK_ERR_SOLVER_NO_CONVERGE : AAK_OK;
+}
+
+int aak_ctx_create(int32_t device, aak_ctx **out) {
+  if (!out) return AAK_ERR_INVALID_PARAM;
+  *out = nullptr;
+  int r = select_device(device);
+  if (r != AAK_OK) return r;
+  aak_ctx *c = new (std::nothrow) aak_ctx();
+  if (!c) return AAK_ERR_NO_MEMORY;
+  c->device = device;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) c->num_sms = sms;
+  *out = c;
+  return AAK_OK;
+}
+
+void aak_ctx_destroy(aak_ctx *c) {
+  if (!c) return;
+  if (select_device(c->device) == AAK_OK) {
+    c->d_src.release();
+    c->d_tile_start.release();
+    c->d_knot_t.release();
+    c->d_knot_y.release();
+    c->d_knot_c.release();
+    c->d_bessel.release();
+    c->d_summ.release();
+    c->d_carry.release();
+    c->d_counter.release();
+    c->d_out.release();
+  }
+  delete c;
+}
+
+int aak_batch_plan(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nm, int32_t nthreads) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return plan_common(ctx, P, nullptr, nsrc, nm, nthreads);
+}
+
+int aak_batch_plan_mapped(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32_t nsrc, const int32_t *nm,
+                          int32_t nthreads) {
+  if (!ctx || !maps) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return plan_common(ctx, P, maps, nsrc, nm, nthreads);
+}
+
+int aak_batch_info(aak_ctx *ctx, int64_t *total, int64_t *offsets, int32_t *status, int32_t *i_plunge, int32_t *i_buffer) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (total) *total = ctx->total_samples;
+  for (int s = 0; s < ctx->nsrc; ++s) {
+    if (status) status[s] = ctx->status[s];
+    if (i_plunge) i_plunge[s] = ctx->status[s] == AAK_OK ? ctx->plans[s].i_plunge : -1;
+    if (i_buffer) i_buffer[s] = ctx->status[s] == AAK_OK ? ctx->plans[s].i_buffer : -1;
+  }
+  if (offsets)
+    for (int s = 0; s <= ctx->nsrc; ++s) offsets[s] = ctx->offsets[s];
+  return AAK_OK;
+}
+
+int aak_batch_upload(aak_ctx *ctx, void *stream) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return upload(ctx, (cudaStream_t)stream);
+}
+
+int aak_batch_run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride,
+                  int32_t precision, void *stream) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return run(ctx, hI, hII, t, traj, traj_stride, precision, (cudaStream_t)stream);
+}
+
+int aak_batch_last_launches(aak_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
+
+int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nm, int32_t nthreads,
+                        double *h_hI, double *h_hII, int64_t *offsets, int32_t *status) {
+  if (!ctx || !h_hI || !h_hII) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  int r = plan_common(ctx, P, nullptr, nsrc, nm, nthreads);
+  if (r != AAK_OK) return r;
+  if (offsets)
+    for (int s = 0; s <= nsrc; ++s) offsets[s] = ctx->offsets[s];
+  if (status)
+    for (int s = 0; s < nsrc; ++s) status[s] = ctx->status[s];
+  return host_roundtrip(ctx, nullptr, h_hI, h_hII);
+}
+
+int aak_wave(const aak_params *p, double *t, double *hI, double *hII, double *seconds) {
+  if (!p || !t || !hI || !hII) return AAK_ERR_INVALID_PARAM;
+  const auto t0 = std::chrono::steady_clock::now();
+  aak_ctx *ctx = nullptr;
+  int r = default_ctx(&ctx);
+  if (r != AAK_OK) return r;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  r = plan_common(ctx, p, nullptr, 1, nullptr, 1);
+  if (r != AAK_OK) return r;
+  if (ctx->status[0] != AAK_OK) return ctx->status[0];
+  r = host_roundtrip(ctx, t, hI, hII);
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
+int aak_genwave(double *t, double *hI, double *hII, double timestep, int32_t vlength, const double *e_traj,
+                const double *v_map, double M_phys, const double *M_map, double mu, double S_phys, const double *S_map,
+                double dist, double inc, double gim0, double Phi0, double qS, double phiS, double alp0, double qK,
+                double phiK, const double *dt_map, int32_t steps, int32_t backint, int32_t mich, int32_t nmodes_override) {
+  if (!t || !hI || !hII || !e_traj || !v_map || !M_map || !S_map || !dt_map) return AAK_ERR_INVALID_PARAM;
+  if (steps < 3 || steps > kMaxCoarseSteps || vlength < 2) return AAK_ERR_INVALID_PARAM;
+  aak_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.length = vlength;
+  p.dt = timestep;
+  p.mu = mu;
+  p.M = M_phys;
+  p.s = S_phys;
+  p.e = e_traj[0];
+  p.iota = inc;
+  p.gamma = gim0;
+  p.theta_S = qS;
+  p.phi_S = phiS;
+  p.theta_K = qK;
+  p.phi_K = phiK;
+  p.alpha = alp0;
+  p.D = dist;
+  p.p = 1.0;
+  p.T_fit = 1.0;
+  p.backint = backint;
+  p.LISA = mich;
+  aak_mapped m;
+  std::memset(&m, 0, sizeof(m));
+  m.steps = steps;
+  m.Phi0 = Phi0;
+  for (int i = 0; i < steps; ++i) {
+    m.e_traj[i] = e_traj[i];
+    m.v_map[i] = v_map[i];
+    m.M_map[i] = M_map[i];
+    m.s_map[i] = S_map[i];
+    m.dt_map[i] = dt_map[i];
+  }
+  aak_ctx *ctx = nullptr;
+  int r = default_ctx(&ctx);
+  if (r != AAK_OK) return r;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int32_t nm = nmodes_override;
+  r = plan_common(ctx, &p, &m, 1, &nm, 1);
+  if (r != AAK_OK) return r;
+  if (ctx->status[0] != AAK_OK) return ctx->status[0];
+  return host_roundtrip(ctx, t, hI, hII);
+}
+
+}  // extern "C"

@@ -1,0 +1,594 @@
+// pipeline.cpp -- see pipeline.hpp.
+#include "pipeline.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "inspiral.hpp"
+#include "kerr.hpp"
+
+namespace aak {
+
+// ------------------------------------------------------------------ validation
+int validate(const Params &P) {
+  const double v[] = {P.dt, P.p, P.T_fit, P.mu, P.M, P.s, P.e, P.iota, P.gamma, P.psi,
+                      P.theta_S, P.phi_S, P.theta_K, P.phi_K, P.alpha, P.D};
+  for (double x : v)
+    if (!std::isfinite(x)) return kErrInvalidParam;
+  if (P.length < 2 || P.length > (int64_t)1 << 31) return kErrInvalidParam;
+  if (!(P.dt > 0) || !(P.p > 0) || !(P.T_fit > 0) || !(P.mu > 0) || !(P.M > 0) || !(P.D > 0)) return kErrInvalidParam;
+  if (!(P.mu < P.M)) return kErrInvalidParam;
+  if (!(P.e > 0.0 && P.e < 1.0)) return kErrInvalidParam;   // e = 0 has no eccentric inspiral
+  if (!(std::fabs(P.s) < 1.0)) return kErrInvalidParam;
+  if (std::fabs(std::cos(P.iota)) < 1e-9) return kErrInvalidParam;  // polar orbits: flux kludge singular
+  if (std::fabs(std::sin(P.theta_K)) == 0.0) return kErrInvalidParam;
+  return kOk;
+}
+
+// ------------------------------------------------------------------ front end
+int coarse_kerr(const Params &P, CoarseKerr *out) {
+  int st = validate(P);
+  if (st != kOk) return st;
+  KerrInspiral insp(std::cos(P.iota), P.s);
+  const int maxsteps = kMaxCoarseSteps;
+  const double dt_fit = std::min(P.T_fit, P.length * P.dt / kMsunSec / P.M / P.M * P.mu) / (maxsteps - 1);
+  TrajPoint pts[kMaxCoarseSteps];
+  int steps = 0;
+  out->inspiral_flag = insp.eccentric(P.p, P.e, dt_fit, maxsteps, pts, &steps);
+  if (out->inspiral_flag == kInspUnstableStart) return kErrUnstableStart;
+  out->steps = steps;
+  for (int i = 0; i < steps; ++i) {
+    out->t_rr[i] = pts[i].t;
+    out->p[i] = pts[i].p;
+    out->e[i] = pts[i].e;
+    out->cosi[i] = pts[i].cosi;
+    KerrGeodesic g;
+    g.set_full(pts[i].p, pts[i].e, pts[i].cosi, P.s);
+    g.frequencies(out->Omega[i]);
+  }
+  if (steps < 3) return kErrTooFewSteps;
+  return kOk;
+}
+
+namespace {
+// Kerr->AK residual: Omega_k M_map - Omega_k^PN(v_map, s_map) M  (KSParMap.cc:323-358)
+void parmap_residual(const double Om[3], double M, double e, double Y, const double x[3], double f[3]) {
+  const double v = x[0], Mm = x[1], s = x[2];
+  double Or, Ot, Op;
+  const double inv2pi = 1.0 / (2.0 * kPi);
+  if (Y > 0) {
+    const double tm = pn_dtdm(v, e, Y, s);
+    Or = pn_drdm(v, e, Y, s) / tm / 2. / kPi;
+    Ot = pn_dthetadm(v, e, Y, s) / tm / 2. / kPi;
+    Op = pn_dphidm(v, e, Y, s) / tm / 2. / kPi;
+  } else {
+    const double tm = pn_dtdm(v, e, -Y, -s);
+    Or = pn_drdm(v, e, -Y, -s) / tm / 2. / kPi;
+    Ot = pn_dthetadm(v, e, -Y, -s) / tm / 2. / kPi;
+    Op = -pn_dphidm(v, e, -Y, -s) / tm / 2. / kPi;
+  }
+  (void)inv2pi;
+  f[0] = Om[0] * Mm - Or * M;
+  f[1] = Om[1] * Mm - Ot * M;
+  f[2] = Om[2] * Mm - Op * M;
+}
+inline double norm1(const double f[3]) { return std::fabs(f[0]) + std::fabs(f[1]) + std::fabs(f[2]); }
+
+bool solve3(double A[3][3], double b[3], double x[3]) {
+  int piv[3] = {0, 1, 2};
+  for (int k = 0; k < 3; ++k) {
+    int p = k;
+    for (int i = k + 1; i < 3; ++i)
+      if (std::fabs(A[i][k]) > std::fabs(A[p][k])) p = i;
+    if (A[p][k] == 0.0) return false;
+    if (p != k) {
+      for (int j = 0; j < 3; ++j) std::swap(A[k][j], A[p][j]);
+      std::swap(b[k], b[p]);
+      std::swap(piv[k], piv[p]);
+    }
+    for (int i = k + 1; i < 3; ++i) {
+      const double m = A[i][k] / A[k][k];
+      for (int j = k; j < 3; ++j) A[i][j] -= m * A[k][j];
+      b[i] -= m * b[k];
+    }
+  }
+  for (int k = 2; k >= 0; --k) {
+    double s = b[k];
+    for (int j = k + 1; j < 3; ++j) s -= A[k][j] * x[j];
+    x[k] = s / A[k][k];
+  }
+  return true;
+}
+}  // namespace
+
+int parmap(const double Om[3], double p, double M, double s, double e, double iota, const double *x0, double map[3]) {
+  const double Y = std::cos(iota);
+  double x[3];
+  if (x0) {
+    x[0] = x0[0];
+    x[1] = x0[1];
+    x[2] = x0[2];
+  } else {
+    x[0] = 1. / std::sqrt(p);
+    x[1] = M;
+    x[2] = s;
+  }
+  double f[3];
+  parmap_residual(Om, M, e, Y, x, f);
+  int iters = 0;
+  bool reached = norm1(f) < 1e-6;
+  for (int it = 0; it < 200; ++it) {
+    // Jacobian: central differences in v_map and s_map, exact in M_map
+    double J[3][3];
+    for (int col : {0, 2}) {
+      const double h = 1e-6 * std::max(std::fabs(x[col]), 1e-2);
+      double xp[3] = {x[0], x[1], x[2]}, xm[3] = {x[0], x[1], x[2]}, fp[3], fm[3];
+      xp[col] += h;
+      xm[col] -= h;
+      parmap_residual(Om, M, e, Y, xp, fp);
+      parmap_residual(Om, M, e, Y, xm, fm);
+      const double hh = xp[col] - xm[col];
+      for (int r = 0; r < 3; ++r) J[r][col] = (fp[r] - fm[r]) / hh;
+    }
+    for (int r = 0; r < 3; ++r) J[r][1] = Om[r];
+    double rhs[3] = {-f[0], -f[1], -f[2]}, dx[3];
+    if (!solve3(J, rhs, dx)) break;
+    double lam = 1.0, xt[3], ft[3];
+    bool ok = false;
+    for (int ls = 0; ls < 40; ++ls) {
+      for (int i = 0; i < 3; ++i) xt[i] = x[i] + lam * dx[i];
+      parmap_residual(Om, M, e, Y, xt, ft);
+      if (std::isfinite(ft[0]) && std::isfinite(ft[1]) && std::isfinite(ft[2]) && norm1(ft) < norm1(f)) {
+        ok = true;
+        break;
+      }
+      lam *= 0.5;
+    }
+    if (!ok) break;  // no further decrease: at the rounding floor (or stuck)
+    double rel = 0.0;
+    for (int i = 0; i < 3; ++i) rel = std::max(rel, std::fabs(xt[i] - x[i]) / std::max(std::fabs(x[i]), 1e-300));
+    for (int i = 0; i < 3; ++i) {
+      x[i] = xt[i];
+      f[i] = ft[i];
+    }
+    ++iters;
+    if (norm1(f) < 1e-6) reached = true;
+    if (reached && rel < 4e-16) break;
+    if (norm1(f) == 0.0) break;
+  }
+  map[0] = x[0];
+  map[1] = x[1];
+  map[2] = x[2];
+  if (!(norm1(f) < 1e-6)) return -1 - iters;
+  return iters;
+}
+
+double initial_mean_anomaly(double e, double psi) {
+  const double se = std::sqrt(1. - e * e);
+  return std::atan2(se * std::sin(psi), e + std::cos(psi)) - e * se * std::sin(psi) / (1. + e * std::cos(psi));
+}
+
+int front_end(const Params &P, MappedTrajectory *out, const double *warm) {
+  CoarseKerr ck;
+  int st = coarse_kerr(P, &ck);
+  if (st != kOk) return st;
+  out->steps = ck.steps;
+  out->inspiral_flag = ck.inspiral_flag;
+  out->Phi0 = initial_mean_anomaly(P.e, P.psi);
+  out->newton_iterations = 0;
+  for (int i = 0; i < ck.steps; ++i) {
+    double map[3];
+    int it = parmap(ck.Omega[i], ck.p[i], P.M, P.s, ck.e[i], P.iota, warm ? warm + 3 * i : nullptr, map);
+    if (it < 0 && warm) it = parmap(ck.Omega[i], ck.p[i], P.M, P.s, ck.e[i], P.iota, nullptr, map);  // fallback
+    if (it < 0) return kErrSolverNoConverge;
+    out->newton_iterations += it;
+    out->e_traj[i] = ck.e[i];
+    out->v_map[i] = map[0];
+    out->M_map[i] = map[1];
+    out->s_map[i] = map[2];
+    out->dt_map[i] = ck.t_rr[i] * kMsunSec * P.M * P.M / P.mu;
+  }
+  return kOk;
+}
+
+void genwave_inputs(const Params &P, const MappedTrajectory &mt, int nmodes_override, WaveInputs *w) {
+  std::memset(w, 0, sizeof(*w));
+  w->par[0] = P.mu * kMsunSec;
+  w->par[1] = mt.M_map[0] * kMsunSec;
+  w->par[2] = mt.s_map[0];
+  w->par[3] = mt.e_traj[0];
+  w->par[4] = P.iota;
+  w->par[5] = P.gamma;
+  w->par[6] = mt.Phi0;
+  w->par[7] = P.theta_S;
+  w->par[8] = P.phi_S;
+  w->par[9] = P.theta_K;
+  w->par[10] = P.phi_K;
+  w->par[11] = P.alpha;
+  int nmodes = (int)(30 * w->par[3]);
+  if (w->par[3] < 0.135) nmodes = 4;
+  if (nmodes_override > 0) nmodes = nmodes_override;
+  w->nmodes = nmodes;
+  w->zeta = w->par[0] / P.D / kGpc;
+  w->timestep = P.dt;
+  w->vlength = (int)P.length;
+  w->e_traj = mt.e_traj;
+  w->v_map = mt.v_map;
+  w->M_map = mt.M_map;
+  w->S_map = mt.s_map;
+  w->dt_map = mt.dt_map;
+  w->M_phys = P.M;
+  w->S_phys = P.s;
+  w->steps = mt.steps;
+  w->backint = P.backint;
+  w->mich = P.LISA;
+}
+
+// ------------------------------------------------------------------ splines
+void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c) {
+  for (int k = 0; k < n; ++k) c[k * stride] = 0.0;
+  if (n < 3) return;
+  const int m = n - 2;
+  std::vector<double> cp(m), dp(m);
+  for (int k = 0; k < m; ++k) {
+    const int i = k + 1;
+    const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
+    const double diag = 2.0 * (h0 + h1);
+    const double rhs = 3.0 * ((y[(i + 1) * stride] - y[i * stride]) / h1 - (y[i * stride] - y[(i - 1) * stride]) / h0);
+    const double sup = (k + 1 < m) ? h1 : 0.0;
+    if (k == 0) {
+      cp[k] = sup / diag;
+      dp[k] = rhs / diag;
+    } else {
+      const double den = diag - h0 * cp[k - 1];
+      cp[k] = sup / den;
+      dp[k] = (rhs - h0 * dp[k - 1]) / den;
+    }
+  }
+  for (int k = m - 2; k >= 0; --k) dp[k] -= cp[k] * dp[k + 1];
+  for (int k = 0; k < m; ++k) c[(k + 1) * stride] = dp[k];
+}
+
+double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv) {
+  int lo = 0, hi = n - 1;
+  while (hi > lo + 1) {
+    const int mid = (lo + hi) / 2;
+    if (x[mid] > xv) hi = mid;
+    else lo = mid;
+  }
+  int i = std::min(lo, n - 2);
+  const double h = x[i + 1] - x[i], dx = xv - x[i];
+  const double yi = y[i * stride], yi1 = y[(i + 1) * stride];
+  const double ci = c[i * stride], ci1 = c[(i + 1) * stride];
+  const double b = (yi1 - yi) / h - h * (ci1 + 2.0 * ci) / 3.0;
+  const double d = (ci1 - ci) / (3.0 * h);
+  return yi + dx * (b + dx * (ci + dx * d));
+}
+
+// ------------------------------------------------------------------ Bessel start order
+int bessel_start_order(int n, double e_max) {
+  const int nmax = (n == 1) ? 3 : n + 2;
+  const double x = n * e_max;
+  int k = std::max(nmax, (int)std::ceil(x));
+  double prod = 1.0;
+  while (prod > 1e-19 && k < 8192) {
+    const double kk = k + 1.0;
+    const double r = x / (kk + std::sqrt(std::max(kk * kk - x * x, 0.0)));
+    prod *= r;
+    ++k;
+  }
+  k += 4;
+  if (k & 1) ++k;
+  return k;
+}
+
+// ------------------------------------------------------------------ coarse AK evolution
+namespace {
+double dvdt(double v, double e, double Y, double m, double M, double q) {
+  const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
+  const double e2 = e * e, e4 = e2 * e2, e6 = e4 * e2;
+  const double Y2 = Y * Y, q2 = q * q;
+  const double l2 = std::log(2.), l3 = std::log(3.), l5 = std::log(5.);
+  double s = 1. + 7. * e2 / 8.;
+  s += (-5944. - 7040. * e2 + 8539. * e4) * v2 / 2688.;
+  s -= v3 * ((-18432. - 55872. * e2 - 7056. * e4 + 49. * e6) * kPi + 48. * (1064. + 1516. * e2 + 475. * e4) * q * Y) / 4608.;
+  s += v3 * v2 *
+       ((-4791168. - 28113984. * e2 + 12239226. * e4 + 4005097. * e6) * kPi -
+        144. * (139296. + 58408. * e2 + 249968. * e4 + 106707. * e6) * q * Y) /
+       774144.;
+  s += v2 * v2 *
+       (953325. * e6 + 8. * (34103. + 189. * q2 * (-329. + 815. * Y2)) + 12. * e2 * (-526955. + 126. * q2 * (-929. + 1431. * Y2)) +
+        3. * e4 * (-1232809. + 63. * q2 * (-1051. + 2997. * Y2))) /
+       145152.;
+  double c6 = 117.72574285227559 - 1712. * kEulerGamma / 105. + 16. * kPi2Trunc / 3. - 331. * q2 / 192. -
+              289. * kPi * q * Y / 6. + 145759. * q2 * Y2 / 1344. - 3424. * l2 / 105.;
+  c6 += e2 * (764.5906705662063 - 24503. * kEulerGamma / 210. + 229. * kPi2Trunc / 6. + 2129. * q2 / 42. -
+              4225. * kPi * q * Y / 24. + 27191. * q2 * Y2 / 224. + 1391. * l2 / 30. - 78003. * l3 / 280.);
+  c6 += e4 * (723.1604428881717 - 11663. * kEulerGamma / 140. + 109. * kPi2Trunc / 4. - 56239. * q2 / 10752. -
+              17113. * kPi * q * Y / 192. + 414439. * q2 * Y2 / 3584. - 418049. * l2 / 84. + 3042117. * l3 / 1120.);
+  c6 += e6 * (202.0979603432282 - 2461. * kEulerGamma / 560. + 23. * kPi2Trunc / 16. - 3571. * q2 / 3584. -
+              108577. * kPi * q * Y / 13824. + 41071. * q2 * Y2 / 1536. + 94138279. * l2 / 2160. - 42667641. * l3 / 3584. -
+              1044921875. * l5 / 96768.);
+  c6 -= 107. * (256. + 1832. * e2 + 1308. * e4 + 69. * e6) * std::log(v) / 1680.;
+  s += v6 * c6;
+  return 32. * std::pow(1. - e2, 1.5) * m * v6 * v3 * s / (5. * M * M);
+}
+
+double dedt(double v, double e, double Y, double m, double M, double q) {
+  const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
+  const double e2 = e * e, e4 = e2 * e2;
+  const double Y2 = Y * Y, q2 = q * q;
+  const double l2 = std::log(2.), l3 = std::log(3.), l5 = std::log(5.);
+  double s = 2451456. + 975744. * e2;
+  s += 144. * (-54792. - 18600. * e2 + 22579. * e4) * v2;
+  s += 84. * v3 * ((189120. + 286512. * e2 + 24217. * e4) * kPi - 48. * (7032. + 5592. * e2 + 1313. * e4) * q * Y);
+  s += 3. * v3 * v2 * ((-16885824. - 42474444. * e2 + 5678971. * e4) * kPi - 48. * (106568. + 187862. * e2 + 442811. * e4) * q * Y);
+  s += 8. * v2 * v2 *
+       (6. * e2 * (-2070667. + 126. * q2 * (-2975. + 4009. * Y2)) + 8. * (-286397. + 63. * q2 * (-3179. + 5869. * Y2)) +
+        e4 * (-3506201. + 63. * q2 * (-3191. + 9009. * Y2)));
+  double c6 = 241.02948298890263 - 82283. * kEulerGamma / 1995. + 769. * kPi2Trunc / 57. + 180255. * q2 / 8512. -
+              11809. * kPi * q * Y / 152. + 598987. * q2 * Y2 / 8512. - 11021. * l2 / 285. - 234009. * l3 / 5320.;
+  c6 += e2 * (1048.5728116817568 - 297674. * kEulerGamma / 1995. + 2782. * kPi2Trunc / 57. + 536653. * q2 / 8512. -
+              91375. * kPi * q * Y / 608. + 356845. * q2 * Y2 / 8512. - 2982946. * l2 / 1995. + 1638063. * l3 / 3040.);
+  c6 += e4 * (725.9069951397873 - 1147147. * kEulerGamma / 15960. + 10721. * kPi2Trunc / 456. + 56509. * q2 / 9728. -
+              1739605. * kPi * q * Y / 29184. + 3248951. * q2 * Y2 / 68096. + 760314287. * l2 / 47880. -
+              1022385321. * l3 / 340480. - 1044921875. * l5 / 204228.);
+  c6 -= 107. * (6152. + 22256. * e2 + 10721. * e4) * std::log(v) / 15960.;
+  s += 2451456. * v6 * c6;
+  return -(e * std::pow(1. - e2, 1.5) * m * v6 * v2 * s) / (120960. * M * M);
+}
+
+// Two-term least squares of y[i+1]-y[0] on (x[i+1]-x[0], (x[i+1]-x[0])^2)
+// (KSParMap.cc:500-530), column-scaled normal equations in long double.
+void polyfit(double *coeff, const double *x, const double *y, int n) {
+  long double s1 = 0;
+  for (int i = 0; i < n - 1; ++i) s1 = std::max(s1, std::fabs((long double)(x[i + 1] - x[0])));
+  if (s1 == 0) s1 = 1;
+  const long double s2 = s1 * s1;
+  long double a11 = 0, a12 = 0, a22 = 0, b1 = 0, b2 = 0;
+  for (int i = 0; i < n - 1; ++i) {
+    const long double d = (long double)(x[i + 1] - x[0]);
+    const long double c1 = d / s1, c2 = (d * d) / s2, r = (long double)(y[i + 1] - y[0]);
+    a11 += c1 * c1;
+    a12 += c1 * c2;
+    a22 += c2 * c2;
+    b1 += c1 * r;
+    b2 += c2 * r;
+  }
+  const long double det = a11 * a22 - a12 * a12;
+  coeff[0] = (double)(((b1 * a22 - b2 * a12) / det) / s1);
+  coeff[1] = (double)(((a11 * b2 - a12 * b1) / det) / s2);
+}
+
+inline double p_of(double v, double e, double coslam, double S, double M, double M_phys) {
+  return (1. - e * e) * std::pow(omega_phi(v, e, coslam, S, M) * M_phys * kMsunSec, -2. / 3.);
+}
+}  // namespace
+
+int plan_source(const WaveInputs &w, SourcePlan *plan) {
+  plan->status = kOk;
+  const int vlength = w.vlength, steps = w.steps;
+  const double timestep = w.timestep;
+  if (steps < 3) return plan->status = kErrTooFewSteps;
+  const double *par = w.par;
+  const double mu = par[0], M0 = par[1], S0 = par[2], e0 = par[3], v0 = w.v_map[0];
+  const double coslam = std::cos(par[4]);
+  const double *dt_map = w.dt_map;
+  const double dt_large = dt_map[1];
+  if (!(dt_large > 0)) return plan->status = kErrInvalidParam;
+  const double j0d = (vlength * timestep - dt_map[steps - 1]) / dt_large + steps + 1;
+  if (!(j0d < 1.0e9)) return plan->status = kErrCapacity;
+  const int j0 = (int)j0d;
+  int j_start = j0, j_min = j_start, j_end = 2 * j0 - 1, j_max = j_end, j_max_temp = j_max;
+  double t_end = vlength * timestep;
+  const size_t nA = (size_t)(2 * j0);
+  std::vector<double> e_AK(nA), v_AK(nA), t_fit(nA), e_fit(nA), v_fit(nA), M_fit(nA), S_fit(nA);
+  double edot = 0, vdot = 0, edotm, vdotm;
+
+  // AB2 of the AK equations over the fit window
+  e_AK[j0] = e0;
+  v_AK[j0] = v0;
+  for (int j = j0; j < j0 + steps - 1; ++j) {
+    edotm = edot;
+    vdotm = vdot;
+    edot = dedt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+    vdot = dvdt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+    if (j == j0) {
+      edotm = edot;
+      vdotm = vdot;
+    }
+    const double h = dt_map[j - j0 + 1] - dt_map[j - j0];
+    e_AK[j + 1] = e_AK[j] + (1.5 * edot - .5 * edotm) * h;
+    v_AK[j + 1] = v_AK[j] + (1.5 * vdot - .5 * vdotm) * h;
+    if (e_AK[j + 1] < 0. || v_AK[j + 1] < v_AK[j] || std::isnan(e_AK[j + 1]) || std::isnan(v_AK[j + 1])) {
+      if (j_max == j_max_temp) j_max = j;
+      e_AK[j + 1] = e_AK[j_max];
+      v_AK[j + 1] = v_AK[j_max];
+    }
+  }
+  j_max_temp = j_max;
+
+  // quadratic corrections (Kerr-mapped minus AK)
+  int points = std::min(steps, j_max - j0 + 1);
+  while (points >= 2 && w.e_traj[points - 1] > w.e_traj[points - 2]) points--;
+  if (points < 3) return plan->status = kErrFitTooCloseToPlunge;
+  std::vector<double> e_diff(points), v_diff(points);
+  for (int i = 0; i < points; ++i) {
+    e_diff[i] = w.e_traj[i] - e_AK[i + j0];
+    v_diff[i] = w.v_map[i] - v_AK[i + j0];
+  }
+  double ec[2], vc[2], Mc[2], Sc[2];
+  polyfit(ec, dt_map, e_diff.data(), points);
+  polyfit(vc, dt_map, v_diff.data(), points);
+  polyfit(Mc, dt_map, w.M_map, points);
+  polyfit(Sc, dt_map, w.S_map, points);
+
+  // AB2 beyond the fit window
+  for (int j = j0 + steps - 1; j < j_end; ++j) {
+    edotm = edot;
+    vdotm = vdot;
+    edot = dedt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+    vdot = dvdt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+    e_AK[j + 1] = e_AK[j] + (1.5 * edot - .5 * edotm) * dt_large;
+    v_AK[j + 1] = v_AK[j] + (1.5 * vdot - .5 * vdotm) * dt_large;
+    if (e_AK[j + 1] < 0. || v_AK[j + 1] < v_AK[j] || std::isnan(e_AK[j + 1]) || std::isnan(v_AK[j + 1])) {
+      if (j_max == j_max_temp) j_max = j;
+      e_AK[j + 1] = e_AK[j_max];
+      v_AK[j + 1] = v_AK[j_max];
+    }
+  }
+  j_max_temp = j_max;
+
+  // fitted trajectory with freezing once it turns unphysical
+  for (int j = j0; j <= j_end; ++j) {
+    const double dt = (j < j0 + steps) ? dt_map[j - j0] : dt_map[steps - 1] + dt_large * (j - j0 - steps + 1);
+    const double dt2 = dt * dt;
+    t_fit[j] = dt;
+    e_fit[j] = e_AK[j] + ec[0] * dt + ec[1] * dt2;
+    v_fit[j] = v_AK[j] + vc[0] * dt + vc[1] * dt2;
+    M_fit[j] = M0 + (Mc[0] * dt + Mc[1] * dt2) * kMsunSec;
+    S_fit[j] = S0 + Sc[0] * dt + Sc[1] * dt2;
+    if (e_fit[j] < 0. || v_fit[j] < v_fit[std::max(j0, j - 1)]) {
+      if (j_max == j_max_temp) j_max = j - 1;
+      e_fit[j] = e_fit[j_max];
+      v_fit[j] = v_fit[j_max];
+      M_fit[j] = M_fit[j_max];
+      S_fit[j] = S_fit[j_max];
+    }
+  }
+  j_max_temp = j_max;
+
+  // plunge search: LSO bracket then stability bisection (AAK.cc:148-173)
+  const double M_phys = w.M_phys, S_phys = w.S_phys;
+  const int j_RR = (int)((kMsunSec * M_phys * kMsunSec * M_phys / mu) / dt_large) + 1;
+  const double z1 = 1. + std::pow(1. - S_phys * S_phys, 1. / 3.) * (std::pow(1. + S_phys, 1. / 3.) + std::pow(1. - S_phys, 1. / 3.));
+  const double z2 = std::sqrt(3. * S_phys * S_phys + z1 * z1);
+  const double LSO_min = 3. + z2 - std::sqrt((3. - z1) * (3. + z1 + 2. * z2));
+  const double LSO_max = 3. + z2 + std::sqrt((3. - z1) * (3. + z1 + 2. * z2));
+  for (int j = j0; j <= j_max_temp; ++j) {
+    if (j > j_max) break;
+    const double pj = p_of(v_fit[j], e_fit[j], coslam, S_fit[j], M_fit[j], M_phys);
+    if (pj < LSO_min && j_max == j_max_temp) {
+      j_min = std::max(j - j_RR, j0);
+      j_max = std::min(j + 1, j_max_temp);
+    }
+    if (j > j0 && (j - j0) % j_RR == 0 && pj < LSO_max && j_max == j_max_temp) {
+      j_min = std::max(j - j_RR, j0);
+      KerrGeodesic g;
+      g.set_full(pj, e_fit[j], coslam, S_phys);
+      if (g.stable == -1 || g.E > 1) j_max = std::min(j + 1, j_max_temp);
+    }
+  }
+  while (j_max - j_min > 1) {
+    const int j_mid = (j_max + j_min) / 2;
+    const double pm = p_of(v_fit[j_mid], e_fit[j_mid], coslam, S_fit[j_mid], M_fit[j_mid], M_phys);
+    KerrGeodesic g;
+    g.set_full(pm, e_fit[j_mid], coslam, S_phys);
+    if (g.stable == -1 || g.E > 1) j_max = j_mid;
+    else j_min = j_mid;
+  }
+
+  // optional backward extension (AAK.cc:176-209)
+  if (w.backint) {
+    j_end = j_max;
+    t_end = std::min(t_fit[j_end], vlength * timestep);
+    j_start = j0 + (int)std::floor((t_end - vlength * timestep) / dt_large);
+    if (j_start < 0) return plan->status = kErrCapacity;
+    double edotp, vdotp;
+    for (int j = j0; j > j_start; --j) {
+      edotp = edot;
+      vdotp = vdot;
+      edot = dedt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+      vdot = dvdt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+      if (j == j0) {
+        edotp = edot;
+        vdotp = vdot;
+      }
+      e_AK[j - 1] = e_AK[j] - (1.5 * edot - .5 * edotp) * dt_large;
+      v_AK[j - 1] = v_AK[j] - (1.5 * vdot - .5 * vdotp) * dt_large;
+    }
+    for (int j = j_start; j < j0; ++j) {
+      const double dtu = dt_large * (j - j0);
+      const double dt = (j > j0 - points) ? (dtu + dtu * (j - j0 + points) / points) / 2. : -dt_large * points / 2.;
+      const double dt2 = dt * dt;
+      t_fit[j] = dtu;
+      e_fit[j] = e_AK[j] + ec[0] * dt + ec[1] * dt2;
+      v_fit[j] = v_AK[j] + vc[0] * dt + vc[1] * dt2;
+      M_fit[j] = M0 + (Mc[0] * dt + Mc[1] * dt2) * kMsunSec;
+      S_fit[j] = S0 + Sc[0] * dt + Sc[1] * dt2;
+    }
+  }
+
+  // knots and natural-spline coefficients of (e, v, M, S)
+  const int n_in = j_end - j_start + 1;
+  plan->knot_t.assign(t_fit.begin() + j_start, t_fit.begin() + j_end + 1);
+  plan->knot_y.resize((size_t)n_in * 4);
+  plan->knot_c.resize((size_t)n_in * 4);
+  double e_max = 0.0;
+  for (int k = 0; k < n_in; ++k) {
+    plan->knot_y[4 * k + 0] = e_fit[j_start + k];
+    plan->knot_y[4 * k + 1] = v_fit[j_start + k];
+    plan->knot_y[4 * k + 2] = M_fit[j_start + k];
+    plan->knot_y[4 * k + 3] = S_fit[j_start + k];
+    e_max = std::max(e_max, e_fit[j_start + k]);
+  }
+  for (int q = 0; q < 4; ++q)
+    spline_second_derivs(plan->knot_t.data(), plan->knot_y.data() + q, n_in, 4, plan->knot_c.data() + q);
+
+  const int i0 = vlength - (int)(t_end / timestep);
+  plan->vlength = vlength;
+  plan->i0 = i0;
+  plan->dt = timestep;
+  plan->t_first = plan->knot_t[0];
+  plan->t_last = plan->knot_t[n_in - 1];
+  plan->nmodes = w.nmodes;
+  plan->e_max = std::min(e_max * 1.0001 + 1e-6, 0.9999);
+
+  // plunge index and the 10-orbit buffer (AAK.cc:240-242)
+  const int ip = (j_max == j_max_temp) ? vlength - 1 : i0 + (int)(t_fit[j_min] / timestep);
+  if (ip < 0 || ip >= vlength) return plan->status = kErrInvalidParam;
+  const double t_ip = (ip == 0) ? plan->t_first : (ip - i0) * timestep;
+  const double *kt = plan->knot_t.data(), *ky = plan->knot_y.data(), *kc = plan->knot_c.data();
+  const double e_ip = spline_eval(kt, ky + 0, kc + 0, n_in, 4, t_ip);
+  const double v_ip = spline_eval(kt, ky + 1, kc + 1, n_in, 4, t_ip);
+  const double M_ip = spline_eval(kt, ky + 2, kc + 2, n_in, 4, t_ip);
+  const double S_ip = spline_eval(kt, ky + 3, kc + 3, n_in, 4, t_ip);
+  plan->i_plunge = ip;
+  plan->i_buffer = (int)(10. / (omega_phi(v_ip, e_ip, coslam, S_ip, M_ip) / 2. / kPi) / timestep) + 1;
+
+  // kernel descriptor (batch offsets are filled in by the caller)
+  SourceDesc &d = plan->desc;
+  std::memset(&d, 0, sizeof(d));
+  d.lam = par[4];
+  d.coslam = std::cos(par[4]);
+  d.sinlam = std::sin(par[4]);
+  d.qS = par[7];
+  d.cosqS = std::cos(par[7]);
+  d.sinqS = std::sin(par[7]);
+  d.phiS = par[8];
+  d.qK = par[9];
+  d.cosqK = std::cos(par[9]);
+  d.sinqK = std::sin(par[9]);
+  d.phiK = par[10];
+  d.cosphiK = std::cos(par[10]);
+  d.sinphiK = std::sin(par[10]);
+  d.zeta = w.zeta;
+  d.M_phys_sec = M_phys * kMsunSec;
+  d.dt = timestep;
+  d.t_first = plan->t_first;
+  d.gim0 = par[5];
+  d.Phi0 = par[6];
+  d.alp0 = par[11];
+  d.vlength = vlength;
+  d.n_knots = n_in;
+  d.i0 = i0;
+  d.i_plunge = ip;
+  d.i_buffer = plan->i_buffer;
+  d.nmodes = w.nmodes;
+  d.mich = w.mich ? 1 : 0;
+  d.status = kOk;
+  return kOk;
+}
+
+}  // namespace aak

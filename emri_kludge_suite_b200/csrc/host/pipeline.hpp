@@ -1,0 +1,114 @@
+// pipeline.hpp -- host half of the AAK waveform: parameter record, the front
+// end (coarse Kerr inspiral -> Kerr frequencies -> Kerr-to-AK parameter map)
+// and the coarse AK evolution that yields the spline knots the dense kernels
+// interpolate.  Everything here is re-entrant (no static state).
+#pragma once
+
+#include <stdint.h>
+
+#include <vector>
+
+#include "../aak_common.hpp"
+
+namespace aak {
+
+// Status codes returned through the C-ABI (mirrored in include/aak.h).
+enum Status : int32_t {
+  kOk = 0,
+  kErrInvalidParam = 1,
+  kErrUnstableStart = 2,       // p0 inside the last stable orbit
+  kErrFitTooCloseToPlunge = 3, // fewer than three usable fit points
+  kErrSolverNoConverge = 4,    // Kerr->AK map did not converge
+  kErrCuda = 5,
+  kErrNoMemory = 6,
+  kErrTooFewSteps = 7,         // coarse inspiral produced < 3 points
+  kErrCapacity = 8,            // request larger than a fixed-size buffer
+};
+
+// Numeric fields of the reference SetPar record (include/KSTools.h:21-53).
+struct Params {
+  int64_t length;
+  double dt, p, T, f, T_fit, mu, M, s, e, iota, gamma, psi, theta_S, phi_S, theta_K, phi_K, alpha, D;
+  int32_t backint, LISA;
+};
+
+constexpr int kMaxCoarseSteps = 100;  // the reference's maxsteps (AAKpy.cc:23)
+
+// What the reference front end hands to GenWave (AAKpy.cc:20-44).
+struct MappedTrajectory {
+  int steps = 0;
+  double e_traj[kMaxCoarseSteps];
+  double v_map[kMaxCoarseSteps];
+  double M_map[kMaxCoarseSteps];
+  double s_map[kMaxCoarseSteps];
+  double dt_map[kMaxCoarseSteps];
+  double Phi0 = 0;
+  int inspiral_flag = 0;
+  int newton_iterations = 0;  // total Kerr->AK Newton iterations over all points
+};
+
+// Kerr fundamental frequencies at each coarse inspiral point, for callers
+// that want to solve the map themselves (e.g. with a learned warm start).
+struct CoarseKerr {
+  int steps = 0;
+  double t_rr[kMaxCoarseSteps], p[kMaxCoarseSteps], e[kMaxCoarseSteps], cosi[kMaxCoarseSteps];
+  double Omega[kMaxCoarseSteps][3];
+  int inspiral_flag = 0;
+};
+
+int validate(const Params &P);
+int coarse_kerr(const Params &P, CoarseKerr *out);
+
+// Kerr -> AK map at one point (KSParMap.cc:397-440): solve for
+// x = (v_map, M_map, s_map).  x0 == nullptr uses the reference's initial
+// guess (1/sqrt(p), M, s).  Returns Newton iterations (< 0 on failure).
+int parmap(const double Omega[3], double p, double M, double s, double e, double iota, const double *x0, double map[3]);
+
+// Initial mean anomaly from the initial true anomaly psi (KSParMap.cc:25).
+double initial_mean_anomaly(double e, double psi);
+
+// Full front end (AAKpy.cc:20-44).  warm (optional, steps x 3) seeds the map.
+int front_end(const Params &P, MappedTrajectory *out, const double *warm = nullptr);
+
+// Inputs of the reference GenWave/waveform (AAK.cc:321, 565).
+struct WaveInputs {
+  double timestep;
+  int vlength;
+  int nmodes;
+  double zeta;
+  double par[12];
+  const double *e_traj, *v_map, *M_map, *S_map, *dt_map;
+  double M_phys, S_phys;
+  int steps;
+  int backint;
+  int mich;
+};
+
+// Pack GenWave's par[12], zeta and harmonic count (AAK.cc:565-591).
+void genwave_inputs(const Params &P, const MappedTrajectory &mt, int nmodes_override, WaveInputs *w);
+
+// Coarse AK evolution and spline knots (AAK.cc:27-242): everything of
+// PNevolution except the dense loops, which the kernels perform.
+struct SourcePlan {
+  int status = kOk;
+  int vlength = 0;
+  int i0 = 0, i_plunge = 0, i_buffer = 0;
+  int nmodes = 0;
+  double dt = 0, t_first = 0, t_last = 0;
+  double e_max = 0;
+  std::vector<double> knot_t;   // n_knots
+  std::vector<double> knot_y;   // n_knots x 4 (e, v, M, S)
+  std::vector<double> knot_c;   // n_knots x 4 (natural-spline half second derivatives)
+  SourceDesc desc;              // offsets filled in by the batch builder
+};
+
+int plan_source(const WaveInputs &w, SourcePlan *plan);
+
+// Natural cubic spline helpers (shared by the plan and tests).
+void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c);
+double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv);
+
+// Miller start order for J_{n-2..n+2}(n e) accurate to ~1e-17 for all e <= e_max.
+int bessel_start_order(int n, double e_max);
+
+}  // namespace aak

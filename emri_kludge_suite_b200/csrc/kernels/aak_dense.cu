@@ -1,0 +1,703 @@
+// aak_dense.cu -- sm_100a kernels for the dense part of the AAK waveform:
+// spline interpolation of the coarse (e, v, M, S) trajectory, the
+// Adams-Bashforth-2 phase accumulation (gamma~, Phi, alpha) as a two-pass
+// tiled scan, and the Peters-Mathews harmonic sum with the LISA h_I/h_II
+// response and the Planck taper.  Reference semantics: src/suite/AAK.cc:213-547.
+//
+// Pass 1 (k_phase_tiles):  per 1024-sample tile, the sums of the AB2
+//   increments (no dense arrays are materialised).
+// Carry (k_phase_carry):   per source, exclusive tile prefixes in
+//   double-double arithmetic.
+// Pass 2 (k_waveform_fp64): persistent CTAs pull tiles from a work queue,
+//   recompute the rates, scan the increments inside the tile, and evaluate the
+//   harmonic sum in FP64; h_I, h_II are written with coalesced stores.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "aak_dense.cuh"
+
+namespace aak {
+namespace {
+
+constexpr double kTwoPi = 2.0 * kPi;
+constexpr double kHalfSqrt3 = 0.86602540378443864676;
+
+// ------------------------------------------------------------------ small helpers
+__device__ __forceinline__ int find_source(const int64_t *tile_start, int nsrc, int64_t g) {
+  int lo = 0, hi = nsrc;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (tile_start[mid] <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int find_knot(const double *kt, int n, double t) {
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (kt[mid] > t) hi = mid;
+    else lo = mid;
+  }
+  return lo;
+}
+
+struct Traj4 {
+  double e, v, M, S;
+};
+
+__device__ __forceinline__ double piece(double y0, double y1, double c0, double c1, double h, double dx) {
+  const double b = (y1 - y0) / h - h * (c1 + 2.0 * c0) / 3.0;
+  const double d = (c1 - c0) / (3.0 * h);
+  return y0 + dx * (b + dx * (c0 + dx * d));
+}
+
+__device__ __forceinline__ Traj4 spline4(const BatchView &bv, const SourceDesc &d, double t) {
+  const double *kt = bv.knot_t + d.knot_offset;
+  const int k = find_knot(kt, d.n_knots, t);
+  const double x0 = kt[k], x1 = kt[k + 1];
+  const double h = x1 - x0, dx = t - x0;
+  const double4 y0 = bv.knot_y[d.knot_offset + k], y1 = bv.knot_y[d.knot_offset + k + 1];
+  const double4 c0 = bv.knot_c[d.knot_offset + k], c1 = bv.knot_c[d.knot_offset + k + 1];
+  Traj4 q;
+  q.e = piece(y0.x, y1.x, c0.x, c1.x, h, dx);
+  q.v = piece(y0.y, y1.y, c0.y, c1.y, h, dx);
+  q.M = piece(y0.z, y1.z, c0.z, c1.z, h, dx);
+  q.S = piece(y0.w, y1.w, c0.w, c1.w, h, dx);
+  return q;
+}
+
+// gamma~dot, Phidot, alphadot (AAK.cc:251-253)
+__device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q, double r[3]) {
+  const double tm = pn_dtdm(q.v, q.e, d.coslam, q.S);
+  const double rm = pn_drdm(q.v, q.e, d.coslam, q.S);
+  const double thm = pn_dthetadm(q.v, q.e, d.coslam, q.S);
+  const double phm = pn_dphidm(q.v, q.e, d.coslam, q.S);
+  r[0] = (thm - rm) / tm / q.M;
+  r[1] = rm / tm / q.M;
+  r[2] = (phm - thm) / tm / q.M;
+}
+
+__device__ __forceinline__ double sample_time(const SourceDesc &d, int i) {
+  return (i == 0) ? d.t_first : (double)(i - d.i0) * d.dt;
+}
+
+// samples whose phases feed the output (the rest are zero after the taper)
+__device__ __forceinline__ int n_eff(const SourceDesc &d) {
+  const long long e = (long long)d.i_plunge + (long long)d.i_buffer;
+  return (int)min((long long)d.vlength, e);
+}
+
+// error-free transformation for double-double accumulation
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &err) {
+  s = a + b;
+  const double bb = s - a;
+  err = (a - (s - bb)) + (b - bb);
+}
+__device__ __forceinline__ void dd_add(double &hi, double &lo, double x) {
+  double s, e;
+  two_sum(hi, x, s, e);
+  e += lo;
+  hi = s + e;
+  lo = e - (hi - s);
+}
+
+// block-wide sum over 256 threads (all threads get the result)
+__device__ __forceinline__ double block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTileThreads / 32; ++k) s += red[k];
+  return s;
+}
+
+// block-wide inclusive scan over 256 threads
+__device__ __forceinline__ double block_scan(double v, double *red, double &total) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double n = __shfl_up_sync(0xffffffffu, v, o);
+    if (l >= o) v += n;
+  }
+  __syncthreads();
+  if (l == 31) red[w] = v;
+  __syncthreads();
+  double pre = 0.0, tot = 0.0;
+#pragma unroll
+  for (int k = 0; k < kTileThreads / 32; ++k) {
+    const double r = red[k];
+    if (k < w) pre += r;
+    tot += r;
+  }
+  total = tot;
+  return v + pre;
+}
+
+// ------------------------------------------------------------------ tile geometry
+struct TileCtx {
+  int s;        // source
+  int start;    // first sample of the tile
+  int end;      // one past the last sample of the tile
+  int neff;     // samples feeding the output
+  int64_t lt;   // tile index inside the source
+};
+
+__device__ __forceinline__ TileCtx tile_ctx(const BatchView &bv, int64_t g, const SourceDesc *&dp) {
+  TileCtx c;
+  c.s = find_source(bv.tile_start, bv.nsrc, g);
+  dp = bv.src + c.s;
+  c.lt = g - bv.tile_start[c.s];
+  c.start = (int)(c.lt * kTileSamples);
+  c.end = min(c.start + kTileSamples, dp->vlength);
+  c.neff = n_eff(*dp);
+  return c;
+}
+
+// Clamped Phidot (AAK.cc:254): P_i = raw_i if raw_i > 0, else the previous
+// P.  Represented as a + b*C, where C is the clamped rate just before the tile.
+struct Lin {
+  double a, b;
+};
+
+// ------------------------------------------------------------------ pass 1
+__global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
+  __shared__ double s_raw[kTileThreads];
+  __shared__ double s_Pa[kTileThreads], s_Pb[kTileThreads];
+  __shared__ double s_r[3][kTileThreads];
+  __shared__ double red[kTileThreads / 32];
+  __shared__ double s_bc[4];
+  const int tid = threadIdx.x;
+  for (int64_t g = blockIdx.x; g < bv.total_tiles; g += gridDim.x) {
+    const SourceDesc *dp;
+    const TileCtx c = tile_ctx(bv, g, dp);
+    const SourceDesc &d = *dp;
+    if (d.status != 0) continue;
+    double fA[3] = {0, 0, 0}, fB = 0.0, bA[3] = {0, 0, 0};
+    // rate just before the tile (concrete unless non-positive for Phi)
+    if (tid == 0) {
+      double rp[3] = {0, 0, 0};
+      const int ip = c.start - 1;
+      if (ip >= 0 && ip < d.vlength) phase_rates(d, spline4(bv, d, sample_time(d, ip)), rp);
+      s_bc[0] = rp[0];
+      s_bc[1] = rp[1];
+      s_bc[2] = rp[2];
+    }
+    __syncthreads();
+    double prev[3] = {s_bc[0], 0.0, s_bc[2]};
+    Lin prevP = (s_bc[1] > 0.0) ? Lin{s_bc[1], 0.0} : Lin{0.0, 1.0};
+    Lin lastP = prevP;
+    for (int ch = 0; ch < kTileChunks; ++ch) {
+      const int i = c.start + ch * kTileThreads + tid;
+      const bool in = i < c.end && i < c.neff;
+      const bool vf = in && i >= d.i0;
+      const bool vb = in && i >= 1 && i <= d.i0;
+      double r[3] = {0, 0, 0};
+      if (vf || vb) phase_rates(d, spline4(bv, d, sample_time(d, i)), r);
+      s_raw[tid] = vf ? r[1] : -1.0;
+      s_r[0][tid] = r[0];
+      s_r[1][tid] = r[1];
+      s_r[2][tid] = r[2];
+      __syncthreads();
+      // clamp
+      Lin P = {r[1], 0.0};
+      if (vf && !(r[1] > 0.0)) {
+        int k = tid - 1;
+        while (k >= 0 && !(s_raw[k] > 0.0)) --k;
+        P = (k >= 0) ? Lin{s_raw[k], 0.0} : lastP;
+      }
+      s_Pa[tid] = P.a;
+      s_Pb[tid] = P.b;
+      __syncthreads();
+      const Lin Pm = (tid > 0) ? Lin{s_Pa[tid - 1], s_Pb[tid - 1]} : lastP;
+      if (vf) {
+        if (i == d.i0) {
+          fA[0] += r[0] * d.dt;
+          fA[1] += P.a * d.dt;
+          fB += P.b * d.dt;
+          fA[2] += r[2] * d.dt;
+        } else {
+          const double rm0 = (tid > 0) ? s_r[0][tid - 1] : prev[0];
+          const double rm2 = (tid > 0) ? s_r[2][tid - 1] : prev[2];
+          fA[0] += (1.5 * r[0] - .5 * rm0) * d.dt;
+          fA[1] += (1.5 * P.a - .5 * Pm.a) * d.dt;
+          fB += (1.5 * P.b - .5 * Pm.b) * d.dt;
+          fA[2] += (1.5 * r[2] - .5 * rm2) * d.dt;
+        }
+      }
+      if (vb) {
+        double rn[3];
+        if (i == d.i0) {
+          bA[0] += r[0] * d.dt;
+          bA[1] += r[1] * d.dt;
+          bA[2] += r[2] * d.dt;
+        } else {
+          if (tid < kTileThreads - 1) {
+            rn[0] = s_r[0][tid + 1];
+            rn[1] = s_r[1][tid + 1];
+            rn[2] = s_r[2][tid + 1];
+          } else {
+            phase_rates(d, spline4(bv, d, sample_time(d, i + 1)), rn);
+          }
+          bA[0] += (1.5 * r[0] - .5 * rn[0]) * d.dt;
+          bA[1] += (1.5 * r[1] - .5 * rn[1]) * d.dt;
+          bA[2] += (1.5 * r[2] - .5 * rn[2]) * d.dt;
+        }
+      }
+      // carry chunk state: clamped P and raw rates of the last thread
+      const Lin P255 = {s_Pa[kTileThreads - 1], s_Pb[kTileThreads - 1]};
+      const int ilast = c.start + ch * kTileThreads + kTileThreads - 1;
+      if (ilast >= d.i0) lastP = P255;
+      prev[0] = s_r[0][kTileThreads - 1];
+      prev[2] = s_r[2][kTileThreads - 1];
+      __syncthreads();
+    }
+    // reductions
+    TileSummary &ts = bv.summ[g];
+    for (int q = 0; q < 3; ++q) {
+      const double a = block_sum(fA[q], red);
+      if (tid == 0) ts.fA[q] = a;
+      const double b = block_sum(bA[q], red);
+      if (tid == 0) ts.bA[q] = b;
+    }
+    const double fb = block_sum(fB, red);
+    if (tid == 0) {
+      ts.fB[0] = 0.0;
+      ts.fB[1] = fb;
+      ts.fB[2] = 0.0;
+      ts.bB[0] = ts.bB[1] = ts.bB[2] = 0.0;
+      // last clamped Phidot in the tile if concrete
+      const int last_f = min(c.end, c.neff) - 1;
+      ts.has_last[1] = (last_f >= max(c.start, d.i0) && lastP.b == 0.0) ? 1 : 0;
+      ts.last_rate[1] = lastP.a;
+      ts.has_last[0] = ts.has_last[2] = 0;
+      ts.last_rate[0] = ts.last_rate[2] = 0.0;
+      ts.first_rate[0] = ts.first_rate[1] = ts.first_rate[2] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ carry
+// One CTA per source walks its tiles in order (a handful of thousand at most).
+__global__ void __launch_bounds__(32) k_phase_carry(BatchView bv) {
+  const int s = blockIdx.x;
+  if (s >= bv.nsrc || threadIdx.x != 0) return;
+  const SourceDesc &d = bv.src[s];
+  const int64_t t0 = bv.tile_start[s], t1 = bv.tile_start[s + 1];
+  if (d.status != 0) return;
+  double fh[3] = {0, 0, 0}, fl[3] = {0, 0, 0};
+  double C = 0.0;  // clamped Phidot before the tile
+  for (int64_t g = t0; g < t1; ++g) {
+    TileCarry &tc = bv.carry[g];
+    const TileSummary &ts = bv.summ[g];
+    for (int q = 0; q < 3; ++q) {
+      tc.fwd_hi[q] = fh[q];
+      tc.fwd_lo[q] = fl[q];
+    }
+    tc.Cf[0] = 0.0;
+    tc.Cf[1] = C;
+    tc.Cf[2] = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      const double tot = ts.fA[q] + ts.fB[q] * C;
+      dd_add(fh[q], fl[q], tot);
+    }
+    if (ts.has_last[1]) C = ts.last_rate[1];
+  }
+  double bh[3] = {0, 0, 0}, bl[3] = {0, 0, 0};
+  for (int64_t g = t1 - 1; g >= t0; --g) {
+    TileCarry &tc = bv.carry[g];
+    const TileSummary &ts = bv.summ[g];
+    for (int q = 0; q < 3; ++q) {
+      tc.bwd_hi[q] = bh[q];
+      tc.bwd_lo[q] = bl[q];
+      tc.Cb[q] = 0.0;
+      dd_add(bh[q], bl[q], ts.bA[q]);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ Bessel functions
+// J_{lo..lo+4}(x) for x > 0 (lo = n-2 for n >= 2; lo = 0 for n = 1).
+// x < 1: power series.  x >= 1: Miller's backward recurrence from the
+// host-chosen start order, renormalised at J_lo, normalised by
+// J_0 + 2 sum_k J_2k = 1.
+__device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double J[5]) {
+  if (x < 1.0) {
+    const double hx = 0.5 * x, q = -hx * hx;
+    double pref = exp((double)lo * log(hx) - lgamma((double)lo + 1.0));
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      const double nu = (double)(lo + m);
+      double term = 1.0, sum = 1.0;
+#pragma unroll 1
+      for (int k = 1; k < 14; ++k) {
+        term *= q / ((double)k * (nu + (double)k));
+        sum += term;
+      }
+      J[m] = pref * sum;
+      pref *= hx / (nu + 1.0);
+    }
+    return;
+  }
+  const double tx = 2.0 / x;
+  const int hi = lo + 4;
+  double jk = 1.0e-300, jk1 = 0.0;  // J_k, J_{k+1} (unnormalised), k = start (even)
+  double sum = 2.0 * jk, w = 0.0;   // w: weight 2 for even orders produced next
+  int k = start;
+  // phase 1: down to order hi + 1
+#pragma unroll 2
+  for (; k > hi + 1; --k) {
+    const double jm = (double)k * tx * jk - jk1;
+    jk1 = jk;
+    jk = jm;
+    sum = fma(w, jm, sum);
+    w = 2.0 - w;
+  }
+  // phase 2: orders hi .. lo
+  double v[5];
+#pragma unroll
+  for (int m = 4; m >= 0; --m) {
+    const double jm = (double)k * tx * jk - jk1;
+    jk1 = jk;
+    jk = jm;
+    sum = fma(w, jm, sum);
+    w = 2.0 - w;
+    v[m] = jm;
+    --k;
+  }
+  // renormalise at J_lo to keep phase 3 in range
+  const double sc = 1.0 / v[0];
+  jk *= sc;
+  jk1 *= sc;
+  sum *= sc;
+#pragma unroll
+  for (int m = 0; m < 5; ++m) v[m] *= sc;
+  // phase 3: orders lo-1 .. 0 (k == lo here)
+#pragma unroll 2
+  for (; k > 0; --k) {
+    const double jm = (double)k * tx * jk - jk1;
+    jk1 = jk;
+    jk = jm;
+    sum = fma(w, jm, sum);
+    w = 2.0 - w;
+  }
+  // the last produced order is J_0, counted once (its weight was 2 or 0)
+  if (w == 0.0) sum -= jk;       // J_0 was added with weight 2
+  else sum += jk;                // J_0 was added with weight 0
+  const double inv = 1.0 / sum;
+#pragma unroll
+  for (int m = 0; m < 5; ++m) J[m] = v[m] * inv;
+}
+
+// ------------------------------------------------------------------ harmonic sum
+// h_I, h_II at one sample (AAK.cc:409-528) with the modes accumulated as
+// Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
+// rotation and antenna factors applied once per sample.
+__device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, double t, const Traj4 &q, double gim,
+                                  double Phi, double alp, double nu, double gimdot, double &hI, double &hII) {
+  const double e = q.e;
+  const double cosalp = cos(alp), sinalp = sin(alp);
+  const double cosqL = d.cosqK * d.coslam + d.sinqK * d.sinlam * cosalp;
+  const double sinqL = sqrt(1. - cosqL * cosqL);
+  const double phiLup = d.sinqK * d.sinphiK * d.coslam - d.cosphiK * d.sinlam * sinalp - d.cosqK * d.sinphiK * d.sinlam * cosalp;
+  const double phiLdown = d.sinqK * d.cosphiK * d.coslam + d.sinphiK * d.sinlam * sinalp - d.cosqK * d.cosphiK * d.sinlam * cosalp;
+  const double phiL = atan2(phiLup, phiLdown);
+  const double Ldotn = cosqL * d.cosqS + sinqL * d.sinqS * cos(phiL - d.phiS);
+  const double Ldotn2 = Ldotn * Ldotn;
+  const double Sdotn = d.cosqK * d.cosqS + d.sinqK * d.sinqS * cos(d.phiK - d.phiS);
+  const double betaup = -Sdotn + d.coslam * Ldotn;
+  const double betadown = d.sinqS * sin(d.phiK - d.phiS) * d.sinlam * cosalp + (d.cosqK * Sdotn - d.cosqS) / d.sinqK * d.sinlam * sinalp;
+  const double beta = atan2(betaup, betadown);
+  double sin2gam, cos2gam;
+  sincos(2. * (gim + beta), &sin2gam, &cos2gam);
+
+  double cosorbphs = 0.0, FplusI, FcrosI, FplusII, FcrosII, K;
+  if (d.mich) {
+    const double orbphs = kTwoPi * t / kYear;
+    double sinorbphs;
+    sincos(orbphs - d.phiS, &sinorbphs, &cosorbphs);
+    const double cosq = .5 * d.cosqS - kHalfSqrt3 * d.sinqS * cosorbphs;
+    const double phiw = orbphs + atan2(kHalfSqrt3 * d.cosqS + .5 * d.sinqS * cosorbphs, d.sinqS * sinorbphs);
+    const double psiup = .5 * d.cosqK - kHalfSqrt3 * d.sinqK * cos(orbphs - d.phiK) - cosq * Sdotn;
+    double so, co;
+    sincos(orbphs, &so, &co);
+    const double psidown = .5 * d.sinqK * d.sinqS * sin(d.phiK - d.phiS) -
+                           kHalfSqrt3 * co * (d.cosqK * d.sinqS * sin(d.phiS) - d.cosqS * d.sinqK * sin(d.phiK)) -
+                           kHalfSqrt3 * so * (d.cosqS * d.sinqK * cos(d.phiK) - d.cosqK * d.sinqS * cos(d.phiS));
+    const double psi = atan2(psiup, psidown);
+    const double cosq1 = .5 * (1. + cosq * cosq);
+    double sin2phi, cos2phi, sin2psi, cos2psi;
+    sincos(2. * phiw, &sin2phi, &cos2phi);
+    sincos(2. * psi, &sin2psi, &cos2psi);
+    FplusI = cosq1 * cos2phi * cos2psi - cosq * sin2phi * sin2psi;
+    FcrosI = cosq1 * cos2phi * sin2psi + cosq * sin2phi * cos2psi;
+    FplusII = cosq1 * sin2phi * cos2psi + cosq * cos2phi * sin2psi;
+    FcrosII = cosq1 * sin2phi * sin2psi - cosq * cos2phi * cos2psi;
+    K = kHalfSqrt3;
+  } else {
+    const double up_ldc = d.cosqS * d.sinqK * cos(d.phiS - d.phiK) - d.cosqK * d.sinqS;
+    const double dw_ldc = d.sinqK * sin(d.phiS - d.phiK);
+    const double psi_ldc = (dw_ldc != 0.0) ? -atan2(up_ldc, dw_ldc) : 0.5 * kPi;
+    double s2, c2;
+    sincos(2. * psi_ldc, &s2, &c2);
+    FplusI = c2;
+    FcrosI = -s2;
+    FplusII = s2;
+    FcrosII = c2;
+    K = 1.0;
+  }
+  const double Amp = pow(omega_phi(q.v, e, d.coslam, q.S, q.M) * d.M_phys_sec, 2. / 3.) * d.zeta;
+
+  // rotation to the NK wave frame (RotCoeff, KSParMap.cc:532-574): depends on alpha only
+  double rot0, rot1;
+  {
+    const double sqS = d.sinqS, cqS = d.cosqS;
+    const double n0 = sqS * cos(d.phiS), n1 = sqS * sin(d.phiS), n2 = cqS;
+    const double S0 = d.sinqK * d.cosphiK, S1 = d.sinqK * d.sinphiK, S2 = d.cosqK;
+    const double L0 = d.coslam * d.sinqK * d.cosphiK + d.sinlam * (sinalp * d.sinphiK - cosalp * d.cosqK * d.cosphiK);
+    const double L1 = d.coslam * d.sinqK * d.sinphiK - d.sinlam * (sinalp * d.cosphiK + cosalp * d.cosqK * d.sinphiK);
+    const double L2 = d.coslam * d.cosqK + d.sinlam * cosalp * d.sinqK;
+    const double nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
+    const double nS0 = n1 * S2 - n2 * S1, nS1 = n2 * S0 - n0 * S2, nS2 = n0 * S1 - n1 * S0;
+    const double norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * sqrt(nS0 * nS0 + nS1 * nS1 + nS2 * nS2);
+    const double cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
+    const double sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
+    rot0 = 2. * cosrot * cosrot - 1.;
+    rot1 = cosrot * sinrot;
+  }
+  // rot = [rot0, rot1, -rot1, rot0]
+  const double uI = FplusI * rot0 - FcrosI * rot1, wI = FplusI * rot1 + FcrosI * rot0;
+  const double uII = FplusII * rot0 - FcrosII * rot1, wII = FplusII * rot1 + FcrosII * rot0;
+  const double opL2 = 1. + Ldotn2, omL2 = 1. - Ldotn2, twoL = 2. * Ldotn;
+  const double caI = K * (-uI * opL2 * cos2gam + wI * twoL * sin2gam);
+  const double cbI = K * (uI * opL2 * sin2gam + wI * twoL * cos2gam);
+  const double ccI = K * uI * omL2;
+  const double caII = K * (-uII * opL2 * cos2gam + wII * twoL * sin2gam);
+  const double cbII = K * (uII * opL2 * sin2gam + wII * twoL * cos2gam);
+  const double ccII = K * uII * omL2;
+
+  // harmonic phases: n Phi + Doppler_n = n (Phi + D1) + D0
+  double D1 = 0.0, D0 = 0.0;
+  if (d.mich) {
+    D1 = kTwoPi * nu * kAUsec * d.sinqS * cosorbphs;
+    D0 = 2.0 * gimdot * kAUsec * d.sinqS * cosorbphs;
+  }
+  double s1, c1, sD, cD;
+  sincos(Phi + D1, &s1, &c1);
+  sincos(D0, &sD, &cD);
+  double zr = 1.0, zi = 0.0;  // (c1 + i s1)^n
+  const double se = sqrt(1. - e * e);
+  double Sa = 0.0, Sb = 0.0, Sc = 0.0;
+  for (int n = 1; n <= d.nmodes; ++n) {
+    const double tr = zr * c1 - zi * s1;
+    zi = zr * s1 + zi * c1;
+    zr = tr;
+    const double cn = zr * cD - zi * sD;
+    const double sn = zi * cD + zr * sD;
+    double J[5];
+    const double x = n * e;
+    if (n == 1) {
+      double Jt[5];
+      bessel5_fp64(0, x, bstart[0], Jt);
+      J[0] = -Jt[1];
+      J[1] = Jt[0];
+      J[2] = Jt[1];
+      J[3] = Jt[2];
+      J[4] = Jt[3];
+    } else {
+      bessel5_fp64(n - 2, x, bstart[n - 1], J);
+    }
+    const double dn = (double)n;
+    Sa += dn * (J[0] - 2. * e * J[1] + 2. / dn * J[2] + 2. * e * J[3] - J[4]) * cn;
+    Sb += dn * (J[0] - 2. * J[2] + J[4]) * sn;
+    Sc += J[2] * cn;
+  }
+  const double a = -Amp * Sa, b = -Amp * se * Sb, cc = 2. * Amp * Sc;
+  hI = caI * a + cbI * b + ccI * cc;
+  hII = caII * a + cbII * b + ccII * cc;
+}
+
+// ------------------------------------------------------------------ pass 2
+__global__ void __launch_bounds__(kTileThreads) k_waveform_fp64(BatchView bv) {
+  __shared__ double s_raw[kTileThreads];
+  __shared__ double s_Pa[kTileThreads];
+  __shared__ double s_r[3][kTileThreads];
+  __shared__ double red[3][kTileThreads / 32];
+  __shared__ double s_bc[4];
+  __shared__ long long s_tile;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
+    __syncthreads();
+    const long long g = s_tile;
+    __syncthreads();
+    if (g >= bv.total_tiles) break;
+    const SourceDesc *dp;
+    const TileCtx c = tile_ctx(bv, g, dp);
+    const SourceDesc &d = *dp;
+    const int32_t *bstart = bv.bessel_start + d.bessel_offset;
+    const TileCarry &tc = bv.carry[g];
+    const TileSummary &ts = bv.summ[g];
+    const double X0[3] = {d.gim0, d.Phi0, d.alp0};
+    if (d.status != 0) {
+      for (int ch = 0; ch < kTileChunks; ++ch) {
+        const int i = c.start + ch * kTileThreads + tid;
+        if (i < c.end) {
+          bv.hI[d.out_offset + i] = 0.0;
+          bv.hII[d.out_offset + i] = 0.0;
+        }
+      }
+      continue;
+    }
+    if (tid == 0) {
+      double rp[3] = {0, 0, 0};
+      const int ip = c.start - 1;
+      if (ip >= 0 && ip < d.vlength) phase_rates(d, spline4(bv, d, sample_time(d, ip)), rp);
+      s_bc[0] = rp[0];
+      s_bc[1] = rp[1];
+      s_bc[2] = rp[2];
+    }
+    __syncthreads();
+    double prev[3] = {s_bc[0], (s_bc[1] > 0.0) ? s_bc[1] : tc.Cf[1], s_bc[2]};
+    double lastP = prev[1];
+    // running in-tile prefix (forward) and inclusive prefix of backward increments
+    double runF[3] = {0, 0, 0}, runB[3] = {0, 0, 0};
+    const double t_plunge = sample_time(d, d.i_plunge);
+    const double t_zero = t_plunge + d.dt * d.i_buffer;
+    for (int ch = 0; ch < kTileChunks; ++ch) {
+      const int i = c.start + ch * kTileThreads + tid;
+      const bool inrange = i < c.end;
+      const bool in = inrange && i < c.neff;
+      const bool vf = in && i >= d.i0;
+      const bool vb = in && i >= 1 && i <= d.i0;
+      const double t = sample_time(d, i);
+      Traj4 q = {0, 0, 0, 0};
+      double r[3] = {0, 0, 0};
+      if (in) {
+        q = spline4(bv, d, t);
+        phase_rates(d, q, r);
+      }
+      s_raw[tid] = vf ? r[1] : -1.0;
+      s_r[0][tid] = r[0];
+      s_r[1][tid] = r[1];
+      s_r[2][tid] = r[2];
+      __syncthreads();
+      double P = r[1];
+      if (vf && !(r[1] > 0.0)) {
+        int k = tid - 1;
+        while (k >= 0 && !(s_raw[k] > 0.0)) --k;
+        P = (k >= 0) ? s_raw[k] : lastP;
+      }
+      s_Pa[tid] = P;
+      __syncthreads();
+      const double Pm = (tid > 0) ? s_Pa[tid - 1] : lastP;
+      double incF[3] = {0, 0, 0}, incB[3] = {0, 0, 0};
+      if (vf) {
+        if (i == d.i0) {
+          incF[0] = r[0] * d.dt;
+          incF[1] = P * d.dt;
+          incF[2] = r[2] * d.dt;
+        } else {
+          const double rm0 = (tid > 0) ? s_r[0][tid - 1] : prev[0];
+          const double rm2 = (tid > 0) ? s_r[2][tid - 1] : prev[2];
+          incF[0] = (1.5 * r[0] - .5 * rm0) * d.dt;
+          incF[1] = (1.5 * P - .5 * Pm) * d.dt;
+          incF[2] = (1.5 * r[2] - .5 * rm2) * d.dt;
+        }
+      }
+      if (vb) {
+        if (i == d.i0) {
+          incB[0] = r[0] * d.dt;
+          incB[1] = r[1] * d.dt;
+          incB[2] = r[2] * d.dt;
+        } else {
+          double rn[3];
+          if (tid < kTileThreads - 1) {
+            rn[0] = s_r[0][tid + 1];
+            rn[1] = s_r[1][tid + 1];
+            rn[2] = s_r[2][tid + 1];
+          } else {
+            phase_rates(d, spline4(bv, d, sample_time(d, i + 1)), rn);
+          }
+          incB[0] = (1.5 * r[0] - .5 * rn[0]) * d.dt;
+          incB[1] = (1.5 * r[1] - .5 * rn[1]) * d.dt;
+          incB[2] = (1.5 * r[2] - .5 * rn[2]) * d.dt;
+        }
+      }
+      double X[3];
+#pragma unroll
+      for (int qq = 0; qq < 3; ++qq) {
+        double totF, totB;
+        const double inclF = block_scan(incF[qq], red[qq], totF);
+        const double inclB = block_scan(incB[qq], red[qq], totB);
+        if (i > d.i0) {
+          // X_i = X0 + carry + (forward increments of samples < i in this tile)
+          X[qq] = X0[qq] + (tc.fwd_hi[qq] + (tc.fwd_lo[qq] + (runF[qq] + (inclF - incF[qq]))));
+        } else if (i == d.i0) {
+          X[qq] = X0[qq];
+        } else {
+          // X_i = X0 - (backward increments of samples in (i, i0])
+          const double after_in_tile = ts.bA[qq] - (runB[qq] + inclB);
+          X[qq] = X0[qq] - (tc.bwd_hi[qq] + (tc.bwd_lo[qq] + after_in_tile));
+        }
+        runF[qq] += totF;
+        runB[qq] += totB;
+      }
+      // output sample
+      if (inrange) {
+        double hI = 0.0, hII = 0.0;
+        if (in) {
+          const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
+          harmonic_sum_fp64(d, bstart, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
+          if (i > d.i_plunge) {
+            const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
+            hI = hI / wgt;
+            hII = hII / wgt;
+          }
+          if (bv.traj_out) {
+            const int64_t o = d.out_offset + i;
+            const int64_t st = bv.traj_stride;
+            bv.traj_out[0 * st + o] = q.e;
+            bv.traj_out[1 * st + o] = q.v;
+            bv.traj_out[2 * st + o] = q.M;
+            bv.traj_out[3 * st + o] = q.S;
+            bv.traj_out[4 * st + o] = X[0];
+            bv.traj_out[5 * st + o] = X[1];
+            bv.traj_out[6 * st + o] = X[2];
+            bv.traj_out[7 * st + o] = nu;
+            bv.traj_out[8 * st + o] = r[0];
+          }
+        }
+        bv.hI[d.out_offset + i] = hI;
+        bv.hII[d.out_offset + i] = hII;
+        if (bv.t_out) bv.t_out[d.out_offset + i] = t;
+      }
+      // chunk carries
+      const int ilast = c.start + ch * kTileThreads + kTileThreads - 1;
+      if (ilast >= d.i0) lastP = s_Pa[kTileThreads - 1];
+      prev[0] = s_r[0][kTileThreads - 1];
+      prev[2] = s_r[2][kTileThreads - 1];
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace
+
+void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream) {
+  if (bv.total_tiles <= 0) return;
+  const int grid1 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 8);
+  k_phase_tiles<<<grid1, kTileThreads, 0, stream>>>(bv);
+  k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
+  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
+  const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 4);
+  k_waveform_fp64<<<grid2, kTileThreads, 0, stream>>>(bv);
+}
+
+}  // namespace aak

@@ -1,0 +1,59 @@
+// aak_dense.cuh -- device-side layout shared by the dense AAK kernels and
+// their host launcher.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../aak_common.hpp"
+
+namespace aak {
+
+constexpr int kTileThreads = 256;                      // threads per CTA
+constexpr int kTileChunks = 4;                         // 256-sample chunks per tile
+constexpr int kTileSamples = kTileThreads * kTileChunks;  // 1024 samples per tile
+
+// Per-tile partial sums of the Adams-Bashforth-2 phase increments written by
+// pass 1.  For each phase q (0: gamma~, 1: Phi, 2: alpha) the forward sum over
+// the tile is fA[q] + fB[q] * C[q], where C[q] is the (clamped) rate of the
+// sample just before the tile; the backward sum is bA[q] + bB[q] * C'[q] with
+// C'[q] the rate of the sample just after the tile.
+struct TileSummary {
+  double fA[3], fB[3];
+  double bA[3], bB[3];
+  double last_rate[3];   // gim/alp: rate of the last forward sample; Phi: last positive raw rate
+  double first_rate[3];  // raw rates of the first sample in the tile
+  int32_t has_last[3];   // last_rate valid
+  int32_t pad;
+};
+
+// Per-tile carries written by the carry kernel and read by pass 2.
+struct TileCarry {
+  double fwd_hi[3], fwd_lo[3];  // sum of forward increments before the tile (double-double)
+  double bwd_hi[3], bwd_lo[3];  // sum of backward increments after the tile
+  double Cf[3];                 // rate carried into the tile's first forward increment
+  double Cb[3];                 // rate carried into the tile's last backward increment
+};
+
+// Everything the kernels read about a batch.
+struct BatchView {
+  const SourceDesc *src;
+  int32_t nsrc;
+  int64_t total_tiles;
+  const int64_t *tile_start;    // nsrc + 1 prefix of tiles (device)
+  const double *knot_t;         // knots
+  const double4 *knot_y;        // (e, v, M, S) at the knots
+  const double4 *knot_c;        // natural-spline half second derivatives
+  const int32_t *bessel_start;  // Miller start orders, per source x mode
+  TileSummary *summ;
+  TileCarry *carry;
+  double *hI, *hII;             // outputs, indexed by src.out_offset + i
+  double *t_out;                // optional
+  double *traj_out;             // optional dense trajectory, 9 x total samples (e,v,M,S,gim,Phi,alp,nu,gimdot)
+  int64_t traj_stride;
+  unsigned long long *work_counter;  // persistent work queue head (pass 2)
+};
+
+void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream);
+
+}  // namespace aak

@@ -1,0 +1,154 @@
+/*
+ * aak.h -- C ABI of libaak_b200.so, the B200 (sm_100a) implementation of the
+ * augmented analytic kludge (AAK) EMRI waveform and its LISA noise-weighted
+ * inner product.
+ *
+ * Plain C types only.  Every entry point returns an aak_status (0 = OK) and
+ * never terminates the process; the library keeps no global mutable state
+ * besides one lazily created default context per device, so independent
+ * contexts may be used from independent host threads.
+ *
+ * Each declaration names the reference interface it replaces
+ * (alvincjk/EMRI_Kludge_Suite, path:line).
+ */
+#ifndef AAK_B200_H
+#define AAK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum aak_status {
+  AAK_OK = 0,
+  AAK_ERR_INVALID_PARAM = 1,            /* reference: undefined behaviour / Die()      */
+  AAK_ERR_UNSTABLE_START = 2,           /* p0 inside the LSO (GKTrajFast flag -1)      */
+  AAK_ERR_FIT_TOO_CLOSE_TO_PLUNGE = 3,  /* reference: exit(EXIT_FAILURE), AAK.cc:88    */
+  AAK_ERR_SOLVER_NO_CONVERGE = 4,       /* Kerr->AK map did not reach |f|_1 < 1e-6     */
+  AAK_ERR_CUDA = 5,                     /* no usable GPU, or a CUDA/cuFFT call failed  */
+  AAK_ERR_NO_MEMORY = 6,
+  AAK_ERR_TOO_FEW_STEPS = 7,            /* coarse inspiral gave fewer than 3 points    */
+  AAK_ERR_CAPACITY = 8                  /* request exceeds a fixed-size buffer         */
+};
+
+const char *aak_status_string(int status);
+int aak_version(void);
+
+/* ------------------------------------------------------------------ parameters */
+/* Numeric fields of the reference's SetPar (include/KSTools.h:21-53) and the
+ * keys of AAKwrapper.wave's pars dict (AAKwrapper/AAKwrapper.pyx:50-80). */
+typedef struct aak_params {
+  int64_t length; /* waveform samples                               */
+  double dt;      /* sample spacing [s]                             */
+  double p;       /* initial semi-latus rectum [M]                  */
+  double T;       /* duration [yr] (informational, as in SetPar)    */
+  double f;       /* reference GW frequency [Hz] (informational)    */
+  double T_fit;   /* local-fit duration [M^2/mu]                    */
+  double mu;      /* compact-object mass [Msun]                     */
+  double M;       /* black-hole mass [Msun]                         */
+  double s;       /* spin a/M                                       */
+  double e;       /* initial eccentricity                           */
+  double iota;    /* inclination of L from S [rad]                  */
+  double gamma;   /* initial periapsis angle from L x S             */
+  double psi;     /* initial true anomaly                           */
+  double theta_S, phi_S, theta_K, phi_K; /* ecliptic source / spin angles */
+  double alpha;   /* initial azimuthal orientation                  */
+  double D;       /* distance [Gpc]                                 */
+  int32_t backint; /* integrate backwards from plunge              */
+  int32_t LISA;    /* LISA h_I/h_II response (else detector-frame) */
+} aak_params;
+
+/* Output of the front end: the arrays the reference hands to GenWave
+ * (src/suite/AAKpy.cc:29-44).  Arrays hold up to 100 entries. */
+typedef struct aak_mapped {
+  int32_t steps;
+  int32_t inspiral_flag;     /* GKTrajFast::Eccentric return value */
+  int32_t newton_iterations; /* summed over the coarse points      */
+  int32_t pad;
+  double Phi0;               /* initial mean anomaly (ParAng)      */
+  double e_traj[100], v_map[100], M_map[100], s_map[100], dt_map[100];
+} aak_mapped;
+
+/* ------------------------------------------------------------------ host-only stages */
+/* Front end of AAKwave (src/suite/AAKpy.cc:20-44): coarse Kerr inspiral
+ * (GKTrajFast::Eccentric), Kerr frequencies (IEKG::Frequencies), initial mean
+ * anomaly (ParAng) and the Kerr->AK map (ParMap, KSParMap.cc:397-440).
+ * warm_start: optional steps x 3 initial guesses (v_map, M_map, s_map), or NULL. */
+int aak_front_end(const aak_params *p, const double *warm_start, aak_mapped *out);
+
+/* Coarse Kerr inspiral + fundamental frequencies only (no map).
+ * out_t/p/e/cosi/Omega hold up to 100 (Omega: 100 x 3) entries. */
+int aak_coarse_kerr(const aak_params *p, int32_t *steps, double *t_rr, double *pp, double *e, double *cosi,
+                    double *Omega);
+
+/* One Kerr->AK map solve (ParMap, src/suite/KSParMap.cc:397-440); x0 may be NULL
+ * for the reference's initial guess.  *iterations receives the Newton count. */
+int aak_parmap(const double Omega[3], double p, double M, double s, double e, double iota, const double *x0,
+               double map[3], int32_t *iterations);
+
+/* ------------------------------------------------------------------ single-source waveform (GPU) */
+/* Replaces AAKwave (include/AAKpy.h:19, src/suite/AAKpy.cc:16-51).  Host
+ * buffers of p->length doubles.  *seconds (optional) receives the wall time.
+ * Runs on the current CUDA device; fails with AAK_ERR_CUDA without one. */
+int aak_wave(const aak_params *p, double *t, double *hI, double *hII, double *seconds);
+
+/* Replaces GenWave -> waveform (src/suite/AAK.cc:321-591) on an already
+ * mapped trajectory; nmodes_override <= 0 keeps the reference harmonic rule
+ * int(30 e0) (4 below e0 = 0.135).  Host buffers of vlength doubles. */
+int aak_genwave(double *t, double *hI, double *hII, double timestep, int32_t vlength, const double *e_traj,
+                const double *v_map, double M_phys, const double *M_map, double mu, double S_phys, const double *S_map,
+                double dist, double inc, double gim0, double Phi0, double qS, double phiS, double alp0, double qK,
+                double phiK, const double *dt_map, int32_t steps, int32_t backint, int32_t mich,
+                int32_t nmodes_override);
+
+/* ------------------------------------------------------------------ batched waveforms */
+/* A context owns the device buffers of one batch on one device. */
+typedef struct aak_ctx aak_ctx;
+
+int aak_ctx_create(int32_t device, aak_ctx **out);
+void aak_ctx_destroy(aak_ctx *ctx);
+
+/* Host planning of a batch (front end + coarse AK evolution + spline knots),
+ * spread over nthreads host threads (<= 0: all hardware threads).
+ * nmodes_override: per-source harmonic counts (<= 0 entries keep the
+ * reference rule) or NULL.  Per-source failures are reported in the source
+ * status (aak_batch_info) and yield zero waveforms; the call itself fails
+ * only for context-level errors.  Replaces the per-template host loop of
+ * pygpuAAK.pyGPUAAK.NLL (pygpuAAK/pygpuAAK.py:204-232). */
+int aak_batch_plan(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nmodes_override, int32_t nthreads);
+
+/* Plan from already mapped trajectories (one aak_mapped per source). */
+int aak_batch_plan_mapped(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32_t nsrc,
+                          const int32_t *nmodes_override, int32_t nthreads);
+
+/* Batch geometry after planning: offsets (nsrc + 1 prefix of sample counts),
+ * per-source status, plunge index and buffer length; any pointer may be NULL. */
+int aak_batch_info(aak_ctx *ctx, int64_t *total_samples, int64_t *offsets, int32_t *status, int32_t *i_plunge,
+                   int32_t *i_buffer);
+
+/* Copy the planned batch to the device (stream-ordered on `stream`, a
+ * cudaStream_t or NULL for the legacy default stream). */
+int aak_batch_upload(aak_ctx *ctx, void *stream);
+
+/* Run the dense kernels into caller device buffers indexed by offsets:
+ * hI, hII (required), t (optional), traj (optional 9 x traj_stride dense
+ * trajectory e, v, M, S, gamma~, Phi, alpha, nu, gamma~dot; diagnostic).
+ * precision: 0 = FP64 throughout. */
+int aak_batch_run(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_t, double *d_traj, int64_t traj_stride,
+                  int32_t precision, void *stream);
+
+/* Number of CUDA kernels the last aak_batch_run launched. */
+int aak_batch_last_launches(aak_ctx *ctx);
+
+/* End to end with host buffers: plan + upload + run + copy back.
+ * h_hI / h_hII hold total_samples doubles (offsets as from aak_batch_info). */
+int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nmodes_override,
+                        int32_t nthreads, double *h_hI, double *h_hII, int64_t *offsets, int32_t *status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AAK_B200_H */
