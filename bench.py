@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""AAK waveform throughput on B200 (one JSON line on rank 0).
+
+Workload (configuration 1 of the AAK benchmark): 512 sources drawn from a
+fixed seed -- log10 M ~ U(5,7) Msun, mu ~ U(1,100) Msun, a ~ U(0,0.95),
+e0 ~ U(0.05,0.5), cos(iota) ~ U(-1,1), isotropic sky and spin directions,
+phases ~ U(0,2pi), D = 1 Gpc, T ~ U(0.1,1) yr, dt = 10 s, harmonics n = 1..30,
+LISA response, FP64 throughout; p0 chosen so that the source does not plunge
+within T (checked on the planned trajectory, redrawn otherwise).
+
+A step is one pass of the dense AAK path over the whole batch.
+  value : samples/s of the GPU kernels with the planned batch resident in HBM
+  e2e   : samples/s through the C ABI (aak_wave_batch_host) with host
+          parameters in and pinned host waveforms out: host front end and
+          coarse evolution on all host threads, H2D, kernels, D2H
+  --impl reference : the reference's own CPU AAK (oracle/_ref, compiled from
+          its sources) on all host cores, same workload, bounded sample.
+
+Multi-GPU (torchrun, one rank per GPU): every rank generates its own
+512-source batch (seed + rank); no collective on the data path; value is the
+total over ranks divided by the max-over-ranks device time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+YEAR = 31558149.8
+MSUN_SEC = 6.67259e-11 * 1.98892e30 / 299792458.0**3
+NMODES = 30
+DT = 10.0
+SEED = 20261203
+
+
+# ----------------------------------------------------------------------------- workload
+def draw_source(rng) -> dict:
+    while True:
+        logM = rng.uniform(5.0, 7.0)
+        mu = rng.uniform(1.0, 100.0)
+        a = rng.uniform(0.0, 0.95)
+        e0 = rng.uniform(0.05, 0.5)
+        cosi = rng.uniform(-1.0, 1.0)
+        thS = math.acos(rng.uniform(-1.0, 1.0))
+        phS = rng.uniform(0.0, 2 * math.pi)
+        thK = math.acos(rng.uniform(-1.0, 1.0))
+        phK = rng.uniform(0.0, 2 * math.pi)
+        gam, psi, alp = (rng.uniform(0.0, 2 * math.pi) for _ in range(3))
+        T = rng.uniform(0.1, 1.0)
+        if abs(cosi) < 0.05:  # the flux kludge is singular for polar orbits
+            continue
+        M = 10.0**logM
+        rr = (M * MSUN_SEC) ** 2 / (mu * MSUN_SEC)  # radiation-reaction time [s]
+        n = int(T * YEAR / DT)
+        p_end = 10.0 + 3.0 * e0  # above the LSO for every spin / inclination
+        p0 = (p_end**4 + 2.0 * (256.0 / 5.0) * n * DT / rr) ** 0.25
+        p0 = min(max(p0, 9.0), 80.0)
+        return dict(backint=False, LISA=True, length=n, dt=DT, p=p0, T=T, f=2e-3, T_fit=1.0, mu=mu, M=M, s=a, e=e0,
+                    iota=math.acos(cosi), gamma=gam, psi=psi, theta_S=thS, phi_S=phS, theta_K=thK, phi_K=phK,
+                    alpha=alp, D=1.0)
+
+
+def config1(seed: int, nsrc: int = 512):
+    rng = np.random.default_rng(seed)
+    return [draw_source(rng) for _ in range(nsrc)], rng
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    smax.append(float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------------------- CPU reference
+def _ref_worker(args):
+    """Run the reference AAK (front end + waveform with n = 1..30) until the time budget is used."""
+    tasks, budget = args
+    sys.path.insert(0, REPO)
+    from oracle import oracle as O
+
+    samples, busy, done = 0, 0.0, 0
+    t_start = time.perf_counter()
+    for pars in tasks:
+        if time.perf_counter() - t_start > budget:
+            break
+        t0 = time.perf_counter()
+        mt = O.ref_front(pars)
+        if mt.steps < 3:
+            continue
+        O.ref_genwave(pars, mt, NMODES)
+        busy += time.perf_counter() - t0
+        samples += int(pars["length"])
+        done += 1
+    return samples, busy, done
+
+
+def cpu_reference(sources, budget_s: float = 15.0, sample_len: int = 20000, procs: int = 0) -> dict:
+    """Reference CPU AAK throughput on the host cores (spawn pool; the reference is not thread-safe)."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        raise RuntimeError("oracle/_ref/libaakref.so is not built")
+    procs = procs or (os.cpu_count() or 1)
+    # bounded sample: the config-1 sources truncated to sample_len samples each
+    tasks = []
+    for p in sources:
+        q = dict(p)
+        q["length"] = min(int(p["length"]), sample_len)
+        q["T"] = q["length"] * q["dt"] / YEAR
+        tasks.append(q)
+    per = [tasks[i::procs] for i in range(procs)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(t, budget_s) for t in per])
+    wall = time.perf_counter() - t0
+    samples = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    done = sum(r[2] for r in res)
+    return {"value": samples / busy if busy > 0 else 0.0, "unit": "samples/s", "cores": procs, "kind": "reference",
+            "sample": f"{done} config-1 sources truncated to {sample_len} samples, front end + waveform() with "
+                      f"n=1..{NMODES} (reference AAK, GSL shim), {procs} processes, {budget_s:.0f} s budget each",
+            "wall_s": wall}
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    import emri_kludge_suite_b200 as E
+    from emri_kludge_suite_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    sources, rng = config1(SEED + rank, args.nsrc)
+    wb = E.WaveBatch(local_rank)
+    nthreads = os.cpu_count() or 1
+    t_plan0 = time.perf_counter()
+    for _ in range(8):  # redraw sources that fail or plunge inside T
+        wb.plan(sources, nmodes=NMODES, nthreads=nthreads)
+        bad = [i for i in range(len(sources))
+               if wb.status[i] != 0 or wb.i_plunge[i] != int(sources[i]["length"]) - 1]
+        if not bad:
+            break
+        for i in bad:
+            sources[i] = draw_source(rng)
+    t_plan = time.perf_counter() - t_plan0
+    N = wb.total_samples
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    wb.upload(sptr)
+    hI = torch.empty(N, dtype=torch.float64, device="cuda")
+    hII = torch.empty(N, dtype=torch.float64, device="cuda")
+    L = _lib.lib()
+    import ctypes
+
+    tfl = ctypes.c_double(0.0)
+    _lib.check(L.aak_probe_fp64_tflops(local_rank, ctypes.byref(tfl)), "fp64 probe")
+    fp64_peak = tfl.value
+    for _ in range(args.warmup):
+        wb.run(hI.data_ptr(), hII.data_ptr(), stream=sptr)
+    torch.cuda.synchronize()
+
+    L.aak_batch_set_profiling(wb._ctx, 1)
+    ms3 = (ctypes.c_float * 3)()
+    kern = np.zeros(3)
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        wb.run(hI.data_ptr(), hII.data_ptr(), stream=sptr)
+        _lib.check(L.aak_batch_kernel_ms(wb._ctx, ms3), "kernel timing")
+        kern += np.array(ms3[:])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    L.aak_batch_set_profiling(wb._ctx, 0)
+    ms = ev0.elapsed_time(ev1)
+    kern /= args.steps
+    launches = wb.launches() * args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        tot = torch.tensor([float(N)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tot)
+        N_all = float(tot.item())
+    else:
+        N_all = float(N)
+    value = N_all * args.steps / (ms * 1e-3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e_steps = max(1, min(args.steps, args.e2e_steps))
+    hIh = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    hIIh = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    P = _lib.params_array(sources)
+    offs = np.zeros(len(sources) + 1, dtype=np.int64)
+    st = np.zeros(len(sources), dtype=np.int32)
+    nm = np.full(len(sources), NMODES, dtype=np.int32)
+    h2d = 0
+    e2e_times = []
+    for k in range(e2e_steps + 1):  # first call warms the host buffers
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        _lib.check(L.aak_wave_batch_host(wb._ctx, P, len(sources), _lib.ptr(nm), nthreads,
+                                         ctypes.cast(hIh.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                         ctypes.cast(hIIh.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                         _lib.ptr(offs), _lib.ptr(st)), "aak_wave_batch_host")
+        dt_e2e = time.perf_counter() - t0
+        if k > 0:
+            e2e_times.append(dt_e2e)
+    e2e_s = float(np.mean(e2e_times))
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    # plan bytes copied to the device per call (descriptors, knots, Bessel table)
+    h2d = int(wb.plan_bytes())
+    e2e = {"value": N_all / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": int(16 * N), "seconds_per_step": e2e_s, "host_threads": nthreads}
+
+    # ---- roofline of the dominant kernel (harmonic sum)
+    flops_per_sample = 60.0 + NMODES * 33.0  # algorithmic count per sample, see DESIGN.md
+    wave_ms = kern[2]
+    achieved = flops_per_sample * N / (wave_ms * 1e-3) / 1e12
+    roofline = {"kernel": "k_waveform_fp64", "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp64_peak if fp64_peak > 0 else None, "traffic": None,
+                "peak_source": "measured FP64 FMA rate on this GPU (aak_probe_fp64_tflops)",
+                "flops_per_sample": flops_per_sample}
+    out = {
+        "metric": "AAK samples/s & likelihoods/s on 1 B200 at mismatch<=1e-6 vs plain FP64 path",
+        "value": value,
+        "unit": "samples/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded configuration-1 draw)",
+        "config": {"workload": f"config1: {len(sources)} AAK sources/GPU, T~U(0.1,1) yr, dt=10 s, n=1..30, LISA, FP64",
+                   "nsrc_per_gpu": len(sources), "samples_per_gpu": int(N), "nmodes": NMODES, "seed": SEED,
+                   "l2": "outputs 16 B/sample x samples_per_gpu exceed the 126 MB L2",
+                   "parallelism": f"sources sharded, {world} rank(s)"},
+        "kernel_ms": {"phase_tile_sums": kern[0], "phase_carry": kern[1], "waveform_fp64": kern[2]},
+        "roofline": roofline,
+        "clocks": clk,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "host_plan_seconds": t_plan,
+    }
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nsrc", type=int, default=512)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        sources, _ = config1(SEED, args.nsrc)
+        samples_per_step = []
+        t_all = time.perf_counter()
+        res = None
+        for _ in range(args.warmup + args.steps):
+            res = cpu_reference(sources, budget_s=args.cpu_budget / max(1, args.steps))
+            samples_per_step.append(res["value"])
+        vals = samples_per_step[args.warmup:] or samples_per_step
+        v = float(np.mean(vals))
+        line = {"metric": "AAK samples/s & likelihoods/s on 1 B200 at mismatch<=1e-6 vs plain FP64 path", "value": v,
+                "unit": "samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": (time.perf_counter() - t_all) * 1e3 / (args.warmup + args.steps),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded configuration-1 draw)", "impl": "reference",
+                "config": {"workload": f"config1: {len(sources)} AAK sources, T~U(0.1,1) yr, dt=10 s, n=1..30, LISA, FP64",
+                           "nsrc": len(sources), "nmodes": NMODES, "seed": SEED},
+                "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # before any CUDA call: the pool is spawned from a process without a CUDA context
+        try:
+            sources, _ = config1(SEED, args.nsrc)
+            cpu = cpu_reference(sources, budget_s=args.cpu_budget)
+        except Exception as ex:  # reported, never fatal for the GPU arm
+            cpu = {"value": None, "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {ex}"}
+    out = run_gpu(args, rank, world, local_rank)
+    if rank == 0:
+        if cpu is not None:
+            out["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -119,8 +119,12 @@ def lib():
     L.aak_batch_plan_mapped.argtypes = [_vp, ctypes.POINTER(AAKParams), ctypes.POINTER(AAKMapped), _i32, _i32p, _i32]
     L.aak_batch_info.argtypes = [_vp, _i64p, _i64p, _i32p, _i32p, _i32p]
     L.aak_batch_upload.argtypes = [_vp, _vp]
+    L.aak_batch_plan_bytes.argtypes = [_vp, _i64p]
     L.aak_batch_run.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _i32, _vp]
     L.aak_batch_last_launches.argtypes = [_vp]
+    L.aak_batch_set_profiling.argtypes = [_vp, _i32]
+    L.aak_batch_kernel_ms.argtypes = [_vp, ctypes.POINTER(ctypes.c_float)]
+    L.aak_probe_fp64_tflops.argtypes = [_i32, _dp]
     L.aak_wave_batch_host.argtypes = [_vp, ctypes.POINTER(AAKParams), _i32, _i32p, _i32, _dp, _dp, _i64p, _i32p]
     _lib = L
     return L

@@ -1,0 +1,204 @@
+"""Python surface of the B200 AAK library.
+
+* :func:`wave` -- the call shape of the reference ``AAKwrapper.wave(pars)``
+  (AAKwrapper/AAKwrapper.pyx:50-88): returns ``(t, hI, hII, timing)``.
+* :func:`front_end` / :func:`genwave` -- the two halves of ``AAKwave``
+  (src/suite/AAKpy.cc:16-51): mapped trajectory, then GenWave/waveform.
+* :class:`WaveBatch` -- many sources in one launch, outputs in device memory.
+
+Failures raise :class:`AAKValueError` (a ``ValueError``) where the reference
+would terminate the process.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import AAKMapped, AAKValueError, check, lib, make_params, params_array, ptr
+
+__all__ = ["wave", "front_end", "genwave", "Mapped", "WaveBatch", "AAKValueError"]
+
+
+@dataclass
+class Mapped:
+    """Mapped trajectory handed to GenWave (src/suite/AAKpy.cc:29-44)."""
+
+    steps: int
+    e_traj: np.ndarray
+    v_map: np.ndarray
+    M_map: np.ndarray
+    s_map: np.ndarray
+    dt_map: np.ndarray
+    Phi0: float
+    inspiral_flag: int
+    newton_iterations: int
+
+    def to_struct(self) -> AAKMapped:
+        m = AAKMapped()
+        m.steps = self.steps
+        m.inspiral_flag = self.inspiral_flag
+        m.newton_iterations = self.newton_iterations
+        m.Phi0 = self.Phi0
+        for name in ("e_traj", "v_map", "M_map", "s_map", "dt_map"):
+            arr = getattr(m, name)
+            src = getattr(self, name)
+            for i in range(self.steps):
+                arr[i] = float(src[i])
+        return m
+
+    @staticmethod
+    def from_struct(m: AAKMapped) -> "Mapped":
+        n = m.steps
+        return Mapped(
+            n,
+            *[np.array(getattr(m, k)[:n], dtype=np.float64) for k in ("e_traj", "v_map", "M_map", "s_map", "dt_map")],
+            float(m.Phi0),
+            int(m.inspiral_flag),
+            int(m.newton_iterations),
+        )
+
+
+def front_end(pars: dict, warm_start: np.ndarray | None = None) -> Mapped:
+    """Coarse Kerr inspiral, Kerr frequencies and the Kerr->AK map (host)."""
+    m = AAKMapped()
+    ws = None
+    if warm_start is not None:
+        ws = np.ascontiguousarray(warm_start, dtype=np.float64)
+    check(lib().aak_front_end(ctypes.byref(make_params(pars)), ptr(ws), ctypes.byref(m)), "aak_front_end")
+    return Mapped.from_struct(m)
+
+
+def wave(pars: dict):
+    """AAKwrapper.wave: ``(t, hI, hII, timing)`` for the dict of SetPar fields."""
+    n = int(pars["length"])
+    t = np.zeros(n)
+    hI = np.zeros(n)
+    hII = np.zeros(n)
+    secs = ctypes.c_double(0.0)
+    check(lib().aak_wave(ctypes.byref(make_params(pars)), ptr(t), ptr(hI), ptr(hII), ctypes.byref(secs)), "aak_wave")
+    return t, hI, hII, secs.value
+
+
+def genwave(pars: dict, mapped: Mapped, nmodes: int = 0):
+    """GenWave -> waveform on a mapped trajectory (src/suite/AAK.cc:565-591).
+
+    ``nmodes <= 0`` keeps the reference harmonic rule.  Returns (t, hI, hII).
+    """
+    n = int(pars["length"])
+    t, hI, hII = np.zeros(n), np.zeros(n), np.zeros(n)
+    arrs = [np.ascontiguousarray(getattr(mapped, k), dtype=np.float64) for k in ("e_traj", "v_map", "M_map", "s_map", "dt_map")]
+    e, v, Mm, sm, dtm = arrs
+    check(
+        lib().aak_genwave(
+            ptr(t), ptr(hI), ptr(hII), float(pars["dt"]), n, ptr(e), ptr(v), float(pars["M"]), ptr(Mm),
+            float(pars["mu"]), float(pars["s"]), ptr(sm), float(pars["D"]), float(pars["iota"]), float(pars["gamma"]),
+            float(mapped.Phi0), float(pars["theta_S"]), float(pars["phi_S"]), float(pars["alpha"]),
+            float(pars["theta_K"]), float(pars["phi_K"]), ptr(dtm), int(mapped.steps), int(bool(pars["backint"])),
+            int(bool(pars["LISA"])), int(nmodes),
+        ),
+        "aak_genwave",
+    )
+    return t, hI, hII
+
+
+class WaveBatch:
+    """A batch of sources planned on host threads and generated on one GPU.
+
+    Outputs live in caller-provided device memory (``torch.cuda`` tensors or
+    raw pointers) laid out by :attr:`offsets`.
+    """
+
+    def __init__(self, device: int = 0):
+        self._ctx = ctypes.c_void_p()
+        check(lib().aak_ctx_create(int(device), ctypes.byref(self._ctx)), "aak_ctx_create")
+        self.device = device
+        self.nsrc = 0
+        self.offsets = np.zeros(1, dtype=np.int64)
+        self.status = np.zeros(0, dtype=np.int32)
+        self.i_plunge = np.zeros(0, dtype=np.int32)
+        self.i_buffer = np.zeros(0, dtype=np.int32)
+        self.total_samples = 0
+
+    def close(self):
+        if self._ctx:
+            lib().aak_ctx_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _info(self):
+        n = self.nsrc
+        self.offsets = np.zeros(n + 1, dtype=np.int64)
+        self.status = np.zeros(n, dtype=np.int32)
+        self.i_plunge = np.zeros(n, dtype=np.int32)
+        self.i_buffer = np.zeros(n, dtype=np.int32)
+        tot = ctypes.c_int64()
+        check(
+            lib().aak_batch_info(self._ctx, ctypes.byref(tot), ptr(self.offsets), ptr(self.status), ptr(self.i_plunge),
+                                 ptr(self.i_buffer)),
+            "aak_batch_info",
+        )
+        self.total_samples = int(tot.value)
+
+    def plan(self, params, nmodes=None, nthreads: int = 0, mapped=None):
+        """Host planning; ``params`` is a list of pars dicts (or aak_params)."""
+        self.nsrc = len(params)
+        P = params_array(params)
+        nm = None
+        if nmodes is not None:
+            nm = np.ascontiguousarray(np.broadcast_to(np.asarray(nmodes, dtype=np.int32), (self.nsrc,)))
+        if mapped is not None:
+            M = (AAKMapped * self.nsrc)()
+            for i, m in enumerate(mapped):
+                M[i] = m.to_struct() if isinstance(m, Mapped) else m
+            check(lib().aak_batch_plan_mapped(self._ctx, P, M, self.nsrc, ptr(nm), int(nthreads)), "aak_batch_plan_mapped")
+        else:
+            check(lib().aak_batch_plan(self._ctx, P, self.nsrc, ptr(nm), int(nthreads)), "aak_batch_plan")
+        self._info()
+        return self
+
+    def plan_bytes(self) -> int:
+        b = ctypes.c_int64()
+        check(lib().aak_batch_plan_bytes(self._ctx, ctypes.byref(b)), "aak_batch_plan_bytes")
+        return int(b.value)
+
+    def upload(self, stream: int = 0):
+        check(lib().aak_batch_upload(self._ctx, ctypes.c_void_p(stream)), "aak_batch_upload")
+
+    def run(self, hI_ptr: int, hII_ptr: int, t_ptr: int = 0, traj_ptr: int = 0, traj_stride: int = 0,
+            precision: int = 0, stream: int = 0):
+        check(
+            lib().aak_batch_run(self._ctx, ctypes.c_void_p(hI_ptr), ctypes.c_void_p(hII_ptr), ctypes.c_void_p(t_ptr),
+                                ctypes.c_void_p(traj_ptr), int(traj_stride), int(precision), ctypes.c_void_p(stream)),
+            "aak_batch_run",
+        )
+
+    def launches(self) -> int:
+        return int(lib().aak_batch_last_launches(self._ctx))
+
+    def generate_host(self, params, nmodes=None, nthreads: int = 0):
+        """Plan + upload + run + copy back (host buffers).  Returns (hI, hII, offsets, status)."""
+        self.nsrc = len(params)
+        P = params_array(params)
+        total = int(sum(int(p["length"]) if isinstance(p, dict) else int(p.length) for p in params))
+        hI = np.zeros(total)
+        hII = np.zeros(total)
+        offs = np.zeros(self.nsrc + 1, dtype=np.int64)
+        st = np.zeros(self.nsrc, dtype=np.int32)
+        nm = None
+        if nmodes is not None:
+            nm = np.ascontiguousarray(np.broadcast_to(np.asarray(nmodes, dtype=np.int32), (self.nsrc,)))
+        check(
+            lib().aak_wave_batch_host(self._ctx, P, self.nsrc, ptr(nm), int(nthreads), ptr(hI), ptr(hII), ptr(offs),
+                                      ptr(st)),
+            "aak_wave_batch_host",
+        )
+        self._info()
+        return hI, hII, offs, st

@@ -80,6 +80,8 @@ struct aak_ctx {
   DevBuf<unsigned long long> d_counter;
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
   int last_launches = 0;
+  bool profile = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::mutex mu;
 };
 
@@ -309,7 +311,9 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   bv.traj_out = traj;
   bv.traj_stride = traj_stride;
   bv.work_counter = ctx->d_counter.ptr;
-  launch_dense_fp64(bv, ctx->num_sms, st);
+  if (ctx->profile && !ctx->ev[0])
+    for (auto &e : ctx->ev) cudaEventCreate(&e);
+  launch_dense_fp64(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr);
   ctx->last_launches = 3;
   return cuda_ok(cudaGetLastError());
 }
@@ -430,6 +434,8 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_carry.release();
     c->d_counter.release();
     c->d_out.release();
+    for (auto &e : c->ev)
+      if (e) cudaEventDestroy(e);
   }
   delete c;
 }
@@ -461,6 +467,15 @@ int aak_batch_info(aak_ctx *ctx, int64_t *total, int64_t *offsets, int32_t *stat
   return AAK_OK;
 }
 
+int aak_batch_plan_bytes(aak_ctx *ctx, int64_t *bytes) {
+  if (!ctx || !bytes) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  *bytes = (int64_t)(ctx->descs.size() * sizeof(SourceDesc) + ctx->tile_start.size() * sizeof(int64_t) +
+                     ctx->knot_t.size() * sizeof(double) + 2 * ctx->knot_y.size() * sizeof(double4) +
+                     ctx->bessel.size() * sizeof(int32_t));
+  return AAK_OK;
+}
+
 int aak_batch_upload(aak_ctx *ctx, void *stream) {
   if (!ctx) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -475,6 +490,32 @@ int aak_batch_run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj
 }
 
 int aak_batch_last_launches(aak_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
+
+int aak_batch_set_profiling(aak_ctx *ctx, int32_t on) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->profile = on != 0;
+  return AAK_OK;
+}
+
+int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3) {
+  if (!ctx || !ms3 || !ctx->profile || !ctx->ev[0]) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaEventSynchronize(ctx->ev[3]) != cudaSuccess) return cuda_ok(cudaGetLastError());
+  for (int k = 0; k < 3; ++k)
+    if (cudaEventElapsedTime(&ms3[k], ctx->ev[k], ctx->ev[k + 1]) != cudaSuccess) return cuda_ok(cudaGetLastError());
+  return AAK_OK;
+}
+
+int aak_probe_fp64_tflops(int32_t device, double *tflops) {
+  if (!tflops) return AAK_ERR_INVALID_PARAM;
+  int r = select_device(device);
+  if (r != AAK_OK) return r;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  *tflops = probe_fp64_fma_tflops(sms, 20, 0);
+  return *tflops > 0 ? AAK_OK : AAK_ERR_CUDA;
+}
 
 int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nm, int32_t nthreads,
                         double *h_hI, double *h_hII, int64_t *offsets, int32_t *status) {

@@ -690,14 +690,61 @@ __global__ void __launch_bounds__(kTileThreads) k_waveform_fp64(BatchView bv) {
 
 }  // namespace
 
-void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream) {
+void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev) {
   if (bv.total_tiles <= 0) return;
   const int grid1 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 8);
-  k_phase_tiles<<<grid1, kTileThreads, 0, stream>>>(bv);
-  k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
   cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
+  if (ev) cudaEventRecord(ev[0], stream);
+  k_phase_tiles<<<grid1, kTileThreads, 0, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[1], stream);
+  k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[2], stream);
   const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 4);
   k_waveform_fp64<<<grid2, kTileThreads, 0, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[3], stream);
+}
+
+namespace {
+// 8 independent FMA chains per thread; the result is stored so nothing is elided.
+__global__ void __launch_bounds__(256) k_fp64_fma_probe(double *out, int reps, double a, double b) {
+  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1e-9, x2 = x0 + 2e-9, x3 = x0 + 3e-9;
+  double x4 = x0 + 4e-9, x5 = x0 + 5e-9, x6 = x0 + 6e-9, x7 = x0 + 7e-9;
+  for (int r = 0; r < reps; ++r) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 = fma(x0, a, b);
+      x1 = fma(x1, a, b);
+      x2 = fma(x2, a, b);
+      x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b);
+      x5 = fma(x5, a, b);
+      x6 = fma(x6, a, b);
+      x7 = fma(x7, a, b);
+    }
+  }
+  out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+}  // namespace
+
+double probe_fp64_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
+  const int blocks = num_sms * 8, threads = 256, reps = 2048;
+  double *out = nullptr;
+  if (cudaMalloc(&out, (size_t)blocks * threads * sizeof(double)) != cudaSuccess) return -1.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_fp64_fma_probe<<<blocks, threads, 0, stream>>>(out, reps, 0.999999, 1e-7);  // warm-up
+  cudaEventRecord(e0, stream);
+  for (int i = 0; i < iters; ++i) k_fp64_fma_probe<<<blocks, threads, 0, stream>>>(out, reps, 0.999999, 1e-7);
+  cudaEventRecord(e1, stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  const double flops = 2.0 * 8.0 * 16.0 * reps * (double)blocks * threads * iters;
+  return cudaGetLastError() == cudaSuccess && ms > 0 ? flops / (ms * 1e-3) / 1e12 : -1.0;
 }
 
 }  // namespace aak

@@ -54,6 +54,12 @@ struct BatchView {
   unsigned long long *work_counter;  // persistent work queue head (pass 2)
 };
 
-void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream);
+// Launch pass 1, the carry scan and pass 2 on `stream`.  ev (optional, 4
+// events) brackets the three kernels for per-kernel timing.
+void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev);
+
+// Diagnostic: sustained FP64 FMA issue rate of this device in TFLOP/s
+// (2 flops per FMA), measured with CUDA events over `iters` launches.
+double probe_fp64_fma_tflops(int num_sms, int iters, cudaStream_t stream);
 
 }  // namespace aak

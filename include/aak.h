@@ -128,6 +128,9 @@ int aak_batch_plan_mapped(aak_ctx *ctx, const aak_params *P, const aak_mapped *m
 int aak_batch_info(aak_ctx *ctx, int64_t *total_samples, int64_t *offsets, int32_t *status, int32_t *i_plunge,
                    int32_t *i_buffer);
 
+/* Bytes aak_batch_upload copies to the device for the planned batch. */
+int aak_batch_plan_bytes(aak_ctx *ctx, int64_t *bytes);
+
 /* Copy the planned batch to the device (stream-ordered on `stream`, a
  * cudaStream_t or NULL for the legacy default stream). */
 int aak_batch_upload(aak_ctx *ctx, void *stream);
@@ -141,6 +144,15 @@ int aak_batch_run(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_t, double
 
 /* Number of CUDA kernels the last aak_batch_run launched. */
 int aak_batch_last_launches(aak_ctx *ctx);
+
+/* Per-kernel timing of aak_batch_run with CUDA events on its stream: after
+ * aak_batch_set_profiling(ctx, 1), aak_batch_kernel_ms returns the durations
+ * of (pass 1 phase sums, carry scan, waveform) of the last run in ms. */
+int aak_batch_set_profiling(aak_ctx *ctx, int32_t on);
+int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3);
+
+/* Diagnostic: sustained FP64 FMA rate of `device` in TFLOP/s (roofline denominator). */
+int aak_probe_fp64_tflops(int32_t device, double *tflops);
 
 /* End to end with host buffers: plan + upload + run + copy back.
  * h_hI / h_hII hold total_samples doubles (offsets as from aak_batch_info). */
