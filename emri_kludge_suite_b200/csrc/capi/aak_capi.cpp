@@ -489,6 +489,54 @@ int aak_batch_run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj
   return run(ctx, hI, hII, t, traj, traj_stride, precision, (cudaStream_t)stream);
 }
 
+int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_t *required_bytes, double *d_hI,
+                          double *d_hII, void *stream) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (ctx->nsrc <= 0) return AAK_ERR_INVALID_PARAM;
+  // caller buffer layout: descriptors | tile prefix | knot times | knot values | knot
+  // second derivatives | Bessel start orders, each segment 256-byte aligned
+  auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t o_ts = al(ctx->descs.size() * sizeof(SourceDesc));
+  const size_t o_kt = o_ts + al(ctx->tile_start.size() * sizeof(int64_t));
+  const size_t o_ky = o_kt + al(ctx->knot_t.size() * sizeof(double));
+  const size_t o_kc = o_ky + al(ctx->knot_y.size() * sizeof(double4));
+  const size_t o_bs = o_kc + al(ctx->knot_c.size() * sizeof(double4));
+  const size_t need = o_bs + al(ctx->bessel.size() * sizeof(int32_t));
+  if (required_bytes) *required_bytes = (int64_t)need;
+  if (!d_plan) return AAK_OK;  // size query only
+  if (plan_bytes < 0 || (size_t)plan_bytes < need) return AAK_ERR_CAPACITY;
+  if (ctx->total_tiles > kStaticScratchTiles) return AAK_ERR_CAPACITY;
+  if (!d_hI || !d_hII || ((uintptr_t)d_plan & 255u) != 0) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned char *base = static_cast<unsigned char *>(d_plan);
+  auto cp = [&](size_t off, const void *src, size_t bytes) {
+    return cuda_ok(cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st));
+  };
+  if ((r = cp(0, ctx->descs.data(), ctx->descs.size() * sizeof(SourceDesc))) ||
+      (r = cp(o_ts, ctx->tile_start.data(), ctx->tile_start.size() * sizeof(int64_t))) ||
+      (r = cp(o_kt, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
+      (r = cp(o_ky, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
+      (r = cp(o_kc, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
+      (r = cp(o_bs, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
+    return r;
+  BatchView bv;
+  std::memset(&bv, 0, sizeof(bv));
+  bv.src = reinterpret_cast<const SourceDesc *>(base);
+  bv.nsrc = ctx->nsrc;
+  bv.total_tiles = ctx->total_tiles;
+  bv.tile_start = reinterpret_cast<const int64_t *>(base + o_ts);
+  bv.knot_t = reinterpret_cast<const double *>(base + o_kt);
+  bv.knot_y = reinterpret_cast<const double4 *>(base + o_ky);
+  bv.knot_c = reinterpret_cast<const double4 *>(base + o_kc);
+  bv.bessel_start = reinterpret_cast<const int32_t *>(base + o_bs);
+  bv.hI = d_hI;
+  bv.hII = d_hII;
+  return launch_dense_fp64_static_scratch(bv, ctx->device, ctx->num_sms, st);
+}
+
 int aak_batch_last_launches(aak_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
 
 int aak_batch_set_profiling(aak_ctx *ctx, int32_t on) {

@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <mutex>
+
 #include "aak_dense.cuh"
 
 namespace aak {
@@ -745,6 +747,52 @@ double probe_fp64_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
   cudaFree(out);
   const double flops = 2.0 * 8.0 * 16.0 * reps * (double)blocks * threads * iters;
   return cudaGetLastError() == cudaSuccess && ms > 0 ? flops / (ms * 1e-3) / 1e12 : -1.0;
+}
+
+// ------------------------------------------------------------------ allocation-free launch
+// Tile scratch (per-tile phase sums, carries and the work-queue head) for
+// callers that must not allocate device memory.  The array is part of the
+// module image: every GPU that loads this library holds its 10 MB until the
+// process exits.  All calls share it and it keeps the last call's contents;
+// launches that overlap on the GPU race on it.
+namespace {
+constexpr size_t kStaticSummaryBytes = (size_t)kStaticScratchTiles * sizeof(TileSummary);
+constexpr size_t kStaticCarryOffset = (kStaticSummaryBytes + 255) / 256 * 256;
+constexpr size_t kStaticCounterOffset = (kStaticCarryOffset + (size_t)kStaticScratchTiles * sizeof(TileCarry) + 255) / 256 * 256;
+constexpr size_t kStaticScratchBytes = kStaticCounterOffset + 256;
+static __device__ __align__(256) unsigned char g_tile_scratch[kStaticScratchBytes];
+
+std::mutex g_scratch_mu;
+void *g_scratch_addr[kMaxStaticDevices] = {nullptr};
+}  // namespace
+
+int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream) {
+  if (bv.total_tiles > kStaticScratchTiles) return 8;  // AAK_ERR_CAPACITY
+  if (device < 0 || device >= kMaxStaticDevices) return 1;
+  void *base = nullptr;
+  {
+    // host code needs the device address of the array: look it up once per
+    // device, with that device current (the caller has selected it)
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    if (!g_scratch_addr[device]) {
+      void *p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_tile_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return 5;  // AAK_ERR_CUDA
+      }
+      g_scratch_addr[device] = p;
+    }
+    base = g_scratch_addr[device];
+  }
+  unsigned char *b = static_cast<unsigned char *>(base);
+  bv.summ = reinterpret_cast<TileSummary *>(b);
+  bv.carry = reinterpret_cast<TileCarry *>(b + kStaticCarryOffset);
+  bv.work_counter = reinterpret_cast<unsigned long long *>(b + kStaticCounterOffset);
+  // the work-queue head must start at zero; launch_dense_fp64 clears it on
+  // `stream`, and pass 1 / the carry kernel overwrite every tile entry that
+  // pass 2 reads before it reads it
+  launch_dense_fp64(bv, num_sms, stream, nullptr);
+  return cudaGetLastError() == cudaSuccess ? 0 : 5;
 }
 
 }  // namespace aak

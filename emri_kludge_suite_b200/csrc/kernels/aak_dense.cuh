@@ -62,4 +62,15 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
 // (2 flops per FMA), measured with CUDA events over `iters` launches.
 double probe_fp64_fma_tflops(int num_sms, int iters, cudaStream_t stream);
 
+// Largest batch (in 1024-sample tiles) the allocation-free launch accepts,
+// and the number of devices whose scratch address is cached.
+constexpr int64_t kStaticScratchTiles = 32768;
+constexpr int kMaxStaticDevices = 64;
+
+// Same kernels as launch_dense_fp64, with the tile scratch (bv.summ,
+// bv.carry, bv.work_counter are ignored) taken from a file-scope __device__
+// array instead of caller or context allocations.  Returns an aak_status.
+// The first call on a device looks the array's address up (once per device).
+int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream);
+
 }  // namespace aak

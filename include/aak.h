@@ -142,6 +142,24 @@ int aak_batch_upload(aak_ctx *ctx, void *stream);
 int aak_batch_run(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_t, double *d_traj, int64_t traj_stride,
                   int32_t precision, void *stream);
 
+/* Allocation-free variant of aak_batch_run, for callers that cannot call
+ * cudaMalloc: code whose device memory belongs to a host framework or a
+ * pre-reserved pool (a sampler that owns the GPU's memory budget, a caching
+ * allocator), where an allocation would synchronise the device or break the
+ * budget.  No counterpart in the reference.
+ * The caller passes the planned ctx (aak_batch_plan* only -- no upload),
+ * one device buffer of its own for the plan (256-byte aligned, plan_bytes
+ * long) and the outputs hI, hII (indexed by the batch offsets).  Call with
+ * d_plan == NULL to receive the required size in *required_bytes.  The tile
+ * scratch lives in a 10 MB file-scope device array held by every GPU that
+ * loads the library until exit; batches above 32768 tiles of 1024 samples
+ * (33,554,432 samples) are rejected with AAK_ERR_CAPACITY.  The first call
+ * on a device looks the array's address up; make that call before any stream
+ * capture.  Every call shares the array: calls that overlap on the GPU race.
+ * Nothing here calls cudaMalloc, cudaFree or an allocating library routine. */
+int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_t *required_bytes, double *d_hI,
+                          double *d_hII, void *stream);
+
 /* Number of CUDA kernels the last aak_batch_run launched. */
 int aak_batch_last_launches(aak_ctx *ctx);
 
