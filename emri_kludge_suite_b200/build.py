@@ -56,7 +56,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     cc = nvcc()
     hdrs = _headers()
-    extra = list(extra_flags or [])
+    extra = list(extra_flags or []) + os.environ.get("AAK_EXTRA_NVCC_FLAGS", "").split()
     jobs = []
     objs = []
     for rel in SOURCES:

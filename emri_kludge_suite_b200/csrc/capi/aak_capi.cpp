@@ -212,7 +212,7 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
       }
       d.knot_offset = ko;
       d.bessel_offset = (int32_t)bo;
-      for (int m = 1; m <= pl.nmodes; ++m) ctx->bessel[bo + m - 1] = bessel_start_order(m, pl.e_max);
+      for (int m = 1; m <= pl.nmodes; ++m) ctx->bessel[bo + m - 1] = bessel_start_order(m, pl.e_max, 12);  // table rows reach order n + 2 + 12
       ko += nk;
       bo += pl.nmodes;
     } else {

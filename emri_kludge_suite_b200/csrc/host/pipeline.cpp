@@ -267,8 +267,8 @@ double spline_eval(const double *x, const double *y, const double *c, int n, int
 }
 
 // ------------------------------------------------------------------ Bessel start order
-int bessel_start_order(int n, double e_max) {
-  const int nmax = (n == 1) ? 3 : n + 2;
+int bessel_start_order(int n, double e_max, int extra) {
+  const int nmax = ((n == 1) ? 3 : n + 2) + extra;
   const double x = n * e_max;
   int k = std::max(nmax, (int)std::ceil(x));
   double prod = 1.0;

@@ -108,7 +108,7 @@ int plan_source(const WaveInputs &w, SourcePlan *plan);
 void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c);
 double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv);
 
-// Miller start order for J_{n-2..n+2}(n e) accurate to ~1e-17 for all e <= e_max.
-int bessel_start_order(int n, double e_max);
+// Miller start order for J_{n-2..n+2+extra}(n e) accurate to ~1e-17 for all e <= e_max.
+int bessel_start_order(int n, double e_max, int extra = 0);
 
 }  // namespace aak

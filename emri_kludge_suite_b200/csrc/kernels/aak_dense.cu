@@ -24,6 +24,11 @@ namespace {
 constexpr double kTwoPi = 2.0 * kPi;
 constexpr double kHalfSqrt3 = 0.86602540378443864676;
 
+// Resident CTAs per SM requested for the waveform kernel (register budget).
+#ifndef AAK_WAVE_MIN_BLOCKS
+#define AAK_WAVE_MIN_BLOCKS 2
+#endif
+
 // ------------------------------------------------------------------ small helpers
 __device__ __forceinline__ int find_source(const int64_t *tile_start, int nsrc, int64_t g) {
   int lo = 0, hi = nsrc;
@@ -397,12 +402,159 @@ __device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double
   for (int m = 0; m < 5; ++m) J[m] = v[m] * inv;
 }
 
+// ------------------------------------------------------------------ per-tile Bessel table
+// Within a 1024-sample tile the eccentricity moves by ~1e-4 at most, so the
+// Bessel values at x = n e are obtained from values at the tile's central
+// eccentricity e_c through the multiplication theorem (DLMF 10.23.1):
+//   J_nu(lambda z) = lambda^nu sum_{k>=0} ((1 - lambda^2) z / 2)^k / k! J_{nu+k}(z),
+// z = n e_c, lambda = e / e_c.  Row n of the table holds J_{b+m}(n e_c) for
+// m = 0 .. 4 + K, b = n - 2 (b = -1 for n = 1, with J_{-1} = -J_1).
+constexpr int kKMax = 12;
+constexpr int kTabStride = 5 + kKMax;
+constexpr int kTabModes = 128;
+
+// one row of the table, built by one thread (x = n e_c > 0)
+__device__ void build_bessel_row(double *Tn, int n, double x, int K, int start) {
+  const int b = (n == 1) ? -1 : n - 2;
+  const int lo = max(b, 0), hi = b + 4 + K;
+  if (x < 1.0) {
+    const double hx = 0.5 * x, q = -hx * hx;
+    double pref = exp((double)lo * log(hx) - lgamma((double)lo + 1.0));
+    for (int nu = lo; nu <= hi; ++nu) {
+      double term = 1.0, sum = 1.0;
+      for (int k = 1; k < 16; ++k) {
+        term *= q / ((double)k * ((double)nu + (double)k));
+        sum += term;
+      }
+      Tn[nu - b] = pref * sum;
+      pref *= hx / ((double)nu + 1.0);
+    }
+  } else {
+    const double tx = 2.0 / x;
+    int k = max(start, hi + 8);
+    if (k & 1) ++k;
+    double jk = 1.0e-280, jk1 = 0.0, sum = 2.0 * jk, w = 0.0;
+    for (; k > 0; --k) {
+      const double jm = (double)k * tx * jk - jk1;  // order k - 1
+      jk1 = jk;
+      jk = jm;
+      sum = fma(w, jm, sum);
+      w = 2.0 - w;
+      const int ord = k - 1;
+      if (ord >= lo && ord <= hi) Tn[ord - b] = jm;
+      if (fabs(jm) > 1.0e250) {  // rescale everything produced so far
+        jk *= 1.0e-250;
+        jk1 *= 1.0e-250;
+        sum *= 1.0e-250;
+        for (int o = max(ord, lo); o <= hi; ++o) Tn[o - b] *= 1.0e-250;
+      }
+    }
+    sum -= jk;  // J_0 was added with weight 2; count it once
+    const double inv = 1.0 / sum;
+    for (int o = lo; o <= hi; ++o) Tn[o - b] *= inv;
+  }
+  if (n == 1) Tn[0] = -Tn[2];
+}
+
+// Number of multiplication-theorem terms for a tile where |(1-lambda^2) z/2|
+// stays below qmax (tail < 1e-17 of the largest J); 0 = use per-sample Miller.
+__device__ __forceinline__ int choose_terms(double qmax) {
+  if (qmax <= 1e-3) return 4;
+  if (qmax <= 1e-2) return 6;
+  if (qmax <= 5e-2) return 8;
+  if (qmax <= 2e-1) return 12;
+  return 0;
+}
+
+// Mode sums Sa, Sb, Sc (see harmonic_sum_fp64) from the tile table.
+template <int K>
+__device__ __forceinline__ void mode_sums_table(const double *T, int nmodes, double e, double ec, double c1, double s1,
+                                                double cD, double sD, double &Sa, double &Sb, double &Sc) {
+  const double lam = e / ec;
+  const double half_dl = (1.0 - lam) * (1.0 + lam) * ec * 0.5;  // (1 - lambda^2) e_c / 2
+  double p = 1.0 / lam;                                         // lambda^b, b = -1 for n = 1
+  double zr = 1.0, zi = 0.0;
+  double sa = 0.0, sb = 0.0, sc = 0.0;
+#pragma unroll 1
+  for (int n = 1; n <= nmodes; ++n) {
+    const double *Tn = T + (n - 1) * kTabStride;
+    const double c = (double)n * half_dl;
+    double w[K + 1];
+    w[0] = 1.0;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) w[k] = w[k - 1] * c * (1.0 / (double)k);
+    double J[5];
+    double pj = p;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      double s = w[K] * Tn[j + K];
+#pragma unroll
+      for (int k = K - 1; k >= 0; --k) s = fma(w[k], Tn[j + k], s);
+      J[j] = pj * s;
+      pj *= lam;
+    }
+    p *= lam;
+    const double tr = zr * c1 - zi * s1;
+    zi = zr * s1 + zi * c1;
+    zr = tr;
+    const double cn = zr * cD - zi * sD;
+    const double sn = zi * cD + zr * sD;
+    const double dn = (double)n;
+    sa += dn * (J[0] - 2. * e * J[1] + 2. / dn * J[2] + 2. * e * J[3] - J[4]) * cn;
+    sb += dn * (J[0] - 2. * J[2] + J[4]) * sn;
+    sc += J[2] * cn;
+  }
+  Sa = sa;
+  Sb = sb;
+  Sc = sc;
+}
+
+// Mode sums with a per-sample Miller recurrence (fallback when the table does not apply).
+__device__ void mode_sums_miller(const int32_t *bstart, int nmodes, double e, double c1, double s1, double cD,
+                                 double sD, double &Sa, double &Sb, double &Sc) {
+  double zr = 1.0, zi = 0.0;
+  double sa = 0.0, sb = 0.0, sc = 0.0;
+  for (int n = 1; n <= nmodes; ++n) {
+    const double tr = zr * c1 - zi * s1;
+    zi = zr * s1 + zi * c1;
+    zr = tr;
+    const double cn = zr * cD - zi * sD;
+    const double sn = zi * cD + zr * sD;
+    double J[5];
+    const double x = n * e;
+    if (x <= 0.0) {
+      J[0] = J[1] = J[2] = J[3] = J[4] = 0.0;
+      if (n == 1) J[1] = 1.0;
+      if (n == 2) J[0] = 1.0;
+    } else if (n == 1) {
+      double Jt[5];
+      bessel5_fp64(0, x, bstart[0], Jt);
+      J[0] = -Jt[1];
+      J[1] = Jt[0];
+      J[2] = Jt[1];
+      J[3] = Jt[2];
+      J[4] = Jt[3];
+    } else {
+      bessel5_fp64(n - 2, x, bstart[n - 1], J);
+    }
+    const double dn = (double)n;
+    sa += dn * (J[0] - 2. * e * J[1] + 2. / dn * J[2] + 2. * e * J[3] - J[4]) * cn;
+    sb += dn * (J[0] - 2. * J[2] + J[4]) * sn;
+    sc += J[2] * cn;
+  }
+  Sa = sa;
+  Sb = sb;
+  Sc = sc;
+}
+
 // ------------------------------------------------------------------ harmonic sum
 // h_I, h_II at one sample (AAK.cc:409-528) with the modes accumulated as
 // Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
-// rotation and antenna factors applied once per sample.
-__device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, double t, const Traj4 &q, double gim,
-                                  double Phi, double alp, double nu, double gimdot, double &hI, double &hII) {
+// rotation and antenna factors applied once per sample.  The Bessel values
+// come from the tile table (K > 0) or a per-sample recurrence (K == 0).
+__device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, const double *T, double ec, int K,
+                                  double t, const Traj4 &q, double gim, double Phi, double alp, double nu,
+                                  double gimdot, double &hI, double &hII) {
   const double e = q.e;
   const double cosalp = cos(alp), sinalp = sin(alp);
   const double cosqL = d.cosqK * d.coslam + d.sinqK * d.sinlam * cosalp;
@@ -419,7 +571,7 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, do
   double sin2gam, cos2gam;
   sincos(2. * (gim + beta), &sin2gam, &cos2gam);
 
-  double cosorbphs = 0.0, FplusI, FcrosI, FplusII, FcrosII, K;
+  double cosorbphs = 0.0, FplusI, FcrosI, FplusII, FcrosII, Kresp;
   if (d.mich) {
     const double orbphs = kTwoPi * t / kYear;
     double sinorbphs;
@@ -441,7 +593,7 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, do
     FcrosI = cosq1 * cos2phi * sin2psi + cosq * sin2phi * cos2psi;
     FplusII = cosq1 * sin2phi * cos2psi + cosq * cos2phi * sin2psi;
     FcrosII = cosq1 * sin2phi * sin2psi - cosq * cos2phi * cos2psi;
-    K = kHalfSqrt3;
+    Kresp = kHalfSqrt3;
   } else {
     const double up_ldc = d.cosqS * d.sinqK * cos(d.phiS - d.phiK) - d.cosqK * d.sinqS;
     const double dw_ldc = d.sinqK * sin(d.phiS - d.phiK);
@@ -452,7 +604,7 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, do
     FcrosI = -s2;
     FplusII = s2;
     FcrosII = c2;
-    K = 1.0;
+    Kresp = 1.0;
   }
   const double Amp = pow(omega_phi(q.v, e, d.coslam, q.S, q.M) * d.M_phys_sec, 2. / 3.) * d.zeta;
 
@@ -477,12 +629,12 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, do
   const double uI = FplusI * rot0 - FcrosI * rot1, wI = FplusI * rot1 + FcrosI * rot0;
   const double uII = FplusII * rot0 - FcrosII * rot1, wII = FplusII * rot1 + FcrosII * rot0;
   const double opL2 = 1. + Ldotn2, omL2 = 1. - Ldotn2, twoL = 2. * Ldotn;
-  const double caI = K * (-uI * opL2 * cos2gam + wI * twoL * sin2gam);
-  const double cbI = K * (uI * opL2 * sin2gam + wI * twoL * cos2gam);
-  const double ccI = K * uI * omL2;
-  const double caII = K * (-uII * opL2 * cos2gam + wII * twoL * sin2gam);
-  const double cbII = K * (uII * opL2 * sin2gam + wII * twoL * cos2gam);
-  const double ccII = K * uII * omL2;
+  const double caI = Kresp * (-uI * opL2 * cos2gam + wI * twoL * sin2gam);
+  const double cbI = Kresp * (uI * opL2 * sin2gam + wI * twoL * cos2gam);
+  const double ccI = Kresp * uI * omL2;
+  const double caII = Kresp * (-uII * opL2 * cos2gam + wII * twoL * sin2gam);
+  const double cbII = Kresp * (uII * opL2 * sin2gam + wII * twoL * cos2gam);
+  const double ccII = Kresp * uII * omL2;
 
   // harmonic phases: n Phi + Doppler_n = n (Phi + D1) + D0
   double D1 = 0.0, D0 = 0.0;
@@ -491,34 +643,16 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, do
     D0 = 2.0 * gimdot * kAUsec * d.sinqS * cosorbphs;
   }
   double s1, c1, sD, cD;
-  sincos(Phi + D1, &s1, &c1);
+  sincos(Phi + D1, &s1, &c1);  // harmonic n: (c1 + i s1)^n (cD + i sD)
   sincos(D0, &sD, &cD);
-  double zr = 1.0, zi = 0.0;  // (c1 + i s1)^n
   const double se = sqrt(1. - e * e);
-  double Sa = 0.0, Sb = 0.0, Sc = 0.0;
-  for (int n = 1; n <= d.nmodes; ++n) {
-    const double tr = zr * c1 - zi * s1;
-    zi = zr * s1 + zi * c1;
-    zr = tr;
-    const double cn = zr * cD - zi * sD;
-    const double sn = zi * cD + zr * sD;
-    double J[5];
-    const double x = n * e;
-    if (n == 1) {
-      double Jt[5];
-      bessel5_fp64(0, x, bstart[0], Jt);
-      J[0] = -Jt[1];
-      J[1] = Jt[0];
-      J[2] = Jt[1];
-      J[3] = Jt[2];
-      J[4] = Jt[3];
-    } else {
-      bessel5_fp64(n - 2, x, bstart[n - 1], J);
-    }
-    const double dn = (double)n;
-    Sa += dn * (J[0] - 2. * e * J[1] + 2. / dn * J[2] + 2. * e * J[3] - J[4]) * cn;
-    Sb += dn * (J[0] - 2. * J[2] + J[4]) * sn;
-    Sc += J[2] * cn;
+  double Sa, Sb, Sc;
+  switch (K) {
+    case 4: mode_sums_table<4>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 6: mode_sums_table<6>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 8: mode_sums_table<8>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 12: mode_sums_table<12>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    default: mode_sums_miller(bstart, d.nmodes, e, c1, s1, cD, sD, Sa, Sb, Sc); break;
   }
   const double a = -Amp * Sa, b = -Amp * se * Sb, cc = 2. * Amp * Sc;
   hI = caI * a + cbI * b + ccI * cc;
@@ -526,13 +660,16 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, do
 }
 
 // ------------------------------------------------------------------ pass 2
-__global__ void __launch_bounds__(kTileThreads) k_waveform_fp64(BatchView bv) {
+__global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_fp64(BatchView bv) {
   __shared__ double s_raw[kTileThreads];
   __shared__ double s_Pa[kTileThreads];
   __shared__ double s_r[3][kTileThreads];
   __shared__ double red[3][kTileThreads / 32];
   __shared__ double s_bc[4];
   __shared__ long long s_tile;
+  __shared__ double s_T[kTabModes * kTabStride];
+  __shared__ double s_ec;
+  __shared__ int s_K;
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
@@ -564,7 +701,26 @@ __global__ void __launch_bounds__(kTileThreads) k_waveform_fp64(BatchView bv) {
       s_bc[0] = rp[0];
       s_bc[1] = rp[1];
       s_bc[2] = rp[2];
+      // Bessel table centre and term count from e at the tile's first, middle and last output samples
+      const int last = min(c.end, c.neff) - 1;
+      int K = 0;
+      double ec = 0.0;
+      if (last >= c.start && d.nmodes <= kTabModes) {
+        const double e0 = spline4(bv, d, sample_time(d, c.start)).e;
+        const double e2 = spline4(bv, d, sample_time(d, last)).e;
+        ec = spline4(bv, d, sample_time(d, (c.start + last) / 2)).e;
+        const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
+        if (ec > 1e-6) K = choose_terms(2.0 * d.nmodes * de * (1.0 + de / ec));
+      }
+      s_ec = ec;
+      s_K = K;
     }
+    __syncthreads();
+    const int K = s_K;
+    const double ec = s_ec;
+    if (K > 0)
+      for (int n = tid + 1; n <= d.nmodes; n += kTileThreads)
+        build_bessel_row(s_T + (n - 1) * kTabStride, n, n * ec, K, bstart[n - 1]);
     __syncthreads();
     double prev[3] = {s_bc[0], (s_bc[1] > 0.0) ? s_bc[1] : tc.Cf[1], s_bc[2]};
     double lastP = prev[1];
@@ -656,7 +812,7 @@ __global__ void __launch_bounds__(kTileThreads) k_waveform_fp64(BatchView bv) {
         double hI = 0.0, hII = 0.0;
         if (in) {
           const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
-          harmonic_sum_fp64(d, bstart, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
+          harmonic_sum_fp64(d, bstart, s_T, ec, K, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
           if (i > d.i_plunge) {
             const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
             hI = hI / wgt;
