@@ -30,6 +30,7 @@ SOURCES = [
     "host/inspiral.cpp",
     "host/pipeline.cpp",
     "kernels/aak_dense.cu",
+    "kernels/likelihood.cu",
     "capi/aak_capi.cpp",
 ]
 

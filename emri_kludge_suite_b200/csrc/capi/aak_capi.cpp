@@ -13,8 +13,11 @@
 #include <thread>
 #include <vector>
 
+#include <cufft.h>
+
 #include "../host/pipeline.hpp"
 #include "../kernels/aak_dense.cuh"
+#include "../kernels/likelihood.cuh"
 
 using namespace aak;
 
@@ -68,6 +71,7 @@ struct aak_ctx {
   std::vector<double4> knot_y, knot_c;
   std::vector<int32_t> bessel;
   int64_t total_samples = 0, total_tiles = 0, total_knots = 0;
+  int64_t out_stride = 0;  // > 0: source s writes at s * out_stride (FFT-padded rows)
   bool uploaded = false;
   // device buffers
   DevBuf<SourceDesc> d_src;
@@ -184,7 +188,7 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
   for (int s = 0; s < n; ++s) {
     const SourcePlan &pl = ctx->plans[s];
     const int64_t len = P[s].length;
-    ctx->offsets[s + 1] = ctx->offsets[s] + len;
+    ctx->offsets[s + 1] = ctx->offsets[s] + (ctx->out_stride > 0 ? ctx->out_stride : len);
     ctx->tile_start[s + 1] = ctx->tile_start[s] + (len + kTileSamples - 1) / kTileSamples;
     if (ctx->status[s] == AAK_OK) {
       knots += (int64_t)pl.knot_t.size();
@@ -641,4 +645,280 @@ int aak_genwave(double *t, double *hI, double *hII, double timestep, int32_t vle
   return host_roundtrip(ctx, t, hI, hII);
 }
 
+
+// ====================================================================== GPU likelihood
+// GPUAAK counterpart (include/AAK_manager.hh:106-153, src/cuda/AAK_manager.cu):
+// templates are generated into FFT-padded rows, transformed in place by a
+// batched cuFFT D2Z plan and reduced against the pre-weighted data.
+struct aak_gpu {
+  aak_ctx *ctx = nullptr;
+  double T_fit = 1.0, dt = 0.0, init_dt = 0.0;
+  int32_t length = 0, init_length = 0, LISA = 1, backint = 0;
+  int64_t nbins = 0;  // length / 2 + 1
+  int64_t row = 0;    // doubles per padded template row = 2 * nbins
+  DevBuf<double> d_H[2], d_D[2], d_w[2], d_partial, d_out, d_t;
+  cufftHandle plan = 0;
+  int plan_batch = 0;
+  int32_t count = 0;     // templates currently in the rows
+  bool spectral = false; // rows hold spectra (after a likelihood)
+  std::vector<double> like;
+  double ms[4] = {0, 0, 0, 0};  // host plan, generate, FFT, reduce of the last batch
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+int gpu_capacity(aak_gpu *g, int B) {
+  int r;
+  if ((r = g->d_H[0].reserve((size_t)B * g->row)) || (r = g->d_H[1].reserve((size_t)B * g->row)) ||
+      (r = g->d_partial.reserve((size_t)B * kIpBlocksPerTemplate * 2)) || (r = g->d_out.reserve((size_t)B * 2)))
+    return r;
+  if (g->plan_batch < B) {
+    if (g->plan) cufftDestroy(g->plan);
+    g->plan = 0;
+    g->plan_batch = 0;
+    int n = g->length;
+    int inembed = (int)g->row, onembed = (int)(g->row / 2);
+    if (cufftPlanMany(&g->plan, 1, &n, &inembed, 1, (int)g->row, &onembed, 1, (int)(g->row / 2), CUFFT_D2Z, B) !=
+        CUFFT_SUCCESS) {
+      g->plan = 0;
+      return AAK_ERR_CUDA;
+    }
+    g->plan_batch = B;
+  }
+  return AAK_OK;
+}
+
+// Parameters in gpu_gen_AAK order: iota, s, p, e, M, mu, gamma, psi, alph, theta_S, phi_S, theta_K, phi_K, D.
+aak_params gpu_params(const aak_gpu *g, const double *x) {
+  aak_params p;
+  std::memset(&p, 0, sizeof(p));
+  p.length = g->length;
+  p.dt = g->dt;
+  p.T = g->length * g->dt / kYear;
+  p.f = 0.0;
+  p.T_fit = g->T_fit;
+  p.iota = x[0];
+  p.s = x[1];
+  p.p = x[2];
+  p.e = x[3];
+  p.M = x[4];
+  p.mu = x[5];
+  p.gamma = x[6];
+  p.psi = x[7];
+  p.alpha = x[8];
+  p.theta_S = x[9];
+  p.phi_S = x[10];
+  p.theta_K = x[11];
+  p.phi_K = x[12];
+  p.D = x[13];
+  p.LISA = g->LISA;
+  p.backint = g->backint;
+  return p;
+}
+
+int gpu_generate(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status, bool with_t) {
+  int r;
+  if ((r = gpu_capacity(g, B)) != AAK_OK) return r;
+  std::vector<aak_params> P(B);
+  for (int k = 0; k < B; ++k) P[k] = gpu_params(g, x + 14 * (size_t)k);
+  const auto t0 = std::chrono::steady_clock::now();
+  g->ctx->out_stride = g->row;
+  r = plan_common(g->ctx, P.data(), nullptr, B, nullptr, nthreads);
+  g->ctx->out_stride = 0;
+  g->ms[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  if (r != AAK_OK) return r;
+  for (int k = 0; k < B; ++k)
+    if (status) status[k] = g->ctx->status[k];
+  if ((r = upload(g->ctx, 0)) != AAK_OK) return r;
+  double *dt = nullptr;
+  if (with_t) {
+    if ((r = g->d_t.reserve((size_t)g->row)) != AAK_OK) return r;
+    if ((r = cuda_ok(cudaMemsetAsync(g->d_t.ptr, 0, g->row * sizeof(double), 0))) != AAK_OK) return r;
+    dt = g->d_t.ptr;
+  }
+  if (!g->ev[0])
+    for (auto &e : g->ev) cudaEventCreate(&e);
+  cudaEventRecord(g->ev[0], 0);
+  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, 0, 0)) != AAK_OK) return r;
+  cudaEventRecord(g->ev[1], 0);
+  g->count = B;
+  g->spectral = false;
+  return AAK_OK;
+}
+
+int gpu_likelihood(aak_gpu *g, double *out) {
+  if (g->count <= 0) return AAK_ERR_INVALID_PARAM;
+  if (!g->ev[0])
+    for (auto &e : g->ev) cudaEventCreate(&e);
+  if (!g->spectral) {
+    if (g->plan_batch != g->count) {
+      // a plan of a larger batch would transform stale rows: make one of this size
+      if (g->plan) cufftDestroy(g->plan);
+      g->plan = 0;
+      g->plan_batch = 0;
+      int r = gpu_capacity(g, g->count);
+      if (r != AAK_OK) return r;
+    }
+    if (cufftSetStream(g->plan, 0) != CUFFT_SUCCESS) return AAK_ERR_CUDA;
+    if (cufftExecD2Z(g->plan, g->d_H[0].ptr, reinterpret_cast<cufftDoubleComplex *>(g->d_H[0].ptr)) != CUFFT_SUCCESS ||
+        cufftExecD2Z(g->plan, g->d_H[1].ptr, reinterpret_cast<cufftDoubleComplex *>(g->d_H[1].ptr)) != CUFFT_SUCCESS)
+      return AAK_ERR_CUDA;
+    g->spectral = true;
+  }
+  cudaEventRecord(g->ev[2], 0);
+  InnerProductArgs a;
+  a.H[0] = g->d_H[0].ptr;
+  a.H[1] = g->d_H[1].ptr;
+  a.row_doubles = g->row;
+  a.D[0] = g->d_D[0].ptr;
+  a.D[1] = g->d_D[1].ptr;
+  a.w[0] = g->d_w[0].ptr;
+  a.w[1] = g->d_w[1].ptr;
+  a.nbins = g->nbins;
+  a.ntemplates = g->count;
+  a.partial = g->d_partial.ptr;
+  a.out = g->d_out.ptr;
+  launch_inner_products(a, 0);
+  cudaEventRecord(g->ev[3], 0);
+  int r = cuda_ok(cudaMemcpy(out, g->d_out.ptr, (size_t)g->count * 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (r != AAK_OK) return r;
+  float f;
+  if (cudaEventElapsedTime(&f, g->ev[0], g->ev[1]) == cudaSuccess) g->ms[1] = f;
+  if (cudaEventElapsedTime(&f, g->ev[1], g->ev[2]) == cudaSuccess) g->ms[2] = f;
+  if (cudaEventElapsedTime(&f, g->ev[2], g->ev[3]) == cudaSuccess) g->ms[3] = f;
+  cudaGetLastError();
+  return AAK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aak_gpu_create(double T_fit, int32_t init_length, int32_t length, double init_dt, double dt, int32_t LISA,
+                   int32_t backint, aak_gpu **out) {
+  if (!out) return AAK_ERR_INVALID_PARAM;
+  *out = nullptr;
+  if (length < 2 || !(dt > 0) || !(T_fit > 0)) return AAK_ERR_INVALID_PARAM;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return AAK_ERR_CUDA;
+  }
+  aak_gpu *g = new (std::nothrow) aak_gpu();
+  if (!g) return AAK_ERR_NO_MEMORY;
+  int r = aak_ctx_create(dev, &g->ctx);
+  if (r != AAK_OK) {
+    delete g;
+    return r;
+  }
+  g->T_fit = T_fit;
+  g->init_length = init_length;
+  g->length = length;
+  g->init_dt = init_dt;
+  g->dt = dt;
+  g->LISA = LISA;
+  g->backint = backint;
+  g->nbins = length / 2 + 1;
+  g->row = 2 * g->nbins;
+  // until input_data: zero data, unit weights
+  for (int ch = 0; ch < 2; ++ch) {
+    if ((r = g->d_D[ch].reserve(2 * g->nbins)) || (r = g->d_w[ch].reserve(g->nbins))) {
+      aak_gpu_destroy(g);
+      return r;
+    }
+    cudaMemset(g->d_D[ch].ptr, 0, 2 * g->nbins * sizeof(double));
+    std::vector<double> ones(g->nbins, 1.0);
+    cudaMemcpy(g->d_w[ch].ptr, ones.data(), g->nbins * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  *out = g;
+  return cuda_ok(cudaGetLastError());
+}
+
+void aak_gpu_destroy(aak_gpu *g) {
+  if (!g) return;
+  if (g->plan) cufftDestroy(g->plan);
+  for (int ch = 0; ch < 2; ++ch) {
+    g->d_H[ch].release();
+    g->d_D[ch].release();
+    g->d_w[ch].release();
+  }
+  g->d_partial.release();
+  g->d_out.release();
+  g->d_t.release();
+  for (auto &e : g->ev)
+    if (e) cudaEventDestroy(e);
+  aak_ctx_destroy(g->ctx);
+  delete g;
+}
+
+int aak_gpu_input_data(aak_gpu *g, const double *hI_f, const double *hII_f, const double *ASDinv1,
+                       const double *ASDinv2, int32_t len) {
+  if (!g || !hI_f || !hII_f || !ASDinv1 || !ASDinv2) return AAK_ERR_INVALID_PARAM;
+  if (len != g->nbins) return AAK_ERR_INVALID_PARAM;  // the reference asserts len == fft_length
+  int r;
+  if ((r = cuda_ok(cudaMemcpy(g->d_D[0].ptr, hI_f, 2 * (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
+      (r = cuda_ok(cudaMemcpy(g->d_D[1].ptr, hII_f, 2 * (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
+      (r = cuda_ok(cudaMemcpy(g->d_w[0].ptr, ASDinv1, (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
+      (r = cuda_ok(cudaMemcpy(g->d_w[1].ptr, ASDinv2, (size_t)len * sizeof(double), cudaMemcpyHostToDevice))))
+    return r;
+  return AAK_OK;
+}
+
+int aak_gpu_gen(aak_gpu *g, const double *pars14) {
+  if (!g || !pars14) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(g->ctx->mu);
+  int32_t st = 0;
+  int r = gpu_generate(g, pars14, 1, 1, &st, true);
+  if (r != AAK_OK) return r;
+  return st;
+}
+
+int aak_gpu_get_waveform(aak_gpu *g, double *t, double *hI, double *hII) {
+  if (!g || !t || !hI || !hII || g->count < 1) return AAK_ERR_INVALID_PARAM;
+  const size_t n = (size_t)g->length + 2;
+  std::vector<double> buf(n, 0.0);
+  int r;
+  const size_t m = std::min(n, (size_t)g->row);
+  double *dst[3] = {t, hI, hII};
+  const double *src[3] = {g->d_t.ptr, g->d_H[0].ptr, g->d_H[1].ptr};
+  for (int k = 0; k < 3; ++k) {
+    std::fill(dst[k], dst[k] + n, 0.0);
+    if (!src[k]) continue;
+    if ((r = cuda_ok(cudaMemcpy(dst[k], src[k], m * sizeof(double), cudaMemcpyDeviceToHost))) != AAK_OK) return r;
+  }
+  return AAK_OK;
+}
+
+int aak_gpu_likelihood(aak_gpu *g, double *out2) {
+  if (!g || !out2) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(g->ctx->mu);
+  if (g->count != 1) return AAK_ERR_INVALID_PARAM;
+  return gpu_likelihood(g, out2);
+}
+
+int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int32_t max_batch, int32_t nthreads,
+                             double *out, int32_t *status) {
+  if (!g || !params || !out || nsrc <= 0) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(g->ctx->mu);
+  if (max_batch <= 0) max_batch = 256;
+  double tot[4] = {0, 0, 0, 0};
+  for (int32_t k0 = 0; k0 < nsrc; k0 += max_batch) {
+    const int B = std::min<int32_t>(max_batch, nsrc - k0);
+    int r = gpu_generate(g, params + 14 * (size_t)k0, B, nthreads, status ? status + k0 : nullptr, false);
+    if (r != AAK_OK) return r;
+    if ((r = gpu_likelihood(g, out + 2 * (size_t)k0)) != AAK_OK) return r;
+    for (int q = 0; q < 4; ++q) tot[q] += g->ms[q];
+  }
+  for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
+  return AAK_OK;
+}
+
+int aak_gpu_last_timing(aak_gpu *g, double *ms4) {
+  if (!g || !ms4) return AAK_ERR_INVALID_PARAM;
+  for (int q = 0; q < 4; ++q) ms4[q] = g->ms[q];
+  return AAK_OK;
+}
+
 }  // extern "C"
+}  // extern "C" (GPU likelihood)

@@ -177,6 +177,46 @@ int aak_probe_fp64_tflops(int32_t device, double *tflops);
 int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nmodes_override,
                         int32_t nthreads, double *h_hI, double *h_hII, int64_t *offsets, int32_t *status);
 
+/* ------------------------------------------------------------------ GPU likelihood */
+/* Counterpart of the reference class GPUAAK (include/AAK_manager.hh:106-153,
+ * src/cuda/AAK_manager.cu, pygpuAAK/GPUAAK.pyx:50-93), on the current CUDA
+ * device.  init_length / init_dt are accepted for call compatibility; the
+ * coarse grid follows the reference CPU AAK.  Templates are generated with
+ * the reference CPU conventions. */
+typedef struct aak_gpu aak_gpu;
+
+/* GPUAAK(T_fit, init_length, length, init_dt, dt, LISA, backint) */
+int aak_gpu_create(double T_fit, int32_t init_length, int32_t length, double init_dt, double dt, int32_t LISA,
+                   int32_t backint, aak_gpu **out);
+void aak_gpu_destroy(aak_gpu *g);
+
+/* input_data (AAK_manager.cu:135-152): pre-weighted data spectra of both
+ * channels as interleaved complex (2 x len doubles) and the weights
+ * S_n^{-1/2} sqrt(dt/N) (len doubles); len must be length/2 + 1. */
+int aak_gpu_input_data(aak_gpu *g, const double *hI_f, const double *hII_f, const double *ASDinv1,
+                       const double *ASDinv2, int32_t len);
+
+/* gpu_gen_AAK (AAK_manager.cu:154-260): pars14 = iota, s, p, e, M, mu, gamma,
+ * psi, alph, theta_S, phi_S, theta_K, phi_K, D. */
+int aak_gpu_gen(aak_gpu *g, const double *pars14);
+
+/* GetWaveform (AAK_manager.cu:454-458): t, hI, hII of length+2 doubles; after
+ * aak_gpu_likelihood hI/hII hold the interleaved half spectra. */
+int aak_gpu_get_waveform(aak_gpu *g, double *t, double *hI, double *hII);
+
+/* Likelihood (AAK_manager.cu:352-446): out2 = [4 Re<h|d>, 4 <h|h>]. */
+int aak_gpu_likelihood(aak_gpu *g, double *out2);
+
+/* Batched likelihoods (no reference counterpart; replaces the serial loop of
+ * pygpuAAK.py:204-232): params nsrc x 14 (gpu_gen_AAK order), out nsrc x 2,
+ * per-template status (optional).  Templates run in batches of max_batch
+ * (<= 0: 256); host planning uses nthreads threads (<= 0: all). */
+int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int32_t max_batch, int32_t nthreads,
+                             double *out, int32_t *status);
+
+/* Milliseconds of the last batch: host planning, waveform kernels, FFT, reduction. */
+int aak_gpu_last_timing(aak_gpu *g, double *ms4);
+
 #ifdef __cplusplus
 }
 #endif
