@@ -181,6 +181,60 @@ def cpu_reference(sources, budget_s: float = 15.0, sample_len: int = 20000, proc
             "wall_s": wall}
 
 
+# ----------------------------------------------------------------------------- likelihood (config 4)
+FIDUCIAL = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])  # gpu_gen_AAK order
+LIKE_LENGTH = 3_200_000  # 1 yr at dt = 10 s rounded up to the 5-smooth FFT length 2^10 * 5^5
+
+
+def config4_templates(n: int, seed: int = SEED + 4):
+    """Fiducial (configuration 0 source, T ~ 1 yr) perturbed by 1e-5 relative in M, mu, p0 and 1e-3 rad in angles."""
+    rng = np.random.default_rng(seed)
+    X = np.tile(FIDUCIAL, (n, 1))
+    for j in (2, 4, 5):
+        X[:, j] *= 1.0 + 1e-5 * rng.standard_normal(n)
+    for j in (0, 6, 7, 8, 9, 10, 11, 12):
+        X[:, j] += 1e-3 * rng.standard_normal(n)
+    return X
+
+
+def run_likelihood(n_templates: int, local_rank: int) -> dict:
+    """likelihoods/s of the batched path: host planning + waveforms + FFT + reduction, end to end per call."""
+    from emri_kludge_suite_b200.gpuAAK import GPUAAK
+    from emri_kludge_suite_b200.LISAnoise import LISA_Noise, generate_noise_frequencies, generate_noise_single_channel
+
+    g = GPUAAK(1.0, 100, LIKE_LENGTH, 100.0, DT, True, False)
+    freqs = generate_noise_frequencies(LIKE_LENGTH * DT, 1 / DT)
+    freqs[0] = freqs[1] / 10.0
+    w = 1.0 / np.sqrt(LISA_Noise(freqs, dur=1)) * np.sqrt(DT / LIKE_LENGTH)
+    # data: fiducial waveform + seeded LISA-coloured noise, pre-weighted
+    ones = np.ones_like(w)
+    zero = np.zeros(len(w), dtype=np.complex128)
+    g.input_data(zero, zero, ones, ones)
+    g.gpu_gen_AAK(*FIDUCIAL)
+    g.Likelihood()
+    _, sI, sII = g.GetWaveform(is_Fourier=True)
+    nb = len(w)
+    hI_f = sI[0:2 * nb:2] + 1j * sI[1:2 * nb:2]
+    hII_f = sII[0:2 * nb:2] + 1j * sII[1:2 * nb:2]
+    rng = np.random.default_rng(SEED + 40)
+    df = 1.0 / (LIKE_LENGTH * DT)
+    n1 = generate_noise_single_channel(LISA_Noise, [], {"dur": 1}, df, freqs, rng)
+    n2 = generate_noise_single_channel(LISA_Noise, [], {"dur": 1}, df, freqs, rng)
+    g.input_data(w * (hI_f + n1), w * (hII_f + n2), w, w)
+    X = config4_templates(n_templates)
+    g.likelihood_batch(X[: min(64, n_templates)])  # warm-up (plans, FFT plan)
+    t0 = time.perf_counter()
+    out, st = g.likelihood_batch(X, return_status=True)
+    wall = time.perf_counter() - t0
+    ms = g.last_timing_ms()
+    gpu_s = (ms["waveform"] + ms["fft"] + ms["reduce"]) * 1e-3
+    return {"likelihoods_per_s": n_templates / wall, "likelihoods_per_s_gpu": n_templates / gpu_s,
+            "templates": n_templates, "samples_per_template": LIKE_LENGTH, "failed": int(np.sum(st != 0)),
+            "ms": ms, "workload": "config4: fiducial config-0 source, 3.2e6 samples (1.014 yr, dt=10 s), LISA-coloured "
+                                  "noise, templates perturbed 1e-5 rel (M, mu, p0) / 1e-3 rad (angles), "
+                                  "reference harmonic rule, FP64"}
+
+
 # ----------------------------------------------------------------------------- GPU arm
 def run_gpu(args, rank, world, local_rank):
     import torch
@@ -320,6 +374,11 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": launches,
         "host_plan_seconds": t_plan,
     }
+    if args.likelihood > 0:
+        del hI, hII, hIh, hIIh
+        wb.close()
+        torch.cuda.empty_cache()
+        out["likelihood"] = run_likelihood(args.likelihood, local_rank)
     return out
 
 
@@ -333,6 +392,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--likelihood", type=int, default=1024, help="config-4 templates to time (0: skip)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

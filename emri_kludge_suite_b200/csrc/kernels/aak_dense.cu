@@ -146,6 +146,38 @@ __device__ __forceinline__ double block_scan(double v, double *red, double &tota
   return v + pre;
 }
 
+// block-wide inclusive scan of three values at once (one pair of barriers)
+__device__ __forceinline__ void block_scan3(double v[3], double (*red)[kTileThreads / 32], double tot[3]) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const double n = __shfl_up_sync(0xffffffffu, v[q], o);
+      if (l >= o) v[q] += n;
+    }
+  }
+  __syncthreads();
+  if (l == 31) {
+    red[0][w] = v[0];
+    red[1][w] = v[1];
+    red[2][w] = v[2];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double pre = 0.0, t = 0.0;
+#pragma unroll
+    for (int k = 0; k < kTileThreads / 32; ++k) {
+      const double r = red[q][k];
+      if (k < w) pre += r;
+      t += r;
+    }
+    v[q] += pre;
+    tot[q] = t;
+  }
+}
+
 // ------------------------------------------------------------------ tile geometry
 struct TileCtx {
   int s;        // source
@@ -173,115 +205,128 @@ struct Lin {
 };
 
 // ------------------------------------------------------------------ pass 1
+// Per tile: (A) the three phase rates of every sample of the tile and of the
+// samples just before and after it, independent per thread (instruction-level
+// parallelism), into shared memory; (B) the clamped Phidot, the AB2
+// increments and their tile sums; (C) one fused block reduction.
+constexpr int kSlots = kTileSamples + 2;  // slot s <-> sample start - 1 + s
+
+__device__ __forceinline__ Lin clamp_phidot(const double *raw, int slot, int first_fwd_slot) {
+  // P at `slot`: the raw rate if positive, else the last positive raw rate at a
+  // forward sample before it in the tile, else the rate carried into the tile
+  if (raw[slot] > 0.0) return Lin{raw[slot], 0.0};
+  for (int k = slot - 1; k >= first_fwd_slot; --k)
+    if (raw[k] > 0.0) return Lin{raw[k], 0.0};
+  return Lin{0.0, 1.0};
+}
+
 __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
-  __shared__ double s_raw[kTileThreads];
-  __shared__ double s_Pa[kTileThreads], s_Pb[kTileThreads];
-  __shared__ double s_r[3][kTileThreads];
-  __shared__ double red[kTileThreads / 32];
-  __shared__ double s_bc[4];
+  __shared__ double s_r[3][kSlots];
+  __shared__ double red[7][kTileThreads / 32];
   const int tid = threadIdx.x;
   for (int64_t g = blockIdx.x; g < bv.total_tiles; g += gridDim.x) {
     const SourceDesc *dp;
     const TileCtx c = tile_ctx(bv, g, dp);
     const SourceDesc &d = *dp;
     if (d.status != 0) continue;
-    double fA[3] = {0, 0, 0}, fB = 0.0, bA[3] = {0, 0, 0};
-    // rate just before the tile (concrete unless non-positive for Phi)
-    if (tid == 0) {
-      double rp[3] = {0, 0, 0};
-      const int ip = c.start - 1;
-      if (ip >= 0 && ip < d.vlength) phase_rates(d, spline4(bv, d, sample_time(d, ip)), rp);
-      s_bc[0] = rp[0];
-      s_bc[1] = rp[1];
-      s_bc[2] = rp[2];
+    const int lim = min(c.end, c.neff);  // samples [start, lim) feed the output
+    TileSummary &ts = bv.summ[g];
+    if (lim <= c.start) {  // nothing to accumulate (after the taper)
+      if (tid == 0) {
+        for (int q = 0; q < 3; ++q) ts.fA[q] = ts.fB[q] = ts.bA[q] = ts.bB[q] = ts.last_rate[q] = ts.first_rate[q] = 0.0;
+        ts.has_last[0] = ts.has_last[1] = ts.has_last[2] = 0;
+      }
+      continue;
+    }
+    // (A) rates, two independent samples per pass
+#pragma unroll 1
+    for (int s = tid; s < kSlots; s += 2 * kTileThreads) {
+      const int s2 = s + kTileThreads;
+      const int i1 = c.start - 1 + s, i2 = c.start - 1 + s2;
+      double r1[3] = {0, 0, 0}, r2[3] = {0, 0, 0};
+      const bool n1 = i1 >= 0 && i1 < d.vlength && i1 <= lim;
+      const bool n2 = s2 < kSlots && i2 >= 0 && i2 < d.vlength && i2 <= lim;
+      if (n1) phase_rates(d, spline4(bv, d, sample_time(d, i1)), r1);
+      if (n2) phase_rates(d, spline4(bv, d, sample_time(d, i2)), r2);
+      s_r[0][s] = r1[0];
+      s_r[1][s] = n1 ? r1[1] : -1.0;
+      s_r[2][s] = r1[2];
+      if (s2 < kSlots) {
+        s_r[0][s2] = r2[0];
+        s_r[1][s2] = n2 ? r2[1] : -1.0;
+        s_r[2][s2] = r2[2];
+      }
     }
     __syncthreads();
-    double prev[3] = {s_bc[0], 0.0, s_bc[2]};
-    Lin prevP = (s_bc[1] > 0.0) ? Lin{s_bc[1], 0.0} : Lin{0.0, 1.0};
-    Lin lastP = prevP;
+    // (B) increments
+    const int first_fwd_slot = max(d.i0, c.start) - c.start + 1;
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // fA[0..2], fB, bA[0..2]
+#pragma unroll 1
     for (int ch = 0; ch < kTileChunks; ++ch) {
-      const int i = c.start + ch * kTileThreads + tid;
-      const bool in = i < c.end && i < c.neff;
-      const bool vf = in && i >= d.i0;
-      const bool vb = in && i >= 1 && i <= d.i0;
-      double r[3] = {0, 0, 0};
-      if (vf || vb) phase_rates(d, spline4(bv, d, sample_time(d, i)), r);
-      s_raw[tid] = vf ? r[1] : -1.0;
-      s_r[0][tid] = r[0];
-      s_r[1][tid] = r[1];
-      s_r[2][tid] = r[2];
-      __syncthreads();
-      // clamp
-      Lin P = {r[1], 0.0};
-      if (vf && !(r[1] > 0.0)) {
-        int k = tid - 1;
-        while (k >= 0 && !(s_raw[k] > 0.0)) --k;
-        P = (k >= 0) ? Lin{s_raw[k], 0.0} : lastP;
-      }
-      s_Pa[tid] = P.a;
-      s_Pb[tid] = P.b;
-      __syncthreads();
-      const Lin Pm = (tid > 0) ? Lin{s_Pa[tid - 1], s_Pb[tid - 1]} : lastP;
-      if (vf) {
-        if (i == d.i0) {
-          fA[0] += r[0] * d.dt;
-          fA[1] += P.a * d.dt;
-          fB += P.b * d.dt;
-          fA[2] += r[2] * d.dt;
+      const int k = c.start + ch * kTileThreads + tid;
+      if (k >= lim) continue;
+      const int sl = k - c.start + 1;
+      if (k >= d.i0) {
+        const Lin P = clamp_phidot(s_r[1], sl, first_fwd_slot);
+        if (k == d.i0) {
+          acc[0] += s_r[0][sl] * d.dt;
+          acc[1] += P.a * d.dt;
+          acc[3] += P.b * d.dt;
+          acc[2] += s_r[2][sl] * d.dt;
         } else {
-          const double rm0 = (tid > 0) ? s_r[0][tid - 1] : prev[0];
-          const double rm2 = (tid > 0) ? s_r[2][tid - 1] : prev[2];
-          fA[0] += (1.5 * r[0] - .5 * rm0) * d.dt;
-          fA[1] += (1.5 * P.a - .5 * Pm.a) * d.dt;
-          fB += (1.5 * P.b - .5 * Pm.b) * d.dt;
-          fA[2] += (1.5 * r[2] - .5 * rm2) * d.dt;
+          // P at k-1: inside the tile the same clamp; k-1 = start-1 is the tile boundary
+          const Lin Pm = (sl - 1 >= first_fwd_slot) ? clamp_phidot(s_r[1], sl - 1, first_fwd_slot)
+                                                    : ((s_r[1][0] > 0.0) ? Lin{s_r[1][0], 0.0} : Lin{0.0, 1.0});
+          acc[0] += (1.5 * s_r[0][sl] - .5 * s_r[0][sl - 1]) * d.dt;
+          acc[1] += (1.5 * P.a - .5 * Pm.a) * d.dt;
+          acc[3] += (1.5 * P.b - .5 * Pm.b) * d.dt;
+          acc[2] += (1.5 * s_r[2][sl] - .5 * s_r[2][sl - 1]) * d.dt;
         }
       }
-      if (vb) {
-        double rn[3];
-        if (i == d.i0) {
-          bA[0] += r[0] * d.dt;
-          bA[1] += r[1] * d.dt;
-          bA[2] += r[2] * d.dt;
+      if (k >= 1 && k <= d.i0) {
+        if (k == d.i0) {
+          acc[4] += s_r[0][sl] * d.dt;
+          acc[5] += s_r[1][sl] * d.dt;
+          acc[6] += s_r[2][sl] * d.dt;
         } else {
-          if (tid < kTileThreads - 1) {
-            rn[0] = s_r[0][tid + 1];
-            rn[1] = s_r[1][tid + 1];
-            rn[2] = s_r[2][tid + 1];
-          } else {
-            phase_rates(d, spline4(bv, d, sample_time(d, i + 1)), rn);
-          }
-          bA[0] += (1.5 * r[0] - .5 * rn[0]) * d.dt;
-          bA[1] += (1.5 * r[1] - .5 * rn[1]) * d.dt;
-          bA[2] += (1.5 * r[2] - .5 * rn[2]) * d.dt;
+          acc[4] += (1.5 * s_r[0][sl] - .5 * s_r[0][sl + 1]) * d.dt;
+          acc[5] += (1.5 * s_r[1][sl] - .5 * s_r[1][sl + 1]) * d.dt;
+          acc[6] += (1.5 * s_r[2][sl] - .5 * s_r[2][sl + 1]) * d.dt;
         }
       }
-      // carry chunk state: clamped P and raw rates of the last thread
-      const Lin P255 = {s_Pa[kTileThreads - 1], s_Pb[kTileThreads - 1]};
-      const int ilast = c.start + ch * kTileThreads + kTileThreads - 1;
-      if (ilast >= d.i0) lastP = P255;
-      prev[0] = s_r[0][kTileThreads - 1];
-      prev[2] = s_r[2][kTileThreads - 1];
-      __syncthreads();
     }
-    // reductions
-    TileSummary &ts = bv.summ[g];
-    for (int q = 0; q < 3; ++q) {
-      const double a = block_sum(fA[q], red);
-      if (tid == 0) ts.fA[q] = a;
-      const double b = block_sum(bA[q], red);
-      if (tid == 0) ts.bA[q] = b;
-    }
-    const double fb = block_sum(fB, red);
+    // (C) fused reduction of the seven sums
+#pragma unroll
+    for (int q = 0; q < 7; ++q)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    const int w = tid >> 5, l = tid & 31;
+    if (l == 0)
+#pragma unroll
+      for (int q = 0; q < 7; ++q) red[q][w] = acc[q];
+    __syncthreads();
     if (tid == 0) {
+      double tot[7];
+      for (int q = 0; q < 7; ++q) {
+        tot[q] = 0.0;
+        for (int k = 0; k < kTileThreads / 32; ++k) tot[q] += red[q][k];
+      }
+      ts.fA[0] = tot[0];
+      ts.fA[1] = tot[1];
+      ts.fA[2] = tot[2];
       ts.fB[0] = 0.0;
-      ts.fB[1] = fb;
+      ts.fB[1] = tot[3];
       ts.fB[2] = 0.0;
+      ts.bA[0] = tot[4];
+      ts.bA[1] = tot[5];
+      ts.bA[2] = tot[6];
       ts.bB[0] = ts.bB[1] = ts.bB[2] = 0.0;
-      // last clamped Phidot in the tile if concrete
-      const int last_f = min(c.end, c.neff) - 1;
-      ts.has_last[1] = (last_f >= max(c.start, d.i0) && lastP.b == 0.0) ? 1 : 0;
-      ts.last_rate[1] = lastP.a;
+      // last clamped Phidot of the tile, if it does not depend on the carry
+      const int last_f = lim - 1;
+      Lin Pl = {0.0, 1.0};
+      if (last_f >= max(c.start, d.i0)) Pl = clamp_phidot(s_r[1], last_f - c.start + 1, first_fwd_slot);
+      ts.has_last[1] = (last_f >= max(c.start, d.i0) && Pl.b == 0.0) ? 1 : 0;
+      ts.last_rate[1] = Pl.a;
       ts.has_last[0] = ts.has_last[2] = 0;
       ts.last_rate[0] = ts.last_rate[2] = 0.0;
       ts.first_rate[0] = ts.first_rate[1] = ts.first_rate[2] = 0.0;
@@ -789,23 +834,29 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_
         }
       }
       double X[3];
+      double inclF[3] = {incF[0], incF[1], incF[2]}, totF[3];
+      block_scan3(inclF, red, totF);
+      double inclB[3] = {0.0, 0.0, 0.0}, totB[3] = {0.0, 0.0, 0.0};
+      if (d.i0 > 0 && c.start <= d.i0) {  // backward region present in this tile (tile-uniform)
+        inclB[0] = incB[0];
+        inclB[1] = incB[1];
+        inclB[2] = incB[2];
+        block_scan3(inclB, red, totB);
+      }
 #pragma unroll
       for (int qq = 0; qq < 3; ++qq) {
-        double totF, totB;
-        const double inclF = block_scan(incF[qq], red[qq], totF);
-        const double inclB = block_scan(incB[qq], red[qq], totB);
         if (i > d.i0) {
           // X_i = X0 + carry + (forward increments of samples < i in this tile)
-          X[qq] = X0[qq] + (tc.fwd_hi[qq] + (tc.fwd_lo[qq] + (runF[qq] + (inclF - incF[qq]))));
+          X[qq] = X0[qq] + (tc.fwd_hi[qq] + (tc.fwd_lo[qq] + (runF[qq] + (inclF[qq] - incF[qq]))));
         } else if (i == d.i0) {
           X[qq] = X0[qq];
         } else {
           // X_i = X0 - (backward increments of samples in (i, i0])
-          const double after_in_tile = ts.bA[qq] - (runB[qq] + inclB);
+          const double after_in_tile = ts.bA[qq] - (runB[qq] + inclB[qq]);
           X[qq] = X0[qq] - (tc.bwd_hi[qq] + (tc.bwd_lo[qq] + after_in_tile));
         }
-        runF[qq] += totF;
-        runB[qq] += totB;
+        runF[qq] += totF[qq];
+        runB[qq] += totB[qq];
       }
       // output sample
       if (inrange) {
