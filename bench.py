@@ -311,6 +311,44 @@ def run_gpu(args, rank, world, local_rank):
         N_all = float(N)
     value = N_all * args.steps / (ms * 1e-3)
 
+    # ---- split precision on the same batch, and its accuracy against the FP64 outputs
+    hI2 = torch.empty_like(hI)
+    hII2 = torch.empty_like(hII)
+    for _ in range(args.warmup):
+        wb.run(hI2.data_ptr(), hII2.data_ptr(), precision=1, stream=sptr)
+    L.aak_batch_set_profiling(wb._ctx, 1)
+    kern_s = np.zeros(3)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        wb.run(hI2.data_ptr(), hII2.data_ptr(), precision=1, stream=sptr)
+        _lib.check(L.aak_batch_kernel_ms(wb._ctx, ms3), "kernel timing")
+        kern_s += np.array(ms3[:])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    L.aak_batch_set_profiling(wb._ctx, 0)
+    ms_split = ev0.elapsed_time(ev1)
+    kern_s /= args.steps
+    worst_mm, worst_rel, mms = 0.0, 0.0, []
+    o = wb.offsets
+    for s in range(len(sources)):
+        a1, a2 = hI[o[s]:o[s + 1]], hII[o[s]:o[s + 1]]
+        b1, b2 = hI2[o[s]:o[s + 1]], hII2[o[s]:o[s + 1]]
+        aa = float(a1.dot(a1) + a2.dot(a2))
+        bb = float(b1.dot(b1) + b2.dot(b2))
+        ab = float(a1.dot(b1) + a2.dot(b2))
+        mm = 1.0 - ab / math.sqrt(aa * bb) if aa > 0 and bb > 0 else 0.0
+        rel = float(torch.maximum((a1 - b1).abs().max(), (a2 - b2).abs().max()) /
+                    torch.maximum(a1.abs().max(), a2.abs().max()))
+        mms.append(mm)
+        worst_mm, worst_rel = max(worst_mm, mm), max(worst_rel, rel)
+    split = {"value": N_all * args.steps / (ms_split * 1e-3), "unit": "samples/s", "ms_per_step": ms_split / args.steps,
+             "kernel_ms": {"phase_tile_sums": kern_s[0], "phase_carry": kern_s[1], "waveform_split": kern_s[2]},
+             "vs_fp64_path": {"max_mismatch": worst_mm, "median_mismatch": float(np.median(mms)),
+                              "max_rel_dh": worst_rel},
+             "speedup_vs_fp64": ms / ms_split}
+    del hI2, hII2
+
     # ---- end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     hIh = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -368,6 +406,7 @@ def run_gpu(args, rank, world, local_rank):
                    "l2": "outputs 16 B/sample x samples_per_gpu exceed the 126 MB L2",
                    "parallelism": f"sources sharded, {world} rank(s)"},
         "kernel_ms": {"phase_tile_sums": kern[0], "phase_carry": kern[1], "waveform_fp64": kern[2]},
+        "split_precision": split,
         "roofline": roofline,
         "clocks": clk,
         "e2e": e2e,

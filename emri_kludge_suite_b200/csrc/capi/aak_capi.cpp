@@ -295,7 +295,7 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   if (!ctx->uploaded) return AAK_ERR_INVALID_PARAM;
   if (!hI || !hII) return AAK_ERR_INVALID_PARAM;
   if (traj && traj_stride < ctx->total_samples) return AAK_ERR_INVALID_PARAM;
-  if (precision != 0) return AAK_ERR_INVALID_PARAM;
+  if (precision != 0 && precision != 1) return AAK_ERR_INVALID_PARAM;
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
   BatchView bv;
@@ -317,7 +317,7 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   bv.work_counter = ctx->d_counter.ptr;
   if (ctx->profile && !ctx->ev[0])
     for (auto &e : ctx->ev) cudaEventCreate(&e);
-  launch_dense_fp64(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr);
+  launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
   ctx->last_launches = 3;
   return cuda_ok(cudaGetLastError());
 }
@@ -653,7 +653,7 @@ int aak_genwave(double *t, double *hI, double *hII, double timestep, int32_t vle
 struct aak_gpu {
   aak_ctx *ctx = nullptr;
   double T_fit = 1.0, dt = 0.0, init_dt = 0.0;
-  int32_t length = 0, init_length = 0, LISA = 1, backint = 0;
+  int32_t length = 0, init_length = 0, LISA = 1, backint = 0, precision = 0;
   int64_t nbins = 0;  // length / 2 + 1
   int64_t row = 0;    // doubles per padded template row = 2 * nbins
   DevBuf<double> d_H[2], d_D[2], d_w[2], d_partial, d_out, d_t;
@@ -740,7 +740,7 @@ int gpu_generate(aak_gpu *g, const double *x, int B, int nthreads, int32_t *stat
   if (!g->ev[0])
     for (auto &e : g->ev) cudaEventCreate(&e);
   cudaEventRecord(g->ev[0], 0);
-  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, 0, 0)) != AAK_OK) return r;
+  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, g->precision, 0)) != AAK_OK) return r;
   cudaEventRecord(g->ev[1], 0);
   g->count = B;
   g->spectral = false;
@@ -911,6 +911,12 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
     for (int q = 0; q < 4; ++q) tot[q] += g->ms[q];
   }
   for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
+  return AAK_OK;
+}
+
+int aak_gpu_set_precision(aak_gpu *g, int32_t precision) {
+  if (!g || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
+  g->precision = precision;
   return AAK_OK;
 }
 

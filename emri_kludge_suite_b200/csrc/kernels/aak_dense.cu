@@ -704,8 +704,195 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, co
   hII = caII * a + cbII * b + ccII * cc;
 }
 
+// ------------------------------------------------------------------ split precision
+// FP64: spline, rates, phase sums and every angle reduction; FP32: geometry,
+// antenna response, Bessel evaluation and the harmonic recurrence.
+constexpr int kTabStrideF = 16;  // floats per FP32 table row (rows padded to 64 B)
+
+// x mod 2pi in [-pi, pi], two-term Cody-Waite reduction in FP64, returned as float
+__device__ __forceinline__ float reduce_2pi_f(double x) {
+  const double k = rint(x * (1.0 / kTwoPi));
+  const double r = fma(-k, 2.4492935982947064e-16, fma(-k, 6.283185307179586, x));
+  return (float)r;
+}
+
+__device__ __forceinline__ int choose_terms_f32(double qmax) {
+  if (qmax <= 3e-3) return 3;
+  if (qmax <= 2e-2) return 4;
+  if (qmax <= 1e-1) return 6;
+  if (qmax <= 3e-1) return 8;
+  return 0;
+}
+
+template <int K>
+__device__ __forceinline__ void mode_sums_table_f32(const float *Tf, int nmodes, float e, float lp, float half_dl,
+                                                    float c1, float s1, float cD, float sD, float &Sa, float &Sb,
+                                                    float &Sc) {
+  const float lam = exp2f(lp);
+  float zr = 1.f, zi = 0.f;
+  float sa = 0.f, sb = 0.f, sc = 0.f;
+#pragma unroll 2
+  for (int n = 1; n <= nmodes; ++n) {
+    const float4 *row = reinterpret_cast<const float4 *>(Tf + (n - 1) * kTabStrideF);
+    float T[16];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const float4 x = row[v];
+      T[4 * v] = x.x;
+      T[4 * v + 1] = x.y;
+      T[4 * v + 2] = x.z;
+      T[4 * v + 3] = x.w;
+    }
+    const float c = (float)n * half_dl;
+    float w[K + 1];
+    w[0] = 1.f;
+#pragma unroll
+    for (int k = 1; k <= K; ++k) w[k] = w[k - 1] * c * (1.f / (float)k);
+    float pj = exp2f((float)((n == 1) ? -1 : n - 2) * lp);  // lambda^b
+    float J[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      float s = w[K] * T[j + K];
+#pragma unroll
+      for (int k = K - 1; k >= 0; --k) s = fmaf(w[k], T[j + k], s);
+      J[j] = pj * s;
+      pj *= lam;
+    }
+    const float tr = zr * c1 - zi * s1;
+    zi = fmaf(zr, s1, zi * c1);
+    zr = tr;
+    const float cn = zr * cD - zi * sD;
+    const float sn = fmaf(zi, cD, zr * sD);
+    const float dn = (float)n;
+    sa += dn * (J[0] - 2.f * e * J[1] + 2.f / dn * J[2] + 2.f * e * J[3] - J[4]) * cn;
+    sb += dn * (J[0] - 2.f * J[2] + J[4]) * sn;
+    sc += J[2] * cn;
+  }
+  Sa = sa;
+  Sb = sb;
+  Sc = sc;
+}
+
+// h_I, h_II at one sample in split precision (same algebra as harmonic_sum_fp64).
+__device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, const float *Tf, double ec, int K,
+                                   double t, const Traj4 &q, double gim, double Phi, double alp, double nu,
+                                   double gimdot, double &hI, double &hII) {
+  const float coslam = (float)d.coslam, sinlam = (float)d.sinlam;
+  const float cosqS = (float)d.cosqS, sinqS = (float)d.sinqS, cosqK = (float)d.cosqK, sinqK = (float)d.sinqK;
+  const float cosphiK = (float)d.cosphiK, sinphiK = (float)d.sinphiK;
+  const float phiS = (float)d.phiS, phiK = (float)d.phiK;
+  float sinalp, cosalp;
+  sincosf(reduce_2pi_f(alp), &sinalp, &cosalp);
+  const float cosqL = cosqK * coslam + sinqK * sinlam * cosalp;
+  const float sinqL = sqrtf(fmaxf(1.f - cosqL * cosqL, 0.f));
+  const float phiLup = sinqK * sinphiK * coslam - cosphiK * sinlam * sinalp - cosqK * sinphiK * sinlam * cosalp;
+  const float phiLdown = sinqK * cosphiK * coslam + sinphiK * sinlam * sinalp - cosqK * cosphiK * sinlam * cosalp;
+  const float phiL = atan2f(phiLup, phiLdown);
+  const float Ldotn = cosqL * cosqS + sinqL * sinqS * cosf(phiL - phiS);
+  const float Ldotn2 = Ldotn * Ldotn;
+  const float Sdotn = cosqK * cosqS + sinqK * sinqS * cosf(phiK - phiS);
+  const float betaup = -Sdotn + coslam * Ldotn;
+  const float betadown = sinqS * sinf(phiK - phiS) * sinlam * cosalp + (cosqK * Sdotn - cosqS) / sinqK * sinlam * sinalp;
+  const float beta = atan2f(betaup, betadown);
+  float sin2gam, cos2gam;
+  sincosf(2.f * (reduce_2pi_f(gim) + beta), &sin2gam, &cos2gam);
+
+  float cosorbphs = 0.f, FplusI, FcrosI, FplusII, FcrosII, Kresp;
+  const float hs3 = (float)kHalfSqrt3;
+  if (d.mich) {
+    const double orbd = kTwoPi * t / kYear;
+    const float orbphs = reduce_2pi_f(orbd);
+    float sinorbphs;
+    sincosf(reduce_2pi_f(orbd - d.phiS), &sinorbphs, &cosorbphs);
+    const float cosq = .5f * cosqS - hs3 * sinqS * cosorbphs;
+    const float phiw = orbphs + atan2f(hs3 * cosqS + .5f * sinqS * cosorbphs, sinqS * sinorbphs);
+    const float psiup = .5f * cosqK - hs3 * sinqK * cosf(reduce_2pi_f(orbd - d.phiK)) - cosq * Sdotn;
+    float so, co;
+    sincosf(orbphs, &so, &co);
+    const float psidown = .5f * sinqK * sinqS * sinf(phiK - phiS) -
+                          hs3 * co * (cosqK * sinqS * sinf(phiS) - cosqS * sinqK * sinf(phiK)) -
+                          hs3 * so * (cosqS * sinqK * cosf(phiK) - cosqK * sinqS * cosf(phiS));
+    const float psi = atan2f(psiup, psidown);
+    const float cosq1 = .5f * (1.f + cosq * cosq);
+    float sin2phi, cos2phi, sin2psi, cos2psi;
+    sincosf(2.f * phiw, &sin2phi, &cos2phi);
+    sincosf(2.f * psi, &sin2psi, &cos2psi);
+    FplusI = cosq1 * cos2phi * cos2psi - cosq * sin2phi * sin2psi;
+    FcrosI = cosq1 * cos2phi * sin2psi + cosq * sin2phi * cos2psi;
+    FplusII = cosq1 * sin2phi * cos2psi + cosq * cos2phi * sin2psi;
+    FcrosII = cosq1 * sin2phi * sin2psi - cosq * cos2phi * cos2psi;
+    Kresp = hs3;
+  } else {
+    const float up_ldc = cosqS * sinqK * cosf(phiS - phiK) - cosqK * sinqS;
+    const float dw_ldc = sinqK * sinf(phiS - phiK);
+    const float psi_ldc = (dw_ldc != 0.f) ? -atan2f(up_ldc, dw_ldc) : 0.5f * (float)kPi;
+    float s2, c2;
+    sincosf(2.f * psi_ldc, &s2, &c2);
+    FplusI = c2;
+    FcrosI = -s2;
+    FplusII = s2;
+    FcrosII = c2;
+    Kresp = 1.f;
+  }
+  const float Amp = powf((float)(omega_phi(q.v, q.e, d.coslam, q.S, q.M) * d.M_phys_sec), 2.f / 3.f) * (float)d.zeta;
+  float rot0, rot1;
+  {
+    const float n0 = sinqS * cosf(phiS), n1 = sinqS * sinf(phiS), n2 = cosqS;
+    const float S0 = sinqK * cosphiK, S1 = sinqK * sinphiK, S2 = cosqK;
+    const float L0 = coslam * sinqK * cosphiK + sinlam * (sinalp * sinphiK - cosalp * cosqK * cosphiK);
+    const float L1 = coslam * sinqK * sinphiK - sinlam * (sinalp * cosphiK + cosalp * cosqK * sinphiK);
+    const float L2 = coslam * cosqK + sinlam * cosalp * sinqK;
+    const float nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
+    const float nS0 = n1 * S2 - n2 * S1, nS1 = n2 * S0 - n0 * S2, nS2 = n0 * S1 - n1 * S0;
+    const float norm = sqrtf(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * sqrtf(nS0 * nS0 + nS1 * nS1 + nS2 * nS2);
+    const float cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
+    const float sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
+    rot0 = 2.f * cosrot * cosrot - 1.f;
+    rot1 = cosrot * sinrot;
+  }
+  const float uI = FplusI * rot0 - FcrosI * rot1, wI = FplusI * rot1 + FcrosI * rot0;
+  const float uII = FplusII * rot0 - FcrosII * rot1, wII = FplusII * rot1 + FcrosII * rot0;
+  const float opL2 = 1.f + Ldotn2, omL2 = 1.f - Ldotn2, twoL = 2.f * Ldotn;
+  // harmonic phases: n (Phi + D1) + D0, reduced in FP64
+  double D1 = 0.0;
+  float D0 = 0.f;
+  if (d.mich) {
+    D1 = kTwoPi * nu * kAUsec * d.sinqS * (double)cosorbphs;
+    D0 = (float)(2.0 * gimdot * kAUsec) * sinqS * cosorbphs;
+  }
+  float s1, c1, sD, cD;
+  sincosf(reduce_2pi_f(Phi + D1), &s1, &c1);
+  sincosf(D0, &sD, &cD);
+  const float e = (float)q.e;
+  float Sa, Sb, Sc;
+  if (K > 0) {
+    const double del = (q.e - ec) / ec;
+    const float lp = (float)(log1p(del) * 1.4426950408889634);
+    const float half_dl = (float)(-del * (2.0 + del) * ec * 0.5);
+    switch (K) {
+      case 3: mode_sums_table_f32<3>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      case 4: mode_sums_table_f32<4>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      case 6: mode_sums_table_f32<6>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      default: mode_sums_table_f32<8>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    }
+  } else {
+    double sa, sb, sc;
+    mode_sums_miller(bstart, d.nmodes, q.e, c1, s1, cD, sD, sa, sb, sc);
+    Sa = (float)sa;
+    Sb = (float)sb;
+    Sc = (float)sc;
+  }
+  const float se = sqrtf(1.f - e * e);
+  const float a = -Amp * Sa, b = -Amp * se * Sb, cc = 2.f * Amp * Sc;
+  hI = (double)(Kresp * ((-uI * opL2 * cos2gam + wI * twoL * sin2gam) * a + (uI * opL2 * sin2gam + wI * twoL * cos2gam) * b +
+                         uI * omL2 * cc));
+  hII = (double)(Kresp * ((-uII * opL2 * cos2gam + wII * twoL * sin2gam) * a +
+                          (uII * opL2 * sin2gam + wII * twoL * cos2gam) * b + uII * omL2 * cc));
+}
+
 // ------------------------------------------------------------------ pass 2
-__global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_fp64(BatchView bv) {
+template <bool kSplit>
+__global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
   __shared__ double s_raw[kTileThreads];
   __shared__ double s_Pa[kTileThreads];
   __shared__ double s_r[3][kTileThreads];
@@ -713,6 +900,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_
   __shared__ double s_bc[4];
   __shared__ long long s_tile;
   __shared__ double s_T[kTabModes * kTabStride];
+  __shared__ __align__(16) float s_Tf[kSplit ? kTabModes * kTabStrideF : 4];
   __shared__ double s_ec;
   __shared__ int s_K;
   const int tid = threadIdx.x;
@@ -755,7 +943,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_
         const double e2 = spline4(bv, d, sample_time(d, last)).e;
         ec = spline4(bv, d, sample_time(d, (c.start + last) / 2)).e;
         const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
-        if (ec > 1e-6) K = choose_terms(2.0 * d.nmodes * de * (1.0 + de / ec));
+        if (ec > 1e-6) {
+          const double qmax = 2.0 * d.nmodes * de * (1.0 + de / ec);
+          K = kSplit ? choose_terms_f32(qmax) : choose_terms(qmax);
+        }
       }
       s_ec = ec;
       s_K = K;
@@ -764,8 +955,12 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_
     const int K = s_K;
     const double ec = s_ec;
     if (K > 0)
-      for (int n = tid + 1; n <= d.nmodes; n += kTileThreads)
-        build_bessel_row(s_T + (n - 1) * kTabStride, n, n * ec, K, bstart[n - 1]);
+      for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
+        double *Tn = s_T + (n - 1) * kTabStride;
+        build_bessel_row(Tn, n, n * ec, K, bstart[n - 1]);
+        if (kSplit)
+          for (int m = 0; m < kTabStrideF; ++m) s_Tf[(n - 1) * kTabStrideF + m] = (m <= 4 + K) ? (float)Tn[m] : 0.f;
+      }
     __syncthreads();
     double prev[3] = {s_bc[0], (s_bc[1] > 0.0) ? s_bc[1] : tc.Cf[1], s_bc[2]};
     double lastP = prev[1];
@@ -863,7 +1058,8 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_
         double hI = 0.0, hII = 0.0;
         if (in) {
           const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
-          harmonic_sum_fp64(d, bstart, s_T, ec, K, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
+          if (kSplit) harmonic_sum_split(d, bstart, s_Tf, ec, K, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
+          else harmonic_sum_fp64(d, bstart, s_T, ec, K, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
           if (i > d.i_plunge) {
             const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
             hI = hI / wgt;
@@ -900,6 +1096,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform_
 }  // namespace
 
 void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev) {
+  launch_dense(bv, num_sms, stream, ev, 0);
+}
+
+void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision) {
   if (bv.total_tiles <= 0) return;
   const int grid1 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 8);
   cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
@@ -909,7 +1109,8 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
   k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
   if (ev) cudaEventRecord(ev[2], stream);
   const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 4);
-  k_waveform_fp64<<<grid2, kTileThreads, 0, stream>>>(bv);
+  if (precision == 1) k_waveform<true><<<grid2, kTileThreads, 0, stream>>>(bv);
+  else k_waveform<false><<<grid2, kTileThreads, 0, stream>>>(bv);
   if (ev) cudaEventRecord(ev[3], stream);
 }
 

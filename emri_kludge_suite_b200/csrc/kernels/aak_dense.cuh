@@ -57,6 +57,9 @@ struct BatchView {
 // Launch pass 1, the carry scan and pass 2 on `stream`.  ev (optional, 4
 // events) brackets the three kernels for per-kernel timing.
 void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev);
+// precision 0: FP64 throughout; 1: split (FP64 phases and reductions, FP32
+// geometry, response, Bessel evaluation and harmonic recurrence).
+void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision);
 
 // Diagnostic: sustained FP64 FMA issue rate of this device in TFLOP/s
 // (2 flops per FMA), measured with CUDA events over `iters` launches.

@@ -33,6 +33,7 @@ def _bind():
     L.aak_gpu_likelihood.argtypes = [v, _dp]
     L.aak_gpu_likelihood_batch.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp, _i32p]
     L.aak_gpu_last_timing.argtypes = [v, _dp]
+    L.aak_gpu_set_precision.argtypes = [v, ctypes.c_int32]
     L._gpu_bound = True
     return L
 
@@ -110,6 +111,10 @@ class GPUAAK:
               "likelihood_batch")
         self._spectral = False
         return (out, st) if return_status else out
+
+    def set_precision(self, precision: int):
+        """0: FP64 throughout (default); 1: split precision."""
+        check(lib().aak_gpu_set_precision(self._g, int(precision)), "set_precision")
 
     def last_timing_ms(self):
         ms = np.zeros(4)

@@ -138,7 +138,9 @@ int aak_batch_upload(aak_ctx *ctx, void *stream);
 /* Run the dense kernels into caller device buffers indexed by offsets:
  * hI, hII (required), t (optional), traj (optional 9 x traj_stride dense
  * trajectory e, v, M, S, gamma~, Phi, alpha, nu, gamma~dot; diagnostic).
- * precision: 0 = FP64 throughout. */
+ * precision: 0 = FP64 throughout; 1 = split precision (FP64 spline, phases
+ * and angle reductions; FP32 geometry, LISA response, Bessel evaluation and
+ * harmonic recurrence). */
 int aak_batch_run(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_t, double *d_traj, int64_t traj_stride,
                   int32_t precision, void *stream);
 
@@ -213,6 +215,10 @@ int aak_gpu_likelihood(aak_gpu *g, double *out2);
  * (<= 0: 256); host planning uses nthreads threads (<= 0: all). */
 int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int32_t max_batch, int32_t nthreads,
                              double *out, int32_t *status);
+
+/* Template precision: 0 = FP64 throughout (default), 1 = split (FP64 phases
+ * and angle reductions, FP32 geometry, response, Bessel evaluation). */
+int aak_gpu_set_precision(aak_gpu *g, int32_t precision);
 
 /* Milliseconds of the last batch: host planning, waveform kernels, FFT, reduction. */
 int aak_gpu_last_timing(aak_gpu *g, double *ms4);
