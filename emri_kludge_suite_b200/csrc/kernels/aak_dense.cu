@@ -75,6 +75,79 @@ __device__ __forceinline__ Traj4 spline4(const BatchView &bv, const SourceDesc &
   return q;
 }
 
+// ------------------------------------------------------------------ knot windows
+// The knots a tile needs are a short contiguous run; each CTA brackets it once
+// and stages it in shared memory, so per-sample lookups search a handful of
+// shared-memory entries instead of walking the whole knot array in global
+// memory.  Runs longer than kWin (sources whose coarse grid is finer than the
+// sample spacing) are searched in global memory within the bracket.
+constexpr int kWin = 64;
+
+struct KnotWin {
+  double *t;   // kWin
+  double4 *y;  // kWin
+  double4 *c;  // kWin
+  int k0;      // first knot of the window (source-relative)
+  int n;       // knots in the window
+  int staged;  // 1: window is in shared memory
+};
+
+__device__ __forceinline__ Traj4 eval_piece(const double4 &y0, const double4 &y1, const double4 &c0, const double4 &c1,
+                                            double x0, double x1, double t) {
+  const double h = x1 - x0, dx = t - x0;
+  Traj4 q;
+  q.e = piece(y0.x, y1.x, c0.x, c1.x, h, dx);
+  q.v = piece(y0.y, y1.y, c0.y, c1.y, h, dx);
+  q.M = piece(y0.z, y1.z, c0.z, c1.z, h, dx);
+  q.S = piece(y0.w, y1.w, c0.w, c1.w, h, dx);
+  return q;
+}
+
+__device__ __forceinline__ Traj4 spline4w(const BatchView &bv, const SourceDesc &d, double t, const KnotWin &w) {
+  if (w.staged) {
+    int lo = 0, hi = w.n - 1;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (w.t[mid] > t) hi = mid;
+      else lo = mid;
+    }
+    return eval_piece(w.y[lo], w.y[lo + 1], w.c[lo], w.c[lo + 1], w.t[lo], w.t[lo + 1], t);
+  }
+  const double *kt = bv.knot_t + d.knot_offset;
+  int lo = w.k0, hi = w.k0 + w.n - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (kt[mid] > t) hi = mid;
+    else lo = mid;
+  }
+  const int64_t o = d.knot_offset + lo;
+  return eval_piece(bv.knot_y[o], bv.knot_y[o + 1], bv.knot_c[o], bv.knot_c[o + 1], kt[lo], kt[lo + 1], t);
+}
+
+// Bracket the knots for times [ta, tb] (thread 0), then stage them (all threads).
+__device__ __forceinline__ void load_window(const BatchView &bv, const SourceDesc &d, double ta, double tb, KnotWin &w,
+                                            int *s_kk) {
+  if (threadIdx.x == 0) {
+    const double *kt = bv.knot_t + d.knot_offset;
+    const int k0 = find_knot(kt, d.n_knots, ta);
+    const int k1 = find_knot(kt, d.n_knots, tb);
+    s_kk[0] = k0;
+    s_kk[1] = k1 + 2 - k0;  // knots k0 .. k1 + 1
+  }
+  __syncthreads();
+  w.k0 = s_kk[0];
+  w.n = s_kk[1];
+  w.staged = w.n <= kWin;
+  if (w.staged)
+    for (int k = threadIdx.x; k < w.n; k += blockDim.x) {
+      const int64_t o = d.knot_offset + w.k0 + k;
+      w.t[k] = bv.knot_t[o];
+      w.y[k] = bv.knot_y[o];
+      w.c[k] = bv.knot_c[o];
+    }
+  __syncthreads();
+}
+
 // gamma~dot, Phidot, alphadot (AAK.cc:251-253)
 __device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q, double r[3]) {
   const double tm = pn_dtdm(q.v, q.e, d.coslam, q.S);
@@ -223,6 +296,9 @@ __device__ __forceinline__ Lin clamp_phidot(const double *raw, int slot, int fir
 __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
   __shared__ double s_r[3][kSlots];
   __shared__ double red[7][kTileThreads / 32];
+  __shared__ double s_wt[kWin];
+  __shared__ double4 s_wy[kWin], s_wc[kWin];
+  __shared__ int s_kk[2];
   const int tid = threadIdx.x;
   for (int64_t g = blockIdx.x; g < bv.total_tiles; g += gridDim.x) {
     const SourceDesc *dp;
@@ -238,6 +314,9 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
       }
       continue;
     }
+    KnotWin w{s_wt, s_wy, s_wc, 0, 0, 0};
+    load_window(bv, d, sample_time(d, max(c.start - 1, 0)), sample_time(d, min(c.start + kTileSamples, d.vlength - 1)),
+                w, s_kk);
     // (A) rates, two independent samples per pass
 #pragma unroll 1
     for (int s = tid; s < kSlots; s += 2 * kTileThreads) {
@@ -246,8 +325,8 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
       double r1[3] = {0, 0, 0}, r2[3] = {0, 0, 0};
       const bool n1 = i1 >= 0 && i1 < d.vlength && i1 <= lim;
       const bool n2 = s2 < kSlots && i2 >= 0 && i2 < d.vlength && i2 <= lim;
-      if (n1) phase_rates(d, spline4(bv, d, sample_time(d, i1)), r1);
-      if (n2) phase_rates(d, spline4(bv, d, sample_time(d, i2)), r2);
+      if (n1) phase_rates(d, spline4w(bv, d, sample_time(d, i1), w), r1);
+      if (n2) phase_rates(d, spline4w(bv, d, sample_time(d, i2), w), r2);
       s_r[0][s] = r1[0];
       s_r[1][s] = n1 ? r1[1] : -1.0;
       s_r[2][s] = r1[2];
@@ -300,10 +379,10 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
     for (int q = 0; q < 7; ++q)
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-    const int w = tid >> 5, l = tid & 31;
+    const int wp = tid >> 5, l = tid & 31;
     if (l == 0)
 #pragma unroll
-      for (int q = 0; q < 7; ++q) red[q][w] = acc[q];
+      for (int q = 0; q < 7; ++q) red[q][wp] = acc[q];
     __syncthreads();
     if (tid == 0) {
       double tot[7];
@@ -903,6 +982,9 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   __shared__ __align__(16) float s_Tf[kSplit ? kTabModes * kTabStrideF : 4];
   __shared__ double s_ec;
   __shared__ int s_K;
+  __shared__ double s_wt[kWin];
+  __shared__ double4 s_wy[kWin], s_wc[kWin];
+  __shared__ int s_kk[2];
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
@@ -927,10 +1009,13 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
       continue;
     }
+    KnotWin w{s_wt, s_wy, s_wc, 0, 0, 0};
+    load_window(bv, d, sample_time(d, max(c.start - 1, 0)), sample_time(d, min(c.start + kTileSamples, d.vlength - 1)),
+                w, s_kk);
     if (tid == 0) {
       double rp[3] = {0, 0, 0};
       const int ip = c.start - 1;
-      if (ip >= 0 && ip < d.vlength) phase_rates(d, spline4(bv, d, sample_time(d, ip)), rp);
+      if (ip >= 0 && ip < d.vlength) phase_rates(d, spline4w(bv, d, sample_time(d, ip), w), rp);
       s_bc[0] = rp[0];
       s_bc[1] = rp[1];
       s_bc[2] = rp[2];
@@ -939,9 +1024,9 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       int K = 0;
       double ec = 0.0;
       if (last >= c.start && d.nmodes <= kTabModes) {
-        const double e0 = spline4(bv, d, sample_time(d, c.start)).e;
-        const double e2 = spline4(bv, d, sample_time(d, last)).e;
-        ec = spline4(bv, d, sample_time(d, (c.start + last) / 2)).e;
+        const double e0 = spline4w(bv, d, sample_time(d, c.start), w).e;
+        const double e2 = spline4w(bv, d, sample_time(d, last), w).e;
+        ec = spline4w(bv, d, sample_time(d, (c.start + last) / 2), w).e;
         const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
         if (ec > 1e-6) {
           const double qmax = 2.0 * d.nmodes * de * (1.0 + de / ec);
@@ -978,7 +1063,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       Traj4 q = {0, 0, 0, 0};
       double r[3] = {0, 0, 0};
       if (in) {
-        q = spline4(bv, d, t);
+        q = spline4w(bv, d, t, w);
         phase_rates(d, q, r);
       }
       s_raw[tid] = vf ? r[1] : -1.0;
@@ -1021,7 +1106,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
             rn[1] = s_r[1][tid + 1];
             rn[2] = s_r[2][tid + 1];
           } else {
-            phase_rates(d, spline4(bv, d, sample_time(d, i + 1)), rn);
+            phase_rates(d, spline4w(bv, d, sample_time(d, i + 1), w), rn);
           }
           incB[0] = (1.5 * r[0] - .5 * rn[0]) * d.dt;
           incB[1] = (1.5 * r[1] - .5 * rn[1]) * d.dt;
