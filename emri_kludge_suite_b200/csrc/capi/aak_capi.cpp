@@ -67,6 +67,7 @@ struct aak_ctx {
   std::vector<int32_t> status;
   std::vector<SourceDesc> descs;
   std::vector<int64_t> tile_start;
+  std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
   std::vector<double> knot_t;
   std::vector<double4> knot_y, knot_c;
   std::vector<int32_t> bessel;
@@ -76,6 +77,7 @@ struct aak_ctx {
   // device buffers
   DevBuf<SourceDesc> d_src;
   DevBuf<int64_t> d_tile_start;
+  DevBuf<int32_t> d_tile_knot;
   DevBuf<double> d_knot_t;
   DevBuf<double4> d_knot_y, d_knot_c;
   DevBuf<int32_t> d_bessel;
@@ -229,6 +231,26 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
     d.n_tiles = (int32_t)(ctx->tile_start[s + 1] - ctx->tile_start[s]);
     ctx->descs[s] = d;
   }
+  // knot window of every tile: knots bracketing samples start-1 .. start+1024
+  ctx->tile_knot.assign(2 * std::max<int64_t>(ctx->total_tiles, 1), 0);
+  for (int s = 0; s < n; ++s) {
+    if (ctx->status[s] != AAK_OK) continue;
+    const SourceDesc &d = ctx->descs[s];
+    const double *kt = ctx->knot_t.data() + d.knot_offset;
+    const int nk = d.n_knots;
+    auto tsample = [&](int i) { return (i == 0) ? d.t_first : (double)(i - d.i0) * d.dt; };
+    int k0 = 0, k1 = 0;
+    for (int64_t t = 0; t < d.n_tiles; ++t) {
+      const int start = (int)(t * kTileSamples);
+      const double ta = tsample(std::max(start - 1, 0));
+      const double tb = tsample(std::min(start + kTileSamples, d.vlength - 1));
+      while (k0 + 1 <= nk - 2 && kt[k0 + 1] <= ta) ++k0;
+      k1 = std::max(k1, k0);
+      while (k1 + 1 <= nk - 2 && kt[k1 + 1] <= tb) ++k1;
+      ctx->tile_knot[2 * (d.tile_offset + t)] = k0;
+      ctx->tile_knot[2 * (d.tile_offset + t) + 1] = k1 + 2 - k0;
+    }
+  }
   ctx->uploaded = false;
 }
 
@@ -271,6 +293,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
   const int n = ctx->nsrc;
   if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
+      (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) ||
       (r = ctx->d_knot_t.reserve(ctx->knot_t.size())) || (r = ctx->d_knot_y.reserve(ctx->knot_y.size())) ||
       (r = ctx->d_knot_c.reserve(ctx->knot_c.size())) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
       (r = ctx->d_summ.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
@@ -281,6 +304,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   };
   if ((r = cp(ctx->d_src.ptr, ctx->descs.data(), n * sizeof(SourceDesc))) ||
       (r = cp(ctx->d_tile_start.ptr, ctx->tile_start.data(), (n + 1) * sizeof(int64_t))) ||
+      (r = cp(ctx->d_tile_knot.ptr, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
       (r = cp(ctx->d_knot_t.ptr, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
       (r = cp(ctx->d_knot_y.ptr, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
       (r = cp(ctx->d_knot_c.ptr, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
@@ -303,6 +327,7 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   bv.nsrc = ctx->nsrc;
   bv.total_tiles = ctx->total_tiles;
   bv.tile_start = ctx->d_tile_start.ptr;
+  bv.tile_knot = ctx->d_tile_knot.ptr;
   bv.knot_t = ctx->d_knot_t.ptr;
   bv.knot_y = ctx->d_knot_y.ptr;
   bv.knot_c = ctx->d_knot_c.ptr;
@@ -430,6 +455,7 @@ void aak_ctx_destroy(aak_ctx *c) {
   if (select_device(c->device) == AAK_OK) {
     c->d_src.release();
     c->d_tile_start.release();
+    c->d_tile_knot.release();
     c->d_knot_t.release();
     c->d_knot_y.release();
     c->d_knot_c.release();
@@ -498,11 +524,13 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   if (!ctx) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (ctx->nsrc <= 0) return AAK_ERR_INVALID_PARAM;
-  // caller buffer layout: descriptors | tile prefix | knot times | knot values | knot
-  // second derivatives | Bessel start orders, each segment 256-byte aligned
+  // caller buffer layout: descriptors | tile prefix | tile knot windows | knot times |
+  // knot values | knot second derivatives | Bessel start orders, each segment 256-byte
+  // aligned
   auto al = [](size_t x) { return (x + 255) / 256 * 256; };
   const size_t o_ts = al(ctx->descs.size() * sizeof(SourceDesc));
-  const size_t o_kt = o_ts + al(ctx->tile_start.size() * sizeof(int64_t));
+  const size_t o_tk = o_ts + al(ctx->tile_start.size() * sizeof(int64_t));
+  const size_t o_kt = o_tk + al(ctx->tile_knot.size() * sizeof(int32_t));
   const size_t o_ky = o_kt + al(ctx->knot_t.size() * sizeof(double));
   const size_t o_kc = o_ky + al(ctx->knot_y.size() * sizeof(double4));
   const size_t o_bs = o_kc + al(ctx->knot_c.size() * sizeof(double4));
@@ -521,6 +549,7 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   };
   if ((r = cp(0, ctx->descs.data(), ctx->descs.size() * sizeof(SourceDesc))) ||
       (r = cp(o_ts, ctx->tile_start.data(), ctx->tile_start.size() * sizeof(int64_t))) ||
+      (r = cp(o_tk, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
       (r = cp(o_kt, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
       (r = cp(o_ky, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
       (r = cp(o_kc, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
@@ -532,6 +561,7 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   bv.nsrc = ctx->nsrc;
   bv.total_tiles = ctx->total_tiles;
   bv.tile_start = reinterpret_cast<const int64_t *>(base + o_ts);
+  bv.tile_knot = reinterpret_cast<const int32_t *>(base + o_tk);
   bv.knot_t = reinterpret_cast<const double *>(base + o_kt);
   bv.knot_y = reinterpret_cast<const double4 *>(base + o_ky);
   bv.knot_c = reinterpret_cast<const double4 *>(base + o_kc);

@@ -124,19 +124,10 @@ __device__ __forceinline__ Traj4 spline4w(const BatchView &bv, const SourceDesc 
   return eval_piece(bv.knot_y[o], bv.knot_y[o + 1], bv.knot_c[o], bv.knot_c[o + 1], kt[lo], kt[lo + 1], t);
 }
 
-// Bracket the knots for times [ta, tb] (thread 0), then stage them (all threads).
-__device__ __forceinline__ void load_window(const BatchView &bv, const SourceDesc &d, double ta, double tb, KnotWin &w,
-                                            int *s_kk) {
-  if (threadIdx.x == 0) {
-    const double *kt = bv.knot_t + d.knot_offset;
-    const int k0 = find_knot(kt, d.n_knots, ta);
-    const int k1 = find_knot(kt, d.n_knots, tb);
-    s_kk[0] = k0;
-    s_kk[1] = k1 + 2 - k0;  // knots k0 .. k1 + 1
-  }
-  __syncthreads();
-  w.k0 = s_kk[0];
-  w.n = s_kk[1];
+// Stage the knots of tile g (bracket precomputed on the host, tile_knot).
+__device__ __forceinline__ void load_window(const BatchView &bv, const SourceDesc &d, int64_t g, KnotWin &w) {
+  w.k0 = bv.tile_knot[2 * g];
+  w.n = bv.tile_knot[2 * g + 1];
   w.staged = w.n <= kWin;
   if (w.staged)
     for (int k = threadIdx.x; k < w.n; k += blockDim.x) {
@@ -293,12 +284,17 @@ __device__ __forceinline__ Lin clamp_phidot(const double *raw, int slot, int fir
   return Lin{0.0, 1.0};
 }
 
+// term-count rules of the multiplication theorem (defined with the harmonic sums);
+// sources with more modes than kTabModes evaluate Bessel functions per sample
+constexpr int kTabModes = 128;
+__device__ __forceinline__ int choose_terms(double qmax);
+__device__ __forceinline__ int choose_terms_f32(double qmax);
+
 __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
   __shared__ double s_r[3][kSlots];
   __shared__ double red[7][kTileThreads / 32];
   __shared__ double s_wt[kWin];
   __shared__ double4 s_wy[kWin], s_wc[kWin];
-  __shared__ int s_kk[2];
   const int tid = threadIdx.x;
   for (int64_t g = blockIdx.x; g < bv.total_tiles; g += gridDim.x) {
     const SourceDesc *dp;
@@ -309,14 +305,15 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
     TileSummary &ts = bv.summ[g];
     if (lim <= c.start) {  // nothing to accumulate (after the taper)
       if (tid == 0) {
-        for (int q = 0; q < 3; ++q) ts.fA[q] = ts.fB[q] = ts.bA[q] = ts.bB[q] = ts.last_rate[q] = ts.first_rate[q] = 0.0;
+        for (int q = 0; q < 3; ++q) ts.fA[q] = ts.fB[q] = ts.bA[q] = ts.bB[q] = ts.last_rate[q] = ts.first_rate[q] = ts.rate_before[q] = 0.0;
+        ts.ec = 0.0;
+        ts.k64 = ts.k32 = 0;
         ts.has_last[0] = ts.has_last[1] = ts.has_last[2] = 0;
       }
       continue;
     }
     KnotWin w{s_wt, s_wy, s_wc, 0, 0, 0};
-    load_window(bv, d, sample_time(d, max(c.start - 1, 0)), sample_time(d, min(c.start + kTileSamples, d.vlength - 1)),
-                w, s_kk);
+    load_window(bv, d, g, w);
     // (A) rates, two independent samples per pass
 #pragma unroll 1
     for (int s = tid; s < kSlots; s += 2 * kTileThreads) {
@@ -409,6 +406,27 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
       ts.has_last[0] = ts.has_last[2] = 0;
       ts.last_rate[0] = ts.last_rate[2] = 0.0;
       ts.first_rate[0] = ts.first_rate[1] = ts.first_rate[2] = 0.0;
+      // for pass 2: rates just before the tile, and the Bessel-table centre and
+      // term counts from e at the tile's first, middle and last output samples
+      ts.rate_before[0] = s_r[0][0];
+      ts.rate_before[1] = s_r[1][0];
+      ts.rate_before[2] = s_r[2][0];
+      double ec = 0.0;
+      int k64 = 0, k32 = 0;
+      if (d.nmodes <= kTabModes) {
+        const double e0 = spline4w(bv, d, sample_time(d, c.start), w).e;
+        const double e2 = spline4w(bv, d, sample_time(d, last_f), w).e;
+        ec = spline4w(bv, d, sample_time(d, (c.start + last_f) / 2), w).e;
+        const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
+        if (ec > 1e-6) {
+          const double qmax = 2.0 * d.nmodes * de * (1.0 + de / ec);
+          k64 = choose_terms(qmax);
+          k32 = choose_terms_f32(qmax);
+        }
+      }
+      ts.ec = ec;
+      ts.k64 = k64;
+      ts.k32 = k32;
     }
     __syncthreads();
   }
@@ -535,7 +553,6 @@ __device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double
 // m = 0 .. 4 + K, b = n - 2 (b = -1 for n = 1, with J_{-1} = -J_1).
 constexpr int kKMax = 12;
 constexpr int kTabStride = 5 + kKMax;
-constexpr int kTabModes = 128;
 
 // one row of the table, built by one thread (x = n e_c > 0)
 __device__ void build_bessel_row(double *Tn, int n, double x, int K, int start) {
@@ -677,9 +694,8 @@ __device__ void mode_sums_miller(const int32_t *bstart, int nmodes, double e, do
 // rotation and antenna factors applied once per sample.  The Bessel values
 // come from the tile table (K > 0) or a per-sample recurrence (K == 0).
 __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, const double *T, double ec, int K,
-                                  double t, const Traj4 &q, double gim, double Phi, double alp, double nu,
+                                  double t, double e, double om_M, double gim, double Phi, double alp, double nu,
                                   double gimdot, double &hI, double &hII) {
-  const double e = q.e;
   const double cosalp = cos(alp), sinalp = sin(alp);
   const double cosqL = d.cosqK * d.coslam + d.sinqK * d.sinlam * cosalp;
   const double sinqL = sqrt(1. - cosqL * cosqL);
@@ -730,7 +746,7 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, co
     FcrosII = c2;
     Kresp = 1.0;
   }
-  const double Amp = pow(omega_phi(q.v, e, d.coslam, q.S, q.M) * d.M_phys_sec, 2. / 3.) * d.zeta;
+  const double Amp = pow(om_M, 2. / 3.) * d.zeta;
 
   // rotation to the NK wave frame (RotCoeff, KSParMap.cc:532-574): depends on alpha only
   double rot0, rot1;
@@ -854,7 +870,7 @@ __device__ __forceinline__ void mode_sums_table_f32(const float *Tf, int nmodes,
 
 // h_I, h_II at one sample in split precision (same algebra as harmonic_sum_fp64).
 __device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, const float *Tf, double ec, int K,
-                                   double t, const Traj4 &q, double gim, double Phi, double alp, double nu,
+                                   double t, double e_d, double om_M, double gim, double Phi, double alp, double nu,
                                    double gimdot, double &hI, double &hII) {
   const float coslam = (float)d.coslam, sinlam = (float)d.sinlam;
   const float cosqS = (float)d.cosqS, sinqS = (float)d.sinqS, cosqK = (float)d.cosqK, sinqK = (float)d.sinqK;
@@ -913,7 +929,7 @@ __device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, c
     FcrosII = c2;
     Kresp = 1.f;
   }
-  const float Amp = powf((float)(omega_phi(q.v, q.e, d.coslam, q.S, q.M) * d.M_phys_sec), 2.f / 3.f) * (float)d.zeta;
+  const float Amp = powf((float)om_M, 2.f / 3.f) * (float)d.zeta;
   float rot0, rot1;
   {
     const float n0 = sinqS * cosf(phiS), n1 = sinqS * sinf(phiS), n2 = cosqS;
@@ -942,10 +958,10 @@ __device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, c
   float s1, c1, sD, cD;
   sincosf(reduce_2pi_f(Phi + D1), &s1, &c1);
   sincosf(D0, &sD, &cD);
-  const float e = (float)q.e;
+  const float e = (float)e_d;
   float Sa, Sb, Sc;
   if (K > 0) {
-    const double del = (q.e - ec) / ec;
+    const double del = (e_d - ec) / ec;
     const float lp = (float)(log1p(del) * 1.4426950408889634);
     const float half_dl = (float)(-del * (2.0 + del) * ec * 0.5);
     switch (K) {
@@ -956,7 +972,7 @@ __device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, c
     }
   } else {
     double sa, sb, sc;
-    mode_sums_miller(bstart, d.nmodes, q.e, c1, s1, cD, sD, sa, sb, sc);
+    mode_sums_miller(bstart, d.nmodes, e_d, c1, s1, cD, sD, sa, sb, sc);
     Sa = (float)sa;
     Sb = (float)sb;
     Sc = (float)sc;
@@ -970,21 +986,29 @@ __device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, c
 }
 
 // ------------------------------------------------------------------ pass 2
+// Per tile: phase 1 computes, for the tile's 1024 samples, the spline, rates,
+// clamped Phidot and the block-scanned AB2 phases (uniform, cheap work with
+// the tile's barriers) and parks each sample's harmonic-sum inputs in shared
+// memory; after one barrier, phase 2 evaluates the harmonic sums of each
+// thread's own samples with no further barriers.
+constexpr int kDynVals = 7;  // e, Omega_phi M_phys, gamma~, Phi, alpha, nu, gamma~dot
+constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double);
+
 template <bool kSplit>
 __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
+  extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
   __shared__ double s_raw[kTileThreads];
   __shared__ double s_Pa[kTileThreads];
   __shared__ double s_r[3][kTileThreads];
   __shared__ double red[3][kTileThreads / 32];
-  __shared__ double s_bc[4];
   __shared__ long long s_tile;
   __shared__ double s_T[kTabModes * kTabStride];
   __shared__ __align__(16) float s_Tf[kSplit ? kTabModes * kTabStrideF : 4];
-  __shared__ double s_ec;
-  __shared__ int s_K;
   __shared__ double s_wt[kWin];
   __shared__ double4 s_wy[kWin], s_wc[kWin];
-  __shared__ int s_kk[2];
+  double *sv_e = s_dyn, *sv_om = s_dyn + kTileSamples, *sv_gim = s_dyn + 2 * kTileSamples;
+  double *sv_Phi = s_dyn + 3 * kTileSamples, *sv_alp = s_dyn + 4 * kTileSamples, *sv_nu = s_dyn + 5 * kTileSamples;
+  double *sv_gd = s_dyn + 6 * kTileSamples;
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
@@ -999,46 +1023,24 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const TileCarry &tc = bv.carry[g];
     const TileSummary &ts = bv.summ[g];
     const double X0[3] = {d.gim0, d.Phi0, d.alp0};
-    if (d.status != 0) {
+    if (d.status != 0 || min(c.end, c.neff) <= c.start) {
+      // failed source, or a tile entirely after the taper: zeros
       for (int ch = 0; ch < kTileChunks; ++ch) {
         const int i = c.start + ch * kTileThreads + tid;
         if (i < c.end) {
           bv.hI[d.out_offset + i] = 0.0;
           bv.hII[d.out_offset + i] = 0.0;
+          if (bv.t_out) bv.t_out[d.out_offset + i] = (d.status != 0) ? 0.0 : sample_time(d, i);
         }
       }
       continue;
     }
     KnotWin w{s_wt, s_wy, s_wc, 0, 0, 0};
-    load_window(bv, d, sample_time(d, max(c.start - 1, 0)), sample_time(d, min(c.start + kTileSamples, d.vlength - 1)),
-                w, s_kk);
-    if (tid == 0) {
-      double rp[3] = {0, 0, 0};
-      const int ip = c.start - 1;
-      if (ip >= 0 && ip < d.vlength) phase_rates(d, spline4w(bv, d, sample_time(d, ip), w), rp);
-      s_bc[0] = rp[0];
-      s_bc[1] = rp[1];
-      s_bc[2] = rp[2];
-      // Bessel table centre and term count from e at the tile's first, middle and last output samples
-      const int last = min(c.end, c.neff) - 1;
-      int K = 0;
-      double ec = 0.0;
-      if (last >= c.start && d.nmodes <= kTabModes) {
-        const double e0 = spline4w(bv, d, sample_time(d, c.start), w).e;
-        const double e2 = spline4w(bv, d, sample_time(d, last), w).e;
-        ec = spline4w(bv, d, sample_time(d, (c.start + last) / 2), w).e;
-        const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
-        if (ec > 1e-6) {
-          const double qmax = 2.0 * d.nmodes * de * (1.0 + de / ec);
-          K = kSplit ? choose_terms_f32(qmax) : choose_terms(qmax);
-        }
-      }
-      s_ec = ec;
-      s_K = K;
-    }
-    __syncthreads();
-    const int K = s_K;
-    const double ec = s_ec;
+    load_window(bv, d, g, w);
+    // boundary rate and Bessel-table parameters recorded by pass 1
+    const int K = kSplit ? ts.k32 : ts.k64;
+    const double ec = ts.ec;
+    // Bessel table rows (one thread per harmonic); its barrier is the first one of phase 1
     if (K > 0)
       for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
         double *Tn = s_T + (n - 1) * kTabStride;
@@ -1046,24 +1048,20 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
         if (kSplit)
           for (int m = 0; m < kTabStrideF; ++m) s_Tf[(n - 1) * kTabStrideF + m] = (m <= 4 + K) ? (float)Tn[m] : 0.f;
       }
-    __syncthreads();
-    double prev[3] = {s_bc[0], (s_bc[1] > 0.0) ? s_bc[1] : tc.Cf[1], s_bc[2]};
+    // ---------------- phase 1: phases of the tile's samples
+    double prev[3] = {ts.rate_before[0], (ts.rate_before[1] > 0.0) ? ts.rate_before[1] : tc.Cf[1], ts.rate_before[2]};
     double lastP = prev[1];
-    // running in-tile prefix (forward) and inclusive prefix of backward increments
     double runF[3] = {0, 0, 0}, runB[3] = {0, 0, 0};
-    const double t_plunge = sample_time(d, d.i_plunge);
-    const double t_zero = t_plunge + d.dt * d.i_buffer;
     for (int ch = 0; ch < kTileChunks; ++ch) {
       const int i = c.start + ch * kTileThreads + tid;
-      const bool inrange = i < c.end;
-      const bool in = inrange && i < c.neff;
+      const int sl = ch * kTileThreads + tid;
+      const bool in = i < c.end && i < c.neff;
       const bool vf = in && i >= d.i0;
       const bool vb = in && i >= 1 && i <= d.i0;
-      const double t = sample_time(d, i);
       Traj4 q = {0, 0, 0, 0};
       double r[3] = {0, 0, 0};
       if (in) {
-        q = spline4w(bv, d, t, w);
+        q = spline4w(bv, d, sample_time(d, i), w);
         phase_rates(d, q, r);
       }
       s_raw[tid] = vf ? r[1] : -1.0;
@@ -1138,42 +1136,60 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
         runF[qq] += totF[qq];
         runB[qq] += totB[qq];
       }
-      // output sample
-      if (inrange) {
-        double hI = 0.0, hII = 0.0;
-        if (in) {
-          const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
-          if (kSplit) harmonic_sum_split(d, bstart, s_Tf, ec, K, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
-          else harmonic_sum_fp64(d, bstart, s_T, ec, K, t, q, X[0], X[1], X[2], nu, r[0], hI, hII);
-          if (i > d.i_plunge) {
-            const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
-            hI = hI / wgt;
-            hII = hII / wgt;
-          }
-          if (bv.traj_out) {
-            const int64_t o = d.out_offset + i;
-            const int64_t st = bv.traj_stride;
-            bv.traj_out[0 * st + o] = q.e;
-            bv.traj_out[1 * st + o] = q.v;
-            bv.traj_out[2 * st + o] = q.M;
-            bv.traj_out[3 * st + o] = q.S;
-            bv.traj_out[4 * st + o] = X[0];
-            bv.traj_out[5 * st + o] = X[1];
-            bv.traj_out[6 * st + o] = X[2];
-            bv.traj_out[7 * st + o] = nu;
-            bv.traj_out[8 * st + o] = r[0];
-          }
+      if (in) {
+        const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
+        sv_e[sl] = q.e;
+        sv_om[sl] = omega_phi(q.v, q.e, d.coslam, q.S, q.M) * d.M_phys_sec;
+        sv_gim[sl] = X[0];
+        sv_Phi[sl] = X[1];
+        sv_alp[sl] = X[2];
+        sv_nu[sl] = nu;
+        sv_gd[sl] = r[0];
+        if (bv.traj_out) {
+          const int64_t o = d.out_offset + i;
+          const int64_t st = bv.traj_stride;
+          bv.traj_out[0 * st + o] = q.e;
+          bv.traj_out[1 * st + o] = q.v;
+          bv.traj_out[2 * st + o] = q.M;
+          bv.traj_out[3 * st + o] = q.S;
+          bv.traj_out[4 * st + o] = X[0];
+          bv.traj_out[5 * st + o] = X[1];
+          bv.traj_out[6 * st + o] = X[2];
+          bv.traj_out[7 * st + o] = nu;
+          bv.traj_out[8 * st + o] = r[0];
         }
-        bv.hI[d.out_offset + i] = hI;
-        bv.hII[d.out_offset + i] = hII;
-        if (bv.t_out) bv.t_out[d.out_offset + i] = t;
       }
-      // chunk carries
       const int ilast = c.start + ch * kTileThreads + kTileThreads - 1;
       if (ilast >= d.i0) lastP = s_Pa[kTileThreads - 1];
       prev[0] = s_r[0][kTileThreads - 1];
       prev[2] = s_r[2][kTileThreads - 1];
       __syncthreads();
+    }
+    // ---------------- phase 2: harmonic sums of this thread's own samples
+    const double t_plunge = sample_time(d, d.i_plunge);
+    const double t_zero = t_plunge + d.dt * d.i_buffer;
+    for (int ch = 0; ch < kTileChunks; ++ch) {
+      const int i = c.start + ch * kTileThreads + tid;
+      const int sl = ch * kTileThreads + tid;
+      if (i >= c.end) continue;
+      const double t = sample_time(d, i);
+      double hI = 0.0, hII = 0.0;
+      if (i < c.neff) {
+        if (kSplit)
+          harmonic_sum_split(d, bstart, s_Tf, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+                             sv_nu[sl], sv_gd[sl], hI, hII);
+        else
+          harmonic_sum_fp64(d, bstart, s_T, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+                            sv_nu[sl], sv_gd[sl], hI, hII);
+        if (i > d.i_plunge) {
+          const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
+          hI = hI / wgt;
+          hII = hII / wgt;
+        }
+      }
+      bv.hI[d.out_offset + i] = hI;
+      bv.hII[d.out_offset + i] = hII;
+      if (bv.t_out) bv.t_out[d.out_offset + i] = t;
     }
   }
 }
@@ -1194,8 +1210,14 @@ void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
   k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
   if (ev) cudaEventRecord(ev[2], stream);
   const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 4);
-  if (precision == 1) k_waveform<true><<<grid2, kTileThreads, 0, stream>>>(bv);
-  else k_waveform<false><<<grid2, kTileThreads, 0, stream>>>(bv);
+  static bool attrs_set = false;  // opt in to > 48 KB of shared memory once per process
+  if (!attrs_set) {
+    cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
+    cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
+    attrs_set = true;
+  }
+  if (precision == 1) k_waveform<true><<<grid2, kTileThreads, kWaveDynSmem, stream>>>(bv);
+  else k_waveform<false><<<grid2, kTileThreads, kWaveDynSmem, stream>>>(bv);
   if (ev) cudaEventRecord(ev[3], stream);
 }
 

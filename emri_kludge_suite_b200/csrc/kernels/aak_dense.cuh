@@ -25,6 +25,9 @@ struct TileSummary {
   double first_rate[3];  // raw rates of the first sample in the tile
   int32_t has_last[3];   // last_rate valid
   int32_t pad;
+  double rate_before[3]; // raw rates of the sample just before the tile (Phi: -1 if none)
+  double ec;             // Bessel-table centre eccentricity of the tile (0: no output samples)
+  int32_t k64, k32;      // multiplication-theorem terms for the FP64 / split harmonic sums (0: per-sample)
 };
 
 // Per-tile carries written by the carry kernel and read by pass 2.
@@ -41,6 +44,7 @@ struct BatchView {
   int32_t nsrc;
   int64_t total_tiles;
   const int64_t *tile_start;    // nsrc + 1 prefix of tiles (device)
+  const int32_t *tile_knot;     // 2 per tile: first knot of the tile's window, knots in it
   const double *knot_t;         // knots
   const double4 *knot_y;        // (e, v, M, S) at the knots
   const double4 *knot_c;        // natural-spline half second derivatives
