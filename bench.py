@@ -197,7 +197,70 @@ def config4_templates(n: int, seed: int = SEED + 4):
     return X
 
 
-def run_likelihood(n_templates: int, local_rank: int) -> dict:
+def run_parmap_warm_start(n_train: int, local_rank: int):
+    """Configuration 3: train the warm-start network on n_train seeded points
+    (labels from the plain map solve), evaluate it on 2^16 held-out points and
+    time its tensor-core inference kernel.  Returns (report, model)."""
+    import torch
+
+    from emri_kludge_suite_b200 import parmap_mlp as PM
+
+    t0 = time.perf_counter()
+    train = PM.make_dataset(n_train, SEED + 3)
+    held = PM.make_dataset(1 << 16, SEED + 33)
+    t_data = time.perf_counter() - t0
+    m = PM.ParMapMLP(local_rank, seed=SEED)
+    v = train["valid"]
+    hist = m.train(train["x"][v], train["y"][v], epochs=60, batch=8192, lr=1e-2, seed=SEED)
+    ev = PM.evaluate(m, held)
+    # inference kernel throughput: n_train points resident on the device
+    xd = torch.tensor(train["x"].astype(np.float32), device="cuda")
+    yd = torch.empty((n_train, 3), dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        m.forward_device(xd.data_ptr(), yd.data_ptr(), n_train)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        m.forward_device(xd.data_ptr(), yd.data_ptr(), n_train)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    tc_flops = 2.0 * 2 * 128 * 128  # the two 128 x 128 tensor-core layers, per point
+    all_flops = 2.0 * (4 * 128 + 2 * 128 * 128 + 3 * 128)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    bf16_peak = peaks.get("bf16_tflops") or 1590.0
+    tflops = tc_flops * n_train / (ms * 1e-3) / 1e12
+    rep = {
+        "workload": "config3: MLP 4->128->128->128->3 SiLU, BF16 weights/activations, FP32 accumulate; "
+                    f"{n_train} training points p~U(p_sep+0.1,20), e~U(0,0.7), iota~U(0,pi), a~U(0,0.95); "
+                    "2^16 held out; labels = plain map solve",
+        "train_points": int(v.sum()), "label_failures": int((~v).sum()), "heldout_points": ev["points"],
+        "dataset_seconds": t_data, "epochs": hist["epochs"], "batch": hist["batch"], "train_steps": hist["steps"],
+        "train_seconds": hist["seconds"], "train_rows_per_s": hist["epochs"] * int(v.sum()) / hist["seconds"],
+        "loss_first_epoch": hist["loss"][0], "loss_final": hist["loss"][-1],
+        "newton": {k: ev[k] for k in ("iters_cold", "iters_warm", "iterations_saved_frac", "iters_to_tol_cold",
+                                       "iters_to_tol_warm", "iterations_to_tol_saved_frac", "fallback_rate",
+                                       "failed_cold", "failed_warm")},
+        "residual": {"rel_cold_max": ev["residual_rel_cold_max"], "rel_warm_max": ev["residual_rel_warm_max"],
+                     "abs_warm_max": ev["residual_abs_warm_max"], "guess_rel": ev["guess_residual_rel"]},
+        "prediction_abs_err_max": ev["prediction_abs_err"],
+        "warm_vs_cold_solution_max_rel": ev["warm_vs_cold_solution_max_rel"],
+        "solve_seconds": {"cold": ev["solve_seconds_cold"], "warm": ev["solve_seconds_warm"],
+                          "predict": ev["predict_seconds"]},
+        "inference": {"points_per_s": n_train / (ms * 1e-3), "ms_per_launch": ms, "points": n_train,
+                      "flops_per_point": all_flops, "tensor_tflops": tflops, "bf16_peak_tflops": bf16_peak,
+                      "frac_of_measured_bf16": tflops / bf16_peak},
+    }
+    return rep, m
+
+
+def run_likelihood(n_templates: int, local_rank: int, model=None) -> dict:
     """likelihoods/s of the batched path: host planning + waveforms + FFT + reduction, end to end per call."""
     from emri_kludge_suite_b200.gpuAAK import GPUAAK
     from emri_kludge_suite_b200.LISAnoise import LISA_Noise, generate_noise_frequencies, generate_noise_single_channel
@@ -220,19 +283,40 @@ def run_likelihood(n_templates: int, local_rank: int) -> dict:
     df = 1.0 / (LIKE_LENGTH * DT)
     n1 = generate_noise_single_channel(LISA_Noise, [], {"dur": 1}, df, freqs, rng)
     n2 = generate_noise_single_channel(LISA_Noise, [], {"dur": 1}, df, freqs, rng)
-    g.input_data(w * (hI_f + n1), w * (hII_f + n2), w, w)
+    dI, dII = w * (hI_f + n1), w * (hII_f + n2)
+    g.input_data(dI, dII, w, w)
     X = config4_templates(n_templates)
-    g.likelihood_batch(X[: min(64, n_templates)])  # warm-up (plans, FFT plan)
-    t0 = time.perf_counter()
-    out, st = g.likelihood_batch(X, return_status=True)
-    wall = time.perf_counter() - t0
-    ms = g.last_timing_ms()
-    gpu_s = (ms["waveform"] + ms["fft"] + ms["reduce"]) * 1e-3
-    return {"likelihoods_per_s": n_templates / wall, "likelihoods_per_s_gpu": n_templates / gpu_s,
-            "templates": n_templates, "samples_per_template": LIKE_LENGTH, "failed": int(np.sum(st != 0)),
-            "ms": ms, "workload": "config4: fiducial config-0 source, 3.2e6 samples (1.014 yr, dt=10 s), LISA-coloured "
-                                  "noise, templates perturbed 1e-5 rel (M, mu, p0) / 1e-3 rad (angles), "
-                                  "reference harmonic rule, FP64"}
+    d_d = 4.0 * float(np.sum(np.abs(dI) ** 2) + np.sum(np.abs(dII) ** 2))  # pygpuAAK.py:67
+
+    def timed():
+        g.likelihood_batch(X[: min(64, n_templates)])  # warm-up (plans, FFT plan)
+        t0 = time.perf_counter()
+        o, st = g.likelihood_batch(X, return_status=True)
+        wall = time.perf_counter() - t0
+        ms = g.last_timing_ms()
+        gpu_s = (ms["waveform"] + ms["fft"] + ms["reduce"]) * 1e-3
+        return o, st, {"likelihoods_per_s": n_templates / wall, "likelihoods_per_s_gpu": n_templates / gpu_s,
+                       "failed": int(np.sum(st != 0)), "ms": ms}
+
+    out64, st64, plain = timed()
+    res = {"workload": "config4: fiducial config-0 source, 3.2e6 samples (1.014 yr, dt=10 s), LISA-coloured noise, "
+                       "templates perturbed 1e-5 rel (M, mu, p0) / 1e-3 rad (angles), reference harmonic rule",
+           "templates": n_templates, "samples_per_template": LIKE_LENGTH, "fp64_plain": plain}
+    res.update({k: plain[k] for k in ("likelihoods_per_s", "likelihoods_per_s_gpu", "failed", "ms")})
+    # split precision + learned warm start vs the plain FP64 path
+    g.set_precision(1)
+    g.set_warm_start(model)
+    outs, sts, fast = timed()
+    g.set_precision(0)
+    g.set_warm_start(None)
+    ok = (st64 == 0) & (sts == 0)
+    logl64 = -0.5 * (d_d + out64[:, 1] - 2.0 * out64[:, 0])
+    logls = -0.5 * (d_d + outs[:, 1] - 2.0 * outs[:, 0])
+    fast["max_abs_dlogL_vs_fp64"] = float(np.max(np.abs(logls - logl64)[ok])) if ok.any() else None
+    fast["max_abs_logL"] = float(np.max(np.abs(logl64[ok]))) if ok.any() else None
+    fast["warm_start"] = model is not None
+    res["split_warm"] = fast
+    return res
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -381,7 +465,7 @@ def run_gpu(args, rank, world, local_rank):
            "d2h_bytes_per_step": int(16 * N), "seconds_per_step": e2e_s, "host_threads": nthreads}
 
     # ---- roofline of the dominant kernel (harmonic sum)
-    flops_per_sample = 60.0 + NMODES * 33.0  # algorithmic count per sample, see DESIGN.md
+    flops_per_sample = 60.0 + NMODES * 33.0  # algorithmic flops per sample: 60 per sample + 33 per harmonic
     wave_ms = kern[2]
     achieved = flops_per_sample * N / (wave_ms * 1e-3) / 1e12
     roofline = {"kernel": "k_waveform_fp64", "bound": "fp64", "achieved": achieved, "peak": fp64_peak,
@@ -413,11 +497,14 @@ def run_gpu(args, rank, world, local_rank):
         "gpu_launches": launches,
         "host_plan_seconds": t_plan,
     }
+    model = None
+    if args.parmap_points > 0 and rank == 0:
+        out["parmap_warm_start"], model = run_parmap_warm_start(args.parmap_points, local_rank)
     if args.likelihood > 0:
         del hI, hII, hIh, hIIh
         wb.close()
         torch.cuda.empty_cache()
-        out["likelihood"] = run_likelihood(args.likelihood, local_rank)
+        out["likelihood"] = run_likelihood(args.likelihood, local_rank, model)
     return out
 
 
@@ -432,6 +519,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--likelihood", type=int, default=1024, help="config-4 templates to time (0: skip)")
+    ap.add_argument("--parmap-points", type=int, default=1 << 20,
+                    help="config-3 training points of the warm-start network (0: skip)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

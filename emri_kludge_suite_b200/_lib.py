@@ -25,6 +25,7 @@ STATUS_NAMES = {
     6: "AAK_ERR_NO_MEMORY",
     7: "AAK_ERR_TOO_FEW_STEPS",
     8: "AAK_ERR_CAPACITY",
+    9: "AAK_ERR_DEVICE_TIMEOUT",
 }
 
 PARAM_FIELDS = "length dt p T f T_fit mu M s e iota gamma psi theta_S phi_S theta_K phi_K alpha D".split()
@@ -63,6 +64,9 @@ class AAKError(RuntimeError):
         msg = f"{what}: {name}" if what else name
         try:
             msg += f" ({lib().aak_status_string(status).decode()})"
+            detail = lib().aak_last_error_detail().decode()
+            if status in (5, 6) and detail:
+                msg += f" [{detail}]"
         except Exception:
             pass
         super().__init__(msg)
@@ -106,6 +110,8 @@ def lib():
     L.aak_status_string.restype = ctypes.c_char_p
     L.aak_status_string.argtypes = [ctypes.c_int]
     L.aak_version.restype = ctypes.c_int
+    L.aak_last_error_detail.restype = ctypes.c_char_p
+    L.aak_last_error_detail.argtypes = []
     L.aak_front_end.argtypes = [ctypes.POINTER(AAKParams), _dp, ctypes.POINTER(AAKMapped)]
     L.aak_coarse_kerr.argtypes = [ctypes.POINTER(AAKParams), _i32p, _dp, _dp, _dp, _dp, _dp]
     L.aak_parmap.argtypes = [_dp, _d, _d, _d, _d, _d, _dp, _dp, _i32p]
@@ -127,6 +133,28 @@ def lib():
     L.aak_batch_kernel_ms.argtypes = [_vp, ctypes.POINTER(ctypes.c_float)]
     L.aak_probe_fp64_tflops.argtypes = [_i32, _dp]
     L.aak_wave_batch_host.argtypes = [_vp, ctypes.POINTER(AAKParams), _i32, _i32p, _i32, _dp, _dp, _i64p, _i32p]
+    # learned ParMap warm start
+    _fp = ctypes.POINTER(ctypes.c_float)
+    L.aak_mlp_num_params.argtypes = []
+    L.aak_mlp_max_train_rows.argtypes = []
+    L.aak_mlp_create.argtypes = [_i32, ctypes.POINTER(_vp)]
+    L.aak_mlp_destroy.argtypes = [_vp]
+    L.aak_mlp_destroy.restype = None
+    L.aak_mlp_set_params.argtypes = [_vp, _fp]
+    L.aak_mlp_get_params.argtypes = [_vp, _fp]
+    L.aak_mlp_set_norm.argtypes = [_vp, _fp, _fp, _fp, _fp]
+    L.aak_mlp_set_adam.argtypes = [_vp, ctypes.c_float, ctypes.c_float, ctypes.c_float]
+    L.aak_mlp_forward.argtypes = [_vp, _vp, _vp, _i64, _vp]
+    L.aak_mlp_gradients.argtypes = [_vp, _vp, _vp, _vp, _i64, _vp, _fp, _vp]
+    L.aak_mlp_train_step.argtypes = [_vp, _vp, _vp, _vp, _i64, ctypes.c_float, _fp, _vp]
+    L.aak_mlp_status.argtypes = [_vp]
+    L.aak_mlp_predict_host.argtypes = [_vp, _dp, _dp, _i64]
+    L.aak_parmap_separatrix.argtypes = [_d, _d, _d, _dp]
+    L.aak_parmap_dataset.argtypes = [_i64, ctypes.c_uint64, ctypes.c_uint64, _i32, _dp, _dp, _dp, _i32p]
+    L.aak_parmap_solve_batch.argtypes = [_i64, _dp, _dp, _dp, _i32, _dp, _i32p, _i32p, _dp, _dp, _i32p]
+    L.aak_ctx_set_parmap_model.argtypes = [_vp, _vp]
+    L.aak_batch_newton_stats.argtypes = [_vp, _i64p, _i64p, _i64p]
+    L.aak_gpu_set_parmap_model.argtypes = [_vp, _vp]
     _lib = L
     return L
 
@@ -137,6 +165,8 @@ def ptr(a: np.ndarray):
     assert a.flags["C_CONTIGUOUS"]
     if a.dtype == np.float64:
         return a.ctypes.data_as(_dp)
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
     if a.dtype == np.int32:
         return a.ctypes.data_as(_i32p)
     if a.dtype == np.int64:

@@ -147,6 +147,21 @@ class WaveBatch:
         )
         self.total_samples = int(tot.value)
 
+    def set_parmap_model(self, model=None):
+        """Warm-start the Kerr->AK map of every coarse point with a trained
+        :class:`~emri_kludge_suite_b200.parmap_mlp.ParMapMLP` (None: plain guess).
+        The model must stay alive while this batch plans with it."""
+        self._model = model
+        check(lib().aak_ctx_set_parmap_model(self._ctx, model.handle if model is not None else None),
+              "aak_ctx_set_parmap_model")
+
+    def newton_stats(self) -> dict:
+        """Map statistics of the last plan: points, Newton iterations, fallbacks."""
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib().aak_batch_newton_stats(self._ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+              "aak_batch_newton_stats")
+        return {"points": a.value, "iterations": b.value, "fallbacks": c.value}
+
     def plan(self, params, nmodes=None, nthreads: int = 0, mapped=None):
         """Host planning; ``params`` is a list of pars dicts (or aak_params)."""
         self.nsrc = len(params)

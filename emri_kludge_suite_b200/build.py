@@ -29,9 +29,12 @@ SOURCES = [
     "host/kerr.cpp",
     "host/inspiral.cpp",
     "host/pipeline.cpp",
+    "host/parmap_data.cpp",
     "kernels/aak_dense.cu",
     "kernels/likelihood.cu",
+    "kernels/parmap_mlp.cu",
     "capi/aak_capi.cpp",
+    "capi/mlp_capi.cpp",
 ]
 
 

@@ -15,9 +15,13 @@
 
 #include <cufft.h>
 
+#include "../host/parallel.hpp"
+#include "../host/parmap_data.hpp"
 #include "../host/pipeline.hpp"
 #include "../kernels/aak_dense.cuh"
 #include "../kernels/likelihood.cuh"
+#include "errors.hpp"
+#include "mlp_model.hpp"
 
 using namespace aak;
 
@@ -49,11 +53,7 @@ struct DevBuf {
   }
 };
 
-int cuda_ok(cudaError_t e) {
-  if (e == cudaSuccess) return AAK_OK;
-  cudaGetLastError();
-  return e == cudaErrorMemoryAllocation ? AAK_ERR_NO_MEMORY : AAK_ERR_CUDA;
-}
+int cuda_ok(cudaError_t e) { return cuda_status_of(e); }
 
 }  // namespace
 
@@ -87,6 +87,8 @@ struct aak_ctx {
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
   int last_launches = 0;
   bool profile = false;
+  aak_mlp *model = nullptr;  // learned warm start of the map (optional)
+  int64_t newton_points = 0, newton_iters = 0, newton_fallbacks = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::mutex mu;
 };
@@ -94,6 +96,7 @@ struct aak_ctx {
 namespace {
 
 int select_device(int dev) {
+  if (dev < 0) return AAK_ERR_INVALID_PARAM;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
     cudaGetLastError();
@@ -158,27 +161,6 @@ void from_mapped(const aak_mapped &o, MappedTrajectory *m) {
   }
 }
 
-template <typename F>
-void parallel_for(int n, int nthreads, F &&fn) {
-  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
-  nthreads = std::min(nthreads, n);
-  if (nthreads <= 1) {
-    for (int i = 0; i < n; ++i) fn(i);
-    return;
-  }
-  std::atomic<int> next(0);
-  std::vector<std::thread> pool;
-  pool.reserve(nthreads);
-  for (int t = 0; t < nthreads; ++t)
-    pool.emplace_back([&]() {
-      for (;;) {
-        const int i = next.fetch_add(1);
-        if (i >= n) break;
-        fn(i);
-      }
-    });
-  for (auto &th : pool) th.join();
-}
 
 // Pack per-source plans into the flat arrays the kernels read.
 void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
@@ -254,6 +236,22 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
   ctx->uploaded = false;
 }
 
+// Coarse AK evolution and knots of source s from its mapped trajectory.
+void finish_source(aak_ctx *ctx, int s, const Params &Pp, const MappedTrajectory &mt, const int32_t *nm, int st) {
+  if (st == kOk) {
+    WaveInputs w;
+    genwave_inputs(Pp, mt, nm ? nm[s] : 0, &w);
+    if (w.nmodes > 4096) st = kErrCapacity;
+    else st = plan_source(w, &ctx->plans[s]);
+  }
+  ctx->status[s] = st;
+  if (st != kOk) {
+    ctx->plans[s].knot_t.clear();
+    ctx->plans[s].knot_y.clear();
+    ctx->plans[s].knot_c.clear();
+  }
+}
+
 int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32_t nsrc, const int32_t *nm,
                 int32_t nthreads) {
   if (!ctx || !P || nsrc <= 0) return AAK_ERR_INVALID_PARAM;
@@ -263,27 +261,67 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   ctx->nsrc = nsrc;
   ctx->plans.assign(nsrc, SourcePlan());
   ctx->status.assign(nsrc, AAK_OK);
-  parallel_for(nsrc, nthreads, [&](int s) {
+  ctx->newton_points = ctx->newton_iters = ctx->newton_fallbacks = 0;
+  if (maps) {
+    parallel_for(nsrc, nthreads, [&](int64_t s) {
+      const Params Pp = to_params(Pv[s]);
+      MappedTrajectory mt;
+      const int st = validate(Pp);
+      if (st == kOk) from_mapped(maps[s], &mt);
+      finish_source(ctx, (int)s, Pp, mt, nm, st);
+    });
+    pack(ctx, Pv);
+    return AAK_OK;
+  }
+  // (1) coarse Kerr inspiral and Kerr frequencies
+  std::vector<CoarseKerr> ck(nsrc);
+  parallel_for(nsrc, nthreads, [&](int64_t s) {
     const Params Pp = to_params(Pv[s]);
     int st = validate(Pp);
-    MappedTrajectory mt;
-    if (st == kOk) {
-      if (maps) from_mapped(maps[s], &mt);
-      else st = front_end(Pp, &mt, nullptr);
-    }
-    if (st == kOk) {
-      WaveInputs w;
-      genwave_inputs(Pp, mt, nm ? nm[s] : 0, &w);
-      if (w.nmodes > 4096) st = kErrCapacity;
-      else st = plan_source(w, &ctx->plans[s]);
-    }
+    if (st == kOk) st = coarse_kerr(Pp, &ck[s]);
     ctx->status[s] = st;
-    if (st != kOk) {
-      ctx->plans[s].knot_t.clear();
-      ctx->plans[s].knot_y.clear();
-      ctx->plans[s].knot_c.clear();
-    }
   });
+  // (2) optional learned warm start: every coarse point of the batch in one launch
+  std::vector<int64_t> first(nsrc + 1, 0);
+  std::vector<double> warm;
+  if (ctx->model) {
+    for (int s = 0; s < nsrc; ++s) first[s + 1] = first[s] + (ctx->status[s] == kOk ? ck[s].steps : 0);
+    const int64_t np = first[nsrc];
+    std::vector<double> xs(4 * np), ys(3 * np);
+    for (int s = 0; s < nsrc; ++s)
+      for (int64_t i = 0; i < first[s + 1] - first[s]; ++i) {
+        double *x = &xs[4 * (first[s] + i)];
+        x[0] = ck[s].p[i];
+        x[1] = ck[s].e[i];
+        x[2] = Pv[s].iota;
+        x[3] = Pv[s].s;
+      }
+    const int r = mlp_predict_host(ctx->model, xs.data(), ys.data(), np);
+    if (r != AAK_OK) return r;
+    warm.resize(3 * np);
+    for (int s = 0; s < nsrc; ++s)
+      for (int64_t i = first[s]; i < first[s + 1]; ++i) parmap_from_coords(&xs[4 * i], Pv[s].M, &ys[3 * i], &warm[3 * i]);
+  }
+  // (3) Kerr -> AK map, coarse AK evolution, knots
+  std::atomic<int64_t> points(0), iters(0), fallbacks(0);
+  parallel_for(nsrc, nthreads, [&](int64_t s) {
+    const Params Pp = to_params(Pv[s]);
+    MappedTrajectory mt;
+    int st = ctx->status[s];
+    if (st == kOk) {
+      int fb = 0;
+      st = map_coarse(Pp, ck[s], &mt, warm.empty() ? nullptr : &warm[3 * first[s]], &fb);
+      if (st == kOk) {
+        points += ck[s].steps;
+        iters += mt.newton_iterations;
+        fallbacks += fb;
+      }
+    }
+    finish_source(ctx, (int)s, Pp, mt, nm, st);
+  });
+  ctx->newton_points = points;
+  ctx->newton_iters = iters;
+  ctx->newton_fallbacks = fallbacks;
   pack(ctx, Pv);
   return AAK_OK;
 }
@@ -396,11 +434,14 @@ const char *aak_status_string(int s) {
     case AAK_ERR_NO_MEMORY: return "out of device memory";
     case AAK_ERR_TOO_FEW_STEPS: return "coarse inspiral produced fewer than 3 points";
     case AAK_ERR_CAPACITY: return "request exceeds a fixed-size buffer";
+    case AAK_ERR_DEVICE_TIMEOUT: return "a bounded device-side wait gave up";
     default: return "unknown status";
   }
 }
 
 int aak_version(void) { return 10000; }
+
+const char *aak_last_error_detail(void) { return last_error_buffer(); }
 
 int aak_front_end(const aak_params *p, const double *warm, aak_mapped *out) {
   if (!p || !out) return AAK_ERR_INVALID_PARAM;
@@ -439,20 +480,23 @@ int aak_parmap(const double Omega[3], double p, double M, double s, double e, do
 int aak_ctx_create(int32_t device, aak_ctx **out) {
   if (!out) return AAK_ERR_INVALID_PARAM;
   *out = nullptr;
-  int r = select_device(device);
-  if (r != AAK_OK) return r;
+  if (device != -1) {  // -1: host-only context (planning without a GPU)
+    const int r = select_device(device);
+    if (r != AAK_OK) return r;
+  }
   aak_ctx *c = new (std::nothrow) aak_ctx();
   if (!c) return AAK_ERR_NO_MEMORY;
   c->device = device;
   int sms = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0) c->num_sms = sms;
+  if (device >= 0 && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+    c->num_sms = sms;
   *out = c;
   return AAK_OK;
 }
 
 void aak_ctx_destroy(aak_ctx *c) {
   if (!c) return;
-  if (select_device(c->device) == AAK_OK) {
+  if (c->device >= 0 && select_device(c->device) == AAK_OK) {
     c->d_src.release();
     c->d_tile_start.release();
     c->d_tile_knot.release();
@@ -481,6 +525,22 @@ int aak_batch_plan_mapped(aak_ctx *ctx, const aak_params *P, const aak_mapped *m
   if (!ctx || !maps) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
   return plan_common(ctx, P, maps, nsrc, nm, nthreads);
+}
+
+int aak_ctx_set_parmap_model(aak_ctx *ctx, aak_mlp *m) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->model = m;
+  return AAK_OK;
+}
+
+int aak_batch_newton_stats(aak_ctx *ctx, int64_t *points, int64_t *iterations, int64_t *fallbacks) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (points) *points = ctx->newton_points;
+  if (iterations) *iterations = ctx->newton_iters;
+  if (fallbacks) *fallbacks = ctx->newton_fallbacks;
+  return AAK_OK;
 }
 
 int aak_batch_info(aak_ctx *ctx, int64_t *total, int64_t *offsets, int32_t *status, int32_t *i_plunge, int32_t *i_buffer) {
@@ -942,6 +1002,11 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   }
   for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
   return AAK_OK;
+}
+
+int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m) {
+  if (!g) return AAK_ERR_INVALID_PARAM;
+  return aak_ctx_set_parmap_model(g->ctx, m);
 }
 
 int aak_gpu_set_precision(aak_gpu *g, int32_t precision) {

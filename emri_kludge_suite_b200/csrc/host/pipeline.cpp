@@ -7,6 +7,7 @@
 
 #include "inspiral.hpp"
 #include "kerr.hpp"
+#include "parmap_data.hpp"
 
 namespace aak {
 
@@ -102,7 +103,8 @@ bool solve3(double A[3][3], double b[3], double x[3]) {
 }
 }  // namespace
 
-int parmap(const double Om[3], double p, double M, double s, double e, double iota, const double *x0, double map[3]) {
+int parmap(const double Om[3], double p, double M, double s, double e, double iota, const double *x0, double map[3],
+           int *iters_to_tol) {
   const double Y = std::cos(iota);
   double x[3];
   if (x0) {
@@ -118,6 +120,7 @@ int parmap(const double Om[3], double p, double M, double s, double e, double io
   parmap_residual(Om, M, e, Y, x, f);
   int iters = 0;
   bool reached = norm1(f) < 1e-6;
+  if (iters_to_tol) *iters_to_tol = reached ? 0 : -1;
   for (int it = 0; it < 200; ++it) {
     // Jacobian: central differences in v_map and s_map, exact in M_map
     double J[3][3];
@@ -153,7 +156,10 @@ int parmap(const double Om[3], double p, double M, double s, double e, double io
       f[i] = ft[i];
     }
     ++iters;
-    if (norm1(f) < 1e-6) reached = true;
+    if (norm1(f) < 1e-6 && !reached) {
+      reached = true;
+      if (iters_to_tol) *iters_to_tol = iters;
+    }
     if (reached && rel < 4e-16) break;
     if (norm1(f) == 0.0) break;
   }
@@ -169,18 +175,50 @@ double initial_mean_anomaly(double e, double psi) {
   return std::atan2(se * std::sin(psi), e + std::cos(psi)) - e * se * std::sin(psi) / (1. + e * std::cos(psi));
 }
 
+int parmap_warm(const double Om[3], double p, double M, double s, double e, double iota, const double guess[3],
+                double map[3], int *fallback, int *iters_to_tol) {
+  int it = parmap(Om, p, M, s, e, iota, guess, map, iters_to_tol);
+  // the warm solution must be the root the guess points at: a converged solve
+  // that wandered off (another root of the PN system) is redone from the plain guess
+  const bool near = it >= 0 && std::fabs(map[0] - guess[0]) * std::sqrt(p) < kWarmAcceptance &&
+                    std::fabs(map[1] - guess[1]) < kWarmAcceptance * M && std::fabs(map[2] - guess[2]) < kWarmAcceptance;
+  if (near) {
+    if (fallback) *fallback = 0;
+    return it;
+  }
+  if (fallback) *fallback = 1;
+  const int spent = it >= 0 ? it : -1 - it;
+  int tol2 = -1;
+  const int it2 = parmap(Om, p, M, s, e, iota, nullptr, map, &tol2);
+  if (iters_to_tol) *iters_to_tol = tol2 >= 0 ? tol2 + spent : -1;
+  return it2 >= 0 ? it2 + spent : it2 - spent;
+}
+
+double parmap_residual_norm(const double Om[3], double M, double e, double iota, const double map[3]) {
+  double f[3];
+  parmap_residual(Om, M, e, std::cos(iota), map, f);
+  return norm1(f);
+}
+
 int front_end(const Params &P, MappedTrajectory *out, const double *warm) {
   CoarseKerr ck;
   int st = coarse_kerr(P, &ck);
   if (st != kOk) return st;
+  return map_coarse(P, ck, out, warm, nullptr);
+}
+
+int map_coarse(const Params &P, const CoarseKerr &ck, MappedTrajectory *out, const double *warm, int *fallbacks) {
+  if (fallbacks) *fallbacks = 0;
   out->steps = ck.steps;
   out->inspiral_flag = ck.inspiral_flag;
   out->Phi0 = initial_mean_anomaly(P.e, P.psi);
   out->newton_iterations = 0;
   for (int i = 0; i < ck.steps; ++i) {
     double map[3];
-    int it = parmap(ck.Omega[i], ck.p[i], P.M, P.s, ck.e[i], P.iota, warm ? warm + 3 * i : nullptr, map);
-    if (it < 0 && warm) it = parmap(ck.Omega[i], ck.p[i], P.M, P.s, ck.e[i], P.iota, nullptr, map);  // fallback
+    int it, fb = 0;
+    if (warm) it = parmap_warm(ck.Omega[i], ck.p[i], P.M, P.s, ck.e[i], P.iota, warm + 3 * i, map, &fb);
+    else it = parmap(ck.Omega[i], ck.p[i], P.M, P.s, ck.e[i], P.iota, nullptr, map);
+    if (fallbacks) *fallbacks += fb;
     if (it < 0) return kErrSolverNoConverge;
     out->newton_iterations += it;
     out->e_traj[i] = ck.e[i];

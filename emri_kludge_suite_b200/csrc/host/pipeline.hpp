@@ -61,14 +61,31 @@ int coarse_kerr(const Params &P, CoarseKerr *out);
 
 // Kerr -> AK map at one point (KSParMap.cc:397-440): solve for
 // x = (v_map, M_map, s_map).  x0 == nullptr uses the reference's initial
-// guess (1/sqrt(p), M, s).  Returns Newton iterations (< 0 on failure).
-int parmap(const double Omega[3], double p, double M, double s, double e, double iota, const double *x0, double map[3]);
+// guess (1/sqrt(p), M, s).  The solve first reaches the reference's stopping
+// test |f|_1 < 1e-6 (after *iters_to_tol iterations, optional; -1 never) and
+// then polishes until the Newton step stalls at rounding level.  Returns the
+// Newton iterations (< 0 on failure).
+int parmap(const double Omega[3], double p, double M, double s, double e, double iota, const double *x0, double map[3],
+           int *iters_to_tol = nullptr);
+
+// The map from a warm guess.  The plain solve from the reference's guess
+// redoes a point when the warm solve fails the residual test or converges
+// farther than kWarmAcceptance (in v_map sqrt(p), M_map / M, s_map) from the
+// guess; *fallback (optional) is set then.  Returns the Newton iterations of
+// both solves (< 0 on failure).
+constexpr double kWarmAcceptance = 0.05;
+int parmap_warm(const double Omega[3], double p, double M, double s, double e, double iota, const double guess[3],
+                double map[3], int *fallback, int *iters_to_tol = nullptr);
 
 // Initial mean anomaly from the initial true anomaly psi (KSParMap.cc:25).
 double initial_mean_anomaly(double e, double psi);
 
 // Full front end (AAKpy.cc:20-44).  warm (optional, steps x 3) seeds the map.
 int front_end(const Params &P, MappedTrajectory *out, const double *warm = nullptr);
+// Second half of the front end: the map at every coarse point of ck.  Points
+// whose warm solve fails the residual test are re-solved from the plain
+// initial guess and counted in *fallbacks (optional).
+int map_coarse(const Params &P, const CoarseKerr &ck, MappedTrajectory *out, const double *warm, int *fallbacks);
 
 // Inputs of the reference GenWave/waveform (AAK.cc:321, 565).
 struct WaveInputs {

@@ -116,6 +116,13 @@ class GPUAAK:
         """0: FP64 throughout (default); 1: split precision."""
         check(lib().aak_gpu_set_precision(self._g, int(precision)), "set_precision")
 
+    def set_warm_start(self, model=None):
+        """Seed every Kerr->AK map solve of the template batches with a trained
+        :class:`~emri_kludge_suite_b200.parmap_mlp.ParMapMLP` (None: plain guess)."""
+        self._model = model
+        check(lib().aak_gpu_set_parmap_model(self._g, model.handle if model is not None else None),
+              "set_warm_start")
+
     def last_timing_ms(self):
         ms = np.zeros(4)
         check(lib().aak_gpu_last_timing(self._g, ptr(ms)), "timing")

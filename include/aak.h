@@ -30,11 +30,15 @@ enum aak_status {
   AAK_ERR_CUDA = 5,                     /* no usable GPU, or a CUDA/cuFFT call failed  */
   AAK_ERR_NO_MEMORY = 6,
   AAK_ERR_TOO_FEW_STEPS = 7,            /* coarse inspiral gave fewer than 3 points    */
-  AAK_ERR_CAPACITY = 8                  /* request exceeds a fixed-size buffer         */
+  AAK_ERR_CAPACITY = 8,                 /* request exceeds a fixed-size buffer         */
+  AAK_ERR_DEVICE_TIMEOUT = 9            /* a bounded device-side wait gave up          */
 };
 
 const char *aak_status_string(int status);
 int aak_version(void);
+/* Name and text of the last CUDA error this thread's calls turned into a
+ * status (empty if none). */
+const char *aak_last_error_detail(void);
 
 /* ------------------------------------------------------------------ parameters */
 /* Numeric fields of the reference's SetPar (include/KSTools.h:21-53) and the
@@ -104,7 +108,9 @@ int aak_genwave(double *t, double *hI, double *hII, double timestep, int32_t vle
                 int32_t nmodes_override);
 
 /* ------------------------------------------------------------------ batched waveforms */
-/* A context owns the device buffers of one batch on one device. */
+/* A context owns the device buffers of one batch on one device.  device -1
+ * makes a host-only context: planning and the plan queries work without a
+ * GPU, the upload and run calls return AAK_ERR_INVALID_PARAM. */
 typedef struct aak_ctx aak_ctx;
 
 int aak_ctx_create(int32_t device, aak_ctx **out);
@@ -184,7 +190,8 @@ int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const i
  * src/cuda/AAK_manager.cu, pygpuAAK/GPUAAK.pyx:50-93), on the current CUDA
  * device.  init_length / init_dt are accepted for call compatibility; the
  * coarse grid follows the reference CPU AAK.  Templates are generated with
- * the reference CPU conventions. */
+ * the reference CPU conventions (the AAKwave path, src/suite/AAK.cc), not the
+ * GPU port's own coarse grid. */
 typedef struct aak_gpu aak_gpu;
 
 /* GPUAAK(T_fit, init_length, length, init_dt, dt, LISA, backint) */
@@ -222,6 +229,77 @@ int aak_gpu_set_precision(aak_gpu *g, int32_t precision);
 
 /* Milliseconds of the last batch: host planning, waveform kernels, FFT, reduction. */
 int aak_gpu_last_timing(aak_gpu *g, double *ms4);
+
+/* ------------------------------------------------------------------ learned ParMap warm start */
+/* No reference counterpart: a 4 -> 128 -> 128 -> 128 -> 3 SiLU network (BF16
+ * weights and activations, FP32 accumulation, tcgen05 tensor cores for the
+ * 128 x 128 layers) that predicts the solution of the Kerr -> AK map
+ * (ParMap, src/suite/KSParMap.cc:397-440) from (p, e, iota, a), as the
+ * initial guess of the plain Newton solve, which stays the fallback and the
+ * judge (|f|_1 < 1e-6).  Outputs are map coordinates
+ * y = (v_map sqrt(p), M_map / M, s_map - a).  Parameters are one FP32 vector
+ * of aak_mlp_num_params() values: W1[128][4] b1 W2[128][128] b2 W3[128][128]
+ * b3 W4[3][128] b4.  Inputs enter as ((1/sqrt(p), e, cos iota, a) - in_shift)
+ * * in_scale; outputs leave as net * out_scale + out_shift. */
+typedef struct aak_mlp aak_mlp;
+
+int aak_mlp_num_params(void);
+int aak_mlp_max_train_rows(void);
+int aak_mlp_create(int32_t device, aak_mlp **out);
+void aak_mlp_destroy(aak_mlp *m);
+/* Host FP32 parameters in / out; set_params also resets the Adam state. */
+int aak_mlp_set_params(aak_mlp *m, const float *params);
+int aak_mlp_get_params(aak_mlp *m, float *params);
+int aak_mlp_set_norm(aak_mlp *m, const float in_shift[4], const float in_scale[4], const float out_shift[3],
+                     const float out_scale[3]);
+int aak_mlp_set_adam(aak_mlp *m, float beta1, float beta2, float eps);
+/* Device pointers: d_x n x 4 (p, e, iota, a), d_y n x 3 map coordinates. */
+int aak_mlp_forward(aak_mlp *m, const float *d_x, float *d_y, int64_t n, void *stream);
+/* Gradient of the mean squared error in normalised output units over rows
+ * d_perm[0..n) (d_perm NULL: rows 0..n) of (d_x, d_y); n <= aak_mlp_max_train_rows().
+ * d_grad: aak_mlp_num_params() floats (device).  *loss (optional, host)
+ * synchronises the stream. */
+int aak_mlp_gradients(aak_mlp *m, const float *d_x, const float *d_y, const int32_t *d_perm, int64_t n, float *d_grad,
+                      float *loss, void *stream);
+/* One Adam step (learning rate lr) on the same loss. */
+int aak_mlp_train_step(aak_mlp *m, const float *d_x, const float *d_y, const int32_t *d_perm, int64_t n, float lr,
+                       float *loss, void *stream);
+/* AAK_ERR_DEVICE_TIMEOUT if a kernel of the model gave up a bounded wait. */
+int aak_mlp_status(aak_mlp *m);
+/* Host convenience: x n x 4 -> y n x 3 (synchronous). */
+int aak_mlp_predict_host(aak_mlp *m, const double *x, double *y, int64_t n);
+
+/* Separatrix p_sep(e, iota, a) by bisection on geodesic stability (the test
+ * of the reference's LSO search, src/suite/GKTrajFast.cc constructor). */
+int aak_parmap_separatrix(double e, double iota, double a, double *p_sep);
+/* Points first_index .. first_index + n - 1 of the seeded distribution
+ * p ~ U(p_sep + 0.1, 20), e ~ U(0, 0.7) (redrawn below 1e-3), iota ~ U(0, pi),
+ * a ~ U(0, 0.95), labelled by the plain map solve at M = 1e6: x n x 4, y n x 3
+ * (map coordinates, NaN where the solve failed), omega n x 3 Kerr frequencies,
+ * iters n (Newton iterations; < 0: failed). */
+int aak_parmap_dataset(int64_t n, uint64_t seed, uint64_t first_index, int32_t nthreads, double *x, double *y,
+                       double *omega, int32_t *iters);
+/* Map solves from the guesses (n x 3 map coordinates; NULL: the reference's
+ * plain initial guess).  A guess whose solve fails the residual test, or
+ * converges more than 0.05 (in map coordinates) away from the guess, is
+ * re-solved from the plain guess (fallback[i] = 1; iters counts both).
+ * iters: Newton iterations to the converged (rounding-level) solution;
+ * iters_to_tol (optional): iterations until |f|_1 < 1e-6, the reference's
+ * stopping test (-1: never reached). 
+ * residual / guess_residual: |f|_1 at the solution / at the guess (optional). */
+int aak_parmap_solve_batch(int64_t n, const double *x, const double *omega, const double *guess, int32_t nthreads,
+                           double *y, int32_t *iters, int32_t *iters_to_tol, double *residual, double *guess_residual,
+                           int32_t *fallback);
+
+/* Batch planning with the warm start: every coarse point of every source is
+ * predicted in one launch, then solved from its prediction.  m NULL restores
+ * the plain initial guess.  The model must outlive its use by the context. */
+int aak_ctx_set_parmap_model(aak_ctx *ctx, aak_mlp *m);
+/* Map statistics of the last plan: coarse points solved, Newton iterations,
+ * warm starts that fell back to the plain guess. */
+int aak_batch_newton_stats(aak_ctx *ctx, int64_t *points, int64_t *iterations, int64_t *fallbacks);
+/* The same for the likelihood object's template batches. */
+int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m);
 
 #ifdef __cplusplus
 }
