@@ -433,6 +433,34 @@ def run_gpu(args, rank, world, local_rank):
              "speedup_vs_fp64": ms / ms_split}
     del hI2, hII2
 
+    # ---- plain FP64 per-source path on a subset of the same sources (the baseline)
+    plain = None
+    if args.plain_sources > 0:
+        sub = sources[:: max(1, len(sources) // args.plain_sources)][: args.plain_sources]
+        wp = E.WaveBatch(local_rank)
+        wp.plan(sub, nmodes=NMODES, nthreads=nthreads)
+        wp.upload(sptr)
+        Np = wp.total_samples
+        pI = torch.empty(Np, dtype=torch.float64, device="cuda")
+        pII = torch.empty_like(pI)
+        traj = torch.empty(9 * Np, dtype=torch.float64, device="cuda")
+        wp.run_plain(pI.data_ptr(), pII.data_ptr(), traj.data_ptr(), Np, stream=sptr)  # warm-up
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        wp.run_plain(pI.data_ptr(), pII.data_ptr(), traj.data_ptr(), Np, stream=sptr)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms_plain = ev0.elapsed_time(ev1)
+        sps = Np / (ms_plain * 1e-3)
+        plain = {"samples_per_s": sps, "sources": len(sub), "samples": int(Np), "ms": ms_plain,
+                 "launches": wp.launches(),
+                 "method": "per source: phase kernels on a one-source view writing the dense FP64 trajectory "
+                           "(72 B/sample), then one thread per sample with 5 jn() + cos/sin + rotation per harmonic",
+                 "speedup_batched_fp64": (N_all * args.steps / (ms * 1e-3)) / sps,
+                 "speedup_batched_split": split["value"] / sps}
+        del pI, pII, traj
+        wp.close()
+
     # ---- end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     hIh = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -491,6 +519,7 @@ def run_gpu(args, rank, world, local_rank):
                    "parallelism": f"sources sharded, {world} rank(s)"},
         "kernel_ms": {"phase_tile_sums": kern[0], "phase_carry": kern[1], "waveform_fp64": kern[2]},
         "split_precision": split,
+        "plain_fp64_per_source": plain,
         "roofline": roofline,
         "clocks": clk,
         "e2e": e2e,
@@ -519,6 +548,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--likelihood", type=int, default=1024, help="config-4 templates to time (0: skip)")
+    ap.add_argument("--plain-sources", type=int, default=16,
+                    help="sources of the plain FP64 per-source baseline (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,
                     help="config-3 training points of the warm-start network (0: skip)")
     args = ap.parse_args()

@@ -128,6 +128,7 @@ def lib():
     L.aak_batch_plan_bytes.argtypes = [_vp, _i64p]
     L.aak_batch_run.argtypes = [_vp, _vp, _vp, _vp, _vp, _i64, _i32, _vp]
     L.aak_batch_run_noalloc.argtypes = [_vp, _vp, _i64, _i64p, _vp, _vp, _vp]
+    L.aak_batch_run_plain.argtypes = [_vp, _vp, _vp, _vp, _i64, _vp]
     L.aak_batch_last_launches.argtypes = [_vp]
     L.aak_batch_set_profiling.argtypes = [_vp, _i32]
     L.aak_batch_kernel_ms.argtypes = [_vp, ctypes.POINTER(ctypes.c_float)]

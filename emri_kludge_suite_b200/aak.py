@@ -198,6 +198,13 @@ class WaveBatch:
     def launches(self) -> int:
         return int(lib().aak_batch_last_launches(self._ctx))
 
+    def run_plain(self, hI_ptr: int, hII_ptr: int, traj_ptr: int, traj_stride: int, stream: int = 0):
+        """The plain FP64 per-source path (baseline): one source at a time, dense
+        trajectory in ``traj_ptr`` (9 x traj_stride doubles), five jn() per harmonic."""
+        check(lib().aak_batch_run_plain(self._ctx, ctypes.c_void_p(hI_ptr), ctypes.c_void_p(hII_ptr),
+                                        ctypes.c_void_p(traj_ptr), int(traj_stride), ctypes.c_void_p(stream)),
+              "aak_batch_run_plain")
+
     def generate_host(self, params, nmodes=None, nthreads: int = 0):
         """Plan + upload + run + copy back (host buffers).  Returns (hI, hII, offsets, status)."""
         self.nsrc = len(params)

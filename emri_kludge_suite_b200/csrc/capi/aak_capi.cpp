@@ -67,6 +67,7 @@ struct aak_ctx {
   std::vector<int32_t> status;
   std::vector<SourceDesc> descs;
   std::vector<int64_t> tile_start;
+  std::vector<int64_t> tile_pairs;  // per source {0, its tiles}: the tile prefix of a one-source view
   std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
   std::vector<double> knot_t;
   std::vector<double4> knot_y, knot_c;
@@ -76,7 +77,7 @@ struct aak_ctx {
   bool uploaded = false;
   // device buffers
   DevBuf<SourceDesc> d_src;
-  DevBuf<int64_t> d_tile_start;
+  DevBuf<int64_t> d_tile_start, d_tile_pairs;
   DevBuf<int32_t> d_tile_knot;
   DevBuf<double> d_knot_t;
   DevBuf<double4> d_knot_y, d_knot_c;
@@ -213,6 +214,8 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
     d.n_tiles = (int32_t)(ctx->tile_start[s + 1] - ctx->tile_start[s]);
     ctx->descs[s] = d;
   }
+  ctx->tile_pairs.assign(2 * (size_t)n, 0);
+  for (int s = 0; s < n; ++s) ctx->tile_pairs[2 * s + 1] = ctx->tile_start[s + 1] - ctx->tile_start[s];
   // knot window of every tile: knots bracketing samples start-1 .. start+1024
   ctx->tile_knot.assign(2 * std::max<int64_t>(ctx->total_tiles, 1), 0);
   for (int s = 0; s < n; ++s) {
@@ -331,7 +334,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
   const int n = ctx->nsrc;
   if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
-      (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) ||
+      (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) || (r = ctx->d_tile_pairs.reserve(ctx->tile_pairs.size())) ||
       (r = ctx->d_knot_t.reserve(ctx->knot_t.size())) || (r = ctx->d_knot_y.reserve(ctx->knot_y.size())) ||
       (r = ctx->d_knot_c.reserve(ctx->knot_c.size())) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
       (r = ctx->d_summ.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
@@ -343,6 +346,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   if ((r = cp(ctx->d_src.ptr, ctx->descs.data(), n * sizeof(SourceDesc))) ||
       (r = cp(ctx->d_tile_start.ptr, ctx->tile_start.data(), (n + 1) * sizeof(int64_t))) ||
       (r = cp(ctx->d_tile_knot.ptr, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
+      (r = cp(ctx->d_tile_pairs.ptr, ctx->tile_pairs.data(), ctx->tile_pairs.size() * sizeof(int64_t))) ||
       (r = cp(ctx->d_knot_t.ptr, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
       (r = cp(ctx->d_knot_y.ptr, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
       (r = cp(ctx->d_knot_c.ptr, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
@@ -382,6 +386,47 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
     for (auto &e : ctx->ev) cudaEventCreate(&e);
   launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
   ctx->last_launches = 3;
+  return cuda_ok(cudaGetLastError());
+}
+
+// Plain FP64 per-source path: source by source, the phase kernels on a
+// one-source view write the dense trajectory, then the per-harmonic kernel.
+int run_plain(aak_ctx *ctx, double *hI, double *hII, double *traj, int64_t traj_stride, cudaStream_t st) {
+  if (!ctx->uploaded || !hI || !hII || !traj || traj_stride < ctx->total_samples) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  int launches = 0;
+  for (int s = 0; s < ctx->nsrc; ++s) {
+    const SourceDesc &d = ctx->descs[s];
+    if (ctx->status[s] != AAK_OK) {
+      cudaMemsetAsync(hI + d.out_offset, 0, sizeof(double) * d.vlength, st);
+      cudaMemsetAsync(hII + d.out_offset, 0, sizeof(double) * d.vlength, st);
+      continue;
+    }
+    BatchView v;
+    v.src = ctx->d_src.ptr + s;
+    v.nsrc = 1;
+    v.total_tiles = d.n_tiles;
+    v.tile_start = ctx->d_tile_pairs.ptr + 2 * s;
+    v.tile_knot = ctx->d_tile_knot.ptr + 2 * d.tile_offset;
+    v.knot_t = ctx->d_knot_t.ptr;
+    v.knot_y = ctx->d_knot_y.ptr;
+    v.knot_c = ctx->d_knot_c.ptr;
+    v.bessel_start = ctx->d_bessel.ptr;
+    v.summ = ctx->d_summ.ptr + d.tile_offset;
+    v.carry = ctx->d_carry.ptr + d.tile_offset;
+    v.hI = hI;
+    v.hII = hII;
+    v.t_out = nullptr;
+    v.traj_out = traj;
+    v.traj_stride = traj_stride;
+    v.work_counter = ctx->d_counter.ptr;
+    v.trajectory_only = 1;
+    launch_dense(v, ctx->num_sms, st, nullptr, 0);
+    launch_plain_waveform(ctx->d_src.ptr, s, d.vlength, traj, traj_stride, hI, hII, st);
+    launches += 4;
+  }
+  ctx->last_launches = launches;
   return cuda_ok(cudaGetLastError());
 }
 
@@ -500,6 +545,7 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_src.release();
     c->d_tile_start.release();
     c->d_tile_knot.release();
+    c->d_tile_pairs.release();
     c->d_knot_t.release();
     c->d_knot_y.release();
     c->d_knot_c.release();
@@ -577,6 +623,12 @@ int aak_batch_run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj
   if (!ctx) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
   return run(ctx, hI, hII, t, traj, traj_stride, precision, (cudaStream_t)stream);
+}
+
+int aak_batch_run_plain(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_traj, int64_t traj_stride, void *stream) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return run_plain(ctx, d_hI, d_hII, d_traj, traj_stride, (cudaStream_t)stream);
 }
 
 int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_t *required_bytes, double *d_hI,

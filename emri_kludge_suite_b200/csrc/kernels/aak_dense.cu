@@ -1041,7 +1041,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const int K = kSplit ? ts.k32 : ts.k64;
     const double ec = ts.ec;
     // Bessel table rows (one thread per harmonic); its barrier is the first one of phase 1
-    if (K > 0)
+    if (K > 0 && !bv.trajectory_only)
       for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
         double *Tn = s_T + (n - 1) * kTabStride;
         build_bessel_row(Tn, n, n * ec, K, bstart[n - 1]);
@@ -1166,6 +1166,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       __syncthreads();
     }
     // ---------------- phase 2: harmonic sums of this thread's own samples
+    if (bv.trajectory_only) continue;
     const double t_plunge = sample_time(d, d.i_plunge);
     const double t_zero = t_plunge + d.dt * d.i_buffer;
     for (int ch = 0; ch < kTileChunks; ++ch) {
@@ -1194,7 +1195,125 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   }
 }
 
+// ------------------------------------------------------------------ plain FP64 per-source path
+// One thread per sample, everything per harmonic, as the reference's CUDA
+// port evaluates it (src/cuda/kernel.cu:374-555); the response, orientation
+// and taper conventions are those of the FP64 path above, so the two agree.
+__global__ void __launch_bounds__(256) k_plain_waveform(const SourceDesc *__restrict__ src, int s,
+                                                        const double *__restrict__ traj, int64_t st,
+                                                        double *__restrict__ hI_out, double *__restrict__ hII_out) {
+  const SourceDesc &d = src[s];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.vlength) return;
+  const int64_t o = d.out_offset + i;
+  const double t = sample_time(d, i);
+  if (i >= n_eff(d)) {
+    hI_out[o] = 0.0;
+    hII_out[o] = 0.0;
+    return;
+  }
+  const double e = traj[o], gim = traj[4 * st + o], Phi = traj[5 * st + o], alp = traj[6 * st + o];
+  const double nu = traj[7 * st + o], gimdot = traj[8 * st + o];
+  const double om_M = omega_phi(traj[st + o], e, d.coslam, traj[3 * st + o], traj[2 * st + o]) * d.M_phys_sec;
+
+  const double cosalp = cos(alp), sinalp = sin(alp);
+  const double cosqL = d.cosqK * d.coslam + d.sinqK * d.sinlam * cosalp;
+  const double sinqL = sqrt(1. - cosqL * cosqL);
+  const double phiLup = d.sinqK * d.sinphiK * d.coslam - d.cosphiK * d.sinlam * sinalp - d.cosqK * d.sinphiK * d.sinlam * cosalp;
+  const double phiLdown = d.sinqK * d.cosphiK * d.coslam + d.sinphiK * d.sinlam * sinalp - d.cosqK * d.cosphiK * d.sinlam * cosalp;
+  const double Ldotn = cosqL * d.cosqS + sinqL * d.sinqS * cos(atan2(phiLup, phiLdown) - d.phiS);
+  const double Ldotn2 = Ldotn * Ldotn;
+  const double Sdotn = d.cosqK * d.cosqS + d.sinqK * d.sinqS * cos(d.phiK - d.phiS);
+  const double beta = atan2(-Sdotn + d.coslam * Ldotn,
+                            d.sinqS * sin(d.phiK - d.phiS) * d.sinlam * cosalp + (d.cosqK * Sdotn - d.cosqS) / d.sinqK * d.sinlam * sinalp);
+  const double cos2gam = cos(2. * (gim + beta)), sin2gam = sin(2. * (gim + beta));
+
+  double cosorbphs = 0.0, FplusI, FcrosI, FplusII, FcrosII, Kresp;
+  if (d.mich) {
+    const double orbphs = kTwoPi * t / kYear;
+    cosorbphs = cos(orbphs - d.phiS);
+    const double sinorbphs = sin(orbphs - d.phiS);
+    const double cosq = .5 * d.cosqS - kHalfSqrt3 * d.sinqS * cosorbphs;
+    const double phiw = orbphs + atan2(kHalfSqrt3 * d.cosqS + .5 * d.sinqS * cosorbphs, d.sinqS * sinorbphs);
+    const double psiup = .5 * d.cosqK - kHalfSqrt3 * d.sinqK * cos(orbphs - d.phiK) - cosq * Sdotn;
+    const double psidown = .5 * d.sinqK * d.sinqS * sin(d.phiK - d.phiS) -
+                           kHalfSqrt3 * cos(orbphs) * (d.cosqK * d.sinqS * sin(d.phiS) - d.cosqS * d.sinqK * sin(d.phiK)) -
+                           kHalfSqrt3 * sin(orbphs) * (d.cosqS * d.sinqK * cos(d.phiK) - d.cosqK * d.sinqS * cos(d.phiS));
+    const double psi = atan2(psiup, psidown);
+    const double cosq1 = .5 * (1. + cosq * cosq);
+    const double cos2phi = cos(2. * phiw), sin2phi = sin(2. * phiw), cos2psi = cos(2. * psi), sin2psi = sin(2. * psi);
+    FplusI = cosq1 * cos2phi * cos2psi - cosq * sin2phi * sin2psi;
+    FcrosI = cosq1 * cos2phi * sin2psi + cosq * sin2phi * cos2psi;
+    FplusII = cosq1 * sin2phi * cos2psi + cosq * cos2phi * sin2psi;
+    FcrosII = cosq1 * sin2phi * sin2psi - cosq * cos2phi * cos2psi;
+    Kresp = kHalfSqrt3;
+  } else {
+    const double up_ldc = d.cosqS * d.sinqK * cos(d.phiS - d.phiK) - d.cosqK * d.sinqS;
+    const double dw_ldc = d.sinqK * sin(d.phiS - d.phiK);
+    const double psi_ldc = (dw_ldc != 0.0) ? -atan2(up_ldc, dw_ldc) : 0.5 * kPi;
+    FplusI = cos(2. * psi_ldc);
+    FcrosI = -sin(2. * psi_ldc);
+    FplusII = sin(2. * psi_ldc);
+    FcrosII = cos(2. * psi_ldc);
+    Kresp = 1.0;
+  }
+  const double Amp = pow(om_M, 2. / 3.) * d.zeta;
+  const double se = sqrt(1. - e * e);
+  double hI = 0.0, hII = 0.0;
+  for (int n = 1; n <= d.nmodes; ++n) {
+    double nPhi = n * Phi;
+    if (d.mich) nPhi += kTwoPi * (n * nu + gimdot / kPi) * kAUsec * d.sinqS * cosorbphs;
+    const double ne = n * e;
+    double J[5];
+    if (n == 1) {
+      J[0] = -j1(ne);
+      J[1] = j0(ne);
+      J[2] = j1(ne);
+      J[3] = jn(2, ne);
+      J[4] = jn(3, ne);
+    } else {
+      for (int k = 0; k < 5; ++k) J[k] = jn(n - 2 + k, ne);
+    }
+    const double cn = cos(nPhi), sn = sin(nPhi);
+    const double a = -n * Amp * (J[0] - 2. * e * J[1] + 2. / n * J[2] + 2. * e * J[3] - J[4]) * cn;
+    const double b = -n * Amp * se * (J[0] - 2. * J[2] + J[4]) * sn;
+    const double c = 2. * Amp * J[2] * cn;
+    const double Aplus = -(1. + Ldotn2) * (a * cos2gam - b * sin2gam) + c * (1. - Ldotn2);
+    const double Acros = 2. * Ldotn * (b * cos2gam + a * sin2gam);
+    // rotation to the NK wave frame, per harmonic as in the port
+    const double n0 = d.sinqS * cos(d.phiS), n1 = d.sinqS * sin(d.phiS), n2 = d.cosqS;
+    const double S0 = d.sinqK * d.cosphiK, S1 = d.sinqK * d.sinphiK, S2 = d.cosqK;
+    const double L0 = d.coslam * d.sinqK * d.cosphiK + d.sinlam * (sinalp * d.sinphiK - cosalp * d.cosqK * d.cosphiK);
+    const double L1 = d.coslam * d.sinqK * d.sinphiK - d.sinlam * (sinalp * d.cosphiK + cosalp * d.cosqK * d.sinphiK);
+    const double L2 = d.coslam * d.cosqK + d.sinlam * cosalp * d.sinqK;
+    const double nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
+    const double nS0 = n1 * S2 - n2 * S1, nS1 = n2 * S0 - n0 * S2, nS2 = n0 * S1 - n1 * S0;
+    const double norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * sqrt(nS0 * nS0 + nS1 * nS1 + nS2 * nS2);
+    const double cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
+    const double sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
+    const double r0 = 2. * cosrot * cosrot - 1., r1 = cosrot * sinrot;
+    const double Ap = Aplus * r0 + Acros * r1, Ac = -Aplus * r1 + Acros * r0;
+    hI += Kresp * (FplusI * Ap + FcrosI * Ac);
+    hII += Kresp * (FplusII * Ap + FcrosII * Ac);
+  }
+  if (i > d.i_plunge) {
+    const double t_plunge = sample_time(d, d.i_plunge);
+    const double t_zero = t_plunge + d.dt * d.i_buffer;
+    const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
+    hI /= wgt;
+    hII /= wgt;
+  }
+  hI_out[o] = hI;
+  hII_out[o] = hII;
+}
+
 }  // namespace
+
+void launch_plain_waveform(const SourceDesc *src, int s, int vlength, const double *traj, int64_t traj_stride,
+                           double *hI, double *hII, cudaStream_t stream) {
+  if (vlength <= 0) return;
+  k_plain_waveform<<<(vlength + 255) / 256, 256, 0, stream>>>(src, s, traj, traj_stride, hI, hII);
+}
 
 void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev) {
   launch_dense(bv, num_sms, stream, ev, 0);

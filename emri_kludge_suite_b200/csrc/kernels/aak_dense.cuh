@@ -56,6 +56,7 @@ struct BatchView {
   double *traj_out;             // optional dense trajectory, 9 x total samples (e,v,M,S,gim,Phi,alp,nu,gimdot)
   int64_t traj_stride;
   unsigned long long *work_counter;  // persistent work queue head (pass 2)
+  int32_t trajectory_only = 0;       // 1: pass 2 writes traj_out and skips the harmonic sums
 };
 
 // Launch pass 1, the carry scan and pass 2 on `stream`.  ev (optional, 4
@@ -64,6 +65,14 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
 // precision 0: FP64 throughout; 1: split (FP64 phases and reductions, FP32
 // geometry, response, Bessel evaluation and harmonic recurrence).
 void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision);
+
+// Plain FP64 per-source harmonic sum: the per-sample algorithm of the
+// reference's CUDA port (src/cuda/kernel.cu:374-555) -- five Bessel functions
+// jn(n-2 .. n+2, n e), one cos/sin of n Phi and the NK-frame rotation per
+// harmonic -- on the dense trajectory (9 x traj_stride doubles, as pass 2
+// writes with trajectory_only) of source s of the batch.
+void launch_plain_waveform(const SourceDesc *src, int s, int vlength, const double *traj, int64_t traj_stride,
+                           double *hI, double *hII, cudaStream_t stream);
 
 // Diagnostic: sustained FP64 FMA issue rate of this device in TFLOP/s
 // (2 flops per FMA), measured with CUDA events over `iters` launches.

@@ -177,6 +177,16 @@ int aak_batch_last_launches(aak_ctx *ctx);
 int aak_batch_set_profiling(aak_ctx *ctx, int32_t on);
 int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3);
 
+/* Plain FP64 per-source path (the baseline the batched paths are measured
+ * against; no reference counterpart as an entry point): source by source,
+ * the phase kernels write the dense FP64 trajectory (9 x traj_stride doubles
+ * in d_traj: e, v, M, S, gamma~, Phi, alpha, nu, gamma~dot), then one thread
+ * per sample evaluates the harmonic sum as the reference's CUDA port does
+ * (src/cuda/kernel.cu:374-555): five jn() Bessel calls, cos/sin of n Phi and
+ * the NK-frame rotation per harmonic.  Same outputs as aak_batch_run with
+ * precision 0, to Bessel-evaluation rounding. */
+int aak_batch_run_plain(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_traj, int64_t traj_stride, void *stream);
+
 /* Diagnostic: sustained FP64 FMA rate of `device` in TFLOP/s (roofline denominator). */
 int aak_probe_fp64_tflops(int32_t device, double *tflops);
 
