@@ -86,7 +86,7 @@ AAK_HD double omega_phi(double v, double e, double cosiota, double s, double M) 
 
 // ---------------------------------------------------------------------------
 // Per-source record consumed by the dense kernels.  One per source, built by
-// the host pipeline (evolve.cpp) and copied to HBM as an array of structs.
+// the host pipeline (pipeline.cpp) and copied to HBM as an array of structs.
 // All times are in seconds; masses M_sec in seconds.
 struct alignas(16) SourceDesc {
   // orientation (reference waveform(), AAK.cc:323-338)
@@ -99,6 +99,16 @@ struct alignas(16) SourceDesc {
   double t_first;    // time of dense sample 0 (first knot time)
   double Phi0, gim0, alp0;
   double rot_sign;   // unused padding slot (kept for alignment)
+  // per-source constants of the orientation and response (host-computed):
+  // L(alpha) = Lc + sin(alpha) Ls + cos(alpha) Lq is the orbital angular
+  // momentum direction of AAK.cc:427-431 / KSParMap.cc:547-549
+  double nv[3], Sv[3], Lc[3], Ls[3], Lq[3];
+  double nxS[3], nxS_norm;  // n x S and |n x S| (RotCoeff)
+  double Sdotn;
+  double beta_c, beta_s;    // denominator of beta: beta_c cos(alpha) + beta_s sin(alpha)
+  double cphiS, sphiS;
+  double psd0, psd1, psd2;  // LISA psi denominator: psd0 - psd1 cos(orb) - psd2 sin(orb)
+  double F0[4];             // response without LISA: F+_I, Fx_I, F+_II, Fx_II
   int64_t out_offset;   // first output sample of this source in the batch arrays
   int64_t knot_offset;  // first knot of this source in the knot arrays
   int64_t tile_offset;  // first tile of this source in the tile arrays

@@ -73,6 +73,7 @@ struct aak_ctx {
   std::vector<double4> knot_y, knot_c;
   std::vector<int32_t> bessel;
   int64_t total_samples = 0, total_tiles = 0, total_knots = 0;
+  int32_t max_nmodes = 0;
   int64_t out_stride = 0;  // > 0: source s writes at s * out_stride (FFT-padded rows)
   bool uploaded = false;
   // device buffers
@@ -180,6 +181,9 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
       bes += pl.nmodes;
     }
   }
+  ctx->max_nmodes = 0;
+  for (int s = 0; s < n; ++s)
+    if (ctx->status[s] == AAK_OK) ctx->max_nmodes = std::max(ctx->max_nmodes, (int32_t)ctx->plans[s].nmodes);
   ctx->total_samples = ctx->offsets[n];
   ctx->total_tiles = ctx->tile_start[n];
   ctx->total_knots = knots;
@@ -382,6 +386,7 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   bv.traj_out = traj;
   bv.traj_stride = traj_stride;
   bv.work_counter = ctx->d_counter.ptr;
+  bv.max_nmodes = ctx->max_nmodes;
   if (ctx->profile && !ctx->ev[0])
     for (auto &e : ctx->ev) cudaEventCreate(&e);
   launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
@@ -422,6 +427,7 @@ int run_plain(aak_ctx *ctx, double *hI, double *hII, double *traj, int64_t traj_
     v.traj_stride = traj_stride;
     v.work_counter = ctx->d_counter.ptr;
     v.trajectory_only = 1;
+    v.max_nmodes = ctx->max_nmodes;
     launch_dense(v, ctx->num_sms, st, nullptr, 0);
     launch_plain_waveform(ctx->d_src.ptr, s, d.vlength, traj, traj_stride, hI, hII, st);
     launches += 4;
@@ -678,6 +684,7 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   bv.knot_y = reinterpret_cast<const double4 *>(base + o_ky);
   bv.knot_c = reinterpret_cast<const double4 *>(base + o_kc);
   bv.bessel_start = reinterpret_cast<const int32_t *>(base + o_bs);
+  bv.max_nmodes = ctx->max_nmodes;
   bv.hI = d_hI;
   bv.hII = d_hII;
   return launch_dense_fp64_static_scratch(bv, ctx->device, ctx->num_sms, st);

@@ -404,6 +404,45 @@ inline double p_of(double v, double e, double coslam, double S, double M, double
 }
 }  // namespace
 
+// Per-source constants of the waveform geometry (the alpha-independent
+// pieces of AAK.cc:425-478 and of RotCoeff, KSParMap.cc:532-574).
+void fill_geometry(SourceDesc *d) {
+  const double hs3 = 0.5 * std::sqrt(3.0);
+  const double cS = d->cosqS, sS = d->sinqS, cK = d->cosqK, sK = d->sinqK;
+  const double cpK = d->cosphiK, spK = d->sinphiK, cl = d->coslam, sl = d->sinlam;
+  d->cphiS = std::cos(d->phiS);
+  d->sphiS = std::sin(d->phiS);
+  const double n[3] = {sS * d->cphiS, sS * d->sphiS, cS};
+  const double S[3] = {sK * cpK, sK * spK, cK};
+  const double Ls[3] = {sl * spK, -sl * cpK, 0.0};
+  const double Lq[3] = {-sl * cK * cpK, -sl * cK * spK, sl * sK};
+  for (int i = 0; i < 3; ++i) {
+    d->nv[i] = n[i];
+    d->Sv[i] = S[i];
+    d->Lc[i] = cl * S[i];
+    d->Ls[i] = Ls[i];
+    d->Lq[i] = Lq[i];
+  }
+  d->nxS[0] = n[1] * S[2] - n[2] * S[1];
+  d->nxS[1] = n[2] * S[0] - n[0] * S[2];
+  d->nxS[2] = n[0] * S[1] - n[1] * S[0];
+  d->nxS_norm = std::sqrt(d->nxS[0] * d->nxS[0] + d->nxS[1] * d->nxS[1] + d->nxS[2] * d->nxS[2]);
+  d->Sdotn = cK * cS + sK * sS * std::cos(d->phiK - d->phiS);
+  d->beta_c = sS * std::sin(d->phiK - d->phiS) * sl;
+  d->beta_s = (cK * d->Sdotn - cS) / sK * sl;
+  d->psd0 = .5 * sK * sS * std::sin(d->phiK - d->phiS);
+  d->psd1 = hs3 * (cK * sS * std::sin(d->phiS) - cS * sK * std::sin(d->phiK));
+  d->psd2 = hs3 * (cS * sK * std::cos(d->phiK) - cK * sS * std::cos(d->phiS));
+  // without LISA: polarisation angle of the source frame (AAK.cc:463-478)
+  const double up = cS * sK * std::cos(d->phiS - d->phiK) - cK * sS;
+  const double dw = sK * std::sin(d->phiS - d->phiK);
+  const double psi = (dw != 0.0) ? -std::atan2(up, dw) : 0.5 * kPi;
+  d->F0[0] = std::cos(2. * psi);
+  d->F0[1] = -std::sin(2. * psi);
+  d->F0[2] = std::sin(2. * psi);
+  d->F0[3] = std::cos(2. * psi);
+}
+
 int plan_source(const WaveInputs &w, SourcePlan *plan) {
   plan->status = kOk;
   const int vlength = w.vlength, steps = w.steps;
@@ -612,6 +651,7 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   d.cosphiK = std::cos(par[10]);
   d.sinphiK = std::sin(par[10]);
   d.zeta = w.zeta;
+  fill_geometry(&d);
   d.M_phys_sec = M_phys * kMsunSec;
   d.dt = timestep;
   d.t_first = plan->t_first;

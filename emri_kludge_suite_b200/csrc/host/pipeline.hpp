@@ -120,6 +120,8 @@ struct SourcePlan {
 };
 
 int plan_source(const WaveInputs &w, SourcePlan *plan);
+// Per-source geometry constants of the waveform (orientation fields set).
+void fill_geometry(SourceDesc *d);
 
 // Natural cubic spline helpers (shared by the plan and tests).
 void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c);

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "aak_dense.cuh"
@@ -284,11 +285,11 @@ __device__ __forceinline__ Lin clamp_phidot(const double *raw, int slot, int fir
   return Lin{0.0, 1.0};
 }
 
-// term-count rules of the multiplication theorem (defined with the harmonic sums);
-// sources with more modes than kTabModes evaluate Bessel functions per sample
+// Taylor-table term counts (defined with the harmonic sums); sources with
+// more modes than kTabModes evaluate Bessel functions per sample
 constexpr int kTabModes = 128;
-__device__ __forceinline__ int choose_terms(double qmax);
-__device__ __forceinline__ int choose_terms_f32(double qmax);
+__device__ __forceinline__ int taylor_terms_fp64(double q, int nmodes);
+__device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes);
 
 __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
   __shared__ double s_r[3][kSlots];
@@ -419,9 +420,9 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
         ec = spline4w(bv, d, sample_time(d, (c.start + last_f) / 2), w).e;
         const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
         if (ec > 1e-6) {
-          const double qmax = 2.0 * d.nmodes * de * (1.0 + de / ec);
-          k64 = choose_terms(qmax);
-          k32 = choose_terms_f32(qmax);
+          const double q = d.nmodes * (1.25 * de + 1e-15);  // bounds n |e - e_c| over the tile
+          k64 = taylor_terms_fp64(q, d.nmodes);
+          k32 = taylor_terms_fp32(q, d.nmodes);
         }
       }
       ts.ec = ec;
@@ -544,106 +545,169 @@ __device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double
   for (int m = 0; m < 5; ++m) J[m] = v[m] * inv;
 }
 
-// ------------------------------------------------------------------ per-tile Bessel table
-// Within a 1024-sample tile the eccentricity moves by ~1e-4 at most, so the
-// Bessel values at x = n e are obtained from values at the tile's central
-// eccentricity e_c through the multiplication theorem (DLMF 10.23.1):
-//   J_nu(lambda z) = lambda^nu sum_{k>=0} ((1 - lambda^2) z / 2)^k / k! J_{nu+k}(z),
-// z = n e_c, lambda = e / e_c.  Row n of the table holds J_{b+m}(n e_c) for
-// m = 0 .. 4 + K, b = n - 2 (b = -1 for n = 1, with J_{-1} = -J_1).
-constexpr int kKMax = 12;
-constexpr int kTabStride = 5 + kKMax;
+// ------------------------------------------------------------------ per-tile Taylor table
+// Within a 1024-sample tile the eccentricity moves by ~1e-4 at most.  The
+// Peters-Mathews combinations of one harmonic,
+//   A_n(e) = n [J_{n-2} - 2e J_{n-1} + (2/n) J_n + 2e J_{n+1} - J_{n+2}](n e),
+//   B_n(e) = n [J_{n-2} - 2 J_n + J_{n+2}](n e),      C_n(e) = J_n(n e),
+// are therefore tabulated per tile as Taylor polynomials in delta = e - e_c
+// about the tile's central eccentricity e_c, so that a sample evaluates each
+// with K fused multiply-adds.  The coefficients follow from
+//   J_nu(n (e_c + delta)) = sum_k (n delta)^k / k! J_nu^(k)(n e_c),
+//   J_nu^(k)(x) = 2^-k sum_j (-1)^j C(k, j) J_{nu-k+2j}(x)     (DLMF 10.6.7),
+// with the J values of one row from a Miller backward recurrence (or the
+// power series below x = 1), and the 2e factors of A_n expanded exactly.
+// Row n holds [A_0 .. A_K | B_0 .. B_K | C_0 .. C_K].
+constexpr int kTaylorMax64 = 10;                          // FP64 terms at most
+constexpr int kTaylorMax32 = 6;                           // FP32 terms at most
+constexpr int kRowD = (3 * (kTaylorMax64 + 1) + 1) / 2 * 2;  // doubles per FP64 row (34)
+constexpr int kRowF = (3 * (kTaylorMax32 + 1) + 3) / 4 * 4;  // floats per FP32 row (24)
+constexpr int kWin5 = 2 * kTaylorMax64 + 5;               // J orders a row needs
 
-// one row of the table, built by one thread (x = n e_c > 0)
-__device__ void build_bessel_row(double *Tn, int n, double x, int K, int start) {
-  const int b = (n == 1) ? -1 : n - 2;
-  const int lo = max(b, 0), hi = b + 4 + K;
+// J_m(x) for m = mlo .. mhi (x >= 0) into J[m - mlo].
+__device__ void bessel_window(double x, int mlo, int mhi, int start, double *J) {
   if (x < 1.0) {
+    if (x <= 0.0) {
+      for (int m = mlo; m <= mhi; ++m) J[m - mlo] = (m == 0) ? 1.0 : 0.0;
+      return;
+    }
     const double hx = 0.5 * x, q = -hx * hx;
-    double pref = exp((double)lo * log(hx) - lgamma((double)lo + 1.0));
-    for (int nu = lo; nu <= hi; ++nu) {
+    double pref = exp((double)mlo * log(hx) - lgamma((double)mlo + 1.0));
+    for (int nu = mlo; nu <= mhi; ++nu) {
       double term = 1.0, sum = 1.0;
       for (int k = 1; k < 16; ++k) {
         term *= q / ((double)k * ((double)nu + (double)k));
         sum += term;
       }
-      Tn[nu - b] = pref * sum;
+      J[nu - mlo] = pref * sum;
       pref *= hx / ((double)nu + 1.0);
     }
-  } else {
-    const double tx = 2.0 / x;
-    int k = max(start, hi + 8);
-    if (k & 1) ++k;
-    double jk = 1.0e-280, jk1 = 0.0, sum = 2.0 * jk, w = 0.0;
-    for (; k > 0; --k) {
-      const double jm = (double)k * tx * jk - jk1;  // order k - 1
-      jk1 = jk;
-      jk = jm;
-      sum = fma(w, jm, sum);
-      w = 2.0 - w;
-      const int ord = k - 1;
-      if (ord >= lo && ord <= hi) Tn[ord - b] = jm;
-      if (fabs(jm) > 1.0e250) {  // rescale everything produced so far
-        jk *= 1.0e-250;
-        jk1 *= 1.0e-250;
-        sum *= 1.0e-250;
-        for (int o = max(ord, lo); o <= hi; ++o) Tn[o - b] *= 1.0e-250;
-      }
-    }
-    sum -= jk;  // J_0 was added with weight 2; count it once
-    const double inv = 1.0 / sum;
-    for (int o = lo; o <= hi; ++o) Tn[o - b] *= inv;
+    return;
   }
-  if (n == 1) Tn[0] = -Tn[2];
+  const double tx = 2.0 / x;
+  int k = max(start, mhi + 8);
+  if (k & 1) ++k;
+  double jk = 1.0e-280, jk1 = 0.0, sum = 2.0 * jk, w = 0.0;
+  for (; k > 0; --k) {
+    const double jm = (double)k * tx * jk - jk1;  // order k - 1
+    jk1 = jk;
+    jk = jm;
+    sum = fma(w, jm, sum);
+    w = 2.0 - w;
+    const int ord = k - 1;
+    if (ord >= mlo && ord <= mhi) J[ord - mlo] = jm;
+    if (fabs(jm) > 1.0e250) {  // rescale everything produced so far
+      jk *= 1.0e-250;
+      jk1 *= 1.0e-250;
+      sum *= 1.0e-250;
+      for (int o = max(ord, mlo); o <= mhi; ++o) J[o - mlo] *= 1.0e-250;
+    }
+  }
+  sum -= jk;  // J_0 was added with weight 2; count it once
+  const double inv = 1.0 / sum;
+  for (int o = mlo; o <= mhi; ++o) J[o - mlo] *= inv;
 }
 
-// Number of multiplication-theorem terms for a tile where |(1-lambda^2) z/2|
-// stays below qmax (tail < 1e-17 of the largest J); 0 = use per-sample Miller.
-__device__ __forceinline__ int choose_terms(double qmax) {
-  if (qmax <= 1e-3) return 4;
-  if (qmax <= 1e-2) return 6;
-  if (qmax <= 5e-2) return 8;
-  if (qmax <= 2e-1) return 12;
+// One table row (harmonic n, K + 1 terms), built by one thread in FP64.
+template <typename T>
+__device__ void build_taylor_row(T *row, int n, double ec, int K, int start) {
+  const int mlo = max(0, n - 2 - K), mhi = n + 2 + K;
+  double Jw[kWin5];
+  bessel_window(n * ec, mlo, mhi, start, Jw);
+  double prev[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  double fac = 1.0;  // (n / 2)^k / k!
+  const double dn = (double)n;
+  for (int k = 0; k <= K; ++k) {
+    if (k > 0) fac *= 0.5 * dn / (double)k;
+    double c[5];
+    for (int v = 0; v < 5; ++v) {
+      const int nu = n - 2 + v;
+      double s = 0.0, binom = 1.0;
+      for (int j = 0; j <= k; ++j) {
+        const int m = nu - k + 2 * j;
+        const double Jm = (m >= 0) ? Jw[m - mlo] : (((-m) & 1) ? -Jw[-m - mlo] : Jw[-m - mlo]);
+        s += (j & 1) ? -binom * Jm : binom * Jm;
+        binom = binom * (double)(k - j) / (double)(j + 1);
+      }
+      c[v] = fac * s;  // delta^k coefficient of J_nu(n e)
+    }
+    const double A = dn * (c[0] - 2.0 * ec * c[1] - 2.0 * prev[1] + (2.0 / dn) * c[2] + 2.0 * ec * c[3] +
+                           2.0 * prev[3] - c[4]);
+    const double B = dn * (c[0] - 2.0 * c[2] + c[4]);
+    row[k] = (T)A;
+    row[K + 1 + k] = (T)B;
+    row[2 * (K + 1) + k] = (T)c[2];
+    for (int v = 0; v < 5; ++v) prev[v] = c[v];
+  }
+}
+
+// Terms for a tile where n |delta| <= q: the remainder of A_n, B_n, C_n is
+// below 8 nmodes q^(K+1) / (K+1)! e^q (|J^(k)| <= 1); 0 = per-sample Miller.
+__device__ __forceinline__ double taylor_tail(double q, int nmodes, int K) {
+  double t = 8.0 * nmodes * exp(q);
+  for (int k = 1; k <= K + 1; ++k) t *= q / (double)k;
+  return t;
+}
+__device__ __forceinline__ int taylor_terms_fp64(double q, int nmodes) {
+  if (!(q <= 1.0)) return 0;
+  const int opts[5] = {4, 5, 6, 8, 10};
+  for (int i = 0; i < 5; ++i)
+    if (taylor_tail(q, nmodes, opts[i]) < 1e-17) return opts[i];
+  return 0;
+}
+__device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes) {
+  if (!(q <= 1.0)) return 0;
+  const int opts[4] = {2, 3, 4, 6};
+  for (int i = 0; i < 4; ++i)
+    if (taylor_tail(q, nmodes, opts[i]) < 1e-9) return opts[i];
   return 0;
 }
 
-// Mode sums Sa, Sb, Sc (see harmonic_sum_fp64) from the tile table.
-template <int K>
-__device__ __forceinline__ void mode_sums_table(const double *T, int nmodes, double e, double ec, double c1, double s1,
-                                                double cD, double sD, double &Sa, double &Sb, double &Sc) {
-  const double lam = e / ec;
-  const double half_dl = (1.0 - lam) * (1.0 + lam) * ec * 0.5;  // (1 - lambda^2) e_c / 2
-  double p = 1.0 / lam;                                         // lambda^b, b = -1 for n = 1
-  double zr = 1.0, zi = 0.0;
-  double sa = 0.0, sb = 0.0, sc = 0.0;
-#pragma unroll 1
+// Mode sums Sa = sum A_n cos(n Phi'), Sb = sum B_n sin(n Phi'), Sc = sum C_n
+// cos(n Phi') from the tile table at delta = e - e_c, with the harmonic
+// phases from the rotation recurrence z_n = z_1^n z_D.
+template <int K, typename T>
+__device__ __forceinline__ void mode_sums_taylor(const T *tab, int nmodes, int stride, T dl, T c1, T s1, T cD, T sD,
+                                                 T &Sa, T &Sb, T &Sc) {
+  constexpr int NV = 3 * (K + 1);
+  T zr = T(1), zi = T(0), sa = T(0), sb = T(0), sc = T(0);
+#pragma unroll 2
   for (int n = 1; n <= nmodes; ++n) {
-    const double *Tn = T + (n - 1) * kTabStride;
-    const double c = (double)n * half_dl;
-    double w[K + 1];
-    w[0] = 1.0;
+    T v[(sizeof(T) == 4) ? (NV + 3) / 4 * 4 : (NV + 1) / 2 * 2];
+    if constexpr (sizeof(T) == 4) {
+      const float4 *r4 = reinterpret_cast<const float4 *>(tab + (n - 1) * stride);
 #pragma unroll
-    for (int k = 1; k <= K; ++k) w[k] = w[k - 1] * c * (1.0 / (double)k);
-    double J[5];
-    double pj = p;
+      for (int i = 0; i < (NV + 3) / 4; ++i) {
+        const float4 q = r4[i];
+        v[4 * i] = q.x;
+        v[4 * i + 1] = q.y;
+        v[4 * i + 2] = q.z;
+        v[4 * i + 3] = q.w;
+      }
+    } else {
+      const double2 *r2 = reinterpret_cast<const double2 *>(tab + (n - 1) * stride);
 #pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      double s = w[K] * Tn[j + K];
-#pragma unroll
-      for (int k = K - 1; k >= 0; --k) s = fma(w[k], Tn[j + k], s);
-      J[j] = pj * s;
-      pj *= lam;
+      for (int i = 0; i < (NV + 1) / 2; ++i) {
+        const double2 q = r2[i];
+        v[2 * i] = q.x;
+        v[2 * i + 1] = q.y;
+      }
     }
-    p *= lam;
-    const double tr = zr * c1 - zi * s1;
-    zi = zr * s1 + zi * c1;
+    T A = v[K], B = v[2 * K + 1], C = v[3 * K + 2];
+#pragma unroll
+    for (int k = K - 1; k >= 0; --k) {
+      A = fma(A, dl, v[k]);
+      B = fma(B, dl, v[K + 1 + k]);
+      C = fma(C, dl, v[2 * (K + 1) + k]);
+    }
+    const T tr = zr * c1 - zi * s1;
+    zi = fma(zr, s1, zi * c1);
     zr = tr;
-    const double cn = zr * cD - zi * sD;
-    const double sn = zi * cD + zr * sD;
-    const double dn = (double)n;
-    sa += dn * (J[0] - 2. * e * J[1] + 2. / dn * J[2] + 2. * e * J[3] - J[4]) * cn;
-    sb += dn * (J[0] - 2. * J[2] + J[4]) * sn;
-    sc += J[2] * cn;
+    const T cn = zr * cD - zi * sD;
+    const T sn = fma(zi, cD, zr * sD);
+    sa = fma(A, cn, sa);
+    sb = fma(B, sn, sb);
+    sc = fma(C, cn, sc);
   }
   Sa = sa;
   Sb = sb;
@@ -693,116 +757,141 @@ __device__ void mode_sums_miller(const int32_t *bstart, int nmodes, double e, do
 // Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
 // rotation and antenna factors applied once per sample.  The Bessel values
 // come from the tile table (K > 0) or a per-sample recurrence (K == 0).
-__device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, const double *T, double ec, int K,
-                                  double t, double e, double om_M, double gim, double Phi, double alp, double nu,
-                                  double gimdot, double &hI, double &hII) {
-  const double cosalp = cos(alp), sinalp = sin(alp);
-  const double cosqL = d.cosqK * d.coslam + d.sinqK * d.sinlam * cosalp;
-  const double sinqL = sqrt(1. - cosqL * cosqL);
-  const double phiLup = d.sinqK * d.sinphiK * d.coslam - d.cosphiK * d.sinlam * sinalp - d.cosqK * d.sinphiK * d.sinlam * cosalp;
-  const double phiLdown = d.sinqK * d.cosphiK * d.coslam + d.sinphiK * d.sinlam * sinalp - d.cosqK * d.cosphiK * d.sinlam * cosalp;
-  const double phiL = atan2(phiLup, phiLdown);
-  const double Ldotn = cosqL * d.cosqS + sinqL * d.sinqS * cos(phiL - d.phiS);
-  const double Ldotn2 = Ldotn * Ldotn;
-  const double Sdotn = d.cosqK * d.cosqS + d.sinqK * d.sinqS * cos(d.phiK - d.phiS);
-  const double betaup = -Sdotn + d.coslam * Ldotn;
-  const double betadown = d.sinqS * sin(d.phiK - d.phiS) * d.sinlam * cosalp + (d.cosqK * Sdotn - d.cosqS) / d.sinqK * d.sinlam * sinalp;
-  const double beta = atan2(betaup, betadown);
-  double sin2gam, cos2gam;
-  sincos(2. * (gim + beta), &sin2gam, &cos2gam);
+// cos 2 atan2(y, x) and sin 2 atan2(y, x) without the angle (atan2(0, 0) = 0)
+template <typename T>
+__device__ __forceinline__ void double_angle(T y, T x, T &c2, T &s2) {
+  const T r2 = x * x + y * y;
+  if (r2 > T(0)) {
+    const T inv = T(1) / r2;
+    c2 = (x * x - y * y) * inv;
+    s2 = T(2) * x * y * inv;
+  } else {
+    c2 = T(1);
+    s2 = T(0);
+  }
+}
 
-  double cosorbphs = 0.0, FplusI, FcrosI, FplusII, FcrosII, Kresp;
+// Response and orientation factors of one sample (AAK.cc:425-478 with the
+// NK-frame rotation of KSParMap.cc:532-574), from the per-source constants of
+// SourceDesc and the sample's (cos alpha, sin alpha), (cos 2 gamma~, sin 2 gamma~)
+// and orbital phase (cos, sin).  The angles the reference forms with atan2
+// (phi_L, beta, the LISA phi and psi) enter only through cos/sin of them or
+// of twice them, which follow from the atan2 arguments algebraically.
+// Output: the coefficients of Sa, Sb, Sc in h_I and h_II.
+template <typename T>
+struct Resp {
+  T caI, cbI, ccI, caII, cbII, ccII;
+  T cosorb_S;  // cos(orbital phase - phi_S), for the Doppler term
+};
+
+template <typename T>
+__device__ __forceinline__ Resp<T> response(const SourceDesc &d, T ca, T sa, T c2g, T s2g, T co, T so) {
+  const T L0 = (T)d.Lc[0] + sa * (T)d.Ls[0] + ca * (T)d.Lq[0];
+  const T L1 = (T)d.Lc[1] + sa * (T)d.Ls[1] + ca * (T)d.Lq[1];
+  const T L2 = (T)d.Lc[2] + ca * (T)d.Lq[2];
+  const T n0 = (T)d.nv[0], n1 = (T)d.nv[1], n2 = (T)d.nv[2];
+  const T Ldotn = L0 * n0 + L1 * n1 + L2 * n2;
+  const T Ldotn2 = Ldotn * Ldotn;
+  const T Sdotn = (T)d.Sdotn;
+  // gamma = 2 (gamma~ + beta), beta = atan2(-S.n + cos(lambda) L.n, beta_c cos(alpha) + beta_s sin(alpha))
+  T c2b, s2b;
+  double_angle<T>(-Sdotn + (T)d.coslam * Ldotn, (T)d.beta_c * ca + (T)d.beta_s * sa, c2b, s2b);
+  const T cos2gam = c2g * c2b - s2g * s2b, sin2gam = s2g * c2b + c2g * s2b;
+
+  T FplusI, FcrosI, FplusII, FcrosII, Kr;
+  T cosorb_S = T(0);
   if (d.mich) {
-    const double orbphs = kTwoPi * t / kYear;
-    double sinorbphs;
-    sincos(orbphs - d.phiS, &sinorbphs, &cosorbphs);
-    const double cosq = .5 * d.cosqS - kHalfSqrt3 * d.sinqS * cosorbphs;
-    const double phiw = orbphs + atan2(kHalfSqrt3 * d.cosqS + .5 * d.sinqS * cosorbphs, d.sinqS * sinorbphs);
-    const double psiup = .5 * d.cosqK - kHalfSqrt3 * d.sinqK * cos(orbphs - d.phiK) - cosq * Sdotn;
-    double so, co;
-    sincos(orbphs, &so, &co);
-    const double psidown = .5 * d.sinqK * d.sinqS * sin(d.phiK - d.phiS) -
-                           kHalfSqrt3 * co * (d.cosqK * d.sinqS * sin(d.phiS) - d.cosqS * d.sinqK * sin(d.phiK)) -
-                           kHalfSqrt3 * so * (d.cosqS * d.sinqK * cos(d.phiK) - d.cosqK * d.sinqS * cos(d.phiS));
-    const double psi = atan2(psiup, psidown);
-    const double cosq1 = .5 * (1. + cosq * cosq);
-    double sin2phi, cos2phi, sin2psi, cos2psi;
-    sincos(2. * phiw, &sin2phi, &cos2phi);
-    sincos(2. * psi, &sin2psi, &cos2psi);
+    const T hs3 = (T)kHalfSqrt3;
+    const T cS = (T)d.cosqS, sS = (T)d.sinqS, cK = (T)d.cosqK, sK = (T)d.sinqK;
+    cosorb_S = co * (T)d.cphiS + so * (T)d.sphiS;
+    const T sinorb_S = so * (T)d.cphiS - co * (T)d.sphiS;
+    const T cosorb_K = co * (T)d.cosphiK + so * (T)d.sinphiK;
+    const T cosq = T(.5) * cS - hs3 * sS * cosorb_S;
+    // 2 phi_w = 2 orb + 2 atan2(hs3 cos qS + sin qS cos(orb - phiS) / 2, sin qS sin(orb - phiS))
+    T c2w, s2w;
+    double_angle<T>(hs3 * cS + T(.5) * sS * cosorb_S, sS * sinorb_S, c2w, s2w);
+    const T c2o = co * co - so * so, s2o = T(2) * so * co;
+    const T cos2phi = c2o * c2w - s2o * s2w, sin2phi = s2o * c2w + c2o * s2w;
+    T cos2psi, sin2psi;
+    double_angle<T>(T(.5) * cK - hs3 * sK * cosorb_K - cosq * Sdotn, (T)d.psd0 - (T)d.psd1 * co - (T)d.psd2 * so,
+                    cos2psi, sin2psi);
+    const T cosq1 = T(.5) * (T(1) + cosq * cosq);
     FplusI = cosq1 * cos2phi * cos2psi - cosq * sin2phi * sin2psi;
     FcrosI = cosq1 * cos2phi * sin2psi + cosq * sin2phi * cos2psi;
     FplusII = cosq1 * sin2phi * cos2psi + cosq * cos2phi * sin2psi;
     FcrosII = cosq1 * sin2phi * sin2psi - cosq * cos2phi * cos2psi;
-    Kresp = kHalfSqrt3;
+    Kr = hs3;
   } else {
-    const double up_ldc = d.cosqS * d.sinqK * cos(d.phiS - d.phiK) - d.cosqK * d.sinqS;
-    const double dw_ldc = d.sinqK * sin(d.phiS - d.phiK);
-    const double psi_ldc = (dw_ldc != 0.0) ? -atan2(up_ldc, dw_ldc) : 0.5 * kPi;
-    double s2, c2;
-    sincos(2. * psi_ldc, &s2, &c2);
-    FplusI = c2;
-    FcrosI = -s2;
-    FplusII = s2;
-    FcrosII = c2;
-    Kresp = 1.0;
+    FplusI = (T)d.F0[0];
+    FcrosI = (T)d.F0[1];
+    FplusII = (T)d.F0[2];
+    FcrosII = (T)d.F0[3];
+    Kr = T(1);
   }
-  const double Amp = pow(om_M, 2. / 3.) * d.zeta;
+  // rotation to the NK wave frame: rot = [r0, r1, -r1, r0]
+  const T nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
+  const T S0 = (T)d.Sv[0], S1 = (T)d.Sv[1], S2 = (T)d.Sv[2];
+  const T nS0 = (T)d.nxS[0], nS1 = (T)d.nxS[1], nS2 = (T)d.nxS[2];
+  const T norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * (T)d.nxS_norm;
+  const T cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
+  const T sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
+  const T r0 = T(2) * cosrot * cosrot - T(1), r1 = cosrot * sinrot;
+  const T uI = FplusI * r0 - FcrosI * r1, wI = FplusI * r1 + FcrosI * r0;
+  const T uII = FplusII * r0 - FcrosII * r1, wII = FplusII * r1 + FcrosII * r0;
+  const T opL2 = T(1) + Ldotn2, omL2 = T(1) - Ldotn2, twoL = T(2) * Ldotn;
+  Resp<T> R;
+  R.caI = Kr * (-uI * opL2 * cos2gam + wI * twoL * sin2gam);
+  R.cbI = Kr * (uI * opL2 * sin2gam + wI * twoL * cos2gam);
+  R.ccI = Kr * uI * omL2;
+  R.caII = Kr * (-uII * opL2 * cos2gam + wII * twoL * sin2gam);
+  R.cbII = Kr * (uII * opL2 * sin2gam + wII * twoL * cos2gam);
+  R.ccII = Kr * uII * omL2;
+  R.cosorb_S = cosorb_S;
+  return R;
+}
 
-  // rotation to the NK wave frame (RotCoeff, KSParMap.cc:532-574): depends on alpha only
-  double rot0, rot1;
-  {
-    const double sqS = d.sinqS, cqS = d.cosqS;
-    const double n0 = sqS * cos(d.phiS), n1 = sqS * sin(d.phiS), n2 = cqS;
-    const double S0 = d.sinqK * d.cosphiK, S1 = d.sinqK * d.sinphiK, S2 = d.cosqK;
-    const double L0 = d.coslam * d.sinqK * d.cosphiK + d.sinlam * (sinalp * d.sinphiK - cosalp * d.cosqK * d.cosphiK);
-    const double L1 = d.coslam * d.sinqK * d.sinphiK - d.sinlam * (sinalp * d.cosphiK + cosalp * d.cosqK * d.sinphiK);
-    const double L2 = d.coslam * d.cosqK + d.sinlam * cosalp * d.sinqK;
-    const double nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
-    const double nS0 = n1 * S2 - n2 * S1, nS1 = n2 * S0 - n0 * S2, nS2 = n0 * S1 - n1 * S0;
-    const double norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * sqrt(nS0 * nS0 + nS1 * nS1 + nS2 * nS2);
-    const double cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
-    const double sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
-    rot0 = 2. * cosrot * cosrot - 1.;
-    rot1 = cosrot * sinrot;
-  }
-  // rot = [rot0, rot1, -rot1, rot0]
-  const double uI = FplusI * rot0 - FcrosI * rot1, wI = FplusI * rot1 + FcrosI * rot0;
-  const double uII = FplusII * rot0 - FcrosII * rot1, wII = FplusII * rot1 + FcrosII * rot0;
-  const double opL2 = 1. + Ldotn2, omL2 = 1. - Ldotn2, twoL = 2. * Ldotn;
-  const double caI = Kresp * (-uI * opL2 * cos2gam + wI * twoL * sin2gam);
-  const double cbI = Kresp * (uI * opL2 * sin2gam + wI * twoL * cos2gam);
-  const double ccI = Kresp * uI * omL2;
-  const double caII = Kresp * (-uII * opL2 * cos2gam + wII * twoL * sin2gam);
-  const double cbII = Kresp * (uII * opL2 * sin2gam + wII * twoL * cos2gam);
-  const double ccII = Kresp * uII * omL2;
+// h_I, h_II at one sample (AAK.cc:409-528) with the modes accumulated as
+// Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
+// rotation and antenna factors applied once per sample.  The Bessel values
+// come from the tile table (K > 0) or a per-sample recurrence (K == 0).
+__device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, const double *tab, double ec, int K,
+                                  double t, double e, double om_M, double gim, double Phi, double alp, double nu,
+                                  double gimdot, double &hI, double &hII) {
+  double sa, ca, s2g, c2g, so = 0.0, co = 1.0;
+  sincos(alp, &sa, &ca);
+  sincos(2. * gim, &s2g, &c2g);
+  if (d.mich) sincos(kTwoPi * t / kYear, &so, &co);
+  const Resp<double> R = response<double>(d, ca, sa, c2g, s2g, co, so);
+  const double Amp = pow(om_M, 2. / 3.) * d.zeta;
 
   // harmonic phases: n Phi + Doppler_n = n (Phi + D1) + D0
   double D1 = 0.0, D0 = 0.0;
   if (d.mich) {
-    D1 = kTwoPi * nu * kAUsec * d.sinqS * cosorbphs;
-    D0 = 2.0 * gimdot * kAUsec * d.sinqS * cosorbphs;
+    D1 = kTwoPi * nu * kAUsec * d.sinqS * R.cosorb_S;
+    D0 = 2.0 * gimdot * kAUsec * d.sinqS * R.cosorb_S;
   }
   double s1, c1, sD, cD;
   sincos(Phi + D1, &s1, &c1);  // harmonic n: (c1 + i s1)^n (cD + i sD)
   sincos(D0, &sD, &cD);
   const double se = sqrt(1. - e * e);
   double Sa, Sb, Sc;
+  const double dl = e - ec;
   switch (K) {
-    case 4: mode_sums_table<4>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 6: mode_sums_table<6>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 8: mode_sums_table<8>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 12: mode_sums_table<12>(T, d.nmodes, e, ec, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 4: mode_sums_taylor<4, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 5: mode_sums_taylor<5, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 6: mode_sums_taylor<6, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 8: mode_sums_taylor<8, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+    case 10: mode_sums_taylor<10, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
     default: mode_sums_miller(bstart, d.nmodes, e, c1, s1, cD, sD, Sa, Sb, Sc); break;
   }
   const double a = -Amp * Sa, b = -Amp * se * Sb, cc = 2. * Amp * Sc;
-  hI = caI * a + cbI * b + ccI * cc;
-  hII = caII * a + cbII * b + ccII * cc;
+  hI = R.caI * a + R.cbI * b + R.ccI * cc;
+  hII = R.caII * a + R.cbII * b + R.ccII * cc;
 }
 
 // ------------------------------------------------------------------ split precision
 // FP64: spline, rates, phase sums and every angle reduction; FP32: geometry,
 // antenna response, Bessel evaluation and the harmonic recurrence.
-constexpr int kTabStrideF = 16;  // floats per FP32 table row (rows padded to 64 B)
 
 // x mod 2pi in [-pi, pi], two-term Cody-Waite reduction in FP64, returned as float
 __device__ __forceinline__ float reduce_2pi_f(double x) {
@@ -811,178 +900,49 @@ __device__ __forceinline__ float reduce_2pi_f(double x) {
   return (float)r;
 }
 
-__device__ __forceinline__ int choose_terms_f32(double qmax) {
-  if (qmax <= 3e-3) return 3;
-  if (qmax <= 2e-2) return 4;
-  if (qmax <= 1e-1) return 6;
-  if (qmax <= 3e-1) return 8;
-  return 0;
-}
-
-template <int K>
-__device__ __forceinline__ void mode_sums_table_f32(const float *Tf, int nmodes, float e, float lp, float half_dl,
-                                                    float c1, float s1, float cD, float sD, float &Sa, float &Sb,
-                                                    float &Sc) {
-  const float lam = exp2f(lp);
-  float zr = 1.f, zi = 0.f;
-  float sa = 0.f, sb = 0.f, sc = 0.f;
-#pragma unroll 2
-  for (int n = 1; n <= nmodes; ++n) {
-    const float4 *row = reinterpret_cast<const float4 *>(Tf + (n - 1) * kTabStrideF);
-    float T[16];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const float4 x = row[v];
-      T[4 * v] = x.x;
-      T[4 * v + 1] = x.y;
-      T[4 * v + 2] = x.z;
-      T[4 * v + 3] = x.w;
-    }
-    const float c = (float)n * half_dl;
-    float w[K + 1];
-    w[0] = 1.f;
-#pragma unroll
-    for (int k = 1; k <= K; ++k) w[k] = w[k - 1] * c * (1.f / (float)k);
-    float pj = exp2f((float)((n == 1) ? -1 : n - 2) * lp);  // lambda^b
-    float J[5];
-#pragma unroll
-    for (int j = 0; j < 5; ++j) {
-      float s = w[K] * T[j + K];
-#pragma unroll
-      for (int k = K - 1; k >= 0; --k) s = fmaf(w[k], T[j + k], s);
-      J[j] = pj * s;
-      pj *= lam;
-    }
-    const float tr = zr * c1 - zi * s1;
-    zi = fmaf(zr, s1, zi * c1);
-    zr = tr;
-    const float cn = zr * cD - zi * sD;
-    const float sn = fmaf(zi, cD, zr * sD);
-    const float dn = (float)n;
-    sa += dn * (J[0] - 2.f * e * J[1] + 2.f / dn * J[2] + 2.f * e * J[3] - J[4]) * cn;
-    sb += dn * (J[0] - 2.f * J[2] + J[4]) * sn;
-    sc += J[2] * cn;
-  }
-  Sa = sa;
-  Sb = sb;
-  Sc = sc;
-}
-
-// h_I, h_II at one sample in split precision (same algebra as harmonic_sum_fp64).
-__device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, const float *Tf, double ec, int K,
+// h_I, h_II at one sample in split precision: the angle reductions in FP64,
+// the trigonometry, response and harmonic sums in FP32 (same algebra as
+// harmonic_sum_fp64).
+__device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, const float *tab, double ec, int K,
                                    double t, double e_d, double om_M, double gim, double Phi, double alp, double nu,
                                    double gimdot, double &hI, double &hII) {
-  const float coslam = (float)d.coslam, sinlam = (float)d.sinlam;
-  const float cosqS = (float)d.cosqS, sinqS = (float)d.sinqS, cosqK = (float)d.cosqK, sinqK = (float)d.sinqK;
-  const float cosphiK = (float)d.cosphiK, sinphiK = (float)d.sinphiK;
-  const float phiS = (float)d.phiS, phiK = (float)d.phiK;
-  float sinalp, cosalp;
-  sincosf(reduce_2pi_f(alp), &sinalp, &cosalp);
-  const float cosqL = cosqK * coslam + sinqK * sinlam * cosalp;
-  const float sinqL = sqrtf(fmaxf(1.f - cosqL * cosqL, 0.f));
-  const float phiLup = sinqK * sinphiK * coslam - cosphiK * sinlam * sinalp - cosqK * sinphiK * sinlam * cosalp;
-  const float phiLdown = sinqK * cosphiK * coslam + sinphiK * sinlam * sinalp - cosqK * cosphiK * sinlam * cosalp;
-  const float phiL = atan2f(phiLup, phiLdown);
-  const float Ldotn = cosqL * cosqS + sinqL * sinqS * cosf(phiL - phiS);
-  const float Ldotn2 = Ldotn * Ldotn;
-  const float Sdotn = cosqK * cosqS + sinqK * sinqS * cosf(phiK - phiS);
-  const float betaup = -Sdotn + coslam * Ldotn;
-  const float betadown = sinqS * sinf(phiK - phiS) * sinlam * cosalp + (cosqK * Sdotn - cosqS) / sinqK * sinlam * sinalp;
-  const float beta = atan2f(betaup, betadown);
-  float sin2gam, cos2gam;
-  sincosf(2.f * (reduce_2pi_f(gim) + beta), &sin2gam, &cos2gam);
-
-  float cosorbphs = 0.f, FplusI, FcrosI, FplusII, FcrosII, Kresp;
-  const float hs3 = (float)kHalfSqrt3;
-  if (d.mich) {
-    const double orbd = kTwoPi * t / kYear;
-    const float orbphs = reduce_2pi_f(orbd);
-    float sinorbphs;
-    sincosf(reduce_2pi_f(orbd - d.phiS), &sinorbphs, &cosorbphs);
-    const float cosq = .5f * cosqS - hs3 * sinqS * cosorbphs;
-    const float phiw = orbphs + atan2f(hs3 * cosqS + .5f * sinqS * cosorbphs, sinqS * sinorbphs);
-    const float psiup = .5f * cosqK - hs3 * sinqK * cosf(reduce_2pi_f(orbd - d.phiK)) - cosq * Sdotn;
-    float so, co;
-    sincosf(orbphs, &so, &co);
-    const float psidown = .5f * sinqK * sinqS * sinf(phiK - phiS) -
-                          hs3 * co * (cosqK * sinqS * sinf(phiS) - cosqS * sinqK * sinf(phiK)) -
-                          hs3 * so * (cosqS * sinqK * cosf(phiK) - cosqK * sinqS * cosf(phiS));
-    const float psi = atan2f(psiup, psidown);
-    const float cosq1 = .5f * (1.f + cosq * cosq);
-    float sin2phi, cos2phi, sin2psi, cos2psi;
-    sincosf(2.f * phiw, &sin2phi, &cos2phi);
-    sincosf(2.f * psi, &sin2psi, &cos2psi);
-    FplusI = cosq1 * cos2phi * cos2psi - cosq * sin2phi * sin2psi;
-    FcrosI = cosq1 * cos2phi * sin2psi + cosq * sin2phi * cos2psi;
-    FplusII = cosq1 * sin2phi * cos2psi + cosq * cos2phi * sin2psi;
-    FcrosII = cosq1 * sin2phi * sin2psi - cosq * cos2phi * cos2psi;
-    Kresp = hs3;
-  } else {
-    const float up_ldc = cosqS * sinqK * cosf(phiS - phiK) - cosqK * sinqS;
-    const float dw_ldc = sinqK * sinf(phiS - phiK);
-    const float psi_ldc = (dw_ldc != 0.f) ? -atan2f(up_ldc, dw_ldc) : 0.5f * (float)kPi;
-    float s2, c2;
-    sincosf(2.f * psi_ldc, &s2, &c2);
-    FplusI = c2;
-    FcrosI = -s2;
-    FplusII = s2;
-    FcrosII = c2;
-    Kresp = 1.f;
-  }
-  const float Amp = powf((float)om_M, 2.f / 3.f) * (float)d.zeta;
-  float rot0, rot1;
-  {
-    const float n0 = sinqS * cosf(phiS), n1 = sinqS * sinf(phiS), n2 = cosqS;
-    const float S0 = sinqK * cosphiK, S1 = sinqK * sinphiK, S2 = cosqK;
-    const float L0 = coslam * sinqK * cosphiK + sinlam * (sinalp * sinphiK - cosalp * cosqK * cosphiK);
-    const float L1 = coslam * sinqK * sinphiK - sinlam * (sinalp * cosphiK + cosalp * cosqK * sinphiK);
-    const float L2 = coslam * cosqK + sinlam * cosalp * sinqK;
-    const float nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
-    const float nS0 = n1 * S2 - n2 * S1, nS1 = n2 * S0 - n0 * S2, nS2 = n0 * S1 - n1 * S0;
-    const float norm = sqrtf(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * sqrtf(nS0 * nS0 + nS1 * nS1 + nS2 * nS2);
-    const float cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
-    const float sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
-    rot0 = 2.f * cosrot * cosrot - 1.f;
-    rot1 = cosrot * sinrot;
-  }
-  const float uI = FplusI * rot0 - FcrosI * rot1, wI = FplusI * rot1 + FcrosI * rot0;
-  const float uII = FplusII * rot0 - FcrosII * rot1, wII = FplusII * rot1 + FcrosII * rot0;
-  const float opL2 = 1.f + Ldotn2, omL2 = 1.f - Ldotn2, twoL = 2.f * Ldotn;
+  float sa, ca, s2g, c2g, so = 0.f, co = 1.f;
+  __sincosf(reduce_2pi_f(alp), &sa, &ca);
+  __sincosf(reduce_2pi_f(2.0 * gim), &s2g, &c2g);
+  if (d.mich) __sincosf(reduce_2pi_f(kTwoPi * t / kYear), &so, &co);
+  const Resp<float> R = response<float>(d, ca, sa, c2g, s2g, co, so);
+  const float Amp = exp2f((2.f / 3.f) * __log2f((float)om_M)) * (float)d.zeta;
   // harmonic phases: n (Phi + D1) + D0, reduced in FP64
   double D1 = 0.0;
   float D0 = 0.f;
   if (d.mich) {
-    D1 = kTwoPi * nu * kAUsec * d.sinqS * (double)cosorbphs;
-    D0 = (float)(2.0 * gimdot * kAUsec) * sinqS * cosorbphs;
+    D1 = kTwoPi * nu * kAUsec * d.sinqS * (double)R.cosorb_S;
+    D0 = (float)(2.0 * gimdot * kAUsec * d.sinqS) * R.cosorb_S;
   }
   float s1, c1, sD, cD;
-  sincosf(reduce_2pi_f(Phi + D1), &s1, &c1);
-  sincosf(D0, &sD, &cD);
+  __sincosf(reduce_2pi_f(Phi + D1), &s1, &c1);
+  __sincosf(D0, &sD, &cD);
   const float e = (float)e_d;
   float Sa, Sb, Sc;
   if (K > 0) {
-    const double del = (e_d - ec) / ec;
-    const float lp = (float)(log1p(del) * 1.4426950408889634);
-    const float half_dl = (float)(-del * (2.0 + del) * ec * 0.5);
+    const float dl = (float)(e_d - ec);
     switch (K) {
-      case 3: mode_sums_table_f32<3>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-      case 4: mode_sums_table_f32<4>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-      case 6: mode_sums_table_f32<6>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-      default: mode_sums_table_f32<8>(Tf, d.nmodes, e, lp, half_dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      case 2: mode_sums_taylor<2, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      case 3: mode_sums_taylor<3, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      case 4: mode_sums_taylor<4, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+      default: mode_sums_taylor<6, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
     }
   } else {
-    double sa, sb, sc;
-    mode_sums_miller(bstart, d.nmodes, e_d, c1, s1, cD, sD, sa, sb, sc);
-    Sa = (float)sa;
-    Sb = (float)sb;
-    Sc = (float)sc;
+    double sa64, sb64, sc64;
+    mode_sums_miller(bstart, d.nmodes, e_d, c1, s1, cD, sD, sa64, sb64, sc64);
+    Sa = (float)sa64;
+    Sb = (float)sb64;
+    Sc = (float)sc64;
   }
   const float se = sqrtf(1.f - e * e);
   const float a = -Amp * Sa, b = -Amp * se * Sb, cc = 2.f * Amp * Sc;
-  hI = (double)(Kresp * ((-uI * opL2 * cos2gam + wI * twoL * sin2gam) * a + (uI * opL2 * sin2gam + wI * twoL * cos2gam) * b +
-                         uI * omL2 * cc));
-  hII = (double)(Kresp * ((-uII * opL2 * cos2gam + wII * twoL * sin2gam) * a +
-                          (uII * opL2 * sin2gam + wII * twoL * cos2gam) * b + uII * omL2 * cc));
+  hI = (double)(R.caI * a + R.cbI * b + R.ccI * cc);
+  hII = (double)(R.caII * a + R.cbII * b + R.ccII * cc);
 }
 
 // ------------------------------------------------------------------ pass 2
@@ -1002,13 +962,13 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   __shared__ double s_r[3][kTileThreads];
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
-  __shared__ double s_T[kTabModes * kTabStride];
-  __shared__ __align__(16) float s_Tf[kSplit ? kTabModes * kTabStrideF : 4];
   __shared__ double s_wt[kWin];
   __shared__ double4 s_wy[kWin], s_wc[kWin];
   double *sv_e = s_dyn, *sv_om = s_dyn + kTileSamples, *sv_gim = s_dyn + 2 * kTileSamples;
   double *sv_Phi = s_dyn + 3 * kTileSamples, *sv_alp = s_dyn + 4 * kTileSamples, *sv_nu = s_dyn + 5 * kTileSamples;
   double *sv_gd = s_dyn + 6 * kTileSamples;
+  double *tabD = s_dyn + kDynVals * kTileSamples;  // Taylor table after the per-sample values
+  float *tabF = reinterpret_cast<float *>(tabD);
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
@@ -1040,13 +1000,11 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     // boundary rate and Bessel-table parameters recorded by pass 1
     const int K = kSplit ? ts.k32 : ts.k64;
     const double ec = ts.ec;
-    // Bessel table rows (one thread per harmonic); its barrier is the first one of phase 1
+    // Taylor table rows (one thread per harmonic); its barrier is the first one of phase 1
     if (K > 0 && !bv.trajectory_only)
       for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
-        double *Tn = s_T + (n - 1) * kTabStride;
-        build_bessel_row(Tn, n, n * ec, K, bstart[n - 1]);
-        if (kSplit)
-          for (int m = 0; m < kTabStrideF; ++m) s_Tf[(n - 1) * kTabStrideF + m] = (m <= 4 + K) ? (float)Tn[m] : 0.f;
+        if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
+        else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
       }
     // ---------------- phase 1: phases of the tile's samples
     double prev[3] = {ts.rate_before[0], (ts.rate_before[1] > 0.0) ? ts.rate_before[1] : tc.Cf[1], ts.rate_before[2]};
@@ -1177,10 +1135,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       double hI = 0.0, hII = 0.0;
       if (i < c.neff) {
         if (kSplit)
-          harmonic_sum_split(d, bstart, s_Tf, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+          harmonic_sum_split(d, bstart, tabF, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
                              sv_nu[sl], sv_gd[sl], hI, hII);
         else
-          harmonic_sum_fp64(d, bstart, s_T, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+          harmonic_sum_fp64(d, bstart, tabD, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
                             sv_nu[sl], sv_gd[sl], hI, hII);
         if (i > d.i_plunge) {
           const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
@@ -1329,14 +1287,21 @@ void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
   k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
   if (ev) cudaEventRecord(ev[2], stream);
   const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 4);
-  static bool attrs_set = false;  // opt in to > 48 KB of shared memory once per process
-  if (!attrs_set) {
-    cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
-    cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
-    attrs_set = true;
+  // per-sample values, then the Taylor table sized for the batch's harmonic count
+  const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
+  const size_t dyn = kWaveDynSmem + (size_t)rows * (precision == 1 ? kRowF * sizeof(float) : kRowD * sizeof(double));
+  static std::atomic<unsigned long long> attrs_set{0};  // opt in to > 48 KB of shared memory once per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attrs_set.load() & bit)) {
+    const int most = (int)(kWaveDynSmem + (size_t)kTabModes * kRowD * sizeof(double));
+    cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    attrs_set.fetch_or(bit);
   }
-  if (precision == 1) k_waveform<true><<<grid2, kTileThreads, kWaveDynSmem, stream>>>(bv);
-  else k_waveform<false><<<grid2, kTileThreads, kWaveDynSmem, stream>>>(bv);
+  if (precision == 1) k_waveform<true><<<grid2, kTileThreads, dyn, stream>>>(bv);
+  else k_waveform<false><<<grid2, kTileThreads, dyn, stream>>>(bv);
   if (ev) cudaEventRecord(ev[3], stream);
 }
 

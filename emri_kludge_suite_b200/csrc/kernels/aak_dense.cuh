@@ -57,6 +57,7 @@ struct BatchView {
   int64_t traj_stride;
   unsigned long long *work_counter;  // persistent work queue head (pass 2)
   int32_t trajectory_only = 0;       // 1: pass 2 writes traj_out and skips the harmonic sums
+  int32_t max_nmodes = 0;            // largest harmonic count of the batch (0: unknown) -- sizes the tile table
 };
 
 // Launch pass 1, the carry scan and pass 2 on `stream`.  ev (optional, 4
