@@ -30,7 +30,9 @@ constexpr double kPi2Trunc = 9.86960440109;
 // Kerr-geodesic frequency ratios in the 3PN AK mapping (Sago & Fujita 2015),
 // as functions of v = 1/sqrt(p), e, Y = cos(iota), q = spin.  Same expressions
 // as src/suite/KSParMap.cc:146-209, grouped by powers of v.
-AAK_HD double pn_dtdm(double v, double e, double Y, double q) {
+// Numerators of the PN derivatives below: pn_dtdm = pn_dtdm_num / (256 v^4),
+// the other three = num / (16 v).
+AAK_HD double pn_dtdm_num(double v, double e, double Y, double q) {
   const double v2 = v * v, v3 = v2 * v, v4 = v2 * v2;
   const double e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
   double s = 2. * e4 *
@@ -44,30 +46,36 @@ AAK_HD double pn_dtdm(double v, double e, double Y, double q) {
                      v4 * (1233. + 8. * q2 * (-47. + 150. * Y2))));
   s += 16. * (16. + v2 * (24. + v2 * (27. * (2. + 5. * v2) - 48. * q * v * Y +
                                       4. * q2 * (2. - v2 + (-2. + 3. * v2) * Y2))));
-  return s / (256. * v4);
+  return s;
+}
+AAK_HD double pn_dtdm(double v, double e, double Y, double q) {
+  const double v2 = v * v;
+  return pn_dtdm_num(v, e, Y, q) / (256. * (v2 * v2));
 }
 
-AAK_HD double pn_drdm(double v, double e, double Y, double q) {
+AAK_HD double pn_drdm_num(double v, double e, double Y, double q) {
   const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
   double s = 16. + 8. * (-3. + e2) * v2 - 16. * (-3. + e2) * q * v3 * Y + 8. * (33. + 4. * e2 - 3. * e4) * q * v3 * v2 * Y;
   s += v3 * v3 *
        (-351. + 132. * q2 + e2 * (-135. + 21. * e2 + 5. * e4 + 2. * (7. + e2) * q2) +
         2. * (-204. + 13. * e2 * (-3. + e2)) * q2 * Y2);
   s += 2. * v2 * v2 * (-45. + 3. * e4 + 4. * q2 * (1. - 4. * Y2) + 2. * e2 * q2 * (1. + Y2));
-  return s / (16. * v);
+  return s;
 }
+AAK_HD double pn_drdm(double v, double e, double Y, double q) { return pn_drdm_num(v, e, Y, q) / (16. * v); }
 
-AAK_HD double pn_dthetadm(double v, double e, double Y, double q) {
+AAK_HD double pn_dthetadm_num(double v, double e, double Y, double q) {
   const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
   double s = 16. + 8. * (3. + e2) * v2 - 16. * (3. + e2) * q * v3 * Y - 8. * (3. + e2) * (5. + 3. * e2) * q * v3 * v2 * Y;
   s += v3 * v3 *
        (135. - 54. * q2 + e2 * (5. * (27. + 9. * e2 + e4) + 2. * (-38. + e2) * q2) +
         2. * (57. + 90. * e2 + 13. * e4) * q2 * Y2);
   s += 2. * v2 * v2 * (27. + 3. * e4 + 2. * q2 * (-1. + 7. * Y2) + 2. * e2 * (9. + q2 * (1. + Y2)));
-  return s / (16. * v);
+  return s;
 }
+AAK_HD double pn_dthetadm(double v, double e, double Y, double q) { return pn_dthetadm_num(v, e, Y, q) / (16. * v); }
 
-AAK_HD double pn_dphidm(double v, double e, double Y, double q) {
+AAK_HD double pn_dphidm_num(double v, double e, double Y, double q) {
   const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
   double s = 16. + 8. * (3. + e2) * v2 - 16. * q * v3 * (-2. + (3. + e2) * Y) -
              8. * q * v3 * v2 * (-6. + 15. * Y + 3. * e4 * Y + 2. * e2 * (-4. + 7. * Y));
@@ -75,8 +83,9 @@ AAK_HD double pn_dphidm(double v, double e, double Y, double q) {
   s += v3 * v3 *
        (5. * e4 * e2 + e4 * (45. + q2 * (2. + 26. * Y2)) + e2 * (135. + 4. * q2 * (-19. + 5. * Y * (-7. + 9. * Y))) +
         3. * (45. + 2. * q2 * (-9. + Y * (-6. + 19. * Y))));
-  return s / (16. * v);
+  return s;
 }
+AAK_HD double pn_dphidm(double v, double e, double Y, double q) { return pn_dphidm_num(v, e, Y, q) / (16. * v); }
 
 // Azimuthal frequency magnitude for pro/retrograde orbits (src/suite/AAK.cc:15-23).
 AAK_HD double omega_phi(double v, double e, double cosiota, double s, double M) {

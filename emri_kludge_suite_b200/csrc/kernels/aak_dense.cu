@@ -88,9 +88,10 @@ struct KnotWin {
   double *t;   // kWin
   double4 *y;  // kWin
   double4 *c;  // kWin
-  int k0;      // first knot of the window (source-relative)
-  int n;       // knots in the window
-  int staged;  // 1: window is in shared memory
+  int k0;        // first knot of the window (source-relative)
+  int n;         // knots in the window
+  int staged;    // 1: window is in shared memory
+  double inv_h;  // (n - 1) / (t_{n-1} - t_0): pieces per unit time
 };
 
 __device__ __forceinline__ Traj4 eval_piece(const double4 &y0, const double4 &y1, const double4 &c0, const double4 &c1,
@@ -106,13 +107,13 @@ __device__ __forceinline__ Traj4 eval_piece(const double4 &y0, const double4 &y1
 
 __device__ __forceinline__ Traj4 spline4w(const BatchView &bv, const SourceDesc &d, double t, const KnotWin &w) {
   if (w.staged) {
-    int lo = 0, hi = w.n - 1;
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) >> 1;
-      if (w.t[mid] > t) hi = mid;
-      else lo = mid;
-    }
-    return eval_piece(w.y[lo], w.y[lo + 1], w.c[lo], w.c[lo + 1], w.t[lo], w.t[lo + 1], t);
+    // the knots are (nearly) evenly spaced: guess the piece, then step to the
+    // largest k <= n - 2 with t_k <= t (the binary search's answer)
+    int k = __double2int_rd((t - w.t[0]) * w.inv_h);
+    k = min(max(k, 0), w.n - 2);
+    while (k < w.n - 2 && w.t[k + 1] <= t) ++k;
+    while (k > 0 && w.t[k] > t) --k;
+    return eval_piece(w.y[k], w.y[k + 1], w.c[k], w.c[k + 1], w.t[k], w.t[k + 1], t);
   }
   const double *kt = bv.knot_t + d.knot_offset;
   int lo = w.k0, hi = w.k0 + w.n - 1;
@@ -138,17 +139,26 @@ __device__ __forceinline__ void load_window(const BatchView &bv, const SourceDes
       w.c[k] = bv.knot_c[o];
     }
   __syncthreads();
+  if (w.staged) {
+    const double span = w.t[w.n - 1] - w.t[0];
+    w.inv_h = (span > 0.0) ? (double)(w.n - 1) / span : 0.0;
+  }
 }
 
 // gamma~dot, Phidot, alphadot (AAK.cc:251-253)
-__device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q, double r[3]) {
-  const double tm = pn_dtdm(q.v, q.e, d.coslam, q.S);
-  const double rm = pn_drdm(q.v, q.e, d.coslam, q.S);
-  const double thm = pn_dthetadm(q.v, q.e, d.coslam, q.S);
-  const double phm = pn_dphidm(q.v, q.e, d.coslam, q.S);
-  r[0] = (thm - rm) / tm / q.M;
-  r[1] = rm / tm / q.M;
-  r[2] = (phm - thm) / tm / q.M;
+// with one division: d(x)/dm / dt/dm / M = 16 v^3 num_x / (num_t M) for the
+// PN numerators of aak_common.hpp.  om (optional) receives Omega_phi, the
+// same ratio for phi on prograde orbits (omega_phi, AAK.cc:15-23).
+__device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q, double r[3], double *om = nullptr) {
+  const double st = pn_dtdm_num(q.v, q.e, d.coslam, q.S);
+  const double sr = pn_drdm_num(q.v, q.e, d.coslam, q.S);
+  const double sth = pn_dthetadm_num(q.v, q.e, d.coslam, q.S);
+  const double sph = pn_dphidm_num(q.v, q.e, d.coslam, q.S);
+  const double inv = 16. * (q.v * q.v * q.v) / (st * q.M);
+  r[0] = (sth - sr) * inv;
+  r[1] = sr * inv;
+  r[2] = (sph - sth) * inv;
+  if (om) *om = (d.coslam > 0) ? sph * inv : omega_phi(q.v, q.e, d.coslam, q.S, q.M);
 }
 
 __device__ __forceinline__ double sample_time(const SourceDesc &d, int i) {
@@ -1017,10 +1027,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       const bool vf = in && i >= d.i0;
       const bool vb = in && i >= 1 && i <= d.i0;
       Traj4 q = {0, 0, 0, 0};
-      double r[3] = {0, 0, 0};
+      double r[3] = {0, 0, 0}, om = 0.0;
       if (in) {
         q = spline4w(bv, d, sample_time(d, i), w);
-        phase_rates(d, q, r);
+        phase_rates(d, q, r, &om);
       }
       s_raw[tid] = vf ? r[1] : -1.0;
       s_r[0][tid] = r[0];
@@ -1097,7 +1107,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       if (in) {
         const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
         sv_e[sl] = q.e;
-        sv_om[sl] = omega_phi(q.v, q.e, d.coslam, q.S, q.M) * d.M_phys_sec;
+        sv_om[sl] = om * d.M_phys_sec;
         sv_gim[sl] = X[0];
         sv_Phi[sl] = X[1];
         sv_alp[sl] = X[2];
