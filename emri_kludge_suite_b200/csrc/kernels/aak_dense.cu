@@ -15,6 +15,7 @@
 #include <math.h>
 
 #include <atomic>
+#include <type_traits>
 #include <mutex>
 
 #include "aak_dense.cuh"
@@ -86,8 +87,10 @@ constexpr int kWin = 64;
 
 struct KnotWin {
   double *t;   // kWin
-  double4 *y;  // kWin
-  double4 *c;  // kWin
+  double4 *y;  // kWin: values at the knots
+  double4 *c;  // kWin: half second derivatives
+  double4 *b;  // kWin: first-order coefficients of the pieces (staged windows)
+  double4 *d;  // kWin: third-order coefficients of the pieces (staged windows)
   int k0;        // first knot of the window (source-relative)
   int n;         // knots in the window
   int staged;    // 1: window is in shared memory
@@ -113,17 +116,24 @@ __device__ __forceinline__ Traj4 spline4w(const BatchView &bv, const SourceDesc 
     k = min(max(k, 0), w.n - 2);
     while (k < w.n - 2 && w.t[k + 1] <= t) ++k;
     while (k > 0 && w.t[k] > t) --k;
-    return eval_piece(w.y[k], w.y[k + 1], w.c[k], w.c[k + 1], w.t[k], w.t[k + 1], t);
+    const double dx = t - w.t[k];
+    const double4 y = w.y[k], b = w.b[k], c = w.c[k], dd = w.d[k];
+    Traj4 q;
+    q.e = y.x + dx * (b.x + dx * (c.x + dx * dd.x));
+    q.v = y.y + dx * (b.y + dx * (c.y + dx * dd.y));
+    q.M = y.z + dx * (b.z + dx * (c.z + dx * dd.z));
+    q.S = y.w + dx * (b.w + dx * (c.w + dx * dd.w));
+    return q;
   }
+  // long windows stay in global memory: the same guess-and-step search there
   const double *kt = bv.knot_t + d.knot_offset;
-  int lo = w.k0, hi = w.k0 + w.n - 1;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (kt[mid] > t) hi = mid;
-    else lo = mid;
-  }
-  const int64_t o = d.knot_offset + lo;
-  return eval_piece(bv.knot_y[o], bv.knot_y[o + 1], bv.knot_c[o], bv.knot_c[o + 1], kt[lo], kt[lo + 1], t);
+  const int last = w.k0 + w.n - 2;
+  int k = w.k0 + __double2int_rd((t - kt[w.k0]) * w.inv_h);
+  k = min(max(k, w.k0), last);
+  while (k < last && kt[k + 1] <= t) ++k;
+  while (k > w.k0 && kt[k] > t) --k;
+  const int64_t o = d.knot_offset + k;
+  return eval_piece(bv.knot_y[o], bv.knot_y[o + 1], bv.knot_c[o], bv.knot_c[o + 1], kt[k], kt[k + 1], t);
 }
 
 // Stage the knots of tile g (bracket precomputed on the host, tile_knot).
@@ -139,9 +149,25 @@ __device__ __forceinline__ void load_window(const BatchView &bv, const SourceDes
       w.c[k] = bv.knot_c[o];
     }
   __syncthreads();
-  if (w.staged) {
+  if (!w.staged) {
+    const double *kt = bv.knot_t + d.knot_offset;
+    const double span = kt[w.k0 + w.n - 1] - kt[w.k0];
+    w.inv_h = (span > 0.0) ? (double)(w.n - 1) / span : 0.0;
+  } else {
     const double span = w.t[w.n - 1] - w.t[0];
     w.inv_h = (span > 0.0) ? (double)(w.n - 1) / span : 0.0;
+    // piece coefficients y + dx (b + dx (c + dx d)) of the natural spline, once per window
+    for (int k = threadIdx.x; k < w.n - 1; k += blockDim.x) {
+      const double h = w.t[k + 1] - w.t[k];
+      const double4 y0 = w.y[k], y1 = w.y[k + 1], c0 = w.c[k], c1 = w.c[k + 1];
+      w.b[k] = make_double4((y1.x - y0.x) / h - h * (c1.x + 2.0 * c0.x) / 3.0,
+                            (y1.y - y0.y) / h - h * (c1.y + 2.0 * c0.y) / 3.0,
+                            (y1.z - y0.z) / h - h * (c1.z + 2.0 * c0.z) / 3.0,
+                            (y1.w - y0.w) / h - h * (c1.w + 2.0 * c0.w) / 3.0);
+      w.d[k] = make_double4((c1.x - c0.x) / (3.0 * h), (c1.y - c0.y) / (3.0 * h), (c1.z - c0.z) / (3.0 * h),
+                            (c1.w - c0.w) / (3.0 * h));
+    }
+    __syncthreads();
   }
 }
 
@@ -305,7 +331,7 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
   __shared__ double s_r[3][kSlots];
   __shared__ double red[7][kTileThreads / 32];
   __shared__ double s_wt[kWin];
-  __shared__ double4 s_wy[kWin], s_wc[kWin];
+  __shared__ double4 s_wy[kWin], s_wc[kWin], s_wb[kWin], s_wd[kWin];
   const int tid = threadIdx.x;
   for (int64_t g = blockIdx.x; g < bv.total_tiles; g += gridDim.x) {
     const SourceDesc *dp;
@@ -323,7 +349,7 @@ __global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
       }
       continue;
     }
-    KnotWin w{s_wt, s_wy, s_wc, 0, 0, 0};
+    KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
     load_window(bv, d, g, w);
     // (A) rates, two independent samples per pass
 #pragma unroll 1
@@ -724,6 +750,68 @@ __device__ __forceinline__ void mode_sums_taylor(const T *tab, int nmodes, int s
   Sc = sc;
 }
 
+// The same for M samples of one tile at once: each table row is loaded once
+// for all of them and the M phase recurrences run side by side.
+template <int K, typename T, int M>
+__device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes, int stride, const T *dl, const T *c1,
+                                                       const T *s1, const T *cD, const T *sD, T *Sa, T *Sb, T *Sc) {
+  constexpr int NV = 3 * (K + 1);
+  T zr[M], zi[M], sa[M], sb[M], sc[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    zr[m] = T(1);
+    zi[m] = T(0);
+    sa[m] = sb[m] = sc[m] = T(0);
+  }
+#pragma unroll 1
+  for (int n = 1; n <= nmodes; ++n) {
+    T v[(sizeof(T) == 4) ? (NV + 3) / 4 * 4 : (NV + 1) / 2 * 2];
+    if constexpr (sizeof(T) == 4) {
+      const float4 *r4 = reinterpret_cast<const float4 *>(tab + (n - 1) * stride);
+#pragma unroll
+      for (int i = 0; i < (NV + 3) / 4; ++i) {
+        const float4 q = r4[i];
+        v[4 * i] = q.x;
+        v[4 * i + 1] = q.y;
+        v[4 * i + 2] = q.z;
+        v[4 * i + 3] = q.w;
+      }
+    } else {
+      const double2 *r2 = reinterpret_cast<const double2 *>(tab + (n - 1) * stride);
+#pragma unroll
+      for (int i = 0; i < (NV + 1) / 2; ++i) {
+        const double2 q = r2[i];
+        v[2 * i] = q.x;
+        v[2 * i + 1] = q.y;
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      T A = v[K], B = v[2 * K + 1], C = v[3 * K + 2];
+#pragma unroll
+      for (int k = K - 1; k >= 0; --k) {
+        A = fma(A, dl[m], v[k]);
+        B = fma(B, dl[m], v[K + 1 + k]);
+        C = fma(C, dl[m], v[2 * (K + 1) + k]);
+      }
+      const T tr = zr[m] * c1[m] - zi[m] * s1[m];
+      zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
+      zr[m] = tr;
+      const T cn = zr[m] * cD[m] - zi[m] * sD[m];
+      const T sn = fma(zi[m], cD[m], zr[m] * sD[m]);
+      sa[m] = fma(A, cn, sa[m]);
+      sb[m] = fma(B, sn, sb[m]);
+      sc[m] = fma(C, cn, sc[m]);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    Sa[m] = sa[m];
+    Sb[m] = sb[m];
+    Sc[m] = sc[m];
+  }
+}
+
 // Mode sums with a per-sample Miller recurrence (fallback when the table does not apply).
 __device__ void mode_sums_miller(const int32_t *bstart, int nmodes, double e, double c1, double s1, double cD,
                                  double sD, double &Sa, double &Sb, double &Sc) {
@@ -763,10 +851,6 @@ __device__ void mode_sums_miller(const int32_t *bstart, int nmodes, double e, do
 }
 
 // ------------------------------------------------------------------ harmonic sum
-// h_I, h_II at one sample (AAK.cc:409-528) with the modes accumulated as
-// Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
-// rotation and antenna factors applied once per sample.  The Bessel values
-// come from the tile table (K > 0) or a per-sample recurrence (K == 0).
 // cos 2 atan2(y, x) and sin 2 atan2(y, x) without the angle (atan2(0, 0) = 0)
 template <typename T>
 __device__ __forceinline__ void double_angle(T y, T x, T &c2, T &s2) {
@@ -860,6 +944,76 @@ __device__ __forceinline__ Resp<T> response(const SourceDesc &d, T ca, T sa, T c
   return R;
 }
 
+// x mod 2pi in [-pi, pi], two-term Cody-Waite reduction in FP64, returned as float
+__device__ __forceinline__ float reduce_2pi_f(double x) {
+  const double k = rint(x * (1.0 / kTwoPi));
+  const double r = fma(-k, 2.4492935982947064e-16, fma(-k, 6.283185307179586, x));
+  return (float)r;
+}
+
+// Everything of one sample's harmonic sum except the mode sums: response
+// coefficients, amplitude and the harmonic phase rotors.
+template <typename T>
+struct SamplePrep {
+  Resp<T> R;
+  T Amp, se;            // amplitude, sqrt(1 - e^2)
+  T c1, s1, cD, sD;     // harmonic n: (c1 + i s1)^n (cD + i sD)
+  T dl;                 // e - e_c
+};
+
+__device__ __forceinline__ SamplePrep<double> prep_fp64(const SourceDesc &d, double ec, double t, double e,
+                                                         double om_M, double gim, double Phi, double alp, double nu,
+                                                         double gimdot) {
+  SamplePrep<double> P;
+  double sa, ca, s2g, c2g, so = 0.0, co = 1.0;
+  sincos(alp, &sa, &ca);
+  sincos(2. * gim, &s2g, &c2g);
+  if (d.mich) sincos(kTwoPi * t / kYear, &so, &co);
+  P.R = response<double>(d, ca, sa, c2g, s2g, co, so);
+  P.Amp = pow(om_M, 2. / 3.) * d.zeta;
+  double D1 = 0.0, D0 = 0.0;
+  if (d.mich) {
+    D1 = kTwoPi * nu * kAUsec * d.sinqS * P.R.cosorb_S;
+    D0 = 2.0 * gimdot * kAUsec * d.sinqS * P.R.cosorb_S;
+  }
+  sincos(Phi + D1, &P.s1, &P.c1);
+  sincos(D0, &P.sD, &P.cD);
+  P.se = sqrt(1. - e * e);
+  P.dl = e - ec;
+  return P;
+}
+
+__device__ __forceinline__ SamplePrep<float> prep_split(const SourceDesc &d, double ec, double t, double e_d,
+                                                        double om_M, double gim, double Phi, double alp, double nu,
+                                                        double gimdot) {
+  SamplePrep<float> P;
+  float sa, ca, s2g, c2g, so = 0.f, co = 1.f;
+  __sincosf(reduce_2pi_f(alp), &sa, &ca);
+  __sincosf(reduce_2pi_f(2.0 * gim), &s2g, &c2g);
+  if (d.mich) __sincosf(reduce_2pi_f(kTwoPi * t / kYear), &so, &co);
+  P.R = response<float>(d, ca, sa, c2g, s2g, co, so);
+  P.Amp = exp2f((2.f / 3.f) * __log2f((float)om_M)) * (float)d.zeta;
+  double D1 = 0.0;
+  float D0 = 0.f;
+  if (d.mich) {
+    D1 = kTwoPi * nu * kAUsec * d.sinqS * (double)P.R.cosorb_S;
+    D0 = (float)(2.0 * gimdot * kAUsec * d.sinqS) * P.R.cosorb_S;
+  }
+  __sincosf(reduce_2pi_f(Phi + D1), &P.s1, &P.c1);
+  __sincosf(D0, &P.sD, &P.cD);
+  const float e = (float)e_d;
+  P.se = sqrtf(1.f - e * e);
+  P.dl = (float)(e_d - ec);
+  return P;
+}
+
+template <typename T>
+__device__ __forceinline__ void finish(const SamplePrep<T> &P, T Sa, T Sb, T Sc, double &hI, double &hII) {
+  const T a = -P.Amp * Sa, b = -P.Amp * P.se * Sb, cc = T(2) * P.Amp * Sc;
+  hI = (double)(P.R.caI * a + P.R.cbI * b + P.R.ccI * cc);
+  hII = (double)(P.R.caII * a + P.R.cbII * b + P.R.ccII * cc);
+}
+
 // h_I, h_II at one sample (AAK.cc:409-528) with the modes accumulated as
 // Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
 // rotation and antenna factors applied once per sample.  The Bessel values
@@ -903,12 +1057,6 @@ __device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, co
 // FP64: spline, rates, phase sums and every angle reduction; FP32: geometry,
 // antenna response, Bessel evaluation and the harmonic recurrence.
 
-// x mod 2pi in [-pi, pi], two-term Cody-Waite reduction in FP64, returned as float
-__device__ __forceinline__ float reduce_2pi_f(double x) {
-  const double k = rint(x * (1.0 / kTwoPi));
-  const double r = fma(-k, 2.4492935982947064e-16, fma(-k, 6.283185307179586, x));
-  return (float)r;
-}
 
 // h_I, h_II at one sample in split precision: the angle reductions in FP64,
 // the trigonometry, response and harmonic sums in FP32 (same algebra as
@@ -956,6 +1104,14 @@ __device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, c
 }
 
 // ------------------------------------------------------------------ pass 2
+// Samples per thread whose harmonic sums run side by side (divides kTileChunks).
+#ifndef AAK_JOINT_SPLIT
+#define AAK_JOINT_SPLIT 2
+#endif
+#ifndef AAK_JOINT_FP64
+#define AAK_JOINT_FP64 1
+#endif
+static_assert(kTileChunks % AAK_JOINT_SPLIT == 0 && kTileChunks % AAK_JOINT_FP64 == 0, "joint samples must divide the chunks");
 // Per tile: phase 1 computes, for the tile's 1024 samples, the spline, rates,
 // clamped Phidot and the block-scanned AB2 phases (uniform, cheap work with
 // the tile's barriers) and parks each sample's harmonic-sum inputs in shared
@@ -973,7 +1129,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
   __shared__ double s_wt[kWin];
-  __shared__ double4 s_wy[kWin], s_wc[kWin];
+  __shared__ double4 s_wy[kWin], s_wc[kWin], s_wb[kWin], s_wd[kWin];
   double *sv_e = s_dyn, *sv_om = s_dyn + kTileSamples, *sv_gim = s_dyn + 2 * kTileSamples;
   double *sv_Phi = s_dyn + 3 * kTileSamples, *sv_alp = s_dyn + 4 * kTileSamples, *sv_nu = s_dyn + 5 * kTileSamples;
   double *sv_gd = s_dyn + 6 * kTileSamples;
@@ -1005,7 +1161,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
       continue;
     }
-    KnotWin w{s_wt, s_wy, s_wc, 0, 0, 0};
+    KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
     load_window(bv, d, g, w);
     // boundary rate and Bessel-table parameters recorded by pass 1
     const int K = kSplit ? ts.k32 : ts.k64;
@@ -1133,32 +1289,84 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       prev[2] = s_r[2][kTileThreads - 1];
       __syncthreads();
     }
-    // ---------------- phase 2: harmonic sums of this thread's own samples
+    // ---------------- phase 2: harmonic sums of this thread's own samples,
+    // kJoint of them at a time (shared table loads, independent recurrences)
     if (bv.trajectory_only) continue;
     const double t_plunge = sample_time(d, d.i_plunge);
     const double t_zero = t_plunge + d.dt * d.i_buffer;
-    for (int ch = 0; ch < kTileChunks; ++ch) {
-      const int i = c.start + ch * kTileThreads + tid;
-      const int sl = ch * kTileThreads + tid;
-      if (i >= c.end) continue;
-      const double t = sample_time(d, i);
-      double hI = 0.0, hII = 0.0;
-      if (i < c.neff) {
-        if (kSplit)
-          harmonic_sum_split(d, bstart, tabF, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
-                             sv_nu[sl], sv_gd[sl], hI, hII);
-        else
-          harmonic_sum_fp64(d, bstart, tabD, ec, K, t, sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
-                            sv_nu[sl], sv_gd[sl], hI, hII);
-        if (i > d.i_plunge) {
-          const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
-          hI = hI / wgt;
-          hII = hII / wgt;
+    using T = typename std::conditional<kSplit, float, double>::type;
+    constexpr int kJoint = kSplit ? AAK_JOINT_SPLIT : AAK_JOINT_FP64;
+    const T *tab = kSplit ? reinterpret_cast<const T *>(tabF) : reinterpret_cast<const T *>(tabD);
+#pragma unroll 1
+    for (int g0 = 0; g0 < kTileChunks; g0 += kJoint) {
+      SamplePrep<T> P[kJoint];
+      T dl[kJoint], c1[kJoint], s1[kJoint], cD[kJoint], sD[kJoint], Sa[kJoint], Sb[kJoint], Sc[kJoint];
+#pragma unroll
+      for (int m = 0; m < kJoint; ++m) {
+        const int i = c.start + (g0 + m) * kTileThreads + tid;
+        const int sl = (g0 + m) * kTileThreads + tid;
+        if (i < c.end && i < c.neff) {
+          if constexpr (kSplit)
+            P[m] = prep_split(d, ec, sample_time(d, i), sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+                              sv_nu[sl], sv_gd[sl]);
+          else
+            P[m] = prep_fp64(d, ec, sample_time(d, i), sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+                             sv_nu[sl], sv_gd[sl]);
+        } else {
+          P[m] = SamplePrep<T>{};
+          P[m].c1 = P[m].cD = T(1);
+        }
+        dl[m] = P[m].dl;
+        c1[m] = P[m].c1;
+        s1[m] = P[m].s1;
+        cD[m] = P[m].cD;
+        sD[m] = P[m].sD;
+      }
+      if constexpr (kSplit) {
+        switch (K) {
+          case 2: mode_sums_taylor_multi<2, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 3: mode_sums_taylor_multi<3, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          default: break;
+        }
+      } else {
+        switch (K) {
+          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 5: mode_sums_taylor_multi<5, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 8: mode_sums_taylor_multi<8, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 10: mode_sums_taylor_multi<10, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          default: break;
         }
       }
-      bv.hI[d.out_offset + i] = hI;
-      bv.hII[d.out_offset + i] = hII;
-      if (bv.t_out) bv.t_out[d.out_offset + i] = t;
+#pragma unroll
+      for (int m = 0; m < kJoint; ++m) {
+        const int i = c.start + (g0 + m) * kTileThreads + tid;
+        const int sl = (g0 + m) * kTileThreads + tid;
+        if (i >= c.end) continue;
+        const double t = sample_time(d, i);
+        double hI = 0.0, hII = 0.0;
+        if (i < c.neff) {
+          if (K == 0) {  // no table for this tile: per-sample Miller recurrence in FP64
+            double a64, b64, c64;
+            mode_sums_miller(bstart, d.nmodes, sv_e[sl], (double)c1[m], (double)s1[m], (double)cD[m], (double)sD[m],
+                             a64, b64, c64);
+            Sa[m] = (T)a64;
+            Sb[m] = (T)b64;
+            Sc[m] = (T)c64;
+          }
+          finish<T>(P[m], Sa[m], Sb[m], Sc[m], hI, hII);
+          if (i > d.i_plunge) {
+            const double wgt = exp((t_plunge - t_zero) / (t - t_plunge) + (t_plunge - t_zero) / (t - t_zero)) + 1.;
+            hI = hI / wgt;
+            hII = hII / wgt;
+          }
+        }
+        bv.hI[d.out_offset + i] = hI;
+        bv.hII[d.out_offset + i] = hII;
+        if (bv.t_out) bv.t_out[d.out_offset + i] = t;
+      }
     }
   }
 }
