@@ -701,57 +701,9 @@ __device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes) {
 
 // Mode sums Sa = sum A_n cos(n Phi'), Sb = sum B_n sin(n Phi'), Sc = sum C_n
 // cos(n Phi') from the tile table at delta = e - e_c, with the harmonic
-// phases from the rotation recurrence z_n = z_1^n z_D.
-template <int K, typename T>
-__device__ __forceinline__ void mode_sums_taylor(const T *tab, int nmodes, int stride, T dl, T c1, T s1, T cD, T sD,
-                                                 T &Sa, T &Sb, T &Sc) {
-  constexpr int NV = 3 * (K + 1);
-  T zr = T(1), zi = T(0), sa = T(0), sb = T(0), sc = T(0);
-#pragma unroll 2
-  for (int n = 1; n <= nmodes; ++n) {
-    T v[(sizeof(T) == 4) ? (NV + 3) / 4 * 4 : (NV + 1) / 2 * 2];
-    if constexpr (sizeof(T) == 4) {
-      const float4 *r4 = reinterpret_cast<const float4 *>(tab + (n - 1) * stride);
-#pragma unroll
-      for (int i = 0; i < (NV + 3) / 4; ++i) {
-        const float4 q = r4[i];
-        v[4 * i] = q.x;
-        v[4 * i + 1] = q.y;
-        v[4 * i + 2] = q.z;
-        v[4 * i + 3] = q.w;
-      }
-    } else {
-      const double2 *r2 = reinterpret_cast<const double2 *>(tab + (n - 1) * stride);
-#pragma unroll
-      for (int i = 0; i < (NV + 1) / 2; ++i) {
-        const double2 q = r2[i];
-        v[2 * i] = q.x;
-        v[2 * i + 1] = q.y;
-      }
-    }
-    T A = v[K], B = v[2 * K + 1], C = v[3 * K + 2];
-#pragma unroll
-    for (int k = K - 1; k >= 0; --k) {
-      A = fma(A, dl, v[k]);
-      B = fma(B, dl, v[K + 1 + k]);
-      C = fma(C, dl, v[2 * (K + 1) + k]);
-    }
-    const T tr = zr * c1 - zi * s1;
-    zi = fma(zr, s1, zi * c1);
-    zr = tr;
-    const T cn = zr * cD - zi * sD;
-    const T sn = fma(zi, cD, zr * sD);
-    sa = fma(A, cn, sa);
-    sb = fma(B, sn, sb);
-    sc = fma(C, cn, sc);
-  }
-  Sa = sa;
-  Sb = sb;
-  Sc = sc;
-}
-
-// The same for M samples of one tile at once: each table row is loaded once
-// for all of them and the M phase recurrences run side by side.
+// phases from the rotation recurrence z_n = z_1^n z_D, for M samples of one
+// tile at once: each table row is loaded once for all of them and the M
+// recurrences run side by side.
 template <int K, typename T, int M>
 __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes, int stride, const T *dl, const T *c1,
                                                        const T *s1, const T *cD, const T *sD, T *Sa, T *Sb, T *Sc) {
@@ -878,8 +830,49 @@ struct Resp {
   T cosorb_S;  // cos(orbital phase - phi_S), for the Doppler term
 };
 
+// The per-source constants response() reads, in the arithmetic type of the
+// harmonic sum; one copy per tile in shared memory.
 template <typename T>
-__device__ __forceinline__ Resp<T> response(const SourceDesc &d, T ca, T sa, T c2g, T s2g, T co, T so) {
+struct Geom {
+  T Lc[3], Ls[3], Lq[3], nv[3], Sv[3], nxS[3];
+  T nxS_norm, Sdotn, coslam, beta_c, beta_s, cphiS, sphiS, cosphiK, sinphiK;
+  T cosqS, sinqS, cosqK, sinqK, psd0, psd1, psd2, F0[4], zeta;
+  int mich;
+};
+
+template <typename T>
+__device__ void make_geom(const SourceDesc &d, Geom<T> &g) {
+  for (int i = 0; i < 3; ++i) {
+    g.Lc[i] = (T)d.Lc[i];
+    g.Ls[i] = (T)d.Ls[i];
+    g.Lq[i] = (T)d.Lq[i];
+    g.nv[i] = (T)d.nv[i];
+    g.Sv[i] = (T)d.Sv[i];
+    g.nxS[i] = (T)d.nxS[i];
+  }
+  g.nxS_norm = (T)d.nxS_norm;
+  g.Sdotn = (T)d.Sdotn;
+  g.coslam = (T)d.coslam;
+  g.beta_c = (T)d.beta_c;
+  g.beta_s = (T)d.beta_s;
+  g.cphiS = (T)d.cphiS;
+  g.sphiS = (T)d.sphiS;
+  g.cosphiK = (T)d.cosphiK;
+  g.sinphiK = (T)d.sinphiK;
+  g.cosqS = (T)d.cosqS;
+  g.sinqS = (T)d.sinqS;
+  g.cosqK = (T)d.cosqK;
+  g.sinqK = (T)d.sinqK;
+  g.psd0 = (T)d.psd0;
+  g.psd1 = (T)d.psd1;
+  g.psd2 = (T)d.psd2;
+  for (int i = 0; i < 4; ++i) g.F0[i] = (T)d.F0[i];
+  g.zeta = (T)d.zeta;
+  g.mich = d.mich;
+}
+
+template <typename T>
+__device__ __forceinline__ Resp<T> response(const Geom<T> &d, T ca, T sa, T c2g, T s2g, T co, T so) {
   const T L0 = (T)d.Lc[0] + sa * (T)d.Ls[0] + ca * (T)d.Lq[0];
   const T L1 = (T)d.Lc[1] + sa * (T)d.Ls[1] + ca * (T)d.Lq[1];
   const T L2 = (T)d.Lc[2] + ca * (T)d.Lq[2];
@@ -961,7 +954,7 @@ struct SamplePrep {
   T dl;                 // e - e_c
 };
 
-__device__ __forceinline__ SamplePrep<double> prep_fp64(const SourceDesc &d, double ec, double t, double e,
+__device__ __forceinline__ SamplePrep<double> prep_fp64(const SourceDesc &d, const Geom<double> &g, double ec, double t, double e,
                                                          double om_M, double gim, double Phi, double alp, double nu,
                                                          double gimdot) {
   SamplePrep<double> P;
@@ -969,7 +962,7 @@ __device__ __forceinline__ SamplePrep<double> prep_fp64(const SourceDesc &d, dou
   sincos(alp, &sa, &ca);
   sincos(2. * gim, &s2g, &c2g);
   if (d.mich) sincos(kTwoPi * t / kYear, &so, &co);
-  P.R = response<double>(d, ca, sa, c2g, s2g, co, so);
+  P.R = response<double>(g, ca, sa, c2g, s2g, co, so);
   P.Amp = pow(om_M, 2. / 3.) * d.zeta;
   double D1 = 0.0, D0 = 0.0;
   if (d.mich) {
@@ -983,7 +976,7 @@ __device__ __forceinline__ SamplePrep<double> prep_fp64(const SourceDesc &d, dou
   return P;
 }
 
-__device__ __forceinline__ SamplePrep<float> prep_split(const SourceDesc &d, double ec, double t, double e_d,
+__device__ __forceinline__ SamplePrep<float> prep_split(const SourceDesc &d, const Geom<float> &g, double ec, double t, double e_d,
                                                         double om_M, double gim, double Phi, double alp, double nu,
                                                         double gimdot) {
   SamplePrep<float> P;
@@ -991,8 +984,8 @@ __device__ __forceinline__ SamplePrep<float> prep_split(const SourceDesc &d, dou
   __sincosf(reduce_2pi_f(alp), &sa, &ca);
   __sincosf(reduce_2pi_f(2.0 * gim), &s2g, &c2g);
   if (d.mich) __sincosf(reduce_2pi_f(kTwoPi * t / kYear), &so, &co);
-  P.R = response<float>(d, ca, sa, c2g, s2g, co, so);
-  P.Amp = exp2f((2.f / 3.f) * __log2f((float)om_M)) * (float)d.zeta;
+  P.R = response<float>(g, ca, sa, c2g, s2g, co, so);
+  P.Amp = exp2f((2.f / 3.f) * __log2f((float)om_M)) * g.zeta;
   double D1 = 0.0;
   float D0 = 0.f;
   if (d.mich) {
@@ -1014,94 +1007,12 @@ __device__ __forceinline__ void finish(const SamplePrep<T> &P, T Sa, T Sb, T Sc,
   hII = (double)(P.R.caII * a + P.R.cbII * b + P.R.ccII * cc);
 }
 
-// h_I, h_II at one sample (AAK.cc:409-528) with the modes accumulated as
-// Sa = sum a_n, Sb = sum b_n, Sc = sum c_n and the (linear) orientation,
-// rotation and antenna factors applied once per sample.  The Bessel values
-// come from the tile table (K > 0) or a per-sample recurrence (K == 0).
-__device__ void harmonic_sum_fp64(const SourceDesc &d, const int32_t *bstart, const double *tab, double ec, int K,
-                                  double t, double e, double om_M, double gim, double Phi, double alp, double nu,
-                                  double gimdot, double &hI, double &hII) {
-  double sa, ca, s2g, c2g, so = 0.0, co = 1.0;
-  sincos(alp, &sa, &ca);
-  sincos(2. * gim, &s2g, &c2g);
-  if (d.mich) sincos(kTwoPi * t / kYear, &so, &co);
-  const Resp<double> R = response<double>(d, ca, sa, c2g, s2g, co, so);
-  const double Amp = pow(om_M, 2. / 3.) * d.zeta;
-
-  // harmonic phases: n Phi + Doppler_n = n (Phi + D1) + D0
-  double D1 = 0.0, D0 = 0.0;
-  if (d.mich) {
-    D1 = kTwoPi * nu * kAUsec * d.sinqS * R.cosorb_S;
-    D0 = 2.0 * gimdot * kAUsec * d.sinqS * R.cosorb_S;
-  }
-  double s1, c1, sD, cD;
-  sincos(Phi + D1, &s1, &c1);  // harmonic n: (c1 + i s1)^n (cD + i sD)
-  sincos(D0, &sD, &cD);
-  const double se = sqrt(1. - e * e);
-  double Sa, Sb, Sc;
-  const double dl = e - ec;
-  switch (K) {
-    case 4: mode_sums_taylor<4, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 5: mode_sums_taylor<5, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 6: mode_sums_taylor<6, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 8: mode_sums_taylor<8, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    case 10: mode_sums_taylor<10, double>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    default: mode_sums_miller(bstart, d.nmodes, e, c1, s1, cD, sD, Sa, Sb, Sc); break;
-  }
-  const double a = -Amp * Sa, b = -Amp * se * Sb, cc = 2. * Amp * Sc;
-  hI = R.caI * a + R.cbI * b + R.ccI * cc;
-  hII = R.caII * a + R.cbII * b + R.ccII * cc;
-}
 
 // ------------------------------------------------------------------ split precision
 // FP64: spline, rates, phase sums and every angle reduction; FP32: geometry,
 // antenna response, Bessel evaluation and the harmonic recurrence.
 
 
-// h_I, h_II at one sample in split precision: the angle reductions in FP64,
-// the trigonometry, response and harmonic sums in FP32 (same algebra as
-// harmonic_sum_fp64).
-__device__ void harmonic_sum_split(const SourceDesc &d, const int32_t *bstart, const float *tab, double ec, int K,
-                                   double t, double e_d, double om_M, double gim, double Phi, double alp, double nu,
-                                   double gimdot, double &hI, double &hII) {
-  float sa, ca, s2g, c2g, so = 0.f, co = 1.f;
-  __sincosf(reduce_2pi_f(alp), &sa, &ca);
-  __sincosf(reduce_2pi_f(2.0 * gim), &s2g, &c2g);
-  if (d.mich) __sincosf(reduce_2pi_f(kTwoPi * t / kYear), &so, &co);
-  const Resp<float> R = response<float>(d, ca, sa, c2g, s2g, co, so);
-  const float Amp = exp2f((2.f / 3.f) * __log2f((float)om_M)) * (float)d.zeta;
-  // harmonic phases: n (Phi + D1) + D0, reduced in FP64
-  double D1 = 0.0;
-  float D0 = 0.f;
-  if (d.mich) {
-    D1 = kTwoPi * nu * kAUsec * d.sinqS * (double)R.cosorb_S;
-    D0 = (float)(2.0 * gimdot * kAUsec * d.sinqS) * R.cosorb_S;
-  }
-  float s1, c1, sD, cD;
-  __sincosf(reduce_2pi_f(Phi + D1), &s1, &c1);
-  __sincosf(D0, &sD, &cD);
-  const float e = (float)e_d;
-  float Sa, Sb, Sc;
-  if (K > 0) {
-    const float dl = (float)(e_d - ec);
-    switch (K) {
-      case 2: mode_sums_taylor<2, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-      case 3: mode_sums_taylor<3, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-      case 4: mode_sums_taylor<4, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-      default: mode_sums_taylor<6, float>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-    }
-  } else {
-    double sa64, sb64, sc64;
-    mode_sums_miller(bstart, d.nmodes, e_d, c1, s1, cD, sD, sa64, sb64, sc64);
-    Sa = (float)sa64;
-    Sb = (float)sb64;
-    Sc = (float)sc64;
-  }
-  const float se = sqrtf(1.f - e * e);
-  const float a = -Amp * Sa, b = -Amp * se * Sb, cc = 2.f * Amp * Sc;
-  hI = (double)(R.caI * a + R.cbI * b + R.ccI * cc);
-  hII = (double)(R.caII * a + R.cbII * b + R.ccII * cc);
-}
 
 // ------------------------------------------------------------------ pass 2
 // Samples per thread whose harmonic sums run side by side (divides kTileChunks).
@@ -1128,6 +1039,8 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   __shared__ double s_r[3][kTileThreads];
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
+  __shared__ __align__(16) SourceDesc s_desc;           // this tile's source
+  __shared__ Geom<typename std::conditional<kSplit, float, double>::type> s_geom;
   __shared__ double s_wt[kWin];
   __shared__ double4 s_wy[kWin], s_wc[kWin], s_wb[kWin], s_wd[kWin];
   double *sv_e = s_dyn, *sv_om = s_dyn + kTileSamples, *sv_gim = s_dyn + 2 * kTileSamples;
@@ -1144,25 +1057,33 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     if (g >= bv.total_tiles) break;
     const SourceDesc *dp;
     const TileCtx c = tile_ctx(bv, g, dp);
-    const SourceDesc &d = *dp;
-    const int32_t *bstart = bv.bessel_start + d.bessel_offset;
     const TileCarry &tc = bv.carry[g];
     const TileSummary &ts = bv.summ[g];
-    const double X0[3] = {d.gim0, d.Phi0, d.alp0};
-    if (d.status != 0 || min(c.end, c.neff) <= c.start) {
+    if (dp->status != 0 || min(c.end, c.neff) <= c.start) {
       // failed source, or a tile entirely after the taper: zeros
+      const SourceDesc &dz = *dp;
       for (int ch = 0; ch < kTileChunks; ++ch) {
         const int i = c.start + ch * kTileThreads + tid;
         if (i < c.end) {
-          bv.hI[d.out_offset + i] = 0.0;
-          bv.hII[d.out_offset + i] = 0.0;
-          if (bv.t_out) bv.t_out[d.out_offset + i] = (d.status != 0) ? 0.0 : sample_time(d, i);
+          bv.hI[dz.out_offset + i] = 0.0;
+          bv.hII[dz.out_offset + i] = 0.0;
+          if (bv.t_out) bv.t_out[dz.out_offset + i] = (dz.status != 0) ? 0.0 : sample_time(dz, i);
         }
       }
       continue;
     }
+    // stage the source record and its response constants (the window's barrier publishes them)
+    {
+      const uint4 *src4 = reinterpret_cast<const uint4 *>(dp);
+      uint4 *dst4 = reinterpret_cast<uint4 *>(&s_desc);
+      for (int k = tid; k < (int)(sizeof(SourceDesc) / 16); k += kTileThreads) dst4[k] = src4[k];
+      if (tid == kTileThreads - 1) make_geom(*dp, s_geom);
+    }
     KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
-    load_window(bv, d, g, w);
+    load_window(bv, *dp, g, w);
+    const SourceDesc &d = s_desc;
+    const int32_t *bstart = bv.bessel_start + d.bessel_offset;
+    const double X0[3] = {d.gim0, d.Phi0, d.alp0};
     // boundary rate and Bessel-table parameters recorded by pass 1
     const int K = kSplit ? ts.k32 : ts.k64;
     const double ec = ts.ec;
@@ -1307,10 +1228,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
         const int sl = (g0 + m) * kTileThreads + tid;
         if (i < c.end && i < c.neff) {
           if constexpr (kSplit)
-            P[m] = prep_split(d, ec, sample_time(d, i), sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+            P[m] = prep_split(d, s_geom, ec, sample_time(d, i), sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
                               sv_nu[sl], sv_gd[sl]);
           else
-            P[m] = prep_fp64(d, ec, sample_time(d, i), sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
+            P[m] = prep_fp64(d, s_geom, ec, sample_time(d, i), sv_e[sl], sv_om[sl], sv_gim[sl], sv_Phi[sl], sv_alp[sl],
                              sv_nu[sl], sv_gd[sl]);
         } else {
           P[m] = SamplePrep<T>{};
