@@ -55,6 +55,55 @@ struct DevBuf {
 
 int cuda_ok(cudaError_t e) { return cuda_status_of(e); }
 
+// Host array for the packed plan: page-locked when a device is in use (the
+// upload then runs at full PCIe rate), capacity kept across plans, resized
+// without value-initialisation.
+template <typename T>
+struct HostBuf {
+  T *p = nullptr;
+  size_t n = 0, cap = 0;
+  bool pinned = false;
+  bool want_pinned = true;
+  HostBuf() = default;
+  HostBuf(const HostBuf &) = delete;
+  HostBuf &operator=(const HostBuf &) = delete;
+  ~HostBuf() { release(); }
+  int resize(size_t m) {
+    if (m <= cap && p) {
+      n = m;
+      return AAK_OK;
+    }
+    release();
+    const size_t want = std::max<size_t>(m + m / 8, 1);
+    void *q = nullptr;
+    if (want_pinned && cudaHostAlloc(&q, want * sizeof(T), cudaHostAllocPortable) == cudaSuccess) {
+      pinned = true;
+    } else {
+      cudaGetLastError();
+      q = std::malloc(want * sizeof(T));
+      pinned = false;
+      if (!q) return AAK_ERR_NO_MEMORY;
+    }
+    p = static_cast<T *>(q);
+    cap = want;
+    n = m;
+    return AAK_OK;
+  }
+  void release() {
+    if (p) {
+      if (pinned) cudaFreeHost(p);
+      else std::free(p);
+    }
+    p = nullptr;
+    n = cap = 0;
+  }
+  T *data() { return p; }
+  const T *data() const { return p; }
+  size_t size() const { return n; }
+  T &operator[](size_t i) { return p[i]; }
+  const T &operator[](size_t i) const { return p[i]; }
+};
+
 }  // namespace
 
 struct aak_ctx {
@@ -69,8 +118,8 @@ struct aak_ctx {
   std::vector<int64_t> tile_start;
   std::vector<int64_t> tile_pairs;  // per source {0, its tiles}: the tile prefix of a one-source view
   std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
-  std::vector<double> knot_t;
-  std::vector<double4> knot_y, knot_c;
+  HostBuf<double> knot_t;
+  HostBuf<double4> knot_y, knot_c;
   std::vector<int32_t> bessel;
   int64_t total_samples = 0, total_tiles = 0, total_knots = 0;
   int32_t max_nmodes = 0;
@@ -165,7 +214,7 @@ void from_mapped(const aak_mapped &o, MappedTrajectory *m) {
 
 
 // Pack per-source plans into the flat arrays the kernels read.
-void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
+int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
   const int n = ctx->nsrc;
   ctx->offsets.assign(n + 1, 0);
   ctx->tile_start.assign(n + 1, 0);
@@ -187,16 +236,28 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
   ctx->total_samples = ctx->offsets[n];
   ctx->total_tiles = ctx->tile_start[n];
   ctx->total_knots = knots;
-  ctx->knot_t.resize(std::max<int64_t>(knots, 1));
-  ctx->knot_y.resize(std::max<int64_t>(knots, 1));
-  ctx->knot_c.resize(std::max<int64_t>(knots, 1));
+  int r;
+  if ((r = ctx->knot_t.resize(std::max<int64_t>(knots, 1))) || (r = ctx->knot_y.resize(std::max<int64_t>(knots, 1))) ||
+      (r = ctx->knot_c.resize(std::max<int64_t>(knots, 1))))
+    return r;
   ctx->bessel.resize(std::max<int64_t>(bes, 1));
-  int64_t ko = 0, bo = 0;
+  // per-source offsets into the flat arrays, then the copies in parallel
+  std::vector<int64_t> kofs(n + 1, 0), bofs(n + 1, 0);
   for (int s = 0; s < n; ++s) {
+    const bool ok = ctx->status[s] == AAK_OK;
+    kofs[s + 1] = kofs[s] + (ok ? (int64_t)ctx->plans[s].knot_t.size() : 0);
+    bofs[s + 1] = bofs[s] + (ok ? ctx->plans[s].nmodes : 0);
+  }
+  ctx->tile_pairs.assign(2 * (size_t)n, 0);
+  for (int s = 0; s < n; ++s) ctx->tile_pairs[2 * s + 1] = ctx->tile_start[s + 1] - ctx->tile_start[s];
+  ctx->tile_knot.assign(2 * std::max<int64_t>(ctx->total_tiles, 1), 0);
+  parallel_for(n, nthreads, [&](int64_t s64) {
+    const int s = (int)s64;
     SourceDesc d;
     const SourcePlan &pl = ctx->plans[s];
     if (ctx->status[s] == AAK_OK) {
       d = pl.desc;
+      const int64_t ko = kofs[s], bo = bofs[s];
       const int64_t nk = (int64_t)pl.knot_t.size();
       for (int64_t k = 0; k < nk; ++k) {
         ctx->knot_t[ko + k] = pl.knot_t[k];
@@ -206,8 +267,6 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
       d.knot_offset = ko;
       d.bessel_offset = (int32_t)bo;
       for (int m = 1; m <= pl.nmodes; ++m) ctx->bessel[bo + m - 1] = bessel_start_order(m, pl.e_max, 12);  // table rows reach order n + 2 + 12
-      ko += nk;
-      bo += pl.nmodes;
     } else {
       std::memset(&d, 0, sizeof(d));
       d.status = ctx->status[s];
@@ -217,14 +276,8 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
     d.tile_offset = ctx->tile_start[s];
     d.n_tiles = (int32_t)(ctx->tile_start[s + 1] - ctx->tile_start[s]);
     ctx->descs[s] = d;
-  }
-  ctx->tile_pairs.assign(2 * (size_t)n, 0);
-  for (int s = 0; s < n; ++s) ctx->tile_pairs[2 * s + 1] = ctx->tile_start[s + 1] - ctx->tile_start[s];
-  // knot window of every tile: knots bracketing samples start-1 .. start+1024
-  ctx->tile_knot.assign(2 * std::max<int64_t>(ctx->total_tiles, 1), 0);
-  for (int s = 0; s < n; ++s) {
-    if (ctx->status[s] != AAK_OK) continue;
-    const SourceDesc &d = ctx->descs[s];
+    if (ctx->status[s] != AAK_OK) return;
+    // knot window of every tile: knots bracketing samples start-1 .. start+1024
     const double *kt = ctx->knot_t.data() + d.knot_offset;
     const int nk = d.n_knots;
     auto tsample = [&](int i) { return (i == 0) ? d.t_first : (double)(i - d.i0) * d.dt; };
@@ -239,8 +292,9 @@ void pack(aak_ctx *ctx, const std::vector<aak_params> &P) {
       ctx->tile_knot[2 * (d.tile_offset + t)] = k0;
       ctx->tile_knot[2 * (d.tile_offset + t) + 1] = k1 + 2 - k0;
     }
-  }
+  });
   ctx->uploaded = false;
+  return AAK_OK;
 }
 
 // Coarse AK evolution and knots of source s from its mapped trajectory.
@@ -266,7 +320,7 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   for (auto &p : Pv)
     if (p.length < 2 || p.length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
   ctx->nsrc = nsrc;
-  ctx->plans.assign(nsrc, SourcePlan());
+  ctx->plans.resize(nsrc);  // earlier plans keep their array capacity
   ctx->status.assign(nsrc, AAK_OK);
   ctx->newton_points = ctx->newton_iters = ctx->newton_fallbacks = 0;
   if (maps) {
@@ -277,8 +331,7 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
       if (st == kOk) from_mapped(maps[s], &mt);
       finish_source(ctx, (int)s, Pp, mt, nm, st);
     });
-    pack(ctx, Pv);
-    return AAK_OK;
+    return pack(ctx, Pv, nthreads);
   }
   // (1) coarse Kerr inspiral and Kerr frequencies
   std::vector<CoarseKerr> ck(nsrc);
@@ -329,8 +382,7 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   ctx->newton_points = points;
   ctx->newton_iters = iters;
   ctx->newton_fallbacks = fallbacks;
-  pack(ctx, Pv);
-  return AAK_OK;
+  return pack(ctx, Pv, nthreads);
 }
 
 int upload(aak_ctx *ctx, cudaStream_t st) {
@@ -356,6 +408,9 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
       (r = cp(ctx->d_knot_c.ptr, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
       (r = cp(ctx->d_bessel.ptr, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
     return r;
+  // copies from page-locked memory run asynchronously: finish them before the
+  // host arrays can be refilled by the next plan
+  if (ctx->knot_t.pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
   ctx->uploaded = true;
   return AAK_OK;
 }
@@ -538,6 +593,7 @@ int aak_ctx_create(int32_t device, aak_ctx **out) {
   aak_ctx *c = new (std::nothrow) aak_ctx();
   if (!c) return AAK_ERR_NO_MEMORY;
   c->device = device;
+  c->knot_t.want_pinned = c->knot_y.want_pinned = c->knot_c.want_pinned = device >= 0;
   int sms = 0;
   if (device >= 0 && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
     c->num_sms = sms;
@@ -673,6 +729,7 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
       (r = cp(o_kc, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
       (r = cp(o_bs, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
     return r;
+  if (ctx->knot_t.pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;  // host arrays reusable on return
   BatchView bv;
   std::memset(&bv, 0, sizeof(bv));
   bv.src = reinterpret_cast<const SourceDesc *>(base);

@@ -288,6 +288,33 @@ void spline_second_derivs(const double *x, const double *y, int n, int stride, d
   for (int k = 0; k < m; ++k) c[(k + 1) * stride] = dp[k];
 }
 
+void spline_second_derivs4(const double *x, const double *y, int n, double *c) {
+  for (int k = 0; k < 4 * n; ++k) c[k] = 0.0;
+  if (n < 3) return;
+  const int m = n - 2;
+  std::vector<double> cp(m), dp(4 * (size_t)m);
+  double inv_h0 = 1.0 / (x[1] - x[0]);
+  for (int k = 0; k < m; ++k) {
+    const int i = k + 1;
+    const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
+    const double inv_h1 = 1.0 / h1;
+    const double sup = (k + 1 < m) ? h1 : 0.0;
+    const double den = (k == 0) ? 2.0 * (h0 + h1) : 2.0 * (h0 + h1) - h0 * cp[k - 1];
+    const double inv = 1.0 / den;
+    cp[k] = sup * inv;
+    for (int q = 0; q < 4; ++q) {
+      const double rhs =
+          3.0 * ((y[4 * (i + 1) + q] - y[4 * i + q]) * inv_h1 - (y[4 * i + q] - y[4 * (i - 1) + q]) * inv_h0);
+      dp[4 * (size_t)k + q] = (k == 0) ? rhs * inv : (rhs - h0 * dp[4 * (size_t)(k - 1) + q]) * inv;
+    }
+    inv_h0 = inv_h1;
+  }
+  for (int k = m - 2; k >= 0; --k)
+    for (int q = 0; q < 4; ++q) dp[4 * (size_t)k + q] -= cp[k] * dp[4 * (size_t)(k + 1) + q];
+  for (int k = 0; k < m; ++k)
+    for (int q = 0; q < 4; ++q) c[4 * (size_t)(k + 1) + q] = dp[4 * (size_t)k + q];
+}
+
 double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv) {
   int lo = 0, hi = n - 1;
   while (hi > lo + 1) {
@@ -323,14 +350,16 @@ int bessel_start_order(int n, double e_max, int extra) {
 
 // ------------------------------------------------------------------ coarse AK evolution
 namespace {
-double dvdt(double v, double e, double Y, double m, double M, double q) {
+// dv/dt and de/dt of the AK equations (KSParMap.cc:86-144); lv = log(v) and
+// ome15 = (1 - e^2)^1.5 are shared by the two.
+double dvdt_core(double v, double e, double Y, double m, double M, double q, double lv, double ome15) {
   const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
   const double e2 = e * e, e4 = e2 * e2, e6 = e4 * e2;
   const double Y2 = Y * Y, q2 = q * q;
   const double l2 = std::log(2.), l3 = std::log(3.), l5 = std::log(5.);
-  double s = 1. + 7. * e2 / 8.;
-  s += (-5944. - 7040. * e2 + 8539. * e4) * v2 / 2688.;
-  s -= v3 * ((-18432. - 55872. * e2 - 7056. * e4 + 49. * e6) * kPi + 48. * (1064. + 1516. * e2 + 475. * e4) * q * Y) / 4608.;
+  double s = 1. + 7. * e2 * (1. / 8.);
+  s += (-5944. - 7040. * e2 + 8539. * e4) * v2 * (1. / 2688.);
+  s -= v3 * ((-18432. - 55872. * e2 - 7056. * e4 + 49. * e6) * kPi + 48. * (1064. + 1516. * e2 + 475. * e4) * q * Y) * (1. / 4608.);
   s += v3 * v2 *
        ((-4791168. - 28113984. * e2 + 12239226. * e4 + 4005097. * e6) * kPi -
         144. * (139296. + 58408. * e2 + 249968. * e4 + 106707. * e6) * q * Y) /
@@ -339,21 +368,21 @@ double dvdt(double v, double e, double Y, double m, double M, double q) {
        (953325. * e6 + 8. * (34103. + 189. * q2 * (-329. + 815. * Y2)) + 12. * e2 * (-526955. + 126. * q2 * (-929. + 1431. * Y2)) +
         3. * e4 * (-1232809. + 63. * q2 * (-1051. + 2997. * Y2))) /
        145152.;
-  double c6 = 117.72574285227559 - 1712. * kEulerGamma / 105. + 16. * kPi2Trunc / 3. - 331. * q2 / 192. -
-              289. * kPi * q * Y / 6. + 145759. * q2 * Y2 / 1344. - 3424. * l2 / 105.;
-  c6 += e2 * (764.5906705662063 - 24503. * kEulerGamma / 210. + 229. * kPi2Trunc / 6. + 2129. * q2 / 42. -
-              4225. * kPi * q * Y / 24. + 27191. * q2 * Y2 / 224. + 1391. * l2 / 30. - 78003. * l3 / 280.);
-  c6 += e4 * (723.1604428881717 - 11663. * kEulerGamma / 140. + 109. * kPi2Trunc / 4. - 56239. * q2 / 10752. -
-              17113. * kPi * q * Y / 192. + 414439. * q2 * Y2 / 3584. - 418049. * l2 / 84. + 3042117. * l3 / 1120.);
-  c6 += e6 * (202.0979603432282 - 2461. * kEulerGamma / 560. + 23. * kPi2Trunc / 16. - 3571. * q2 / 3584. -
-              108577. * kPi * q * Y / 13824. + 41071. * q2 * Y2 / 1536. + 94138279. * l2 / 2160. - 42667641. * l3 / 3584. -
-              1044921875. * l5 / 96768.);
-  c6 -= 107. * (256. + 1832. * e2 + 1308. * e4 + 69. * e6) * std::log(v) / 1680.;
+  double c6 = 117.72574285227559 - 1712. * kEulerGamma * (1. / 105.) + 16. * kPi2Trunc * (1. / 3.) - 331. * q2 * (1. / 192.) -
+              289. * kPi * q * Y * (1. / 6.) + 145759. * q2 * Y2 * (1. / 1344.) - 3424. * l2 * (1. / 105.);
+  c6 += e2 * (764.5906705662063 - 24503. * kEulerGamma * (1. / 210.) + 229. * kPi2Trunc * (1. / 6.) + 2129. * q2 * (1. / 42.) -
+              4225. * kPi * q * Y * (1. / 24.) + 27191. * q2 * Y2 * (1. / 224.) + 1391. * l2 * (1. / 30.) - 78003. * l3 * (1. / 280.));
+  c6 += e4 * (723.1604428881717 - 11663. * kEulerGamma * (1. / 140.) + 109. * kPi2Trunc * (1. / 4.) - 56239. * q2 * (1. / 10752.) -
+              17113. * kPi * q * Y * (1. / 192.) + 414439. * q2 * Y2 * (1. / 3584.) - 418049. * l2 * (1. / 84.) + 3042117. * l3 * (1. / 1120.));
+  c6 += e6 * (202.0979603432282 - 2461. * kEulerGamma * (1. / 560.) + 23. * kPi2Trunc * (1. / 16.) - 3571. * q2 * (1. / 3584.) -
+              108577. * kPi * q * Y * (1. / 13824.) + 41071. * q2 * Y2 * (1. / 1536.) + 94138279. * l2 * (1. / 2160.) - 42667641. * l3 * (1. / 3584.) -
+              1044921875. * l5 * (1. / 96768.));
+  c6 -= 107. * (256. + 1832. * e2 + 1308. * e4 + 69. * e6) * lv * (1. / 1680.);
   s += v6 * c6;
-  return 32. * std::pow(1. - e2, 1.5) * m * v6 * v3 * s / (5. * M * M);
+  return 32. * ome15 * m * v6 * v3 * s / (5. * M * M);
 }
 
-double dedt(double v, double e, double Y, double m, double M, double q) {
+double dedt_core(double v, double e, double Y, double m, double M, double q, double lv, double ome15) {
   const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
   const double e2 = e * e, e4 = e2 * e2;
   const double Y2 = Y * Y, q2 = q * q;
@@ -365,16 +394,23 @@ double dedt(double v, double e, double Y, double m, double M, double q) {
   s += 8. * v2 * v2 *
        (6. * e2 * (-2070667. + 126. * q2 * (-2975. + 4009. * Y2)) + 8. * (-286397. + 63. * q2 * (-3179. + 5869. * Y2)) +
         e4 * (-3506201. + 63. * q2 * (-3191. + 9009. * Y2)));
-  double c6 = 241.02948298890263 - 82283. * kEulerGamma / 1995. + 769. * kPi2Trunc / 57. + 180255. * q2 / 8512. -
-              11809. * kPi * q * Y / 152. + 598987. * q2 * Y2 / 8512. - 11021. * l2 / 285. - 234009. * l3 / 5320.;
-  c6 += e2 * (1048.5728116817568 - 297674. * kEulerGamma / 1995. + 2782. * kPi2Trunc / 57. + 536653. * q2 / 8512. -
-              91375. * kPi * q * Y / 608. + 356845. * q2 * Y2 / 8512. - 2982946. * l2 / 1995. + 1638063. * l3 / 3040.);
-  c6 += e4 * (725.9069951397873 - 1147147. * kEulerGamma / 15960. + 10721. * kPi2Trunc / 456. + 56509. * q2 / 9728. -
-              1739605. * kPi * q * Y / 29184. + 3248951. * q2 * Y2 / 68096. + 760314287. * l2 / 47880. -
-              1022385321. * l3 / 340480. - 1044921875. * l5 / 204228.);
-  c6 -= 107. * (6152. + 22256. * e2 + 10721. * e4) * std::log(v) / 15960.;
+  double c6 = 241.02948298890263 - 82283. * kEulerGamma * (1. / 1995.) + 769. * kPi2Trunc * (1. / 57.) + 180255. * q2 * (1. / 8512.) -
+              11809. * kPi * q * Y * (1. / 152.) + 598987. * q2 * Y2 * (1. / 8512.) - 11021. * l2 * (1. / 285.) - 234009. * l3 * (1. / 5320.);
+  c6 += e2 * (1048.5728116817568 - 297674. * kEulerGamma * (1. / 1995.) + 2782. * kPi2Trunc * (1. / 57.) + 536653. * q2 * (1. / 8512.) -
+              91375. * kPi * q * Y * (1. / 608.) + 356845. * q2 * Y2 * (1. / 8512.) - 2982946. * l2 * (1. / 1995.) + 1638063. * l3 * (1. / 3040.));
+  c6 += e4 * (725.9069951397873 - 1147147. * kEulerGamma * (1. / 15960.) + 10721. * kPi2Trunc * (1. / 456.) + 56509. * q2 * (1. / 9728.) -
+              1739605. * kPi * q * Y * (1. / 29184.) + 3248951. * q2 * Y2 * (1. / 68096.) + 760314287. * l2 * (1. / 47880.) -
+              1022385321. * l3 * (1. / 340480.) - 1044921875. * l5 * (1. / 204228.));
+  c6 -= 107. * (6152. + 22256. * e2 + 10721. * e4) * lv * (1. / 15960.);
   s += 2451456. * v6 * c6;
-  return -(e * std::pow(1. - e2, 1.5) * m * v6 * v2 * s) / (120960. * M * M);
+  return -(e * ome15 * m * v6 * v2 * s) / (120960. * M * M);
+}
+
+void ak_rates(double v, double e, double Y, double m, double M, double q, double *edot, double *vdot) {
+  const double ome = 1. - e * e;
+  const double lv = std::log(v), ome15 = ome * std::sqrt(ome);
+  *edot = dedt_core(v, e, Y, m, M, q, lv, ome15);
+  *vdot = dvdt_core(v, e, Y, m, M, q, lv, ome15);
 }
 
 // Two-term least squares of y[i+1]-y[0] on (x[i+1]-x[0], (x[i+1]-x[0])^2)
@@ -399,9 +435,23 @@ void polyfit(double *coeff, const double *x, const double *y, int n) {
   coeff[1] = (double)(((a11 * b2 - a12 * b1) / det) / s2);
 }
 
+// Semi-latus rectum from the AK azimuthal frequency: (1 - e^2) (Omega_phi M_phys)^(-2/3)
+// (AAK.cc:157-170), with Omega_phi's two PN ratios taken with one division.
 inline double p_of(double v, double e, double coslam, double S, double M, double M_phys) {
-  return (1. - e * e) * std::pow(omega_phi(v, e, coslam, S, M) * M_phys * kMsunSec, -2. / 3.);
+  double om;
+  if (coslam > 0) om = 16. * (v * v * v) * pn_dphidm_num(v, e, coslam, S) / (pn_dtdm_num(v, e, coslam, S) * M);
+  else om = omega_phi(v, e, coslam, S, M);
+  const double c = std::cbrt(om * M_phys * kMsunSec);
+  return (1. - e * e) / (c * c);
 }
+
+// Strided view of an array indexed by the global step j (first index base).
+struct Win {
+  double *p;
+  int base;
+  int stride;
+  double &operator[](int j) const { return p[(size_t)(j - base) * stride]; }
+};
 }  // namespace
 
 // Per-source constants of the waveform geometry (the alpha-independent
@@ -459,8 +509,19 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   const int j0 = (int)j0d;
   int j_start = j0, j_min = j_start, j_end = 2 * j0 - 1, j_max = j_end, j_max_temp = j_max;
   double t_end = vlength * timestep;
-  const size_t nA = (size_t)(2 * j0);
-  std::vector<double> e_AK(nA), v_AK(nA), t_fit(nA), e_fit(nA), v_fit(nA), M_fit(nA), S_fit(nA);
+  // Index window of the arrays: without backward integration only j >= j0 is
+  // ever touched.  The fitted (t, e, v, M, S) are written straight into the
+  // plan's knot arrays; the AK scratch is kept per host thread.
+  const int jb = w.backint ? 0 : j0;
+  const size_t L = (size_t)(2 * j0 - jb);
+  static thread_local std::vector<double> ak_scratch;
+  if (ak_scratch.size() < 2 * L) ak_scratch.resize(2 * L);
+  plan->knot_t.resize(L);
+  plan->knot_y.resize(4 * L);
+  const Win e_AK{ak_scratch.data(), jb, 1}, v_AK{ak_scratch.data() + L, jb, 1};
+  const Win t_fit{plan->knot_t.data(), jb, 1};
+  const Win e_fit{plan->knot_y.data() + 0, jb, 4}, v_fit{plan->knot_y.data() + 1, jb, 4};
+  const Win M_fit{plan->knot_y.data() + 2, jb, 4}, S_fit{plan->knot_y.data() + 3, jb, 4};
   double edot = 0, vdot = 0, edotm, vdotm;
 
   // AB2 of the AK equations over the fit window
@@ -469,8 +530,7 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   for (int j = j0; j < j0 + steps - 1; ++j) {
     edotm = edot;
     vdotm = vdot;
-    edot = dedt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
-    vdot = dvdt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+    ak_rates(v_AK[j], e_AK[j], coslam, mu, M0, S0, &edot, &vdot);
     if (j == j0) {
       edotm = edot;
       vdotm = vdot;
@@ -505,8 +565,7 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   for (int j = j0 + steps - 1; j < j_end; ++j) {
     edotm = edot;
     vdotm = vdot;
-    edot = dedt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
-    vdot = dvdt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+    ak_rates(v_AK[j], e_AK[j], coslam, mu, M0, S0, &edot, &vdot);
     e_AK[j + 1] = e_AK[j] + (1.5 * edot - .5 * edotm) * dt_large;
     v_AK[j + 1] = v_AK[j] + (1.5 * vdot - .5 * vdotm) * dt_large;
     if (e_AK[j + 1] < 0. || v_AK[j + 1] < v_AK[j] || std::isnan(e_AK[j + 1]) || std::isnan(v_AK[j + 1])) {
@@ -576,8 +635,7 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
     for (int j = j0; j > j_start; --j) {
       edotp = edot;
       vdotp = vdot;
-      edot = dedt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
-      vdot = dvdt(v_AK[j], e_AK[j], coslam, mu, M0, S0);
+      ak_rates(v_AK[j], e_AK[j], coslam, mu, M0, S0, &edot, &vdot);
       if (j == j0) {
         edotp = edot;
         vdotp = vdot;
@@ -597,21 +655,19 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
     }
   }
 
-  // knots and natural-spline coefficients of (e, v, M, S)
+  // knots [j_start, j_end] and natural-spline coefficients of (e, v, M, S)
   const int n_in = j_end - j_start + 1;
-  plan->knot_t.assign(t_fit.begin() + j_start, t_fit.begin() + j_end + 1);
-  plan->knot_y.resize((size_t)n_in * 4);
-  plan->knot_c.resize((size_t)n_in * 4);
-  double e_max = 0.0;
-  for (int k = 0; k < n_in; ++k) {
-    plan->knot_y[4 * k + 0] = e_fit[j_start + k];
-    plan->knot_y[4 * k + 1] = v_fit[j_start + k];
-    plan->knot_y[4 * k + 2] = M_fit[j_start + k];
-    plan->knot_y[4 * k + 3] = S_fit[j_start + k];
-    e_max = std::max(e_max, e_fit[j_start + k]);
+  const size_t off = (size_t)(j_start - jb);
+  if (off > 0) {
+    std::memmove(plan->knot_t.data(), plan->knot_t.data() + off, (size_t)n_in * sizeof(double));
+    std::memmove(plan->knot_y.data(), plan->knot_y.data() + 4 * off, 4 * (size_t)n_in * sizeof(double));
   }
-  for (int q = 0; q < 4; ++q)
-    spline_second_derivs(plan->knot_t.data(), plan->knot_y.data() + q, n_in, 4, plan->knot_c.data() + q);
+  plan->knot_t.resize(n_in);
+  plan->knot_y.resize(4 * (size_t)n_in);
+  plan->knot_c.resize(4 * (size_t)n_in);
+  double e_max = 0.0;
+  for (int k = 0; k < n_in; ++k) e_max = std::max(e_max, plan->knot_y[4 * (size_t)k]);
+  spline_second_derivs4(plan->knot_t.data(), plan->knot_y.data(), n_in, plan->knot_c.data());
 
   const int i0 = vlength - (int)(t_end / timestep);
   plan->vlength = vlength;

@@ -125,6 +125,8 @@ void fill_geometry(SourceDesc *d);
 
 // Natural cubic spline helpers (shared by the plan and tests).
 void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c);
+// The same for the four interleaved series y[n][4] (one factorisation): c[n][4].
+void spline_second_derivs4(const double *x, const double *y, int n, double *c);
 double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv);
 
 // Miller start order for J_{n-2..n+2+extra}(n e) accurate to ~1e-17 for all e <= e_max.
