@@ -198,6 +198,15 @@ class WaveBatch:
     def launches(self) -> int:
         return int(lib().aak_batch_last_launches(self._ctx))
 
+    def run_graph(self, hI_ptr: int, hII_ptr: int, precision: int = 0, stream: int = 0):
+        """:meth:`run` as one CUDA graph (captured on first use, replayed after)."""
+        check(lib().aak_batch_run_graph(self._ctx, ctypes.c_void_p(hI_ptr), ctypes.c_void_p(hII_ptr), int(precision),
+                                        ctypes.c_void_p(stream)), "aak_batch_run_graph")
+
+    def set_precision(self, precision: int):
+        """Precision of :meth:`generate_host` (0: FP64, 1: split)."""
+        check(lib().aak_ctx_set_precision(self._ctx, int(precision)), "aak_ctx_set_precision")
+
     def run_plain(self, hI_ptr: int, hII_ptr: int, traj_ptr: int, traj_stride: int, stream: int = 0):
         """The plain FP64 per-source path (baseline): one source at a time, dense
         trajectory in ``traj_ptr`` (9 x traj_stride doubles), five jn() per harmonic."""

@@ -139,6 +139,15 @@ struct aak_ctx {
   int last_launches = 0;
   bool profile = false;
   aak_mlp *model = nullptr;  // learned warm start of the map (optional)
+  int precision = 0;         // precision of the host-buffer entry points
+  uint64_t upload_gen = 0;   // bumped by every upload (device buffers may move)
+  // CUDA graph of the three dense launches for fixed outputs / precision / upload
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t cap_stream = nullptr;
+  double *g_hI = nullptr, *g_hII = nullptr;
+  int g_prec = -1;
+  uint64_t g_gen = ~0ull;
   int64_t newton_points = 0, newton_iters = 0, newton_fallbacks = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::mutex mu;
@@ -412,8 +421,11 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   // host arrays can be refilled by the next plan
   if (ctx->knot_t.pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
   ctx->uploaded = true;
+  ++ctx->upload_gen;
   return AAK_OK;
 }
+
+BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride);
 
 int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride, int precision,
         cudaStream_t st) {
@@ -423,6 +435,58 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   if (precision != 0 && precision != 1) return AAK_ERR_INVALID_PARAM;
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  const BatchView bv = batch_view(ctx, hI, hII, t, traj, traj_stride);
+  if (ctx->profile && !ctx->ev[0])
+    for (auto &e : ctx->ev) cudaEventCreate(&e);
+  launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
+  ctx->last_launches = 3;
+  return cuda_ok(cudaGetLastError());
+}
+
+void drop_graph(aak_ctx *ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->gexec = nullptr;
+  ctx->graph = nullptr;
+}
+
+// The three dense launches as one CUDA graph, captured on the first call for
+// a given (outputs, precision, upload) and replayed afterwards.
+int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t st) {
+  if (!ctx->uploaded || !hI || !hII || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  if (ctx->gexec && (ctx->g_hI != hI || ctx->g_hII != hII || ctx->g_prec != precision || ctx->g_gen != ctx->upload_gen))
+    drop_graph(ctx);
+  if (!ctx->gexec) {
+    if (!ctx->cap_stream && (r = cuda_ok(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking))) != AAK_OK)
+      return r;
+    prepare_dense_launch();
+    const BatchView bv = batch_view(ctx, hI, hII, nullptr, nullptr, 0);
+    if ((r = cuda_ok(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal))) != AAK_OK) return r;
+    launch_dense(bv, ctx->num_sms, ctx->cap_stream, nullptr, precision);
+    const cudaError_t launch_err = cudaGetLastError();
+    cudaGraph_t g = nullptr;
+    const cudaError_t end_err = cudaStreamEndCapture(ctx->cap_stream, &g);
+    if (launch_err != cudaSuccess || end_err != cudaSuccess || !g) {
+      if (g) cudaGraphDestroy(g);
+      return cuda_ok(launch_err != cudaSuccess ? launch_err : (end_err != cudaSuccess ? end_err : cudaErrorUnknown));
+    }
+    ctx->graph = g;
+    if ((r = cuda_ok(cudaGraphInstantiate(&ctx->gexec, ctx->graph, 0))) != AAK_OK) {
+      drop_graph(ctx);
+      return r;
+    }
+    ctx->g_hI = hI;
+    ctx->g_hII = hII;
+    ctx->g_prec = precision;
+    ctx->g_gen = ctx->upload_gen;
+  }
+  ctx->last_launches = 3;
+  return cuda_ok(cudaGraphLaunch(ctx->gexec, st));
+}
+
+BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride) {
   BatchView bv;
   bv.src = ctx->d_src.ptr;
   bv.nsrc = ctx->nsrc;
@@ -442,11 +506,7 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   bv.traj_stride = traj_stride;
   bv.work_counter = ctx->d_counter.ptr;
   bv.max_nmodes = ctx->max_nmodes;
-  if (ctx->profile && !ctx->ev[0])
-    for (auto &e : ctx->ev) cudaEventCreate(&e);
-  launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
-  ctx->last_launches = 3;
-  return cuda_ok(cudaGetLastError());
+  return bv;
 }
 
 // Plain FP64 per-source path: source by source, the phase kernels on a
@@ -517,7 +577,7 @@ int host_roundtrip(aak_ctx *ctx, double *t, double *hI, double *hII) {
   if ((r = upload(ctx, 0)) != AAK_OK) return r;
   if ((r = ctx->d_out.reserve((size_t)(t ? 3 : 2) * N)) != AAK_OK) return r;
   double *dI = ctx->d_out.ptr, *dII = dI + N, *dt = t ? dII + N : nullptr;
-  if ((r = run(ctx, dI, dII, dt, nullptr, 0, 0, 0)) != AAK_OK) return r;
+  if ((r = run(ctx, dI, dII, dt, nullptr, 0, ctx->precision, 0)) != AAK_OK) return r;
   if ((r = cuda_ok(cudaMemcpyAsync(hI, dI, N * sizeof(double), cudaMemcpyDeviceToHost, 0))) ||
       (r = cuda_ok(cudaMemcpyAsync(hII, dII, N * sizeof(double), cudaMemcpyDeviceToHost, 0))))
     return r;
@@ -618,6 +678,8 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_out.release();
     for (auto &e : c->ev)
       if (e) cudaEventDestroy(e);
+    drop_graph(c);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   }
   delete c;
 }
@@ -763,6 +825,29 @@ int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3) {
   for (int k = 0; k < 3; ++k)
     if (cudaEventElapsedTime(&ms3[k], ctx->ev[k], ctx->ev[k + 1]) != cudaSuccess) return cuda_ok(cudaGetLastError());
   return AAK_OK;
+}
+
+int aak_probe_fp32_tflops(int32_t device, double *tflops) {
+  if (!tflops) return AAK_ERR_INVALID_PARAM;
+  int r = select_device(device);
+  if (r != AAK_OK) return r;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  *tflops = probe_fp32_fma_tflops(sms, 20, 0);
+  return *tflops > 0 ? AAK_OK : AAK_ERR_CUDA;
+}
+
+int aak_ctx_set_precision(aak_ctx *ctx, int32_t precision) {
+  if (!ctx || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->precision = precision;
+  return AAK_OK;
+}
+
+int aak_batch_run_graph(aak_ctx *ctx, double *d_hI, double *d_hII, int32_t precision, void *stream) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return run_graph(ctx, d_hI, d_hII, precision, (cudaStream_t)stream);
 }
 
 int aak_probe_fp64_tflops(int32_t device, double *tflops) {

@@ -1416,19 +1416,7 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
   launch_dense(bv, num_sms, stream, ev, 0);
 }
 
-void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision) {
-  if (bv.total_tiles <= 0) return;
-  const int grid1 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 8);
-  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
-  if (ev) cudaEventRecord(ev[0], stream);
-  k_phase_tiles<<<grid1, kTileThreads, 0, stream>>>(bv);
-  if (ev) cudaEventRecord(ev[1], stream);
-  k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
-  if (ev) cudaEventRecord(ev[2], stream);
-  const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 4);
-  // per-sample values, then the Taylor table sized for the batch's harmonic count
-  const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
-  const size_t dyn = kWaveDynSmem + (size_t)rows * (precision == 1 ? kRowF * sizeof(float) : kRowD * sizeof(double));
+void prepare_dense_launch() {
   static std::atomic<unsigned long long> attrs_set{0};  // opt in to > 48 KB of shared memory once per device
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1439,6 +1427,27 @@ void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
     cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     attrs_set.fetch_or(bit);
   }
+}
+
+void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision) {
+  if (bv.total_tiles <= 0) return;
+  const int grid1 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 8);
+  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
+  if (ev) cudaEventRecord(ev[0], stream);
+  k_phase_tiles<<<grid1, kTileThreads, 0, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[1], stream);
+  k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[2], stream);
+  // per-sample values, then the Taylor table sized for the batch's harmonic count
+  const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
+  const size_t dyn = kWaveDynSmem + (size_t)rows * (precision == 1 ? kRowF * sizeof(float) : kRowD * sizeof(double));
+  prepare_dense_launch();
+  // persistent grid: every CTA that fits on the device at once
+  int resident = 0;
+  if (precision == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<true>, kTileThreads, dyn);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false>, kTileThreads, dyn);
+  resident = std::max(resident, 1);
+  const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
   if (precision == 1) k_waveform<true><<<grid2, kTileThreads, dyn, stream>>>(bv);
   else k_waveform<false><<<grid2, kTileThreads, dyn, stream>>>(bv);
   if (ev) cudaEventRecord(ev[3], stream);
@@ -1476,6 +1485,47 @@ double probe_fp64_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
   k_fp64_fma_probe<<<blocks, threads, 0, stream>>>(out, reps, 0.999999, 1e-7);  // warm-up
   cudaEventRecord(e0, stream);
   for (int i = 0; i < iters; ++i) k_fp64_fma_probe<<<blocks, threads, 0, stream>>>(out, reps, 0.999999, 1e-7);
+  cudaEventRecord(e1, stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  const double flops = 2.0 * 8.0 * 16.0 * reps * (double)blocks * threads * iters;
+  return cudaGetLastError() == cudaSuccess && ms > 0 ? flops / (ms * 1e-3) / 1e12 : -1.0;
+}
+
+namespace {
+// 8 independent FP32 FMA chains per thread.
+__global__ void __launch_bounds__(256) k_fp32_fma_probe(float *out, int reps, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-6f + k * 1e-6f;
+  for (int r = 0; r < reps; ++r) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) x[k] = fmaf(x[k], a, b);
+    }
+  }
+  float acc = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc += x[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+}  // namespace
+
+double probe_fp32_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
+  const int blocks = num_sms * 8, threads = 256, reps = 4096;
+  float *out = nullptr;
+  if (cudaMalloc(&out, (size_t)blocks * threads * sizeof(float)) != cudaSuccess) return -1.0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_fp32_fma_probe<<<blocks, threads, 0, stream>>>(out, reps, 0.999999f, 1e-7f);  // warm-up
+  cudaEventRecord(e0, stream);
+  for (int i = 0; i < iters; ++i) k_fp32_fma_probe<<<blocks, threads, 0, stream>>>(out, reps, 0.999999f, 1e-7f);
   cudaEventRecord(e1, stream);
   cudaEventSynchronize(e1);
   float ms = 0.f;

@@ -10,7 +10,10 @@
 namespace aak {
 
 constexpr int kTileThreads = 256;                      // threads per CTA
-constexpr int kTileChunks = 4;                         // 256-sample chunks per tile
+#ifndef AAK_TILE_CHUNKS
+#define AAK_TILE_CHUNKS 4
+#endif
+constexpr int kTileChunks = AAK_TILE_CHUNKS;           // 256-sample chunks per tile
 constexpr int kTileSamples = kTileThreads * kTileChunks;  // 1024 samples per tile
 
 // Per-tile partial sums of the Adams-Bashforth-2 phase increments written by
@@ -78,6 +81,12 @@ void launch_plain_waveform(const SourceDesc *src, int s, int vlength, const doub
 // Diagnostic: sustained FP64 FMA issue rate of this device in TFLOP/s
 // (2 flops per FMA), measured with CUDA events over `iters` launches.
 double probe_fp64_fma_tflops(int num_sms, int iters, cudaStream_t stream);
+// The same for FP32 FMA.
+double probe_fp32_fma_tflops(int num_sms, int iters, cudaStream_t stream);
+
+// Per-device launch set-up of the dense kernels (shared-memory opt-in); done
+// by launch_dense itself, and needed before capturing it into a CUDA graph.
+void prepare_dense_launch();
 
 // Largest batch (in 1024-sample tiles) the allocation-free launch accepts,
 // and the number of devices whose scratch address is cached.

@@ -187,6 +187,22 @@ int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3);
  * precision 0, to Bessel-evaluation rounding. */
 int aak_batch_run_plain(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_traj, int64_t traj_stride, void *stream);
 
+/* The same three launches as aak_batch_run (no t / trajectory outputs),
+ * captured into one CUDA graph on the first call for a given (d_hI, d_hII,
+ * precision, upload) and replayed on later calls; a new upload or other
+ * outputs recapture.  Capture runs on a stream of the context, so `stream`
+ * may be the legacy default stream.  No reference counterpart: the
+ * reference launches its kernels one by one with a device synchronisation
+ * after each (src/cuda/AAK_manager.cu:154-260). */
+int aak_batch_run_graph(aak_ctx *ctx, double *d_hI, double *d_hII, int32_t precision, void *stream);
+
+/* Precision of the host-buffer entry points of this context
+ * (aak_wave_batch_host): 0 = FP64 throughout (default), 1 = split. */
+int aak_ctx_set_precision(aak_ctx *ctx, int32_t precision);
+
+/* Diagnostic: sustained FP32 FMA rate of `device` in TFLOP/s (roofline denominator of the split path). */
+int aak_probe_fp32_tflops(int32_t device, double *tflops);
+
 /* Diagnostic: sustained FP64 FMA rate of `device` in TFLOP/s (roofline denominator). */
 int aak_probe_fp64_tflops(int32_t device, double *tflops);
 

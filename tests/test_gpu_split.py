@@ -83,3 +83,26 @@ def test_split_precision_configuration2_sample():
     assert np.sum(wb.status == 0) >= 20
     mm, rel = _compare(wb)
     print(f"configuration-2 sample: worst mismatch {mm:.2e}, worst max|dh|/max|h| {rel:.2e}")
+
+
+def test_graph_replay_matches_direct_launches():
+    gs = [load_golden(n) for n in golden_names()]
+    wb = E.WaveBatch(0)
+    wb.plan([g["pars"] for g in gs], nmodes=[int(g["nmodes"]) for g in gs], mapped=[golden_mapped(g) for g in gs])
+    for precision in (0, 1):
+        ref = _run(wb, precision)
+        N = wb.total_samples
+        hI = torch.full((N,), float("nan"), dtype=torch.float64, device="cuda")
+        hII = torch.full_like(hI, float("nan"))
+        for _ in range(2):  # capture, then replay
+            wb.run_graph(hI.data_ptr(), hII.data_ptr(), precision=precision)
+            torch.cuda.synchronize()
+            assert np.array_equal(hI.cpu().numpy(), ref[0]) and np.array_equal(hII.cpu().numpy(), ref[1])
+    # a new upload is picked up by the next replay
+    wb.plan([gs[0]["pars"]], nmodes=[int(gs[0]["nmodes"])], mapped=[golden_mapped(gs[0])])
+    ref = _run(wb, 1)
+    hI = torch.zeros(wb.total_samples, dtype=torch.float64, device="cuda")
+    hII = torch.zeros_like(hI)
+    wb.run_graph(hI.data_ptr(), hII.data_ptr(), precision=1)
+    torch.cuda.synchronize()
+    assert np.array_equal(hI.cpu().numpy(), ref[0])
