@@ -37,7 +37,7 @@ import numpy as np
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-from emri_kludge_suite_b200.workloads import DT, MSUN_SEC, NMODES, SEED, YEAR, config1, draw_source  # noqa: E402
+from emri_kludge_suite_b200.workloads import DT, MSUN_SEC, NMODES, SEED, YEAR, config1, config2, draw_source  # noqa: E402
 
 
 # ----------------------------------------------------------------------------- workload
@@ -454,6 +454,43 @@ def run_gpu(args, rank, world, local_rank):
         del pI, pII, traj
         wp.close()
 
+    # ---- configuration 2: split precision vs FP64 per source at high eccentricity
+    cfg2 = None
+    if args.config2_sources > 0:
+        src2, nm2 = config2(SEED + 2 + rank, args.config2_sources)
+        w2 = E.WaveBatch(local_rank)
+        w2.plan(src2, nmodes=nm2, nthreads=nthreads)
+        w2.upload(sptr)
+        N2 = w2.total_samples
+        a64 = torch.empty(2 * N2, dtype=torch.float64, device="cuda")
+        a32 = torch.empty_like(a64)
+        w2.run(a64.data_ptr(), a64.data_ptr() + 8 * N2, precision=0, stream=sptr)
+        w2.run(a32.data_ptr(), a32.data_ptr() + 8 * N2, precision=1, stream=sptr)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        w2.run(a32.data_ptr(), a32.data_ptr() + 8 * N2, precision=1, stream=sptr)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms2 = ev0.elapsed_time(ev1)
+        o2 = w2.offsets
+        mm2, rel2 = [], []
+        for s_ in range(len(src2)):
+            if w2.status[s_] != 0:
+                continue
+            x1, x2 = a64[o2[s_]:o2[s_ + 1]], a64[N2 + o2[s_]:N2 + o2[s_ + 1]]
+            y1, y2 = a32[o2[s_]:o2[s_ + 1]], a32[N2 + o2[s_]:N2 + o2[s_ + 1]]
+            aa, bb, ab = float(x1.dot(x1) + x2.dot(x2)), float(y1.dot(y1) + y2.dot(y2)), float(x1.dot(y1) + x2.dot(y2))
+            mm2.append(1.0 - ab / math.sqrt(aa * bb) if aa > 0 and bb > 0 else 0.0)
+            rel2.append(float(torch.maximum((x1 - y1).abs().max(), (x2 - y2).abs().max()) /
+                              torch.maximum(x1.abs().max(), x2.abs().max())))
+        cfg2 = {"workload": "config2: e0~U(0.05,0.7), n_max=min(100,ceil(10/(1-e0)^1.5)), otherwise config1",
+                "sources": len(src2), "ok_sources": int(np.sum(w2.status == 0)), "samples": int(N2),
+                "nmodes_min_max": [int(min(nm2)), int(max(nm2))], "split_samples_per_s": N2 / (ms2 * 1e-3),
+                "max_mismatch": float(max(mm2)), "median_mismatch": float(np.median(mm2)),
+                "max_rel_dh": float(max(rel2)), "median_rel_dh": float(np.median(rel2)), "bar": 1e-6}
+        del a64, a32
+        w2.close()
+
     # ---- end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     hIh = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -515,6 +552,7 @@ def run_gpu(args, rank, world, local_rank):
                    "l2": "outputs 16 B/sample x samples_per_gpu exceed the 126 MB L2",
                    "parallelism": f"sources sharded, {world} rank(s)", "launch": "one CUDA graph replay per step"},
         "accuracy_vs_fp64": accuracy,
+        "config2_split_vs_fp64": cfg2,
         "kernel_ms": split["kernel_ms"],
         "fp64_path": fp64,
         "plain_fp64_per_source": plain,
@@ -546,6 +584,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--likelihood", type=int, default=1024, help="config-4 templates to time (0: skip)")
+    ap.add_argument("--config2-sources", type=int, default=128,
+                    help="sources of the configuration-2 accuracy check (0: skip)")
     ap.add_argument("--plain-sources", type=int, default=16,
                     help="sources of the plain FP64 per-source baseline (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,

@@ -1,5 +1,6 @@
 """Seeded synthetic workloads of the benchmark and of the profiling runs.
 
+* :func:`config2` -- the same with e0 ~ U(0.05, 0.7) and n_max = min(100, ceil(10 / (1 - e0)^1.5)).
 * :func:`config1` -- the 512-source batch: log10 M ~ U(5, 7), mu ~ U(1, 100),
   a ~ U(0, 0.95), e0 ~ U(0.05, 0.5), cos iota ~ U(-1, 1) (|cos iota| < 0.05
   redrawn: the flux kludge is singular for polar orbits), isotropic sky and
@@ -26,12 +27,12 @@ DT = 10.0
 SEED = 20261203
 
 
-def draw_source(rng) -> dict:
+def draw_source(rng, e_max: float = 0.5) -> dict:
     while True:
         logM = rng.uniform(5.0, 7.0)
         mu = rng.uniform(1.0, 100.0)
         a = rng.uniform(0.0, 0.95)
-        e0 = rng.uniform(0.05, 0.5)
+        e0 = rng.uniform(0.05, e_max)
         cosi = rng.uniform(-1.0, 1.0)
         thS = math.acos(rng.uniform(-1.0, 1.0))
         phS = rng.uniform(0.0, 2 * math.pi)
@@ -55,6 +56,14 @@ def draw_source(rng) -> dict:
 def config1(seed: int, nsrc: int = 512):
     rng = np.random.default_rng(seed)
     return [draw_source(rng) for _ in range(nsrc)], rng
+
+
+def config2(seed: int, nsrc: int = 512):
+    """The configuration-1 draw with e0 ~ U(0.05, 0.7) and the harmonic cutoff
+    n_max = min(100, ceil(10 / (1 - e0)^1.5)); returns (sources, nmodes)."""
+    rng = np.random.default_rng(seed)
+    src = [draw_source(rng, e_max=0.7) for _ in range(nsrc)]
+    return src, [min(100, math.ceil(10.0 / (1.0 - p["e"]) ** 1.5)) for p in src]
 
 
 def profile_waveform():
