@@ -598,11 +598,14 @@ constexpr int kTaylorMax64 = 10;                          // FP64 terms at most
 constexpr int kTaylorMax32 = 6;                           // FP32 terms at most
 constexpr int kRowD = (3 * (kTaylorMax64 + 1) + 1) / 2 * 2;  // doubles per FP64 row (34)
 constexpr int kRowF = (3 * (kTaylorMax32 + 1) + 3) / 4 * 4;  // floats per FP32 row (24)
-constexpr int kWin5 = 2 * kTaylorMax64 + 5;               // J orders a row needs
 
-// J_m(x) for m = mlo .. mhi (x >= 0) into J[m - mlo].
+// J_m(x) for m = mlo .. mhi (x >= 0) into J[m - mlo]: Miller's backward
+// recurrence from order max(start, mhi + 8), normalised by
+// J_0 + 2 sum_k J_2k = 1 and rescaled on the way down whenever a value grows
+// past 1e250.  Below x = 1e-3 the power series is used instead: there
+// |x^2 / 4| <= 2.5e-7, so three terms leave a remainder below 1e-26.
 __device__ void bessel_window(double x, int mlo, int mhi, int start, double *J) {
-  if (x < 1.0) {
+  if (x < 1.0e-3) {
     if (x <= 0.0) {
       for (int m = mlo; m <= mhi; ++m) J[m - mlo] = (m == 0) ? 1.0 : 0.0;
       return;
@@ -611,7 +614,8 @@ __device__ void bessel_window(double x, int mlo, int mhi, int start, double *J) 
     double pref = exp((double)mlo * log(hx) - lgamma((double)mlo + 1.0));
     for (int nu = mlo; nu <= mhi; ++nu) {
       double term = 1.0, sum = 1.0;
-      for (int k = 1; k < 16; ++k) {
+#pragma unroll
+      for (int k = 1; k <= 3; ++k) {
         term *= q / ((double)k * ((double)nu + (double)k));
         sum += term;
       }
@@ -644,36 +648,66 @@ __device__ void bessel_window(double x, int mlo, int mhi, int start, double *J) 
   for (int o = mlo; o <= mhi; ++o) J[o - mlo] *= inv;
 }
 
-// One table row (harmonic n, K + 1 terms), built by one thread in FP64.
-template <typename T>
-__device__ void build_taylor_row(T *row, int n, double ec, int K, int start) {
-  const int mlo = max(0, n - 2 - K), mhi = n + 2 + K;
-  double Jw[kWin5];
-  bessel_window(n * ec, mlo, mhi, start, Jw);
-  double prev[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  double fac = 1.0;  // (n / 2)^k / k!
-  const double dn = (double)n;
+// One table row (harmonic n, K + 1 terms), built by one thread in FP64.  The
+// window holds J_m(n e_c) for m = n-2-K .. n+2+K (negative orders by
+// J_{-m} = (-1)^m J_m); each derivative order comes from the previous one by
+// J'_nu = (J_{nu-1} - J_{nu+1}) / 2 (DLMF 10.6.1) applied in place, which
+// narrows the valid window by one order on each side and leaves orders
+// n-2 .. n+2 at positions K .. K+4.
+template <int K, typename T>
+__device__ __forceinline__ void build_taylor_row_k(T *row, int n, double ec, int start) {
+  constexpr int W = 2 * K + 5;
+  const int lo = n - 2 - K, mlo = max(0, lo);
+  double Jw[W];
+  bessel_window(n * ec, mlo, n + 2 + K, start, Jw + (mlo - lo));
+  for (int m = lo; m < 0; ++m) Jw[m - lo] = ((-m) & 1) ? -Jw[-m - lo] : Jw[-m - lo];
+  double D[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) D[i] = Jw[i];
+  const double dn = (double)n, te = 2.0 * ec, tn = 2.0 / dn;
+  double fac = 1.0;            // n^k / k!
+  double p1 = 0.0, p3 = 0.0;   // previous order's coefficients of J_{n-1}, J_{n+1}
+#pragma unroll
   for (int k = 0; k <= K; ++k) {
-    if (k > 0) fac *= 0.5 * dn / (double)k;
-    double c[5];
-    for (int v = 0; v < 5; ++v) {
-      const int nu = n - 2 + v;
-      double s = 0.0, binom = 1.0;
-      for (int j = 0; j <= k; ++j) {
-        const int m = nu - k + 2 * j;
-        const double Jm = (m >= 0) ? Jw[m - mlo] : (((-m) & 1) ? -Jw[-m - mlo] : Jw[-m - mlo]);
-        s += (j & 1) ? -binom * Jm : binom * Jm;
-        binom = binom * (double)(k - j) / (double)(j + 1);
+    if (k > 0) {
+      double left = D[k - 1];
+#pragma unroll
+      for (int i = k; i <= W - 1 - k; ++i) {
+        const double old = D[i];
+        D[i] = 0.5 * (left - D[i + 1]);
+        left = old;
       }
-      c[v] = fac * s;  // delta^k coefficient of J_nu(n e)
+      fac *= dn * (1.0 / (double)k);
     }
-    const double A = dn * (c[0] - 2.0 * ec * c[1] - 2.0 * prev[1] + (2.0 / dn) * c[2] + 2.0 * ec * c[3] +
-                           2.0 * prev[3] - c[4]);
-    const double B = dn * (c[0] - 2.0 * c[2] + c[4]);
+    // delta^k coefficients of J_{n-2} .. J_{n+2} at e_c + delta
+    const double c0 = fac * D[K], c1 = fac * D[K + 1], c2 = fac * D[K + 2], c3 = fac * D[K + 3], c4 = fac * D[K + 4];
+    const double A = dn * (c0 - te * c1 - 2.0 * p1 + tn * c2 + te * c3 + 2.0 * p3 - c4);
+    const double B = dn * (c0 - 2.0 * c2 + c4);
     row[k] = (T)A;
     row[K + 1 + k] = (T)B;
-    row[2 * (K + 1) + k] = (T)c[2];
-    for (int v = 0; v < 5; ++v) prev[v] = c[v];
+    row[2 * (K + 1) + k] = (T)c2;
+    p1 = c1;
+    p3 = c3;
+  }
+}
+
+template <typename T>
+__device__ void build_taylor_row(T *row, int n, double ec, int K, int start) {
+  if constexpr (sizeof(T) == 4) {
+    switch (K) {
+      case 2: build_taylor_row_k<2, T>(row, n, ec, start); break;
+      case 3: build_taylor_row_k<3, T>(row, n, ec, start); break;
+      case 4: build_taylor_row_k<4, T>(row, n, ec, start); break;
+      default: build_taylor_row_k<6, T>(row, n, ec, start); break;
+    }
+  } else {
+    switch (K) {
+      case 4: build_taylor_row_k<4, T>(row, n, ec, start); break;
+      case 5: build_taylor_row_k<5, T>(row, n, ec, start); break;
+      case 6: build_taylor_row_k<6, T>(row, n, ec, start); break;
+      case 8: build_taylor_row_k<8, T>(row, n, ec, start); break;
+      default: build_taylor_row_k<10, T>(row, n, ec, start); break;
+    }
   }
 }
 
