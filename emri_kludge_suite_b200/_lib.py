@@ -130,6 +130,8 @@ def lib():
     L.aak_batch_run_noalloc.argtypes = [_vp, _vp, _i64, _i64p, _vp, _vp, _vp]
     L.aak_batch_run_plain.argtypes = [_vp, _vp, _vp, _vp, _i64, _vp]
     L.aak_batch_last_launches.argtypes = [_vp]
+    L.aak_batch_device_status.argtypes = [_vp]
+    L.aak_selftest_lookback_timeout.argtypes = [_i64]
     L.aak_batch_set_profiling.argtypes = [_vp, _i32]
     L.aak_batch_kernel_ms.argtypes = [_vp, ctypes.POINTER(ctypes.c_float)]
     L.aak_probe_fp64_tflops.argtypes = [_i32, _dp]

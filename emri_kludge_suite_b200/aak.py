@@ -198,6 +198,11 @@ class WaveBatch:
     def launches(self) -> int:
         return int(lib().aak_batch_last_launches(self._ctx))
 
+    def device_status(self) -> int:
+        """Wait for the device; the aak_status of the batch kernels' bounded
+        waits since the last upload or call (0, or AAK_ERR_DEVICE_TIMEOUT)."""
+        return int(lib().aak_batch_device_status(self._ctx))
+
     def run_graph(self, hI_ptr: int, hII_ptr: int, precision: int = 0, stream: int = 0):
         """:meth:`run` as one CUDA graph (captured on first use, replayed after)."""
         check(lib().aak_batch_run_graph(self._ctx, ctypes.c_void_p(hI_ptr), ctypes.c_void_p(hII_ptr), int(precision),

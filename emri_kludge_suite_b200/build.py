@@ -46,7 +46,10 @@ def nvcc() -> str:
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "**", "*.h*"), recursive=True) + glob.glob(os.path.join(REPO, "include", "*.h"))
+    found = []
+    for pat in ("*.h", "*.hpp", "*.cuh"):
+        found += glob.glob(os.path.join(CSRC, "**", pat), recursive=True)
+    return found + glob.glob(os.path.join(REPO, "include", "*.h"))
 
 
 def _stale(obj: str, deps) -> bool:

@@ -132,16 +132,16 @@ struct aak_ctx {
   DevBuf<double> d_knot_t;
   DevBuf<double4> d_knot_y, d_knot_c;
   DevBuf<int32_t> d_bessel;
-  DevBuf<TileSummary> d_summ;
-  DevBuf<TileCarry> d_carry;
-  DevBuf<unsigned long long> d_counter;
+  DevBuf<TileLink> d_link;                // look-back records, one per tile
+  DevBuf<int32_t> d_flag;                 // look-back flags, one per tile
+  DevBuf<unsigned long long> d_counter;   // [0] work-queue head, [1] device status word
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
   int last_launches = 0;
   bool profile = false;
   aak_mlp *model = nullptr;  // learned warm start of the map (optional)
   int precision = 0;         // precision of the host-buffer entry points
   uint64_t upload_gen = 0;   // bumped by every upload (device buffers may move)
-  // CUDA graph of the three dense launches for fixed outputs / precision / upload
+  // CUDA graph of the dense launch (clears + waveform kernel) for fixed outputs / precision / upload
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t cap_stream = nullptr;
@@ -402,9 +402,11 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
       (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) || (r = ctx->d_tile_pairs.reserve(ctx->tile_pairs.size())) ||
       (r = ctx->d_knot_t.reserve(ctx->knot_t.size())) || (r = ctx->d_knot_y.reserve(ctx->knot_y.size())) ||
       (r = ctx->d_knot_c.reserve(ctx->knot_c.size())) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
-      (r = ctx->d_summ.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
-      (r = ctx->d_carry.reserve(std::max<int64_t>(ctx->total_tiles, 1))) || (r = ctx->d_counter.reserve(1)))
+      (r = ctx->d_link.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
+      (r = ctx->d_flag.reserve(std::max<int64_t>(ctx->total_tiles, 1))) || (r = ctx->d_counter.reserve(2)))
     return r;
+  // the work-queue head is cleared by every launch; the status word here
+  if ((r = cuda_ok(cudaMemsetAsync(ctx->d_counter.ptr, 0, 2 * sizeof(unsigned long long), st))) != AAK_OK) return r;
   auto cp = [&](void *dst, const void *src, size_t bytes) {
     return cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
   };
@@ -439,7 +441,7 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   if (ctx->profile && !ctx->ev[0])
     for (auto &e : ctx->ev) cudaEventCreate(&e);
   launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
-  ctx->last_launches = 3;
+  ctx->last_launches = 1;
   return cuda_ok(cudaGetLastError());
 }
 
@@ -450,7 +452,7 @@ void drop_graph(aak_ctx *ctx) {
   ctx->graph = nullptr;
 }
 
-// The three dense launches as one CUDA graph, captured on the first call for
+// The dense launch (two clears and the waveform kernel) as one CUDA graph, captured on the first call for
 // a given (outputs, precision, upload) and replayed afterwards.
 int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t st) {
   if (!ctx->uploaded || !hI || !hII || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
@@ -482,7 +484,7 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
     ctx->g_prec = precision;
     ctx->g_gen = ctx->upload_gen;
   }
-  ctx->last_launches = 3;
+  ctx->last_launches = 1;
   return cuda_ok(cudaGraphLaunch(ctx->gexec, st));
 }
 
@@ -497,14 +499,15 @@ BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *t
   bv.knot_y = ctx->d_knot_y.ptr;
   bv.knot_c = ctx->d_knot_c.ptr;
   bv.bessel_start = ctx->d_bessel.ptr;
-  bv.summ = ctx->d_summ.ptr;
-  bv.carry = ctx->d_carry.ptr;
+  bv.link = ctx->d_link.ptr;
+  bv.link_flag = ctx->d_flag.ptr;
   bv.hI = hI;
   bv.hII = hII;
   bv.t_out = t;
   bv.traj_out = traj;
   bv.traj_stride = traj_stride;
   bv.work_counter = ctx->d_counter.ptr;
+  bv.device_status = reinterpret_cast<unsigned int *>(ctx->d_counter.ptr + 1);
   bv.max_nmodes = ctx->max_nmodes;
   return bv;
 }
@@ -533,19 +536,20 @@ int run_plain(aak_ctx *ctx, double *hI, double *hII, double *traj, int64_t traj_
     v.knot_y = ctx->d_knot_y.ptr;
     v.knot_c = ctx->d_knot_c.ptr;
     v.bessel_start = ctx->d_bessel.ptr;
-    v.summ = ctx->d_summ.ptr + d.tile_offset;
-    v.carry = ctx->d_carry.ptr + d.tile_offset;
+    v.link = ctx->d_link.ptr + d.tile_offset;
+    v.link_flag = ctx->d_flag.ptr + d.tile_offset;
     v.hI = hI;
     v.hII = hII;
     v.t_out = nullptr;
     v.traj_out = traj;
     v.traj_stride = traj_stride;
     v.work_counter = ctx->d_counter.ptr;
+    v.device_status = reinterpret_cast<unsigned int *>(ctx->d_counter.ptr + 1);
     v.trajectory_only = 1;
     v.max_nmodes = ctx->max_nmodes;
     launch_dense(v, ctx->num_sms, st, nullptr, 0);
     launch_plain_waveform(ctx->d_src.ptr, s, d.vlength, traj, traj_stride, hI, hII, st);
-    launches += 4;
+    launches += 2;
   }
   ctx->last_launches = launches;
   return cuda_ok(cudaGetLastError());
@@ -570,6 +574,25 @@ int default_ctx(aak_ctx **out) {
   return AAK_OK;
 }
 
+// Synchronise the device and read (and clear) the status words of the
+// context and of the allocation-free scratch.
+int device_status(aak_ctx *ctx) {
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  if ((r = cuda_ok(cudaDeviceSynchronize())) != AAK_OK) return r;
+  bool gave_up = false;
+  if (ctx->d_counter.ptr) {
+    unsigned int v = 0;
+    unsigned int *word = reinterpret_cast<unsigned int *>(ctx->d_counter.ptr + 1);
+    if ((r = cuda_ok(cudaMemcpy(&v, word, sizeof(v), cudaMemcpyDeviceToHost))) != AAK_OK) return r;
+    if (v && (r = cuda_ok(cudaMemset(word, 0, sizeof(v)))) != AAK_OK) return r;
+    gave_up = v != 0;
+  }
+  const int sv = static_scratch_status(ctx->device, true);
+  if (sv < 0) return cuda_ok(cudaGetLastError());
+  return (gave_up || sv > 0) ? AAK_ERR_DEVICE_TIMEOUT : AAK_OK;
+}
+
 // Plan, upload and run one batch into ctx-owned device outputs, then copy to host.
 int host_roundtrip(aak_ctx *ctx, double *t, double *hI, double *hII) {
   int r;
@@ -582,7 +605,8 @@ int host_roundtrip(aak_ctx *ctx, double *t, double *hI, double *hII) {
       (r = cuda_ok(cudaMemcpyAsync(hII, dII, N * sizeof(double), cudaMemcpyDeviceToHost, 0))))
     return r;
   if (t && (r = cuda_ok(cudaMemcpyAsync(t, dt, N * sizeof(double), cudaMemcpyDeviceToHost, 0)))) return r;
-  return cuda_ok(cudaStreamSynchronize(0));
+  if ((r = cuda_ok(cudaStreamSynchronize(0))) != AAK_OK) return r;
+  return device_status(ctx);
 }
 
 }  // namespace
@@ -672,8 +696,8 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_knot_y.release();
     c->d_knot_c.release();
     c->d_bessel.release();
-    c->d_summ.release();
-    c->d_carry.release();
+    c->d_link.release();
+    c->d_flag.release();
     c->d_counter.release();
     c->d_out.release();
     for (auto &e : c->ev)
@@ -810,6 +834,18 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
 }
 
 int aak_batch_last_launches(aak_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
+
+int aak_selftest_lookback_timeout(int64_t cycles) {
+  const int v = lookback_timeout_selftest((long long)cycles, nullptr);
+  if (v < 0) return cuda_ok(cudaGetLastError());
+  return v == 1 ? AAK_OK : AAK_ERR_CUDA;
+}
+
+int aak_batch_device_status(aak_ctx *ctx) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return device_status(ctx);
+}
 
 int aak_batch_set_profiling(aak_ctx *ctx, int32_t on) {
   if (!ctx) return AAK_ERR_INVALID_PARAM;

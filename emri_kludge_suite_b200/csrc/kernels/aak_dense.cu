@@ -1,16 +1,16 @@
 // aak_dense.cu -- sm_100a kernels for the dense part of the AAK waveform:
 // spline interpolation of the coarse (e, v, M, S) trajectory, the
-// Adams-Bashforth-2 phase accumulation (gamma~, Phi, alpha) as a two-pass
+// Adams-Bashforth-2 phase accumulation (gamma~, Phi, alpha) as a single-pass
 // tiled scan, and the Peters-Mathews harmonic sum with the LISA h_I/h_II
 // response and the Planck taper.  Reference semantics: src/suite/AAK.cc:213-547.
 //
-// Pass 1 (k_phase_tiles):  per 1024-sample tile, the sums of the AB2
-//   increments (no dense arrays are materialised).
-// Carry (k_phase_carry):   per source, exclusive tile prefixes in
-//   double-double arithmetic.
-// Pass 2 (k_waveform_fp64): persistent CTAs pull tiles from a work queue,
-//   recompute the rates, scan the increments inside the tile, and evaluate the
-//   harmonic sum in FP64; h_I, h_II are written with coalesced stores.
+// k_waveform<precision>: persistent CTAs pull 1024-sample tiles from a work
+//   queue; per tile, phase 1 evaluates the spline and the rates and scans the
+//   AB2 increments inside the tile, a decoupled look-back over the tile's
+//   phase chain (per-tile records in double-double arithmetic) supplies the
+//   carry from the earlier tiles of the source, and phase 2 evaluates the
+//   harmonic sums (FP64, or split precision); h_I, h_II are written with
+//   coalesced stores.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -42,16 +42,6 @@ __device__ __forceinline__ int find_source(const int64_t *tile_start, int nsrc, 
   return lo;
 }
 
-__device__ __forceinline__ int find_knot(const double *kt, int n, double t) {
-  int lo = 0, hi = n - 1;
-  while (hi - lo > 1) {
-    const int mid = (lo + hi) >> 1;
-    if (kt[mid] > t) hi = mid;
-    else lo = mid;
-  }
-  return lo;
-}
-
 struct Traj4 {
   double e, v, M, S;
 };
@@ -60,21 +50,6 @@ __device__ __forceinline__ double piece(double y0, double y1, double c0, double 
   const double b = (y1 - y0) / h - h * (c1 + 2.0 * c0) / 3.0;
   const double d = (c1 - c0) / (3.0 * h);
   return y0 + dx * (b + dx * (c0 + dx * d));
-}
-
-__device__ __forceinline__ Traj4 spline4(const BatchView &bv, const SourceDesc &d, double t) {
-  const double *kt = bv.knot_t + d.knot_offset;
-  const int k = find_knot(kt, d.n_knots, t);
-  const double x0 = kt[k], x1 = kt[k + 1];
-  const double h = x1 - x0, dx = t - x0;
-  const double4 y0 = bv.knot_y[d.knot_offset + k], y1 = bv.knot_y[d.knot_offset + k + 1];
-  const double4 c0 = bv.knot_c[d.knot_offset + k], c1 = bv.knot_c[d.knot_offset + k + 1];
-  Traj4 q;
-  q.e = piece(y0.x, y1.x, c0.x, c1.x, h, dx);
-  q.v = piece(y0.y, y1.y, c0.y, c1.y, h, dx);
-  q.M = piece(y0.z, y1.z, c0.z, c1.z, h, dx);
-  q.S = piece(y0.w, y1.w, c0.w, c1.w, h, dx);
-  return q;
 }
 
 // ------------------------------------------------------------------ knot windows
@@ -211,42 +186,6 @@ __device__ __forceinline__ void dd_add(double &hi, double &lo, double x) {
   lo = e - (hi - s);
 }
 
-// block-wide sum over 256 threads (all threads get the result)
-__device__ __forceinline__ double block_sum(double v, double *red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  double s = 0.0;
-#pragma unroll
-  for (int k = 0; k < kTileThreads / 32; ++k) s += red[k];
-  return s;
-}
-
-// block-wide inclusive scan over 256 threads
-__device__ __forceinline__ double block_scan(double v, double *red, double &total) {
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const double n = __shfl_up_sync(0xffffffffu, v, o);
-    if (l >= o) v += n;
-  }
-  __syncthreads();
-  if (l == 31) red[w] = v;
-  __syncthreads();
-  double pre = 0.0, tot = 0.0;
-#pragma unroll
-  for (int k = 0; k < kTileThreads / 32; ++k) {
-    const double r = red[k];
-    if (k < w) pre += r;
-    tot += r;
-  }
-  total = tot;
-  return v + pre;
-}
-
 // block-wide inclusive scan of three values at once (one pair of barriers)
 __device__ __forceinline__ void block_scan3(double v[3], double (*red)[kTileThreads / 32], double tot[3]) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
@@ -285,40 +224,163 @@ struct TileCtx {
   int start;    // first sample of the tile
   int end;      // one past the last sample of the tile
   int neff;     // samples feeding the output
-  int64_t lt;   // tile index inside the source
+  int lt;       // tile index inside the source
+  int head;     // tile holding sample i0 (t = 0): head of both phase chains
+  int64_t g;    // global tile index (records, knot windows)
 };
 
-__device__ __forceinline__ TileCtx tile_ctx(const BatchView &bv, int64_t g, const SourceDesc *&dp) {
+// Queue item j -> tile.  Inside a source the queue runs from the head tile
+// through the later tiles in increasing order, then through the earlier tiles
+// in decreasing order, so that every tile comes after its predecessor in its
+// phase chain (the tile next to it, towards the head).
+__device__ __forceinline__ TileCtx tile_ctx(const BatchView &bv, int64_t j, const SourceDesc *&dp) {
   TileCtx c;
-  c.s = find_source(bv.tile_start, bv.nsrc, g);
+  c.s = find_source(bv.tile_start, bv.nsrc, j);
   dp = bv.src + c.s;
-  c.lt = g - bv.tile_start[c.s];
-  c.start = (int)(c.lt * kTileSamples);
+  const int64_t t0 = bv.tile_start[c.s];
+  const int T = (int)(bv.tile_start[c.s + 1] - t0);
+  const int jj = (int)(j - t0);
+  const int i0 = dp->i0;
+  c.head = (i0 <= 0) ? 0 : min(i0 / kTileSamples, T - 1);
+  c.lt = (jj < T - c.head) ? c.head + jj : T - 1 - jj;
+  c.g = t0 + c.lt;
+  c.start = c.lt * kTileSamples;
   c.end = min(c.start + kTileSamples, dp->vlength);
   c.neff = n_eff(*dp);
   return c;
 }
 
-// Clamped Phidot (AAK.cc:254): P_i = raw_i if raw_i > 0, else the previous
-// P.  Represented as a + b*C, where C is the clamped rate just before the tile.
-struct Lin {
-  double a, b;
-};
+// ------------------------------------------------------------------ look-back
+// Bounded waits: a wait gives up after bv.lookback_cycles SM clocks (default
+// kLookBackCycles, about 2 s), or at once when another wait of the launch
+// already gave up, sets *device_status and returns a zero carry.
+constexpr long long kLookBackCycles = 4000000000LL;
 
-// ------------------------------------------------------------------ pass 1
-// Per tile: (A) the three phase rates of every sample of the tile and of the
-// samples just before and after it, independent per thread (instruction-level
-// parallelism), into shared memory; (B) the clamped Phidot, the AB2
-// increments and their tile sums; (C) one fused block reduction.
-constexpr int kSlots = kTileSamples + 2;  // slot s <-> sample start - 1 + s
+__device__ __forceinline__ int ld_acquire(const int32_t *p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int32_t *p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
-__device__ __forceinline__ Lin clamp_phidot(const double *raw, int slot, int first_fwd_slot) {
-  // P at `slot`: the raw rate if positive, else the last positive raw rate at a
-  // forward sample before it in the tile, else the rate carried into the tile
-  if (raw[slot] > 0.0) return Lin{raw[slot], 0.0};
-  for (int k = slot - 1; k >= first_fwd_slot; --k)
-    if (raw[k] > 0.0) return Lin{raw[k], 0.0};
-  return Lin{0.0, 1.0};
+// double-double sum (hi, lo) += (bh, bl)
+__device__ __forceinline__ void dd_add_dd(double &hi, double &lo, double bh, double bl) {
+  double s, e;
+  two_sum(hi, bh, s, e);
+  e += lo + bl;
+  hi = s + e;
+  lo = e - (hi - s);
+}
+
+// Publish tile g's aggregate or inclusive record (one thread): the fields go
+// to L2 (st.cg) before the flag is released.
+__device__ __forceinline__ void publish_aggregate(const BatchView &bv, int64_t g, const double x[3], double C, bool hasC) {
+  TileLink *L = bv.link + g;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) __stcg(&L->agg[q], x[q]);
+  __stcg(&L->agg_C, C);
+  __stcg(&L->agg_hasC, hasC ? 1 : 0);
+  __threadfence();
+  st_release(bv.link_flag + g, 1);
+}
+__device__ __forceinline__ void publish_inclusive(const BatchView &bv, int64_t g, const double fh[3], const double fl[3],
+                                                  const double bh[3], const double bl[3], double C) {
+  TileLink *L = bv.link + g;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    __stcg(&L->inc_f_hi[q], fh[q]);
+    __stcg(&L->inc_f_lo[q], fl[q]);
+    __stcg(&L->inc_b_hi[q], bh[q]);
+    __stcg(&L->inc_b_lo[q], bl[q]);
+  }
+  __stcg(&L->inc_C, C);
+  __threadfence();
+  st_release(bv.link_flag + g, 2);
+}
+
+// Exclusive prefix of tile c.lt along its chain (dir +1: forward, -1:
+// backward), computed by one whole warp.  Each round looks at the 32 nearest
+// predecessors not yet summed (lane k: k + 1 tiles further towards the head),
+// waits until every one of them nearer than the first inclusive record (or
+// than the head tile) is written, and sums their aggregates and that
+// inclusive record in double-double.  C (forward chains): the clamped Phidot
+// of the nearest record that sets one, else 0.  Every lane returns the sums.
+__device__ void look_back_warp(const BatchView &bv, const TileCtx &c, int dir, double hi[3], double lo[3], double &C) {
+  const unsigned kAll = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int64_t t0 = c.g - c.lt;
+  const long long bound = (bv.lookback_cycles > 0) ? bv.lookback_cycles : kLookBackCycles;
+  const long long start = clock64();
+  bool haveC = false;
+  C = 0.0;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) hi[q] = lo[q] = 0.0;
+  for (int p = c.lt - dir;; p -= 32 * dir) {
+    const int q = p - dir * lane;
+    const bool valid = (dir > 0) ? (q >= c.head) : (q <= c.head);
+    int f = 0;
+    unsigned stop_mask, need;
+    for (;;) {
+      f = valid ? ld_acquire(bv.link_flag + t0 + q) : 0;
+      stop_mask = __ballot_sync(kAll, valid && (f == 2 || (f == 1 && q == c.head)));
+      const unsigned vmask = __ballot_sync(kAll, valid);
+      const unsigned ready = __ballot_sync(kAll, valid && f != 0);
+      need = stop_mask ? ((stop_mask & (0u - stop_mask)) << 1) - 1u : vmask;  // lanes up to the first stop
+      if ((ready & need) == need) break;
+      int give_up = 0;
+      if (lane == 0)
+        give_up = (*(volatile unsigned int *)bv.device_status != 0u || clock64() - start > bound) ? 1 : 0;
+      if (__shfl_sync(kAll, give_up, 0)) {
+        if (lane == 0) atomicExch(bv.device_status, 1u);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) hi[k] = lo[k] = 0.0;
+        C = 0.0;
+        return;
+      }
+      __nanosleep(32);
+    }
+    const bool use = (need >> lane) & 1u;
+    const bool is_stop = stop_mask != 0u && lane == __ffs(stop_mask) - 1;
+    double xh[3] = {0.0, 0.0, 0.0}, xl[3] = {0.0, 0.0, 0.0}, cv = 0.0;
+    bool hasc = false;
+    if (use) {
+      const TileLink *L = bv.link + t0 + q;
+      if (is_stop && f == 2) {
+        const double *ph = (dir > 0) ? L->inc_f_hi : L->inc_b_hi, *pl = (dir > 0) ? L->inc_f_lo : L->inc_b_lo;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          xh[k] = __ldcg(ph + k);
+          xl[k] = __ldcg(pl + k);
+        }
+        cv = __ldcg(&L->inc_C);
+        hasc = true;
+      } else {  // an aggregate (the head's too, when it holds only one)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) xh[k] = __ldcg(&L->agg[k]);
+        cv = __ldcg(&L->agg_C);
+        hasc = __ldcg(&L->agg_hasC) != 0;
+      }
+    }
+    if (dir > 0 && !haveC) {
+      const unsigned cm = __ballot_sync(kAll, use && hasc);
+      if (cm) {
+        C = __shfl_sync(kAll, cv, __ffs(cm) - 1);
+        haveC = true;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double bh = __shfl_xor_sync(kAll, xh[k], o), bl = __shfl_xor_sync(kAll, xl[k], o);
+        dd_add_dd(xh[k], xl[k], bh, bl);
+      }
+      dd_add_dd(hi[k], lo[k], xh[k], xl[k]);
+    }
+    if (stop_mask) return;
+  }
 }
 
 // Taylor-table term counts (defined with the harmonic sums); sources with
@@ -326,187 +388,6 @@ __device__ __forceinline__ Lin clamp_phidot(const double *raw, int slot, int fir
 constexpr int kTabModes = 128;
 __device__ __forceinline__ int taylor_terms_fp64(double q, int nmodes);
 __device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes);
-
-__global__ void __launch_bounds__(kTileThreads) k_phase_tiles(BatchView bv) {
-  __shared__ double s_r[3][kSlots];
-  __shared__ double red[7][kTileThreads / 32];
-  __shared__ double s_wt[kWin];
-  __shared__ double4 s_wy[kWin], s_wc[kWin], s_wb[kWin], s_wd[kWin];
-  const int tid = threadIdx.x;
-  for (int64_t g = blockIdx.x; g < bv.total_tiles; g += gridDim.x) {
-    const SourceDesc *dp;
-    const TileCtx c = tile_ctx(bv, g, dp);
-    const SourceDesc &d = *dp;
-    if (d.status != 0) continue;
-    const int lim = min(c.end, c.neff);  // samples [start, lim) feed the output
-    TileSummary &ts = bv.summ[g];
-    if (lim <= c.start) {  // nothing to accumulate (after the taper)
-      if (tid == 0) {
-        for (int q = 0; q < 3; ++q) ts.fA[q] = ts.fB[q] = ts.bA[q] = ts.bB[q] = ts.last_rate[q] = ts.first_rate[q] = ts.rate_before[q] = 0.0;
-        ts.ec = 0.0;
-        ts.k64 = ts.k32 = 0;
-        ts.has_last[0] = ts.has_last[1] = ts.has_last[2] = 0;
-      }
-      continue;
-    }
-    KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
-    load_window(bv, d, g, w);
-    // (A) rates, two independent samples per pass
-#pragma unroll 1
-    for (int s = tid; s < kSlots; s += 2 * kTileThreads) {
-      const int s2 = s + kTileThreads;
-      const int i1 = c.start - 1 + s, i2 = c.start - 1 + s2;
-      double r1[3] = {0, 0, 0}, r2[3] = {0, 0, 0};
-      const bool n1 = i1 >= 0 && i1 < d.vlength && i1 <= lim;
-      const bool n2 = s2 < kSlots && i2 >= 0 && i2 < d.vlength && i2 <= lim;
-      if (n1) phase_rates(d, spline4w(bv, d, sample_time(d, i1), w), r1);
-      if (n2) phase_rates(d, spline4w(bv, d, sample_time(d, i2), w), r2);
-      s_r[0][s] = r1[0];
-      s_r[1][s] = n1 ? r1[1] : -1.0;
-      s_r[2][s] = r1[2];
-      if (s2 < kSlots) {
-        s_r[0][s2] = r2[0];
-        s_r[1][s2] = n2 ? r2[1] : -1.0;
-        s_r[2][s2] = r2[2];
-      }
-    }
-    __syncthreads();
-    // (B) increments
-    const int first_fwd_slot = max(d.i0, c.start) - c.start + 1;
-    double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // fA[0..2], fB, bA[0..2]
-#pragma unroll 1
-    for (int ch = 0; ch < kTileChunks; ++ch) {
-      const int k = c.start + ch * kTileThreads + tid;
-      if (k >= lim) continue;
-      const int sl = k - c.start + 1;
-      if (k >= d.i0) {
-        const Lin P = clamp_phidot(s_r[1], sl, first_fwd_slot);
-        if (k == d.i0) {
-          acc[0] += s_r[0][sl] * d.dt;
-          acc[1] += P.a * d.dt;
-          acc[3] += P.b * d.dt;
-          acc[2] += s_r[2][sl] * d.dt;
-        } else {
-          // P at k-1: inside the tile the same clamp; k-1 = start-1 is the tile boundary
-          const Lin Pm = (sl - 1 >= first_fwd_slot) ? clamp_phidot(s_r[1], sl - 1, first_fwd_slot)
-                                                    : ((s_r[1][0] > 0.0) ? Lin{s_r[1][0], 0.0} : Lin{0.0, 1.0});
-          acc[0] += (1.5 * s_r[0][sl] - .5 * s_r[0][sl - 1]) * d.dt;
-          acc[1] += (1.5 * P.a - .5 * Pm.a) * d.dt;
-          acc[3] += (1.5 * P.b - .5 * Pm.b) * d.dt;
-          acc[2] += (1.5 * s_r[2][sl] - .5 * s_r[2][sl - 1]) * d.dt;
-        }
-      }
-      if (k >= 1 && k <= d.i0) {
-        if (k == d.i0) {
-          acc[4] += s_r[0][sl] * d.dt;
-          acc[5] += s_r[1][sl] * d.dt;
-          acc[6] += s_r[2][sl] * d.dt;
-        } else {
-          acc[4] += (1.5 * s_r[0][sl] - .5 * s_r[0][sl + 1]) * d.dt;
-          acc[5] += (1.5 * s_r[1][sl] - .5 * s_r[1][sl + 1]) * d.dt;
-          acc[6] += (1.5 * s_r[2][sl] - .5 * s_r[2][sl + 1]) * d.dt;
-        }
-      }
-    }
-    // (C) fused reduction of the seven sums
-#pragma unroll
-    for (int q = 0; q < 7; ++q)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-    const int wp = tid >> 5, l = tid & 31;
-    if (l == 0)
-#pragma unroll
-      for (int q = 0; q < 7; ++q) red[q][wp] = acc[q];
-    __syncthreads();
-    if (tid == 0) {
-      double tot[7];
-      for (int q = 0; q < 7; ++q) {
-        tot[q] = 0.0;
-        for (int k = 0; k < kTileThreads / 32; ++k) tot[q] += red[q][k];
-      }
-      ts.fA[0] = tot[0];
-      ts.fA[1] = tot[1];
-      ts.fA[2] = tot[2];
-      ts.fB[0] = 0.0;
-      ts.fB[1] = tot[3];
-      ts.fB[2] = 0.0;
-      ts.bA[0] = tot[4];
-      ts.bA[1] = tot[5];
-      ts.bA[2] = tot[6];
-      ts.bB[0] = ts.bB[1] = ts.bB[2] = 0.0;
-      // last clamped Phidot of the tile, if it does not depend on the carry
-      const int last_f = lim - 1;
-      Lin Pl = {0.0, 1.0};
-      if (last_f >= max(c.start, d.i0)) Pl = clamp_phidot(s_r[1], last_f - c.start + 1, first_fwd_slot);
-      ts.has_last[1] = (last_f >= max(c.start, d.i0) && Pl.b == 0.0) ? 1 : 0;
-      ts.last_rate[1] = Pl.a;
-      ts.has_last[0] = ts.has_last[2] = 0;
-      ts.last_rate[0] = ts.last_rate[2] = 0.0;
-      ts.first_rate[0] = ts.first_rate[1] = ts.first_rate[2] = 0.0;
-      // for pass 2: rates just before the tile, and the Bessel-table centre and
-      // term counts from e at the tile's first, middle and last output samples
-      ts.rate_before[0] = s_r[0][0];
-      ts.rate_before[1] = s_r[1][0];
-      ts.rate_before[2] = s_r[2][0];
-      double ec = 0.0;
-      int k64 = 0, k32 = 0;
-      if (d.nmodes <= kTabModes) {
-        const double e0 = spline4w(bv, d, sample_time(d, c.start), w).e;
-        const double e2 = spline4w(bv, d, sample_time(d, last_f), w).e;
-        ec = spline4w(bv, d, sample_time(d, (c.start + last_f) / 2), w).e;
-        const double de = fmax(fabs(e0 - ec), fabs(e2 - ec));
-        if (ec > 1e-6) {
-          const double q = d.nmodes * (1.25 * de + 1e-15);  // bounds n |e - e_c| over the tile
-          k64 = taylor_terms_fp64(q, d.nmodes);
-          k32 = taylor_terms_fp32(q, d.nmodes);
-        }
-      }
-      ts.ec = ec;
-      ts.k64 = k64;
-      ts.k32 = k32;
-    }
-    __syncthreads();
-  }
-}
-
-// ------------------------------------------------------------------ carry
-// One CTA per source walks its tiles in order (a handful of thousand at most).
-__global__ void __launch_bounds__(32) k_phase_carry(BatchView bv) {
-  const int s = blockIdx.x;
-  if (s >= bv.nsrc || threadIdx.x != 0) return;
-  const SourceDesc &d = bv.src[s];
-  const int64_t t0 = bv.tile_start[s], t1 = bv.tile_start[s + 1];
-  if (d.status != 0) return;
-  double fh[3] = {0, 0, 0}, fl[3] = {0, 0, 0};
-  double C = 0.0;  // clamped Phidot before the tile
-  for (int64_t g = t0; g < t1; ++g) {
-    TileCarry &tc = bv.carry[g];
-    const TileSummary &ts = bv.summ[g];
-    for (int q = 0; q < 3; ++q) {
-      tc.fwd_hi[q] = fh[q];
-      tc.fwd_lo[q] = fl[q];
-    }
-    tc.Cf[0] = 0.0;
-    tc.Cf[1] = C;
-    tc.Cf[2] = 0.0;
-    for (int q = 0; q < 3; ++q) {
-      const double tot = ts.fA[q] + ts.fB[q] * C;
-      dd_add(fh[q], fl[q], tot);
-    }
-    if (ts.has_last[1]) C = ts.last_rate[1];
-  }
-  double bh[3] = {0, 0, 0}, bl[3] = {0, 0, 0};
-  for (int64_t g = t1 - 1; g >= t0; --g) {
-    TileCarry &tc = bv.carry[g];
-    const TileSummary &ts = bv.summ[g];
-    for (int q = 0; q < 3; ++q) {
-      tc.bwd_hi[q] = bh[q];
-      tc.bwd_lo[q] = bl[q];
-      tc.Cb[q] = 0.0;
-      dd_add(bh[q], bl[q], ts.bA[q]);
-    }
-  }
-}
 
 // ------------------------------------------------------------------ Bessel functions
 // J_{lo..lo+4}(x) for x > 0 (lo = n-2 for n >= 2; lo = 0 for n = 1).
@@ -1048,8 +929,13 @@ __device__ __forceinline__ void finish(const SamplePrep<T> &P, T Sa, T Sb, T Sc,
 
 
 
-// ------------------------------------------------------------------ pass 2
+// ------------------------------------------------------------------ waveform kernel
 // Samples per thread whose harmonic sums run side by side (divides kTileChunks).
+// 1: build the Taylor table after phase 1, on warps 1-7 while warp 0 looks
+// back; 0: before phase 1, overlapping its first chunk.
+#ifndef AAK_TABLE_AFTER_SCAN
+#define AAK_TABLE_AFTER_SCAN 1
+#endif
 #ifndef AAK_JOINT_SPLIT
 #define AAK_JOINT_SPLIT 2
 #endif
@@ -1073,6 +959,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   __shared__ double s_r[3][kTileThreads];
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
+  __shared__ double s_par[3], s_rb[3], s_cy[7], s_lastP;  // tile parameters, chain carry
   __shared__ __align__(16) SourceDesc s_desc;           // this tile's source
   __shared__ Geom<typename std::conditional<kSplit, float, double>::type> s_geom;
   __shared__ double s_wt[kWin];
@@ -1086,15 +973,16 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
     __syncthreads();
-    const long long g = s_tile;
+    const long long j = s_tile;
     __syncthreads();
-    if (g >= bv.total_tiles) break;
+    if (j >= bv.total_tiles) break;
     const SourceDesc *dp;
-    const TileCtx c = tile_ctx(bv, g, dp);
-    const TileCarry &tc = bv.carry[g];
-    const TileSummary &ts = bv.summ[g];
-    if (dp->status != 0 || min(c.end, c.neff) <= c.start) {
-      // failed source, or a tile entirely after the taper: zeros
+    const TileCtx c = tile_ctx(bv, j, dp);
+    const int64_t g = c.g;
+    const int lim = min(c.end, c.neff);  // samples [start, lim) feed the output
+    if (dp->status != 0 || lim <= c.start) {
+      // failed source, or a tile entirely after the taper: zeros, and an
+      // empty aggregate for the chain
       const SourceDesc &dz = *dp;
       for (int ch = 0; ch < kTileChunks; ++ch) {
         const int i = c.start + ch * kTileThreads + tid;
@@ -1103,6 +991,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           bv.hII[dz.out_offset + i] = 0.0;
           if (bv.t_out) bv.t_out[dz.out_offset + i] = (dz.status != 0) ? 0.0 : sample_time(dz, i);
         }
+      }
+      if (tid == 0) {
+        const double zero[3] = {0.0, 0.0, 0.0};
+        publish_aggregate(bv, g, zero, 0.0, false);
       }
       continue;
     }
@@ -1118,17 +1010,63 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const SourceDesc &d = s_desc;
     const int32_t *bstart = bv.bessel_start + d.bessel_offset;
     const double X0[3] = {d.gim0, d.Phi0, d.alp0};
-    // boundary rate and Bessel-table parameters recorded by pass 1
-    const int K = kSplit ? ts.k32 : ts.k64;
-    const double ec = ts.ec;
+    // tile parameters from the staged window: e at the first, middle and last
+    // output samples (Bessel-table centre and term count), and the raw rates
+    // of the sample just before the tile (Phi: -1 if there is none)
+    if (tid < 3) {
+      const int i = (tid == 0) ? c.start : (tid == 1) ? (c.start + lim - 1) / 2 : lim - 1;
+      s_par[tid] = spline4w(bv, d, sample_time(d, i), w).e;
+    } else if (tid == 32) {
+      double r[3] = {0, 0, 0};
+      const int i = c.start - 1;
+      const bool ok = i >= 0 && i < d.vlength;
+      if (ok) phase_rates(d, spline4w(bv, d, sample_time(d, i), w), r);
+      s_rb[0] = r[0];
+      s_rb[1] = ok ? r[1] : -1.0;
+      s_rb[2] = r[2];
+    }
+    // chain direction: +1 after the head tile, -1 before it, 0 the head
+    const int dir = (c.lt > c.head) ? 1 : (c.lt < c.head) ? -1 : 0;
+    __syncthreads();
+    double ec = 0.0;
+    int K = 0;
+    if (d.nmodes <= kTabModes) {
+      ec = s_par[1];
+      const double de = fmax(fabs(s_par[0] - ec), fabs(s_par[2] - ec));
+      if (ec > 1e-6) {
+        const double q = d.nmodes * (1.25 * de + 1e-15);  // bounds n |e - e_c| over the tile
+        K = kSplit ? taylor_terms_fp32(q, d.nmodes) : taylor_terms_fp64(q, d.nmodes);
+      }
+    }
+    // A forward tile whose Phidot clamp reaches back past its first sample
+    // (raw rate before it not positive) needs the chain's clamped Phidot
+    // first: it waits for its whole prefix before phase 1.
+    const bool needC = dir > 0 && !(s_rb[1] > 0.0);
+    if (needC) {
+      if (tid < 32) {
+        double hi[3], lo[3], C;
+        look_back_warp(bv, c, 1, hi, lo, C);
+        if (tid == 0) {
+          for (int q = 0; q < 3; ++q) {
+            s_cy[q] = hi[q];
+            s_cy[3 + q] = lo[q];
+          }
+          s_cy[6] = C;
+        }
+      }
+      __syncthreads();
+    }
+    const double Cin = needC ? s_cy[6] : 0.0;
+#if !AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread per harmonic); its barrier is the first one of phase 1
     if (K > 0 && !bv.trajectory_only)
       for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
         if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
       }
-    // ---------------- phase 1: phases of the tile's samples
-    double prev[3] = {ts.rate_before[0], (ts.rate_before[1] > 0.0) ? ts.rate_before[1] : tc.Cf[1], ts.rate_before[2]};
+#endif
+    // ---------------- phase 1: phases of the tile's samples, relative to the tile
+    double prev[3] = {s_rb[0], (s_rb[1] > 0.0) ? s_rb[1] : Cin, s_rb[2]};
     double lastP = prev[1];
     double runF[3] = {0, 0, 0}, runB[3] = {0, 0, 0};
     for (int ch = 0; ch < kTileChunks; ++ch) {
@@ -1155,6 +1093,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
         P = (k >= 0) ? s_raw[k] : lastP;
       }
       s_Pa[tid] = P;
+      if (vf && i == lim - 1) s_lastP = P;  // clamped Phidot after the tile's last forward sample
       __syncthreads();
       const double Pm = (tid > 0) ? s_Pa[tid - 1] : lastP;
       double incF[3] = {0, 0, 0}, incB[3] = {0, 0, 0};
@@ -1202,16 +1141,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
 #pragma unroll
       for (int qq = 0; qq < 3; ++qq) {
-        if (i > d.i0) {
-          // X_i = X0 + carry + (forward increments of samples < i in this tile)
-          X[qq] = X0[qq] + (tc.fwd_hi[qq] + (tc.fwd_lo[qq] + (runF[qq] + (inclF[qq] - incF[qq]))));
-        } else if (i == d.i0) {
-          X[qq] = X0[qq];
-        } else {
-          // X_i = X0 - (backward increments of samples in (i, i0])
-          const double after_in_tile = ts.bA[qq] - (runB[qq] + inclB[qq]);
-          X[qq] = X0[qq] - (tc.bwd_hi[qq] + (tc.bwd_lo[qq] + after_in_tile));
-        }
+        // the tile-local part; the chain's carry is added after the look-back
+        if (i > d.i0) X[qq] = runF[qq] + (inclF[qq] - incF[qq]);  // forward increments of samples < i
+        else if (i == d.i0) X[qq] = X0[qq];
+        else X[qq] = runB[qq] + inclB[qq];                      // backward increments of samples <= i
         runF[qq] += totF[qq];
         runB[qq] += totB[qq];
       }
@@ -1231,9 +1164,6 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           bv.traj_out[1 * st + o] = q.v;
           bv.traj_out[2 * st + o] = q.M;
           bv.traj_out[3 * st + o] = q.S;
-          bv.traj_out[4 * st + o] = X[0];
-          bv.traj_out[5 * st + o] = X[1];
-          bv.traj_out[6 * st + o] = X[2];
           bv.traj_out[7 * st + o] = nu;
           bv.traj_out[8 * st + o] = r[0];
         }
@@ -1243,6 +1173,76 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       prev[0] = s_r[0][kTileThreads - 1];
       prev[2] = s_r[2][kTileThreads - 1];
       __syncthreads();
+    }
+    // ---------------- chain carries: warp 0 publishes this tile's aggregate,
+    // looks back for the exclusive prefix and publishes the inclusive record
+    if (tid < 32) {
+      const bool hasF = lim - 1 >= max(c.start, d.i0);  // forward output samples in the tile
+      double hi[3] = {0, 0, 0}, lo[3] = {0, 0, 0}, C = 0.0;
+      if (needC) {
+        for (int q = 0; q < 3; ++q) {
+          hi[q] = s_cy[q];
+          lo[q] = s_cy[3 + q];
+        }
+        C = s_cy[6];
+      } else if (dir != 0) {
+        if (tid == 0) publish_aggregate(bv, g, (dir > 0) ? runF : runB, hasF ? s_lastP : 0.0, hasF);
+        look_back_warp(bv, c, dir, hi, lo, C);
+      }
+      if (tid == 0) {
+        double fh[3] = {0, 0, 0}, fl[3] = {0, 0, 0}, bh[3] = {0, 0, 0}, bl[3] = {0, 0, 0};
+        for (int q = 0; q < 3; ++q) {
+          s_cy[q] = hi[q];
+          s_cy[3 + q] = lo[q];
+          if (dir >= 0) {
+            fh[q] = hi[q];
+            fl[q] = lo[q];
+            dd_add(fh[q], fl[q], runF[q]);
+          }
+          if (dir <= 0) {
+            bh[q] = hi[q];
+            bl[q] = lo[q];
+            dd_add(bh[q], bl[q], runB[q]);
+          }
+        }
+        publish_inclusive(bv, g, fh, fl, bh, bl, hasF ? s_lastP : C);
+      }
+    }
+#if AAK_TABLE_AFTER_SCAN
+    // Taylor table rows (one thread of warps 1-7 per harmonic) while warp 0 looks back
+    else if (K > 0 && !bv.trajectory_only)
+      for (int n = tid - 31; n <= d.nmodes; n += kTileThreads - 32) {
+        if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
+        else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
+      }
+#endif
+    __syncthreads();
+    // the phases of this thread's own samples: X0 + carry + local part
+    // (forward), X0 - (carry + increments after the sample) (backward)
+    {
+      const double cy_hi[3] = {s_cy[0], s_cy[1], s_cy[2]}, cy_lo[3] = {s_cy[3], s_cy[4], s_cy[5]};
+      for (int ch = 0; ch < kTileChunks; ++ch) {
+        const int i = c.start + ch * kTileThreads + tid;
+        const int sl = ch * kTileThreads + tid;
+        if (i >= lim) break;
+        double X[3];
+#pragma unroll
+        for (int qq = 0; qq < 3; ++qq) {
+          double *sv = s_dyn + (2 + qq) * kTileSamples;
+          const double v = sv[sl];
+          if (i > d.i0) X[qq] = X0[qq] + (cy_hi[qq] + (cy_lo[qq] + v));
+          else if (i == d.i0) X[qq] = v;
+          else X[qq] = X0[qq] - (cy_hi[qq] + (cy_lo[qq] + (runB[qq] - v)));
+          sv[sl] = X[qq];
+        }
+        if (bv.traj_out) {
+          const int64_t o = d.out_offset + i;
+          const int64_t st = bv.traj_stride;
+          bv.traj_out[4 * st + o] = X[0];
+          bv.traj_out[5 * st + o] = X[1];
+          bv.traj_out[6 * st + o] = X[2];
+        }
+      }
     }
     // ---------------- phase 2: harmonic sums of this thread's own samples,
     // kJoint of them at a time (shared table loads, independent recurrences)
@@ -1465,13 +1465,13 @@ void prepare_dense_launch() {
 
 void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision) {
   if (bv.total_tiles <= 0) return;
-  const int grid1 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * 8);
-  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
   if (ev) cudaEventRecord(ev[0], stream);
-  k_phase_tiles<<<grid1, kTileThreads, 0, stream>>>(bv);
-  if (ev) cudaEventRecord(ev[1], stream);
-  k_phase_carry<<<bv.nsrc, 32, 0, stream>>>(bv);
-  if (ev) cudaEventRecord(ev[2], stream);
+  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
+  cudaMemsetAsync(bv.link_flag, 0, (size_t)bv.total_tiles * sizeof(int32_t), stream);
+  if (ev) {
+    cudaEventRecord(ev[1], stream);
+    cudaEventRecord(ev[2], stream);
+  }
   // per-sample values, then the Taylor table sized for the batch's harmonic count
   const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
   const size_t dyn = kWaveDynSmem + (size_t)rows * (precision == 1 ? kRowF * sizeof(float) : kRowD * sizeof(double));
@@ -1572,21 +1572,72 @@ double probe_fp32_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
 }
 
 // ------------------------------------------------------------------ allocation-free launch
-// Tile scratch (per-tile phase sums, carries and the work-queue head) for
-// callers that must not allocate device memory.  The array is part of the
-// module image: every GPU that loads this library holds its 10 MB until the
-// process exits.  All calls share it and it keeps the last call's contents;
-// launches that overlap on the GPU race on it.
+// Tile scratch (look-back records and flags, the work-queue head and the
+// device status word) for callers that must not allocate device memory.  The
+// array is part of the module image: every GPU that loads this library holds
+// its 4 MB until the process exits.  All calls share it and it keeps the last
+// call's contents; launches that overlap on the GPU race on it.
 namespace {
-constexpr size_t kStaticSummaryBytes = (size_t)kStaticScratchTiles * sizeof(TileSummary);
-constexpr size_t kStaticCarryOffset = (kStaticSummaryBytes + 255) / 256 * 256;
-constexpr size_t kStaticCounterOffset = (kStaticCarryOffset + (size_t)kStaticScratchTiles * sizeof(TileCarry) + 255) / 256 * 256;
+constexpr size_t kStaticLinkBytes = (size_t)kStaticScratchTiles * sizeof(TileLink);
+constexpr size_t kStaticFlagOffset = (kStaticLinkBytes + 255) / 256 * 256;
+constexpr size_t kStaticCounterOffset = (kStaticFlagOffset + (size_t)kStaticScratchTiles * sizeof(int32_t) + 255) / 256 * 256;
 constexpr size_t kStaticScratchBytes = kStaticCounterOffset + 256;
 static __device__ __align__(256) unsigned char g_tile_scratch[kStaticScratchBytes];
 
 std::mutex g_scratch_mu;
 void *g_scratch_addr[kMaxStaticDevices] = {nullptr};
 }  // namespace
+
+namespace {
+// Tile 1 of a two-tile chain looks back at tile 0, whose flag stays 0 (one warp).
+__global__ void k_lookback_selftest(BatchView bv) {
+  if (blockIdx.x != 0) return;
+  TileCtx c{};
+  c.lt = 1;
+  c.head = 0;
+  c.g = 1;
+  double hi[3], lo[3], C;
+  look_back_warp(bv, c, 1, hi, lo, C);
+}
+}  // namespace
+
+int lookback_timeout_selftest(long long cycles, cudaStream_t stream) {
+  void *buf = nullptr;
+  const size_t bytes = 2 * sizeof(TileLink) + 256;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess) return -1;
+  unsigned char *b = static_cast<unsigned char *>(buf);
+  BatchView bv{};
+  bv.link = reinterpret_cast<TileLink *>(b);
+  bv.link_flag = reinterpret_cast<int32_t *>(b + 2 * sizeof(TileLink));
+  bv.device_status = reinterpret_cast<unsigned int *>(b + 2 * sizeof(TileLink) + 64);
+  bv.lookback_cycles = cycles > 0 ? cycles : 1;
+  unsigned int v = 0;
+  int out = -1;
+  if (cudaMemsetAsync(buf, 0, bytes, stream) == cudaSuccess) {
+    k_lookback_selftest<<<1, 32, 0, stream>>>(bv);
+    if (cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(stream) == cudaSuccess &&
+        cudaMemcpy(&v, bv.device_status, sizeof(v), cudaMemcpyDeviceToHost) == cudaSuccess)
+      out = v ? 1 : 0;
+  }
+  cudaFree(buf);
+  return out;
+}
+
+int static_scratch_status(int device, bool clear) {
+  if (device < 0 || device >= kMaxStaticDevices) return 0;
+  void *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_scratch_mu);
+    base = g_scratch_addr[device];
+  }
+  if (!base) return 0;  // no allocation-free launch on this device yet
+  unsigned int *word = reinterpret_cast<unsigned int *>(static_cast<unsigned char *>(base) + kStaticCounterOffset +
+                                                        sizeof(unsigned long long));
+  unsigned int v = 0;
+  if (cudaMemcpy(&v, word, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  if (v && clear && cudaMemset(word, 0, sizeof(v)) != cudaSuccess) return -1;
+  return v ? 1 : 0;
+}
 
 int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream) {
   if (bv.total_tiles > kStaticScratchTiles) return 8;  // AAK_ERR_CAPACITY
@@ -1607,12 +1658,12 @@ int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cuda
     base = g_scratch_addr[device];
   }
   unsigned char *b = static_cast<unsigned char *>(base);
-  bv.summ = reinterpret_cast<TileSummary *>(b);
-  bv.carry = reinterpret_cast<TileCarry *>(b + kStaticCarryOffset);
+  bv.link = reinterpret_cast<TileLink *>(b);
+  bv.link_flag = reinterpret_cast<int32_t *>(b + kStaticFlagOffset);
   bv.work_counter = reinterpret_cast<unsigned long long *>(b + kStaticCounterOffset);
-  // the work-queue head must start at zero; launch_dense_fp64 clears it on
-  // `stream`, and pass 1 / the carry kernel overwrite every tile entry that
-  // pass 2 reads before it reads it
+  bv.device_status = reinterpret_cast<unsigned int *>(b + kStaticCounterOffset + sizeof(unsigned long long));
+  // launch_dense_fp64 clears the work-queue head and the look-back flags on
+  // `stream`; every record is written before its flag is
   launch_dense_fp64(bv, num_sms, stream, nullptr);
   return cudaGetLastError() == cudaSuccess ? 0 : 5;
 }

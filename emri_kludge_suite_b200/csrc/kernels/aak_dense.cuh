@@ -16,29 +16,25 @@ constexpr int kTileThreads = 256;                      // threads per CTA
 constexpr int kTileChunks = AAK_TILE_CHUNKS;           // 256-sample chunks per tile
 constexpr int kTileSamples = kTileThreads * kTileChunks;  // 1024 samples per tile
 
-// Per-tile partial sums of the Adams-Bashforth-2 phase increments written by
-// pass 1.  For each phase q (0: gamma~, 1: Phi, 2: alpha) the forward sum over
-// the tile is fA[q] + fB[q] * C[q], where C[q] is the (clamped) rate of the
-// sample just before the tile; the backward sum is bA[q] + bB[q] * C'[q] with
-// C'[q] the rate of the sample just after the tile.
-struct TileSummary {
-  double fA[3], fB[3];
-  double bA[3], bB[3];
-  double last_rate[3];   // gim/alp: rate of the last forward sample; Phi: last positive raw rate
-  double first_rate[3];  // raw rates of the first sample in the tile
-  int32_t has_last[3];   // last_rate valid
+// Look-back record of one tile in its source's phase chain (the single-pass
+// scan of the waveform kernel).  The tile holding t = 0 (sample i0) heads two
+// chains: the forward one runs through the later tiles in increasing order,
+// the backward one through the earlier tiles in decreasing order, and the
+// work queue hands tiles out in that order.  link_flag[g] (0: not written,
+// 1: aggregate, 2: inclusive) is stored with release semantics after the
+// record: an aggregate holds the tile's own increments, an inclusive record
+// the increments from the chain head through the tile; the two sets of
+// fields are separate, so that a reader never sees one half-overwritten.
+struct TileLink {
+  // aggregate (flag >= 1): the tile's own increments along its chain
+  double agg[3];            // forward tiles: forward increments; backward tiles: backward increments
+  double agg_C;             // clamped Phidot after the tile's last forward sample
+  int32_t agg_hasC;         // agg_C was set inside the tile
   int32_t pad;
-  double rate_before[3]; // raw rates of the sample just before the tile (Phi: -1 if none)
-  double ec;             // Bessel-table centre eccentricity of the tile (0: no output samples)
-  int32_t k64, k32;      // multiplication-theorem terms for the FP64 / split harmonic sums (0: per-sample)
-};
-
-// Per-tile carries written by the carry kernel and read by pass 2.
-struct TileCarry {
-  double fwd_hi[3], fwd_lo[3];  // sum of forward increments before the tile (double-double)
-  double bwd_hi[3], bwd_lo[3];  // sum of backward increments after the tile
-  double Cf[3];                 // rate carried into the tile's first forward increment
-  double Cb[3];                 // rate carried into the tile's last backward increment
+  // inclusive (flag == 2): increments from the chain head through the tile, double-double
+  double inc_f_hi[3], inc_f_lo[3];
+  double inc_b_hi[3], inc_b_lo[3];
+  double inc_C;             // clamped Phidot after the tile (0 before the first forward sample)
 };
 
 // Everything the kernels read about a batch.
@@ -52,19 +48,22 @@ struct BatchView {
   const double4 *knot_y;        // (e, v, M, S) at the knots
   const double4 *knot_c;        // natural-spline half second derivatives
   const int32_t *bessel_start;  // Miller start orders, per source x mode
-  TileSummary *summ;
-  TileCarry *carry;
+  TileLink *link;               // one per tile
+  int32_t *link_flag;           // one per tile, cleared before every launch
   double *hI, *hII;             // outputs, indexed by src.out_offset + i
   double *t_out;                // optional
   double *traj_out;             // optional dense trajectory, 9 x total samples (e,v,M,S,gim,Phi,alp,nu,gimdot)
   int64_t traj_stride;
-  unsigned long long *work_counter;  // persistent work queue head (pass 2)
-  int32_t trajectory_only = 0;       // 1: pass 2 writes traj_out and skips the harmonic sums
+  unsigned long long *work_counter;  // persistent work queue head, cleared before every launch
+  unsigned int *device_status;       // set to 1 when a bounded look-back wait gave up (never cleared here)
+  int32_t trajectory_only = 0;       // 1: write traj_out and skip the harmonic sums
   int32_t max_nmodes = 0;            // largest harmonic count of the batch (0: unknown) -- sizes the tile table
+  long long lookback_cycles = 0;     // bound of one look-back wait in SM clocks (<= 0: about 2 s)
 };
 
-// Launch pass 1, the carry scan and pass 2 on `stream`.  ev (optional, 4
-// events) brackets the three kernels for per-kernel timing.
+// Clear the work queue and the look-back flags, then launch the waveform
+// kernel, on `stream`.  ev (optional, 4 events): ev[0]..ev[1] bracket the
+// clears, ev[2]..ev[3] the kernel.
 void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev);
 // precision 0: FP64 throughout; 1: split (FP64 phases and reductions, FP32
 // geometry, response, Bessel evaluation and harmonic recurrence).
@@ -73,7 +72,7 @@ void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
 // Plain FP64 per-source harmonic sum: the per-sample algorithm of the
 // reference's CUDA port (src/cuda/kernel.cu:374-555) -- five Bessel functions
 // jn(n-2 .. n+2, n e), one cos/sin of n Phi and the NK-frame rotation per
-// harmonic -- on the dense trajectory (9 x traj_stride doubles, as pass 2
+// harmonic -- on the dense trajectory (9 x traj_stride doubles, as the waveform kernel
 // writes with trajectory_only) of source s of the batch.
 void launch_plain_waveform(const SourceDesc *src, int s, int vlength, const double *traj, int64_t traj_stride,
                            double *hI, double *hII, cudaStream_t stream);
@@ -93,10 +92,20 @@ void prepare_dense_launch();
 constexpr int64_t kStaticScratchTiles = 32768;
 constexpr int kMaxStaticDevices = 64;
 
-// Same kernels as launch_dense_fp64, with the tile scratch (bv.summ,
-// bv.carry, bv.work_counter are ignored) taken from a file-scope __device__
-// array instead of caller or context allocations.  Returns an aak_status.
+// Same kernels as launch_dense_fp64, with the tile scratch (bv.link,
+// bv.link_flag, bv.work_counter and bv.device_status are ignored) taken from a
+// file-scope __device__ array instead of caller or context allocations.  Returns an aak_status.
 // The first call on a device looks the array's address up (once per device).
 int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream);
+// Device status word of the allocation-free scratch on `device` (current):
+// 1 if a bounded look-back wait of one of its launches gave up, 0 if not (or
+// no such launch yet), -1 on a CUDA error; `clear` resets it.  Synchronous.
+int static_scratch_status(int device, bool clear);
+
+// Self-test of the bounded look-back wait: one CTA waits on a flag that
+// nothing sets, for at most `cycles` SM clocks, on `stream`; returns the
+// device status word it left (1: the wait gave up as it should) or -1 on a
+// CUDA error.  Synchronous.
+int lookback_timeout_selftest(long long cycles, cudaStream_t stream);
 
 }  // namespace aak

@@ -171,9 +171,23 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
 /* Number of CUDA kernels the last aak_batch_run launched. */
 int aak_batch_last_launches(aak_ctx *ctx);
 
+/* Waits for the device, then reports whether a bounded device-side wait of
+ * the batch kernels gave up since the last upload or the last call (the
+ * look-back of the phase scan; the allocation-free launches on the device
+ * included): AAK_ERR_DEVICE_TIMEOUT, else AAK_OK.  Clears the condition. No
+ * reference counterpart (the reference's kernels do not wait on one another). */
+int aak_batch_device_status(aak_ctx *ctx);
+
+/* Self-test of that bounded wait on the current device: one thread waits on a
+ * look-back flag that nothing sets, for at most `cycles` SM clocks (a few
+ * million: about a millisecond), and gives up.  Returns AAK_OK when the wait
+ * gave up and reported it, AAK_ERR_CUDA otherwise.  Synchronous. */
+int aak_selftest_lookback_timeout(int64_t cycles);
+
 /* Per-kernel timing of aak_batch_run with CUDA events on its stream: after
  * aak_batch_set_profiling(ctx, 1), aak_batch_kernel_ms returns the durations
- * of (pass 1 phase sums, carry scan, waveform) of the last run in ms. */
+ * of (work-queue and look-back flag clears, 0 -- no separate phase-sum kernel,
+ * waveform kernel) of the last run in ms. */
 int aak_batch_set_profiling(aak_ctx *ctx, int32_t on);
 int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3);
 

@@ -152,3 +152,64 @@ def test_invalid_source_raises_value_error():
     p.update(e=-0.1)
     with pytest.raises(AAKValueError):
         E.wave(p)
+
+
+def test_lookback_wait_gives_up_and_device_stays_usable():
+    """The phase scan's bounded look-back wait: on a flag that nothing sets it
+    gives up after about a millisecond of SM clocks and reports it; kernels
+    launched afterwards run normally."""
+    from emri_kludge_suite_b200._lib import lib
+    assert lib().aak_selftest_lookback_timeout(2_000_000) == 0
+    pars = dict(BASE)
+    pars["length"] = 5000
+    m = E.front_end(pars)
+    mt = O.MappedTrajectory(m.steps, m.e_traj, m.v_map, m.M_map, m.s_map, m.dt_map, m.Phi0, 2)
+    t, hI, hII = E.genwave(pars, m, 30)
+    to, oI, oII, _, _ = O.oracle_genwave(pars, mt, 30)
+    assert mismatch(hI, hII, oI, oII) < 1e-10
+
+
+def test_lookback_chains_forward_and_backward_report_no_timeout():
+    """Batches with forward (t = 0 at the start) and backward (t = 0 at the
+    plunge) phase chains, both precisions and the graph replay: the device
+    status stays clear and the replay equals the direct launch."""
+    names = golden_names()
+    gs = [load_golden(n) for n in names]
+    assert any(g["pars"]["backint"] for g in gs)
+    wb = E.WaveBatch(0)
+    wb.plan([g["pars"] for g in gs], nmodes=[int(g["nmodes"]) for g in gs], mapped=[golden_mapped(g) for g in gs])
+    assert np.all(wb.status == 0)
+    N = wb.total_samples
+    wb.upload()
+    out = {}
+    for prec in (0, 1):
+        a = torch.zeros(N, dtype=torch.float64, device="cuda")
+        b = torch.zeros_like(a)
+        wb.run(a.data_ptr(), b.data_ptr(), precision=prec)
+        a2 = torch.zeros_like(a)
+        b2 = torch.zeros_like(a)
+        wb.run_graph(a2.data_ptr(), b2.data_ptr(), precision=prec)
+        torch.cuda.synchronize()
+        assert torch.equal(a, a2) and torch.equal(b, b2)
+        out[prec] = (a.cpu().numpy(), b.cpu().numpy())
+    assert wb.device_status() == 0
+    o = wb.offsets
+    for s in range(len(gs)):
+        sl = slice(o[s], o[s + 1])
+        assert mismatch(out[1][0][sl], out[1][1][sl], out[0][0][sl], out[0][1][sl]) < 1e-6
+
+
+def test_backward_chain_full_length_against_oracle():
+    """backint with the plunge inside the window: t = 0 at sample 388,582 of
+    400,000 (dt = 100 s), so ~380 tiles chain backward and ~11 forward."""
+    pars = dict(load_golden("plunge_backint")["pars"])
+    pars.update(length=400000, T=400000 * pars["dt"] / O.YEAR, p=7.0)
+    m = E.front_end(pars)
+    t, hI, hII = E.genwave(pars, m, 30)
+    mt = O.MappedTrajectory(m.steps, m.e_traj, m.v_map, m.M_map, m.s_map, m.dt_map, m.Phi0, 2)
+    to, oI, oII, ip, ib = O.oracle_genwave(pars, mt, 30)
+    assert np.array_equal(t, to)
+    assert t[1] < 0.0 < t[-1]
+    mm = mismatch(hI, hII, oI, oII)
+    assert mm < 1e-6, mm
+    assert _maxrel(hI, oI) < 1e-4
