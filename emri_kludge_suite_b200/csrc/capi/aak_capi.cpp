@@ -117,6 +117,7 @@ struct aak_ctx {
   std::vector<SourceDesc> descs;
   std::vector<int64_t> tile_start;
   std::vector<int64_t> tile_pairs;  // per source {0, its tiles}: the tile prefix of a one-source view
+  std::vector<int64_t> queue;       // work-queue order of the tiles (global tile indices)
   std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
   HostBuf<double> knot_t;
   HostBuf<double4> knot_y, knot_c;
@@ -127,7 +128,7 @@ struct aak_ctx {
   bool uploaded = false;
   // device buffers
   DevBuf<SourceDesc> d_src;
-  DevBuf<int64_t> d_tile_start, d_tile_pairs;
+  DevBuf<int64_t> d_tile_start, d_tile_pairs, d_queue;
   DevBuf<int32_t> d_tile_knot;
   DevBuf<double> d_knot_t;
   DevBuf<double4> d_knot_y, d_knot_c;
@@ -302,6 +303,25 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
       ctx->tile_knot[2 * (d.tile_offset + t) + 1] = k1 + 2 - k0;
     }
   });
+  // work-queue order: chain step major, source minor.  Step 0 of a source is
+  // its head tile (the one holding t = 0), then come its later tiles in
+  // increasing order, then its earlier ones in decreasing order; interleaving
+  // the sources puts a tile's chain predecessor a whole batch row earlier in
+  // the queue, so that on many-source batches it is finished when the tile
+  // looks back at it.  The head rule is the waveform kernel's.
+  std::vector<int> T(n), head(n);
+  int maxT = 0;
+  for (int s = 0; s < n; ++s) {
+    T[s] = (int)(ctx->tile_start[s + 1] - ctx->tile_start[s]);
+    const int i0 = ctx->descs[s].i0;
+    head[s] = (i0 <= 0 || T[s] == 0) ? 0 : std::min(i0 / kTileSamples, T[s] - 1);
+    maxT = std::max(maxT, T[s]);
+  }
+  ctx->queue.resize(std::max<int64_t>(ctx->total_tiles, 1));
+  int64_t q = 0;
+  for (int k = 0; k < maxT; ++k)
+    for (int s = 0; s < n; ++s)
+      if (k < T[s]) ctx->queue[q++] = ctx->tile_start[s] + ((k < T[s] - head[s]) ? head[s] + k : T[s] - 1 - k);
   ctx->uploaded = false;
   return AAK_OK;
 }
@@ -400,6 +420,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   const int n = ctx->nsrc;
   if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
       (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) || (r = ctx->d_tile_pairs.reserve(ctx->tile_pairs.size())) ||
+      (r = ctx->d_queue.reserve(ctx->queue.size())) ||
       (r = ctx->d_knot_t.reserve(ctx->knot_t.size())) || (r = ctx->d_knot_y.reserve(ctx->knot_y.size())) ||
       (r = ctx->d_knot_c.reserve(ctx->knot_c.size())) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
       (r = ctx->d_link.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
@@ -414,6 +435,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
       (r = cp(ctx->d_tile_start.ptr, ctx->tile_start.data(), (n + 1) * sizeof(int64_t))) ||
       (r = cp(ctx->d_tile_knot.ptr, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
       (r = cp(ctx->d_tile_pairs.ptr, ctx->tile_pairs.data(), ctx->tile_pairs.size() * sizeof(int64_t))) ||
+      (r = cp(ctx->d_queue.ptr, ctx->queue.data(), ctx->queue.size() * sizeof(int64_t))) ||
       (r = cp(ctx->d_knot_t.ptr, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
       (r = cp(ctx->d_knot_y.ptr, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
       (r = cp(ctx->d_knot_c.ptr, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
@@ -494,6 +516,7 @@ BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *t
   bv.nsrc = ctx->nsrc;
   bv.total_tiles = ctx->total_tiles;
   bv.tile_start = ctx->d_tile_start.ptr;
+  bv.queue = ctx->d_queue.ptr;
   bv.tile_knot = ctx->d_tile_knot.ptr;
   bv.knot_t = ctx->d_knot_t.ptr;
   bv.knot_y = ctx->d_knot_y.ptr;

@@ -186,22 +186,29 @@ __device__ __forceinline__ void dd_add(double &hi, double &lo, double x) {
   lo = e - (hi - s);
 }
 
-// block-wide inclusive scan of three values at once (one pair of barriers)
-__device__ __forceinline__ void block_scan3(double v[3], double (*red)[kTileThreads / 32], double tot[3]) {
+// block-wide exclusive scan of three values; every thread also gets the totals
+__device__ __forceinline__ void block_exscan3(const double v[3], double (*red)[kTileThreads / 32], double ex[3],
+                                              double tot[3]) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  double in[3] = {v[0], v[1], v[2]};
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const double n = __shfl_up_sync(0xffffffffu, v[q], o);
-      if (l >= o) v[q] += n;
+      const double n = __shfl_up_sync(0xffffffffu, in[q], o);
+      if (l >= o) in[q] += n;
     }
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const double e = __shfl_up_sync(0xffffffffu, in[q], 1);
+    ex[q] = (l == 0) ? 0.0 : e;
   }
   __syncthreads();
   if (l == 31) {
-    red[0][w] = v[0];
-    red[1][w] = v[1];
-    red[2][w] = v[2];
+    red[0][w] = in[0];
+    red[1][w] = in[1];
+    red[2][w] = in[2];
   }
   __syncthreads();
 #pragma unroll
@@ -213,7 +220,7 @@ __device__ __forceinline__ void block_scan3(double v[3], double (*red)[kTileThre
       if (k < w) pre += r;
       t += r;
     }
-    v[q] += pre;
+    ex[q] += pre;
     tot[q] = t;
   }
 }
@@ -229,20 +236,28 @@ struct TileCtx {
   int64_t g;    // global tile index (records, knot windows)
 };
 
-// Queue item j -> tile.  Inside a source the queue runs from the head tile
-// through the later tiles in increasing order, then through the earlier tiles
-// in decreasing order, so that every tile comes after its predecessor in its
-// phase chain (the tile next to it, towards the head).
+// Queue item j -> tile.  Without a queue array (one-source views, the
+// allocation-free launch) the queue runs source by source, and inside a
+// source from the head tile through the later tiles in increasing order,
+// then through the earlier tiles in decreasing order, so that every tile
+// comes after its predecessor in its phase chain (the tile next to it,
+// towards the head).  A queue array (batches) lists the same per-source
+// orders interleaved across sources.
 __device__ __forceinline__ TileCtx tile_ctx(const BatchView &bv, int64_t j, const SourceDesc *&dp) {
   TileCtx c;
-  c.s = find_source(bv.tile_start, bv.nsrc, j);
+  const int64_t g = bv.queue ? bv.queue[j] : j;
+  c.s = find_source(bv.tile_start, bv.nsrc, g);
   dp = bv.src + c.s;
   const int64_t t0 = bv.tile_start[c.s];
   const int T = (int)(bv.tile_start[c.s + 1] - t0);
-  const int jj = (int)(j - t0);
   const int i0 = dp->i0;
   c.head = (i0 <= 0) ? 0 : min(i0 / kTileSamples, T - 1);
-  c.lt = (jj < T - c.head) ? c.head + jj : T - 1 - jj;
+  if (bv.queue) {
+    c.lt = (int)(g - t0);
+  } else {
+    const int jj = (int)(g - t0);
+    c.lt = (jj < T - c.head) ? c.head + jj : T - 1 - jj;
+  }
   c.g = t0 + c.lt;
   c.start = c.lt * kTileSamples;
   c.end = min(c.start + kTileSamples, dp->vlength);
@@ -616,7 +631,8 @@ __device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes) {
 
 // Mode sums Sa = sum A_n cos(n Phi'), Sb = sum B_n sin(n Phi'), Sc = sum C_n
 // cos(n Phi') from the tile table at delta = e - e_c, with the harmonic
-// phases from the rotation recurrence z_n = z_1^n z_D, for M samples of one
+// phases from the rotation recurrence w_n = w_{n-1} z_1, w_0 = z_D (so
+// w_n = z_1^n z_D: one complex product per harmonic), for M samples of one
 // tile at once: each table row is loaded once for all of them and the M
 // recurrences run side by side.
 template <int K, typename T, int M>
@@ -626,8 +642,8 @@ __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes,
   T zr[M], zi[M], sa[M], sb[M], sc[M];
 #pragma unroll
   for (int m = 0; m < M; ++m) {
-    zr[m] = T(1);
-    zi[m] = T(0);
+    zr[m] = cD[m];  // w_0 = z_D; w_n = w_{n-1} z_1 = z_1^n z_D
+    zi[m] = sD[m];
     sa[m] = sb[m] = sc[m] = T(0);
   }
 #pragma unroll 1
@@ -664,11 +680,9 @@ __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes,
       const T tr = zr[m] * c1[m] - zi[m] * s1[m];
       zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
       zr[m] = tr;
-      const T cn = zr[m] * cD[m] - zi[m] * sD[m];
-      const T sn = fma(zi[m], cD[m], zr[m] * sD[m]);
-      sa[m] = fma(A, cn, sa[m]);
-      sb[m] = fma(B, sn, sb[m]);
-      sc[m] = fma(C, cn, sc[m]);
+      sa[m] = fma(A, zr[m], sa[m]);
+      sb[m] = fma(B, zi[m], sb[m]);
+      sc[m] = fma(C, zr[m], sc[m]);
     }
   }
 #pragma unroll
@@ -954,12 +968,9 @@ constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double)
 template <bool kSplit>
 __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
-  __shared__ double s_raw[kTileThreads];
-  __shared__ double s_Pa[kTileThreads];
-  __shared__ double s_r[3][kTileThreads];
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
-  __shared__ double s_par[3], s_rb[3], s_cy[7], s_lastP;  // tile parameters, chain carry
+  __shared__ double s_par[3], s_rb[3], s_ra[3], s_cy[7], s_lastP;  // tile parameters, chain carry
   __shared__ __align__(16) SourceDesc s_desc;           // this tile's source
   __shared__ Geom<typename std::conditional<kSplit, float, double>::type> s_geom;
   __shared__ double s_wt[kWin];
@@ -1024,6 +1035,14 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       s_rb[0] = r[0];
       s_rb[1] = ok ? r[1] : -1.0;
       s_rb[2] = r[2];
+    } else if (tid == 64) {
+      // rates of the sample just after the tile, for the backward AB2 step
+      // of its last sample (a backward sample before i0 only)
+      double r[3] = {0, 0, 0};
+      if (c.end - 1 < d.i0 && c.end < d.vlength) phase_rates(d, spline4w(bv, d, sample_time(d, c.end), w), r);
+      s_ra[0] = r[0];
+      s_ra[1] = r[1];
+      s_ra[2] = r[2];
     }
     // chain direction: +1 after the head tile, -1 before it, 0 the head
     const int dir = (c.lt > c.head) ? 1 : (c.lt < c.head) ? -1 : 0;
@@ -1066,97 +1085,21 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
 #endif
     // ---------------- phase 1: phases of the tile's samples, relative to the tile
-    double prev[3] = {s_rb[0], (s_rb[1] > 0.0) ? s_rb[1] : Cin, s_rb[2]};
-    double lastP = prev[1];
-    double runF[3] = {0, 0, 0}, runB[3] = {0, 0, 0};
+    // (A) spline and rates of every sample, kTileChunks per thread (slots
+    //     tid + 256 ch, independent of one another); the rates sit in the
+    //     phase slots until (C)
+    const double Pin = (s_rb[1] > 0.0) ? s_rb[1] : Cin;  // clamped Phidot just before the tile
+    int nonpos = 0;                                      // a forward sample whose raw Phidot is not positive
+#pragma unroll 2
     for (int ch = 0; ch < kTileChunks; ++ch) {
-      const int i = c.start + ch * kTileThreads + tid;
       const int sl = ch * kTileThreads + tid;
-      const bool in = i < c.end && i < c.neff;
-      const bool vf = in && i >= d.i0;
-      const bool vb = in && i >= 1 && i <= d.i0;
+      const int i = c.start + sl;
       Traj4 q = {0, 0, 0, 0};
       double r[3] = {0, 0, 0}, om = 0.0;
-      if (in) {
+      if (i < lim) {
         q = spline4w(bv, d, sample_time(d, i), w);
         phase_rates(d, q, r, &om);
-      }
-      s_raw[tid] = vf ? r[1] : -1.0;
-      s_r[0][tid] = r[0];
-      s_r[1][tid] = r[1];
-      s_r[2][tid] = r[2];
-      __syncthreads();
-      double P = r[1];
-      if (vf && !(r[1] > 0.0)) {
-        int k = tid - 1;
-        while (k >= 0 && !(s_raw[k] > 0.0)) --k;
-        P = (k >= 0) ? s_raw[k] : lastP;
-      }
-      s_Pa[tid] = P;
-      if (vf && i == lim - 1) s_lastP = P;  // clamped Phidot after the tile's last forward sample
-      __syncthreads();
-      const double Pm = (tid > 0) ? s_Pa[tid - 1] : lastP;
-      double incF[3] = {0, 0, 0}, incB[3] = {0, 0, 0};
-      if (vf) {
-        if (i == d.i0) {
-          incF[0] = r[0] * d.dt;
-          incF[1] = P * d.dt;
-          incF[2] = r[2] * d.dt;
-        } else {
-          const double rm0 = (tid > 0) ? s_r[0][tid - 1] : prev[0];
-          const double rm2 = (tid > 0) ? s_r[2][tid - 1] : prev[2];
-          incF[0] = (1.5 * r[0] - .5 * rm0) * d.dt;
-          incF[1] = (1.5 * P - .5 * Pm) * d.dt;
-          incF[2] = (1.5 * r[2] - .5 * rm2) * d.dt;
-        }
-      }
-      if (vb) {
-        if (i == d.i0) {
-          incB[0] = r[0] * d.dt;
-          incB[1] = r[1] * d.dt;
-          incB[2] = r[2] * d.dt;
-        } else {
-          double rn[3];
-          if (tid < kTileThreads - 1) {
-            rn[0] = s_r[0][tid + 1];
-            rn[1] = s_r[1][tid + 1];
-            rn[2] = s_r[2][tid + 1];
-          } else {
-            phase_rates(d, spline4w(bv, d, sample_time(d, i + 1), w), rn);
-          }
-          incB[0] = (1.5 * r[0] - .5 * rn[0]) * d.dt;
-          incB[1] = (1.5 * r[1] - .5 * rn[1]) * d.dt;
-          incB[2] = (1.5 * r[2] - .5 * rn[2]) * d.dt;
-        }
-      }
-      double X[3];
-      double inclF[3] = {incF[0], incF[1], incF[2]}, totF[3];
-      block_scan3(inclF, red, totF);
-      double inclB[3] = {0.0, 0.0, 0.0}, totB[3] = {0.0, 0.0, 0.0};
-      if (d.i0 > 0 && c.start <= d.i0) {  // backward region present in this tile (tile-uniform)
-        inclB[0] = incB[0];
-        inclB[1] = incB[1];
-        inclB[2] = incB[2];
-        block_scan3(inclB, red, totB);
-      }
-#pragma unroll
-      for (int qq = 0; qq < 3; ++qq) {
-        // the tile-local part; the chain's carry is added after the look-back
-        if (i > d.i0) X[qq] = runF[qq] + (inclF[qq] - incF[qq]);  // forward increments of samples < i
-        else if (i == d.i0) X[qq] = X0[qq];
-        else X[qq] = runB[qq] + inclB[qq];                      // backward increments of samples <= i
-        runF[qq] += totF[qq];
-        runB[qq] += totB[qq];
-      }
-      if (in) {
-        const double nu = ((i > d.i0) ? P : r[1]) / 2. / kPi;
-        sv_e[sl] = q.e;
-        sv_om[sl] = om * d.M_phys_sec;
-        sv_gim[sl] = X[0];
-        sv_Phi[sl] = X[1];
-        sv_alp[sl] = X[2];
-        sv_nu[sl] = nu;
-        sv_gd[sl] = r[0];
+        if (i >= d.i0 && !(r[1] > 0.0)) nonpos = 1;
         if (bv.traj_out) {
           const int64_t o = d.out_offset + i;
           const int64_t st = bv.traj_stride;
@@ -1164,16 +1107,138 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           bv.traj_out[1 * st + o] = q.v;
           bv.traj_out[2 * st + o] = q.M;
           bv.traj_out[3 * st + o] = q.S;
-          bv.traj_out[7 * st + o] = nu;
           bv.traj_out[8 * st + o] = r[0];
         }
       }
-      const int ilast = c.start + ch * kTileThreads + kTileThreads - 1;
-      if (ilast >= d.i0) lastP = s_Pa[kTileThreads - 1];
-      prev[0] = s_r[0][kTileThreads - 1];
-      prev[2] = s_r[2][kTileThreads - 1];
+      sv_e[sl] = q.e;
+      sv_om[sl] = om * d.M_phys_sec;
+      sv_gim[sl] = r[0];
+      sv_Phi[sl] = r[1];
+      sv_alp[sl] = r[2];
+      sv_gd[sl] = r[0];
+    }
+    nonpos = __syncthreads_or(nonpos);
+    // (B) the clamped Phidot (AAK.cc:254: the raw rate if positive, else the
+    //     previous clamped value) where the clamp acts: one thread walks the
+    //     tile and parks it in the nu slots
+    if (nonpos) {
+      if (tid == 0) {
+        double P = Pin;
+        for (int sl = 0; sl < lim - c.start; ++sl)
+          if (c.start + sl >= d.i0) {
+            const double raw = sv_Phi[sl];
+            if (raw > 0.0) P = raw;
+            sv_nu[sl] = P;
+          }
+      }
       __syncthreads();
     }
+    // (C) AB2 increments of the thread's kSPT consecutive slots,
+    //     their running sums, and one block scan of the thread totals
+    constexpr int kSPT = kTileSamples / kTileThreads;
+    const int j0 = kSPT * tid;
+    double incF[kSPT][3], incB[kSPT][3], nuv[kSPT], Pl = 0.0;
+    {
+      double rm[3], Pm;  // rates and clamped Phidot of the slot before
+      if (j0 == 0) {
+        rm[0] = s_rb[0];
+        rm[1] = s_rb[1];
+        rm[2] = s_rb[2];
+        Pm = Pin;
+      } else {
+        rm[0] = sv_gim[j0 - 1];
+        rm[1] = sv_Phi[j0 - 1];
+        rm[2] = sv_alp[j0 - 1];
+        Pm = nonpos ? sv_nu[j0 - 1] : rm[1];
+      }
+      double rc[3] = {sv_gim[j0], sv_Phi[j0], sv_alp[j0]};
+#pragma unroll
+      for (int k = 0; k < kSPT; ++k) {
+        const int i = c.start + j0 + k;
+        const bool in = i < lim;
+        const bool vf = in && i >= d.i0;
+        const bool vb = in && i >= 1 && i <= d.i0;
+        double rn[3];  // rates of the slot after (the tile's last slot: the sample after the tile)
+        if (k + 1 < kSPT || j0 + kSPT < kTileSamples) {
+          rn[0] = sv_gim[j0 + k + 1];
+          rn[1] = sv_Phi[j0 + k + 1];
+          rn[2] = sv_alp[j0 + k + 1];
+        } else {
+          rn[0] = s_ra[0];
+          rn[1] = s_ra[1];
+          rn[2] = s_ra[2];
+        }
+        const double P = (vf && nonpos) ? sv_nu[j0 + k] : rc[1];
+        for (int qq = 0; qq < 3; ++qq) incF[k][qq] = incB[k][qq] = 0.0;
+        if (vf) {
+          if (i == d.i0) {
+            incF[k][0] = rc[0] * d.dt;
+            incF[k][1] = P * d.dt;
+            incF[k][2] = rc[2] * d.dt;
+          } else {
+            incF[k][0] = (1.5 * rc[0] - .5 * rm[0]) * d.dt;
+            incF[k][1] = (1.5 * P - .5 * Pm) * d.dt;
+            incF[k][2] = (1.5 * rc[2] - .5 * rm[2]) * d.dt;
+          }
+          if (i == lim - 1) Pl = P;
+        }
+        if (vb) {
+          if (i == d.i0) {
+            incB[k][0] = rc[0] * d.dt;
+            incB[k][1] = rc[1] * d.dt;
+            incB[k][2] = rc[2] * d.dt;
+          } else {
+            incB[k][0] = (1.5 * rc[0] - .5 * rn[0]) * d.dt;
+            incB[k][1] = (1.5 * rc[1] - .5 * rn[1]) * d.dt;
+            incB[k][2] = (1.5 * rc[2] - .5 * rn[2]) * d.dt;
+          }
+        }
+        nuv[k] = ((i > d.i0) ? P : rc[1]) / 2. / kPi;
+        rm[0] = rc[0];
+        rm[1] = rc[1];
+        rm[2] = rc[2];
+        Pm = P;
+        rc[0] = rn[0];
+        rc[1] = rn[1];
+        rc[2] = rn[2];
+      }
+      // the owner of the tile's last output sample records its clamped Phidot (forward samples)
+      if (lim - 1 >= d.i0 && lim - 1 >= c.start + j0 && lim - 1 < c.start + j0 + kSPT) s_lastP = Pl;
+    }
+    double tF[3] = {0, 0, 0}, tB[3] = {0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < kSPT; ++k)
+#pragma unroll
+      for (int qq = 0; qq < 3; ++qq) {
+        tF[qq] += incF[k][qq];
+        tB[qq] += incB[k][qq];
+      }
+    double runF[3], runB[3] = {0.0, 0.0, 0.0}, eF[3], eB[3] = {0.0, 0.0, 0.0};
+    block_exscan3(tF, red, eF, runF);  // its barriers order every read of (C) before the writes of (D)
+    if (d.i0 > 0 && c.start <= d.i0) block_exscan3(tB, red, eB, runB);  // backward region present (tile-uniform)
+    // (D) tile-local phases: forward, the increments of the tile's samples
+    //     before i; backward, those of its samples up to i; the chain's carry
+    //     is added after the look-back
+#pragma unroll
+    for (int k = 0; k < kSPT; ++k) {
+      const int sl = j0 + k;
+      const int i = c.start + sl;
+      if (i >= lim) break;
+      double *const svq[3] = {sv_gim, sv_Phi, sv_alp};
+#pragma unroll
+      for (int qq = 0; qq < 3; ++qq) {
+        double x;
+        if (i > d.i0) x = eF[qq];
+        else if (i == d.i0) x = X0[qq];
+        else x = eB[qq] + incB[k][qq];
+        svq[qq][sl] = x;
+        eF[qq] += incF[k][qq];
+        eB[qq] += incB[k][qq];
+      }
+      sv_nu[sl] = nuv[k];
+      if (bv.traj_out) bv.traj_out[7 * bv.traj_stride + d.out_offset + i] = nuv[k];
+    }
+    __syncthreads();
     // ---------------- chain carries: warp 0 publishes this tile's aggregate,
     // looks back for the exclusive prefix and publishes the inclusive record
     if (tid < 32) {

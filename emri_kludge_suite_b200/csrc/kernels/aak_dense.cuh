@@ -43,6 +43,7 @@ struct BatchView {
   int32_t nsrc;
   int64_t total_tiles;
   const int64_t *tile_start;    // nsrc + 1 prefix of tiles (device)
+  const int64_t *queue = nullptr;  // work-queue order (global tile indices); null: source by source, each in chain order
   const int32_t *tile_knot;     // 2 per tile: first knot of the tile's window, knots in it
   const double *knot_t;         // knots
   const double4 *knot_y;        // (e, v, M, S) at the knots
