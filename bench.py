@@ -150,7 +150,7 @@ def cpu_reference(sources, budget_s: float = 15.0, sample_len: int = 20000, proc
 FIDUCIAL = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])  # gpu_gen_AAK order
 # DRAM bytes (read + write) per sample of the split waveform kernel, from an ncu
 # capture of that kernel on 16 sources of the configuration-1 draw
-TRAFFIC_BYTES_PER_SAMPLE = (244.297728e6 + 403.781120e6) / 28_332_971
+TRAFFIC_BYTES_PER_SAMPLE = (238.248192e6 + 413.877248e6) / 28_332_971
 LIKE_LENGTH = 3_200_000  # 1 yr at dt = 10 s rounded up to the 5-smooth FFT length 2^10 * 5^5
 
 

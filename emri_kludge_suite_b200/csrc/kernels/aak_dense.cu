@@ -1640,7 +1640,7 @@ double probe_fp32_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
 // Tile scratch (look-back records and flags, the work-queue head and the
 // device status word) for callers that must not allocate device memory.  The
 // array is part of the module image: every GPU that loads this library holds
-// its 4 MB until the process exits.  All calls share it and it keeps the last
+// about 5 MB until the process exits.  All calls share it and it keeps the last
 // call's contents; launches that overlap on the GPU race on it.
 namespace {
 constexpr size_t kStaticLinkBytes = (size_t)kStaticScratchTiles * sizeof(TileLink);
