@@ -55,54 +55,6 @@ struct DevBuf {
 
 int cuda_ok(cudaError_t e) { return cuda_status_of(e); }
 
-// Host array for the packed plan: page-locked when a device is in use (the
-// upload then runs at full PCIe rate), capacity kept across plans, resized
-// without value-initialisation.
-template <typename T>
-struct HostBuf {
-  T *p = nullptr;
-  size_t n = 0, cap = 0;
-  bool pinned = false;
-  bool want_pinned = true;
-  HostBuf() = default;
-  HostBuf(const HostBuf &) = delete;
-  HostBuf &operator=(const HostBuf &) = delete;
-  ~HostBuf() { release(); }
-  int resize(size_t m) {
-    if (m <= cap && p) {
-      n = m;
-      return AAK_OK;
-    }
-    release();
-    const size_t want = std::max<size_t>(m + m / 8, 1);
-    void *q = nullptr;
-    if (want_pinned && cudaHostAlloc(&q, want * sizeof(T), cudaHostAllocPortable) == cudaSuccess) {
-      pinned = true;
-    } else {
-      cudaGetLastError();
-      q = std::malloc(want * sizeof(T));
-      pinned = false;
-      if (!q) return AAK_ERR_NO_MEMORY;
-    }
-    p = static_cast<T *>(q);
-    cap = want;
-    n = m;
-    return AAK_OK;
-  }
-  void release() {
-    if (p) {
-      if (pinned) cudaFreeHost(p);
-      else std::free(p);
-    }
-    p = nullptr;
-    n = cap = 0;
-  }
-  T *data() { return p; }
-  const T *data() const { return p; }
-  size_t size() const { return n; }
-  T &operator[](size_t i) { return p[i]; }
-  const T &operator[](size_t i) const { return p[i]; }
-};
 
 }  // namespace
 
@@ -119,8 +71,8 @@ struct aak_ctx {
   std::vector<int64_t> tile_pairs;  // per source {0, its tiles}: the tile prefix of a one-source view
   std::vector<int64_t> queue;       // work-queue order of the tiles (global tile indices)
   std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
-  HostBuf<double> knot_t;
-  HostBuf<double4> knot_y, knot_c;
+  std::vector<int64_t> kofs;       // nsrc + 1 prefix of knots (the sources' knots stay in their plans)
+  bool want_pinned = true;         // plans' knot arrays in page-locked memory
   std::vector<int32_t> bessel;
   int64_t total_samples = 0, total_tiles = 0, total_knots = 0;
   int32_t max_nmodes = 0;
@@ -246,13 +198,12 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
   ctx->total_samples = ctx->offsets[n];
   ctx->total_tiles = ctx->tile_start[n];
   ctx->total_knots = knots;
-  int r;
-  if ((r = ctx->knot_t.resize(std::max<int64_t>(knots, 1))) || (r = ctx->knot_y.resize(std::max<int64_t>(knots, 1))) ||
-      (r = ctx->knot_c.resize(std::max<int64_t>(knots, 1))))
-    return r;
   ctx->bessel.resize(std::max<int64_t>(bes, 1));
-  // per-source offsets into the flat arrays, then the copies in parallel
-  std::vector<int64_t> kofs(n + 1, 0), bofs(n + 1, 0);
+  // per-source offsets into the device arrays; the knots themselves are
+  // uploaded from each plan's page-locked arrays (no host-side repacking)
+  std::vector<int64_t> &kofs = ctx->kofs;
+  kofs.assign(n + 1, 0);
+  std::vector<int64_t> bofs(n + 1, 0);
   for (int s = 0; s < n; ++s) {
     const bool ok = ctx->status[s] == AAK_OK;
     kofs[s + 1] = kofs[s] + (ok ? (int64_t)ctx->plans[s].knot_t.size() : 0);
@@ -268,12 +219,6 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
     if (ctx->status[s] == AAK_OK) {
       d = pl.desc;
       const int64_t ko = kofs[s], bo = bofs[s];
-      const int64_t nk = (int64_t)pl.knot_t.size();
-      for (int64_t k = 0; k < nk; ++k) {
-        ctx->knot_t[ko + k] = pl.knot_t[k];
-        ctx->knot_y[ko + k] = make_double4(pl.knot_y[4 * k], pl.knot_y[4 * k + 1], pl.knot_y[4 * k + 2], pl.knot_y[4 * k + 3]);
-        ctx->knot_c[ko + k] = make_double4(pl.knot_c[4 * k], pl.knot_c[4 * k + 1], pl.knot_c[4 * k + 2], pl.knot_c[4 * k + 3]);
-      }
       d.knot_offset = ko;
       d.bessel_offset = (int32_t)bo;
       for (int m = 1; m <= pl.nmodes; ++m) ctx->bessel[bo + m - 1] = bessel_start_order(m, pl.e_max, 12);  // table rows reach order n + 2 + 12
@@ -288,7 +233,7 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
     ctx->descs[s] = d;
     if (ctx->status[s] != AAK_OK) return;
     // knot window of every tile: knots bracketing samples start-1 .. start+1024
-    const double *kt = ctx->knot_t.data() + d.knot_offset;
+    const double *kt = pl.knot_t.data();
     const int nk = d.n_knots;
     auto tsample = [&](int i) { return (i == 0) ? d.t_first : (double)(i - d.i0) * d.dt; };
     int k0 = 0, k1 = 0;
@@ -350,6 +295,7 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
     if (p.length < 2 || p.length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
   ctx->nsrc = nsrc;
   ctx->plans.resize(nsrc);  // earlier plans keep their array capacity
+  for (auto &pl : ctx->plans) pl.knot_t.want_pinned = pl.knot_y.want_pinned = pl.knot_c.want_pinned = ctx->want_pinned;
   ctx->status.assign(nsrc, AAK_OK);
   ctx->newton_points = ctx->newton_iters = ctx->newton_fallbacks = 0;
   if (maps) {
@@ -421,8 +367,9 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
       (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) || (r = ctx->d_tile_pairs.reserve(ctx->tile_pairs.size())) ||
       (r = ctx->d_queue.reserve(ctx->queue.size())) ||
-      (r = ctx->d_knot_t.reserve(ctx->knot_t.size())) || (r = ctx->d_knot_y.reserve(ctx->knot_y.size())) ||
-      (r = ctx->d_knot_c.reserve(ctx->knot_c.size())) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
+      (r = ctx->d_knot_t.reserve(std::max<int64_t>(ctx->total_knots, 1))) ||
+      (r = ctx->d_knot_y.reserve(std::max<int64_t>(ctx->total_knots, 1))) ||
+      (r = ctx->d_knot_c.reserve(std::max<int64_t>(ctx->total_knots, 1))) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
       (r = ctx->d_link.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
       (r = ctx->d_flag.reserve(std::max<int64_t>(ctx->total_tiles, 1))) || (r = ctx->d_counter.reserve(2)))
     return r;
@@ -436,14 +383,22 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
       (r = cp(ctx->d_tile_knot.ptr, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
       (r = cp(ctx->d_tile_pairs.ptr, ctx->tile_pairs.data(), ctx->tile_pairs.size() * sizeof(int64_t))) ||
       (r = cp(ctx->d_queue.ptr, ctx->queue.data(), ctx->queue.size() * sizeof(int64_t))) ||
-      (r = cp(ctx->d_knot_t.ptr, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
-      (r = cp(ctx->d_knot_y.ptr, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
-      (r = cp(ctx->d_knot_c.ptr, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
       (r = cp(ctx->d_bessel.ptr, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
     return r;
+  // knots straight from each source's plan arrays to its slice of the device arrays
+  for (int s = 0; s < n; ++s) {
+    const SourcePlan &pl = ctx->plans[s];
+    const int64_t nk = ctx->kofs[s + 1] - ctx->kofs[s];
+    if (nk <= 0) continue;
+    const int64_t ko = ctx->kofs[s];
+    if ((r = cp(ctx->d_knot_t.ptr + ko, pl.knot_t.data(), nk * sizeof(double))) ||
+        (r = cp(ctx->d_knot_y.ptr + ko, pl.knot_y.data(), nk * sizeof(double4))) ||
+        (r = cp(ctx->d_knot_c.ptr + ko, pl.knot_c.data(), nk * sizeof(double4))))
+      return r;
+  }
   // copies from page-locked memory run asynchronously: finish them before the
   // host arrays can be refilled by the next plan
-  if (ctx->knot_t.pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
+  if (ctx->want_pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
   ctx->uploaded = true;
   ++ctx->upload_gen;
   return AAK_OK;
@@ -700,7 +655,7 @@ int aak_ctx_create(int32_t device, aak_ctx **out) {
   aak_ctx *c = new (std::nothrow) aak_ctx();
   if (!c) return AAK_ERR_NO_MEMORY;
   c->device = device;
-  c->knot_t.want_pinned = c->knot_y.want_pinned = c->knot_c.want_pinned = device >= 0;
+  c->want_pinned = device >= 0;
   int sms = 0;
   if (device >= 0 && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
     c->num_sms = sms;
@@ -778,8 +733,7 @@ int aak_batch_plan_bytes(aak_ctx *ctx, int64_t *bytes) {
   if (!ctx || !bytes) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
   *bytes = (int64_t)(ctx->descs.size() * sizeof(SourceDesc) + ctx->tile_start.size() * sizeof(int64_t) +
-                     ctx->knot_t.size() * sizeof(double) + 2 * ctx->knot_y.size() * sizeof(double4) +
-                     ctx->bessel.size() * sizeof(int32_t));
+                     ctx->total_knots * (sizeof(double) + 2 * sizeof(double4)) + ctx->bessel.size() * sizeof(int32_t));
   return AAK_OK;
 }
 
@@ -814,9 +768,10 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   const size_t o_ts = al(ctx->descs.size() * sizeof(SourceDesc));
   const size_t o_tk = o_ts + al(ctx->tile_start.size() * sizeof(int64_t));
   const size_t o_kt = o_tk + al(ctx->tile_knot.size() * sizeof(int32_t));
-  const size_t o_ky = o_kt + al(ctx->knot_t.size() * sizeof(double));
-  const size_t o_kc = o_ky + al(ctx->knot_y.size() * sizeof(double4));
-  const size_t o_bs = o_kc + al(ctx->knot_c.size() * sizeof(double4));
+  const size_t nknots = (size_t)std::max<int64_t>(ctx->total_knots, 1);
+  const size_t o_ky = o_kt + al(nknots * sizeof(double));
+  const size_t o_kc = o_ky + al(nknots * sizeof(double4));
+  const size_t o_bs = o_kc + al(nknots * sizeof(double4));
   const size_t need = o_bs + al(ctx->bessel.size() * sizeof(int32_t));
   if (required_bytes) *required_bytes = (int64_t)need;
   if (!d_plan) return AAK_OK;  // size query only
@@ -833,12 +788,19 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   if ((r = cp(0, ctx->descs.data(), ctx->descs.size() * sizeof(SourceDesc))) ||
       (r = cp(o_ts, ctx->tile_start.data(), ctx->tile_start.size() * sizeof(int64_t))) ||
       (r = cp(o_tk, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
-      (r = cp(o_kt, ctx->knot_t.data(), ctx->knot_t.size() * sizeof(double))) ||
-      (r = cp(o_ky, ctx->knot_y.data(), ctx->knot_y.size() * sizeof(double4))) ||
-      (r = cp(o_kc, ctx->knot_c.data(), ctx->knot_c.size() * sizeof(double4))) ||
       (r = cp(o_bs, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
     return r;
-  if (ctx->knot_t.pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;  // host arrays reusable on return
+  for (int s = 0; s < ctx->nsrc; ++s) {
+    const SourcePlan &pl = ctx->plans[s];
+    const int64_t nk = ctx->kofs[s + 1] - ctx->kofs[s];
+    if (nk <= 0) continue;
+    const size_t ko = (size_t)ctx->kofs[s];
+    if ((r = cp(o_kt + ko * sizeof(double), pl.knot_t.data(), nk * sizeof(double))) ||
+        (r = cp(o_ky + ko * sizeof(double4), pl.knot_y.data(), nk * sizeof(double4))) ||
+        (r = cp(o_kc + ko * sizeof(double4), pl.knot_c.data(), nk * sizeof(double4))))
+      return r;
+  }
+  if (ctx->want_pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;  // host arrays reusable on return
   BatchView bv;
   std::memset(&bv, 0, sizeof(bv));
   bv.src = reinterpret_cast<const SourceDesc *>(base);

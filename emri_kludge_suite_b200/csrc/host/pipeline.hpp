@@ -4,8 +4,12 @@
 // interpolate.  Everything here is re-entrant (no static state).
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
+#include <cstring>
+#include <new>
 #include <vector>
 
 #include "../aak_common.hpp"
@@ -104,6 +108,79 @@ struct WaveInputs {
 // Pack GenWave's par[12], zeta and harmonic count (AAK.cc:565-591).
 void genwave_inputs(const Params &P, const MappedTrajectory &mt, int nmodes_override, WaveInputs *w);
 
+// Growable array for a source's knots.  With want_pinned it lives in
+// page-locked host memory (falling back to pageable memory when that fails,
+// e.g. without a GPU), so that the batch upload copies straight from it to the
+// device with no host-side repacking.  Capacity is kept across plans; growth
+// keeps the contents, like std::vector::resize, but new elements are not
+// initialised.
+template <typename T>
+struct KnotBuf {
+  T *p = nullptr;
+  size_t n = 0, cap = 0;
+  bool pinned = false, want_pinned = false;
+  KnotBuf() = default;
+  KnotBuf(const KnotBuf &) = delete;
+  KnotBuf &operator=(const KnotBuf &) = delete;
+  KnotBuf(KnotBuf &&o) noexcept { take(o); }
+  KnotBuf &operator=(KnotBuf &&o) noexcept {
+    if (this != &o) {
+      release();
+      take(o);
+    }
+    return *this;
+  }
+  ~KnotBuf() { release(); }
+  void resize(size_t m) {
+    if (m > cap) {
+      const size_t want = m + m / 8;
+      void *q = nullptr;
+      bool pin = false;
+      if (want_pinned && cudaHostAlloc(&q, want * sizeof(T), cudaHostAllocPortable) == cudaSuccess) {
+        pin = true;
+      } else {
+        if (want_pinned) cudaGetLastError();
+        q = std::malloc(want * sizeof(T));
+        if (!q) throw std::bad_alloc();
+      }
+      if (n) std::memcpy(q, p, n * sizeof(T));
+      release_storage();
+      p = static_cast<T *>(q);
+      cap = want;
+      pinned = pin;
+    }
+    n = m;
+  }
+  void clear() { n = 0; }
+  T *data() { return p; }
+  const T *data() const { return p; }
+  size_t size() const { return n; }
+  T &operator[](size_t i) { return p[i]; }
+  const T &operator[](size_t i) const { return p[i]; }
+
+ private:
+  void take(KnotBuf &o) {
+    p = o.p;
+    n = o.n;
+    cap = o.cap;
+    pinned = o.pinned;
+    want_pinned = o.want_pinned;
+    o.p = nullptr;
+    o.n = o.cap = 0;
+  }
+  void release_storage() {
+    if (p) {
+      if (pinned) cudaFreeHost(p);
+      else std::free(p);
+    }
+    p = nullptr;
+  }
+  void release() {
+    release_storage();
+    n = cap = 0;
+  }
+};
+
 // Coarse AK evolution and spline knots (AAK.cc:27-242): everything of
 // PNevolution except the dense loops, which the kernels perform.
 struct SourcePlan {
@@ -113,9 +190,9 @@ struct SourcePlan {
   int nmodes = 0;
   double dt = 0, t_first = 0, t_last = 0;
   double e_max = 0;
-  std::vector<double> knot_t;   // n_knots
-  std::vector<double> knot_y;   // n_knots x 4 (e, v, M, S)
-  std::vector<double> knot_c;   // n_knots x 4 (natural-spline half second derivatives)
+  KnotBuf<double> knot_t;       // n_knots
+  KnotBuf<double> knot_y;       // n_knots x 4 (e, v, M, S): the layout of double4[n_knots]
+  KnotBuf<double> knot_c;       // n_knots x 4 (natural-spline half second derivatives)
   SourceDesc desc;              // offsets filled in by the batch builder
 };
 
