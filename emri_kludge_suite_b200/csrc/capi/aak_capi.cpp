@@ -337,9 +337,26 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
     for (int s = 0; s < nsrc; ++s)
       for (int64_t i = first[s]; i < first[s + 1]; ++i) parmap_from_coords(&xs[4 * i], Pv[s].M, &ys[3 * i], &warm[3 * i]);
   }
-  // (3) Kerr -> AK map, coarse AK evolution, knots
+  // (3) Kerr -> AK map, coarse AK evolution, knots; largest sources first.
+  // A source's knot count is about (steps - 1) max(1, r / T_fit), r its
+  // observation time in radiation-reaction units (the coarse grid spans
+  // min(T_fit, r)), and the coarse evolution costs about the same per knot,
+  // so handing sources out in that order keeps host threads from idling
+  // behind one long source at the end.
+  std::vector<int> order(nsrc);
+  {
+    std::vector<double> cost(nsrc, 0.0);
+    for (int s = 0; s < nsrc; ++s) {
+      const aak_params &q = Pv[s];
+      const double r = q.length * q.dt * q.mu / (kMsunSec * q.M * q.M);
+      cost[s] = (q.T_fit > 0 && std::isfinite(r)) ? std::max(1.0, r / q.T_fit) : 0.0;
+    }
+    for (int s = 0; s < nsrc; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  }
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
-  parallel_for(nsrc, nthreads, [&](int64_t s) {
+  parallel_for(nsrc, nthreads, [&](int64_t k) {
+    const int64_t s = order[k];
     const Params Pp = to_params(Pv[s]);
     MappedTrajectory mt;
     int st = ctx->status[s];

@@ -289,30 +289,54 @@ void spline_second_derivs(const double *x, const double *y, int n, int stride, d
 }
 
 void spline_second_derivs4(const double *x, const double *y, int n, double *c) {
-  for (int k = 0; k < 4 * n; ++k) c[k] = 0.0;
-  if (n < 3) return;
+  for (int k = 0; k < 4 && k < 4 * n; ++k) c[k] = 0.0;
+  if (n < 3) {
+    for (int k = 4; k < 4 * n; ++k) c[k] = 0.0;
+    return;
+  }
+  for (int q = 0; q < 4; ++q) c[4 * (size_t)(n - 1) + q] = 0.0;
   const int m = n - 2;
-  std::vector<double> cp(m), dp(4 * (size_t)m);
+  // Thomas sweep with the forward values written straight into c (row k + 1);
+  // the knots are (nearly) evenly spaced, so a reciprocal whose operands
+  // repeat bit for bit is reused instead of recomputed (same values, no
+  // division)
+  static thread_local std::vector<double> cp_buf;
+  if (cp_buf.size() < (size_t)m) cp_buf.resize(m);
+  double *cp = cp_buf.data();
   double inv_h0 = 1.0 / (x[1] - x[0]);
+  double dprev[4];
+  for (int q = 0; q < 4; ++q) dprev[q] = y[4 + q] - y[q];
+  double h0p = 0.0, h1p = 0.0, invp = 0.0, inv_h1p = 0.0;
   for (int k = 0; k < m; ++k) {
     const int i = k + 1;
     const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
-    const double inv_h1 = 1.0 / h1;
+    const double inv_h1 = (k > 0 && h1 == h1p) ? inv_h1p : 1.0 / h1;
     const double sup = (k + 1 < m) ? h1 : 0.0;
-    const double den = (k == 0) ? 2.0 * (h0 + h1) : 2.0 * (h0 + h1) - h0 * cp[k - 1];
-    const double inv = 1.0 / den;
+    double inv;
+    if (k >= 2 && h0 == h0p && h1 == h1p && cp[k - 1] == cp[k - 2]) {
+      inv = invp;  // same den = 2 (h0 + h1) - h0 cp[k-1] as the previous row
+    } else {
+      const double den = (k == 0) ? 2.0 * (h0 + h1) : 2.0 * (h0 + h1) - h0 * cp[k - 1];
+      inv = 1.0 / den;
+    }
     cp[k] = sup * inv;
+    double *row = c + 4 * (size_t)i;
     for (int q = 0; q < 4; ++q) {
-      const double rhs =
-          3.0 * ((y[4 * (i + 1) + q] - y[4 * i + q]) * inv_h1 - (y[4 * i + q] - y[4 * (i - 1) + q]) * inv_h0);
-      dp[4 * (size_t)k + q] = (k == 0) ? rhs * inv : (rhs - h0 * dp[4 * (size_t)(k - 1) + q]) * inv;
+      const double dnext = y[4 * (size_t)(i + 1) + q] - y[4 * (size_t)i + q];
+      const double rhs = 3.0 * (dnext * inv_h1 - dprev[q] * inv_h0);
+      row[q] = (k == 0) ? rhs * inv : (rhs - h0 * row[q - 4]) * inv;
+      dprev[q] = dnext;
     }
     inv_h0 = inv_h1;
+    h0p = h0;
+    h1p = h1;
+    invp = inv;
+    inv_h1p = inv_h1;
   }
-  for (int k = m - 2; k >= 0; --k)
-    for (int q = 0; q < 4; ++q) dp[4 * (size_t)k + q] -= cp[k] * dp[4 * (size_t)(k + 1) + q];
-  for (int k = 0; k < m; ++k)
-    for (int q = 0; q < 4; ++q) c[4 * (size_t)(k + 1) + q] = dp[4 * (size_t)k + q];
+  for (int k = m - 2; k >= 0; --k) {
+    double *row = c + 4 * (size_t)(k + 1);
+    for (int q = 0; q < 4; ++q) row[q] -= cp[k] * row[q + 4];
+  }
 }
 
 double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv) {
@@ -437,11 +461,14 @@ void polyfit(double *coeff, const double *x, const double *y, int n) {
 
 // Semi-latus rectum from the AK azimuthal frequency: (1 - e^2) (Omega_phi M_phys)^(-2/3)
 // (AAK.cc:157-170), with Omega_phi's two PN ratios taken with one division.
-inline double p_of(double v, double e, double coslam, double S, double M, double M_phys) {
+inline double om_x(double v, double e, double coslam, double S, double M, double M_phys) {
   double om;
   if (coslam > 0) om = 16. * (v * v * v) * pn_dphidm_num(v, e, coslam, S) / (pn_dtdm_num(v, e, coslam, S) * M);
   else om = omega_phi(v, e, coslam, S, M);
-  const double c = std::cbrt(om * M_phys * kMsunSec);
+  return om * M_phys * kMsunSec;
+}
+inline double p_of(double v, double e, double coslam, double S, double M, double M_phys) {
+  const double c = std::cbrt(om_x(v, e, coslam, S, M, M_phys));
   return (1. - e * e) / (c * c);
 }
 
@@ -602,9 +629,16 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   const double z2 = std::sqrt(3. * S_phys * S_phys + z1 * z1);
   const double LSO_min = 3. + z2 - std::sqrt((3. - z1) * (3. + z1 + 2. * z2));
   const double LSO_max = 3. + z2 + std::sqrt((3. - z1) * (3. + z1 + 2. * z2));
+  // p^3 = (1 - e^2)^3 / x^2: a knot whose p^3 clears LSO_max^3 by a margin far
+  // beyond rounding fails both tests below, and needs no cube root
+  const double lso3 = LSO_max * LSO_max * LSO_max * (1.0 + 1e-9);
   for (int j = j0; j <= j_max_temp; ++j) {
     if (j > j_max) break;
-    const double pj = p_of(v_fit[j], e_fit[j], coslam, S_fit[j], M_fit[j], M_phys);
+    const double x = om_x(v_fit[j], e_fit[j], coslam, S_fit[j], M_fit[j], M_phys);
+    const double ome = 1. - e_fit[j] * e_fit[j];
+    if (ome * ome * ome > lso3 * (x * x)) continue;
+    const double cx = std::cbrt(x);
+    const double pj = ome / (cx * cx);
     if (pj < LSO_min && j_max == j_max_temp) {
       j_min = std::max(j - j_RR, j0);
       j_max = std::min(j + 1, j_max_temp);
