@@ -376,7 +376,8 @@ int bessel_start_order(int n, double e_max, int extra) {
 namespace {
 // dv/dt and de/dt of the AK equations (KSParMap.cc:86-144); lv = log(v) and
 // ome15 = (1 - e^2)^1.5 are shared by the two.
-double dvdt_core(double v, double e, double Y, double m, double M, double q, double lv, double ome15) {
+__attribute__((always_inline)) inline double dvdt_core(double v, double e, double Y, double m, double M, double q, double lv,
+                                                        double ome15) {
   const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
   const double e2 = e * e, e4 = e2 * e2, e6 = e4 * e2;
   const double Y2 = Y * Y, q2 = q * q;
@@ -406,7 +407,8 @@ double dvdt_core(double v, double e, double Y, double m, double M, double q, dou
   return 32. * ome15 * m * v6 * v3 * s / (5. * M * M);
 }
 
-double dedt_core(double v, double e, double Y, double m, double M, double q, double lv, double ome15) {
+__attribute__((always_inline)) inline double dedt_core(double v, double e, double Y, double m, double M, double q, double lv,
+                                                        double ome15) {
   const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
   const double e2 = e * e, e4 = e2 * e2;
   const double Y2 = Y * Y, q2 = q * q;
@@ -430,7 +432,10 @@ double dedt_core(double v, double e, double Y, double m, double M, double q, dou
   return -(e * ome15 * m * v6 * v2 * s) / (120960. * M * M);
 }
 
-void ak_rates(double v, double e, double Y, double m, double M, double q, double *edot, double *vdot) {
+// Inlined into the evolution loops, so that the compiler keeps the terms that
+// depend only on the source (spin, inclination) out of the per-knot work.
+__attribute__((always_inline)) inline void ak_rates(double v, double e, double Y, double m, double M, double q,
+                                                    double *edot, double *vdot) {
   const double ome = 1. - e * e;
   const double lv = std::log(v), ome15 = ome * std::sqrt(ome);
   *edot = dedt_core(v, e, Y, m, M, q, lv, ome15);
