@@ -294,7 +294,9 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   for (auto &p : Pv)
     if (p.length < 2 || p.length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
   ctx->nsrc = nsrc;
-  ctx->plans.resize(nsrc);  // earlier plans keep their array capacity
+  // the plan array only grows: plans past nsrc keep their page-locked knot
+  // arrays for later, larger batches (pinning is slow; only nsrc bounds the live part)
+  if ((int32_t)ctx->plans.size() < nsrc) ctx->plans.resize(nsrc);
   for (auto &pl : ctx->plans) pl.knot_t.want_pinned = pl.knot_y.want_pinned = pl.knot_c.want_pinned = ctx->want_pinned;
   ctx->status.assign(nsrc, AAK_OK);
   ctx->newton_points = ctx->newton_iters = ctx->newton_fallbacks = 0;
