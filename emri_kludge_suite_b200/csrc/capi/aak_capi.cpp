@@ -72,6 +72,7 @@ struct aak_ctx {
   std::vector<int64_t> queue;       // work-queue order of the tiles (global tile indices)
   std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
   std::vector<int64_t> kofs;       // nsrc + 1 prefix of knots (the sources' knots stay in their plans)
+  std::vector<int64_t> spl_blk;    // nsrc + 1 prefix of the device spline solve's blocks
   bool want_pinned = true;         // plans' knot arrays in page-locked memory
   std::vector<int32_t> bessel;
   int64_t total_samples = 0, total_tiles = 0, total_knots = 0;
@@ -80,7 +81,7 @@ struct aak_ctx {
   bool uploaded = false;
   // device buffers
   DevBuf<SourceDesc> d_src;
-  DevBuf<int64_t> d_tile_start, d_tile_pairs, d_queue;
+  DevBuf<int64_t> d_tile_start, d_tile_pairs, d_queue, d_spl_blk;
   DevBuf<int32_t> d_tile_knot;
   DevBuf<double> d_knot_t;
   DevBuf<double4> d_knot_y, d_knot_c;
@@ -209,6 +210,9 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
     kofs[s + 1] = kofs[s] + (ok ? (int64_t)ctx->plans[s].knot_t.size() : 0);
     bofs[s + 1] = bofs[s] + (ok ? ctx->plans[s].nmodes : 0);
   }
+  ctx->spl_blk.assign(n + 1, 0);
+  for (int s = 0; s < n; ++s)
+    ctx->spl_blk[s + 1] = ctx->spl_blk[s] + (ctx->status[s] == AAK_OK ? spline_blocks((int)ctx->plans[s].knot_t.size()) : 0);
   ctx->tile_pairs.assign(2 * (size_t)n, 0);
   for (int s = 0; s < n; ++s) ctx->tile_pairs[2 * s + 1] = ctx->tile_start[s + 1] - ctx->tile_start[s];
   ctx->tile_knot.assign(2 * std::max<int64_t>(ctx->total_tiles, 1), 0);
@@ -283,7 +287,6 @@ void finish_source(aak_ctx *ctx, int s, const Params &Pp, const MappedTrajectory
   if (st != kOk) {
     ctx->plans[s].knot_t.clear();
     ctx->plans[s].knot_y.clear();
-    ctx->plans[s].knot_c.clear();
   }
 }
 
@@ -297,7 +300,7 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   // the plan array only grows: plans past nsrc keep their page-locked knot
   // arrays for later, larger batches (pinning is slow; only nsrc bounds the live part)
   if ((int32_t)ctx->plans.size() < nsrc) ctx->plans.resize(nsrc);
-  for (auto &pl : ctx->plans) pl.knot_t.want_pinned = pl.knot_y.want_pinned = pl.knot_c.want_pinned = ctx->want_pinned;
+  for (auto &pl : ctx->plans) pl.knot_t.want_pinned = pl.knot_y.want_pinned = ctx->want_pinned;
   ctx->status.assign(nsrc, AAK_OK);
   ctx->newton_points = ctx->newton_iters = ctx->newton_fallbacks = 0;
   if (maps) {
@@ -385,7 +388,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   const int n = ctx->nsrc;
   if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
       (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) || (r = ctx->d_tile_pairs.reserve(ctx->tile_pairs.size())) ||
-      (r = ctx->d_queue.reserve(ctx->queue.size())) ||
+      (r = ctx->d_queue.reserve(ctx->queue.size())) || (r = ctx->d_spl_blk.reserve(ctx->spl_blk.size())) ||
       (r = ctx->d_knot_t.reserve(std::max<int64_t>(ctx->total_knots, 1))) ||
       (r = ctx->d_knot_y.reserve(std::max<int64_t>(ctx->total_knots, 1))) ||
       (r = ctx->d_knot_c.reserve(std::max<int64_t>(ctx->total_knots, 1))) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
@@ -402,6 +405,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
       (r = cp(ctx->d_tile_knot.ptr, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
       (r = cp(ctx->d_tile_pairs.ptr, ctx->tile_pairs.data(), ctx->tile_pairs.size() * sizeof(int64_t))) ||
       (r = cp(ctx->d_queue.ptr, ctx->queue.data(), ctx->queue.size() * sizeof(int64_t))) ||
+      (r = cp(ctx->d_spl_blk.ptr, ctx->spl_blk.data(), ctx->spl_blk.size() * sizeof(int64_t))) ||
       (r = cp(ctx->d_bessel.ptr, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
     return r;
   // knots straight from each source's plan arrays to its slice of the device arrays
@@ -411,10 +415,13 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
     if (nk <= 0) continue;
     const int64_t ko = ctx->kofs[s];
     if ((r = cp(ctx->d_knot_t.ptr + ko, pl.knot_t.data(), nk * sizeof(double))) ||
-        (r = cp(ctx->d_knot_y.ptr + ko, pl.knot_y.data(), nk * sizeof(double4))) ||
-        (r = cp(ctx->d_knot_c.ptr + ko, pl.knot_c.data(), nk * sizeof(double4))))
+        (r = cp(ctx->d_knot_y.ptr + ko, pl.knot_y.data(), nk * sizeof(double4))))
       return r;
   }
+  // spline coefficients of every source, solved on the device
+  launch_spline_coeffs(ctx->d_src.ptr, n, ctx->d_spl_blk.ptr, ctx->spl_blk[n], ctx->d_knot_t.ptr, ctx->d_knot_y.ptr,
+                       ctx->d_knot_c.ptr, st);
+  if ((r = cuda_ok(cudaGetLastError())) != AAK_OK) return r;
   // copies from page-locked memory run asynchronously: finish them before the
   // host arrays can be refilled by the next plan
   if (ctx->want_pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
@@ -689,6 +696,8 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_tile_start.release();
     c->d_tile_knot.release();
     c->d_tile_pairs.release();
+    c->d_queue.release();
+    c->d_spl_blk.release();
     c->d_knot_t.release();
     c->d_knot_y.release();
     c->d_knot_c.release();
@@ -751,8 +760,13 @@ int aak_batch_info(aak_ctx *ctx, int64_t *total, int64_t *offsets, int32_t *stat
 int aak_batch_plan_bytes(aak_ctx *ctx, int64_t *bytes) {
   if (!ctx || !bytes) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
+  // everything upload() copies: descriptors, tile and queue arrays, knots (t and
+  // (e, v, M, S); the spline coefficients are solved on the device), Miller
+  // start orders and the spline-block prefix
   *bytes = (int64_t)(ctx->descs.size() * sizeof(SourceDesc) + ctx->tile_start.size() * sizeof(int64_t) +
-                     ctx->total_knots * (sizeof(double) + 2 * sizeof(double4)) + ctx->bessel.size() * sizeof(int32_t));
+                     ctx->tile_knot.size() * sizeof(int32_t) + ctx->tile_pairs.size() * sizeof(int64_t) +
+                     ctx->queue.size() * sizeof(int64_t) + ctx->total_knots * (sizeof(double) + sizeof(double4)) +
+                     ctx->bessel.size() * sizeof(int32_t) + ctx->spl_blk.size() * sizeof(int64_t));
   return AAK_OK;
 }
 
@@ -791,7 +805,8 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   const size_t o_ky = o_kt + al(nknots * sizeof(double));
   const size_t o_kc = o_ky + al(nknots * sizeof(double4));
   const size_t o_bs = o_kc + al(nknots * sizeof(double4));
-  const size_t need = o_bs + al(ctx->bessel.size() * sizeof(int32_t));
+  const size_t o_sb = o_bs + al(ctx->bessel.size() * sizeof(int32_t));
+  const size_t need = o_sb + al(ctx->spl_blk.size() * sizeof(int64_t));
   if (required_bytes) *required_bytes = (int64_t)need;
   if (!d_plan) return AAK_OK;  // size query only
   if (plan_bytes < 0 || (size_t)plan_bytes < need) return AAK_ERR_CAPACITY;
@@ -807,7 +822,8 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   if ((r = cp(0, ctx->descs.data(), ctx->descs.size() * sizeof(SourceDesc))) ||
       (r = cp(o_ts, ctx->tile_start.data(), ctx->tile_start.size() * sizeof(int64_t))) ||
       (r = cp(o_tk, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
-      (r = cp(o_bs, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
+      (r = cp(o_bs, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))) ||
+      (r = cp(o_sb, ctx->spl_blk.data(), ctx->spl_blk.size() * sizeof(int64_t))))
     return r;
   for (int s = 0; s < ctx->nsrc; ++s) {
     const SourcePlan &pl = ctx->plans[s];
@@ -815,10 +831,13 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
     if (nk <= 0) continue;
     const size_t ko = (size_t)ctx->kofs[s];
     if ((r = cp(o_kt + ko * sizeof(double), pl.knot_t.data(), nk * sizeof(double))) ||
-        (r = cp(o_ky + ko * sizeof(double4), pl.knot_y.data(), nk * sizeof(double4))) ||
-        (r = cp(o_kc + ko * sizeof(double4), pl.knot_c.data(), nk * sizeof(double4))))
+        (r = cp(o_ky + ko * sizeof(double4), pl.knot_y.data(), nk * sizeof(double4))))
       return r;
   }
+  launch_spline_coeffs(reinterpret_cast<const SourceDesc *>(base), ctx->nsrc, reinterpret_cast<const int64_t *>(base + o_sb),
+                       ctx->spl_blk[ctx->nsrc], reinterpret_cast<const double *>(base + o_kt),
+                       reinterpret_cast<const double4 *>(base + o_ky), reinterpret_cast<double4 *>(base + o_kc), st);
+  if ((r = cuda_ok(cudaGetLastError())) != AAK_OK) return r;
   if (ctx->want_pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;  // host arrays reusable on return
   BatchView bv;
   std::memset(&bv, 0, sizeof(bv));

@@ -264,95 +264,55 @@ void genwave_inputs(const Params &P, const MappedTrajectory &mt, int nmodes_over
 }
 
 // ------------------------------------------------------------------ splines
-void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c) {
-  for (int k = 0; k < n; ++k) c[k * stride] = 0.0;
-  if (n < 3) return;
-  const int m = n - 2;
-  std::vector<double> cp(m), dp(m);
-  for (int k = 0; k < m; ++k) {
-    const int i = k + 1;
-    const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
-    const double diag = 2.0 * (h0 + h1);
-    const double rhs = 3.0 * ((y[(i + 1) * stride] - y[i * stride]) / h1 - (y[i * stride] - y[(i - 1) * stride]) / h0);
-    const double sup = (k + 1 < m) ? h1 : 0.0;
-    if (k == 0) {
-      cp[k] = sup / diag;
-      dp[k] = rhs / diag;
-    } else {
-      const double den = diag - h0 * cp[k - 1];
-      cp[k] = sup / den;
-      dp[k] = (rhs - h0 * dp[k - 1]) / den;
-    }
-  }
-  for (int k = m - 2; k >= 0; --k) dp[k] -= cp[k] * dp[k + 1];
-  for (int k = 0; k < m; ++k) c[(k + 1) * stride] = dp[k];
-}
-
-void spline_second_derivs4(const double *x, const double *y, int n, double *c) {
-  for (int k = 0; k < 4 && k < 4 * n; ++k) c[k] = 0.0;
-  if (n < 3) {
-    for (int k = 4; k < 4 * n; ++k) c[k] = 0.0;
-    return;
-  }
-  for (int q = 0; q < 4; ++q) c[4 * (size_t)(n - 1) + q] = 0.0;
-  const int m = n - 2;
-  // Thomas sweep with the forward values written straight into c (row k + 1);
-  // the knots are (nearly) evenly spaced, so a reciprocal whose operands
-  // repeat bit for bit is reused instead of recomputed (same values, no
-  // division)
-  static thread_local std::vector<double> cp_buf;
-  if (cp_buf.size() < (size_t)m) cp_buf.resize(m);
-  double *cp = cp_buf.data();
-  double inv_h0 = 1.0 / (x[1] - x[0]);
-  double dprev[4];
-  for (int q = 0; q < 4; ++q) dprev[q] = y[4 + q] - y[q];
-  double h0p = 0.0, h1p = 0.0, invp = 0.0, inv_h1p = 0.0;
-  for (int k = 0; k < m; ++k) {
-    const int i = k + 1;
-    const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
-    const double inv_h1 = (k > 0 && h1 == h1p) ? inv_h1p : 1.0 / h1;
-    const double sup = (k + 1 < m) ? h1 : 0.0;
-    double inv;
-    if (k >= 2 && h0 == h0p && h1 == h1p && cp[k - 1] == cp[k - 2]) {
-      inv = invp;  // same den = 2 (h0 + h1) - h0 cp[k-1] as the previous row
-    } else {
-      const double den = (k == 0) ? 2.0 * (h0 + h1) : 2.0 * (h0 + h1) - h0 * cp[k - 1];
-      inv = 1.0 / den;
-    }
-    cp[k] = sup * inv;
-    double *row = c + 4 * (size_t)i;
-    for (int q = 0; q < 4; ++q) {
-      const double dnext = y[4 * (size_t)(i + 1) + q] - y[4 * (size_t)i + q];
-      const double rhs = 3.0 * (dnext * inv_h1 - dprev[q] * inv_h0);
-      row[q] = (k == 0) ? rhs * inv : (rhs - h0 * row[q - 4]) * inv;
-      dprev[q] = dnext;
-    }
-    inv_h0 = inv_h1;
-    h0p = h0;
-    h1p = h1;
-    invp = inv;
-    inv_h1p = inv_h1;
-  }
-  for (int k = m - 2; k >= 0; --k) {
-    double *row = c + 4 * (size_t)(k + 1);
-    for (int q = 0; q < 4; ++q) row[q] -= cp[k] * row[q + 4];
-  }
-}
-
-double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv) {
+void spline_eval4_local(const double *x, const double *y, int n, double xv, double out[4]) {
   int lo = 0, hi = n - 1;
   while (hi > lo + 1) {
     const int mid = (lo + hi) / 2;
     if (x[mid] > xv) hi = mid;
     else lo = mid;
   }
-  int i = std::min(lo, n - 2);
+  const int i = std::min(lo, n - 2);
+  // c at knots i and i + 1 from the windowed solve the device uses for all
+  // knots (window of kSplineHalo = 40 knots either side, cut ends taken as 0)
+  double ci[4] = {0, 0, 0, 0}, ci1[4] = {0, 0, 0, 0};
+  if (n >= 3) {
+    const int wa = std::max(1, i - 40), wb = std::min(n - 1, i + 2 + 40);
+    const int m = wb - wa;
+    std::vector<double> cp(m), dp(4 * (size_t)m);
+    double cprev = 0.0, dprev[4] = {0, 0, 0, 0};
+    double inv_h0 = 1.0 / (x[wa] - x[wa - 1]);
+    for (int r = wa; r < wb; ++r) {
+      const double h0 = x[r] - x[r - 1], h1 = x[r + 1] - x[r];
+      const double inv_h1 = 1.0 / h1;
+      const double inv = 1.0 / (2.0 * (h0 + h1) - h0 * cprev);
+      const double cc = (r + 1 < wb) ? h1 * inv : 0.0;
+      for (int q = 0; q < 4; ++q) {
+        const double y0 = y[4 * (size_t)(r - 1) + q], y1 = y[4 * (size_t)r + q], y2 = y[4 * (size_t)(r + 1) + q];
+        dprev[q] = (3.0 * ((y2 - y1) * inv_h1 - (y1 - y0) * inv_h0) - h0 * dprev[q]) * inv;
+        dp[4 * (size_t)(r - wa) + q] = dprev[q];
+      }
+      cp[r - wa] = cc;
+      cprev = cc;
+      inv_h0 = inv_h1;
+    }
+    double v[4];
+    for (int q = 0; q < 4; ++q) v[q] = dp[4 * (size_t)(m - 1) + q];
+    for (int r = wb - 1;; --r) {
+      if (r == i)
+        for (int q = 0; q < 4; ++q) ci[q] = v[q];
+      if (r == i + 1)
+        for (int q = 0; q < 4; ++q) ci1[q] = v[q];
+      if (r <= std::max(i, wa)) break;
+      for (int q = 0; q < 4; ++q) v[q] = dp[4 * (size_t)(r - 1 - wa) + q] - cp[r - 1 - wa] * v[q];
+    }
+  }
   const double h = x[i + 1] - x[i], dx = xv - x[i];
-  const double yi = y[i * stride], yi1 = y[(i + 1) * stride];
-  const double ci = c[i * stride], ci1 = c[(i + 1) * stride];
-  const double b = (yi1 - yi) / h - h * (ci1 + 2.0 * ci) / 3.0;
-  const double d = (ci1 - ci) / (3.0 * h);
-  return yi + dx * (b + dx * (ci + dx * d));
+  for (int q = 0; q < 4; ++q) {
+    const double yi = y[4 * (size_t)i + q], yi1 = y[4 * (size_t)(i + 1) + q];
+    const double b = (yi1 - yi) / h - h * (ci1[q] + 2.0 * ci[q]) / 3.0;
+    const double d = (ci1[q] - ci[q]) / (3.0 * h);
+    out[q] = yi + dx * (b + dx * (ci[q] + dx * d));
+  }
 }
 
 // ------------------------------------------------------------------ Bessel start order
@@ -703,10 +663,9 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   }
   plan->knot_t.resize(n_in);
   plan->knot_y.resize(4 * (size_t)n_in);
-  plan->knot_c.resize(4 * (size_t)n_in);
   double e_max = 0.0;
   for (int k = 0; k < n_in; ++k) e_max = std::max(e_max, plan->knot_y[4 * (size_t)k]);
-  spline_second_derivs4(plan->knot_t.data(), plan->knot_y.data(), n_in, plan->knot_c.data());
+  // (the spline coefficients are solved on the device after the upload)
 
   const int i0 = vlength - (int)(t_end / timestep);
   plan->vlength = vlength;
@@ -721,11 +680,9 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   const int ip = (j_max == j_max_temp) ? vlength - 1 : i0 + (int)(t_fit[j_min] / timestep);
   if (ip < 0 || ip >= vlength) return plan->status = kErrInvalidParam;
   const double t_ip = (ip == 0) ? plan->t_first : (ip - i0) * timestep;
-  const double *kt = plan->knot_t.data(), *ky = plan->knot_y.data(), *kc = plan->knot_c.data();
-  const double e_ip = spline_eval(kt, ky + 0, kc + 0, n_in, 4, t_ip);
-  const double v_ip = spline_eval(kt, ky + 1, kc + 1, n_in, 4, t_ip);
-  const double M_ip = spline_eval(kt, ky + 2, kc + 2, n_in, 4, t_ip);
-  const double S_ip = spline_eval(kt, ky + 3, kc + 3, n_in, 4, t_ip);
+  double q_ip[4];
+  spline_eval4_local(plan->knot_t.data(), plan->knot_y.data(), n_in, t_ip, q_ip);
+  const double e_ip = q_ip[0], v_ip = q_ip[1], M_ip = q_ip[2], S_ip = q_ip[3];
   plan->i_plunge = ip;
   plan->i_buffer = (int)(10. / (omega_phi(v_ip, e_ip, coslam, S_ip, M_ip) / 2. / kPi) / timestep) + 1;
 

@@ -192,7 +192,7 @@ struct SourcePlan {
   double e_max = 0;
   KnotBuf<double> knot_t;       // n_knots
   KnotBuf<double> knot_y;       // n_knots x 4 (e, v, M, S): the layout of double4[n_knots]
-  KnotBuf<double> knot_c;       // n_knots x 4 (natural-spline half second derivatives)
+                                // (the spline coefficients are solved on the device)
   SourceDesc desc;              // offsets filled in by the batch builder
 };
 
@@ -200,11 +200,10 @@ int plan_source(const WaveInputs &w, SourcePlan *plan);
 // Per-source geometry constants of the waveform (orientation fields set).
 void fill_geometry(SourceDesc *d);
 
-// Natural cubic spline helpers (shared by the plan and tests).
-void spline_second_derivs(const double *x, const double *y, int n, int stride, double *c);
-// The same for the four interleaved series y[n][4] (one factorisation): c[n][4].
-void spline_second_derivs4(const double *x, const double *y, int n, double *c);
-double spline_eval(const double *x, const double *y, const double *c, int n, int stride, double xv);
+// (e, v, M, S) of the natural spline through the n knots (x, y[4 n]) at xv,
+// with the coefficients of its piece from the windowed solve the device
+// applies to every knot (no full solve).
+void spline_eval4_local(const double *x, const double *y, int n, double xv, double out[4]);
 
 // Miller start order for J_{n-2..n+2+extra}(n e) accurate to ~1e-17 for all e <= e_max.
 int bessel_start_order(int n, double e_max, int extra = 0);

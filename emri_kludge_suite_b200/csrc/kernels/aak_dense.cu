@@ -1505,6 +1505,73 @@ __global__ void __launch_bounds__(256) k_plain_waveform(const SourceDesc *__rest
 
 }  // namespace
 
+namespace {
+__global__ void __launch_bounds__(128) k_spline_coeffs(const SourceDesc *src, int nsrc, const int64_t *blk_start,
+                                                       int64_t total_blocks, const double *knot_t,
+                                                       const double4 *knot_y, double4 *knot_c) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total_blocks) return;
+  const int s = find_source(blk_start, nsrc, g);
+  const SourceDesc &d = src[s];
+  if (d.status != 0) return;  // a failed source has no knots
+  const int n = d.n_knots;
+  const double *x = knot_t + d.knot_offset;
+  const double4 *y = knot_y + d.knot_offset;
+  double4 *c = knot_c + d.knot_offset;
+  const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (n < 3) {
+    for (int i = 0; i < n; ++i) c[i] = zero;
+    return;
+  }
+  // interior unknowns 1 .. n-2; this block owns [a, e), the widened window is [wa, wb)
+  const int b = (int)(g - blk_start[s]);
+  const int a = 1 + b * kSplineBlock, e = min(a + kSplineBlock, n - 1);
+  if (a == 1) c[0] = zero;
+  if (e == n - 1) c[n - 1] = zero;
+  const int wa = max(1, a - kSplineHalo), wb = min(n - 1, e + kSplineHalo);
+  double cp[kSplineBlock + kSplineHalo];
+  double4 dp[kSplineBlock + kSplineHalo];
+  double cprev = 0.0;
+  double4 dprev = zero;
+  double inv_h0 = 1.0 / (x[wa] - x[wa - 1]);
+  for (int i = wa; i < wb; ++i) {
+    const double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
+    const double inv_h1 = 1.0 / h1;
+    const double inv = 1.0 / (2.0 * (h0 + h1) - h0 * cprev);
+    const double cc = (i + 1 < wb) ? h1 * inv : 0.0;
+    const double4 y0 = y[i - 1], y1 = y[i], y2 = y[i + 1];
+    double4 dd;
+    dd.x = (3.0 * ((y2.x - y1.x) * inv_h1 - (y1.x - y0.x) * inv_h0) - h0 * dprev.x) * inv;
+    dd.y = (3.0 * ((y2.y - y1.y) * inv_h1 - (y1.y - y0.y) * inv_h0) - h0 * dprev.y) * inv;
+    dd.z = (3.0 * ((y2.z - y1.z) * inv_h1 - (y1.z - y0.z) * inv_h0) - h0 * dprev.z) * inv;
+    dd.w = (3.0 * ((y2.w - y1.w) * inv_h1 - (y1.w - y0.w) * inv_h0) - h0 * dprev.w) * inv;
+    if (i >= a) {
+      cp[i - a] = cc;
+      dp[i - a] = dd;
+    }
+    cprev = cc;
+    dprev = dd;
+    inv_h0 = inv_h1;
+  }
+  double4 v = dp[wb - 1 - a];  // c at wb - 1 (its neighbour beyond the window taken as 0)
+  if (wb - 1 < e) c[wb - 1] = v;
+  for (int i = wb - 2; i >= a; --i) {
+    const double k = cp[i - a];
+    const double4 q = dp[i - a];
+    v = make_double4(q.x - k * v.x, q.y - k * v.y, q.z - k * v.z, q.w - k * v.w);
+    if (i < e) c[i] = v;
+  }
+}
+}  // namespace
+
+void launch_spline_coeffs(const SourceDesc *src, int nsrc, const int64_t *blk_start, int64_t total_blocks,
+                          const double *knot_t, const double4 *knot_y, double4 *knot_c, cudaStream_t stream) {
+  if (total_blocks <= 0) return;
+  const int threads = 128;
+  k_spline_coeffs<<<(unsigned)((total_blocks + threads - 1) / threads), threads, 0, stream>>>(
+      src, nsrc, blk_start, total_blocks, knot_t, knot_y, knot_c);
+}
+
 void launch_plain_waveform(const SourceDesc *src, int s, int vlength, const double *traj, int64_t traj_stride,
                            double *hI, double *hII, cudaStream_t stream) {
   if (vlength <= 0) return;

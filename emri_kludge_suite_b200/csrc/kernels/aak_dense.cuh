@@ -75,6 +75,21 @@ void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
 // jn(n-2 .. n+2, n e), one cos/sin of n Phi and the NK-frame rotation per
 // harmonic -- on the dense trajectory (9 x traj_stride doubles, as the waveform kernel
 // writes with trajectory_only) of source s of the batch.
+// Natural-spline coefficients c (half second derivatives, c = 0 at both ends)
+// of every source's knots, solved on the device: the interior knots of a
+// source are cut into blocks of kSplineBlock, and one thread solves each block
+// by Thomas elimination over the block widened by kSplineHalo knots on either
+// side, taking c = 0 where the widened window is cut.  The system is
+// diagonally dominant (|h0| + |h1| = half the diagonal 2 (h0 + h1)), so the
+// influence of a cut decays at least as 0.27^k with the distance k in knots:
+// 40 knots leave it below 1e-22.  blk_start: nsrc + 1 prefix of the blocks per
+// source (spline_blocks).
+constexpr int kSplineBlock = 256;
+constexpr int kSplineHalo = 40;
+inline int64_t spline_blocks(int n_knots) { return n_knots < 3 ? 1 : (n_knots - 2 + kSplineBlock - 1) / kSplineBlock; }
+void launch_spline_coeffs(const SourceDesc *src, int nsrc, const int64_t *blk_start, int64_t total_blocks,
+                          const double *knot_t, const double4 *knot_y, double4 *knot_c, cudaStream_t stream);
+
 void launch_plain_waveform(const SourceDesc *src, int s, int vlength, const double *traj, int64_t traj_stride,
                            double *hI, double *hII, cudaStream_t stream);
 
