@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
+#include <functional>
+#include <thread>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -99,6 +102,9 @@ struct aak_ctx {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   cudaStream_t cap_stream = nullptr;
+  // streamed host-buffer batches: two auxiliary contexts, each with its own stream
+  aak_ctx *aux[2] = {nullptr, nullptr};
+  cudaStream_t pipe_stream = nullptr;
   double *g_hI = nullptr, *g_hII = nullptr;
   int g_prec = -1;
   uint64_t g_gen = ~0ull;
@@ -290,12 +296,27 @@ void finish_source(aak_ctx *ctx, int s, const Params &Pp, const MappedTrajectory
   }
 }
 
-int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32_t nsrc, const int32_t *nm,
-                int32_t nthreads) {
-  if (!ctx || !P || nsrc <= 0) return AAK_ERR_INVALID_PARAM;
-  std::vector<aak_params> Pv(P, P + nsrc);
-  for (auto &p : Pv)
-    if (p.length < 2 || p.length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
+// Planning stages (1)-(3) for every source of Pv (lengths already checked);
+// on_done(s), if set, is called on the worker thread right after source s is
+// planned (its plan and status final from then on).
+int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapped *maps, const int32_t *nm,
+                 int32_t nthreads, const std::function<void(int)> &on_done, bool early_small = false) {
+  const int32_t nsrc = (int32_t)Pv.size();
+  // worker threads page-lock knot arrays: make this context's device theirs
+  // (a new thread starts on device 0, where it would otherwise open a context)
+  const int dev = ctx->device;
+  auto on_device = [dev]() {
+    int cur = -1;
+    if (dev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != dev) cudaSetDevice(dev);
+  };
+  int caller_dev = -1;  // the calling thread's device, put back at the end
+  if (dev >= 0 && cudaGetDevice(&caller_dev) != cudaSuccess) caller_dev = -1;
+  struct Restore {
+    int d;
+    ~Restore() {
+      if (d >= 0) cudaSetDevice(d);
+    }
+  } restore{caller_dev};
   ctx->nsrc = nsrc;
   // the plan array only grows: plans past nsrc keep their page-locked knot
   // arrays for later, larger batches (pinning is slow; only nsrc bounds the live part)
@@ -305,13 +326,15 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   ctx->newton_points = ctx->newton_iters = ctx->newton_fallbacks = 0;
   if (maps) {
     parallel_for(nsrc, nthreads, [&](int64_t s) {
+      on_device();
       const Params Pp = to_params(Pv[s]);
       MappedTrajectory mt;
       const int st = validate(Pp);
       if (st == kOk) from_mapped(maps[s], &mt);
       finish_source(ctx, (int)s, Pp, mt, nm, st);
+      if (on_done) on_done((int)s);
     });
-    return pack(ctx, Pv, nthreads);
+    return AAK_OK;
   }
   // (1) coarse Kerr inspiral and Kerr frequencies
   std::vector<CoarseKerr> ck(nsrc);
@@ -358,9 +381,22 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
     }
     for (int s = 0; s < nsrc; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    if (early_small) {
+      // streaming: the sources that bound the planning time (more than a
+      // quarter of a thread's fair share each) still go first, the rest
+      // smallest first, so that finished sources start flowing to the device
+      // early while the long ones are being planned
+      double total = 0.0;
+      for (double c : cost) total += c;
+      const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
+      const double big = total / threads / 4.0;
+      const auto split = std::find_if(order.begin(), order.end(), [&](int s) { return cost[s] <= big; });
+      std::reverse(split, order.end());
+    }
   }
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
   parallel_for(nsrc, nthreads, [&](int64_t k) {
+    on_device();
     const int64_t s = order[k];
     const Params Pp = to_params(Pv[s]);
     MappedTrajectory mt;
@@ -375,10 +411,22 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
       }
     }
     finish_source(ctx, (int)s, Pp, mt, nm, st);
+    if (on_done) on_done((int)s);
   });
   ctx->newton_points = points;
   ctx->newton_iters = iters;
   ctx->newton_fallbacks = fallbacks;
+  return AAK_OK;
+}
+
+int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32_t nsrc, const int32_t *nm,
+                int32_t nthreads) {
+  if (!ctx || !P || nsrc <= 0) return AAK_ERR_INVALID_PARAM;
+  std::vector<aak_params> Pv(P, P + nsrc);
+  for (auto &p : Pv)
+    if (p.length < 2 || p.length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
+  const int r = plan_sources(ctx, Pv, maps, nm, nthreads, nullptr);
+  if (r != AAK_OK) return r;
   return pack(ctx, Pv, nthreads);
 }
 
@@ -613,6 +661,128 @@ int host_roundtrip(aak_ctx *ctx, double *t, double *hI, double *hII) {
   return device_status(ctx);
 }
 
+// aak_wave_batch_host for batches worth streaming.  Host threads plan the
+// sources (the few that bound the planning time first, then the rest smallest
+// first); as they finish, the calling thread gathers them in groups of about
+// nsrc / kStreamGroups (or takes what has finished when 10 ms pass without a
+// full group) and, on one of two auxiliary
+// contexts in turn, packs, uploads, generates and copies back each group on
+// that context's own stream while planning goes on.  Most sources are small
+// and finish early, so nearly all of the transfers and kernels hide behind
+// the planning of the few long sources.  A group's plans are lent to the
+// auxiliary context for its pack and upload and then handed back; at the end
+// this context holds the whole batch's plan, as after aak_batch_plan (not
+// uploaded).  Copies into pageable host buffers are synchronous: correct,
+// with less overlap.
+constexpr int kStreamMinSources = 32;
+constexpr int kStreamGroups = 8;
+
+int wave_batch_streamed(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nm, int32_t nthreads,
+                        double *hI, double *hII) {
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  const std::vector<aak_params> Pv(P, P + nsrc);
+  for (int k = 0; k < 2; ++k) {
+    if (!ctx->aux[k]) {
+      if ((r = aak_ctx_create(ctx->device, &ctx->aux[k])) != AAK_OK) return r;
+      if ((r = cuda_ok(cudaStreamCreateWithFlags(&ctx->aux[k]->pipe_stream, cudaStreamNonBlocking))) != AAK_OK)
+        return r;
+    }
+    ctx->aux[k]->precision = ctx->precision;
+  }
+  std::vector<int64_t> pre(nsrc + 1, 0);  // sample offsets of the sources in the host outputs
+  for (int s = 0; s < nsrc; ++s) pre[s + 1] = pre[s] + Pv[s].length;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<int> done;  // planned sources, in completion order
+  done.reserve(nsrc);
+  bool finished = false;
+  int plan_rc = AAK_OK;
+  std::thread planner([&]() {
+    cudaSetDevice(ctx->device);
+    const int rr = plan_sources(
+        ctx, Pv, nullptr, nm, nthreads,
+        [&](int s) {
+          std::lock_guard<std::mutex> lk(mu);
+          done.push_back(s);
+          cv.notify_one();
+        },
+        true);
+    std::lock_guard<std::mutex> lk(mu);
+    finished = true;
+    plan_rc = rr;
+    cv.notify_one();
+  });
+  const int G = std::max(8, (nsrc + kStreamGroups - 1) / kStreamGroups);
+  int taken = 0, slot = 0, rc = AAK_OK;
+  bool pending[2] = {false, false};
+  std::vector<int> grp;
+  std::vector<aak_params> Pg;
+  for (;;) {
+    {
+      // a full group, or whatever has finished once completions slow down
+      // (the long sources at the end): each then leaves as soon as it is done
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait_for(lk, std::chrono::milliseconds(10), [&]() { return finished || (int)done.size() - taken >= G; });
+      if (finished && plan_rc != AAK_OK) {
+        rc = plan_rc;
+        break;
+      }
+      const int avail = (int)done.size() - taken;
+      if (avail == 0) {
+        if (finished) break;  // all dispatched
+        continue;
+      }
+      const int k = std::min(avail, G);
+      grp.assign(done.begin() + taken, done.begin() + taken + k);
+      taken += k;
+    }
+    aak_ctx *A = ctx->aux[slot];
+    if (pending[slot]) {  // this context's previous group must be done with its device buffers
+      pending[slot] = false;
+      if ((rc = cuda_ok(cudaStreamSynchronize(A->pipe_stream))) != AAK_OK) break;
+    }
+    const int k = (int)grp.size();
+    if ((int)A->plans.size() < k) A->plans.resize(k);
+    Pg.resize(k);
+    A->nsrc = k;
+    A->status.resize(k);
+    for (int i = 0; i < k; ++i) {
+      std::swap(A->plans[i], ctx->plans[grp[i]]);
+      A->status[i] = ctx->status[grp[i]];
+      Pg[i] = Pv[grp[i]];
+    }
+    rc = pack(A, Pg, 2);
+    if (rc == AAK_OK) rc = upload(A, A->pipe_stream);  // waits for its own copies
+    for (int i = 0; i < k; ++i) std::swap(A->plans[i], ctx->plans[grp[i]]);
+    if (rc != AAK_OK) break;
+    const int64_t N = A->total_samples;
+    if ((rc = A->d_out.reserve((size_t)(2 * N))) != AAK_OK) break;
+    double *dI = A->d_out.ptr, *dII = dI + N;
+    if ((rc = run(A, dI, dII, nullptr, nullptr, 0, A->precision, A->pipe_stream)) != AAK_OK) break;
+    for (int i = 0; i < k && rc == AAK_OK; ++i) {
+      const int s = grp[i];
+      const size_t bytes = (size_t)Pv[s].length * sizeof(double);
+      if ((rc = cuda_ok(cudaMemcpyAsync(hI + pre[s], dI + A->offsets[i], bytes, cudaMemcpyDeviceToHost, A->pipe_stream))) ==
+          AAK_OK)
+        rc = cuda_ok(cudaMemcpyAsync(hII + pre[s], dII + A->offsets[i], bytes, cudaMemcpyDeviceToHost, A->pipe_stream));
+    }
+    if (rc != AAK_OK) break;
+    pending[slot] = true;
+    slot ^= 1;
+  }
+  planner.join();
+  for (int k = 0; k < 2; ++k)  // drain both streams whatever happened
+    if (pending[k]) {
+      const int e = cuda_ok(cudaStreamSynchronize(ctx->aux[k]->pipe_stream));
+      if (rc == AAK_OK) rc = e;
+    }
+  if (rc != AAK_OK) return rc;
+  for (int k = 0; k < 2; ++k)
+    if ((r = device_status(ctx->aux[k])) != AAK_OK) return r;
+  return pack(ctx, Pv, nthreads);  // the whole batch's plan in this context
+}
+
 }  // namespace
 
 extern "C" {
@@ -710,7 +880,10 @@ void aak_ctx_destroy(aak_ctx *c) {
       if (e) cudaEventDestroy(e);
     drop_graph(c);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    if (c->pipe_stream) cudaStreamDestroy(c->pipe_stream);
   }
+  aak_ctx_destroy(c->aux[0]);
+  aak_ctx_destroy(c->aux[1]);
   delete c;
 }
 
@@ -923,13 +1096,22 @@ int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const i
                         double *h_hI, double *h_hII, int64_t *offsets, int32_t *status) {
   if (!ctx || !h_hI || !h_hII) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
-  int r = plan_common(ctx, P, nullptr, nsrc, nm, nthreads);
+  int r;
+  if (nsrc >= kStreamMinSources && ctx->device >= 0 && ctx->out_stride == 0) {
+    if (!P) return AAK_ERR_INVALID_PARAM;
+    for (int32_t s = 0; s < nsrc; ++s)
+      if (P[s].length < 2 || P[s].length > ((int64_t)1 << 31)) return AAK_ERR_INVALID_PARAM;
+    r = wave_batch_streamed(ctx, P, nsrc, nm, nthreads, h_hI, h_hII);
+  } else {
+    r = plan_common(ctx, P, nullptr, nsrc, nm, nthreads);
+    if (r == AAK_OK) r = host_roundtrip(ctx, nullptr, h_hI, h_hII);
+  }
   if (r != AAK_OK) return r;
   if (offsets)
     for (int s = 0; s <= nsrc; ++s) offsets[s] = ctx->offsets[s];
   if (status)
     for (int s = 0; s < nsrc; ++s) status[s] = ctx->status[s];
-  return host_roundtrip(ctx, nullptr, h_hI, h_hII);
+  return AAK_OK;
 }
 
 int aak_wave(const aak_params *p, double *t, double *hI, double *hII, double *seconds) {

@@ -213,3 +213,40 @@ def test_backward_chain_full_length_against_oracle():
     mm = mismatch(hI, hII, oI, oII)
     assert mm < 1e-6, mm
     assert _maxrel(hI, oI) < 1e-4
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_streamed_host_batch_matches_device_batch(precision):
+    """aak_wave_batch_host on 40 sources (planned on host threads while groups
+    of finished sources are uploaded, generated and copied back) equals plan +
+    upload + run into device buffers, and leaves the context with the whole
+    batch's plan."""
+    rng = np.random.default_rng(11)
+    params = []
+    for _ in range(40):
+        p = dict(BASE)
+        p.update(e=float(rng.uniform(0.1, 0.4)), p=float(rng.uniform(9, 12)), length=int(rng.integers(5000, 60000)),
+                 iota=float(rng.uniform(0.2, 1.3)), phi_S=float(rng.uniform(0, 6)), mu=float(rng.uniform(5, 60)))
+        params.append(p)
+    params[7] = dict(params[7], e=-0.2)  # one invalid source: zeros and a status
+    wh = E.WaveBatch(0)
+    wh.set_precision(precision)
+    hI = hII = None
+    for _ in range(2):  # twice: the second call reuses the contexts' buffers
+        hI, hII, off, st = wh.generate_host(params, nmodes=20)
+    assert st[7] != 0 and np.all(np.delete(st, 7) == 0)
+    assert np.all(hI[off[7]:off[8]] == 0.0)
+    assert np.array_equal(wh.offsets, off) and np.array_equal(wh.status, st)
+    wd = E.WaveBatch(0)
+    wd.plan(params, nmodes=20)
+    assert np.array_equal(wd.offsets, off) and np.array_equal(wd.i_plunge, wh.i_plunge)
+    N = wd.total_samples
+    a = torch.zeros(N, dtype=torch.float64, device="cuda")
+    b = torch.zeros_like(a)
+    wd.upload()
+    wd.run(a.data_ptr(), b.data_ptr(), precision=precision)
+    torch.cuda.synchronize()
+    a, b = a.cpu().numpy(), b.cpu().numpy()
+    scale = max(np.abs(a).max(), np.abs(b).max())
+    assert np.max(np.abs(hI - a)) <= 1e-13 * scale
+    assert np.max(np.abs(hII - b)) <= 1e-13 * scale
