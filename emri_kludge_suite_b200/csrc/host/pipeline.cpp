@@ -432,6 +432,33 @@ inline double om_x(double v, double e, double coslam, double S, double M, double
   else om = omega_phi(v, e, coslam, S, M);
   return om * M_phys * kMsunSec;
 }
+// Plunge-scan pre-test of n consecutive knots (y4: their (e, v, M, S)):
+// clear[k] = 1 where p^3 = (1 - e^2)^3 / x^2 exceeds lso3, i.e. where the
+// knot fails both plunge tests.  lso3 carries a 1e-9 margin, so the result
+// does not depend on how the compiler rounds (FMA or not); the knots not
+// cleared take the exact path.  Independent per knot: vectorised where the
+// CPU has AVX2 and FMA.
+#define AAK_PLUNGE_PRETEST_BODY                                                   \
+  for (int k = 0; k < n; ++k) {                                                    \
+    const double e = y4[4 * k], v = y4[4 * k + 1], M = y4[4 * k + 2], S = y4[4 * k + 3]; \
+    const double x = om_x(v, e, coslam, S, M, M_phys);                             \
+    const double ome = 1. - e * e;                                                 \
+    clear[k] = (ome * ome * ome > lso3 * (x * x)) ? 1 : 0;                        \
+  }
+__attribute__((target("avx2,fma"))) void plunge_pretest_avx2(const double *y4, int n, double coslam, double M_phys,
+                                                             double lso3, unsigned char *clear) {
+  AAK_PLUNGE_PRETEST_BODY
+}
+void plunge_pretest_plain(const double *y4, int n, double coslam, double M_phys, double lso3, unsigned char *clear) {
+  AAK_PLUNGE_PRETEST_BODY
+}
+#undef AAK_PLUNGE_PRETEST_BODY
+void plunge_pretest(const double *y4, int n, double coslam, double M_phys, double lso3, unsigned char *clear) {
+  static const bool avx2 = __builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma");
+  if (avx2) plunge_pretest_avx2(y4, n, coslam, M_phys, lso3, clear);
+  else plunge_pretest_plain(y4, n, coslam, M_phys, lso3, clear);
+}
+
 inline double p_of(double v, double e, double coslam, double S, double M, double M_phys) {
   const double c = std::cbrt(om_x(v, e, coslam, S, M, M_phys));
   return (1. - e * e) / (c * c);
@@ -597,11 +624,19 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   // p^3 = (1 - e^2)^3 / x^2: a knot whose p^3 clears LSO_max^3 by a margin far
   // beyond rounding fails both tests below, and needs no cube root
   const double lso3 = LSO_max * LSO_max * LSO_max * (1.0 + 1e-9);
+  constexpr int kPretest = 512;
+  unsigned char clear[kPretest];
+  int jc = j0, jc_end = j0;  // knots [jc, jc_end) have their pre-test in clear[]
   for (int j = j0; j <= j_max_temp; ++j) {
     if (j > j_max) break;
+    if (j >= jc_end) {
+      jc = j;
+      jc_end = std::min(j_max_temp + 1, j + kPretest);
+      plunge_pretest(&e_fit[j], jc_end - jc, coslam, M_phys, lso3, clear);
+    }
+    if (clear[j - jc]) continue;
     const double x = om_x(v_fit[j], e_fit[j], coslam, S_fit[j], M_fit[j], M_phys);
     const double ome = 1. - e_fit[j] * e_fit[j];
-    if (ome * ome * ome > lso3 * (x * x)) continue;
     const double cx = std::cbrt(x);
     const double pj = ome / (cx * cx);
     if (pj < LSO_min && j_max == j_max_temp) {
