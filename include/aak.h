@@ -221,7 +221,12 @@ int aak_probe_fp32_tflops(int32_t device, double *tflops);
 int aak_probe_fp64_tflops(int32_t device, double *tflops);
 
 /* End to end with host buffers: plan + upload + run + copy back.
- * h_hI / h_hII hold total_samples doubles (offsets as from aak_batch_info). */
+ * h_hI / h_hII hold total_samples doubles (offsets as from aak_batch_info).
+ * From 32 sources on, the call streams: groups of sources that finished
+ * planning are uploaded, generated and copied back on two internal contexts
+ * while the others are still planned; page-locked output buffers let those
+ * copies overlap.  Either way the context holds the whole batch's plan
+ * afterwards (as after aak_batch_plan). */
 int aak_wave_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const int32_t *nmodes_override,
                         int32_t nthreads, double *h_hI, double *h_hII, int64_t *offsets, int32_t *status);
 
