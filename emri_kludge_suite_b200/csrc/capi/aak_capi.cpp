@@ -282,6 +282,36 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
 }
 
 // Coarse AK evolution and knots of source s from its mapped trajectory.
+// finish_source of two sources on one thread, their coarse AK evolutions
+// interleaved (plan_source_pair: same results).
+void finish_pair(aak_ctx *ctx, int a, const Params &Pa, const MappedTrajectory &ma, int sta, int b, const Params &Pb,
+                 const MappedTrajectory &mb, int stb, const int32_t *nm) {
+  WaveInputs wa, wb;
+  if (sta == kOk) {
+    genwave_inputs(Pa, ma, nm ? nm[a] : 0, &wa);
+    if (wa.nmodes > 4096) sta = kErrCapacity;
+  }
+  if (stb == kOk) {
+    genwave_inputs(Pb, mb, nm ? nm[b] : 0, &wb);
+    if (wb.nmodes > 4096) stb = kErrCapacity;
+  }
+  if (sta == kOk && stb == kOk) {
+    plan_source_pair(wa, &ctx->plans[a], wb, &ctx->plans[b]);
+    sta = ctx->plans[a].status;
+    stb = ctx->plans[b].status;
+  } else {
+    if (sta == kOk) sta = plan_source(wa, &ctx->plans[a]);
+    if (stb == kOk) stb = plan_source(wb, &ctx->plans[b]);
+  }
+  for (const auto &q : {std::make_pair(a, sta), std::make_pair(b, stb)}) {
+    ctx->status[q.first] = q.second;
+    if (q.second != kOk) {
+      ctx->plans[q.first].knot_t.clear();
+      ctx->plans[q.first].knot_y.clear();
+    }
+  }
+}
+
 void finish_source(aak_ctx *ctx, int s, const Params &Pp, const MappedTrajectory &mt, const int32_t *nm, int st) {
   if (st == kOk) {
     WaveInputs w;
@@ -372,6 +402,7 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   // so handing sources out in that order keeps host threads from idling
   // behind one long source at the end.
   std::vector<int> order(nsrc);
+  int nbig = 0;  // the leading sources of order that run alone (the rest in pairs)
   {
     std::vector<double> cost(nsrc, 0.0);
     for (int s = 0; s < nsrc; ++s) {
@@ -381,37 +412,56 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     }
     for (int s = 0; s < nsrc; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    if (early_small) {
-      // streaming: the sources that bound the planning time (more than a
-      // quarter of a thread's fair share each) still go first, the rest
-      // smallest first, so that finished sources start flowing to the device
-      // early while the long ones are being planned
-      double total = 0.0;
-      for (double c : cost) total += c;
-      const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
-      const double big = total / threads / 4.0;
-      const auto split = std::find_if(order.begin(), order.end(), [&](int s) { return cost[s] <= big; });
-      std::reverse(split, order.end());
-    }
+    // The sources that bound the planning time (more than a quarter of a
+    // thread's fair share each) go first and alone; the others are planned two
+    // at a time (neighbours in cost, their recurrences interleaved: the same
+    // results, and most of the recurrence's latency hidden).  Streaming takes
+    // the others smallest first, so that finished sources start flowing to
+    // the device early while the long ones are being planned.
+    double total = 0.0;
+    for (double c : cost) total += c;
+    const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
+    const double big = total / threads / 4.0;
+    const auto split = std::find_if(order.begin(), order.end(), [&](int s) { return cost[s] <= big; });
+    nbig = (int)(split - order.begin());
+    if (early_small) std::reverse(split, order.end());
   }
+  const int64_t ntasks = nbig + (nsrc - nbig + 1) / 2;
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
-  parallel_for(nsrc, nthreads, [&](int64_t k) {
-    on_device();
-    const int64_t s = order[k];
-    const Params Pp = to_params(Pv[s]);
-    MappedTrajectory mt;
+  auto map_one = [&](int s, const Params &Pp, MappedTrajectory *mt) {
     int st = ctx->status[s];
     if (st == kOk) {
       int fb = 0;
-      st = map_coarse(Pp, ck[s], &mt, warm.empty() ? nullptr : &warm[3 * first[s]], &fb);
+      st = map_coarse(Pp, ck[s], mt, warm.empty() ? nullptr : &warm[3 * first[s]], &fb);
       if (st == kOk) {
         points += ck[s].steps;
-        iters += mt.newton_iterations;
+        iters += mt->newton_iterations;
         fallbacks += fb;
       }
     }
-    finish_source(ctx, (int)s, Pp, mt, nm, st);
-    if (on_done) on_done((int)s);
+    return st;
+  };
+  parallel_for(ntasks, nthreads, [&](int64_t t) {
+    on_device();
+    const int64_t k = (t < nbig) ? t : nbig + 2 * (t - nbig);
+    const int a = order[k];
+    const Params Pa = to_params(Pv[a]);
+    MappedTrajectory ma;
+    const int sta = map_one(a, Pa, &ma);
+    if (k + 1 < nsrc && t >= nbig) {
+      const int b = order[k + 1];
+      const Params Pb = to_params(Pv[b]);
+      MappedTrajectory mb;
+      const int stb = map_one(b, Pb, &mb);
+      finish_pair(ctx, a, Pa, ma, sta, b, Pb, mb, stb, nm);
+      if (on_done) {
+        on_done(a);
+        on_done(b);
+      }
+    } else {
+      finish_source(ctx, a, Pa, ma, nm, sta);
+      if (on_done) on_done(a);
+    }
   });
   ctx->newton_points = points;
   ctx->newton_iters = iters;

@@ -512,7 +512,26 @@ void fill_geometry(SourceDesc *d) {
   d->F0[3] = std::cos(2. * psi);
 }
 
-int plan_source(const WaveInputs &w, SourcePlan *plan) {
+namespace {
+// Locals of plan_source that live across the coarse evolution beyond the fit
+// window: the planning is split there, so that two sources' evolutions can
+// run interleaved on one thread (evolve2).
+struct PlanState {
+  const WaveInputs *w = nullptr;
+  SourcePlan *plan = nullptr;
+  std::vector<double> *scratch = nullptr;  // AK (e, v) arrays, 2 L doubles
+  int vlength = 0, steps = 0, j0 = 0, j_start = 0, j_min = 0, j_end = 0, j_max = 0, j_max_temp = 0, jb = 0, points = 0;
+  double timestep = 0, mu = 0, M0 = 0, S0 = 0, coslam = 0, dt_large = 0, t_end = 0, edot = 0, vdot = 0;
+  const double *par = nullptr, *dt_map = nullptr;
+  size_t L = 0;
+  Win e_AK{}, v_AK{}, t_fit{}, e_fit{}, v_fit{}, M_fit{}, S_fit{};
+  double ec[2] = {0, 0}, vc[2] = {0, 0}, Mc[2] = {0, 0}, Sc[2] = {0, 0};
+};
+
+int plan_head(PlanState &S) {
+
+  const WaveInputs &w = *S.w;
+  SourcePlan *plan = S.plan;
   plan->status = kOk;
   const int vlength = w.vlength, steps = w.steps;
   const double timestep = w.timestep;
@@ -533,7 +552,7 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   // plan's knot arrays; the AK scratch is kept per host thread.
   const int jb = w.backint ? 0 : j0;
   const size_t L = (size_t)(2 * j0 - jb);
-  static thread_local std::vector<double> ak_scratch;
+  std::vector<double> &ak_scratch = *S.scratch;
   if (ak_scratch.size() < 2 * L) ak_scratch.resize(2 * L);
   plan->knot_t.resize(L);
   plan->knot_y.resize(4 * L);
@@ -580,7 +599,53 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   polyfit(Mc, dt_map, w.M_map, points);
   polyfit(Sc, dt_map, w.S_map, points);
 
-  // AB2 beyond the fit window
+  // carried to the evolution beyond the fit window and to plan_tail
+  S.vlength = vlength;
+  S.steps = steps;
+  S.j0 = j0;
+  S.j_start = j_start;
+  S.j_min = j_min;
+  S.j_end = j_end;
+  S.j_max = j_max;
+  S.j_max_temp = j_max_temp;
+  S.jb = jb;
+  S.points = points;
+  S.timestep = timestep;
+  S.mu = mu;
+  S.M0 = M0;
+  S.S0 = S0;
+  S.coslam = coslam;
+  S.dt_large = dt_large;
+  S.t_end = t_end;
+  S.edot = edot;
+  S.vdot = vdot;
+  S.par = par;
+  S.dt_map = dt_map;
+  S.L = L;
+  S.e_AK = e_AK;
+  S.v_AK = v_AK;
+  S.t_fit = t_fit;
+  S.e_fit = e_fit;
+  S.v_fit = v_fit;
+  S.M_fit = M_fit;
+  S.S_fit = S_fit;
+  for (int i = 0; i < 2; ++i) {
+    S.ec[i] = ec[i];
+    S.vc[i] = vc[i];
+    S.Mc[i] = Mc[i];
+    S.Sc[i] = Sc[i];
+  }
+  return kOk;
+}
+
+// The AK evolution beyond the fit window (a serial recurrence per source).
+void evolve(PlanState &S) {
+  const Win e_AK = S.e_AK, v_AK = S.v_AK;
+  const double coslam = S.coslam, mu = S.mu, M0 = S.M0, S0 = S.S0, dt_large = S.dt_large;
+  const int j0 = S.j0, steps = S.steps, j_end = S.j_end;
+  int &j_max = S.j_max, &j_max_temp = S.j_max_temp;
+  double &edot = S.edot, &vdot = S.vdot;
+  double edotm, vdotm;
   for (int j = j0 + steps - 1; j < j_end; ++j) {
     edotm = edot;
     vdotm = vdot;
@@ -595,6 +660,95 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   }
   j_max_temp = j_max;
 
+}
+
+// Two sources' evolutions at once: each step of one is independent of the
+// other's, so interleaving them hides most of the latency of the recurrence
+// (log, square root, polynomials, a division per step).  The same operations
+// as evolve() in the same order per source: the results are bit-identical.
+void evolve2(PlanState &A, PlanState &B) {
+  const Win eA = A.e_AK, vA = A.v_AK, eB = B.e_AK, vB = B.v_AK;
+  int ja = A.j0 + A.steps - 1, jb2 = B.j0 + B.steps - 1;
+  const int ea_end = A.j_end, eb_end = B.j_end;
+  double edA = A.edot, vdA = A.vdot, edB = B.edot, vdB = B.vdot;
+  while (ja < ea_end && jb2 < eb_end) {
+    const double edAm = edA, vdAm = vdA, edBm = edB, vdBm = vdB;
+    ak_rates(vA[ja], eA[ja], A.coslam, A.mu, A.M0, A.S0, &edA, &vdA);
+    ak_rates(vB[jb2], eB[jb2], B.coslam, B.mu, B.M0, B.S0, &edB, &vdB);
+    eA[ja + 1] = eA[ja] + (1.5 * edA - .5 * edAm) * A.dt_large;
+    vA[ja + 1] = vA[ja] + (1.5 * vdA - .5 * vdAm) * A.dt_large;
+    eB[jb2 + 1] = eB[jb2] + (1.5 * edB - .5 * edBm) * B.dt_large;
+    vB[jb2 + 1] = vB[jb2] + (1.5 * vdB - .5 * vdBm) * B.dt_large;
+    if (eA[ja + 1] < 0. || vA[ja + 1] < vA[ja] || std::isnan(eA[ja + 1]) || std::isnan(vA[ja + 1])) {
+      if (A.j_max == A.j_max_temp) A.j_max = ja;
+      eA[ja + 1] = eA[A.j_max];
+      vA[ja + 1] = vA[A.j_max];
+    }
+    if (eB[jb2 + 1] < 0. || vB[jb2 + 1] < vB[jb2] || std::isnan(eB[jb2 + 1]) || std::isnan(vB[jb2 + 1])) {
+      if (B.j_max == B.j_max_temp) B.j_max = jb2;
+      eB[jb2 + 1] = eB[B.j_max];
+      vB[jb2 + 1] = vB[B.j_max];
+    }
+    ++ja;
+    ++jb2;
+  }
+  // the longer one alone
+  PlanState &R = (ja < ea_end) ? A : B;
+  int &jr = (ja < ea_end) ? ja : jb2;
+  const int r_end = R.j_end;
+  const Win eR = R.e_AK, vR = R.v_AK;
+  double &edR = (ja < ea_end) ? edA : edB, &vdR = (ja < ea_end) ? vdA : vdB;
+  for (; jr < r_end; ++jr) {
+    const double edRm = edR, vdRm = vdR;
+    ak_rates(vR[jr], eR[jr], R.coslam, R.mu, R.M0, R.S0, &edR, &vdR);
+    eR[jr + 1] = eR[jr] + (1.5 * edR - .5 * edRm) * R.dt_large;
+    vR[jr + 1] = vR[jr] + (1.5 * vdR - .5 * vdRm) * R.dt_large;
+    if (eR[jr + 1] < 0. || vR[jr + 1] < vR[jr] || std::isnan(eR[jr + 1]) || std::isnan(vR[jr + 1])) {
+      if (R.j_max == R.j_max_temp) R.j_max = jr;
+      eR[jr + 1] = eR[R.j_max];
+      vR[jr + 1] = vR[R.j_max];
+    }
+  }
+  A.edot = edA;
+  A.vdot = vdA;
+  B.edot = edB;
+  B.vdot = vdB;
+  A.j_max_temp = A.j_max;
+  B.j_max_temp = B.j_max;
+}
+
+int plan_tail(PlanState &S) {
+  const WaveInputs &w = *S.w;
+  SourcePlan *plan = S.plan;
+  const int vlength = S.vlength;
+  const int steps = S.steps;
+  const int j0 = S.j0;
+  const int jb = S.jb;
+  int &j_start = S.j_start;
+  int &j_min = S.j_min;
+  int &j_end = S.j_end;
+  int &j_max = S.j_max;
+  int &j_max_temp = S.j_max_temp;
+  int &points = S.points;
+  const double timestep = S.timestep;
+  const double mu = S.mu;
+  const double M0 = S.M0;
+  const double S0 = S.S0;
+  const double coslam = S.coslam;
+  const double dt_large = S.dt_large;
+  double &t_end = S.t_end;
+  double &edot = S.edot;
+  double &vdot = S.vdot;
+  const double *par = S.par;
+  const double *dt_map = S.dt_map;
+  const Win e_AK = S.e_AK;
+  const Win v_AK = S.v_AK;
+  const Win t_fit = S.t_fit;
+  const Win e_fit = S.e_fit;
+  const Win v_fit = S.v_fit;
+  const Win M_fit = S.M_fit;
+  const Win S_fit = S.S_fit;
+  const double *ec = S.ec, *vc = S.vc, *Mc = S.Mc, *Sc = S.Sc;
   // fitted trajectory with freezing once it turns unphysical
   for (int j = j0; j <= j_end; ++j) {
     const double dt = (j < j0 + steps) ? dt_map[j - j0] : dt_map[steps - 1] + dt_large * (j - j0 - steps + 1);
@@ -754,6 +908,37 @@ int plan_source(const WaveInputs &w, SourcePlan *plan) {
   d.mich = w.mich ? 1 : 0;
   d.status = kOk;
   return kOk;
+}
+
+}  // namespace
+
+int plan_source(const WaveInputs &w, SourcePlan *plan) {
+  static thread_local std::vector<double> scratch;
+  PlanState S;
+  S.w = &w;
+  S.plan = plan;
+  S.scratch = &scratch;
+  const int r = plan_head(S);
+  if (r != kOk) return r;
+  evolve(S);
+  return plan_tail(S);
+}
+
+void plan_source_pair(const WaveInputs &wa, SourcePlan *pa, const WaveInputs &wb, SourcePlan *pb) {
+  static thread_local std::vector<double> scratch_a, scratch_b;
+  PlanState A, B;
+  A.w = &wa;
+  A.plan = pa;
+  A.scratch = &scratch_a;
+  B.w = &wb;
+  B.plan = pb;
+  B.scratch = &scratch_b;
+  const bool ok_a = plan_head(A) == kOk, ok_b = plan_head(B) == kOk;
+  if (ok_a && ok_b) evolve2(A, B);
+  else if (ok_a) evolve(A);
+  else if (ok_b) evolve(B);
+  if (ok_a) plan_tail(A);
+  if (ok_b) plan_tail(B);
 }
 
 }  // namespace aak

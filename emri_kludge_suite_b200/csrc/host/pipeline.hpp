@@ -197,6 +197,9 @@ struct SourcePlan {
 };
 
 int plan_source(const WaveInputs &w, SourcePlan *plan);
+// plan_source of two sources on one thread, their coarse AK evolutions
+// interleaved (same results; each plan's status in its own plan->status).
+void plan_source_pair(const WaveInputs &wa, SourcePlan *pa, const WaveInputs &wb, SourcePlan *pb);
 // Per-source geometry constants of the waveform (orientation fields set).
 void fill_geometry(SourceDesc *d);
 
