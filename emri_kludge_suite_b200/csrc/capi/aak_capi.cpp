@@ -366,14 +366,18 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     });
     return AAK_OK;
   }
-  // (1) coarse Kerr inspiral and Kerr frequencies
+  // (1) coarse Kerr inspiral and Kerr frequencies: a pass of its own when a
+  // warm-start model needs every coarse point at once, else inside each
+  // source's planning task (the long sources then start at once)
   std::vector<CoarseKerr> ck(nsrc);
-  parallel_for(nsrc, nthreads, [&](int64_t s) {
-    const Params Pp = to_params(Pv[s]);
-    int st = validate(Pp);
-    if (st == kOk) st = coarse_kerr(Pp, &ck[s]);
-    ctx->status[s] = st;
-  });
+  const bool fused = !ctx->model;
+  if (!fused)
+    parallel_for(nsrc, nthreads, [&](int64_t s) {
+      const Params Pp = to_params(Pv[s]);
+      int st = validate(Pp);
+      if (st == kOk) st = coarse_kerr(Pp, &ck[s]);
+      ctx->status[s] = st;
+    });
   // (2) optional learned warm start: every coarse point of the batch in one launch
   std::vector<int64_t> first(nsrc + 1, 0);
   std::vector<double> warm;
@@ -429,6 +433,11 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   const int64_t ntasks = nbig + (nsrc - nbig + 1) / 2;
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
   auto map_one = [&](int s, const Params &Pp, MappedTrajectory *mt) {
+    if (fused) {
+      int st0 = validate(Pp);
+      if (st0 == kOk) st0 = coarse_kerr(Pp, &ck[s]);
+      ctx->status[s] = st0;
+    }
     int st = ctx->status[s];
     if (st == kOk) {
       int fb = 0;
