@@ -1255,6 +1255,9 @@ struct aak_gpu {
   std::vector<double> like;
   double ms[4] = {0, 0, 0, 0};  // host plan, generate, FFT, reduce of the last batch
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // device work of the templates: its own non-blocking stream, so that host
+  // planning (and the warm-start model's copies) can overlap it
+  cudaStream_t stream = nullptr;
 };
 
 namespace {
@@ -1308,37 +1311,51 @@ aak_params gpu_params(const aak_gpu *g, const double *x) {
   return p;
 }
 
-int gpu_generate(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status, bool with_t) {
-  int r;
-  if ((r = gpu_capacity(g, B)) != AAK_OK) return r;
+// Host half of a batch of templates: plan them into the context's rows.
+int gpu_plan(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status) {
   std::vector<aak_params> P(B);
   for (int k = 0; k < B; ++k) P[k] = gpu_params(g, x + 14 * (size_t)k);
   const auto t0 = std::chrono::steady_clock::now();
   g->ctx->out_stride = g->row;
-  r = plan_common(g->ctx, P.data(), nullptr, B, nullptr, nthreads);
+  const int r = plan_common(g->ctx, P.data(), nullptr, B, nullptr, nthreads);
   g->ctx->out_stride = 0;
   g->ms[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (r != AAK_OK) return r;
   for (int k = 0; k < B; ++k)
     if (status) status[k] = g->ctx->status[k];
-  if ((r = upload(g->ctx, 0)) != AAK_OK) return r;
+  return AAK_OK;
+}
+
+// Device half: upload the planned batch and generate it into the rows
+// (asynchronous after the upload, on the legacy default stream).
+int gpu_launch(aak_gpu *g, int B, bool with_t) {
+  int r;
+  if ((r = gpu_capacity(g, B)) != AAK_OK) return r;
+  if ((r = upload(g->ctx, g->stream)) != AAK_OK) return r;
   double *dt = nullptr;
   if (with_t) {
     if ((r = g->d_t.reserve((size_t)g->row)) != AAK_OK) return r;
-    if ((r = cuda_ok(cudaMemsetAsync(g->d_t.ptr, 0, g->row * sizeof(double), 0))) != AAK_OK) return r;
+    if ((r = cuda_ok(cudaMemsetAsync(g->d_t.ptr, 0, g->row * sizeof(double), g->stream))) != AAK_OK) return r;
     dt = g->d_t.ptr;
   }
   if (!g->ev[0])
     for (auto &e : g->ev) cudaEventCreate(&e);
-  cudaEventRecord(g->ev[0], 0);
-  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, g->precision, 0)) != AAK_OK) return r;
-  cudaEventRecord(g->ev[1], 0);
+  cudaEventRecord(g->ev[0], g->stream);
+  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, g->precision, g->stream)) != AAK_OK) return r;
+  cudaEventRecord(g->ev[1], g->stream);
   g->count = B;
   g->spectral = false;
   return AAK_OK;
 }
 
-int gpu_likelihood(aak_gpu *g, double *out) {
+int gpu_generate(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status, bool with_t) {
+  const int r = gpu_plan(g, x, B, nthreads, status);
+  return r != AAK_OK ? r : gpu_launch(g, B, with_t);
+}
+
+// FFT of the rows and the weighted inner products, queued on the legacy
+// default stream; gpu_likelihood_finish copies the results back.
+int gpu_likelihood_launch(aak_gpu *g) {
   if (g->count <= 0) return AAK_ERR_INVALID_PARAM;
   if (!g->ev[0])
     for (auto &e : g->ev) cudaEventCreate(&e);
@@ -1351,13 +1368,13 @@ int gpu_likelihood(aak_gpu *g, double *out) {
       int r = gpu_capacity(g, g->count);
       if (r != AAK_OK) return r;
     }
-    if (cufftSetStream(g->plan, 0) != CUFFT_SUCCESS) return AAK_ERR_CUDA;
+    if (cufftSetStream(g->plan, g->stream) != CUFFT_SUCCESS) return AAK_ERR_CUDA;
     if (cufftExecD2Z(g->plan, g->d_H[0].ptr, reinterpret_cast<cufftDoubleComplex *>(g->d_H[0].ptr)) != CUFFT_SUCCESS ||
         cufftExecD2Z(g->plan, g->d_H[1].ptr, reinterpret_cast<cufftDoubleComplex *>(g->d_H[1].ptr)) != CUFFT_SUCCESS)
       return AAK_ERR_CUDA;
     g->spectral = true;
   }
-  cudaEventRecord(g->ev[2], 0);
+  cudaEventRecord(g->ev[2], g->stream);
   InnerProductArgs a;
   a.H[0] = g->d_H[0].ptr;
   a.H[1] = g->d_H[1].ptr;
@@ -1370,9 +1387,15 @@ int gpu_likelihood(aak_gpu *g, double *out) {
   a.ntemplates = g->count;
   a.partial = g->d_partial.ptr;
   a.out = g->d_out.ptr;
-  launch_inner_products(a, 0);
-  cudaEventRecord(g->ev[3], 0);
-  int r = cuda_ok(cudaMemcpy(out, g->d_out.ptr, (size_t)g->count * 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  launch_inner_products(a, g->stream);
+  cudaEventRecord(g->ev[3], g->stream);
+  return cuda_ok(cudaGetLastError());
+}
+
+int gpu_likelihood_finish(aak_gpu *g, double *out) {
+  int r = cuda_ok(cudaMemcpyAsync(out, g->d_out.ptr, (size_t)g->count * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                  g->stream));
+  if (r == AAK_OK) r = cuda_ok(cudaStreamSynchronize(g->stream));
   if (r != AAK_OK) return r;
   float f;
   if (cudaEventElapsedTime(&f, g->ev[0], g->ev[1]) == cudaSuccess) g->ms[1] = f;
@@ -1380,6 +1403,11 @@ int gpu_likelihood(aak_gpu *g, double *out) {
   if (cudaEventElapsedTime(&f, g->ev[2], g->ev[3]) == cudaSuccess) g->ms[3] = f;
   cudaGetLastError();
   return AAK_OK;
+}
+
+int gpu_likelihood(aak_gpu *g, double *out) {
+  const int r = gpu_likelihood_launch(g);
+  return r != AAK_OK ? r : gpu_likelihood_finish(g, out);
 }
 
 }  // namespace
@@ -1422,12 +1450,20 @@ int aak_gpu_create(double T_fit, int32_t init_length, int32_t length, double ini
     std::vector<double> ones(g->nbins, 1.0);
     cudaMemcpy(g->d_w[ch].ptr, ones.data(), g->nbins * sizeof(double), cudaMemcpyHostToDevice);
   }
+  if ((r = cuda_ok(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking))) != AAK_OK) {
+    aak_gpu_destroy(g);
+    return r;
+  }
   *out = g;
   return cuda_ok(cudaGetLastError());
 }
 
 void aak_gpu_destroy(aak_gpu *g) {
   if (!g) return;
+  if (g->stream) {
+    cudaStreamSynchronize(g->stream);
+    cudaStreamDestroy(g->stream);
+  }
   if (g->plan) cufftDestroy(g->plan);
   for (int ch = 0; ch < 2; ++ch) {
     g->d_H[ch].release();
@@ -1471,6 +1507,7 @@ int aak_gpu_get_waveform(aak_gpu *g, double *t, double *hI, double *hII) {
   std::vector<double> buf(n, 0.0);
   int r;
   const size_t m = std::min(n, (size_t)g->row);
+  if ((r = cuda_ok(cudaStreamSynchronize(g->stream))) != AAK_OK) return r;  // the template's generation
   double *dst[3] = {t, hI, hII};
   const double *src[3] = {g->d_t.ptr, g->d_H[0].ptr, g->d_H[1].ptr};
   for (int k = 0; k < 3; ++k) {
@@ -1494,12 +1531,26 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   std::lock_guard<std::mutex> lk(g->ctx->mu);
   if (max_batch <= 0) max_batch = 256;
   double tot[4] = {0, 0, 0, 0};
+  // batch k + 1 is planned on the host while the device generates,
+  // transforms and reduces batch k (its upload has finished by then, so the
+  // plan arrays are free)
+  int r = gpu_plan(g, params, std::min<int32_t>(max_batch, nsrc), nthreads, status);
+  if (r != AAK_OK) return r;
   for (int32_t k0 = 0; k0 < nsrc; k0 += max_batch) {
     const int B = std::min<int32_t>(max_batch, nsrc - k0);
-    int r = gpu_generate(g, params + 14 * (size_t)k0, B, nthreads, status ? status + k0 : nullptr, false);
-    if (r != AAK_OK) return r;
-    if ((r = gpu_likelihood(g, out + 2 * (size_t)k0)) != AAK_OK) return r;
-    for (int q = 0; q < 4; ++q) tot[q] += g->ms[q];
+    tot[0] += g->ms[0];
+    if ((r = gpu_launch(g, B, false)) != AAK_OK || (r = gpu_likelihood_launch(g)) != AAK_OK) {
+      cudaDeviceSynchronize();
+      return r;
+    }
+    const int32_t k1 = k0 + max_batch;
+    int rp = AAK_OK;
+    if (k1 < nsrc)
+      rp = gpu_plan(g, params + 14 * (size_t)k1, std::min<int32_t>(max_batch, nsrc - k1), nthreads,
+                    status ? status + k1 : nullptr);
+    if ((r = gpu_likelihood_finish(g, out + 2 * (size_t)k0)) != AAK_OK) return r;
+    if (rp != AAK_OK) return rp;
+    for (int q = 1; q < 4; ++q) tot[q] += g->ms[q];
   }
   for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
   return AAK_OK;
