@@ -1,7 +1,9 @@
-"""Module with the reference ``AAKwrapper`` call shape (AAKwrapper/AAKwrapper.pyx:50-88).
+"""Module with the reference ``AAKwrapper`` call shapes (AAKwrapper/AAKwrapper.pyx:50-133).
 
-``wave(pars) -> (t, hI, hII, timing)``; the waveform is computed on the GPU.
+``wave(pars) -> (t, hI, hII, timing)`` and ``phase(pars) -> (t, phase_r,
+phase_theta, phase_phi, omega_r, omega_theta, omega_phi, eccentricity,
+timing)``; both are computed on the GPU.
 """
-from .aak import wave  # noqa: F401
+from .aak import phase, wave  # noqa: F401
 
-__all__ = ["wave"]
+__all__ = ["wave", "phase"]

@@ -2,6 +2,9 @@
 
 * :func:`wave` -- the call shape of the reference ``AAKwrapper.wave(pars)``
   (AAKwrapper/AAKwrapper.pyx:50-88): returns ``(t, hI, hII, timing)``.
+* :func:`phase` -- ``AAKwrapper.phase(pars)`` (AAKwrapper/AAKwrapper.pyx:90-133):
+  returns ``(t, phase_r, phase_theta, phase_phi, omega_r, omega_theta,
+  omega_phi, eccentricity, timing)``.
 * :func:`front_end` / :func:`genwave` -- the two halves of ``AAKwave``
   (src/suite/AAKpy.cc:16-51): mapped trajectory, then GenWave/waveform.
 * :class:`WaveBatch` -- many sources in one launch, outputs in device memory.
@@ -19,7 +22,7 @@ import numpy as np
 from . import _lib
 from ._lib import AAKMapped, AAKValueError, check, lib, make_params, params_array, ptr
 
-__all__ = ["wave", "front_end", "genwave", "Mapped", "WaveBatch", "AAKValueError"]
+__all__ = ["wave", "phase", "PHASE_ROWS", "front_end", "genwave", "Mapped", "WaveBatch", "AAKValueError"]
 
 
 @dataclass
@@ -80,6 +83,21 @@ def wave(pars: dict):
     secs = ctypes.c_double(0.0)
     check(lib().aak_wave(ctypes.byref(make_params(pars)), ptr(t), ptr(hI), ptr(hII), ctypes.byref(secs)), "aak_wave")
     return t, hI, hII, secs.value
+
+
+#: rows of the phase product, in the order of AAKwrapper.phase
+PHASE_ROWS = ("t", "phase_r", "phase_theta", "phase_phi", "omega_r", "omega_theta", "omega_phi", "eccentricity")
+
+
+def phase(pars: dict):
+    """AAKwrapper.phase: ``(t, phase_r, phase_theta, phase_phi, omega_r,
+    omega_theta, omega_phi, eccentricity, timing)`` for the dict of SetPar fields
+    (GenPhase, src/suite/AAKPhase.cc:315-374, on the GPU in FP64)."""
+    n = int(pars["length"])
+    rows = [np.zeros(n) for _ in PHASE_ROWS]
+    secs = ctypes.c_double(0.0)
+    check(lib().aak_phase(ctypes.byref(make_params(pars)), *[ptr(a) for a in rows], ctypes.byref(secs)), "aak_phase")
+    return (*rows, secs.value)
 
 
 def genwave(pars: dict, mapped: Mapped, nmodes: int = 0):
@@ -194,6 +212,26 @@ class WaveBatch:
                                 ctypes.c_void_p(traj_ptr), int(traj_stride), int(precision), ctypes.c_void_p(stream)),
             "aak_batch_run",
         )
+
+    def run_phase(self, out_ptr: int, stride: int, stream: int = 0):
+        """The AAK phase product of every source into device memory: 8 rows
+        (:data:`PHASE_ROWS`) of ``stride`` doubles indexed by :attr:`offsets`."""
+        check(lib().aak_batch_run_phase(self._ctx, ctypes.c_void_p(out_ptr), int(stride), ctypes.c_void_p(stream)),
+              "aak_batch_run_phase")
+
+    def phase_host(self, params, nthreads: int = 0):
+        """Plan + upload + phase product + copy back (host buffers).
+        Returns (rows, offsets, status) with rows of shape (8, total samples)."""
+        self.nsrc = len(params)
+        P = params_array(params)
+        total = int(sum(int(p["length"]) if isinstance(p, dict) else int(p.length) for p in params))
+        rows = np.zeros((8, total))
+        offs = np.zeros(self.nsrc + 1, dtype=np.int64)
+        st = np.zeros(self.nsrc, dtype=np.int32)
+        check(lib().aak_phase_batch_host(self._ctx, P, self.nsrc, int(nthreads), ptr(rows), ptr(offs), ptr(st)),
+              "aak_phase_batch_host")
+        self._info()
+        return rows, offs, st
 
     def launches(self) -> int:
         return int(lib().aak_batch_last_launches(self._ctx))

@@ -623,6 +623,24 @@ BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *t
   return bv;
 }
 
+// The phase product of every source of the uploaded batch into device memory:
+// 8 rows of `stride` doubles (t, phase_r, phase_theta, phase_phi, omega_r,
+// omega_theta, omega_phi, e) indexed by the batch offsets.
+int run_phase(aak_ctx *ctx, double *out, int64_t stride, cudaStream_t st) {
+  if (!ctx->uploaded || !out || stride < ctx->total_samples) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  BatchView bv = batch_view(ctx, nullptr, nullptr, nullptr, nullptr, 0);
+  bv.phase_out = out;
+  bv.phase_stride = stride;
+  bv.trajectory_only = 1;
+  if (ctx->profile && !ctx->ev[0])
+    for (auto &e : ctx->ev) cudaEventCreate(&e);
+  launch_phase(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr);
+  ctx->last_launches = 2;
+  return cuda_ok(cudaGetLastError());
+}
+
 // Plain FP64 per-source path: source by source, the phase kernels on a
 // one-source view write the dense trajectory, then the per-harmonic kernel.
 int run_plain(aak_ctx *ctx, double *hI, double *hII, double *traj, int64_t traj_stride, cudaStream_t st) {
@@ -716,6 +734,25 @@ int host_roundtrip(aak_ctx *ctx, double *t, double *hI, double *hII) {
       (r = cuda_ok(cudaMemcpyAsync(hII, dII, N * sizeof(double), cudaMemcpyDeviceToHost, 0))))
     return r;
   if (t && (r = cuda_ok(cudaMemcpyAsync(t, dt, N * sizeof(double), cudaMemcpyDeviceToHost, 0)))) return r;
+  if ((r = cuda_ok(cudaStreamSynchronize(0))) != AAK_OK) return r;
+  return device_status(ctx);
+}
+
+// Upload, run_phase into the context's device buffer, copy back: rows[k]
+// receives row k (total_samples doubles), or at row k of `base` (stride
+// ldh) when rows is null.
+int phase_roundtrip(aak_ctx *ctx, double *const *rows, double *base, int64_t ldh) {
+  int r;
+  const int64_t N = ctx->total_samples;
+  if ((r = upload(ctx, 0)) != AAK_OK) return r;
+  if ((r = ctx->d_out.reserve((size_t)8 * std::max<int64_t>(N, 1))) != AAK_OK) return r;
+  double *d = ctx->d_out.ptr;
+  if ((r = run_phase(ctx, d, N, 0)) != AAK_OK) return r;
+  for (int k = 0; k < 8; ++k) {
+    double *h = rows ? rows[k] : base + k * ldh;
+    if (h && (r = cuda_ok(cudaMemcpyAsync(h, d + k * N, N * sizeof(double), cudaMemcpyDeviceToHost, 0))) != AAK_OK)
+      return r;
+  }
   if ((r = cuda_ok(cudaStreamSynchronize(0))) != AAK_OK) return r;
   return device_status(ctx);
 }
@@ -1186,6 +1223,44 @@ int aak_wave(const aak_params *p, double *t, double *hI, double *hII, double *se
   r = host_roundtrip(ctx, t, hI, hII);
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return r;
+}
+
+int aak_phase(const aak_params *p, double *t, double *phase_r, double *phase_theta, double *phase_phi,
+              double *omega_r, double *omega_theta, double *omega_phi, double *eccentricity, double *seconds) {
+  if (!p || !t || !phase_r || !phase_theta || !phase_phi || !omega_r || !omega_theta || !omega_phi || !eccentricity)
+    return AAK_ERR_INVALID_PARAM;
+  const auto t0 = std::chrono::steady_clock::now();
+  aak_ctx *ctx = nullptr;
+  int r = default_ctx(&ctx);
+  if (r != AAK_OK) return r;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  r = plan_common(ctx, p, nullptr, 1, nullptr, 1);
+  if (r != AAK_OK) return r;
+  if (ctx->status[0] != AAK_OK) return ctx->status[0];
+  double *const rows[8] = {t, phase_r, phase_theta, phase_phi, omega_r, omega_theta, omega_phi, eccentricity};
+  r = phase_roundtrip(ctx, rows, nullptr, 0);
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r;
+}
+
+int aak_batch_run_phase(aak_ctx *ctx, double *d_out, int64_t stride, void *stream) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return run_phase(ctx, d_out, stride, (cudaStream_t)stream);
+}
+
+int aak_phase_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads, double *h_out,
+                         int64_t *offsets, int32_t *status) {
+  if (!ctx || !P || !h_out || nsrc < 1) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  int r = plan_common(ctx, P, nullptr, nsrc, nullptr, nthreads);
+  if (r == AAK_OK) r = phase_roundtrip(ctx, nullptr, h_out, ctx->total_samples);
+  if (r != AAK_OK) return r;
+  if (offsets)
+    for (int s = 0; s <= nsrc; ++s) offsets[s] = ctx->offsets[s];
+  if (status)
+    for (int s = 0; s < nsrc; ++s) status[s] = ctx->status[s];
+  return AAK_OK;
 }
 
 int aak_genwave(double *t, double *hI, double *hII, double timestep, int32_t vlength, const double *e_traj,

@@ -965,7 +965,13 @@ static_assert(kTileChunks % AAK_JOINT_SPLIT == 0 && kTileChunks % AAK_JOINT_FP64
 constexpr int kDynVals = 7;  // e, Omega_phi M_phys, gamma~, Phi, alpha, nu, gamma~dot
 constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double);
 
-template <bool kSplit>
+// kPhase: the phase product instead of the waveform (FP64 only): every
+// sample of each source runs through phase 1, the harmonic sums are skipped,
+// and the tile's samples are written to bv.phase_out as t, phase_r,
+// phase_theta, phase_phi, omega_r, omega_theta, omega_phi, e (the per-sample
+// packing of GenPhase, AAKPhase.cc:346-355).  The phases of the samples
+// after the plunge buffer are frozen afterwards by k_phase_freeze.
+template <bool kSplit, bool kPhase = false>
 __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
   __shared__ double red[3][kTileThreads / 32];
@@ -990,7 +996,8 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const SourceDesc *dp;
     const TileCtx c = tile_ctx(bv, j, dp);
     const int64_t g = c.g;
-    const int lim = min(c.end, c.neff);  // samples [start, lim) feed the output
+    // samples [start, lim) feed the output (the phase product: every sample)
+    const int lim = kPhase ? c.end : min(c.end, c.neff);
     if (dp->status != 0 || lim <= c.start) {
       // failed source, or a tile entirely after the taper: zeros, and an
       // empty aggregate for the chain
@@ -998,9 +1005,13 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       for (int ch = 0; ch < kTileChunks; ++ch) {
         const int i = c.start + ch * kTileThreads + tid;
         if (i < c.end) {
-          bv.hI[dz.out_offset + i] = 0.0;
-          bv.hII[dz.out_offset + i] = 0.0;
-          if (bv.t_out) bv.t_out[dz.out_offset + i] = (dz.status != 0) ? 0.0 : sample_time(dz, i);
+          if constexpr (kPhase) {
+            for (int r = 0; r < 8; ++r) bv.phase_out[r * bv.phase_stride + dz.out_offset + i] = 0.0;
+          } else {
+            bv.hI[dz.out_offset + i] = 0.0;
+            bv.hII[dz.out_offset + i] = 0.0;
+            if (bv.t_out) bv.t_out[dz.out_offset + i] = (dz.status != 0) ? 0.0 : sample_time(dz, i);
+          }
         }
       }
       if (tid == 0) {
@@ -1078,7 +1089,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const double Cin = needC ? s_cy[6] : 0.0;
 #if !AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread per harmonic); its barrier is the first one of phase 1
-    if (K > 0 && !bv.trajectory_only)
+    if (!kPhase && K > 0 && !bv.trajectory_only)
       for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
         if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
@@ -1111,7 +1122,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
         }
       }
       sv_e[sl] = q.e;
-      sv_om[sl] = om * d.M_phys_sec;
+      sv_om[sl] = kPhase ? r[2] : om * d.M_phys_sec;  // the phase product keeps alphadot here
       sv_gim[sl] = r[0];
       sv_Phi[sl] = r[1];
       sv_alp[sl] = r[2];
@@ -1193,7 +1204,9 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
             incB[k][2] = (1.5 * rc[2] - .5 * rn[2]) * d.dt;
           }
         }
-        nuv[k] = ((i > d.i0) ? P : rc[1]) / 2. / kPi;
+        // nu (the phase product: Phidot itself, clamped after i0 only,
+        // as PNevolutionPhase records it, AAKPhase.cc:246-248, 266-270)
+        nuv[k] = kPhase ? ((i > d.i0) ? P : rc[1]) : ((i > d.i0) ? P : rc[1]) / 2. / kPi;
         rm[0] = rc[0];
         rm[1] = rc[1];
         rm[2] = rc[2];
@@ -1275,7 +1288,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     }
 #if AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread of warps 1-7 per harmonic) while warp 0 looks back
-    else if (K > 0 && !bv.trajectory_only)
+    else if (!kPhase && K > 0 && !bv.trajectory_only)
       for (int n = tid - 31; n <= d.nmodes; n += kTileThreads - 32) {
         if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
@@ -1307,11 +1320,25 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           bv.traj_out[5 * st + o] = X[1];
           bv.traj_out[6 * st + o] = X[2];
         }
+        if constexpr (kPhase) {
+          // GenPhase's packing, sums in its order (AAKPhase.cc:347-354)
+          const int64_t o = d.out_offset + i;
+          const int64_t st = bv.phase_stride;
+          const double Pd = sv_nu[sl], gd = sv_gd[sl], ad = sv_om[sl];
+          bv.phase_out[o] = sample_time(d, i);
+          bv.phase_out[st + o] = X[1];
+          bv.phase_out[2 * st + o] = X[1] + X[0];
+          bv.phase_out[3 * st + o] = X[1] + X[0] + X[2];
+          bv.phase_out[4 * st + o] = Pd;
+          bv.phase_out[5 * st + o] = Pd + gd;
+          bv.phase_out[6 * st + o] = Pd + gd + ad;
+          bv.phase_out[7 * st + o] = sv_e[sl];
+        }
       }
     }
     // ---------------- phase 2: harmonic sums of this thread's own samples,
     // kJoint of them at a time (shared table loads, independent recurrences)
-    if (bv.trajectory_only) continue;
+    if (kPhase || bv.trajectory_only) continue;
     const double t_plunge = sample_time(d, d.i_plunge);
     const double t_zero = t_plunge + d.dt * d.i_buffer;
     using T = typename std::conditional<kSplit, float, double>::type;
@@ -1591,6 +1618,7 @@ void prepare_dense_launch() {
     const int most = (int)(kWaveDynSmem + (size_t)kTabModes * kRowD * sizeof(double));
     cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    cudaFuncSetAttribute(k_waveform<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     attrs_set.fetch_or(bit);
   }
 }
@@ -1616,6 +1644,51 @@ void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
   const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
   if (precision == 1) k_waveform<true><<<grid2, kTileThreads, dyn, stream>>>(bv);
   else k_waveform<false><<<grid2, kTileThreads, dyn, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[3], stream);
+}
+
+// The phases of the samples after the plunge buffer hold their values at
+// i_plunge: GenPhase's evolution sets gim/Phi/alp[i+1] to their values at
+// i_plunge for every forward step i > i_plunge + i_buffer (AAKPhase.cc:253-257),
+// i.e. the samples from max(i_plunge + i_buffer + 2, i0 + 1) on.  Rows 1-3 of
+// phase_out are sums of those three phases, so they take their own values at
+// i_plunge.  y strides over sources, x over each source's frozen samples.
+__global__ void __launch_bounds__(256) k_phase_freeze(const SourceDesc *__restrict__ src, int nsrc,
+                                                      double *__restrict__ out, int64_t st) {
+  for (int s = blockIdx.y; s < nsrc; s += gridDim.y) {
+    const SourceDesc &d = src[s];
+    if (d.status != 0 || d.i_plunge < 0 || d.i_plunge >= d.vlength) continue;
+    const long long first = max((long long)d.i_plunge + (long long)d.i_buffer + 2, (long long)d.i0 + 1);
+    if (first >= d.vlength) continue;
+    const int64_t o = d.out_offset;
+    const double pr = out[st + o + d.i_plunge], pt = out[2 * st + o + d.i_plunge];
+    const double pp = out[3 * st + o + d.i_plunge];
+    for (long long i = first + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < d.vlength;
+         i += (long long)gridDim.x * blockDim.x) {
+      out[st + o + i] = pr;
+      out[2 * st + o + i] = pt;
+      out[3 * st + o + i] = pp;
+    }
+  }
+}
+
+void launch_phase(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev) {
+  if (bv.total_tiles <= 0 || !bv.phase_out) return;
+  if (ev) cudaEventRecord(ev[0], stream);
+  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
+  cudaMemsetAsync(bv.link_flag, 0, (size_t)bv.total_tiles * sizeof(int32_t), stream);
+  if (ev) {
+    cudaEventRecord(ev[1], stream);
+    cudaEventRecord(ev[2], stream);
+  }
+  prepare_dense_launch();
+  int resident = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false, true>, kTileThreads, kWaveDynSmem);
+  resident = std::max(resident, 1);
+  const int grid = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
+  k_waveform<false, true><<<grid, kTileThreads, kWaveDynSmem, stream>>>(bv);
+  const dim3 fgrid(64, (unsigned)std::min(std::max(bv.nsrc, 1), 1024));
+  k_phase_freeze<<<fgrid, 256, 0, stream>>>(bv.src, bv.nsrc, bv.phase_out, bv.phase_stride);
   if (ev) cudaEventRecord(ev[3], stream);
 }
 

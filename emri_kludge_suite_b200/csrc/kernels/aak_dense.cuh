@@ -60,6 +60,8 @@ struct BatchView {
   int32_t trajectory_only = 0;       // 1: write traj_out and skip the harmonic sums
   int32_t max_nmodes = 0;            // largest harmonic count of the batch (0: unknown) -- sizes the tile table
   long long lookback_cycles = 0;     // bound of one look-back wait in SM clocks (<= 0: about 2 s)
+  double *phase_out = nullptr;       // launch_phase: 8 x phase_stride (t, phase_r, phase_theta, phase_phi,
+  int64_t phase_stride = 0;          //   omega_r, omega_theta, omega_phi, e), indexed by src.out_offset + i
 };
 
 // Clear the work queue and the look-back flags, then launch the waveform
@@ -69,6 +71,12 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
 // precision 0: FP64 throughout; 1: split (FP64 phases and reductions, FP32
 // geometry, response, Bessel evaluation and harmonic recurrence).
 void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision);
+// The AAK phase product of GenPhase (src/suite/AAKPhase.cc:315-374) for
+// every source of the batch into bv.phase_out: the waveform kernel's phase
+// pass over all samples (no harmonic sums), then the freeze of the phases
+// after the plunge buffer.  ev (optional, 4 events) as launch_dense, ev[3]
+// after the freeze.
+void launch_phase(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev);
 
 // Plain FP64 per-source harmonic sum: the per-sample algorithm of the
 // reference's CUDA port (src/cuda/kernel.cu:374-555) -- five Bessel functions

@@ -98,6 +98,17 @@ int aak_parmap(const double Omega[3], double p, double M, double s, double e, do
  * Runs on the current CUDA device; fails with AAK_ERR_CUDA without one. */
 int aak_wave(const aak_params *p, double *t, double *hI, double *hII, double *seconds);
 
+/* ------------------------------------------------------------------ AAK phases (GPU) */
+/* Replaces AAKphase (include/AAKpy.h:21, src/suite/AAKpy.cc:53-88, GenPhase
+ * src/suite/AAKPhase.cc:315-374).  Host buffers of p->length doubles: t, the
+ * three phases Phi, Phi + gamma~, Phi + gamma~ + alpha, the three rates Phidot
+ * (clamped after t = 0), Phidot + gamma~dot, Phidot + gamma~dot + alphadot, and
+ * the eccentricity; the phases after i_plunge + i_buffer + 1 hold their values
+ * at i_plunge.  FP64.  *seconds (optional) receives the wall time.  Errors as
+ * aak_wave. */
+int aak_phase(const aak_params *p, double *t, double *phase_r, double *phase_theta, double *phase_phi,
+              double *omega_r, double *omega_theta, double *omega_phi, double *eccentricity, double *seconds);
+
 /* Replaces GenWave -> waveform (src/suite/AAK.cc:321-591) on an already
  * mapped trajectory; nmodes_override <= 0 keeps the reference harmonic rule
  * int(30 e0) (4 below e0 = 0.135).  Host buffers of vlength doubles. */
@@ -149,6 +160,20 @@ int aak_batch_upload(aak_ctx *ctx, void *stream);
  * harmonic recurrence). */
 int aak_batch_run(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_t, double *d_traj, int64_t traj_stride,
                   int32_t precision, void *stream);
+
+/* The AAK phase product (as aak_phase) of every source of the uploaded batch
+ * into caller device memory: 8 rows of `stride` doubles (stride >= the
+ * batch's total samples) -- t, phase_r, phase_theta, phase_phi, omega_r,
+ * omega_theta, omega_phi, eccentricity -- each indexed by the batch offsets.
+ * Batched counterpart of AAKphase (src/suite/AAKpy.cc:53-88); two kernels. */
+int aak_batch_run_phase(aak_ctx *ctx, double *d_out, int64_t stride, void *stream);
+
+/* Plan + upload + phase product + copy back for nsrc sources: h_out holds
+ * 8 rows of sum(P[s].length) doubles in the aak_batch_run_phase layout;
+ * offsets (nsrc + 1) and status (nsrc) optional.  A source that fails has
+ * status != 0 and zeros in its rows. */
+int aak_phase_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads, double *h_out,
+                         int64_t *offsets, int32_t *status);
 
 /* Allocation-free variant of aak_batch_run, for callers that cannot call
  * cudaMalloc: code whose device memory belongs to a host framework or a

@@ -1,5 +1,5 @@
 /*
- * aak_oracle.c -- CPU restatement of the reference AAK dense waveform path.
+ * aak_oracle.c -- CPU restatement of the reference AAK dense waveform and phase paths.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker for the product's
  * host + CUDA path: only tests/, __graft_entry__.smoke() and the CPU-baseline
@@ -19,6 +19,7 @@
  *   - natural cubic spline Interp                            src/suite/KSParMap.cc:487-498
  *   - Kerr constants + radial roots + stability (IEKG)       src/inclecc/IEKG.cc:19-159, IEKGMNewt.cc
  *   - PNevolution                                            src/suite/AAK.cc:27-318
+ *   - PNevolutionPhase + GenPhase (the AAK phases product)   src/suite/AAKPhase.cc:13-374
  *   - RotCoeff                                               src/suite/KSParMap.cc:532-574
  *   - waveform (harmonic sum, LISA response, Planck taper)   src/suite/AAK.cc:321-562
  *   - Bessel J_n by Miller's backward recurrence (long double), standing in
@@ -431,13 +432,16 @@ static double o_p_of(double v, double e, double coslam, double S, double M, doub
   return (1. - e * e) * pow(oracle_omega_phi(v, e, coslam, S, M) * M_phys * O_MSUN_SEC, -2. / 3.);
 }
 
-/* AAK.cc:27-318.  Dense arrays hold vlength+1 entries.  Returns 0, or -1 when
- * the fit has fewer than three points (the reference exits the process). */
-int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, double *gim, double *Phi, double *alp,
-                       double *nu, double *gimdotvec, double timestep, int vlength, const double *par,
-                       const double *e_traj, const double *v_map, double M_phys, const double *M_map, double S_phys,
-                       const double *S_map, const double *dt_map, int steps, int *i_plunge, int *i_buffer,
-                       int backint) {
+/* AAK.cc:27-318, and with Phidotvec/alpdotvec non-null PNevolutionPhase
+ * (AAKPhase.cc:13-313), which also records Phidot (the clamped value on the
+ * forward samples after i0, the raw one elsewhere) and alpdot.  Dense arrays
+ * hold vlength+1 entries.  Returns 0, or -1 when the fit has fewer than three
+ * points (the reference exits the process). */
+static int o_pnevolution(double *t, double *e, double *v, double *M, double *S, double *gim, double *Phi, double *alp,
+                         double *nu, double *gimdotvec, double *Phidotvec, double *alpdotvec, double timestep,
+                         int vlength, const double *par, const double *e_traj, const double *v_map, double M_phys,
+                         const double *M_map, double S_phys, const double *S_map, const double *dt_map, int steps,
+                         int *i_plunge, int *i_buffer, int backint) {
   const double mu = par[0], M0 = par[1], S0 = par[2], e0 = par[3], v0 = v_map[0];
   const double coslam = cos(par[4]);
   const double gim0 = par[5], Phi0 = par[6], alp0 = par[11];
@@ -624,6 +628,10 @@ int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, do
     }
     nu[i] = Phidot / 2. / M_PI;
     gimdotvec[i] = gimdot;
+    if (Phidotvec) {
+      Phidotvec[i] = Phidot;
+      alpdotvec[i] = alpdot;
+    }
     gim[i + 1] = gim[i] + (1.5 * gimdot - .5 * gimdotm) * timestep;
     Phi[i + 1] = Phi[i] + (1.5 * Phidot - .5 * Phidotm) * timestep;
     alp[i + 1] = alp[i] + (1.5 * alpdot - .5 * alpdotm) * timestep;
@@ -639,6 +647,10 @@ int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, do
     double thm = oracle_dthetadm(v[i], e[i], coslam, S[i]);
     nu[i] = rm / tm / (2. * M_PI * M[i]);
     gimdotvec[i] = (thm - rm) / tm / M[i];
+    if (Phidotvec) {
+      Phidotvec[i] = rm / tm / M[i];
+      alpdotvec[i] = (oracle_dphidm(v[i], e[i], coslam, S[i]) - thm) / tm / M[i];
+    }
   }
   /* dense phases, backward from i0 */
   double gimdotp, Phidotp, alpdotp;
@@ -658,6 +670,10 @@ int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, do
     }
     nu[i] = Phidot / 2. / M_PI;
     gimdotvec[i] = gimdot;
+    if (Phidotvec) {
+      Phidotvec[i] = Phidot;
+      alpdotvec[i] = alpdot;
+    }
     gim[i - 1] = gim[i] - (1.5 * gimdot - .5 * gimdotp) * timestep;
     Phi[i - 1] = Phi[i] - (1.5 * Phidot - .5 * Phidotp) * timestep;
     alp[i - 1] = alp[i] - (1.5 * alpdot - .5 * alpdotp) * timestep;
@@ -668,10 +684,23 @@ int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, do
     double thm = oracle_dthetadm(v[i], e[i], coslam, S[i]);
     nu[i] = rm / tm / (2. * M_PI * M[i]);
     gimdotvec[i] = (thm - rm) / tm / M[i];
+    if (Phidotvec) {
+      Phidotvec[i] = rm / tm / M[i];
+      alpdotvec[i] = (oracle_dphidm(v[i], e[i], coslam, S[i]) - thm) / tm / M[i];
+    }
   }
   free(e_AK); free(v_AK); free(t_fit); free(e_fit); free(v_fit); free(M_fit); free(S_fit);
   free(e_diff); free(v_diff);
   return 0;
+}
+
+int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, double *gim, double *Phi, double *alp,
+                       double *nu, double *gimdotvec, double timestep, int vlength, const double *par,
+                       const double *e_traj, const double *v_map, double M_phys, const double *M_map, double S_phys,
+                       const double *S_map, const double *dt_map, int steps, int *i_plunge, int *i_buffer,
+                       int backint) {
+  return o_pnevolution(t, e, v, M, S, gim, Phi, alp, nu, gimdotvec, NULL, NULL, timestep, vlength, par, e_traj, v_map,
+                       M_phys, M_map, S_phys, S_map, dt_map, steps, i_plunge, i_buffer, backint);
 }
 
 /* ------------------------------------------------------------------ waveform */
@@ -834,4 +863,51 @@ int oracle_genwave(double *t, double *hI, double *hII, double timestep, int vlen
   double zeta = par[0] / dist / O_GPC;
   return oracle_waveform(t, hI, hII, timestep, vlength, nmodes, zeta, par, e_traj, v_map, M_phys, M_map, S_phys, S_map,
                          dt_map, steps, backint, mich, i_plunge, i_buffer);
+}
+
+/* ------------------------------------------------------------------ phases */
+/* GenPhase (AAKPhase.cc:315-374): PNevolutionPhase on the GenWave packing,
+ * then per sample phase_r = Phi, phase_theta = Phi + gim, phase_phi =
+ * Phi + gim + alp, omega_r = Phidot, omega_theta = Phidot + gimdot,
+ * omega_phi = Phidot + gimdot + alpdot, eccentricity = e (vlength entries
+ * each).  Returns 0, or -1 when PNevolution fails. */
+int oracle_genphase(double *t, double *phase_r, double *phase_theta, double *phase_phi, double *omega_r,
+                    double *omega_theta, double *omega_phi, double *eccentricity, double timestep, int vlength,
+                    const double *e_traj, const double *v_map, double M_phys, const double *M_map, double mu,
+                    double S_phys, const double *S_map, double inc, double gim0, double Phi0, double alp0,
+                    const double *dt_map, int steps, int backint, int *i_plunge, int *i_buffer) {
+  double par[12] = {0};
+  par[0] = mu * O_MSUN_SEC;
+  par[1] = M_map[0] * O_MSUN_SEC;
+  par[2] = S_map[0];
+  par[3] = e_traj[0];
+  par[4] = inc;
+  par[5] = gim0;
+  par[6] = Phi0;
+  par[11] = alp0;
+  const size_t n1 = (size_t)vlength + 1;
+  double *buf = (double *)malloc(12 * n1 * sizeof(double));
+  if (!buf) return -1;
+  double *tv = buf, *ev = buf + n1, *vv = buf + 2 * n1, *Mv = buf + 3 * n1, *Sv = buf + 4 * n1, *gv = buf + 5 * n1;
+  double *Pv = buf + 6 * n1, *av = buf + 7 * n1, *nv = buf + 8 * n1, *gdv = buf + 9 * n1, *Pdv = buf + 10 * n1;
+  double *adv = buf + 11 * n1;
+  int ip = 0, ib = 0;
+  int rc = o_pnevolution(tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, Pdv, adv, timestep, vlength, par, e_traj, v_map,
+                         M_phys, M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint);
+  if (rc == 0) {
+    for (int i = 0; i < vlength; ++i) {
+      t[i] = tv[i];
+      phase_r[i] = Pv[i];
+      phase_theta[i] = Pv[i] + gv[i];
+      phase_phi[i] = Pv[i] + gv[i] + av[i];
+      omega_r[i] = Pdv[i];
+      omega_theta[i] = Pdv[i] + gdv[i];
+      omega_phi[i] = Pdv[i] + gdv[i] + adv[i];
+      eccentricity[i] = ev[i];
+    }
+  }
+  if (i_plunge) *i_plunge = ip;
+  if (i_buffer) *i_buffer = ib;
+  free(buf);
+  return rc;
 }

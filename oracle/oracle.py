@@ -240,6 +240,66 @@ def oracle_pnevolution(pars: dict, mt: MappedTrajectory):
     return outs, ip.value, ib.value
 
 
+PHASE_KEYS = ("t", "phase_r", "phase_theta", "phase_phi", "omega_r", "omega_theta", "omega_phi", "eccentricity")
+
+
+def ref_aakphase(pars: dict):
+    """Reference AAKphase (src/suite/AAKpy.cc:53-88): the eight arrays of
+    PHASE_KEYS and the timing, as AAKwrapper.phase returns them."""
+    L = ref_lib()
+    p = make_ref_params(pars)
+    n = int(pars["length"])
+    outs = [np.zeros(n) for _ in PHASE_KEYS]
+    L.ref_aakphase.restype = ctypes.c_double
+    secs = L.ref_aakphase(ctypes.byref(p), *[_ptr(o) for o in outs])
+    return (*outs, secs)
+
+
+def _genphase_args(pars: dict, mt: MappedTrajectory):
+    return [
+        ctypes.c_double(pars["dt"]),
+        ctypes.c_int(int(pars["length"])),
+        _ptr(mt.e_traj),
+        _ptr(mt.v_map),
+        ctypes.c_double(pars["M"]),
+        _ptr(mt.M_map),
+        ctypes.c_double(pars["mu"]),
+        ctypes.c_double(pars["s"]),
+        _ptr(mt.s_map),
+    ]
+
+
+def ref_genphase(pars: dict, mt: MappedTrajectory):
+    """Reference GenPhase (src/suite/AAKPhase.cc:315-374) on a mapped trajectory."""
+    L = ref_lib()
+    n = int(pars["length"])
+    outs = [np.zeros(n) for _ in PHASE_KEYS]
+    L.ref_genphase(
+        *[_ptr(o) for o in outs], *_genphase_args(pars, mt), ctypes.c_double(pars["D"]),
+        ctypes.c_double(pars["iota"]), ctypes.c_double(pars["gamma"]), ctypes.c_double(mt.Phi0),
+        ctypes.c_double(pars["theta_S"]), ctypes.c_double(pars["phi_S"]), ctypes.c_double(pars["alpha"]),
+        ctypes.c_double(pars["theta_K"]), ctypes.c_double(pars["phi_K"]), _ptr(mt.dt_map), ctypes.c_int(mt.steps),
+        ctypes.c_int(int(bool(pars["backint"]))),
+    )
+    return tuple(outs)
+
+
+def oracle_genphase(pars: dict, mt: MappedTrajectory):
+    """The oracle's GenPhase: (PHASE_KEYS arrays..., i_plunge, i_buffer)."""
+    L = oracle_lib()
+    n = int(pars["length"])
+    outs = [np.zeros(n) for _ in PHASE_KEYS]
+    ip, ib = ctypes.c_int(), ctypes.c_int()
+    rc = L.oracle_genphase(
+        *[_ptr(o) for o in outs], *_genphase_args(pars, mt), ctypes.c_double(pars["iota"]),
+        ctypes.c_double(pars["gamma"]), ctypes.c_double(mt.Phi0), ctypes.c_double(pars["alpha"]), _ptr(mt.dt_map),
+        ctypes.c_int(mt.steps), ctypes.c_int(int(bool(pars["backint"]))), ctypes.byref(ip), ctypes.byref(ib),
+    )
+    if rc != 0:
+        raise ValueError("oracle: fitting error, t_0 too close to plunge")
+    return (*outs, ip.value, ib.value)
+
+
 def ref_pnevolution(pars: dict, mt: MappedTrajectory):
     L = ref_lib()
     n = int(pars["length"])

@@ -11,6 +11,8 @@
 //   ref_front      : src/suite/AAKpy.cc:20-44   (GKTrajFast + Frequencies + ParAng + ParMap)
 //   ref_genwave    : src/suite/AAK.cc:565-591   (GenWave packing) with an optional nmodes override
 //   ref_aakwave    : src/suite/AAKpy.cc:16-51   (AAKwave itself)
+//   ref_aakphase   : src/suite/AAKpy.cc:53-88   (AAKphase itself)
+//   ref_genphase   : src/suite/AAKPhase.cc:315-374 (GenPhase on a mapped trajectory)
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
@@ -29,14 +31,9 @@
 #include "AAKTDI.h"
 #include "AKTDI.h"
 
-// The reference's AAKpy.cc also defines AAKphase/AAKTDI/AKTDI, whose callees
-// live in translation units outside the waveform path.  They are never
-// called through this harness; these definitions only satisfy the linker.
-void GenPhase(double *, double *, double *, double *, double *, double *, double *, double *, double, int,
-              double[], double[], double, double[], double, double, double[], double, double, double, double,
-              double, double, double, double, double, double[], int, bool, bool, bool) {
-  std::abort();
-}
+// The reference's AAKpy.cc also defines AAKTDI/AKTDI, whose callees live in
+// translation units outside this build.  They are never called through this
+// harness; these definitions only satisfy the linker.
 void GenTDI(double *, double *, double *, double *, double *, double *, double *, double, int, double[], double[],
             double, double[], double, double, double[], double, double, double, double, double, double, double,
             double, double, double[], int, bool, bool, bool) {
@@ -89,6 +86,24 @@ double ref_aakwave(const ref_params *r, double *t, double *hI, double *hII) {
   SetPar s;
   to_setpar(r, &s);
   return AAKwave(s, t, hI, hII);
+}
+
+double ref_aakphase(const ref_params *r, double *t, double *phase_r, double *phase_theta, double *phase_phi,
+                    double *omega_r, double *omega_theta, double *omega_phi, double *eccentricity) {
+  SetPar s;
+  to_setpar(r, &s);
+  return AAKphase(s, t, phase_r, phase_theta, phase_phi, omega_r, omega_theta, omega_phi, eccentricity);
+}
+
+// GenPhase (AAKPhase.cc:315-374) on a mapped trajectory; outputs hold vlength entries.
+void ref_genphase(double *t, double *phase_r, double *phase_theta, double *phase_phi, double *omega_r,
+                  double *omega_theta, double *omega_phi, double *eccentricity, double timestep, int vlength,
+                  const double *e_traj, const double *v_map, double M_phys, const double *M_map, double mu,
+                  double S_phys, const double *S_map, double dist, double inc, double gim0, double Phi0, double qS,
+                  double phiS, double alp0, double qK, double phiK, const double *dt_map, int steps, int backint) {
+  GenPhase(t, phase_r, phase_theta, phase_phi, omega_r, omega_theta, omega_phi, eccentricity, timestep, vlength,
+           (double *)e_traj, (double *)v_map, M_phys, (double *)M_map, mu, S_phys, (double *)S_map, dist, inc, gim0,
+           Phi0, qS, phiS, alp0, qK, phiK, (double *)dt_map, steps, backint != 0, false, false);
 }
 
 // Front end of AAKwave: coarse Kerr inspiral, Kerr frequencies, initial mean

@@ -4,8 +4,10 @@ Runs the reference AAK code compiled from its own sources (oracle/_ref/
 libaakref.so, ``make -C oracle ref``) on a few small parameter sets and
 stores its outputs: the mapped trajectory of the front end
 (src/suite/AAKpy.cc:20-44), the waveform of AAKwave with the reference
-harmonic rule, the waveform of waveform() with a harmonic-count override, and
-for some cases the dense PNevolution arrays (src/suite/AAK.cc:27-318).
+harmonic rule, the waveform of waveform() with a harmonic-count override, the
+seven phase arrays of AAKphase (src/suite/AAKpy.cc:53-88, whose time array is
+the AAKwave one), and for some cases the dense PNevolution arrays
+(src/suite/AAK.cc:27-318).
 
     python tests/golden/make_golden.py
 
@@ -56,6 +58,8 @@ def run_case(name, spec):
     mt = O.ref_front(pars)
     t_w, hI_w, hII_w, _ = O.ref_aakwave(pars)
     t_g, hI_g, hII_g = O.ref_genwave(pars, mt, nmodes)
+    phase = O.ref_aakphase(pars)
+    assert np.array_equal(phase[0], t_w)
     out = dict(
         pars=json.dumps(pars),
         nmodes=np.int32(nmodes),
@@ -74,6 +78,8 @@ def run_case(name, spec):
         genwave_hI=hI_g,
         genwave_hII=hII_g,
     )
+    for k, a in zip(O.PHASE_KEYS[1:], phase[1:8]):
+        out["aakphase_" + k] = a
     if dense:
         arrs, ip, ib = O.ref_pnevolution(pars, mt)
         for k, a in zip("t e v M S gim Phi alp nu gimdot".split(), arrs):

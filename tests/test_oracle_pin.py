@@ -40,6 +40,40 @@ def test_oracle_dense_trajectory_matches_reference_fixture(name):
         assert rel < 1e-12, (k, rel)
 
 
+@pytest.mark.parametrize("name", golden_names())
+def test_oracle_phases_match_reference_fixture(name):
+    """GenPhase restatement against the reference AAKphase outputs."""
+    g = load_golden(name)
+    pars = g["pars"]
+    mt = O.MappedTrajectory(int(g["steps"]), g["e_traj"], g["v_map"], g["M_map"], g["s_map"], g["dt_map"],
+                            float(g["Phi0"]), 2)
+    out = O.oracle_genphase(pars, mt)
+    assert np.array_equal(out[0], g["aakwave_t"])
+    for k, a in zip(O.PHASE_KEYS[1:], out[1:8]):
+        ref = g["aakphase_" + k]
+        # the phases grow to ~1e5 rad: compare them against their largest value;
+        # the rates and e sample by sample
+        den = np.abs(ref).max() if k.startswith("phase") else np.maximum(np.abs(ref), 1e-300)
+        rel = np.max(np.abs(a - ref) / den)
+        assert rel < 1e-13, (k, rel)
+
+
+def test_oracle_phase_freeze_after_plunge_buffer():
+    """The phases of the samples after i_plunge + i_buffer + 1 hold their values at
+    i_plunge (AAKPhase.cc:253-257); the rates and e run on."""
+    g = load_golden("plunge")
+    pars = g["pars"]
+    mt = O.MappedTrajectory(int(g["steps"]), g["e_traj"], g["v_map"], g["M_map"], g["s_map"], g["dt_map"],
+                            float(g["Phi0"]), 2)
+    t, pr, pt, pp, wr, wt, wp, e, ip, ib = O.oracle_genphase(pars, mt)
+    first = ip + ib + 2
+    assert first < len(t)
+    for a in (pr, pt, pp):
+        assert np.all(a[first:] == a[ip])
+        assert a[first - 1] != a[ip]
+    assert not np.all(wr[first:] == wr[ip])
+
+
 def test_oracle_bessel_against_scipy():
     rng = np.random.default_rng(7)
     for _ in range(200):
