@@ -288,6 +288,108 @@ def run_likelihood(n_templates: int, local_rank: int, model=None) -> dict:
 
 
 # ----------------------------------------------------------------------------- GPU arm
+def ref_phase_rate(sources, n_src: int = 16, sample_len: int = 200000) -> dict:
+    """The reference's own AAKphase (front end + GenPhase), one process, on a
+    bounded sample of the configuration-1 sources."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return {"value": None, "unit": "samples/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libaakref.so is not built"}
+    tot, t0 = 0, time.perf_counter()
+    for p in sources[:n_src]:
+        q = dict(p)
+        q["length"] = min(int(p["length"]), sample_len)
+        q["T"] = q["length"] * q["dt"] / YEAR
+        O.ref_aakphase(q)
+        tot += q["length"]
+    dt = time.perf_counter() - t0
+    return {"value": tot / dt, "unit": "samples/s", "cores": 1, "kind": "reference",
+            "sample": f"{n_src} config-1 sources truncated to {sample_len} samples, reference AAKphase "
+                      "(front end + GenPhase), one process"}
+
+
+def run_phases(args, wb, sources, sptr, stream, N, N_all, reduce_max, local_rank, nthreads):
+    """AAK phase product (GenPhase: t, 3 phases, 3 rates, e per sample, FP64) of
+    the uploaded configuration-1 batch: device-resident kernel time, roofline,
+    and end to end through aak_phase_batch_host on a subset."""
+    import ctypes
+
+    import torch
+
+    import emri_kludge_suite_b200 as E
+    from emri_kludge_suite_b200 import _lib
+
+    L = _lib.lib()
+    out = torch.empty(8 * N, dtype=torch.float64, device="cuda")  # 64 B/sample (> L2)
+    for _ in range(args.warmup):
+        wb.run_phase(out.data_ptr(), N, stream=sptr)
+    torch.cuda.synchronize()
+    assert wb.device_status() == 0
+    ms3 = (ctypes.c_float * 3)()
+    L.aak_batch_set_profiling(wb._ctx, 1)
+    kern = np.zeros(3)
+    for _ in range(2):
+        wb.run_phase(out.data_ptr(), N, stream=sptr)
+        _lib.check(L.aak_batch_kernel_ms(wb._ctx, ms3), "kernel timing")
+        kern += np.array(ms3[:])
+    kern /= 2
+    L.aak_batch_set_profiling(wb._ctx, 0)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        wb.run_phase(out.data_ptr(), N, stream=sptr)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = reduce_max(ev0.elapsed_time(ev1)) / args.steps
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    hbm_src = "measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if hbm else "fallback 6650 GB/s"
+    hbm = hbm or 6650.0
+    bytes_per_sample = 64.0  # the eight output rows; knot windows add < 1 B/sample
+    gbs = bytes_per_sample * N / (kern[2] * 1e-3) / 1e9
+    del out
+    torch.cuda.empty_cache()
+    # end to end on the sources of the plain-path subset, pinned host rows
+    sub = sources[:: max(1, len(sources) // 16)][:16]
+    wp = E.WaveBatch(local_rank)
+    Np = int(sum(int(p["length"]) for p in sub))
+    host = torch.empty(8 * Np, dtype=torch.float64, pin_memory=True)
+    P = _lib.params_array(sub)
+    offs = np.zeros(len(sub) + 1, dtype=np.int64)
+    st = np.zeros(len(sub), dtype=np.int32)
+    times = []
+    for k in range(3):  # the first call warms the context's buffers
+        t0 = time.perf_counter()
+        _lib.check(L.aak_phase_batch_host(wp._ctx, P, len(sub), nthreads,
+                                          ctypes.cast(host.data_ptr(), ctypes.POINTER(ctypes.c_double)),
+                                          _lib.ptr(offs), _lib.ptr(st)), "aak_phase_batch_host")
+        if k > 0:
+            times.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(times))
+    h2d = int(wp.plan_bytes())
+    wp.close()
+    return {
+        "workload": "AAK phase product (GenPhase rows t, phase_r/theta/phi, omega_r/theta/phi, e; FP64) "
+                    "of the configuration-1 batch",
+        "value": N_all / (ms * 1e-3), "unit": "samples/s", "ms_per_step": ms,
+        "kernel_ms": {"clears": kern[0], "phase_and_freeze": kern[2]},
+        "roofline": {"kernel": "k_waveform<fp64, phase> + k_phase_freeze", "bound": "hbm", "achieved": gbs,
+                     "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "peak_source": hbm_src,
+                     "bytes_per_sample": bytes_per_sample},
+        "e2e": {"value": Np / e2e_s, "unit": "samples/s", "seconds_per_step": e2e_s, "sources": len(sub),
+                "samples": Np, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 64 * Np, "host_threads": nthreads},
+        "gpu_launches_per_step": 2,
+    }
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
 
@@ -425,6 +527,13 @@ def run_gpu(args, rank, world, local_rank):
     del hI2, hII2
     split = {"value": value, "kernel_ms": {"clears": kern_s[0], "waveform_split": kern_s[2]}}
 
+    # ---- AAK phase product of the same batch
+    phases = None
+    if args.phases:
+        phases = run_phases(args, wb, sources, sptr, stream, N, N_all, reduce_max, local_rank, nthreads)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            phases["cpu_baseline"] = ref_phase_rate(sources)
+
     # ---- plain FP64 per-source path on a subset of the same sources (the baseline)
     plain = None
     if args.plain_sources > 0:
@@ -555,6 +664,7 @@ def run_gpu(args, rank, world, local_rank):
         "kernel_ms": split["kernel_ms"],
         "fp64_path": fp64,
         "plain_fp64_per_source": plain,
+        "phase_product": phases,
         "roofline": roofline,
         "clocks": clk,
         "e2e": e2e,
@@ -587,6 +697,7 @@ def main():
                     help="sources of the configuration-2 accuracy check (0: skip)")
     ap.add_argument("--plain-sources", type=int, default=16,
                     help="sources of the plain FP64 per-source baseline (0: skip)")
+    ap.add_argument("--phases", type=int, default=1, help="time the AAK phase product of the batch (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,
                     help="config-3 training points of the warm-start network (0: skip)")
     args = ap.parse_args()

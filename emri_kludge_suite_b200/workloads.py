@@ -11,6 +11,7 @@
 Profiling workloads (run from the repository root on one GPU)::
 
     python -m emri_kludge_suite_b200.workloads waveform   # 16 of the 512 sources, FP64 and split, twice each
+    python -m emri_kludge_suite_b200.workloads phase      # the phase product of the same 16 sources, twice
     python -m emri_kludge_suite_b200.workloads mlp        # warm-start network: forward on 2^20 points, a training step
 """
 from __future__ import annotations
@@ -85,6 +86,26 @@ def profile_waveform():
     print("waveform workload:", n, "samples")
 
 
+def profile_phase():
+    """The phase product of the same 16 sources as the waveform workload, twice
+    (64 B/sample of outputs: 1.8 GB, above the 126 MB L2)."""
+    import torch
+
+    from .aak import WaveBatch
+
+    src, _ = config1(SEED, 512)
+    wb = WaveBatch(0)
+    wb.plan(src[::32][:16], nmodes=NMODES)
+    wb.upload()
+    n = wb.total_samples
+    out = torch.empty(8 * n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        wb.run_phase(out.data_ptr(), n)
+    torch.cuda.synchronize()
+    assert wb.device_status() == 0
+    print("phase workload:", n, "samples")
+
+
 def profile_mlp():
     import torch
 
@@ -105,4 +126,4 @@ def profile_mlp():
 
 
 if __name__ == "__main__":
-    {"waveform": profile_waveform, "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
+    {"waveform": profile_waveform, "phase": profile_phase, "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
