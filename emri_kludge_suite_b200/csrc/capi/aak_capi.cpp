@@ -1323,6 +1323,7 @@ struct aak_gpu {
   int64_t nbins = 0;  // length / 2 + 1
   int64_t row = 0;    // doubles per padded template row = 2 * nbins
   DevBuf<double> d_H[2], d_D[2], d_w[2], d_partial, d_out, d_t;
+  DevBuf<double> d_fisher;  // Fisher Gram partial sums and the 2 x nd x nd result
   cufftHandle plan = 0;
   int plan_batch = 0;
   int32_t count = 0;     // templates currently in the rows
@@ -1428,12 +1429,8 @@ int gpu_generate(aak_gpu *g, const double *x, int B, int nthreads, int32_t *stat
   return r != AAK_OK ? r : gpu_launch(g, B, with_t);
 }
 
-// FFT of the rows and the weighted inner products, queued on the legacy
-// default stream; gpu_likelihood_finish copies the results back.
-int gpu_likelihood_launch(aak_gpu *g) {
-  if (g->count <= 0) return AAK_ERR_INVALID_PARAM;
-  if (!g->ev[0])
-    for (auto &e : g->ev) cudaEventCreate(&e);
+// In-place D2Z transforms of the rows of both channels (once per generation).
+int gpu_fft_rows(aak_gpu *g) {
   if (!g->spectral) {
     if (g->plan_batch != g->count) {
       // a plan of a larger batch would transform stale rows: make one of this size
@@ -1449,6 +1446,17 @@ int gpu_likelihood_launch(aak_gpu *g) {
       return AAK_ERR_CUDA;
     g->spectral = true;
   }
+  return AAK_OK;
+}
+
+// FFT of the rows and the weighted inner products, queued on the
+// likelihood's stream; gpu_likelihood_finish copies the results back.
+int gpu_likelihood_launch(aak_gpu *g) {
+  if (g->count <= 0) return AAK_ERR_INVALID_PARAM;
+  if (!g->ev[0])
+    for (auto &e : g->ev) cudaEventCreate(&e);
+  int r0 = gpu_fft_rows(g);
+  if (r0 != AAK_OK) return r0;
   cudaEventRecord(g->ev[2], g->stream);
   InnerProductArgs a;
   a.H[0] = g->d_H[0].ptr;
@@ -1483,6 +1491,47 @@ int gpu_likelihood_finish(aak_gpu *g, double *out) {
 int gpu_likelihood(aak_gpu *g, double *out) {
   const int r = gpu_likelihood_launch(g);
   return r != AAK_OK ? r : gpu_likelihood_finish(g, out);
+}
+
+// Fisher matrix of one point (pygpuAAK/pygpuAAK.py:269-300): the 2 nd
+// finite-difference templates are planned and generated as one batch into
+// the rows, transformed, and reduced on the device to the per-channel Gram
+// matrices of the weighted differences; only 2 nd^2 doubles come back.
+int gpu_fisher(aak_gpu *g, const double *x, int nd, double scale, int nthreads, double *gram, int32_t *status) {
+  if (nd < 1 || nd > kFisherMaxDim || !x || !gram || !std::isfinite(scale)) return AAK_ERR_INVALID_PARAM;
+  if (!g->d_w[0].ptr || !g->d_w[1].ptr) return AAK_ERR_INVALID_PARAM;  // input_data first: the weights
+  const int B = 2 * nd;
+  int r = gpu_generate(g, x, B, nthreads, status, false);
+  if (r != AAK_OK) return r;
+  if ((r = gpu_fft_rows(g)) != AAK_OK) return r;
+  const int grid = fisher_grid(g->ctx->num_sms, g->nbins);
+  const int64_t need = fisher_partial_doubles(nd, grid) + 2 * (int64_t)nd * nd;
+  if ((r = g->d_fisher.reserve((size_t)need)) != AAK_OK) return r;
+  cudaEventRecord(g->ev[2], g->stream);
+  FisherArgs a;
+  a.H[0] = g->d_H[0].ptr;
+  a.H[1] = g->d_H[1].ptr;
+  a.row_doubles = g->row;
+  a.w[0] = g->d_w[0].ptr;
+  a.w[1] = g->d_w[1].ptr;
+  a.nbins = g->nbins;
+  a.nd = nd;
+  a.scale = scale;
+  a.partial = g->d_fisher.ptr;
+  a.out = g->d_fisher.ptr + fisher_partial_doubles(nd, grid);
+  launch_fisher_gram(a, g->ctx->num_sms, g->stream);
+  cudaEventRecord(g->ev[3], g->stream);
+  if ((r = cuda_ok(cudaGetLastError())) != AAK_OK) return r;
+  if ((r = cuda_ok(cudaMemcpyAsync(gram, a.out, 2 * (size_t)nd * nd * sizeof(double), cudaMemcpyDeviceToHost,
+                                   g->stream))) != AAK_OK)
+    return r;
+  if ((r = cuda_ok(cudaStreamSynchronize(g->stream))) != AAK_OK) return r;
+  float f;
+  if (cudaEventElapsedTime(&f, g->ev[0], g->ev[1]) == cudaSuccess) g->ms[1] = f;
+  if (cudaEventElapsedTime(&f, g->ev[1], g->ev[2]) == cudaSuccess) g->ms[2] = f;
+  if (cudaEventElapsedTime(&f, g->ev[2], g->ev[3]) == cudaSuccess) g->ms[3] = f;
+  cudaGetLastError();
+  return device_status(g->ctx);
 }
 
 }  // namespace
@@ -1629,6 +1678,13 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   }
   for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
   return AAK_OK;
+}
+
+int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, int32_t nthreads, double *gram,
+                   int32_t *status) {
+  if (!g) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(g->ctx->mu);
+  return gpu_fisher(g, params, nd, scale, nthreads, gram, status);
 }
 
 int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m) {

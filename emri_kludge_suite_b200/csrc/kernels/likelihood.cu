@@ -11,6 +11,8 @@
 // across templates; the template spectra stream from HBM once.
 #include "likelihood.cuh"
 
+#include <algorithm>
+
 namespace aak {
 namespace {
 
@@ -67,7 +69,92 @@ __global__ void k_inner_final(const double *partial, int nblocks, int ntemplates
   out[2 * k + 1] = 4.0 * a1;
 }
 
+// Each CTA stages the weighted differences of kFisherBins bins of every
+// derivative and both channels in shared memory (bins major, the derivative
+// index padded to kFisherMaxDim + 1 so that the staging stores spread over
+// the banks), then each thread adds the products of its one or two (channel,
+// i <= j) pairs over the staged bins.  Each template row streams from HBM once.
+__global__ void __launch_bounds__(kFisherThreads) k_fisher_partial(FisherArgs a) {
+  __shared__ double2 sD[2][kFisherBins][kFisherMaxDim + 1];
+  const int nd = a.nd, tid = threadIdx.x;
+  const int npair = nd * (nd + 1) / 2, ncombo = 2 * npair;
+  int cc[2] = {0, 0}, ii[2] = {0, 0}, jj[2] = {0, 0};
+  double acc[2] = {0.0, 0.0};
+  int mine = 0;
+  for (int q = tid; q < ncombo && mine < 2; q += kFisherThreads, ++mine) {
+    const int c = q / npair;
+    int r = q - c * npair, i = 0;
+    while (r >= nd - i) {  // row-major upper triangle: row i holds nd - i pairs
+      r -= nd - i;
+      ++i;
+    }
+    cc[mine] = c;
+    ii[mine] = i;
+    jj[mine] = i + r;
+  }
+  const int64_t nchunks = (a.nbins + kFisherBins - 1) / kFisherBins;
+  for (int64_t ck = blockIdx.x; ck < nchunks; ck += gridDim.x) {
+    const int64_t b0 = ck * kFisherBins;
+    __syncthreads();  // the previous chunk's products are done
+    for (int idx = tid; idx < 2 * nd * kFisherBins; idx += kFisherThreads) {
+      const int b = idx % kFisherBins, rest = idx / kFisherBins;
+      const int i = rest % nd, c = rest / nd;
+      const int64_t bin = b0 + b;
+      double2 d = make_double2(0.0, 0.0);
+      if (bin < a.nbins) {
+        const double2 *Hu = reinterpret_cast<const double2 *>(a.H[c] + (int64_t)(2 * i + 1) * a.row_doubles);
+        const double2 *Hd = reinterpret_cast<const double2 *>(a.H[c] + (int64_t)(2 * i) * a.row_doubles);
+        const double2 u = Hu[bin], v = Hd[bin];
+        const double wv = __ldg(&a.w[c][bin]) * a.scale;
+        d = make_double2(wv * (u.x - v.x), wv * (u.y - v.y));
+      }
+      sD[c][b][i] = d;
+    }
+    __syncthreads();
+    for (int m = 0; m < mine; ++m) {
+      const int c = cc[m], i = ii[m], j = jj[m];
+      double s = acc[m];
+#pragma unroll 8
+      for (int b = 0; b < kFisherBins; ++b) {
+        const double2 x = sD[c][b][i], y = sD[c][b][j];
+        s = fma(x.x, y.x, fma(x.y, y.y, s));
+      }
+      acc[m] = s;
+    }
+  }
+  for (int m = 0; m < mine; ++m) a.partial[(int64_t)blockIdx.x * ncombo + tid + m * kFisherThreads] = acc[m];
+}
+
+__global__ void k_fisher_final(FisherArgs a, int nblocks) {
+  const int nd = a.nd, npair = nd * (nd + 1) / 2, ncombo = 2 * npair;
+  for (int q = threadIdx.x; q < ncombo; q += blockDim.x) {
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += a.partial[(int64_t)b * ncombo + q];
+    const int c = q / npair;
+    int r = q - c * npair, i = 0;
+    while (r >= nd - i) {
+      r -= nd - i;
+      ++i;
+    }
+    const int j = i + r;
+    a.out[(c * nd + i) * nd + j] = 4.0 * s;
+    a.out[(c * nd + j) * nd + i] = 4.0 * s;
+  }
+}
+
 }  // namespace
+
+int fisher_grid(int num_sms, int64_t nbins) {
+  const int64_t nchunks = (nbins + kFisherBins - 1) / kFisherBins;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(nchunks, (int64_t)num_sms * 4));
+}
+
+void launch_fisher_gram(const FisherArgs &a, int num_sms, cudaStream_t stream) {
+  if (a.nd <= 0 || a.nd > kFisherMaxDim) return;
+  const int grid = fisher_grid(num_sms, a.nbins);
+  k_fisher_partial<<<grid, kFisherThreads, 0, stream>>>(a);
+  k_fisher_final<<<1, kFisherThreads, 0, stream>>>(a, grid);
+}
 
 void launch_inner_products(const InnerProductArgs &a, cudaStream_t stream) {
   if (a.ntemplates <= 0) return;

@@ -28,4 +28,27 @@ constexpr int kIpBlocksPerTemplate = 64;
 
 void launch_inner_products(const InnerProductArgs &a, cudaStream_t stream);
 
+// Fisher-matrix Gram sums of finite-difference template spectra
+// (pygpuAAK/pygpuAAK.py:269-300): rows 2i and 2i+1 of each channel hold the
+// two evaluations of derivative i, D_i = scale w (H[2i+1] - H[2i]), and
+// out[c][i][j] = 4 Re sum_f conj(D_i) D_j over the nbins bins, for both
+// channels c (2 x nd x nd, symmetric).  Partial sums per CTA, then a fixed-
+// order reduction (deterministic, no atomics).
+constexpr int kFisherMaxDim = 16;
+constexpr int kFisherBins = 64;     // bins staged per chunk
+constexpr int kFisherThreads = 256;
+struct FisherArgs {
+  const double *H[2];
+  int64_t row_doubles;
+  const double *w[2];
+  int64_t nbins;
+  int32_t nd;
+  double scale;        // applied to each difference
+  double *partial;     // fisher_partial_doubles(nd, num_sms) scratch
+  double *out;         // 2 x nd x nd
+};
+int fisher_grid(int num_sms, int64_t nbins);
+inline int64_t fisher_partial_doubles(int nd, int grid) { return (int64_t)grid * nd * (nd + 1); }
+void launch_fisher_gram(const FisherArgs &a, int num_sms, cudaStream_t stream);
+
 }  // namespace aak

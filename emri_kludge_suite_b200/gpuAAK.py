@@ -34,6 +34,7 @@ def _bind():
     L.aak_gpu_likelihood_batch.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp, _i32p]
     L.aak_gpu_last_timing.argtypes = [v, _dp]
     L.aak_gpu_set_precision.argtypes = [v, ctypes.c_int32]
+    L.aak_gpu_fisher.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _dp, _i32p]
     L._gpu_bound = True
     return L
 
@@ -111,6 +112,25 @@ class GPUAAK:
               "likelihood_batch")
         self._spectral = False
         return (out, st) if return_status else out
+
+    def fisher_gram(self, params, scale, nthreads=0, return_status=False):
+        """Per-channel Gram matrices of finite-difference template spectra.
+
+        params: (2 nd, 14) in gpu_gen_AAK order, rows 2i and 2i+1 the two
+        evaluations of derivative i (nd <= 16).  The 2 nd templates are generated
+        as one batch, transformed and reduced on the device; returns G of shape
+        (2, nd, nd) with G[c, i, j] = 4 Re sum_f conj(D_i) D_j,
+        D_i = scale * w_c * (FFT h_{2i+1} - FFT h_{2i}), w_c the input_data weights.
+        """
+        x = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+        if x.shape[1] != 14 or x.shape[0] % 2:
+            raise ValueError("params must be (2 nd, 14) in gpu_gen_AAK order")
+        nd = x.shape[0] // 2
+        G = np.zeros((2, nd, nd))
+        st = np.zeros(2 * nd, dtype=np.int32)
+        check(lib().aak_gpu_fisher(self._g, ptr(x), nd, float(scale), int(nthreads), ptr(G), ptr(st)), "fisher")
+        self._spectral = True
+        return (G, st) if return_status else G
 
     def set_precision(self, precision: int):
         """0: FP64 throughout (default); 1: split precision."""

@@ -99,21 +99,34 @@ class pyGPUAAK:
         x_in = self.converter.convert(x.copy())
         return self.NLL(*x_in, **kwargs)
 
-    def get_Fisher(self, x):
-        Mij = np.zeros((self.ndim, self.ndim), dtype=x.dtype)
+    def _physical(self, x):
+        """Sampler coordinates (ndim, n) -> (n, 14) gpu_gen_AAK parameters, as getNLL converts them."""
+        x = self.converter.recycle(x)
+        cols = [np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in self.converter.convert(x.copy())]
+        n = max(len(c) for c in cols)
+        return np.stack([np.broadcast_to(c, (n,)) for c in cols], axis=1)
+
+    def get_Fisher(self, x, form="reference"):
+        """Fisher matrix at x by central differences of step eps in each sampler
+        coordinate (pygpuAAK/pygpuAAK.py:269-300).  The 2 ndim templates are
+        generated as one batch and their weighted spectra reduced on the device
+        (GPUAAK.fisher_gram); only the Gram matrices come back to the host.
+
+        form="reference" reproduces the published formula, which pairs the
+        channel-I derivative j with itself: M_ij = 4 Re(<d_j h_I, d_j h_I> +
+        <d_i h_II, d_j h_II>) for i <= j, mirrored.  form="full" is the
+        two-channel Fisher matrix 4 Re(<d_i h_I, d_j h_I> + <d_i h_II, d_j h_II>).
+        """
         x_in = np.tile(x, (2 * self.ndim, 1))
         for i in range(self.ndim):
             x_in[2 * i, i] += self.eps
             x_in[2 * i + 1, i] -= self.eps
-        hI, hII = self.getNLL(x_in.T, return_TDI=True)
-        for i in range(self.ndim):
-            hi_hI = (hI[2 * i + 1] - hI[2 * i]) / (2 * self.eps)
-            hi_hII = (hII[2 * i + 1] - hII[2 * i]) / (2 * self.eps)
-            for j in range(i, self.ndim):
-                hj_hI = (hI[2 * j + 1] - hI[2 * j]) / (2 * self.eps)
-                hj_hII = (hII[2 * j + 1] - hII[2 * j]) / (2 * self.eps)
-                # the reference pairs hj_hI with itself here (pygpuAAK.py:293-295); kept as published
-                inner = 4 * np.real(np.dot(hj_hI.conj(), hj_hI) + np.dot(hi_hII.conj(), hj_hII))
-                Mij[i][j] = inner
-                Mij[j][i] = inner
-        return Mij
+        G = self.generator.fisher_gram(self._physical(x_in.T), 1.0 / (2 * self.eps))
+        if form == "reference":
+            A = G[0].diagonal()[None, :] + G[1]
+            M = np.triu(A) + np.triu(A, 1).T
+        elif form == "full":
+            M = G[0] + G[1]
+        else:
+            raise ValueError("form must be 'reference' or 'full'")
+        return M.astype(x.dtype)

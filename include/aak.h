@@ -293,6 +293,17 @@ int aak_gpu_likelihood(aak_gpu *g, double *out2);
 int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int32_t max_batch, int32_t nthreads,
                              double *out, int32_t *status);
 
+/* Fisher-matrix Gram sums of one point (replaces the template loop and host
+ * dot products of pyGPUAAK.get_Fisher, pygpuAAK/pygpuAAK.py:269-300):
+ * params holds 2 nd rows x 14 (gpu_gen_AAK order, 1 <= nd <= 16), rows 2i
+ * and 2i + 1 the two evaluations of derivative i.  The 2 nd templates are
+ * generated as one batch, transformed, weighted by the input_data weights w,
+ * and reduced on the device: D_i = scale w (FFT h_{2i+1} - FFT h_{2i}),
+ * gram[c nd^2 + i nd + j] = 4 Re sum_f conj(D_i) D_j for channels c = I, II
+ * (2 x nd x nd, symmetric).  status (optional, 2 nd) per template. */
+int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, int32_t nthreads, double *gram,
+                   int32_t *status);
+
 /* Template precision: 0 = FP64 throughout (default), 1 = split (FP64 phases
  * and angle reductions, FP32 geometry, response, Bessel evaluation). */
 int aak_gpu_set_precision(aak_gpu *g, int32_t precision);

@@ -415,3 +415,29 @@ def inner_products(hI, hII, data1, data2, w1, w2):
     d_h = np.real(np.vdot(HI, data1)) + np.real(np.vdot(HII, data2))
     h_h = np.real(np.vdot(HI, HI)) + np.real(np.vdot(HII, HII))
     return np.array([4.0 * d_h, 4.0 * h_h])
+
+
+def fisher_gram(hI_rows: np.ndarray, hII_rows: np.ndarray, scale: float) -> np.ndarray:
+    """Per-channel Gram matrices of the finite-difference derivatives of
+    weighted template spectra, as pyGPUAAK.get_Fisher forms them
+    (pygpuAAK/pygpuAAK.py:269-300): rows 2i and 2i+1 are the two evaluations of
+    derivative i, D_i = scale (row_{2i+1} - row_{2i}), G[c, i, j] = 4 Re
+    sum_f conj(D_i) D_j.  Returns (2, nd, nd)."""
+    nd = hI_rows.shape[0] // 2
+    G = np.zeros((2, nd, nd))
+    for c, H in enumerate((hI_rows, hII_rows)):
+        D = (H[1::2] - H[0::2]) * scale
+        G[c] = 4.0 * np.real(D.conj() @ D.T)
+    return G
+
+
+def fisher_reference_form(G: np.ndarray) -> np.ndarray:
+    """The matrix the reference's get_Fisher returns from those Gram sums
+    (pygpuAAK/pygpuAAK.py:286-298): for i <= j, M_ij = 4 Re(<D_j^I, D_j^I> +
+    <D_i^II, D_j^II>), mirrored to j < i."""
+    nd = G.shape[1]
+    M = np.zeros((nd, nd))
+    for i in range(nd):
+        for j in range(i, nd):
+            M[i, j] = M[j, i] = G[0, j, j] + G[1, i, j]
+    return M

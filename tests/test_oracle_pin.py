@@ -116,3 +116,27 @@ def test_oracle_kerr_stability_matches_reference(ref_available):
             np.testing.assert_allclose(ours[:3], ref[:3], rtol=1e-12, atol=1e-14)
         if ref[3] in (-1, 0, 1):
             assert ours[3] == ref[3]
+
+
+def test_fisher_oracle_forms_against_pairwise_sums():
+    """The vectorised Fisher oracle against pair-by-pair sums over bins, in the
+    reference's pairing (pygpuAAK/pygpuAAK.py:286-298) and the full one."""
+    rng = np.random.default_rng(9)
+    nd, nb = 5, 257
+    hI = rng.standard_normal((2 * nd, nb)) + 1j * rng.standard_normal((2 * nd, nb))
+    hII = rng.standard_normal((2 * nd, nb)) + 1j * rng.standard_normal((2 * nd, nb))
+    eps = 1e-3
+    G = O.fisher_gram(hI, hII, 1.0 / (2 * eps))
+    M = O.fisher_reference_form(G)
+    for i in range(nd):
+        di = [(h[2 * i + 1] - h[2 * i]) / (2 * eps) for h in (hI, hII)]
+        for j in range(nd):
+            dj = [(h[2 * j + 1] - h[2 * j]) / (2 * eps) for h in (hI, hII)]
+            for c in range(2):
+                want = 4 * np.real(np.sum(np.conj(di[c]) * dj[c]))
+                assert abs(G[c, i, j] - want) <= 1e-12 * abs(want) + 1e-9
+            a, b = min(i, j), max(i, j)
+            da = [(h[2 * a + 1] - h[2 * a]) / (2 * eps) for h in (hI, hII)]
+            db = [(h[2 * b + 1] - h[2 * b]) / (2 * eps) for h in (hI, hII)]
+            want = 4 * np.real(np.sum(np.conj(db[0]) * db[0]) + np.sum(np.conj(da[1]) * db[1]))
+            assert abs(M[i, j] - want) <= 1e-12 * abs(want)
