@@ -228,7 +228,72 @@ def run_parmap_warm_start(n_train: int, local_rank: int):
     return rep, m
 
 
-def run_likelihood(n_templates: int, local_rank: int, model=None) -> dict:
+def run_fisher(g, n_points: int) -> dict:
+    """Fisher matrices (14 x 14, 28 templates each) at config-4 points, one
+    batched call per point: host planning + waveforms + FFT + device Gram."""
+    P = config4_templates(n_points, seed=SEED + 41)
+    step = 1e-6 * np.maximum(np.abs(FIDUCIAL), 1.0)
+    rows = []
+    for x in P:
+        X = np.tile(x, (28, 1))
+        for i in range(14):
+            X[2 * i, i] += step[i]
+            X[2 * i + 1, i] -= step[i]
+        rows.append(X)
+    g.fisher_gram(rows[0], 1.0)  # warm-up (rows, FFT plan, scratch)
+    ms_sum = np.zeros(4)
+    t0 = time.perf_counter()
+    for X in rows:
+        G, st = g.fisher_gram(X, 1.0, return_status=True)
+        if np.any(st != 0):
+            raise RuntimeError("a Fisher template failed")
+        m = g.last_timing_ms()
+        ms_sum += np.array([m["host_plan"], m["waveform"], m["fft"], m["reduce"]])
+    wall = time.perf_counter() - t0
+    ms = ms_sum / n_points
+    nbins = LIKE_LENGTH // 2 + 1
+    gram_bytes = 2 * 28 * nbins * 16.0  # each template spectrum read once, both channels
+    gbs = gram_bytes / (ms[3] * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    return {"workload": "config4 points, 14 parameters, central differences (28 templates of 3.2e6 samples per "
+                        "matrix), reference harmonic rule, FP64",
+            "points": n_points, "fisher_per_s": n_points / wall, "fisher_per_s_gpu": 1e3 / float(ms[1:].sum()),
+            "ms_per_matrix": dict(zip(("host_plan", "waveform", "fft", "gram"), ms.tolist())),
+            "gram_roofline": {"kernel": "k_fisher_partial + k_fisher_final", "bound": "hbm", "achieved": gbs,
+                              "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                              "bytes": gram_bytes, "peak_source": "measured copy bandwidth (MEASURED_PEAKS.json)"
+                              if peaks.get("hbm_gbs") else "fallback"},
+            "gpu_launches_per_matrix": 4,  # k_spline_coeffs, k_waveform, k_fisher_partial, k_fisher_final (+ cuFFT)
+            "cpu_baseline": ref_fisher_seconds()}
+
+
+def ref_fisher_seconds(sample_len: int = 200000) -> dict:
+    """The reference's CPU cost of one such Fisher matrix: its own AAKwave on the
+    fiducial config-4 source truncated to sample_len samples (one process),
+    scaled to 28 templates of 3.2e6 samples.  The reference's get_Fisher adds an
+    FFT and host dot products per template on top."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return {"value": None, "sample": "unavailable: oracle/_ref/libaakref.so is not built"}
+    iota, s_, p, e, M, mu, gamma, psi, alph, thS, phS, thK, phK, D = FIDUCIAL
+    pars = dict(backint=False, LISA=True, length=sample_len, dt=DT, p=p, T=sample_len * DT / YEAR, f=0.0, T_fit=1.0,
+                mu=mu, M=M, s=s_, e=e, iota=iota, gamma=gamma, psi=psi, theta_S=thS, phi_S=phS, theta_K=thK,
+                phi_K=phK, alpha=alph, D=D)
+    t0 = time.perf_counter()
+    O.ref_aakwave(pars)
+    rate = sample_len / (time.perf_counter() - t0)
+    return {"value": 28 * LIKE_LENGTH / rate, "unit": "s per Fisher matrix (waveforms only)", "cores": 1,
+            "kind": "reference", "sample": f"reference AAKwave, fiducial config-4 source, {sample_len} samples, "
+                                          f"{rate:.3g} samples/s, scaled to 28 x {LIKE_LENGTH} samples"}
+
+
+def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int = 0) -> dict:
     """likelihoods/s of the batched path: host planning + waveforms + FFT + reduction, end to end per call."""
     from emri_kludge_suite_b200.gpuAAK import GPUAAK
     from emri_kludge_suite_b200.LISAnoise import LISA_Noise, generate_noise_frequencies, generate_noise_single_channel
@@ -270,6 +335,8 @@ def run_likelihood(n_templates: int, local_rank: int, model=None) -> dict:
     res = {"workload": "config4: fiducial config-0 source, 3.2e6 samples (1.014 yr, dt=10 s), LISA-coloured noise, "
                        "templates perturbed 1e-5 rel (M, mu, p0) / 1e-3 rad (angles), reference harmonic rule",
            "templates": n_templates, "samples_per_template": LIKE_LENGTH, "fp64_plain": plain}
+    if n_fisher > 0:
+        res["fisher"] = run_fisher(g, n_fisher)
     res.update({k: plain[k] for k in ("likelihoods_per_s", "likelihoods_per_s_gpu", "failed", "ms")})
     # split precision + learned warm start vs the plain FP64 path
     g.set_precision(1)
@@ -678,7 +745,7 @@ def run_gpu(args, rank, world, local_rank):
         del hI, hII, hIh, hIIh
         wb.close()
         torch.cuda.empty_cache()
-        out["likelihood"] = run_likelihood(args.likelihood, local_rank, model)
+        out["likelihood"] = run_likelihood(args.likelihood, local_rank, model, args.fisher)
     return out
 
 
@@ -697,6 +764,7 @@ def main():
                     help="sources of the configuration-2 accuracy check (0: skip)")
     ap.add_argument("--plain-sources", type=int, default=16,
                     help="sources of the plain FP64 per-source baseline (0: skip)")
+    ap.add_argument("--fisher", type=int, default=8, help="Fisher matrices to time at config-4 points (0: skip)")
     ap.add_argument("--phases", type=int, default=1, help="time the AAK phase product of the batch (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,
                     help="config-3 training points of the warm-start network (0: skip)")

@@ -80,38 +80,46 @@ __global__ void __launch_bounds__(kFisherThreads) k_fisher_partial(FisherArgs a)
   const int npair = nd * (nd + 1) / 2, ncombo = 2 * npair;
   int cc[2] = {0, 0}, ii[2] = {0, 0}, jj[2] = {0, 0};
   double acc[2] = {0.0, 0.0};
-  int mine = 0;
-  for (int q = tid; q < ncombo && mine < 2; q += kFisherThreads, ++mine) {
+  bool has[2];
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {  // this thread's pairs q = tid, tid + kFisherThreads
+    const int q = tid + m * kFisherThreads;
+    has[m] = q < ncombo;
+    if (!has[m]) continue;
     const int c = q / npair;
     int r = q - c * npair, i = 0;
     while (r >= nd - i) {  // row-major upper triangle: row i holds nd - i pairs
       r -= nd - i;
       ++i;
     }
-    cc[mine] = c;
-    ii[mine] = i;
-    jj[mine] = i + r;
+    cc[m] = c;
+    ii[m] = i;
+    jj[m] = i + r;
   }
   const int64_t nchunks = (a.nbins + kFisherBins - 1) / kFisherBins;
   for (int64_t ck = blockIdx.x; ck < nchunks; ck += gridDim.x) {
     const int64_t b0 = ck * kFisherBins;
     __syncthreads();  // the previous chunk's products are done
+#pragma unroll 4
     for (int idx = tid; idx < 2 * nd * kFisherBins; idx += kFisherThreads) {
       const int b = idx % kFisherBins, rest = idx / kFisherBins;
       const int i = rest % nd, c = rest / nd;
       const int64_t bin = b0 + b;
       double2 d = make_double2(0.0, 0.0);
       if (bin < a.nbins) {
-        const double2 *Hu = reinterpret_cast<const double2 *>(a.H[c] + (int64_t)(2 * i + 1) * a.row_doubles);
-        const double2 *Hd = reinterpret_cast<const double2 *>(a.H[c] + (int64_t)(2 * i) * a.row_doubles);
+        const double *Hc = c ? a.H[1] : a.H[0];  // selected, not indexed: the arguments stay in registers
+        const double2 *Hu = reinterpret_cast<const double2 *>(Hc + (int64_t)(2 * i + 1) * a.row_doubles);
+        const double2 *Hd = reinterpret_cast<const double2 *>(Hc + (int64_t)(2 * i) * a.row_doubles);
         const double2 u = Hu[bin], v = Hd[bin];
-        const double wv = __ldg(&a.w[c][bin]) * a.scale;
+        const double wv = __ldg((c ? a.w[1] : a.w[0]) + bin) * a.scale;
         d = make_double2(wv * (u.x - v.x), wv * (u.y - v.y));
       }
       sD[c][b][i] = d;
     }
     __syncthreads();
-    for (int m = 0; m < mine; ++m) {
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      if (!has[m]) continue;
       const int c = cc[m], i = ii[m], j = jj[m];
       double s = acc[m];
 #pragma unroll 8
@@ -122,24 +130,31 @@ __global__ void __launch_bounds__(kFisherThreads) k_fisher_partial(FisherArgs a)
       acc[m] = s;
     }
   }
-  for (int m = 0; m < mine; ++m) a.partial[(int64_t)blockIdx.x * ncombo + tid + m * kFisherThreads] = acc[m];
+#pragma unroll
+  for (int m = 0; m < 2; ++m)
+    if (has[m]) a.partial[(int64_t)blockIdx.x * ncombo + tid + m * kFisherThreads] = acc[m];
 }
 
-__global__ void k_fisher_final(FisherArgs a, int nblocks) {
+// One warp per (channel, i <= j) pair: lane l adds the partials of CTAs
+// l, l + 32, ... in order, then a fixed shuffle tree (deterministic).
+__global__ void __launch_bounds__(kFisherThreads) k_fisher_final(FisherArgs a, int nblocks) {
   const int nd = a.nd, npair = nd * (nd + 1) / 2, ncombo = 2 * npair;
-  for (int q = threadIdx.x; q < ncombo; q += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += a.partial[(int64_t)b * ncombo + q];
-    const int c = q / npair;
-    int r = q - c * npair, i = 0;
-    while (r >= nd - i) {
-      r -= nd - i;
-      ++i;
-    }
-    const int j = i + r;
-    a.out[(c * nd + i) * nd + j] = 4.0 * s;
-    a.out[(c * nd + j) * nd + i] = 4.0 * s;
+  const int q = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (q >= ncombo) return;
+  double s = 0.0;
+  for (int b = lane; b < nblocks; b += 32) s += a.partial[(int64_t)b * ncombo + q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane != 0) return;
+  const int c = q / npair;
+  int r = q - c * npair, i = 0;
+  while (r >= nd - i) {
+    r -= nd - i;
+    ++i;
   }
+  const int j = i + r;
+  a.out[(c * nd + i) * nd + j] = 4.0 * s;
+  a.out[(c * nd + j) * nd + i] = 4.0 * s;
 }
 
 }  // namespace
@@ -153,7 +168,8 @@ void launch_fisher_gram(const FisherArgs &a, int num_sms, cudaStream_t stream) {
   if (a.nd <= 0 || a.nd > kFisherMaxDim) return;
   const int grid = fisher_grid(num_sms, a.nbins);
   k_fisher_partial<<<grid, kFisherThreads, 0, stream>>>(a);
-  k_fisher_final<<<1, kFisherThreads, 0, stream>>>(a, grid);
+  const int ncombo = a.nd * (a.nd + 1), warps = kFisherThreads / 32;
+  k_fisher_final<<<(ncombo + warps - 1) / warps, kFisherThreads, 0, stream>>>(a, grid);
 }
 
 void launch_inner_products(const InnerProductArgs &a, cudaStream_t stream) {

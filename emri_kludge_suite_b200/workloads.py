@@ -12,6 +12,7 @@ Profiling workloads (run from the repository root on one GPU)::
 
     python -m emri_kludge_suite_b200.workloads waveform   # 16 of the 512 sources, FP64 and split, twice each
     python -m emri_kludge_suite_b200.workloads phase      # the phase product of the same 16 sources, twice
+    python -m emri_kludge_suite_b200.workloads fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
     python -m emri_kludge_suite_b200.workloads mlp        # warm-start network: forward on 2^20 points, a training step
 """
 from __future__ import annotations
@@ -106,6 +107,24 @@ def profile_phase():
     print("phase workload:", n, "samples")
 
 
+def profile_fisher():
+    """Two Fisher-matrix calls at the configuration-4 fiducial point: 28
+    templates of 3.2e6 samples (1.43 GB of spectra, above the 126 MB L2)."""
+    from .gpuAAK import GPUAAK
+
+    length, dt = 3_200_000, 10.0
+    x0 = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])
+    g = GPUAAK(1.0, 100, length, 100.0, dt, True, False)
+    X = np.tile(x0, (28, 1))
+    for i in range(14):
+        X[2 * i, i] += 1e-6 * max(abs(x0[i]), 1.0)
+        X[2 * i + 1, i] -= 1e-6 * max(abs(x0[i]), 1.0)
+    for _ in range(2):
+        G, st = g.fisher_gram(X, 1.0, return_status=True)
+        assert np.all(st == 0) and np.all(np.isfinite(G))
+    print("fisher workload: 28 x", length, "samples")
+
+
 def profile_mlp():
     import torch
 
@@ -126,4 +145,5 @@ def profile_mlp():
 
 
 if __name__ == "__main__":
-    {"waveform": profile_waveform, "phase": profile_phase, "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
+    {"waveform": profile_waveform, "phase": profile_phase, "fisher": profile_fisher,
+     "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
