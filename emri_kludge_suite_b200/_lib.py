@@ -117,6 +117,8 @@ def lib():
     L.aak_parmap.argtypes = [_dp, _d, _d, _d, _d, _d, _dp, _dp, _i32p]
     L.aak_wave.argtypes = [ctypes.POINTER(AAKParams), _dp, _dp, _dp, _dp]
     L.aak_phase.argtypes = [ctypes.POINTER(AAKParams)] + [_dp] * 9
+    L.aak_tdi.argtypes = [ctypes.POINTER(AAKParams)] + [_dp] * 8
+    L.aak_tdi_batch_host.argtypes = [_vp, ctypes.POINTER(AAKParams), _i32, _i32, _dp, _i64p, _i32p]
     L.aak_batch_run_phase.argtypes = [_vp, _vp, _i64, _vp]
     L.aak_phase_batch_host.argtypes = [_vp, ctypes.POINTER(AAKParams), _i32, _i32, _dp, _i64p, _i32p]
     L.aak_genwave.argtypes = [_dp, _dp, _dp, _d, _i32, _dp, _dp, _d, _dp, _d, _d, _dp, _d, _d, _d, _d, _d, _d, _d,

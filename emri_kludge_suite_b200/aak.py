@@ -2,6 +2,8 @@
 
 * :func:`wave` -- the call shape of the reference ``AAKwrapper.wave(pars)``
   (AAKwrapper/AAKwrapper.pyx:50-88): returns ``(t, hI, hII, timing)``.
+* :func:`tdi` -- ``AAKwrapper.tdi(pars)`` (AAKwrapper/AAKwrapper.pyx:135-177):
+  returns ``(f, Xf_r, Xf_im, Yf_r, Yf_im, Zf_r, Zf_im, timing)``.
 * :func:`phase` -- ``AAKwrapper.phase(pars)`` (AAKwrapper/AAKwrapper.pyx:90-133):
   returns ``(t, phase_r, phase_theta, phase_phi, omega_r, omega_theta,
   omega_phi, eccentricity, timing)``.
@@ -22,7 +24,7 @@ import numpy as np
 from . import _lib
 from ._lib import AAKMapped, AAKValueError, check, lib, make_params, params_array, ptr
 
-__all__ = ["wave", "phase", "PHASE_ROWS", "front_end", "genwave", "Mapped", "WaveBatch", "AAKValueError"]
+__all__ = ["wave", "phase", "tdi", "PHASE_ROWS", "TDI_ROWS", "front_end", "genwave", "Mapped", "WaveBatch", "AAKValueError"]
 
 
 @dataclass
@@ -98,6 +100,23 @@ def phase(pars: dict):
     secs = ctypes.c_double(0.0)
     check(lib().aak_phase(ctypes.byref(make_params(pars)), *[ptr(a) for a in rows], ctypes.byref(secs)), "aak_phase")
     return (*rows, secs.value)
+
+
+#: rows of the frequency-domain TDI, in the order of AAKwrapper.tdi (after f)
+TDI_ROWS = ("Xf_r", "Xf_im", "Yf_r", "Yf_im", "Zf_r", "Zf_im")
+
+
+def tdi(pars: dict):
+    """AAKwrapper.tdi: ``(f, Xf_r, Xf_im, Yf_r, Yf_im, Zf_r, Zf_im, timing)`` on the
+    (length + 1) // 2 bins f = i / ((length - 1) dt) (GenTDI,
+    src/suite/AAKTDI.cc:799-829, on the GPU in FP64)."""
+    n = (int(pars["length"]) + 1) // 2
+    f = np.zeros(n)
+    rows = [np.zeros(n) for _ in TDI_ROWS]
+    secs = ctypes.c_double(0.0)
+    check(lib().aak_tdi(ctypes.byref(make_params(pars)), ptr(f), *[ptr(a) for a in rows], ctypes.byref(secs)),
+          "aak_tdi")
+    return (f, *rows, secs.value)
 
 
 def genwave(pars: dict, mapped: Mapped, nmodes: int = 0):
@@ -231,6 +250,20 @@ class WaveBatch:
         check(lib().aak_phase_batch_host(self._ctx, P, self.nsrc, int(nthreads), ptr(rows), ptr(offs), ptr(st)),
               "aak_phase_batch_host")
         self._info()
+        return rows, offs, st
+
+    def tdi_host(self, params, nthreads: int = 0):
+        """Frequency-domain TDI of every source (as :func:`tdi`) in one batch.
+        Returns (rows, bin_offsets, status): rows (6, total bins) in
+        :data:`TDI_ROWS` order, source s at bins bin_offsets[s]:bin_offsets[s + 1]."""
+        self.nsrc = len(params)
+        P = params_array(params)
+        nb = int(sum((int(p["length"] if isinstance(p, dict) else p.length) + 1) // 2 for p in params))
+        rows = np.zeros((6, nb))
+        offs = np.zeros(self.nsrc + 1, dtype=np.int64)
+        st = np.zeros(self.nsrc, dtype=np.int32)
+        check(lib().aak_tdi_batch_host(self._ctx, P, self.nsrc, int(nthreads), ptr(rows), ptr(offs), ptr(st)),
+              "aak_tdi_batch_host")
         return rows, offs, st
 
     def launches(self) -> int:

@@ -93,6 +93,8 @@ struct aak_ctx {
   DevBuf<int32_t> d_flag;                 // look-back flags, one per tile
   DevBuf<unsigned long long> d_counter;   // [0] work-queue head, [1] device status word
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
+  DevBuf<TdiDesc> d_tdi;        // frequency-domain TDI: per-source stationary-phase records
+  DevBuf<int64_t> d_tdi_work;   //   and the prefix of their work items
   int last_launches = 0;
   bool profile = false;
   aak_mlp *model = nullptr;  // learned warm start of the map (optional)
@@ -757,6 +759,192 @@ int phase_roundtrip(aak_ctx *ctx, double *const *rows, double *base, int64_t ldh
   return device_status(ctx);
 }
 
+// ---------------------------------------------------------------- frequency-domain TDI
+// Per-source geometry of the TDI response (AAKTDI.cc:51-84): propagation
+// direction k = -n, polarisation basis u, v and angle psi.
+void tdi_geometry(double qS, double phiS, double qK, double phiK, TdiDesc *d) {
+  const double ctS = std::cos(qS), stS = std::sin(qS), cpS = std::cos(phiS), spS = std::sin(phiS);
+  const double up = ctS * std::sin(qK) * std::cos(phiS - phiK) - std::cos(qK) * stS;
+  const double dw = std::sin(qK) * std::sin(phiS - phiK);
+  const double psi = (dw != 0.0) ? -std::atan2(up, dw) : 0.5 * kPi;
+  d->c2psi = std::cos(2. * psi);
+  d->s2psi = std::sin(2. * psi);
+  d->k[0] = -stS * cpS;
+  d->k[1] = -stS * spS;
+  d->k[2] = -ctS;
+  d->uhat[0] = ctS * cpS;
+  d->uhat[1] = ctS * spS;
+  d->uhat[2] = -stS;
+  d->vhat[0] = spS;
+  d->vhat[1] = -cpS;
+  d->vhat[2] = 0.0;
+}
+
+// Plus / cross amplitudes of the sidebands m = -2..2 of a harmonic
+// (AAKTDI.cc:586-667): the projection of the orbital-plane basis (L at
+// inclination lambda from the spin) onto the sky frame, as trigonometric
+// polynomials in alpha.  AA = [plus cos | plus sin | cross cos | cross sin].
+void tdi_sidebands(double qS, double phiS, double qK, double phiK, double clam, double slam, double AA[20]) {
+  const double cS = std::cos(qS), sS = std::sin(qS), cK = std::cos(qK), sK = std::sin(qK);
+  const double cSp = std::cos(phiS), sSp = std::sin(phiS), cKp = std::cos(phiK), sKp = std::sin(phiK);
+  const double cX = cS * cK + sS * sK * std::cos(phiS - phiK);
+  const double sX = std::sqrt(sS * sS * cK * cK - 2. * sS * sSp * cK * cS * sK * sKp + cS * cS * sK * sK -
+                              2. * cS * sK * cKp * sS * cSp * cK + sS * sS * cSp * cSp * sK * sK * sKp * sKp -
+                              2. * sS * sS * cSp * sK * sK * sKp * sSp * cKp + sS * sS * sSp * sSp * sK * sK * cKp * cKp);
+  // orbital-plane basis vectors p and q, cos / sin / constant parts in alpha, for the two polarisation axes
+  const double pc1 = (-cK * cKp * sS * cSp - cK * sKp * sS * sSp + sK * cS) / sX;
+  const double ps1 = (sKp * sS * cSp - cKp * sS * sSp) / sX;
+  const double pn1 = (cK * cS + sK * cKp * sS * cSp + sK * sKp * sS * sSp - cX) * clam / (sX * slam);
+  const double pc2 = (sS * cSp * sKp - sS * sSp * cKp) * clam / sX;
+  const double ps2 = (cK * cKp * sS * cSp + cK * sKp * sS * sSp - cS * sK) * clam / sX;
+  const double pn2 = 0.0;
+  const double qc1 = (sS * cSp * sKp - sS * sSp * cKp) * cX / sX;
+  const double qs1 = (cK * cKp * sS * cSp + cK * sKp * sS * sSp - cS * sK) * cX / sX;
+  const double qn1 = 0.0;
+  const double qc2 = cX * clam * (cK * cKp * sS * cSp + cK * sKp * sS * sSp - sK * cS) / sX;
+  const double qs2 = -cX * clam * sS * (sKp * cSp - cKp * sSp) / sX;
+  const double qn2 = -(cX * clam * clam * (cK * cS + sK * cKp * sS * cSp + sK * sKp * sS * sSp) + 1. - cX * cX -
+                       clam * clam) / (sX * slam);
+  // products of the two axes: plus (p p - q q) and cross (p q) parts at frequencies 0, alpha, 2 alpha
+  const double P1c1 = 2.0 * (pc1 * pn1 - qc1 * qn1 + qc2 * qn2 - pc2 * pn2);
+  const double P1c2 = 0.5 * (ps2 * ps2 - qc1 * qc1 + pc1 * pc1 - ps1 * ps1 + qc2 * qc2 + qs1 * qs1 - pc2 * pc2 - qs2 * qs2);
+  const double P1s1 = 2.0 * (qs2 * qn2 - ps2 * pn2 - qs1 * qn1 + ps1 * pn1);
+  const double P1s2 = (pc1 * ps1 + qc2 * qs2 - pc2 * ps2 - qc1 * qs1);
+  const double P1cn = 0.5 * (pc1 * pc1 + ps1 * ps1 - qc1 * qc1 - qs1 * qs1 - pc2 * pc2 + qc2 * qc2 + qs2 * qs2 - ps2 * ps2) +
+                      qn2 * qn2 - qn1 * qn1 + pn1 * pn1 - pn2 * pn2;
+  const double P2c1 = (pn1 * pc2 + pc1 * pn2 - qn1 * qc2 - qc1 * qn2);
+  const double P2c2 = 0.5 * (qs1 * qs2 - ps1 * ps2 + pc1 * pc2 - qc1 * qc2);
+  const double P2s1 = (ps1 * pn2 + pn1 * ps2 - qn1 * qs2 - qs1 * qn2);
+  const double P2s2 = 0.5 * (pc1 * ps2 - qc1 * qs2 + ps1 * pc2 - qs1 * qc2);
+  const double P2cn = 0.5 * (ps1 * ps2 - qs1 * qs2 - qc1 * qc2 + pc1 * pc2) - qn1 * qn2 + pn1 * pn2;
+  const double C1c1 = (-pc2 * qn2 - pn2 * qc2 + pc1 * qn1 + pn1 * qc1);
+  const double C1c2 = 0.5 * (pc1 * qc1 - ps1 * qs1 - pc2 * qc2 + ps2 * qs2);
+  const double C1s1 = (pn1 * qs1 - ps2 * qn2 + ps1 * qn1 - pn2 * qs2);
+  const double C1s2 = 0.5 * (-pc2 * qs2 + pc1 * qs1 - ps2 * qc2 + ps1 * qc1);
+  const double C1cn = -pn2 * qn2 + pn1 * qn1 + 0.5 * (pc1 * qc1 - ps2 * qs2 + ps1 * qs1 - pc2 * qc2);
+  const double C2c1 = (qc1 * pn2 + qn1 * pc2 + pc1 * qn2 + pn1 * qc2);
+  const double C2c2 = 0.5 * (pc1 * qc2 - ps1 * qs2 + qc1 * pc2 - qs1 * ps2);
+  const double C2s1 = (pn1 * qs2 + qs1 * pn2 + ps1 * qn2 + qn1 * ps2);
+  const double C2s2 = 0.5 * (qc1 * ps2 + pc1 * qs2 + qs1 * pc2 + ps1 * qc2);
+  const double C2cn = qn1 * pn2 + pn1 * qn2 + 0.5 * (pc1 * qc2 + qs1 * ps2 + ps1 * qs2 + qc1 * pc2);
+  // sideband m: e^{i m alpha} weights (m = -2, -1, 0, 1, 2)
+  const double pcs[5] = {0.5 * (P1c2 + P2s2), 0.5 * (P1c1 + P2s1), P1cn, 0.5 * (P1c1 - P2s1), 0.5 * (P1c2 - P2s2)};
+  const double pss[5] = {0.5 * (P2c2 - P1s2), 0.5 * (P2c1 - P1s1), P2cn, 0.5 * (P2c1 + P1s1), 0.5 * (P2c2 + P1s2)};
+  const double ccs[5] = {0.5 * (C1c2 + C2s2), 0.5 * (C1c1 + C2s1), C1cn, 0.5 * (C1c1 - C2s1), 0.5 * (C1c2 - C2s2)};
+  const double css[5] = {0.5 * (C2c2 - C1s2), 0.5 * (C2c1 - C1s1), C2cn, 0.5 * (C2c1 + C1s1), 0.5 * (C2c2 + C1s2)};
+  for (int m = 0; m < 5; ++m) {
+    AA[m] = pcs[m];
+    AA[5 + m] = pss[m];
+    AA[10 + m] = ccs[m];
+    AA[15 + m] = css[m];
+  }
+}
+
+// The frequency-domain TDI of nsrc sources (GenTDI, AAKTDI.cc:799-829) into
+// host rows: Xr, Xi, Yr, Yi, Zr, Zi, each sum((length + 1) / 2) bins, source s
+// from bin_ofs[s].  Front end on the sources' own (length, dt); then each
+// source's phase grid (dt_ph = 0.01 M^2 / mu, Nph points over the span) is
+// planned, generated by the phase pass and summed by stationary phase.
+int tdi_batch(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads, double *const *rows,
+              std::vector<int64_t> &bin_ofs, std::vector<int32_t> &st_out) {
+  if (!P || nsrc < 1) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  std::vector<aak_mapped> maps(nsrc);
+  std::vector<aak_params> G(P, P + nsrc);
+  std::vector<int32_t> fe(nsrc, AAK_OK), nm(nsrc, 4);
+  std::vector<double> dt_ph(nsrc, 0.0), Tobs(nsrc, 0.0);
+  parallel_for(nsrc, nthreads, [&](int64_t s) {
+    fe[s] = aak_front_end(&P[s], nullptr, &maps[s]);
+    if (fe[s] != AAK_OK) {
+      G[s].e = -1.0;  // fails the grid plan's validation; the front end's status is reported
+      return;
+    }
+    const double mu_s = P[s].mu * kMsunSec, M_s = maps[s].M_map[0] * kMsunSec;
+    Tobs[s] = (double)(P[s].length - 1) * P[s].dt;
+    double h = 0.01 * M_s * M_s / mu_s;
+    const double nph = Tobs[s] / h;
+    if (!(nph >= 3.0 && nph < 2.0e9)) {
+      fe[s] = AAK_ERR_INVALID_PARAM;
+      G[s].e = -1.0;
+      return;
+    }
+    const int Nph = (int)nph;
+    dt_ph[s] = Tobs[s] / (Nph - 1);
+    G[s].length = Nph;
+    G[s].dt = dt_ph[s];
+    const double e0 = maps[s].e_traj[0];
+    nm[s] = (e0 < 0.135) ? 4 : std::max(1, (int)(30 * e0));
+  });
+  ctx->out_stride = 0;
+  if ((r = plan_common(ctx, G.data(), maps.data(), nsrc, nm.data(), nthreads)) != AAK_OK) return r;
+  if ((r = upload(ctx, 0)) != AAK_OK) return r;
+  // records of the stationary-phase sum
+  std::vector<TdiDesc> td(nsrc);
+  std::vector<int64_t> work(nsrc + 1, 0);
+  bin_ofs.assign(nsrc + 1, 0);
+  st_out.assign(nsrc, AAK_OK);
+  for (int s = 0; s < nsrc; ++s) {
+    const int32_t st = (fe[s] != AAK_OK) ? fe[s] : ctx->status[s];
+    st_out[s] = st;
+    bin_ofs[s + 1] = bin_ofs[s] + (P[s].length + 1) / 2;
+    TdiDesc &d = td[s];
+    std::memset(&d, 0, sizeof(d));
+    d.status = st;
+    d.bin_offset = bin_ofs[s];
+    d.nbins = (int32_t)((P[s].length + 1) / 2);
+    if (st == AAK_OK) {
+      const SourceDesc &sd = ctx->descs[s];
+      d.grid_offset = ctx->offsets[s];
+      d.i0 = sd.i0;
+      d.ip = std::min(sd.i_plunge, sd.vlength - 1);  // the sum reads grid points 0 .. ip - 1
+      d.nmodes = nm[s];
+      d.bessel_offset = sd.bessel_offset;
+      d.dt_ph = dt_ph[s];
+      d.dOm = 2. * kPi / Tobs[s];
+      d.DM = kAUsec * std::sin(P[s].theta_S);
+      d.phiS = P[s].phi_S;
+      d.arm = 2.5e9 / kC;
+      tdi_geometry(P[s].theta_S, P[s].phi_S, P[s].theta_K, P[s].phi_K, &d);
+      tdi_sidebands(P[s].theta_S, P[s].phi_S, P[s].theta_K, P[s].phi_K, std::cos(P[s].iota), std::sin(P[s].iota), d.AA);
+    }
+    const int64_t items = (st == AAK_OK && d.ip >= 2) ? (int64_t)(d.ip - 1) * 5 * d.nmodes : 0;
+    work[s + 1] = work[s] + items;
+  }
+  const int64_t N = ctx->total_samples, nb = bin_ofs[nsrc];
+  if ((r = ctx->d_out.reserve((size_t)kTdiRows * std::max<int64_t>(N, 1) + 6 * (size_t)nb)) != AAK_OK ||
+      (r = ctx->d_tdi.reserve(nsrc)) != AAK_OK || (r = ctx->d_tdi_work.reserve(nsrc + 1)) != AAK_OK)
+    return r;
+  double *grid = ctx->d_out.ptr, *out = grid + (size_t)kTdiRows * std::max<int64_t>(N, 1);
+  BatchView bv = batch_view(ctx, nullptr, nullptr, nullptr, nullptr, 0);
+  bv.phase_out = grid;
+  bv.phase_stride = N;
+  bv.trajectory_only = 1;
+  launch_tdi_grid(bv, ctx->num_sms, 0, nullptr);
+  if ((r = cuda_ok(cudaMemcpyAsync(ctx->d_tdi.ptr, td.data(), nsrc * sizeof(TdiDesc), cudaMemcpyHostToDevice, 0))) ||
+      (r = cuda_ok(cudaMemcpyAsync(ctx->d_tdi_work.ptr, work.data(), (nsrc + 1) * sizeof(int64_t),
+                                   cudaMemcpyHostToDevice, 0))))
+    return r;
+  TdiArgs a;
+  a.src = ctx->d_tdi.ptr;
+  a.nsrc = nsrc;
+  a.work_start = ctx->d_tdi_work.ptr;
+  a.total_work = work[nsrc];
+  a.grid = grid;
+  a.grid_stride = N;
+  a.bessel_start = ctx->d_bessel.ptr;
+  a.out = out;
+  a.out_stride = nb;
+  launch_tdi_spa(a, 0);
+  ctx->last_launches = 3;
+  if ((r = cuda_ok(cudaGetLastError())) != AAK_OK) return r;
+  for (int k = 0; k < 6; ++k)
+    if ((r = cuda_ok(cudaMemcpyAsync(rows[k], out + k * nb, nb * sizeof(double), cudaMemcpyDeviceToHost, 0))) != AAK_OK)
+      return r;
+  if ((r = cuda_ok(cudaStreamSynchronize(0))) != AAK_OK) return r;
+  return device_status(ctx);
+}
+
 // aak_wave_batch_host for batches worth streaming.  Host threads plan the
 // sources (the few that bound the planning time first, then the rest smallest
 // first); as they finish, the calling thread gathers them in groups of about
@@ -972,6 +1160,8 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_flag.release();
     c->d_counter.release();
     c->d_out.release();
+    c->d_tdi.release();
+    c->d_tdi_work.release();
     for (auto &e : c->ev)
       if (e) cudaEventDestroy(e);
     drop_graph(c);
@@ -1241,6 +1431,49 @@ int aak_phase(const aak_params *p, double *t, double *phase_r, double *phase_the
   r = phase_roundtrip(ctx, rows, nullptr, 0);
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return r;
+}
+
+int aak_tdi(const aak_params *p, double *f, double *Xf_r, double *Xf_im, double *Yf_r, double *Yf_im, double *Zf_r,
+            double *Zf_im, double *seconds) {
+  if (!p || !Xf_r || !Xf_im || !Yf_r || !Yf_im || !Zf_r || !Zf_im) return AAK_ERR_INVALID_PARAM;
+  const auto t0 = std::chrono::steady_clock::now();
+  aak_ctx *ctx = nullptr;
+  int r = default_ctx(&ctx);
+  if (r != AAK_OK) return r;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  double *const rows[6] = {Xf_r, Xf_im, Yf_r, Yf_im, Zf_r, Zf_im};
+  std::vector<int64_t> ofs;
+  std::vector<int32_t> st;
+  r = tdi_batch(ctx, p, 1, 1, rows, ofs, st);
+  if (r != AAK_OK) return r;
+  if (st[0] != AAK_OK) return st[0];
+  if (f) {
+    const double df = 1. / ((double)(p->length - 1) * p->dt);
+    for (int64_t i = 0; i < (p->length + 1) / 2; ++i) f[i] = (double)i * df;
+  }
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return AAK_OK;
+}
+
+int aak_tdi_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads, double *h_out,
+                       int64_t *bin_offsets, int32_t *status) {
+  if (!ctx || !P || !h_out || nsrc < 1) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  int64_t nb = 0;
+  for (int s = 0; s < nsrc; ++s) {
+    if (P[s].length < 2) return AAK_ERR_INVALID_PARAM;
+    nb += (P[s].length + 1) / 2;
+  }
+  double *const rows[6] = {h_out, h_out + nb, h_out + 2 * nb, h_out + 3 * nb, h_out + 4 * nb, h_out + 5 * nb};
+  std::vector<int64_t> ofs;
+  std::vector<int32_t> st;
+  const int r = tdi_batch(ctx, P, nsrc, nthreads, rows, ofs, st);
+  if (r != AAK_OK) return r;
+  if (bin_offsets)
+    for (int s = 0; s <= nsrc; ++s) bin_offsets[s] = ofs[s];
+  if (status)
+    for (int s = 0; s < nsrc; ++s) status[s] = st[s];
+  return AAK_OK;
 }
 
 int aak_batch_run_phase(aak_ctx *ctx, double *d_out, int64_t stride, void *stream) {

@@ -965,14 +965,17 @@ static_assert(kTileChunks % AAK_JOINT_SPLIT == 0 && kTileChunks % AAK_JOINT_FP64
 constexpr int kDynVals = 7;  // e, Omega_phi M_phys, gamma~, Phi, alpha, nu, gamma~dot
 constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double);
 
-// kPhase: the phase product instead of the waveform (FP64 only): every
+// kMode 1, the phase product instead of the waveform (FP64 only): every
 // sample of each source runs through phase 1, the harmonic sums are skipped,
 // and the tile's samples are written to bv.phase_out as t, phase_r,
 // phase_theta, phase_phi, omega_r, omega_theta, omega_phi, e (the per-sample
 // packing of GenPhase, AAKPhase.cc:346-355).  The phases of the samples
 // after the plunge buffer are frozen afterwards by k_phase_freeze.
-template <bool kSplit, bool kPhase = false>
+// kMode 2, the phase grid of the frequency-domain TDI (PNevolutionTDI,
+// AAKTDI.cc:311-469): the same pass writes kTdiRows rows (TdiRow order).
+template <bool kSplit, int kMode = 0>
 __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
+  constexpr bool kPhase = kMode != 0, kTdi = kMode == 2;
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
@@ -1006,7 +1009,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
         const int i = c.start + ch * kTileThreads + tid;
         if (i < c.end) {
           if constexpr (kPhase) {
-            for (int r = 0; r < 8; ++r) bv.phase_out[r * bv.phase_stride + dz.out_offset + i] = 0.0;
+            for (int r = 0; r < (kTdi ? kTdiRows : 8); ++r) bv.phase_out[r * bv.phase_stride + dz.out_offset + i] = 0.0;
           } else {
             bv.hI[dz.out_offset + i] = 0.0;
             bv.hII[dz.out_offset + i] = 0.0;
@@ -1119,6 +1122,14 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           bv.traj_out[2 * st + o] = q.M;
           bv.traj_out[3 * st + o] = q.S;
           bv.traj_out[8 * st + o] = r[0];
+        }
+        if constexpr (kTdi) {
+          const int64_t o = d.out_offset + i;
+          const int64_t st = bv.phase_stride;
+          bv.phase_out[kTdiE * st + o] = q.e;
+          bv.phase_out[kTdiAmp * st + o] = pow(om * d.M_phys_sec, 2. / 3.) * d.zeta;
+          bv.phase_out[kTdiGd * st + o] = r[0];
+          bv.phase_out[kTdiAd * st + o] = r[2];
         }
       }
       sv_e[sl] = q.e;
@@ -1320,7 +1331,16 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           bv.traj_out[5 * st + o] = X[1];
           bv.traj_out[6 * st + o] = X[2];
         }
-        if constexpr (kPhase) {
+        if constexpr (kTdi) {
+          const int64_t o = d.out_offset + i;
+          const int64_t st = bv.phase_stride;
+          bv.phase_out[kTdiT * st + o] = sample_time(d, i);
+          bv.phase_out[kTdiGim * st + o] = X[0];
+          bv.phase_out[kTdiPhi * st + o] = X[1];
+          bv.phase_out[kTdiAlp * st + o] = X[2];
+          bv.phase_out[kTdiNu * st + o] = sv_nu[sl] / 2. / kPi;  // nuvec = Phidot / 2 / pi
+          bv.phase_out[kTdiPd * st + o] = sv_nu[sl];
+        } else if constexpr (kPhase) {
           // GenPhase's packing, sums in its order (AAKPhase.cc:347-354)
           const int64_t o = d.out_offset + i;
           const int64_t st = bv.phase_stride;
@@ -1618,7 +1638,8 @@ void prepare_dense_launch() {
     const int most = (int)(kWaveDynSmem + (size_t)kTabModes * kRowD * sizeof(double));
     cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
-    cudaFuncSetAttribute(k_waveform<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
+    cudaFuncSetAttribute(k_waveform<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
+    cudaFuncSetAttribute(k_waveform<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     attrs_set.fetch_or(bit);
   }
 }
@@ -1683,13 +1704,235 @@ void launch_phase(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
   }
   prepare_dense_launch();
   int resident = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false, true>, kTileThreads, kWaveDynSmem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false, 1>, kTileThreads, kWaveDynSmem);
   resident = std::max(resident, 1);
   const int grid = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
-  k_waveform<false, true><<<grid, kTileThreads, kWaveDynSmem, stream>>>(bv);
+  k_waveform<false, 1><<<grid, kTileThreads, kWaveDynSmem, stream>>>(bv);
   const dim3 fgrid(64, (unsigned)std::min(std::max(bv.nsrc, 1), 1024));
   k_phase_freeze<<<fgrid, 256, 0, stream>>>(bv.src, bv.nsrc, bv.phase_out, bv.phase_stride);
   if (ev) cudaEventRecord(ev[3], stream);
+}
+
+void launch_tdi_grid(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev) {
+  if (bv.total_tiles <= 0 || !bv.phase_out) return;
+  if (ev) cudaEventRecord(ev[0], stream);
+  cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
+  cudaMemsetAsync(bv.link_flag, 0, (size_t)bv.total_tiles * sizeof(int32_t), stream);
+  if (ev) {
+    cudaEventRecord(ev[1], stream);
+    cudaEventRecord(ev[2], stream);
+  }
+  prepare_dense_launch();
+  int resident = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false, 2>, kTileThreads, kWaveDynSmem);
+  resident = std::max(resident, 1);
+  const int grid = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
+  k_waveform<false, 2><<<grid, kTileThreads, kWaveDynSmem, stream>>>(bv);
+  if (ev) cudaEventRecord(ev[3], stream);
+}
+
+// ------------------------------------------------------------------ stationary-phase TDI
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cscale(double r, double2 a) { return make_double2(r * a.x, r * a.y); }
+// exp(-i x)
+__device__ __forceinline__ double2 cexpm(double x) {
+  double sx, cx;
+  sincos(x, &sx, &cx);
+  return make_double2(cx, -sx);
+}
+// normalised sinc, sin(pi x) / (pi x)
+__device__ __forceinline__ double sinc_pi(double x) { return x == 0.0 ? 1.0 : sinpi(x) / (kPi * x); }
+
+// TDI transfer functions of one harmonic of angular frequency om at time t
+// (AAKTDI.cc:345-392, the LISA constellation of KSParMap.cc:576-596 with
+// kappa0 = lambda0 = 0): F[0..5] = Xp, Xc, Yp, Yc, Zp, Zc.
+__device__ void tdi_transfer(const TdiDesc &d, double t, double om, double2 F[6]) {
+  const double alpha = 2. * kPi * 3.1709791983764586e-8 * t;
+  double sa, ca;
+  sincos(alpha, &sa, &ca);
+  double q[3][3], n[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const double xi = i * 2.0 * kPi / 3.0;
+    double sx, cx;
+    sincos(xi, &sx, &cx);
+    q[i][0] = (sa * ca * sx - (1. + sa * sa) * cx) / (2.0 * sqrt(3.));
+    q[i][1] = (sa * ca * cx - (1. + ca * ca) * sx) / (2.0 * sqrt(3.));
+    q[i][2] = -0.5 * cos(alpha - xi);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    n[0][i] = q[1][i] - q[2][i];
+    n[1][i] = q[2][i] - q[0][i];
+    n[2][i] = q[0][i] - q[1][i];
+  }
+  double kn[3], kq[3], u[3], v[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double a = 0, b = 0, nU = 0, nV = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      a += d.k[i] * n[j][i];
+      b += d.k[i] * q[j][i];
+      nU += d.uhat[i] * n[j][i];
+      nV += d.vhat[i] * n[j][i];
+    }
+    kn[j] = a;
+    kq[j] = b;
+    u[j] = 0.5 * (nU * nU - nV * nV);
+    v[j] = nU * nV;
+  }
+  const double x = om * d.arm, x2 = 0.5 * x, xs = x * sin(x);
+  const double2 emx = cexpm(x);
+  // link a: its two chi forms; the phase uses the kq of the other two spacecraft
+  double2 chim[3], chip[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int p0 = (a == 0) ? 2 : (a == 1) ? 0 : 1, p1 = (a == 0) ? 1 : (a == 1) ? 2 : 0;
+    const double2 ph = cexpm(x2 * (3.0 + kq[p0] + kq[p1]));
+    const double s1 = sinc_pi(x2 * (1. - kn[a])), s2 = sinc_pi(x2 * (1. + kn[a]));
+    chim[a] = cmul(cscale(-xs, cadd(cscale(s1, emx), make_double2(s2, 0.0))), ph);
+    chip[a] = cmul(cscale(xs, cadd(make_double2(s1, 0.0), cscale(s2, emx))), ph);
+  }
+  // X: link 1 (first form) and 2 (second); Y: 2 and 0; Z: 0 and 1
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) {
+    const int a = (ch == 0) ? 1 : (ch == 1) ? 2 : 0, b = (ch == 0) ? 2 : (ch == 1) ? 0 : 1;
+    F[2 * ch] = cadd(cscale(u[a] * d.c2psi - v[a] * d.s2psi, chim[a]), cscale(u[b] * d.c2psi - v[b] * d.s2psi, chip[b]));
+    F[2 * ch + 1] =
+        cadd(cscale(v[a] * d.c2psi + u[a] * d.s2psi, chim[a]), cscale(v[b] * d.c2psi + u[b] * d.s2psi, chip[b]));
+  }
+}
+
+// Second derivative at grid point idx as PNevolutionTDI leaves it: forward
+// differences after i0 (the last point repeats the one before), backward ones
+// at and before i0, point 0 repeating point 1 (AAKTDI.cc:334-343, 407-416).
+__device__ __forceinline__ double tdi_ddot(const double *row, int64_t base, int idx, int i0, int ip, double scale,
+                                           double dt) {
+  if (idx == 0) idx = 1;
+  if (idx <= i0) return scale * (row[base + idx] - row[base + idx - 1]) / dt;
+  if (idx >= ip - 1) idx = ip - 2;
+  return scale * (row[base + idx + 1] - row[base + idx]) / dt;
+}
+
+__global__ void __launch_bounds__(256) k_tdi_zero(double *out, int64_t n) {
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x)
+    out[j] = 0.0;
+}
+
+__global__ void __launch_bounds__(256) k_tdi_spa(TdiArgs a) {
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < a.total_work;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = a.nsrc - 1;  // source holding work item w
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (a.work_start[mid] <= w) lo = mid;
+      else hi = mid - 1;
+    }
+    const TdiDesc &d = a.src[lo];
+    if (d.status != 0) continue;
+    const int64_t local = w - a.work_start[lo];
+    const int nh = 5 * d.nmodes;
+    const int i = 1 + (int)(local / nh), ind = (int)(local % nh);
+    const int j = ind / 5, jj = ind - 5 * j;
+    const double nn = j + 1, mm = jj - 2.;
+    const int64_t st = a.grid_stride, g = d.grid_offset;
+    const double *G = a.grid;
+    const double nu0 = G[kTdiNu * st + g + i - 1], nu1 = G[kTdiNu * st + g + i];
+    const double gd0 = G[kTdiGd * st + g + i - 1], gd1 = G[kTdiGd * st + g + i];
+    const double ad0 = G[kTdiAd * st + g + i - 1], ad1 = G[kTdiAd * st + g + i];
+    const double om_in = nn * 2. * kPi * nu0 + 2. * gd0 + mm * ad0;
+    const double om_fin = nn * 2. * kPi * nu1 + 2. * gd1 + mm * ad1;
+    if (om_in == 0. || om_fin == 0.) continue;
+    if (!(om_in > 0.0) || !(om_fin > om_in)) continue;  // no bin lies in a falling, negative or NaN range
+    // bins ceil(om_in / dOm) .. floor(om_fin / dOm), the last one dropped when
+    // om_fin falls on it (AAKTDI.cc:705-713); kept in doubles until clamped
+    const double lo_b = ceil(om_in / d.dOm);
+    double up_b = floor(om_fin / d.dOm);
+    if (om_fin == up_b * d.dOm) up_b -= 1.0;
+    const double mx_b = fmin(up_b + 1.0, (double)d.nbins);
+    if (!(lo_b < mx_b)) continue;
+    const int ind_low = (int)lo_b, ind_max = (int)mx_b;
+    // the interval's end points
+    const double t0 = G[kTdiT * st + g + i - 1], t1 = G[kTdiT * st + g + i];
+    const double orbOm = 2. * kPi / kYear;
+    const double xi_in = t0 - d.DM * cos(orbOm * t0 - d.phiS);
+    const double xi_fin = t1 - d.DM * cos(orbOm * t1 - d.phiS);
+    const double dxi = xi_fin - xi_in, delom = om_fin - om_in;
+    const double dd0 = nn * tdi_ddot(G, kTdiNu * st + g, i - 1, d.i0, d.ip, 2. * kPi, d.dt_ph) +
+                       2. * tdi_ddot(G, kTdiGd * st + g, i - 1, d.i0, d.ip, 1.0, d.dt_ph) +
+                       mm * tdi_ddot(G, kTdiAd * st + g, i - 1, d.i0, d.ip, 1.0, d.dt_ph);
+    const double dd1 = nn * tdi_ddot(G, kTdiNu * st + g, i, d.i0, d.ip, 2. * kPi, d.dt_ph) +
+                       2. * tdi_ddot(G, kTdiGd * st + g, i, d.i0, d.ip, 1.0, d.dt_ph) +
+                       mm * tdi_ddot(G, kTdiAd * st + g, i, d.i0, d.ip, 1.0, d.dt_ph);
+    const double fz0 = nn * G[kTdiPhi * st + g + i - 1] + 2. * G[kTdiGim * st + g + i - 1] + mm * G[kTdiAlp * st + g + i - 1];
+    const double fz1 = nn * G[kTdiPhi * st + g + i] + 2. * G[kTdiGim * st + g + i] + mm * G[kTdiAlp * st + g + i];
+    const double A0 = G[kTdiAmp * st + g + i - 1], A1 = G[kTdiAmp * st + g + i];
+    const double e0 = G[kTdiE * st + g + i - 1], e1 = G[kTdiE * st + g + i];
+    double2 F0[6], F1[6];
+    tdi_transfer(d, t0, nn * G[kTdiPd * st + g + i - 1] + 2. * gd0 + mm * ad0, F0);
+    tdi_transfer(d, t1, nn * G[kTdiPd * st + g + i] + 2. * gd1 + mm * ad1, F1);
+    const double Apc0 = d.AA[jj], Aps0 = d.AA[5 + jj], Acc0 = 2. * d.AA[10 + jj], Acs0 = 2. * d.AA[15 + jj];
+    const int32_t bstart = a.bessel_start[d.bessel_offset + j];
+    for (int ii = ind_low; ii < ind_max; ++ii) {
+      const double Om = (double)ii * d.dOm;
+      double delta = (Om - om_in) / delom, eps = 1. - delta;
+      const double T = t1 * delta + t0 * eps;
+      const double xi = T - d.DM * cos(orbOm * T - d.phiS);
+      delta = (xi - xi_in) / dxi;
+      eps = 1. - delta;
+      const double dom = dd0 * eps + dd1 * delta;
+      const double faza = fz0 * eps + fz1 * delta;
+      const double amp = A0 * eps + A1 * delta;
+      const double ec = e0 * eps + e1 * delta;
+      const double ne = nn * ec;
+      double J[5];
+      if (!(ne > 0.0)) {
+        for (int m = 0; m < 5; ++m) J[m] = 0.0;
+        if (j == 0) J[1] = 1.0;        // J_0(0) at slot n - 1 for n = 1
+        else if (j == 1) J[0] = 1.0;   // J_0(0) at slot n - 2 for n = 2
+      } else if (j == 0) {
+        double Jt[5];
+        bessel5_fp64(0, ne, bstart, Jt);
+        J[0] = -Jt[1];
+        J[1] = Jt[0];
+        J[2] = Jt[1];
+        J[3] = Jt[2];
+        J[4] = Jt[3];
+      } else {
+        bessel5_fp64(j - 1, ne, bstart, J);
+      }
+      const double hamp = -nn * ((J[0] - 2. * ec * J[1] + 2. / nn * J[2] + 2. * ec * J[3] - J[4]) +
+                                 sqrt(1 - ec * ec) * (J[0] - 2. * J[2] + J[4]));
+      delta = (T - t0) / d.dt_ph;
+      eps = 1. - delta;
+      const double Apc = hamp * Apc0, Aps = hamp * Aps0, Acc = hamp * Acc0, Acs = hamp * Acs0;
+      double sinph, cosph;
+      sincos(faza - Om * xi + kPi * 0.25, &sinph, &cosph);
+      const double fact = 0.5 * amp * sqrt(2. * kPi / dom);
+      const double2 xp = make_double2(fact * (Apc * cosph + Aps * sinph), fact * (Apc * sinph - Aps * cosph));
+      const double2 xc = make_double2(fact * (Acc * cosph + Acs * sinph), fact * (Acc * sinph - Acs * cosph));
+      const int64_t o = d.bin_offset + ii;
+#pragma unroll
+      for (int ch = 0; ch < 3; ++ch) {
+        const double2 cFp = cadd(cscale(eps, F0[2 * ch]), cscale(delta, F1[2 * ch]));
+        const double2 cFc = cadd(cscale(eps, F0[2 * ch + 1]), cscale(delta, F1[2 * ch + 1]));
+        const double2 r = cadd(cmul(cFp, xp), cmul(cFc, xc));
+        atomicAdd(a.out + (2 * ch) * a.out_stride + o, r.x);
+        atomicAdd(a.out + (2 * ch + 1) * a.out_stride + o, r.y);
+      }
+    }
+  }
+}
+
+void launch_tdi_spa(const TdiArgs &a, cudaStream_t stream) {
+  if (a.out_stride > 0) k_tdi_zero<<<1184, 256, 0, stream>>>(a.out, 6 * a.out_stride);
+  if (a.total_work <= 0) return;
+  const int64_t blocks = std::min<int64_t>((a.total_work + 255) / 256, 148 * 64);
+  k_tdi_spa<<<(unsigned)blocks, 256, 0, stream>>>(a);
 }
 
 namespace {

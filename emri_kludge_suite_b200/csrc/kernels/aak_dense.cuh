@@ -71,6 +71,45 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
 // precision 0: FP64 throughout; 1: split (FP64 phases and reductions, FP32
 // geometry, response, Bessel evaluation and harmonic recurrence).
 void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision);
+// ------------------------------------------------------------------ frequency-domain TDI
+// Rows of the TDI phase grid that launch_tdi_grid writes to bv.phase_out
+// (kTdiRows x phase_stride, indexed by src.out_offset + i): the grid time,
+// e, the amplitude (Omega_phi M)^(2/3) zeta, the three phases, nu = Phidot /
+// 2 pi, gamma~dot, alphadot and Phidot (clamped after i0, raw elsewhere).
+constexpr int kTdiT = 0, kTdiE = 1, kTdiAmp = 2, kTdiGim = 3, kTdiPhi = 4, kTdiAlp = 5, kTdiNu = 6, kTdiGd = 7,
+              kTdiAd = 8, kTdiPd = 9, kTdiRows = 10;
+// The phase grid of PNevolutionTDI (src/suite/AAKTDI.cc:27-469) for every
+// source of a batch planned on that grid (length Nph, dt = dt_ph): the
+// waveform kernel's phase pass over all grid points, writing the rows above.
+void launch_tdi_grid(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev);
+
+// One source of the stationary-phase sum (waveformTDI, AAKTDI.cc:520-797).
+struct TdiDesc {
+  int64_t grid_offset;   // first grid point of the source in the grid rows
+  int64_t bin_offset;    // first output bin of the source
+  int32_t i0, ip;        // grid index of t = 0; intervals i = 1 .. ip - 1 are summed
+  int32_t nmodes, nbins; // harmonics; (length + 1) / 2 output bins
+  int32_t bessel_offset, status;
+  double dt_ph, dOm, DM, phiS, arm;
+  double k[3], uhat[3], vhat[3], c2psi, s2psi;  // propagation direction, polarisation basis and angle
+  double AA[20];         // sideband amplitudes: cos / sin of plus, cos / sin of cross, m = -2..2 each
+};
+struct TdiArgs {
+  const TdiDesc *src;
+  int32_t nsrc;
+  const int64_t *work_start;  // nsrc + 1 prefix of (ip - 1) x 5 nmodes work items
+  int64_t total_work;
+  const double *grid;         // kTdiRows x grid_stride
+  int64_t grid_stride;
+  const int32_t *bessel_start;
+  double *out;                // 6 x out_stride: Xr, Xi, Yr, Yi, Zr, Zi (zeroed by the launch)
+  int64_t out_stride;
+};
+// Zero the outputs, then one thread per (source, interval, harmonic n, sideband m):
+// the bins the harmonic crosses in the interval, each added to X, Y, Z with a
+// double atomic add (the order of the adds into one bin is not fixed).
+void launch_tdi_spa(const TdiArgs &a, cudaStream_t stream);
+
 // The AAK phase product of GenPhase (src/suite/AAKPhase.cc:315-374) for
 // every source of the batch into bv.phase_out: the waveform kernel's phase
 // pass over all samples (no harmonic sums), then the freeze of the phases

@@ -98,6 +98,18 @@ int aak_parmap(const double Omega[3], double p, double M, double s, double e, do
  * Runs on the current CUDA device; fails with AAK_ERR_CUDA without one. */
 int aak_wave(const aak_params *p, double *t, double *hI, double *hII, double *seconds);
 
+/* ------------------------------------------------------------------ frequency-domain AAK TDI (GPU) */
+/* Replaces AAKTDI (include/AAKpy.h, src/suite/AAKpy.cc:90-125; GenTDI and
+ * waveformTDI, src/suite/AAKTDI.cc:27-829): stationary-phase Michelson TDI
+ * channels X, Y, Z of the AAK source on the (p->length + 1) / 2 bins
+ * f = i / ((length - 1) dt).  Host buffers of (length + 1) / 2 doubles; f
+ * optional.  The phase grid (spacing 0.01 M^2 / mu) is generated on the
+ * GPU; each (interval, harmonic, sideband) adds its bins with double atomic
+ * adds, so the last bits of a bin may differ between calls.  FP64.  Errors as
+ * aak_wave. */
+int aak_tdi(const aak_params *p, double *f, double *Xf_r, double *Xf_im, double *Yf_r, double *Yf_im, double *Zf_r,
+            double *Zf_im, double *seconds);
+
 /* ------------------------------------------------------------------ AAK phases (GPU) */
 /* Replaces AAKphase (include/AAKpy.h:21, src/suite/AAKpy.cc:53-88, GenPhase
  * src/suite/AAKPhase.cc:315-374).  Host buffers of p->length doubles: t, the
@@ -174,6 +186,12 @@ int aak_batch_run_phase(aak_ctx *ctx, double *d_out, int64_t stride, void *strea
  * status != 0 and zeros in its rows. */
 int aak_phase_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads, double *h_out,
                          int64_t *offsets, int32_t *status);
+
+/* aak_tdi for nsrc sources in one batch: h_out holds 6 rows (Xr, Xi, Yr, Yi,
+ * Zr, Zi) of sum((P[s].length + 1) / 2) doubles; source s starts at bin
+ * bin_offsets[s] (nsrc + 1 entries, optional); status optional. */
+int aak_tdi_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads, double *h_out,
+                       int64_t *bin_offsets, int32_t *status);
 
 /* Allocation-free variant of aak_batch_run, for callers that cannot call
  * cudaMalloc: code whose device memory belongs to a host framework or a

@@ -432,6 +432,15 @@ static double o_p_of(double v, double e, double coslam, double S, double M, doub
   return (1. - e * e) * pow(oracle_omega_phi(v, e, coslam, S, M) * M_phys * O_MSUN_SEC, -2. / 3.);
 }
 
+/* Per-point arrays of the TDI phase grid (PNevolutionTDI, AAKTDI.cc:311-469),
+ * vlength + 1 entries each: amplitude, the three rates (Pd: Phidot as the
+ * transfer functions use it, clamped after i0), nu = Phidot / 2 pi, and the
+ * finite-difference second derivatives. */
+typedef struct {
+  double *Amp, *Pd, *gd, *ad, *nu, *gdd, *Pdd, *add;
+  double zeta;
+} o_tdi_grid;
+
 /* AAK.cc:27-318, and with Phidotvec/alpdotvec non-null PNevolutionPhase
  * (AAKPhase.cc:13-313), which also records Phidot (the clamped value on the
  * forward samples after i0, the raw one elsewhere) and alpdot.  Dense arrays
@@ -441,7 +450,7 @@ static int o_pnevolution(double *t, double *e, double *v, double *M, double *S, 
                          double *nu, double *gimdotvec, double *Phidotvec, double *alpdotvec, double timestep,
                          int vlength, const double *par, const double *e_traj, const double *v_map, double M_phys,
                          const double *M_map, double S_phys, const double *S_map, const double *dt_map, int steps,
-                         int *i_plunge, int *i_buffer, int backint) {
+                         int *i_plunge, int *i_buffer, int backint, o_tdi_grid *tdi) {
   const double mu = par[0], M0 = par[1], S0 = par[2], e0 = par[3], v0 = v_map[0];
   const double coslam = cos(par[4]);
   const double gim0 = par[5], Phi0 = par[6], alp0 = par[11];
@@ -608,6 +617,87 @@ static int o_pnevolution(double *t, double *e, double *v, double *M, double *S, 
   *i_buffer = (int)(10. / (oracle_omega_phi(v[ip], e[ip], coslam, S[ip], M[ip]) / 2. / M_PI) / timestep) + 1;
   int ib = *i_buffer;
   double gimdot = 0, Phidot = 0, alpdot = 0, gimdotm, Phidotm, alpdotm;
+  if (tdi) {
+    /* PNevolutionTDI's phase loops (AAKTDI.cc:311-469): forward to i_plunge
+     * only, no freeze; rates, amplitude and second derivatives recorded */
+    const double Msec = M_phys * O_MSUN_SEC;
+    double gimdotp, Phidotp, alpdotp;
+    gim[i0] = gim0;
+    Phi[i0] = Phi0;
+    alp[i0] = alp0;
+    for (int i = i0; i < ip; ++i) {
+      gimdotm = gimdot;
+      Phidotm = Phidot;
+      alpdotm = alpdot;
+      double tm = oracle_dtdm(v[i], e[i], coslam, S[i]), rm = oracle_drdm(v[i], e[i], coslam, S[i]);
+      double thm = oracle_dthetadm(v[i], e[i], coslam, S[i]), phm = oracle_dphidm(v[i], e[i], coslam, S[i]);
+      gimdot = (thm - rm) / tm / M[i];
+      Phidot = rm / tm / M[i];
+      alpdot = (phm - thm) / tm / M[i];
+      if (Phidot <= 0.) Phidot = Phidotm;
+      if (i == i0) {
+        gimdotm = gimdot;
+        Phidotm = Phidot;
+        alpdotm = alpdot;
+      }
+      tdi->Amp[i] = pow(oracle_omega_phi(v[i], e[i], coslam, S[i], M[i]) * Msec, 2. / 3.) * tdi->zeta;
+      tdi->nu[i] = Phidot / 2. / M_PI;
+      tdi->gd[i] = gimdot;
+      tdi->ad[i] = alpdot;
+      tdi->Pd[i] = Phidot;
+      gim[i + 1] = gim[i] + (1.5 * gimdot - .5 * gimdotm) * timestep;
+      Phi[i + 1] = Phi[i] + (1.5 * Phidot - .5 * Phidotm) * timestep;
+      alp[i + 1] = alp[i] + (1.5 * alpdot - .5 * alpdotm) * timestep;
+      if (i > i0) {
+        tdi->gdd[i - 1] = (tdi->gd[i] - tdi->gd[i - 1]) / timestep;
+        tdi->Pdd[i - 1] = 2. * M_PI * (tdi->nu[i] - tdi->nu[i - 1]) / timestep;
+        tdi->add[i - 1] = (tdi->ad[i] - tdi->ad[i - 1]) / timestep;
+      }
+      if (i == ip - 1) {
+        tdi->gdd[i] = tdi->gdd[i - 1];
+        tdi->Pdd[i] = tdi->Pdd[i - 1];
+        tdi->add[i] = tdi->add[i - 1];
+      }
+    }
+    for (int i = i0; i >= 0; --i) {
+      gimdotp = gimdot;
+      Phidotp = Phidot;
+      alpdotp = alpdot;
+      double tm = oracle_dtdm(v[i], e[i], coslam, S[i]), rm = oracle_drdm(v[i], e[i], coslam, S[i]);
+      double thm = oracle_dthetadm(v[i], e[i], coslam, S[i]), phm = oracle_dphidm(v[i], e[i], coslam, S[i]);
+      gimdot = (thm - rm) / tm / M[i];
+      Phidot = rm / tm / M[i];
+      alpdot = (phm - thm) / tm / M[i];
+      if (i == i0) {
+        gimdotp = gimdot;
+        Phidotp = Phidot;
+        alpdotp = alpdot;
+      }
+      tdi->Amp[i] = pow(oracle_omega_phi(v[i], e[i], coslam, S[i], M[i]) * Msec, 2. / 3.) * tdi->zeta;
+      tdi->nu[i] = Phidot / 2. / M_PI;
+      tdi->gd[i] = gimdot;
+      tdi->ad[i] = alpdot;
+      tdi->Pd[i] = Phidot;
+      if (i > 0) {
+        gim[i - 1] = gim[i] - (1.5 * gimdot - .5 * gimdotp) * timestep;
+        Phi[i - 1] = Phi[i] - (1.5 * Phidot - .5 * Phidotp) * timestep;
+        alp[i - 1] = alp[i] - (1.5 * alpdot - .5 * alpdotp) * timestep;
+      }
+      if (i < i0) {
+        tdi->gdd[i + 1] = (tdi->gd[i + 1] - tdi->gd[i]) / timestep;
+        tdi->Pdd[i + 1] = 2. * M_PI * (tdi->nu[i + 1] - tdi->nu[i]) / timestep;
+        tdi->add[i + 1] = (tdi->ad[i + 1] - tdi->ad[i]) / timestep;
+      }
+      if (i == 0) {
+        tdi->gdd[0] = tdi->gdd[1];
+        tdi->Pdd[0] = tdi->Pdd[1];
+        tdi->add[0] = tdi->add[1];
+      }
+    }
+    free(e_AK); free(v_AK); free(t_fit); free(e_fit); free(v_fit); free(M_fit); free(S_fit);
+    free(e_diff); free(v_diff);
+    return 0;
+  }
   gim[i0] = gim0;
   Phi[i0] = Phi0;
   alp[i0] = alp0;
@@ -700,7 +790,7 @@ int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, do
                        const double *S_map, const double *dt_map, int steps, int *i_plunge, int *i_buffer,
                        int backint) {
   return o_pnevolution(t, e, v, M, S, gim, Phi, alp, nu, gimdotvec, NULL, NULL, timestep, vlength, par, e_traj, v_map,
-                       M_phys, M_map, S_phys, S_map, dt_map, steps, i_plunge, i_buffer, backint);
+                       M_phys, M_map, S_phys, S_map, dt_map, steps, i_plunge, i_buffer, backint, NULL);
 }
 
 /* ------------------------------------------------------------------ waveform */
@@ -893,7 +983,7 @@ int oracle_genphase(double *t, double *phase_r, double *phase_theta, double *pha
   double *adv = buf + 11 * n1;
   int ip = 0, ib = 0;
   int rc = o_pnevolution(tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, Pdv, adv, timestep, vlength, par, e_traj, v_map,
-                         M_phys, M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint);
+                         M_phys, M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint, NULL);
   if (rc == 0) {
     for (int i = 0; i < vlength; ++i) {
       t[i] = tv[i];
@@ -910,4 +1000,270 @@ int oracle_genphase(double *t, double *phase_r, double *phase_theta, double *pha
   if (i_buffer) *i_buffer = ib;
   free(buf);
   return rc;
+}
+
+/* ------------------------------------------------------------------ frequency-domain TDI */
+/* LISA constellation at time t (EccentricLISAMotion, KSParMap.cc:576-596,
+ * kappa0 = lambda0 = 0): unit link vectors n[link][coord] and spacecraft
+ * positions q[sc][coord] in units of the orbit radius. */
+static void o_lisa_motion(double t, double q[3][3], double n[3][3]) {
+  const double Omega = 2. * M_PI * 3.1709791983764586e-8;
+  const double alpha = Omega * t;
+  const double sa = sin(alpha), ca = cos(alpha);
+  for (int i = 0; i < 3; ++i) {
+    const double xi = (float)0.0 + i * 2.0 * M_PI / 3.0;
+    q[i][0] = (sa * ca * sin(xi) - (1. + sa * sa) * cos(xi)) / (2.0 * sqrt(3.));
+    q[i][1] = (sa * ca * cos(xi) - (1. + ca * ca) * sin(xi)) / (2.0 * sqrt(3.));
+    q[i][2] = -0.5 * cos(alpha - xi);
+  }
+  for (int i = 0; i < 3; ++i) {
+    n[0][i] = q[1][i] - q[2][i];
+    n[1][i] = q[2][i] - q[0][i];
+    n[2][i] = q[0][i] - q[1][i];
+  }
+}
+
+static double o_sinc(double x) { return x == 0.0 ? 1.0 : sin(M_PI * x) / (M_PI * x); }
+
+/* Per-source TDI geometry: propagation direction, polarisation basis and angle. */
+typedef struct {
+  double k[3], uhat[3], vhat[3], c2psi, s2psi;
+} o_tdi_geom;
+
+static void o_tdi_geometry(double qS, double phiS, double qK, double phiK, o_tdi_geom *g) {
+  const double ctS = cos(qS), stS = sin(qS), cpS = cos(phiS), spS = sin(phiS);
+  const double up = ctS * sin(qK) * cos(phiS - phiK) - cos(qK) * stS;
+  const double dw = sin(qK) * sin(phiS - phiK);
+  const double psi = (dw != 0.0) ? -atan2(up, dw) : 0.5 * M_PI;
+  g->c2psi = cos(2. * psi);
+  g->s2psi = sin(2. * psi);
+  g->k[0] = -stS * cpS;
+  g->k[1] = -stS * spS;
+  g->k[2] = -ctS;
+  g->uhat[0] = ctS * cpS;
+  g->uhat[1] = ctS * spS;
+  g->uhat[2] = -stS;
+  g->vhat[0] = spS;
+  g->vhat[1] = -cpS;
+  g->vhat[2] = 0.0;
+}
+
+/* TDI transfer functions X, Y, Z (plus and cross) of one harmonic of angular
+ * frequency om at time t (AAKTDI.cc:345-392): out[0..5] = Xp, Xc, Yp, Yc, Zp, Zc. */
+static void o_tdi_transfer(const o_tdi_geom *g, double t, double om, double arm, double complex out[6]) {
+  double q[3][3], n[3][3], kn[3], kq[3], u[3], w[3];
+  o_lisa_motion(t, q, n);
+  for (int j = 0; j < 3; ++j) {
+    double a = 0, b = 0, nU = 0, nV = 0;
+    for (int i = 0; i < 3; ++i) {
+      a += g->k[i] * n[j][i];
+      b += g->k[i] * q[j][i];
+      nU += g->uhat[i] * n[j][i];
+      nV += g->vhat[i] * n[j][i];
+    }
+    kn[j] = a;
+    kq[j] = b;
+    u[j] = 0.5 * (nU * nU - nV * nV);
+    w[j] = nU * nV;
+  }
+  const double x = om * arm, x2 = 0.5 * x, xs = x * sin(x);
+  const double complex emx = cexp(-I * x);
+  /* chi_a (a = 0, 1, 2) in its two forms: "minus" (first in its channel) and "plus" */
+  const int pa[3][2] = {{2, 1}, {0, 2}, {1, 0}}; /* the kq pair of each link */
+  double complex chim[3], chip[3];
+  for (int a = 0; a < 3; ++a) {
+    const double complex ph = cexp(-I * x2 * (3.0 + kq[pa[a][0]] + kq[pa[a][1]]));
+    chim[a] = -xs * (o_sinc(x2 * (1. - kn[a])) * emx + o_sinc(x2 * (1. + kn[a]))) * ph;
+    chip[a] = xs * (o_sinc(x2 * (1. - kn[a])) + emx * o_sinc(x2 * (1. + kn[a]))) * ph;
+  }
+  const double c = g->c2psi, sn = g->s2psi;
+  /* X: links 1 (minus) and 2 (plus); Y: 2 (minus) and 0 (plus); Z: 0 (minus) and 1 (plus) */
+  const int lk[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  for (int ch = 0; ch < 3; ++ch) {
+    const int a = lk[ch][0], b = lk[ch][1];
+    out[2 * ch] = (u[a] * c - w[a] * sn) * chim[a] + (u[b] * c - w[b] * sn) * chip[b];
+    out[2 * ch + 1] = (w[a] * c + u[a] * sn) * chim[a] + (w[b] * c + u[b] * sn) * chip[b];
+  }
+}
+
+/* Polarisation amplitude coefficients of the five m = -2..2 sidebands
+ * (AAKTDI.cc:586-667): AA[0..4] = AApcos, AA[5..9] = AApsin, AA[10..14] =
+ * AAccos, AA[15..19] = AAcsin. */
+static void o_tdi_sidebands(double qS, double phiS, double qK, double phiK, double clam, double slam, double AA[20]) {
+  const double cS = cos(qS), sS = sin(qS), cK = cos(qK), sK = sin(qK);
+  const double cSp = cos(phiS), sSp = sin(phiS), cKp = cos(phiK), sKp = sin(phiK);
+  const double cX = cS * cK + sS * sK * cos(phiS - phiK);
+  const double sX = sqrt(sS * sS * cK * cK - 2. * sS * sSp * cK * cS * sK * sKp + cS * cS * sK * sK -
+                         2. * cS * sK * cKp * sS * cSp * cK + sS * sS * cSp * cSp * sK * sK * sKp * sKp -
+                         2. * sS * sS * cSp * sK * sK * sKp * sSp * cKp + sS * sS * sSp * sSp * sK * sK * cKp * cKp);
+  const double Apc1 = (-cK * cKp * sS * cSp - cK * sKp * sS * sSp + sK * cS) / sX;
+  const double Aps1 = (sKp * sS * cSp - cKp * sS * sSp) / sX;
+  const double Apcn1 = (cK * cS + sK * cKp * sS * cSp + sK * sKp * sS * sSp - cX) * clam / (sX * slam);
+  const double Apc2 = (sS * cSp * sKp - sS * sSp * cKp) * clam / sX;
+  const double Aps2 = (cK * cKp * sS * cSp + cK * sKp * sS * sSp - cS * sK) * clam / sX;
+  const double Apcn2 = 0.0;
+  const double Aqc1 = (sS * cSp * sKp - sS * sSp * cKp) * cX / sX;
+  const double Aqs1 = (cK * cKp * sS * cSp + cK * sKp * sS * sSp - cS * sK) * cX / sX;
+  const double Aqcn1 = 0.0;
+  const double Aqc2 = cX * clam * (cK * cKp * sS * cSp + cK * sKp * sS * sSp - sK * cS) / sX;
+  const double Aqs2 = -cX * clam * sS * (sKp * cSp - cKp * sSp) / sX;
+  const double Aqcn2 = -(cX * clam * clam * (cK * cS + sK * cKp * sS * cSp + sK * sKp * sS * sSp) + 1. - cX * cX -
+                         clam * clam) / (sX * slam);
+  const double Bp1c1 = 2.0 * (Apc1 * Apcn1 - Aqc1 * Aqcn1 + Aqc2 * Aqcn2 - Apc2 * Apcn2);
+  const double Bp1c2 = 0.5 * (Aps2 * Aps2 - Aqc1 * Aqc1 + Apc1 * Apc1 - Aps1 * Aps1 + Aqc2 * Aqc2 + Aqs1 * Aqs1 -
+                              Apc2 * Apc2 - Aqs2 * Aqs2);
+  const double Bp1s1 = 2.0 * (Aqs2 * Aqcn2 - Aps2 * Apcn2 - Aqs1 * Aqcn1 + Aps1 * Apcn1);
+  const double Bp1s2 = (Apc1 * Aps1 + Aqc2 * Aqs2 - Apc2 * Aps2 - Aqc1 * Aqs1);
+  const double Bp1cn = 0.5 * (Apc1 * Apc1 + Aps1 * Aps1 - Aqc1 * Aqc1 - Aqs1 * Aqs1 - Apc2 * Apc2 + Aqc2 * Aqc2 +
+                              Aqs2 * Aqs2 - Aps2 * Aps2) + Aqcn2 * Aqcn2 - Aqcn1 * Aqcn1 + Apcn1 * Apcn1 -
+                       Apcn2 * Apcn2;
+  const double Bp2c1 = (Apcn1 * Apc2 + Apc1 * Apcn2 - Aqcn1 * Aqc2 - Aqc1 * Aqcn2);
+  const double Bp2c2 = 0.5 * (Aqs1 * Aqs2 - Aps1 * Aps2 + Apc1 * Apc2 - Aqc1 * Aqc2);
+  const double Bp2s1 = (Aps1 * Apcn2 + Apcn1 * Aps2 - Aqcn1 * Aqs2 - Aqs1 * Aqcn2);
+  const double Bp2s2 = 0.5 * (Apc1 * Aps2 - Aqc1 * Aqs2 + Aps1 * Apc2 - Aqs1 * Aqc2);
+  const double Bp2cn = 0.5 * (Aps1 * Aps2 - Aqs1 * Aqs2 - Aqc1 * Aqc2 + Apc1 * Apc2) - Aqcn1 * Aqcn2 + Apcn1 * Apcn2;
+  const double Bc1c1 = (-Apc2 * Aqcn2 - Apcn2 * Aqc2 + Apc1 * Aqcn1 + Apcn1 * Aqc1);
+  const double Bc1c2 = 0.5 * (Apc1 * Aqc1 - Aps1 * Aqs1 - Apc2 * Aqc2 + Aps2 * Aqs2);
+  const double Bc1s1 = (Apcn1 * Aqs1 - Aps2 * Aqcn2 + Aps1 * Aqcn1 - Apcn2 * Aqs2);
+  const double Bc1s2 = 0.5 * (-Apc2 * Aqs2 + Apc1 * Aqs1 - Aps2 * Aqc2 + Aps1 * Aqc1);
+  const double Bc1cn = -Apcn2 * Aqcn2 + Apcn1 * Aqcn1 + 0.5 * (Apc1 * Aqc1 - Aps2 * Aqs2 + Aps1 * Aqs1 - Apc2 * Aqc2);
+  const double Bc2c1 = (Aqc1 * Apcn2 + Aqcn1 * Apc2 + Apc1 * Aqcn2 + Apcn1 * Aqc2);
+  const double Bc2c2 = 0.5 * (Apc1 * Aqc2 - Aps1 * Aqs2 + Aqc1 * Apc2 - Aqs1 * Aps2);
+  const double Bc2s1 = (Apcn1 * Aqs2 + Aqs1 * Apcn2 + Aps1 * Aqcn2 + Aqcn1 * Aps2);
+  const double Bc2s2 = 0.5 * (Aqc1 * Aps2 + Apc1 * Aqs2 + Aqs1 * Apc2 + Aps1 * Aqc2);
+  const double Bc2cn = Aqcn1 * Apcn2 + Apcn1 * Aqcn2 + 0.5 * (Apc1 * Aqc2 + Aqs1 * Aps2 + Aps1 * Aqs2 + Aqc1 * Apc2);
+  double *pc = AA, *ps = AA + 5, *cc = AA + 10, *cs = AA + 15;
+  pc[0] = 0.5 * (Bp1c2 + Bp2s2); ps[0] = 0.5 * (Bp2c2 - Bp1s2); cc[0] = 0.5 * (Bc1c2 + Bc2s2); cs[0] = 0.5 * (Bc2c2 - Bc1s2);
+  pc[1] = 0.5 * (Bp1c1 + Bp2s1); ps[1] = 0.5 * (Bp2c1 - Bp1s1); cc[1] = 0.5 * (Bc1c1 + Bc2s1); cs[1] = 0.5 * (Bc2c1 - Bc1s1);
+  pc[2] = Bp1cn; ps[2] = Bp2cn; cc[2] = Bc1cn; cs[2] = Bc2cn;
+  pc[3] = 0.5 * (Bp1c1 - Bp2s1); ps[3] = 0.5 * (Bp2c1 + Bp1s1); cc[3] = 0.5 * (Bc1c1 - Bc2s1); cs[3] = 0.5 * (Bc2c1 + Bc1s1);
+  pc[4] = 0.5 * (Bp1c2 - Bp2s2); ps[4] = 0.5 * (Bp2c2 + Bp1s2); cc[4] = 0.5 * (Bc1c2 - Bc2s2); cs[4] = 0.5 * (Bc2c2 + Bc1s2);
+}
+
+/* GenTDI -> waveformTDI (AAKTDI.cc:520-829): stationary-phase X, Y, Z on the
+ * (vlength + 1) / 2 bins f = i / ((vlength - 1) dt).  out6 = Xr, Xi, Yr, Yi,
+ * Zr, Zi (zeroed here), f (optional).  Returns 0, or -1 when PNevolution
+ * fails. */
+int oracle_gentdi(double *f, double *const *out6, double timestep, int vlength, const double *e_traj,
+                  const double *v_map, double M_phys, const double *M_map, double mu, double S_phys,
+                  const double *S_map, double dist, double inc, double gim0, double Phi0, double qS, double phiS,
+                  double alp0, double qK, double phiK, const double *dt_map, int steps, int backint,
+                  int nmodes_override, int *i_plunge_out) {
+  double par[12];
+  par[0] = mu * O_MSUN_SEC;
+  par[1] = M_map[0] * O_MSUN_SEC;
+  par[2] = S_map[0];
+  par[3] = e_traj[0];
+  par[4] = inc;
+  par[5] = gim0;
+  par[6] = Phi0;
+  par[7] = qS;
+  par[8] = phiS;
+  par[9] = qK;
+  par[10] = phiK;
+  par[11] = alp0;
+  int nmodes = (int)(30 * par[3]);
+  if (par[3] < 0.135) nmodes = 4;
+  if (nmodes_override > 0) nmodes = nmodes_override;
+  const double zeta = par[0] / dist / O_GPC;
+  const int nbins = (vlength + 1) / 2;
+  const double Tobs = (vlength - 1) * timestep, df = 1. / Tobs;
+  if (f)
+    for (int i = 0; i < nbins; ++i) f[i] = i * df;
+  for (int c = 0; c < 6; ++c) memset(out6[c], 0, sizeof(double) * (size_t)nbins);
+  /* phase grid */
+  double dt_ph = 0.01 * par[1] * par[1] / par[0];
+  const int Nph = (int)(Tobs / dt_ph);
+  dt_ph = Tobs / (Nph - 1);
+  const double arm = 2.5e9 / O_C;
+  const size_t n1 = (size_t)Nph + 1;
+  double *buf = calloc(18 * n1, sizeof(double));
+  if (!buf) return -1;
+  double *tv = buf, *ev = buf + n1, *vv = buf + 2 * n1, *Mv = buf + 3 * n1, *Sv = buf + 4 * n1, *gv = buf + 5 * n1;
+  double *Pv = buf + 6 * n1, *av = buf + 7 * n1, *nv0 = buf + 8 * n1, *gdv0 = buf + 9 * n1;
+  o_tdi_grid G = {buf + 10 * n1, buf + 11 * n1, buf + 12 * n1, buf + 13 * n1, buf + 14 * n1, buf + 15 * n1,
+                  buf + 16 * n1, buf + 17 * n1, zeta};
+  int ip = 0, ib = 0;
+  int rc = o_pnevolution(tv, ev, vv, Mv, Sv, gv, Pv, av, nv0, gdv0, NULL, NULL, dt_ph, Nph, par, e_traj, v_map, M_phys,
+                         M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint, &G);
+  if (i_plunge_out) *i_plunge_out = ip;
+  if (rc != 0) {
+    free(buf);
+    return rc;
+  }
+  o_tdi_geom geo;
+  o_tdi_geometry(qS, phiS, qK, phiK, &geo);
+  double AA[20];
+  o_tdi_sidebands(qS, phiS, qK, phiK, cos(inc), sin(inc), AA);
+  const double dOm = 2. * M_PI * df, orbOm = 2. * M_PI / O_YEAR, DM = O_AUSEC * sin(qS);
+  for (int i = 1; i < ip; ++i) {
+    const double xi_in = tv[i - 1] - DM * cos(orbOm * tv[i - 1] - phiS);
+    const double xi_fin = tv[i] - DM * cos(orbOm * tv[i] - phiS);
+    const double dxi = xi_fin - xi_in;
+    for (int j = 0; j < nmodes; ++j) {
+      const double nn = j + 1;
+      for (int jj = 0; jj < 5; ++jj) {
+        const double mm = jj - 2.;
+        const double om_in = nn * 2. * M_PI * G.nu[i - 1] + 2. * G.gd[i - 1] + mm * G.ad[i - 1];
+        const double om_fin = nn * 2. * M_PI * G.nu[i] + 2. * G.gd[i] + mm * G.ad[i];
+        const double delom = om_fin - om_in;
+        const int ind_low = (int)ceil(om_in / dOm);
+        int ind_up = (int)floor(om_fin / dOm);
+        if (om_fin == (double)ind_up * dOm && om_fin != 0.) ind_up = ind_up - 1;
+        if (om_in == 0. || om_fin == 0.) continue;
+        const int ind_max = (ind_up + 1 < (vlength + 1) / 2) ? ind_up + 1 : (vlength + 1) / 2;
+        if (ind_low >= ind_max) continue;
+        /* transfer functions at both ends of the interval, with the rates the phase loops used */
+        double complex F0[6], F1[6];
+        o_tdi_transfer(&geo, tv[i - 1], nn * G.Pd[i - 1] + 2. * G.gd[i - 1] + mm * G.ad[i - 1], arm, F0);
+        o_tdi_transfer(&geo, tv[i], nn * G.Pd[i] + 2. * G.gd[i] + mm * G.ad[i], arm, F1);
+        for (int ii = ind_low; ii < ind_max; ++ii) {
+          const double Om = (double)ii * dOm;
+          double delta = (Om - om_in) / delom, eps = 1. - delta;
+          const double T = tv[i] * delta + tv[i - 1] * eps;
+          const double xi = T - DM * cos(orbOm * T - phiS);
+          delta = (xi - xi_in) / dxi;
+          eps = 1. - delta;
+          const double dom = (nn * G.Pdd[i - 1] + 2. * G.gdd[i - 1] + mm * G.add[i - 1]) * eps +
+                             (nn * G.Pdd[i] + 2. * G.gdd[i] + mm * G.add[i]) * delta;
+          const double faza = (nn * Pv[i - 1] + 2. * gv[i - 1] + mm * av[i - 1]) * eps +
+                              (nn * Pv[i] + 2. * gv[i] + mm * av[i]) * delta;
+          const double amp = G.Amp[i - 1] * eps + G.Amp[i] * delta;
+          const double ec = ev[i - 1] * eps + ev[i] * delta;
+          const double ne = nn * ec;
+          double J[5];
+          if (j == 0) {
+            double Jt[4];
+            oracle_bessel_jn_array(0, 3, ne, Jt);
+            J[0] = -Jt[1];
+            J[1] = Jt[0];
+            J[2] = Jt[1];
+            J[3] = Jt[2];
+            J[4] = Jt[3];
+          } else {
+            oracle_bessel_jn_array(j - 1, j + 3, ne, J);
+          }
+          const double hamp = -nn * ((J[0] - 2. * ec * J[1] + 2. / nn * J[2] + 2. * ec * J[3] - J[4]) +
+                                     sqrt(1 - ec * ec) * (J[0] - 2. * J[2] + J[4]));
+          delta = (T - tv[i - 1]) / dt_ph;
+          eps = 1. - delta;
+          const double Apc = hamp * AA[jj], Aps = hamp * AA[5 + jj];
+          const double Acc = 2. * hamp * AA[10 + jj], Acs = 2. * hamp * AA[15 + jj];
+          const double sinph = sin(faza - Om * xi + M_PI * 0.25), cosph = cos(faza - Om * xi + M_PI * 0.25);
+          const double fact = 0.5 * amp * sqrt(2. * M_PI / dom);
+          const double complex xp = fact * (Apc * cosph + Aps * sinph + I * (Apc * sinph - Aps * cosph));
+          const double complex xc = fact * (Acc * cosph + Acs * sinph + I * (Acc * sinph - Acs * cosph));
+          for (int ch = 0; ch < 3; ++ch) {
+            const double complex cFp = F0[2 * ch] * eps + F1[2 * ch] * delta;
+            const double complex cFc = F0[2 * ch + 1] * eps + F1[2 * ch + 1] * delta;
+            const double complex r = cFp * xp + cFc * xc;
+            out6[2 * ch][ii] += creal(r);
+            out6[2 * ch + 1][ii] += cimag(r);
+          }
+        }
+      }
+    }
+  }
+  free(buf);
+  return 0;
 }

@@ -137,6 +137,13 @@ int gsl_sf_bessel_Jn_array(int nmin, int nmax, double x, double *r) {
   return GSL_SUCCESS;
 }
 
+// ---------------------------------------------------------------- sinc
+double gsl_sf_sinc(double x) {
+  if (x == 0.0) return 1.0;
+  const double px = M_PI * x;
+  return std::sin(px) / px;
+}
+
 // ---------------------------------------------------------------- natural cubic spline
 static const gsl_interp_type cspline_type = {"cspline", 3};
 const gsl_interp_type *gsl_interp_cspline = &cspline_type;

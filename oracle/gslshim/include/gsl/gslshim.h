@@ -80,6 +80,8 @@ double gsl_sf_bessel_J0(double x);
 double gsl_sf_bessel_J1(double x);
 double gsl_sf_bessel_Jn(int n, double x);
 int gsl_sf_bessel_Jn_array(int nmin, int nmax, double x, double *result_array);
+/* normalised sinc, sin(pi x) / (pi x), 1 at x = 0 (the GSL definition) */
+double gsl_sf_sinc(double x);
 
 /* ---- interpolation ---- */
 typedef struct {

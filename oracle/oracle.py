@@ -255,6 +255,55 @@ def ref_aakphase(pars: dict):
     return (*outs, secs)
 
 
+TDI_KEYS = ("f", "Xf_r", "Xf_im", "Yf_r", "Yf_im", "Zf_r", "Zf_im")
+
+
+def ref_aaktdi(pars: dict):
+    """Reference AAKTDI (src/suite/AAKpy.cc:90-125): the seven arrays of TDI_KEYS
+    ((length + 1) // 2 bins each) and the timing, as AAKwrapper.tdi returns them."""
+    L = ref_lib()
+    p = make_ref_params(pars)
+    n = (int(pars["length"]) + 1) // 2
+    outs = [np.zeros(n) for _ in TDI_KEYS]
+    L.ref_aaktdi.restype = ctypes.c_double
+    secs = L.ref_aaktdi(ctypes.byref(p), *[_ptr(o) for o in outs])
+    return (*outs, secs)
+
+
+def ref_gentdi(pars: dict, mt: MappedTrajectory):
+    """Reference GenTDI (src/suite/AAKTDI.cc:799-829) on a mapped trajectory."""
+    L = ref_lib()
+    n = (int(pars["length"]) + 1) // 2
+    outs = [np.zeros(n) for _ in TDI_KEYS]
+    L.ref_gentdi(
+        *[_ptr(o) for o in outs], *_genphase_args(pars, mt), ctypes.c_double(pars["D"]),
+        ctypes.c_double(pars["iota"]), ctypes.c_double(pars["gamma"]), ctypes.c_double(mt.Phi0),
+        ctypes.c_double(pars["theta_S"]), ctypes.c_double(pars["phi_S"]), ctypes.c_double(pars["alpha"]),
+        ctypes.c_double(pars["theta_K"]), ctypes.c_double(pars["phi_K"]), _ptr(mt.dt_map), ctypes.c_int(mt.steps),
+        ctypes.c_int(int(bool(pars["backint"]))),
+    )
+    return tuple(outs)
+
+
+def oracle_gentdi(pars: dict, mt: MappedTrajectory, nmodes: int = 0):
+    """The oracle's GenTDI: (TDI_KEYS arrays..., i_plunge of the phase grid)."""
+    L = oracle_lib()
+    n = (int(pars["length"]) + 1) // 2
+    outs = [np.zeros(n) for _ in TDI_KEYS]
+    rows = (_dp * 6)(*[_ptr(o) for o in outs[1:]])
+    ip = ctypes.c_int()
+    rc = L.oracle_gentdi(
+        _ptr(outs[0]), rows, *_genphase_args(pars, mt), ctypes.c_double(pars["D"]), ctypes.c_double(pars["iota"]),
+        ctypes.c_double(pars["gamma"]), ctypes.c_double(mt.Phi0), ctypes.c_double(pars["theta_S"]),
+        ctypes.c_double(pars["phi_S"]), ctypes.c_double(pars["alpha"]), ctypes.c_double(pars["theta_K"]),
+        ctypes.c_double(pars["phi_K"]), _ptr(mt.dt_map), ctypes.c_int(mt.steps),
+        ctypes.c_int(int(bool(pars["backint"]))), ctypes.c_int(int(nmodes)), ctypes.byref(ip),
+    )
+    if rc != 0:
+        raise ValueError("oracle: fitting error, t_0 too close to plunge")
+    return (*outs, ip.value)
+
+
 def _genphase_args(pars: dict, mt: MappedTrajectory):
     return [
         ctypes.c_double(pars["dt"]),

@@ -13,6 +13,8 @@
 //   ref_aakwave    : src/suite/AAKpy.cc:16-51   (AAKwave itself)
 //   ref_aakphase   : src/suite/AAKpy.cc:53-88   (AAKphase itself)
 //   ref_genphase   : src/suite/AAKPhase.cc:315-374 (GenPhase on a mapped trajectory)
+//   ref_aaktdi     : src/suite/AAKpy.cc:90-125  (AAKTDI itself)
+//   ref_gentdi     : src/suite/AAKTDI.cc:799-829 (GenTDI on a mapped trajectory)
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
@@ -31,14 +33,9 @@
 #include "AAKTDI.h"
 #include "AKTDI.h"
 
-// The reference's AAKpy.cc also defines AAKTDI/AKTDI, whose callees live in
-// translation units outside this build.  They are never called through this
-// harness; these definitions only satisfy the linker.
-void GenTDI(double *, double *, double *, double *, double *, double *, double *, double, int, double[], double[],
-            double, double[], double, double, double[], double, double, double, double, double, double, double,
-            double, double, double[], int, bool, bool, bool) {
-  std::abort();
-}
+// The reference's AAKpy.cc also defines AKTDI, whose callee lives in a
+// translation unit outside this build.  It is never called through this
+// harness; this definition only satisfies the linker.
 void GenAKTDI(double *, double *, double *, double *, double *, double *, double *, double, int, double, double,
               double, double, double, double, double, double, double, double, double, double, double, double,
               bool, bool) {
@@ -93,6 +90,24 @@ double ref_aakphase(const ref_params *r, double *t, double *phase_r, double *pha
   SetPar s;
   to_setpar(r, &s);
   return AAKphase(s, t, phase_r, phase_theta, phase_phi, omega_r, omega_theta, omega_phi, eccentricity);
+}
+
+double ref_aaktdi(const ref_params *r, double *f, double *Xr, double *Xi, double *Yr, double *Yi, double *Zr,
+                  double *Zi) {
+  SetPar s;
+  to_setpar(r, &s);
+  return AAKTDI(s, f, Xr, Xi, Yr, Yi, Zr, Zi);
+}
+
+// GenTDI (AAKTDI.cc:799-829) on a mapped trajectory; outputs hold (vlength + 1) / 2 entries.
+void ref_gentdi(double *f, double *Xr, double *Xi, double *Yr, double *Yi, double *Zr, double *Zi, double timestep,
+                int vlength, const double *e_traj, const double *v_map, double M_phys, const double *M_map,
+                double mu, double S_phys, const double *S_map, double dist, double inc, double gim0, double Phi0,
+                double qS, double phiS, double alp0, double qK, double phiK, const double *dt_map, int steps,
+                int backint) {
+  GenTDI(f, Xr, Xi, Yr, Yi, Zr, Zi, timestep, vlength, (double *)e_traj, (double *)v_map, M_phys, (double *)M_map,
+         mu, S_phys, (double *)S_map, dist, inc, gim0, Phi0, qS, phiS, alp0, qK, phiK, (double *)dt_map, steps,
+         backint != 0, false, false);
 }
 
 // GenPhase (AAKPhase.cc:315-374) on a mapped trajectory; outputs hold vlength entries.

@@ -6,8 +6,9 @@ stores its outputs: the mapped trajectory of the front end
 (src/suite/AAKpy.cc:20-44), the waveform of AAKwave with the reference
 harmonic rule, the waveform of waveform() with a harmonic-count override, the
 seven phase arrays of AAKphase (src/suite/AAKpy.cc:53-88, whose time array is
-the AAKwave one), and for some cases the dense PNevolution arrays
-(src/suite/AAK.cc:27-318).
+the AAKwave one), the six frequency-domain TDI arrays of AAKTDI
+(src/suite/AAKpy.cc:90-125, on f = i / ((length - 1) dt)), and for some cases
+the dense PNevolution arrays (src/suite/AAK.cc:27-318).
 
     python tests/golden/make_golden.py
 
@@ -60,6 +61,7 @@ def run_case(name, spec):
     t_g, hI_g, hII_g = O.ref_genwave(pars, mt, nmodes)
     phase = O.ref_aakphase(pars)
     assert np.array_equal(phase[0], t_w)
+    tdi = O.ref_aaktdi(pars)
     out = dict(
         pars=json.dumps(pars),
         nmodes=np.int32(nmodes),
@@ -80,6 +82,8 @@ def run_case(name, spec):
     )
     for k, a in zip(O.PHASE_KEYS[1:], phase[1:8]):
         out["aakphase_" + k] = a
+    for k, a in zip(O.TDI_KEYS[1:], tdi[1:7]):
+        out["aaktdi_" + k] = a
     if dense:
         arrs, ip, ib = O.ref_pnevolution(pars, mt)
         for k, a in zip("t e v M S gim Phi alp nu gimdot".split(), arrs):
