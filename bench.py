@@ -376,6 +376,51 @@ def ref_phase_rate(sources, n_src: int = 16, sample_len: int = 200000) -> dict:
                       "(front end + GenPhase), one process"}
 
 
+def run_tdi(sources, local_rank: int, nthreads: int, n_ref: int = 4) -> dict:
+    """Frequency-domain AAK TDI (AAKwrapper.tdi) of 16 configuration-1 sources in
+    one batch, end to end through aak_tdi_batch_host (host front end and grid
+    planning, the phase-grid and stationary-phase kernels, copies back); the
+    reference's own AAKTDI timed on the first n_ref of them, one process."""
+    import emri_kludge_suite_b200 as E
+    from oracle import oracle as O
+
+    sub = sources[:: max(1, len(sources) // 16)][:16]
+    wb = E.WaveBatch(local_rank)
+    wb.tdi_host(sub[:2], nthreads=nthreads)  # warm-up (context, buffers)
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        rows, offs, st = wb.tdi_host(sub, nthreads=nthreads)
+        times.append(time.perf_counter() - t0)
+    wall = float(np.mean(times))
+    bins = int(offs[-1])
+    wb.close()
+    res = {"workload": "frequency-domain AAK TDI (X, Y, Z on f = i / T) of 16 configuration-1 sources (every 32nd), "
+                       "reference harmonic rule, FP64",
+           "sources": len(sub), "failed": int(np.sum(st != 0)), "bins": bins, "seconds_per_batch": wall,
+           "sources_per_s": len(sub) / wall, "bins_per_s": bins / wall, "gpu_launches_per_batch": 4,
+           "e2e": {"value": len(sub) / wall, "unit": "TDI waveforms/s", "h2d_bytes_per_step": None,
+                   "d2h_bytes_per_step": 48 * bins}}
+    if O.ref_available():
+        # the reference keeps 30 complex transfer-function rows per harmonic on its phase grid
+        # (0.01 M^2 / mu spacing): time it on sources whose grid stays below 2e5 points
+        def grid_points(p):
+            return (int(p["length"]) - 1) * p["dt"] / (0.01 * p["M"] ** 2 / p["mu"] * MSUN_SEC)
+
+        ref_src = [p for p in sub if grid_points(p) < 2e5][:n_ref]
+        t0 = time.perf_counter()
+        nb = 0
+        for p in ref_src:
+            O.ref_aaktdi(p)
+            nb += (int(p["length"]) + 1) // 2
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": len(ref_src) / dt, "unit": "TDI waveforms/s", "cores": 1,
+                               "kind": "reference", "bins_per_s": nb / dt,
+                               "sample": f"reference AAKTDI (front end + GenTDI) on {len(ref_src)} of the same sources "
+                                         "(phase grids below 2e5 points), one process"}
+    return res
+
+
 def run_phases(args, wb, sources, sptr, stream, N, N_all, reduce_max, local_rank, nthreads):
     """AAK phase product (GenPhase: t, 3 phases, 3 rates, e per sample, FP64) of
     the uploaded configuration-1 batch: device-resident kernel time, roofline,
@@ -594,6 +639,9 @@ def run_gpu(args, rank, world, local_rank):
     del hI2, hII2
     split = {"value": value, "kernel_ms": {"clears": kern_s[0], "waveform_split": kern_s[2]}}
 
+    # ---- frequency-domain TDI of a subset of the batch
+    tdi = run_tdi(sources, local_rank, nthreads) if args.tdi and rank == 0 else None
+
     # ---- AAK phase product of the same batch
     phases = None
     if args.phases:
@@ -732,6 +780,7 @@ def run_gpu(args, rank, world, local_rank):
         "fp64_path": fp64,
         "plain_fp64_per_source": plain,
         "phase_product": phases,
+        "tdi": tdi,
         "roofline": roofline,
         "clocks": clk,
         "e2e": e2e,
@@ -765,6 +814,7 @@ def main():
     ap.add_argument("--plain-sources", type=int, default=16,
                     help="sources of the plain FP64 per-source baseline (0: skip)")
     ap.add_argument("--fisher", type=int, default=8, help="Fisher matrices to time at config-4 points (0: skip)")
+    ap.add_argument("--tdi", type=int, default=1, help="time the frequency-domain TDI of 16 sources (0: skip)")
     ap.add_argument("--phases", type=int, default=1, help="time the AAK phase product of the batch (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,
                     help="config-3 training points of the warm-start network (0: skip)")

@@ -13,6 +13,7 @@ Profiling workloads (run from the repository root on one GPU)::
     python -m emri_kludge_suite_b200.workloads waveform   # 16 of the 512 sources, FP64 and split, twice each
     python -m emri_kludge_suite_b200.workloads phase      # the phase product of the same 16 sources, twice
     python -m emri_kludge_suite_b200.workloads fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
+    python -m emri_kludge_suite_b200.workloads tdi        # frequency-domain TDI of the waveform workload's 16 sources, twice
     python -m emri_kludge_suite_b200.workloads mlp        # warm-start network: forward on 2^20 points, a training step
 """
 from __future__ import annotations
@@ -125,6 +126,18 @@ def profile_fisher():
     print("fisher workload: 28 x", length, "samples")
 
 
+def profile_tdi():
+    """The frequency-domain TDI of the same 16 sources as the waveform workload, twice."""
+    from .aak import WaveBatch
+
+    src, _ = config1(SEED, 512)
+    wb = WaveBatch(0)
+    for _ in range(2):
+        rows, offs, st = wb.tdi_host(src[::32][:16])
+    assert np.all(st == 0) and np.all(np.isfinite(rows))
+    print("tdi workload:", int(offs[-1]), "bins")
+
+
 def profile_mlp():
     import torch
 
@@ -146,4 +159,4 @@ def profile_mlp():
 
 if __name__ == "__main__":
     {"waveform": profile_waveform, "phase": profile_phase, "fisher": profile_fisher,
-     "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
+     "tdi": profile_tdi, "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
