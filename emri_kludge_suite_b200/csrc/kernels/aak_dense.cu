@@ -1823,72 +1823,138 @@ __global__ void __launch_bounds__(256) k_tdi_zero(double *out, int64_t n) {
     out[j] = 0.0;
 }
 
-__global__ void __launch_bounds__(256) k_tdi_spa(TdiArgs a) {
-  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < a.total_work;
-       w += (int64_t)gridDim.x * blockDim.x) {
-    int lo = 0, hi = a.nsrc - 1;  // source holding work item w
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (a.work_start[mid] <= w) lo = mid;
-      else hi = mid - 1;
+// Per-item state of the stationary-phase sum, kept in shared memory while the
+// warp spreads the item's bins over its lanes.
+struct TdiItem {
+  double t0, t1, om_in, delom, xi_in, dxi, dd0, dd1, fz0, fz1, A0, A1, e0, e1, omT0, omT1;
+  double2 F0[6], F1[6];
+  int s, j, lo, pad;
+};
+constexpr int kTdiWarps = 4;  // warps per CTA of k_tdi_spa
+
+// Each warp takes 32 consecutive work items (source, interval, harmonic n,
+// sideband m).  A lane finds its item's bins (most items cross none: a
+// harmonic moves by far less than a bin over one grid interval) and, if it
+// has some, stages the item's end-point quantities in shared memory.  The
+// transfer functions of the items with bins (two per item, one per end) are
+// then dealt out over the lanes, and a warp scan of the bin counts deals the
+// warp's bins out one per lane, so that both heavy parts (constellation and
+// transfer functions; Bessel recurrence, phase, interpolation, atomic adds)
+// run with full warps.
+__global__ void __launch_bounds__(kTdiWarps * 32) k_tdi_spa(TdiArgs a) {
+  __shared__ TdiItem items[kTdiWarps][32];
+  __shared__ int incl_s[kTdiWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  TdiItem *my = items[warp];
+  int *incl_w = incl_s[warp];
+  const double orbOm = 2. * kPi / kYear;
+  const int64_t stride = (int64_t)gridDim.x * kTdiWarps * 32;
+  for (int64_t base = ((int64_t)blockIdx.x * kTdiWarps + warp) * 32; base < a.total_work; base += stride) {
+    const int64_t w = base + lane;
+    int cnt = 0;
+    if (w < a.total_work) {
+      int lo = 0, hi = a.nsrc - 1;  // source holding work item w
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.work_start[mid] <= w) lo = mid;
+        else hi = mid - 1;
+      }
+      const TdiDesc &d = a.src[lo];
+      const int64_t local = w - a.work_start[lo];
+      const int nh = 5 * d.nmodes;
+      const int i = 1 + (int)(local / nh), ind = (int)(local % nh);
+      const int j = ind / 5, jj = ind - 5 * j;
+      const double nn = j + 1, mm = jj - 2.;
+      const int64_t st = a.grid_stride, g = d.grid_offset;
+      const double *G = a.grid;
+      const double nu0 = G[kTdiNu * st + g + i - 1], nu1 = G[kTdiNu * st + g + i];
+      const double gd0 = G[kTdiGd * st + g + i - 1], gd1 = G[kTdiGd * st + g + i];
+      const double ad0 = G[kTdiAd * st + g + i - 1], ad1 = G[kTdiAd * st + g + i];
+      const double om_in = nn * 2. * kPi * nu0 + 2. * gd0 + mm * ad0;
+      const double om_fin = nn * 2. * kPi * nu1 + 2. * gd1 + mm * ad1;
+      // bins ceil(om_in / dOm) .. floor(om_fin / dOm), the last one dropped when
+      // om_fin falls on it (AAKTDI.cc:705-713); kept in doubles until clamped.
+      // No bin lies in a falling, negative or NaN range.
+      if (d.status == 0 && om_in > 0.0 && om_fin > om_in) {
+        const double lo_b = ceil(om_in / d.dOm);
+        double up_b = floor(om_fin / d.dOm);
+        if (om_fin == up_b * d.dOm) up_b -= 1.0;
+        const double mx_b = fmin(up_b + 1.0, (double)d.nbins);
+        if (lo_b < mx_b) {
+          cnt = (int)(mx_b - lo_b);
+          TdiItem &it = my[lane];
+          it.s = lo;
+          it.j = ind;
+          it.lo = (int)lo_b;
+          it.om_in = om_in;
+          it.delom = om_fin - om_in;
+          it.t0 = G[kTdiT * st + g + i - 1];
+          it.t1 = G[kTdiT * st + g + i];
+          it.xi_in = it.t0 - d.DM * cos(orbOm * it.t0 - d.phiS);
+          it.dxi = (it.t1 - d.DM * cos(orbOm * it.t1 - d.phiS)) - it.xi_in;
+          it.dd0 = nn * tdi_ddot(G, kTdiNu * st + g, i - 1, d.i0, d.ip, 2. * kPi, d.dt_ph) +
+                   2. * tdi_ddot(G, kTdiGd * st + g, i - 1, d.i0, d.ip, 1.0, d.dt_ph) +
+                   mm * tdi_ddot(G, kTdiAd * st + g, i - 1, d.i0, d.ip, 1.0, d.dt_ph);
+          it.dd1 = nn * tdi_ddot(G, kTdiNu * st + g, i, d.i0, d.ip, 2. * kPi, d.dt_ph) +
+                   2. * tdi_ddot(G, kTdiGd * st + g, i, d.i0, d.ip, 1.0, d.dt_ph) +
+                   mm * tdi_ddot(G, kTdiAd * st + g, i, d.i0, d.ip, 1.0, d.dt_ph);
+          it.fz0 = nn * G[kTdiPhi * st + g + i - 1] + 2. * G[kTdiGim * st + g + i - 1] + mm * G[kTdiAlp * st + g + i - 1];
+          it.fz1 = nn * G[kTdiPhi * st + g + i] + 2. * G[kTdiGim * st + g + i] + mm * G[kTdiAlp * st + g + i];
+          it.A0 = G[kTdiAmp * st + g + i - 1];
+          it.A1 = G[kTdiAmp * st + g + i];
+          it.e0 = G[kTdiE * st + g + i - 1];
+          it.e1 = G[kTdiE * st + g + i];
+          it.omT0 = nn * G[kTdiPd * st + g + i - 1] + 2. * gd0 + mm * ad0;
+          it.omT1 = nn * G[kTdiPd * st + g + i] + 2. * gd1 + mm * ad1;
+        }
+      }
     }
-    const TdiDesc &d = a.src[lo];
-    if (d.status != 0) continue;
-    const int64_t local = w - a.work_start[lo];
-    const int nh = 5 * d.nmodes;
-    const int i = 1 + (int)(local / nh), ind = (int)(local % nh);
-    const int j = ind / 5, jj = ind - 5 * j;
-    const double nn = j + 1, mm = jj - 2.;
-    const int64_t st = a.grid_stride, g = d.grid_offset;
-    const double *G = a.grid;
-    const double nu0 = G[kTdiNu * st + g + i - 1], nu1 = G[kTdiNu * st + g + i];
-    const double gd0 = G[kTdiGd * st + g + i - 1], gd1 = G[kTdiGd * st + g + i];
-    const double ad0 = G[kTdiAd * st + g + i - 1], ad1 = G[kTdiAd * st + g + i];
-    const double om_in = nn * 2. * kPi * nu0 + 2. * gd0 + mm * ad0;
-    const double om_fin = nn * 2. * kPi * nu1 + 2. * gd1 + mm * ad1;
-    if (om_in == 0. || om_fin == 0.) continue;
-    if (!(om_in > 0.0) || !(om_fin > om_in)) continue;  // no bin lies in a falling, negative or NaN range
-    // bins ceil(om_in / dOm) .. floor(om_fin / dOm), the last one dropped when
-    // om_fin falls on it (AAKTDI.cc:705-713); kept in doubles until clamped
-    const double lo_b = ceil(om_in / d.dOm);
-    double up_b = floor(om_fin / d.dOm);
-    if (om_fin == up_b * d.dOm) up_b -= 1.0;
-    const double mx_b = fmin(up_b + 1.0, (double)d.nbins);
-    if (!(lo_b < mx_b)) continue;
-    const int ind_low = (int)lo_b, ind_max = (int)mx_b;
-    // the interval's end points
-    const double t0 = G[kTdiT * st + g + i - 1], t1 = G[kTdiT * st + g + i];
-    const double orbOm = 2. * kPi / kYear;
-    const double xi_in = t0 - d.DM * cos(orbOm * t0 - d.phiS);
-    const double xi_fin = t1 - d.DM * cos(orbOm * t1 - d.phiS);
-    const double dxi = xi_fin - xi_in, delom = om_fin - om_in;
-    const double dd0 = nn * tdi_ddot(G, kTdiNu * st + g, i - 1, d.i0, d.ip, 2. * kPi, d.dt_ph) +
-                       2. * tdi_ddot(G, kTdiGd * st + g, i - 1, d.i0, d.ip, 1.0, d.dt_ph) +
-                       mm * tdi_ddot(G, kTdiAd * st + g, i - 1, d.i0, d.ip, 1.0, d.dt_ph);
-    const double dd1 = nn * tdi_ddot(G, kTdiNu * st + g, i, d.i0, d.ip, 2. * kPi, d.dt_ph) +
-                       2. * tdi_ddot(G, kTdiGd * st + g, i, d.i0, d.ip, 1.0, d.dt_ph) +
-                       mm * tdi_ddot(G, kTdiAd * st + g, i, d.i0, d.ip, 1.0, d.dt_ph);
-    const double fz0 = nn * G[kTdiPhi * st + g + i - 1] + 2. * G[kTdiGim * st + g + i - 1] + mm * G[kTdiAlp * st + g + i - 1];
-    const double fz1 = nn * G[kTdiPhi * st + g + i] + 2. * G[kTdiGim * st + g + i] + mm * G[kTdiAlp * st + g + i];
-    const double A0 = G[kTdiAmp * st + g + i - 1], A1 = G[kTdiAmp * st + g + i];
-    const double e0 = G[kTdiE * st + g + i - 1], e1 = G[kTdiE * st + g + i];
-    double2 F0[6], F1[6];
-    tdi_transfer(d, t0, nn * G[kTdiPd * st + g + i - 1] + 2. * gd0 + mm * ad0, F0);
-    tdi_transfer(d, t1, nn * G[kTdiPd * st + g + i] + 2. * gd1 + mm * ad1, F1);
-    const double Apc0 = d.AA[jj], Aps0 = d.AA[5 + jj], Acc0 = 2. * d.AA[10 + jj], Acs0 = 2. * d.AA[15 + jj];
-    const int32_t bstart = a.bessel_start[d.bessel_offset + j];
-    for (int ii = ind_low; ii < ind_max; ++ii) {
+    // warp scan of the bin counts
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) continue;  // warp-uniform
+    incl_w[lane] = incl;
+    // transfer functions: task t is end (t & 1) of the (t >> 1)-th item with bins
+    const unsigned act = __ballot_sync(0xffffffffu, cnt > 0);
+    const int nact = __popc(act);
+    __syncwarp();
+    for (int t = lane; t < 2 * nact; t += 32) {
+      unsigned m = act;
+      for (int r = t >> 1; r > 0; --r) m &= m - 1;  // drop the lower set bits
+      TdiItem &it = my[__ffs(m) - 1];
+      const bool hi_end = t & 1;
+      tdi_transfer(a.src[it.s], hi_end ? it.t1 : it.t0, hi_end ? it.omT1 : it.omT0, hi_end ? it.F1 : it.F0);
+    }
+    __syncwarp();
+    for (int b = lane; b < total; b += 32) {
+      int l = 0, h = 31;  // owner: first lane whose inclusive count exceeds b
+      while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (incl_w[mid] > b) h = mid;
+        else l = mid + 1;
+      }
+      const TdiItem &it = my[l];
+      const TdiDesc &d = a.src[it.s];
+      const int ii = it.lo + (b - (l > 0 ? incl_w[l - 1] : 0));
+      const int j = it.j / 5, jj = it.j - 5 * j;
+      const double nn = j + 1;
       const double Om = (double)ii * d.dOm;
-      double delta = (Om - om_in) / delom, eps = 1. - delta;
-      const double T = t1 * delta + t0 * eps;
+      double delta = (Om - it.om_in) / it.delom, eps = 1. - delta;
+      const double T = it.t1 * delta + it.t0 * eps;
       const double xi = T - d.DM * cos(orbOm * T - d.phiS);
-      delta = (xi - xi_in) / dxi;
+      delta = (xi - it.xi_in) / it.dxi;
       eps = 1. - delta;
-      const double dom = dd0 * eps + dd1 * delta;
-      const double faza = fz0 * eps + fz1 * delta;
-      const double amp = A0 * eps + A1 * delta;
-      const double ec = e0 * eps + e1 * delta;
+      const double dom = it.dd0 * eps + it.dd1 * delta;
+      const double faza = it.fz0 * eps + it.fz1 * delta;
+      const double amp = it.A0 * eps + it.A1 * delta;
+      const double ec = it.e0 * eps + it.e1 * delta;
       const double ne = nn * ec;
+      const int32_t bstart = a.bessel_start[d.bessel_offset + j];
       double J[5];
       if (!(ne > 0.0)) {
         for (int m = 0; m < 5; ++m) J[m] = 0.0;
@@ -1907,9 +1973,10 @@ __global__ void __launch_bounds__(256) k_tdi_spa(TdiArgs a) {
       }
       const double hamp = -nn * ((J[0] - 2. * ec * J[1] + 2. / nn * J[2] + 2. * ec * J[3] - J[4]) +
                                  sqrt(1 - ec * ec) * (J[0] - 2. * J[2] + J[4]));
-      delta = (T - t0) / d.dt_ph;
+      delta = (T - it.t0) / d.dt_ph;
       eps = 1. - delta;
-      const double Apc = hamp * Apc0, Aps = hamp * Aps0, Acc = hamp * Acc0, Acs = hamp * Acs0;
+      const double Apc = hamp * d.AA[jj], Aps = hamp * d.AA[5 + jj];
+      const double Acc = hamp * (2. * d.AA[10 + jj]), Acs = hamp * (2. * d.AA[15 + jj]);
       double sinph, cosph;
       sincos(faza - Om * xi + kPi * 0.25, &sinph, &cosph);
       const double fact = 0.5 * amp * sqrt(2. * kPi / dom);
@@ -1918,21 +1985,23 @@ __global__ void __launch_bounds__(256) k_tdi_spa(TdiArgs a) {
       const int64_t o = d.bin_offset + ii;
 #pragma unroll
       for (int ch = 0; ch < 3; ++ch) {
-        const double2 cFp = cadd(cscale(eps, F0[2 * ch]), cscale(delta, F1[2 * ch]));
-        const double2 cFc = cadd(cscale(eps, F0[2 * ch + 1]), cscale(delta, F1[2 * ch + 1]));
+        const double2 cFp = cadd(cscale(eps, it.F0[2 * ch]), cscale(delta, it.F1[2 * ch]));
+        const double2 cFc = cadd(cscale(eps, it.F0[2 * ch + 1]), cscale(delta, it.F1[2 * ch + 1]));
         const double2 r = cadd(cmul(cFp, xp), cmul(cFc, xc));
         atomicAdd(a.out + (2 * ch) * a.out_stride + o, r.x);
         atomicAdd(a.out + (2 * ch + 1) * a.out_stride + o, r.y);
       }
     }
+    __syncwarp();  // the items and counts are reused by the next chunk
   }
 }
 
 void launch_tdi_spa(const TdiArgs &a, cudaStream_t stream) {
   if (a.out_stride > 0) k_tdi_zero<<<1184, 256, 0, stream>>>(a.out, 6 * a.out_stride);
   if (a.total_work <= 0) return;
-  const int64_t blocks = std::min<int64_t>((a.total_work + 255) / 256, 148 * 64);
-  k_tdi_spa<<<(unsigned)blocks, 256, 0, stream>>>(a);
+  constexpr int per_block = kTdiWarps * 32;
+  const int64_t blocks = std::min<int64_t>((a.total_work + per_block - 1) / per_block, 148 * 64);
+  k_tdi_spa<<<(unsigned)blocks, per_block, 0, stream>>>(a);
 }
 
 namespace {
