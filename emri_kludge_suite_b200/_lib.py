@@ -166,6 +166,8 @@ def lib():
     L.aak_ctx_set_parmap_model.argtypes = [_vp, _vp]
     L.aak_batch_newton_stats.argtypes = [_vp, _i64p, _i64p, _i64p]
     L.aak_gpu_set_parmap_model.argtypes = [_vp, _vp]
+    L.aak_ctx_set_parmap_device.argtypes = [_vp, _i32]
+    L.aak_gpu_set_parmap_device.argtypes = [_vp, _i32]
     _lib = L
     return L
 

@@ -192,6 +192,11 @@ class WaveBatch:
         check(lib().aak_ctx_set_parmap_model(self._ctx, model.handle if model is not None else None),
               "aak_ctx_set_parmap_model")
 
+    def set_parmap_device(self, on: bool = True):
+        """Solve the Kerr->AK map of all coarse points of a batch on the GPU (one
+        launch) instead of on the planning threads; results are bit-identical."""
+        check(lib().aak_ctx_set_parmap_device(self._ctx, int(bool(on))), "aak_ctx_set_parmap_device")
+
     def newton_stats(self) -> dict:
         """Map statistics of the last plan: points, Newton iterations, fallbacks."""
         a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

@@ -25,6 +25,9 @@ LIB = os.path.join(PKG, "libaak_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", os.path.join(REPO, "include")]
 
+# per-file flags: the device map solve must round as the host does (no FMA contraction)
+FILE_FLAGS = {"kernels/parmap_newton.cu": ["-fmad=false"]}
+
 SOURCES = [
     "host/kerr.cpp",
     "host/inspiral.cpp",
@@ -33,6 +36,7 @@ SOURCES = [
     "kernels/aak_dense.cu",
     "kernels/likelihood.cu",
     "kernels/parmap_mlp.cu",
+    "kernels/parmap_newton.cu",
     "capi/aak_capi.cpp",
     "capi/mlp_capi.cpp",
 ]
@@ -71,7 +75,7 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
         obj = os.path.join(BUILD, rel.replace("/", "_") + ".o")
         objs.append(obj)
         if force or _stale(obj, [src] + hdrs):
-            cmd = [cc, *ARCH, *COMMON, *extra, "-c", src, "-o", obj]
+            cmd = [cc, *ARCH, *COMMON, *FILE_FLAGS.get(rel, []), *extra, "-c", src, "-o", obj]
             if rel.endswith(".cu"):
                 cmd[1:1] = ["-Xptxas", "-v"] if verbose else []
             jobs.append(cmd)

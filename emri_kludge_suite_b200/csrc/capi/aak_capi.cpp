@@ -23,6 +23,7 @@
 #include "../host/pipeline.hpp"
 #include "../kernels/aak_dense.cuh"
 #include "../kernels/likelihood.cuh"
+#include "../kernels/parmap_newton.cuh"
 #include "errors.hpp"
 #include "mlp_model.hpp"
 
@@ -93,6 +94,12 @@ struct aak_ctx {
   DevBuf<int32_t> d_flag;                 // look-back flags, one per tile
   DevBuf<unsigned long long> d_counter;   // [0] work-queue head, [1] device status word
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
+  // batched device solve of the Kerr -> AK map (opt-in: parmap_device)
+  bool parmap_device = false;
+  DevBuf<ParmapJob> d_pm_jobs;
+  DevBuf<double> d_pm_warm, d_pm_map;
+  DevBuf<int32_t> d_pm_it;
+  cudaStream_t pm_stream = nullptr;
   DevBuf<TdiDesc> d_tdi;        // frequency-domain TDI: per-source stationary-phase records
   DevBuf<int64_t> d_tdi_work;   //   and the prefix of their work items
   int last_launches = 0;
@@ -372,7 +379,8 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   // warm-start model needs every coarse point at once, else inside each
   // source's planning task (the long sources then start at once)
   std::vector<CoarseKerr> ck(nsrc);
-  const bool fused = !ctx->model;
+  const bool dev_map = ctx->parmap_device && dev >= 0;
+  const bool fused = !ctx->model && !dev_map;
   if (!fused)
     parallel_for(nsrc, nthreads, [&](int64_t s) {
       const Params Pp = to_params(Pv[s]);
@@ -383,8 +391,9 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   // (2) optional learned warm start: every coarse point of the batch in one launch
   std::vector<int64_t> first(nsrc + 1, 0);
   std::vector<double> warm;
-  if (ctx->model) {
+  if (!fused)
     for (int s = 0; s < nsrc; ++s) first[s + 1] = first[s] + (ctx->status[s] == kOk ? ck[s].steps : 0);
+  if (ctx->model) {
     const int64_t np = first[nsrc];
     std::vector<double> xs(4 * np), ys(3 * np);
     for (int s = 0; s < nsrc; ++s)
@@ -400,6 +409,53 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     warm.resize(3 * np);
     for (int s = 0; s < nsrc; ++s)
       for (int64_t i = first[s]; i < first[s + 1]; ++i) parmap_from_coords(&xs[4 * i], Pv[s].M, &ys[3 * i], &warm[3 * i]);
+  }
+  // (2b) optional device solve of the map: every coarse point of the batch in
+  // one launch (the same root as the host solve, bit for bit)
+  std::vector<double> dmap;
+  std::vector<int32_t> dit;
+  if (dev_map) {
+    on_device();
+    const int64_t np = first[nsrc];
+    std::vector<ParmapJob> jobs(np);
+    for (int s = 0; s < nsrc; ++s) {
+      const double Y = std::cos(Pv[s].iota);
+      for (int64_t i = 0; i < first[s + 1] - first[s]; ++i) {
+        ParmapJob &j = jobs[first[s] + i];
+        for (int k = 0; k < 3; ++k) j.Om[k] = ck[s].Omega[i][k];
+        j.p = ck[s].p[i];
+        j.M = Pv[s].M;
+        j.s = Pv[s].s;
+        j.e = ck[s].e[i];
+        j.Y = Y;
+      }
+    }
+    dmap.assign(3 * np, 0.0);
+    dit.assign(2 * np, 0);
+    if (np > 0) {
+      int r;
+      if (!ctx->pm_stream &&
+          (r = cuda_ok(cudaStreamCreateWithFlags(&ctx->pm_stream, cudaStreamNonBlocking))) != AAK_OK)
+        return r;
+      if ((r = ctx->d_pm_jobs.reserve(np)) || (r = ctx->d_pm_map.reserve(3 * np)) ||
+          (r = ctx->d_pm_it.reserve(2 * np)) || (!warm.empty() && (r = ctx->d_pm_warm.reserve(3 * np))))
+        return r;
+      cudaStream_t st = ctx->pm_stream;
+      if ((r = cuda_ok(cudaMemcpyAsync(ctx->d_pm_jobs.ptr, jobs.data(), np * sizeof(ParmapJob),
+                                       cudaMemcpyHostToDevice, st))) ||
+          (!warm.empty() && (r = cuda_ok(cudaMemcpyAsync(ctx->d_pm_warm.ptr, warm.data(), 3 * np * sizeof(double),
+                                                         cudaMemcpyHostToDevice, st)))))
+        return r;
+      launch_parmap_newton(ctx->d_pm_jobs.ptr, np, warm.empty() ? nullptr : ctx->d_pm_warm.ptr, ctx->d_pm_map.ptr,
+                           ctx->d_pm_it.ptr, ctx->d_pm_it.ptr + np, st);
+      if ((r = cuda_ok(cudaGetLastError())) ||
+          (r = cuda_ok(cudaMemcpyAsync(dmap.data(), ctx->d_pm_map.ptr, 3 * np * sizeof(double),
+                                       cudaMemcpyDeviceToHost, st))) ||
+          (r = cuda_ok(cudaMemcpyAsync(dit.data(), ctx->d_pm_it.ptr, 2 * np * sizeof(int32_t),
+                                       cudaMemcpyDeviceToHost, st))) ||
+          (r = cuda_ok(cudaStreamSynchronize(st))))
+        return r;
+    }
   }
   // (3) Kerr -> AK map, coarse AK evolution, knots; largest sources first.
   // A source's knot count is about (steps - 1) max(1, r / T_fit), r its
@@ -441,7 +497,35 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
       ctx->status[s] = st0;
     }
     int st = ctx->status[s];
-    if (st == kOk) {
+    if (st == kOk && dev_map) {
+      // the device-solved map of this source's coarse points (map_coarse's layout)
+      const CoarseKerr &c = ck[s];
+      const int64_t np = first[nsrc], f0 = first[s];
+      mt->steps = c.steps;
+      mt->inspiral_flag = c.inspiral_flag;
+      mt->Phi0 = initial_mean_anomaly(Pp.e, Pp.psi);
+      mt->newton_iterations = 0;
+      int fb = 0;
+      for (int i = 0; i < c.steps && st == kOk; ++i) {
+        const int it = dit[f0 + i];
+        if (it < 0) {
+          st = kErrSolverNoConverge;
+          break;
+        }
+        mt->newton_iterations += it;
+        fb += dit[np + f0 + i];
+        mt->e_traj[i] = c.e[i];
+        mt->v_map[i] = dmap[3 * (f0 + i)];
+        mt->M_map[i] = dmap[3 * (f0 + i) + 1];
+        mt->s_map[i] = dmap[3 * (f0 + i) + 2];
+        mt->dt_map[i] = c.t_rr[i] * kMsunSec * Pp.M * Pp.M / Pp.mu;
+      }
+      if (st == kOk) {
+        points += c.steps;
+        iters += mt->newton_iterations;
+        fallbacks += fb;
+      }
+    } else if (st == kOk) {
       int fb = 0;
       st = map_coarse(Pp, ck[s], mt, warm.empty() ? nullptr : &warm[3 * first[s]], &fb);
       if (st == kOk) {
@@ -1162,6 +1246,11 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_out.release();
     c->d_tdi.release();
     c->d_tdi_work.release();
+    c->d_pm_jobs.release();
+    c->d_pm_warm.release();
+    c->d_pm_map.release();
+    c->d_pm_it.release();
+    if (c->pm_stream) cudaStreamDestroy(c->pm_stream);
     for (auto &e : c->ev)
       if (e) cudaEventDestroy(e);
     drop_graph(c);
@@ -1918,6 +2007,18 @@ int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, i
   if (!g) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(g->ctx->mu);
   return gpu_fisher(g, params, nd, scale, nthreads, gram, status);
+}
+
+int aak_ctx_set_parmap_device(aak_ctx *ctx, int32_t on) {
+  if (!ctx || (on && ctx->device < 0)) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->parmap_device = on != 0;
+  return AAK_OK;
+}
+
+int aak_gpu_set_parmap_device(aak_gpu *g, int32_t on) {
+  if (!g) return AAK_ERR_INVALID_PARAM;
+  return aak_ctx_set_parmap_device(g->ctx, on);
 }
 
 int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m) {

@@ -52,122 +52,10 @@ int coarse_kerr(const Params &P, CoarseKerr *out) {
   return kOk;
 }
 
-namespace {
-// Kerr->AK residual: Omega_k M_map - Omega_k^PN(v_map, s_map) M  (KSParMap.cc:323-358)
-void parmap_residual(const double Om[3], double M, double e, double Y, const double x[3], double f[3]) {
-  const double v = x[0], Mm = x[1], s = x[2];
-  double Or, Ot, Op;
-  const double inv2pi = 1.0 / (2.0 * kPi);
-  if (Y > 0) {
-    const double tm = pn_dtdm(v, e, Y, s);
-    Or = pn_drdm(v, e, Y, s) / tm / 2. / kPi;
-    Ot = pn_dthetadm(v, e, Y, s) / tm / 2. / kPi;
-    Op = pn_dphidm(v, e, Y, s) / tm / 2. / kPi;
-  } else {
-    const double tm = pn_dtdm(v, e, -Y, -s);
-    Or = pn_drdm(v, e, -Y, -s) / tm / 2. / kPi;
-    Ot = pn_dthetadm(v, e, -Y, -s) / tm / 2. / kPi;
-    Op = -pn_dphidm(v, e, -Y, -s) / tm / 2. / kPi;
-  }
-  (void)inv2pi;
-  f[0] = Om[0] * Mm - Or * M;
-  f[1] = Om[1] * Mm - Ot * M;
-  f[2] = Om[2] * Mm - Op * M;
-}
-inline double norm1(const double f[3]) { return std::fabs(f[0]) + std::fabs(f[1]) + std::fabs(f[2]); }
-
-bool solve3(double A[3][3], double b[3], double x[3]) {
-  int piv[3] = {0, 1, 2};
-  for (int k = 0; k < 3; ++k) {
-    int p = k;
-    for (int i = k + 1; i < 3; ++i)
-      if (std::fabs(A[i][k]) > std::fabs(A[p][k])) p = i;
-    if (A[p][k] == 0.0) return false;
-    if (p != k) {
-      for (int j = 0; j < 3; ++j) std::swap(A[k][j], A[p][j]);
-      std::swap(b[k], b[p]);
-      std::swap(piv[k], piv[p]);
-    }
-    for (int i = k + 1; i < 3; ++i) {
-      const double m = A[i][k] / A[k][k];
-      for (int j = k; j < 3; ++j) A[i][j] -= m * A[k][j];
-      b[i] -= m * b[k];
-    }
-  }
-  for (int k = 2; k >= 0; --k) {
-    double s = b[k];
-    for (int j = k + 1; j < 3; ++j) s -= A[k][j] * x[j];
-    x[k] = s / A[k][k];
-  }
-  return true;
-}
-}  // namespace
-
+// The map solve itself is parmap_newton.hpp's (shared with the device batch).
 int parmap(const double Om[3], double p, double M, double s, double e, double iota, const double *x0, double map[3],
            int *iters_to_tol) {
-  const double Y = std::cos(iota);
-  double x[3];
-  if (x0) {
-    x[0] = x0[0];
-    x[1] = x0[1];
-    x[2] = x0[2];
-  } else {
-    x[0] = 1. / std::sqrt(p);
-    x[1] = M;
-    x[2] = s;
-  }
-  double f[3];
-  parmap_residual(Om, M, e, Y, x, f);
-  int iters = 0;
-  bool reached = norm1(f) < 1e-6;
-  if (iters_to_tol) *iters_to_tol = reached ? 0 : -1;
-  for (int it = 0; it < 200; ++it) {
-    // Jacobian: central differences in v_map and s_map, exact in M_map
-    double J[3][3];
-    for (int col : {0, 2}) {
-      const double h = 1e-6 * std::max(std::fabs(x[col]), 1e-2);
-      double xp[3] = {x[0], x[1], x[2]}, xm[3] = {x[0], x[1], x[2]}, fp[3], fm[3];
-      xp[col] += h;
-      xm[col] -= h;
-      parmap_residual(Om, M, e, Y, xp, fp);
-      parmap_residual(Om, M, e, Y, xm, fm);
-      const double hh = xp[col] - xm[col];
-      for (int r = 0; r < 3; ++r) J[r][col] = (fp[r] - fm[r]) / hh;
-    }
-    for (int r = 0; r < 3; ++r) J[r][1] = Om[r];
-    double rhs[3] = {-f[0], -f[1], -f[2]}, dx[3];
-    if (!solve3(J, rhs, dx)) break;
-    double lam = 1.0, xt[3], ft[3];
-    bool ok = false;
-    for (int ls = 0; ls < 40; ++ls) {
-      for (int i = 0; i < 3; ++i) xt[i] = x[i] + lam * dx[i];
-      parmap_residual(Om, M, e, Y, xt, ft);
-      if (std::isfinite(ft[0]) && std::isfinite(ft[1]) && std::isfinite(ft[2]) && norm1(ft) < norm1(f)) {
-        ok = true;
-        break;
-      }
-      lam *= 0.5;
-    }
-    if (!ok) break;  // no further decrease: at the rounding floor (or stuck)
-    double rel = 0.0;
-    for (int i = 0; i < 3; ++i) rel = std::max(rel, std::fabs(xt[i] - x[i]) / std::max(std::fabs(x[i]), 1e-300));
-    for (int i = 0; i < 3; ++i) {
-      x[i] = xt[i];
-      f[i] = ft[i];
-    }
-    ++iters;
-    if (norm1(f) < 1e-6 && !reached) {
-      reached = true;
-      if (iters_to_tol) *iters_to_tol = iters;
-    }
-    if (reached && rel < 4e-16) break;
-    if (norm1(f) == 0.0) break;
-  }
-  map[0] = x[0];
-  map[1] = x[1];
-  map[2] = x[2];
-  if (!(norm1(f) < 1e-6)) return -1 - iters;
-  return iters;
+  return pm_newton(Om, p, M, s, e, std::cos(iota), x0, map, iters_to_tol);
 }
 
 double initial_mean_anomaly(double e, double psi) {
@@ -177,27 +65,13 @@ double initial_mean_anomaly(double e, double psi) {
 
 int parmap_warm(const double Om[3], double p, double M, double s, double e, double iota, const double guess[3],
                 double map[3], int *fallback, int *iters_to_tol) {
-  int it = parmap(Om, p, M, s, e, iota, guess, map, iters_to_tol);
-  // the warm solution must be the root the guess points at: a converged solve
-  // that wandered off (another root of the PN system) is redone from the plain guess
-  const bool near = it >= 0 && std::fabs(map[0] - guess[0]) * std::sqrt(p) < kWarmAcceptance &&
-                    std::fabs(map[1] - guess[1]) < kWarmAcceptance * M && std::fabs(map[2] - guess[2]) < kWarmAcceptance;
-  if (near) {
-    if (fallback) *fallback = 0;
-    return it;
-  }
-  if (fallback) *fallback = 1;
-  const int spent = it >= 0 ? it : -1 - it;
-  int tol2 = -1;
-  const int it2 = parmap(Om, p, M, s, e, iota, nullptr, map, &tol2);
-  if (iters_to_tol) *iters_to_tol = tol2 >= 0 ? tol2 + spent : -1;
-  return it2 >= 0 ? it2 + spent : it2 - spent;
+  return pm_newton_warm(Om, p, M, s, e, std::cos(iota), guess, map, fallback, iters_to_tol);
 }
 
 double parmap_residual_norm(const double Om[3], double M, double e, double iota, const double map[3]) {
   double f[3];
-  parmap_residual(Om, M, e, std::cos(iota), map, f);
-  return norm1(f);
+  pm_residual(Om, M, e, std::cos(iota), map, f);
+  return pm_norm1(f);
 }
 
 int front_end(const Params &P, MappedTrajectory *out, const double *warm) {

@@ -4,6 +4,7 @@
 // interpolate.  Everything here is re-entrant (no static state).
 #pragma once
 
+#include "parmap_newton.hpp"
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -77,7 +78,6 @@ int parmap(const double Omega[3], double p, double M, double s, double e, double
 // farther than kWarmAcceptance (in v_map sqrt(p), M_map / M, s_map) from the
 // guess; *fallback (optional) is set then.  Returns the Newton iterations of
 // both solves (< 0 on failure).
-constexpr double kWarmAcceptance = 0.05;
 int parmap_warm(const double Omega[3], double p, double M, double s, double e, double iota, const double guess[3],
                 double map[3], int *fallback, int *iters_to_tol = nullptr);
 

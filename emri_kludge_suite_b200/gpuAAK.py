@@ -132,6 +132,11 @@ class GPUAAK:
         self._spectral = True
         return (G, st) if return_status else G
 
+    def set_parmap_device(self, on: bool = True):
+        """Solve the Kerr->AK map of a template batch's coarse points on the GPU
+        (bit-identical to the host solve)."""
+        check(lib().aak_gpu_set_parmap_device(self._g, int(bool(on))), "set_parmap_device")
+
     def set_precision(self, precision: int):
         """0: FP64 throughout (default); 1: split precision."""
         check(lib().aak_gpu_set_precision(self._g, int(precision)), "set_precision")

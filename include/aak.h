@@ -400,6 +400,16 @@ int aak_batch_newton_stats(aak_ctx *ctx, int64_t *points, int64_t *iterations, i
 /* The same for the likelihood object's template batches. */
 int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m);
 
+/* Solve the Kerr->AK map of every coarse point of a batch on the GPU (one
+ * launch after the host's coarse inspirals) instead of on the planning
+ * threads.  Part of the batched front end the reference has no counterpart
+ * for; the device solve performs the host's operations in the same order
+ * without fused multiply-adds, so the mapped trajectories, and every output,
+ * are the same bit for bit.  on = 0 (default) solves on the host.  Not for
+ * host-only contexts. */
+int aak_ctx_set_parmap_device(aak_ctx *ctx, int32_t on);
+int aak_gpu_set_parmap_device(aak_gpu *g, int32_t on);
+
 #ifdef __cplusplus
 }
 #endif
