@@ -290,33 +290,33 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
   return AAK_OK;
 }
 
-// Coarse AK evolution and knots of source s from its mapped trajectory.
-// finish_source of two sources on one thread, their coarse AK evolutions
-// interleaved (plan_source_pair: same results).
-void finish_pair(aak_ctx *ctx, int a, const Params &Pa, const MappedTrajectory &ma, int sta, int b, const Params &Pb,
-                 const MappedTrajectory &mb, int stb, const int32_t *nm) {
-  WaveInputs wa, wb;
-  if (sta == kOk) {
-    genwave_inputs(Pa, ma, nm ? nm[a] : 0, &wa);
-    if (wa.nmodes > 4096) sta = kErrCapacity;
+// Coarse AK evolution and knots of up to kPlanGroup sources idx[0..n) on one
+// thread, their coarse AK evolutions run together (plan_source_group: the
+// same results as one at a time).
+void finish_group(aak_ctx *ctx, int n, const int *idx, const Params *P, const MappedTrajectory *const *mt, int *st,
+                  const int32_t *nm) {
+  WaveInputs w[kPlanGroup];
+  const WaveInputs *wp[kPlanGroup];
+  SourcePlan *pp[kPlanGroup];
+  int go[kPlanGroup], ngo = 0;
+  for (int i = 0; i < n; ++i) {
+    if (st[i] != kOk) continue;
+    genwave_inputs(P[i], *mt[i], nm ? nm[idx[i]] : 0, &w[i]);
+    if (w[i].nmodes > 4096) {
+      st[i] = kErrCapacity;
+      continue;
+    }
+    wp[ngo] = &w[i];
+    pp[ngo] = &ctx->plans[idx[i]];
+    go[ngo++] = i;
   }
-  if (stb == kOk) {
-    genwave_inputs(Pb, mb, nm ? nm[b] : 0, &wb);
-    if (wb.nmodes > 4096) stb = kErrCapacity;
-  }
-  if (sta == kOk && stb == kOk) {
-    plan_source_pair(wa, &ctx->plans[a], wb, &ctx->plans[b]);
-    sta = ctx->plans[a].status;
-    stb = ctx->plans[b].status;
-  } else {
-    if (sta == kOk) sta = plan_source(wa, &ctx->plans[a]);
-    if (stb == kOk) stb = plan_source(wb, &ctx->plans[b]);
-  }
-  for (const auto &q : {std::make_pair(a, sta), std::make_pair(b, stb)}) {
-    ctx->status[q.first] = q.second;
-    if (q.second != kOk) {
-      ctx->plans[q.first].knot_t.clear();
-      ctx->plans[q.first].knot_y.clear();
+  if (ngo > 0) plan_source_group(wp, pp, ngo);
+  for (int g = 0; g < ngo; ++g) st[go[g]] = ctx->plans[idx[go[g]]].status;
+  for (int i = 0; i < n; ++i) {
+    ctx->status[idx[i]] = st[i];
+    if (st[i] != kOk) {
+      ctx->plans[idx[i]].knot_t.clear();
+      ctx->plans[idx[i]].knot_y.clear();
     }
   }
 }
@@ -464,7 +464,7 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   // so handing sources out in that order keeps host threads from idling
   // behind one long source at the end.
   std::vector<int> order(nsrc);
-  int nbig = 0;  // the leading sources of order that run alone (the rest in pairs)
+  int nbig = 0;  // the leading sources of order that bound the planning time
   {
     std::vector<double> cost(nsrc, 0.0);
     for (int s = 0; s < nsrc; ++s) {
@@ -474,12 +474,13 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     }
     for (int s = 0; s < nsrc; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    // The sources that bound the planning time (more than a quarter of a
-    // thread's fair share each) go first and alone; the others are planned two
-    // at a time (neighbours in cost, their recurrences interleaved: the same
-    // results, and most of the recurrence's latency hidden).  Streaming takes
-    // the others smallest first, so that finished sources start flowing to
-    // the device early while the long ones are being planned.
+    // Sources are planned kPlanGroup at a time, neighbours in cost, their
+    // recurrences run together in vector lanes (the same results; a group
+    // costs little more than its longest member).  The sources that bound the
+    // planning time (more than a quarter of a thread's fair share each) form
+    // the first groups; streaming takes the others smallest first, so that
+    // finished sources start flowing to the device early while the long ones
+    // are being planned.
     double total = 0.0;
     for (double c : cost) total += c;
     const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -488,7 +489,8 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     nbig = (int)(split - order.begin());
     if (early_small) std::reverse(split, order.end());
   }
-  const int64_t ntasks = nbig + (nsrc - nbig + 1) / 2;
+  const int64_t nbig_tasks = (nbig + kPlanGroup - 1) / kPlanGroup;
+  const int64_t ntasks = nbig_tasks + (nsrc - nbig + kPlanGroup - 1) / kPlanGroup;
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
   auto map_one = [&](int s, const Params &Pp, MappedTrajectory *mt) {
     if (fused) {
@@ -538,25 +540,21 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   };
   parallel_for(ntasks, nthreads, [&](int64_t t) {
     on_device();
-    const int64_t k = (t < nbig) ? t : nbig + 2 * (t - nbig);
-    const int a = order[k];
-    const Params Pa = to_params(Pv[a]);
-    MappedTrajectory ma;
-    const int sta = map_one(a, Pa, &ma);
-    if (k + 1 < nsrc && t >= nbig) {
-      const int b = order[k + 1];
-      const Params Pb = to_params(Pv[b]);
-      MappedTrajectory mb;
-      const int stb = map_one(b, Pb, &mb);
-      finish_pair(ctx, a, Pa, ma, sta, b, Pb, mb, stb, nm);
-      if (on_done) {
-        on_done(a);
-        on_done(b);
-      }
-    } else {
-      finish_source(ctx, a, Pa, ma, nm, sta);
-      if (on_done) on_done(a);
+    const int64_t k = (t < nbig_tasks) ? kPlanGroup * t : nbig + kPlanGroup * (t - nbig_tasks);
+    const int n = (int)std::min<int64_t>(kPlanGroup, ((t < nbig_tasks) ? nbig : nsrc) - k);
+    int idx[kPlanGroup], st[kPlanGroup];
+    Params Pg[kPlanGroup];
+    std::vector<MappedTrajectory> mg(n);
+    const MappedTrajectory *mp[kPlanGroup];
+    for (int i = 0; i < n; ++i) {
+      idx[i] = order[k + i];
+      Pg[i] = to_params(Pv[idx[i]]);
+      st[i] = map_one(idx[i], Pg[i], &mg[i]);
+      mp[i] = &mg[i];
     }
+    finish_group(ctx, n, idx, Pg, mp, st, nm);
+    if (on_done)
+      for (int i = 0; i < n; ++i) on_done(idx[i]);
   });
   ctx->newton_points = points;
   ctx->newton_iters = iters;

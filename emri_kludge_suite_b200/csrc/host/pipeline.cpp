@@ -4,6 +4,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 #include "inspiral.hpp"
 #include "kerr.hpp"
@@ -209,14 +212,15 @@ int bessel_start_order(int n, double e_max, int extra) {
 // ------------------------------------------------------------------ coarse AK evolution
 namespace {
 // dv/dt and de/dt of the AK equations (KSParMap.cc:86-144); lv = log(v) and
-// ome15 = (1 - e^2)^1.5 are shared by the two.
-__attribute__((always_inline)) inline double dvdt_core(double v, double e, double Y, double m, double M, double q, double lv,
-                                                        double ome15) {
-  const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
-  const double e2 = e * e, e4 = e2 * e2, e6 = e4 * e2;
-  const double Y2 = Y * Y, q2 = q * q;
+// ome15 = (1 - e^2)^1.5 are shared by the two.  T is double, or a vector of
+// doubles (one source per lane: the same operations lane by lane).
+template <class T>
+__attribute__((always_inline)) inline T dvdt_core(T v, T e, T Y, T m, T M, T q, T lv, T ome15) {
+  const T v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
+  const T e2 = e * e, e4 = e2 * e2, e6 = e4 * e2;
+  const T Y2 = Y * Y, q2 = q * q;
   const double l2 = std::log(2.), l3 = std::log(3.), l5 = std::log(5.);
-  double s = 1. + 7. * e2 * (1. / 8.);
+  T s = 1. + 7. * e2 * (1. / 8.);
   s += (-5944. - 7040. * e2 + 8539. * e4) * v2 * (1. / 2688.);
   s -= v3 * ((-18432. - 55872. * e2 - 7056. * e4 + 49. * e6) * kPi + 48. * (1064. + 1516. * e2 + 475. * e4) * q * Y) * (1. / 4608.);
   s += v3 * v2 *
@@ -227,7 +231,7 @@ __attribute__((always_inline)) inline double dvdt_core(double v, double e, doubl
        (953325. * e6 + 8. * (34103. + 189. * q2 * (-329. + 815. * Y2)) + 12. * e2 * (-526955. + 126. * q2 * (-929. + 1431. * Y2)) +
         3. * e4 * (-1232809. + 63. * q2 * (-1051. + 2997. * Y2))) /
        145152.;
-  double c6 = 117.72574285227559 - 1712. * kEulerGamma * (1. / 105.) + 16. * kPi2Trunc * (1. / 3.) - 331. * q2 * (1. / 192.) -
+  T c6 = 117.72574285227559 - 1712. * kEulerGamma * (1. / 105.) + 16. * kPi2Trunc * (1. / 3.) - 331. * q2 * (1. / 192.) -
               289. * kPi * q * Y * (1. / 6.) + 145759. * q2 * Y2 * (1. / 1344.) - 3424. * l2 * (1. / 105.);
   c6 += e2 * (764.5906705662063 - 24503. * kEulerGamma * (1. / 210.) + 229. * kPi2Trunc * (1. / 6.) + 2129. * q2 * (1. / 42.) -
               4225. * kPi * q * Y * (1. / 24.) + 27191. * q2 * Y2 * (1. / 224.) + 1391. * l2 * (1. / 30.) - 78003. * l3 * (1. / 280.));
@@ -241,20 +245,20 @@ __attribute__((always_inline)) inline double dvdt_core(double v, double e, doubl
   return 32. * ome15 * m * v6 * v3 * s / (5. * M * M);
 }
 
-__attribute__((always_inline)) inline double dedt_core(double v, double e, double Y, double m, double M, double q, double lv,
-                                                        double ome15) {
-  const double v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
-  const double e2 = e * e, e4 = e2 * e2;
-  const double Y2 = Y * Y, q2 = q * q;
+template <class T>
+__attribute__((always_inline)) inline T dedt_core(T v, T e, T Y, T m, T M, T q, T lv, T ome15) {
+  const T v2 = v * v, v3 = v2 * v, v6 = v3 * v3;
+  const T e2 = e * e, e4 = e2 * e2;
+  const T Y2 = Y * Y, q2 = q * q;
   const double l2 = std::log(2.), l3 = std::log(3.), l5 = std::log(5.);
-  double s = 2451456. + 975744. * e2;
+  T s = 2451456. + 975744. * e2;
   s += 144. * (-54792. - 18600. * e2 + 22579. * e4) * v2;
   s += 84. * v3 * ((189120. + 286512. * e2 + 24217. * e4) * kPi - 48. * (7032. + 5592. * e2 + 1313. * e4) * q * Y);
   s += 3. * v3 * v2 * ((-16885824. - 42474444. * e2 + 5678971. * e4) * kPi - 48. * (106568. + 187862. * e2 + 442811. * e4) * q * Y);
   s += 8. * v2 * v2 *
        (6. * e2 * (-2070667. + 126. * q2 * (-2975. + 4009. * Y2)) + 8. * (-286397. + 63. * q2 * (-3179. + 5869. * Y2)) +
         e4 * (-3506201. + 63. * q2 * (-3191. + 9009. * Y2)));
-  double c6 = 241.02948298890263 - 82283. * kEulerGamma * (1. / 1995.) + 769. * kPi2Trunc * (1. / 57.) + 180255. * q2 * (1. / 8512.) -
+  T c6 = 241.02948298890263 - 82283. * kEulerGamma * (1. / 1995.) + 769. * kPi2Trunc * (1. / 57.) + 180255. * q2 * (1. / 8512.) -
               11809. * kPi * q * Y * (1. / 152.) + 598987. * q2 * Y2 * (1. / 8512.) - 11021. * l2 * (1. / 285.) - 234009. * l3 * (1. / 5320.);
   c6 += e2 * (1048.5728116817568 - 297674. * kEulerGamma * (1. / 1995.) + 2782. * kPi2Trunc * (1. / 57.) + 536653. * q2 * (1. / 8512.) -
               91375. * kPi * q * Y * (1. / 608.) + 356845. * q2 * Y2 * (1. / 8512.) - 2982946. * l2 * (1. / 1995.) + 1638063. * l3 * (1. / 3040.));
@@ -591,6 +595,101 @@ void evolve2(PlanState &A, PlanState &B) {
   B.j_max_temp = B.j_max;
 }
 
+#if defined(__x86_64__) && defined(__GNUC__)
+#define AAK_EVOLVE_LANES 1
+typedef double aak_d4 __attribute__((vector_size(32)));
+typedef long long aak_i4 __attribute__((vector_size(32)));
+
+// 4 NV sources' evolutions in the lanes of NV AVX2 vectors (NV independent
+// recurrences interleaved).  Lane k performs source k's operations of
+// evolve() in the same order: the target enables AVX2 but not FMA (no
+// contraction), the square root and division are correctly rounded in
+// either form and log(v) is taken per lane with std::log, so the knots are
+// bit-identical to evolve()'s.  A lane whose source has ended keeps
+// recomputing its last state and stores nothing.
+template <int NV>
+__attribute__((target("avx2"))) void evolve_lanes(PlanState *const S[4 * NV]) {
+  constexpr int NL = 4 * NV;
+  aak_d4 Y[NV], m[NV], M[NV], q[NV], h[NV], e[NV], v[NV], ed[NV], vd[NV];
+  double *eK[NL], *vK[NL];  // each lane's e_AK, v_AK at its current step j
+  int left[NL];
+  unsigned active = 0;
+  for (int k = 0; k < NL; ++k) {
+    PlanState &P = *S[k];
+    const int u = k >> 2, l = k & 3, j = P.j0 + P.steps - 1;
+    Y[u][l] = P.coslam;
+    m[u][l] = P.mu;
+    M[u][l] = P.M0;
+    q[u][l] = P.S0;
+    h[u][l] = P.dt_large;
+    eK[k] = &P.e_AK[j];
+    vK[k] = &P.v_AK[j];
+    e[u][l] = *eK[k];
+    v[u][l] = *vK[k];
+    ed[u][l] = P.edot;
+    vd[u][l] = P.vdot;
+    left[k] = P.j_end - j;
+    if (left[k] > 0) active |= 1u << k;
+  }
+  constexpr unsigned all = (1u << NL) - 1;
+  while (active) {
+    aak_d4 en[NV], vn[NV];
+    unsigned bad = 0;
+#pragma GCC unroll 4
+    for (int u = 0; u < NV; ++u) {
+      const aak_d4 edm = ed[u], vdm = vd[u];
+      const aak_d4 ome = 1. - e[u] * e[u];
+      aak_d4 lv;
+      for (int l = 0; l < 4; ++l) lv[l] = std::log(v[u][l]);
+      const aak_d4 ome15 = ome * (aak_d4)_mm256_sqrt_pd((__m256d)ome);
+      ed[u] = dedt_core(v[u], e[u], Y[u], m[u], M[u], q[u], lv, ome15);
+      vd[u] = dvdt_core(v[u], e[u], Y[u], m[u], M[u], q[u], lv, ome15);
+      en[u] = e[u] + (1.5 * ed[u] - .5 * edm) * h[u];
+      vn[u] = v[u] + (1.5 * vd[u] - .5 * vdm) * h[u];
+      const aak_i4 badv = (en[u] < 0.) | (vn[u] < v[u]) | (en[u] != en[u]) | (vn[u] != vn[u]);
+      bad |= (unsigned)_mm256_movemask_pd((__m256d)badv) << (4 * u);
+    }
+    bad &= active;
+    for (int k = 0; bad; ++k, bad >>= 1) {
+      if (!(bad & 1)) continue;
+      PlanState &P = *S[k];
+      const int j = P.j_end - left[k];
+      if (P.j_max == P.j_max_temp) P.j_max = j;
+      en[k >> 2][k & 3] = P.e_AK[P.j_max];
+      vn[k >> 2][k & 3] = P.v_AK[P.j_max];
+    }
+    if (active == all) {
+#pragma GCC unroll 4
+      for (int u = 0; u < NV; ++u) {
+        e[u] = en[u];
+        v[u] = vn[u];
+      }
+      for (int k = 0; k < NL; ++k) {
+        *++eK[k] = en[k >> 2][k & 3];
+        *++vK[k] = vn[k >> 2][k & 3];
+        --left[k];
+      }
+    } else {
+      for (int k = 0; k < NL; ++k) {
+        if (!(active >> k & 1)) continue;
+        e[k >> 2][k & 3] = en[k >> 2][k & 3];
+        v[k >> 2][k & 3] = vn[k >> 2][k & 3];
+        *++eK[k] = en[k >> 2][k & 3];
+        *++vK[k] = vn[k >> 2][k & 3];
+        --left[k];
+      }
+    }
+    for (int k = 0; k < NL; ++k)
+      if ((active >> k & 1) && left[k] == 0) {
+        S[k]->edot = ed[k >> 2][k & 3];
+        S[k]->vdot = vd[k >> 2][k & 3];
+        active &= ~(1u << k);
+      }
+  }
+  for (int k = 0; k < NL; ++k) S[k]->j_max_temp = S[k]->j_max;
+}
+#endif
+
 int plan_tail(PlanState &S) {
   const WaveInputs &w = *S.w;
   SourcePlan *plan = S.plan;
@@ -813,6 +912,28 @@ void plan_source_pair(const WaveInputs &wa, SourcePlan *pa, const WaveInputs &wb
   else if (ok_b) evolve(B);
   if (ok_a) plan_tail(A);
   if (ok_b) plan_tail(B);
+}
+
+void plan_source_group(const WaveInputs *const w[], SourcePlan *const p[], int n) {
+  static thread_local std::vector<double> scratch[kPlanGroup];
+  PlanState S[kPlanGroup];
+  PlanState *ok[kPlanGroup];
+  int nok = 0;
+  for (int k = 0; k < n && k < kPlanGroup; ++k) {
+    S[k].w = w[k];
+    S[k].plan = p[k];
+    S[k].scratch = &scratch[k];
+    if (plan_head(S[k]) == kOk) ok[nok++] = &S[k];
+  }
+  int k = 0;
+#ifdef AAK_EVOLVE_LANES
+  static const bool lanes = __builtin_cpu_supports("avx2");
+  if (lanes)
+    for (; k + kPlanGroup <= nok; k += kPlanGroup) evolve_lanes<kPlanGroup / 4>(ok + k);
+#endif
+  for (; k + 2 <= nok; k += 2) evolve2(*ok[k], *ok[k + 1]);
+  if (k < nok) evolve(*ok[k]);
+  for (int i = 0; i < nok; ++i) plan_tail(*ok[i]);
 }
 
 }  // namespace aak

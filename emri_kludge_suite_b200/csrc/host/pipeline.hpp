@@ -200,6 +200,15 @@ int plan_source(const WaveInputs &w, SourcePlan *plan);
 // plan_source of two sources on one thread, their coarse AK evolutions
 // interleaved (same results; each plan's status in its own plan->status).
 void plan_source_pair(const WaveInputs &wa, SourcePlan *pa, const WaveInputs &wb, SourcePlan *pb);
+// plan_source of up to kPlanGroup sources on one thread: their coarse AK
+// evolutions run in the lanes of kPlanGroup / 4 AVX2 vectors (where the CPU
+// has AVX2 and all kPlanGroup plan_heads succeed), else two interleaved;
+// every plan equals plan_source's bit for bit.  Each plan's status is in
+// plan->status.  Four measured faster than eight on the 512-source
+// configuration-1 batch: a group waits for its longest member.
+constexpr int kPlanGroup = 4;
+static_assert(kPlanGroup % 4 == 0, "whole AVX2 vectors");
+void plan_source_group(const WaveInputs *const w[], SourcePlan *const p[], int n);
 // Per-source geometry constants of the waveform (orientation fields set).
 void fill_geometry(SourceDesc *d);
 
