@@ -31,11 +31,12 @@ constexpr double kPi2Trunc = 9.86960440109;
 // as functions of v = 1/sqrt(p), e, Y = cos(iota), q = spin.  Same expressions
 // as src/suite/KSParMap.cc:146-209, grouped by powers of v.
 // Numerators of the PN derivatives below: pn_dtdm = pn_dtdm_num / (256 v^4),
-// the other three = num / (16 v).
-AAK_HD double pn_dtdm_num(double v, double e, double Y, double q) {
-  const double v2 = v * v, v3 = v2 * v, v4 = v2 * v2;
-  const double e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
-  double s = 2. * e4 *
+// the other three = num / (16 v).  T is double, or (host) a vector of doubles.
+template <class T>
+AAK_HD T pn_dtdm_num(T v, T e, T Y, T q) {
+  const T v2 = v * v, v3 = v2 * v, v4 = v2 * v2;
+  const T e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  T s = 2. * e4 *
              (240. + v2 * (-120. + v * (42. * (-27. + 4. * q2) * v + (-6567. + 1996. * q2) * v3 +
                                         48. * q * (8. + 77. * v2) * Y - 4. * q2 * v * (90. + 1577. * v2) * Y2)));
   s += e4 * e2 *
@@ -53,9 +54,10 @@ AAK_HD double pn_dtdm(double v, double e, double Y, double q) {
   return pn_dtdm_num(v, e, Y, q) / (256. * (v2 * v2));
 }
 
-AAK_HD double pn_drdm_num(double v, double e, double Y, double q) {
-  const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
-  double s = 16. + 8. * (-3. + e2) * v2 - 16. * (-3. + e2) * q * v3 * Y + 8. * (33. + 4. * e2 - 3. * e4) * q * v3 * v2 * Y;
+template <class T>
+AAK_HD T pn_drdm_num(T v, T e, T Y, T q) {
+  const T v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  T s = 16. + 8. * (-3. + e2) * v2 - 16. * (-3. + e2) * q * v3 * Y + 8. * (33. + 4. * e2 - 3. * e4) * q * v3 * v2 * Y;
   s += v3 * v3 *
        (-351. + 132. * q2 + e2 * (-135. + 21. * e2 + 5. * e4 + 2. * (7. + e2) * q2) +
         2. * (-204. + 13. * e2 * (-3. + e2)) * q2 * Y2);
@@ -64,9 +66,10 @@ AAK_HD double pn_drdm_num(double v, double e, double Y, double q) {
 }
 AAK_HD double pn_drdm(double v, double e, double Y, double q) { return pn_drdm_num(v, e, Y, q) / (16. * v); }
 
-AAK_HD double pn_dthetadm_num(double v, double e, double Y, double q) {
-  const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
-  double s = 16. + 8. * (3. + e2) * v2 - 16. * (3. + e2) * q * v3 * Y - 8. * (3. + e2) * (5. + 3. * e2) * q * v3 * v2 * Y;
+template <class T>
+AAK_HD T pn_dthetadm_num(T v, T e, T Y, T q) {
+  const T v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  T s = 16. + 8. * (3. + e2) * v2 - 16. * (3. + e2) * q * v3 * Y - 8. * (3. + e2) * (5. + 3. * e2) * q * v3 * v2 * Y;
   s += v3 * v3 *
        (135. - 54. * q2 + e2 * (5. * (27. + 9. * e2 + e4) + 2. * (-38. + e2) * q2) +
         2. * (57. + 90. * e2 + 13. * e4) * q2 * Y2);
@@ -75,9 +78,10 @@ AAK_HD double pn_dthetadm_num(double v, double e, double Y, double q) {
 }
 AAK_HD double pn_dthetadm(double v, double e, double Y, double q) { return pn_dthetadm_num(v, e, Y, q) / (16. * v); }
 
-AAK_HD double pn_dphidm_num(double v, double e, double Y, double q) {
-  const double v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
-  double s = 16. + 8. * (3. + e2) * v2 - 16. * q * v3 * (-2. + (3. + e2) * Y) -
+template <class T>
+AAK_HD T pn_dphidm_num(T v, T e, T Y, T q) {
+  const T v2 = v * v, v3 = v2 * v, e2 = e * e, e4 = e2 * e2, Y2 = Y * Y, q2 = q * q;
+  T s = 16. + 8. * (3. + e2) * v2 - 16. * q * v3 * (-2. + (3. + e2) * Y) -
              8. * q * v3 * v2 * (-6. + 15. * Y + 3. * e4 * Y + 2. * e2 * (-4. + 7. * Y));
   s += 2. * v2 * v2 * (27. + 3. * e4 + 2. * q2 * (-1. + Y) * (1. + 7. * Y) + 2. * e2 * (9. + q2 * (1. + Y2)));
   s += v3 * v3 *

@@ -211,6 +211,10 @@ int bessel_start_order(int n, double e_max, int extra) {
 
 // ------------------------------------------------------------------ coarse AK evolution
 namespace {
+#if defined(__x86_64__) && defined(__GNUC__)
+typedef double aak_d4 __attribute__((vector_size(32)));  // four sources or knots, one per lane
+typedef long long aak_i4 __attribute__((vector_size(32)));
+#endif
 // dv/dt and de/dt of the AK equations (KSParMap.cc:86-144); lv = log(v) and
 // ome15 = (1 - e^2)^1.5 are shared by the two.  T is double, or a vector of
 // doubles (one source per lane: the same operations lane by lane).
@@ -312,29 +316,57 @@ inline double om_x(double v, double e, double coslam, double S, double M, double
 }
 // Plunge-scan pre-test of n consecutive knots (y4: their (e, v, M, S)):
 // clear[k] = 1 where p^3 = (1 - e^2)^3 / x^2 exceeds lso3, i.e. where the
-// knot fails both plunge tests.  lso3 carries a 1e-9 margin, so the result
-// does not depend on how the compiler rounds (FMA or not); the knots not
-// cleared take the exact path.  Independent per knot: vectorised where the
-// CPU has AVX2 and FMA.
-#define AAK_PLUNGE_PRETEST_BODY                                                   \
-  for (int k = 0; k < n; ++k) {                                                    \
-    const double e = y4[4 * k], v = y4[4 * k + 1], M = y4[4 * k + 2], S = y4[4 * k + 3]; \
-    const double x = om_x(v, e, coslam, S, M, M_phys);                             \
-    const double ome = 1. - e * e;                                                 \
-    clear[k] = (ome * ome * ome > lso3 * (x * x)) ? 1 : 0;                        \
-  }
-__attribute__((target("avx2,fma"))) void plunge_pretest_avx2(const double *y4, int n, double coslam, double M_phys,
-                                                             double lso3, unsigned char *clear) {
-  AAK_PLUNGE_PRETEST_BODY
+// knot fails both plunge tests.  With x = c v^3 N_phi / (N_t M) (om_x, the
+// retrograde branch being the prograde formula at -Y, -S) the test is
+// (1 - e^2)^3 (N_t M)^2 > lso3 (c v^3 N_phi)^2, without a division.  lso3
+// carries a 1e-9 margin, so the result does not depend on how the compiler
+// rounds (FMA or not); the knots not cleared take the exact path.
+template <class T>
+__attribute__((always_inline)) inline void pretest_terms(T e, T v, T M, T S, T Y, double c, double lso3, T *lhs,
+                                                         T *rhs) {
+  const T num = c * (v * v * v) * pn_dphidm_num(v, e, Y, S);
+  const T den = pn_dtdm_num(v, e, Y, S) * M;
+  const T ome = 1. - e * e;
+  *lhs = ome * ome * ome * (den * den);
+  *rhs = lso3 * (num * num);
 }
 void plunge_pretest_plain(const double *y4, int n, double coslam, double M_phys, double lso3, unsigned char *clear) {
-  AAK_PLUNGE_PRETEST_BODY
+  const double sg = coslam > 0 ? 1. : -1., Y = sg * coslam, c = 16. * M_phys * kMsunSec;
+  for (int k = 0; k < n; ++k) {
+    const double *r = y4 + 4 * (size_t)k;
+    double lhs, rhs;
+    pretest_terms(r[0], r[1], r[2], sg * r[3], Y, c, lso3, &lhs, &rhs);
+    clear[k] = lhs > rhs ? 1 : 0;
+  }
 }
-#undef AAK_PLUNGE_PRETEST_BODY
+#if defined(__x86_64__) && defined(__GNUC__)
+// Four knots per AVX2 vector (the knots' rows transposed into lanes).
+__attribute__((target("avx2,fma"))) void plunge_pretest_avx2(const double *y4, int n, double coslam, double M_phys,
+                                                             double lso3, unsigned char *clear) {
+  const double sg = coslam > 0 ? 1. : -1., c = 16. * M_phys * kMsunSec;
+  const aak_d4 Y = {sg * coslam, sg * coslam, sg * coslam, sg * coslam};
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    const double *r = y4 + 4 * (size_t)k;
+    const aak_d4 e = {r[0], r[4], r[8], r[12]}, v = {r[1], r[5], r[9], r[13]}, M = {r[2], r[6], r[10], r[14]};
+    const aak_d4 S = sg * (aak_d4){r[3], r[7], r[11], r[15]};
+    aak_d4 lhs, rhs;
+    pretest_terms(e, v, M, S, Y, c, lso3, &lhs, &rhs);
+    const int m = _mm256_movemask_pd((__m256d)(lhs > rhs));
+    clear[k] = m & 1;
+    clear[k + 1] = (m >> 1) & 1;
+    clear[k + 2] = (m >> 2) & 1;
+    clear[k + 3] = (m >> 3) & 1;
+  }
+  if (k < n) plunge_pretest_plain(y4 + 4 * (size_t)k, n - k, coslam, M_phys, lso3, clear + k);
+}
+#endif
 void plunge_pretest(const double *y4, int n, double coslam, double M_phys, double lso3, unsigned char *clear) {
+#if defined(__x86_64__) && defined(__GNUC__)
   static const bool avx2 = __builtin_cpu_supports("avx2") && __builtin_cpu_supports("fma");
-  if (avx2) plunge_pretest_avx2(y4, n, coslam, M_phys, lso3, clear);
-  else plunge_pretest_plain(y4, n, coslam, M_phys, lso3, clear);
+  if (avx2) return plunge_pretest_avx2(y4, n, coslam, M_phys, lso3, clear);
+#endif
+  plunge_pretest_plain(y4, n, coslam, M_phys, lso3, clear);
 }
 
 inline double p_of(double v, double e, double coslam, double S, double M, double M_phys) {
@@ -597,8 +629,6 @@ void evolve2(PlanState &A, PlanState &B) {
 
 #if defined(__x86_64__) && defined(__GNUC__)
 #define AAK_EVOLVE_LANES 1
-typedef double aak_d4 __attribute__((vector_size(32)));
-typedef long long aak_i4 __attribute__((vector_size(32)));
 
 // 4 NV sources' evolutions in the lanes of NV AVX2 vectors (NV independent
 // recurrences interleaved).  Lane k performs source k's operations of
