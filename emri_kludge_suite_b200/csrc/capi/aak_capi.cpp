@@ -464,7 +464,7 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   // so handing sources out in that order keeps host threads from idling
   // behind one long source at the end.
   std::vector<int> order(nsrc);
-  int nbig = 0;  // the leading sources of order that bound the planning time
+  int nbig = 0;  // the leading sources of order that run alone (the rest in groups)
   {
     std::vector<double> cost(nsrc, 0.0);
     for (int s = 0; s < nsrc; ++s) {
@@ -474,13 +474,13 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     }
     for (int s = 0; s < nsrc; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    // Sources are planned kPlanGroup at a time, neighbours in cost, their
-    // recurrences run together in vector lanes (the same results; a group
-    // costs little more than its longest member).  The sources that bound the
-    // planning time (more than a quarter of a thread's fair share each) form
-    // the first groups; streaming takes the others smallest first, so that
-    // finished sources start flowing to the device early while the long ones
-    // are being planned.
+    // The sources that bound the planning time (more than a quarter of a
+    // thread's fair share each) go first and alone: a lone recurrence has
+    // the shortest latency per step.  The others are planned kPlanGroup at a
+    // time, neighbours in cost, their recurrences run together in vector
+    // lanes (the same results, at a fraction of the cost per source).
+    // Streaming takes the others smallest first, so that finished sources
+    // start flowing to the device early while the long ones are being planned.
     double total = 0.0;
     for (double c : cost) total += c;
     const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -489,8 +489,7 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     nbig = (int)(split - order.begin());
     if (early_small) std::reverse(split, order.end());
   }
-  const int64_t nbig_tasks = (nbig + kPlanGroup - 1) / kPlanGroup;
-  const int64_t ntasks = nbig_tasks + (nsrc - nbig + kPlanGroup - 1) / kPlanGroup;
+  const int64_t ntasks = nbig + (nsrc - nbig + kPlanGroup - 1) / kPlanGroup;
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
   auto map_one = [&](int s, const Params &Pp, MappedTrajectory *mt) {
     if (fused) {
@@ -540,8 +539,8 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   };
   parallel_for(ntasks, nthreads, [&](int64_t t) {
     on_device();
-    const int64_t k = (t < nbig_tasks) ? kPlanGroup * t : nbig + kPlanGroup * (t - nbig_tasks);
-    const int n = (int)std::min<int64_t>(kPlanGroup, ((t < nbig_tasks) ? nbig : nsrc) - k);
+    const int64_t k = (t < nbig) ? t : nbig + kPlanGroup * (t - nbig);
+    const int n = (t < nbig) ? 1 : (int)std::min<int64_t>(kPlanGroup, nsrc - k);
     int idx[kPlanGroup], st[kPlanGroup];
     Params Pg[kPlanGroup];
     std::vector<MappedTrajectory> mg(n);
