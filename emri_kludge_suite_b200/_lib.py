@@ -143,6 +143,7 @@ def lib():
     L.aak_probe_fp32_tflops.argtypes = [_i32, _dp]
     L.aak_batch_run_graph.argtypes = [_vp, _vp, _vp, _i32, _vp]
     L.aak_ctx_set_precision.argtypes = [_vp, _i32]
+    L.aak_ctx_set_lookback_bound.argtypes = [_vp, _i64]
     L.aak_wave_batch_host.argtypes = [_vp, ctypes.POINTER(AAKParams), _i32, _i32p, _i32, _dp, _dp, _i64p, _i32p]
     # learned ParMap warm start
     _fp = ctypes.POINTER(ctypes.c_float)

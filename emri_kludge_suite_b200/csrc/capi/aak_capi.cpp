@@ -105,7 +105,9 @@ struct aak_ctx {
   int last_launches = 0;
   bool profile = false;
   aak_mlp *model = nullptr;  // learned warm start of the map (optional)
-  int precision = 0;         // precision of the host-buffer entry points
+  int precision = 0;         // precision of the host-buffer entry points and of aak_batch_run_noalloc
+  bool noalloc_used = false; // an allocation-free launch ran since the last status query
+  long long lookback_cycles = 0;  // bound of one look-back wait in SM clocks (<= 0: the kernels' default, about 2 s)
   uint64_t upload_gen = 0;   // bumped by every upload (device buffers may move)
   // CUDA graph of the dense launch (clears + waveform kernel) for fixed outputs / precision / upload
   cudaGraph_t graph = nullptr;
@@ -645,8 +647,8 @@ void drop_graph(aak_ctx *ctx) {
   ctx->graph = nullptr;
 }
 
-// The dense launch (two clears and the waveform kernel) as one CUDA graph, captured on the first call for
-// a given (outputs, precision, upload) and replayed afterwards.
+// The dense stage (spline solve, two clears and the waveform kernel) as one CUDA graph, captured on the
+// first call for a given (outputs, precision, upload) and replayed afterwards.
 int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t st) {
   if (!ctx->uploaded || !hI || !hII || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
   int r;
@@ -659,6 +661,11 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
     prepare_dense_launch();
     const BatchView bv = batch_view(ctx, hI, hII, nullptr, nullptr, 0);
     if ((r = cuda_ok(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal))) != AAK_OK) return r;
+    // the whole dense stage: natural-spline solve of every source's knots
+    // (idempotent: the same knots give the same coefficients), then the clears
+    // and the waveform kernel
+    launch_spline_coeffs(ctx->d_src.ptr, ctx->nsrc, ctx->d_spl_blk.ptr, ctx->spl_blk[ctx->nsrc], ctx->d_knot_t.ptr,
+                         ctx->d_knot_y.ptr, ctx->d_knot_c.ptr, ctx->cap_stream);
     launch_dense(bv, ctx->num_sms, ctx->cap_stream, nullptr, precision);
     const cudaError_t launch_err = cudaGetLastError();
     cudaGraph_t g = nullptr;
@@ -677,7 +684,7 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
     ctx->g_prec = precision;
     ctx->g_gen = ctx->upload_gen;
   }
-  ctx->last_launches = 1;
+  ctx->last_launches = 2;
   return cuda_ok(cudaGraphLaunch(ctx->gexec, st));
 }
 
@@ -703,6 +710,7 @@ BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *t
   bv.work_counter = ctx->d_counter.ptr;
   bv.device_status = reinterpret_cast<unsigned int *>(ctx->d_counter.ptr + 1);
   bv.max_nmodes = ctx->max_nmodes;
+  bv.lookback_cycles = ctx->lookback_cycles;
   return bv;
 }
 
@@ -800,8 +808,14 @@ int device_status(aak_ctx *ctx) {
     if (v && (r = cuda_ok(cudaMemset(word, 0, sizeof(v)))) != AAK_OK) return r;
     gave_up = v != 0;
   }
-  const int sv = static_scratch_status(ctx->device, true);
-  if (sv < 0) return cuda_ok(cudaGetLastError());
+  // the allocation-free scratch's report word, only for a context that used it
+  // (every context that launches through it on this device shares that word)
+  int sv = 0;
+  if (ctx->noalloc_used) {
+    sv = static_scratch_status(ctx->device, true);
+    if (sv < 0) return cuda_ok(cudaGetLastError());
+    ctx->noalloc_used = false;
+  }
   return (gave_up || sv > 0) ? AAK_ERR_DEVICE_TIMEOUT : AAK_OK;
 }
 
@@ -1396,9 +1410,11 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   bv.knot_c = reinterpret_cast<const double4 *>(base + o_kc);
   bv.bessel_start = reinterpret_cast<const int32_t *>(base + o_bs);
   bv.max_nmodes = ctx->max_nmodes;
+  bv.lookback_cycles = ctx->lookback_cycles;
   bv.hI = d_hI;
   bv.hII = d_hII;
-  return launch_dense_fp64_static_scratch(bv, ctx->device, ctx->num_sms, st);
+  ctx->noalloc_used = true;
+  return launch_dense_static_scratch(bv, ctx->device, ctx->num_sms, st, ctx->precision);
 }
 
 int aak_batch_last_launches(aak_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
@@ -1445,6 +1461,14 @@ int aak_ctx_set_precision(aak_ctx *ctx, int32_t precision) {
   if (!ctx || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
   ctx->precision = precision;
+  return AAK_OK;
+}
+
+int aak_ctx_set_lookback_bound(aak_ctx *ctx, int64_t cycles) {
+  if (!ctx) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->lookback_cycles = cycles > 0 ? (long long)cycles : 0;
+  drop_graph(ctx);  // a captured launch holds the old bound
   return AAK_OK;
 }
 

@@ -348,7 +348,10 @@ __device__ void look_back_warp(const BatchView &bv, const TileCtx &c, int dir, d
       if (lane == 0)
         give_up = (*(volatile unsigned int *)bv.device_status != 0u || clock64() - start > bound) ? 1 : 0;
       if (__shfl_sync(kAll, give_up, 0)) {
-        if (lane == 0) atomicExch(bv.device_status, 1u);
+        if (lane == 0) {
+          atomicExch(bv.device_status, 1u);
+          if (bv.status_report) atomicExch(bv.status_report, 1u);
+        }
 #pragma unroll
         for (int k = 0; k < 3; ++k) hi[k] = lo[k] = 0.0;
         C = 0.0;
@@ -2089,17 +2092,18 @@ double probe_fp32_fma_tflops(int num_sms, int iters, cudaStream_t stream) {
 }
 
 // ------------------------------------------------------------------ allocation-free launch
-// Tile scratch (look-back records and flags, the work-queue head and the
-// device status word) for callers that must not allocate device memory.  The
-// array is part of the module image: every GPU that loads this library holds
-// about 5 MB until the process exits.  All calls share it and it keeps the last
-// call's contents; launches that overlap on the GPU race on it.
+// Tile scratch (look-back records and flags, the work-queue head, the
+// per-launch status word and the report word) for callers that must not
+// allocate device memory.  The array is part of the module image: every GPU
+// that loads this library holds kStaticScratchBytes (about 4.9 MB) until the
+// process exits.  All calls share it and it keeps the last call's contents;
+// launches that overlap on the GPU race on it.
 namespace {
-constexpr size_t kStaticLinkBytes = (size_t)kStaticScratchTiles * sizeof(TileLink);
-constexpr size_t kStaticFlagOffset = (kStaticLinkBytes + 255) / 256 * 256;
-constexpr size_t kStaticCounterOffset = (kStaticFlagOffset + (size_t)kStaticScratchTiles * sizeof(int32_t) + 255) / 256 * 256;
-constexpr size_t kStaticScratchBytes = kStaticCounterOffset + 256;
 static __device__ __align__(256) unsigned char g_tile_scratch[kStaticScratchBytes];
+// counters at kStaticCounterOffset: work-queue head (8 bytes), this launch's
+// status word, the report word
+constexpr size_t kStaticStatusOffset = kStaticCounterOffset + sizeof(unsigned long long);
+constexpr size_t kStaticReportOffset = kStaticStatusOffset + sizeof(unsigned int);
 
 std::mutex g_scratch_mu;
 void *g_scratch_addr[kMaxStaticDevices] = {nullptr};
@@ -2148,17 +2152,16 @@ int static_scratch_status(int device, bool clear) {
     base = g_scratch_addr[device];
   }
   if (!base) return 0;  // no allocation-free launch on this device yet
-  unsigned int *word = reinterpret_cast<unsigned int *>(static_cast<unsigned char *>(base) + kStaticCounterOffset +
-                                                        sizeof(unsigned long long));
+  unsigned int *word = reinterpret_cast<unsigned int *>(static_cast<unsigned char *>(base) + kStaticReportOffset);
   unsigned int v = 0;
   if (cudaMemcpy(&v, word, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
   if (v && clear && cudaMemset(word, 0, sizeof(v)) != cudaSuccess) return -1;
   return v ? 1 : 0;
 }
 
-int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream) {
+int launch_dense_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream, int precision) {
   if (bv.total_tiles > kStaticScratchTiles) return 8;  // AAK_ERR_CAPACITY
-  if (device < 0 || device >= kMaxStaticDevices) return 1;
+  if (device < 0 || device >= kMaxStaticDevices || (precision != 0 && precision != 1)) return 1;
   void *base = nullptr;
   {
     // host code needs the device address of the array: look it up once per
@@ -2178,10 +2181,13 @@ int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cuda
   bv.link = reinterpret_cast<TileLink *>(b);
   bv.link_flag = reinterpret_cast<int32_t *>(b + kStaticFlagOffset);
   bv.work_counter = reinterpret_cast<unsigned long long *>(b + kStaticCounterOffset);
-  bv.device_status = reinterpret_cast<unsigned int *>(b + kStaticCounterOffset + sizeof(unsigned long long));
-  // launch_dense_fp64 clears the work-queue head and the look-back flags on
+  bv.device_status = reinterpret_cast<unsigned int *>(b + kStaticStatusOffset);
+  bv.status_report = reinterpret_cast<unsigned int *>(b + kStaticReportOffset);
+  // this launch's waits give up early only on a give-up of this launch
+  if (cudaMemsetAsync(bv.device_status, 0, sizeof(unsigned int), stream) != cudaSuccess) return 5;
+  // launch_dense clears the work-queue head and the look-back flags on
   // `stream`; every record is written before its flag is
-  launch_dense_fp64(bv, num_sms, stream, nullptr);
+  launch_dense(bv, num_sms, stream, nullptr, precision);
   return cudaGetLastError() == cudaSuccess ? 0 : 5;
 }
 

@@ -57,6 +57,7 @@ struct BatchView {
   int64_t traj_stride;
   unsigned long long *work_counter;  // persistent work queue head, cleared before every launch
   unsigned int *device_status;       // set to 1 when a bounded look-back wait gave up (never cleared here)
+  unsigned int *status_report = nullptr;  // optional second word set with it: a report kept across launches
   int32_t trajectory_only = 0;       // 1: write traj_out and skip the harmonic sums
   int32_t max_nmodes = 0;            // largest harmonic count of the batch (0: unknown) -- sizes the tile table
   long long lookback_cycles = 0;     // bound of one look-back wait in SM clocks (<= 0: about 2 s)
@@ -154,15 +155,28 @@ void prepare_dense_launch();
 // and the number of devices whose scratch address is cached.
 constexpr int64_t kStaticScratchTiles = 32768;
 constexpr int kMaxStaticDevices = 64;
+// Size of the file-scope scratch array: 32768 look-back records of 144 bytes,
+// 32768 flags and 256 bytes of counters (4,849,920 bytes, about 4.9 MB).
+constexpr size_t kStaticLinkBytes = (size_t)kStaticScratchTiles * sizeof(TileLink);
+constexpr size_t kStaticFlagOffset = (kStaticLinkBytes + 255) / 256 * 256;
+constexpr size_t kStaticCounterOffset =
+    (kStaticFlagOffset + (size_t)kStaticScratchTiles * sizeof(int32_t) + 255) / 256 * 256;
+constexpr size_t kStaticScratchBytes = kStaticCounterOffset + 256;
 
-// Same kernels as launch_dense_fp64, with the tile scratch (bv.link,
-// bv.link_flag, bv.work_counter and bv.device_status are ignored) taken from a
-// file-scope __device__ array instead of caller or context allocations.  Returns an aak_status.
-// The first call on a device looks the array's address up (once per device).
-int launch_dense_fp64_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream);
-// Device status word of the allocation-free scratch on `device` (current):
-// 1 if a bounded look-back wait of one of its launches gave up, 0 if not (or
-// no such launch yet), -1 on a CUDA error; `clear` resets it.  Synchronous.
+// Same kernels as launch_dense (precision 0 or 1), with the tile scratch
+// (bv.link, bv.link_flag, bv.work_counter, bv.device_status and
+// bv.status_report are ignored) taken from a file-scope __device__ array
+// instead of caller or context allocations.  Every launch starts with its own
+// status word cleared, so a wait that gave up in an earlier launch does not
+// cut the waits of this one short; a give-up is also recorded in a report
+// word that stays set until static_scratch_status clears it.  Returns an
+// aak_status.  The first call on a device looks the array's address up (once
+// per device).
+int launch_dense_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream, int precision);
+// Report word of the allocation-free scratch on `device` (current): 1 if a
+// bounded look-back wait of one of its launches gave up since the last clear,
+// 0 if not (or no such launch yet), -1 on a CUDA error; `clear` resets it.
+// Synchronous.
 int static_scratch_status(int device, bool clear);
 
 // Self-test of the bounded look-back wait: one CTA waits on a flag that

@@ -201,13 +201,20 @@ int aak_tdi_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t 
  * The caller passes the planned ctx (aak_batch_plan* only -- no upload),
  * one device buffer of its own for the plan (256-byte aligned, plan_bytes
  * long) and the outputs hI, hII (indexed by the batch offsets).  Call with
- * d_plan == NULL to receive the required size in *required_bytes.  The tile
- * scratch lives in a 10 MB file-scope device array held by every GPU that
- * loads the library until exit; batches above 32768 tiles of 1024 samples
- * (33,554,432 samples) are rejected with AAK_ERR_CAPACITY.  The first call
- * on a device looks the array's address up; make that call before any stream
- * capture.  Every call shares the array: calls that overlap on the GPU race.
- * Nothing here calls cudaMalloc, cudaFree or an allocating library routine. */
+ * d_plan == NULL to receive the required size in *required_bytes.  The
+ * precision is the context's (aak_ctx_set_precision: 0 FP64, the default, or
+ * 1 split).  The tile scratch lives in a file-scope device array of
+ * 4,849,920 bytes (about 4.9 MB) held by every GPU that loads the library
+ * until exit; batches above 32768 tiles of 1024 samples (33,554,432 samples)
+ * are rejected with AAK_ERR_CAPACITY.  The first call on a device looks the
+ * array's address up; make that call before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race.  Each call clears its
+ * own look-back status word before its kernel, so a wait that gave up in an
+ * earlier call does not affect it; a give-up is kept in a report word that
+ * aak_batch_device_status of a context that made such a call reads and
+ * clears (one word per device, shared by every context using this entry
+ * point there).  Nothing here calls cudaMalloc, cudaFree or an allocating
+ * library routine. */
 int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_t *required_bytes, double *d_hI,
                           double *d_hII, void *stream);
 
@@ -216,10 +223,18 @@ int aak_batch_last_launches(aak_ctx *ctx);
 
 /* Waits for the device, then reports whether a bounded device-side wait of
  * the batch kernels gave up since the last upload or the last call (the
- * look-back of the phase scan; the allocation-free launches on the device
+ * look-back of the phase scan; for a context that used
+ * aak_batch_run_noalloc, that entry point's report word on the device
  * included): AAK_ERR_DEVICE_TIMEOUT, else AAK_OK.  Clears the condition. No
  * reference counterpart (the reference's kernels do not wait on one another). */
 int aak_batch_device_status(aak_ctx *ctx);
+
+/* Bound of one look-back wait of this context's batch launches, in SM clocks
+ * (<= 0: the default, about 2 s).  A wait that reaches it gives up, the tile
+ * takes a zero carry and aak_batch_device_status reports
+ * AAK_ERR_DEVICE_TIMEOUT: a watchdog for callers that want a shorter one.  No
+ * reference counterpart. */
+int aak_ctx_set_lookback_bound(aak_ctx *ctx, int64_t cycles);
 
 /* Self-test of that bounded wait on the current device: one thread waits on a
  * look-back flag that nothing sets, for at most `cycles` SM clocks (a few
@@ -244,10 +259,12 @@ int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3);
  * precision 0, to Bessel-evaluation rounding. */
 int aak_batch_run_plain(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_traj, int64_t traj_stride, void *stream);
 
-/* The same three launches as aak_batch_run (no t / trajectory outputs),
- * captured into one CUDA graph on the first call for a given (d_hI, d_hII,
- * precision, upload) and replayed on later calls; a new upload or other
- * outputs recapture.  Capture runs on a stream of the context, so `stream`
+/* The whole dense stage in one CUDA graph: the natural-spline solve of every
+ * source's knots (as aak_batch_upload runs it; the same knots give the same
+ * coefficients) and the three launches of aak_batch_run (no t / trajectory
+ * outputs), captured on the first call for a given (d_hI, d_hII, precision,
+ * upload) and replayed on later calls; a new upload or other outputs
+ * recapture.  Capture runs on a stream of the context, so `stream`
  * may be the legacy default stream.  No reference counterpart: the
  * reference launches its kernels one by one with a device synchronisation
  * after each (src/cuda/AAK_manager.cu:154-260). */
