@@ -27,6 +27,7 @@
  */
 #include <complex.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -794,37 +795,37 @@ int oracle_pnevolution(double *t, double *e, double *v, double *M, double *S, do
 }
 
 /* ------------------------------------------------------------------ waveform */
-/* AAK.cc:321-562 (traj == false).  t, hI, hII hold vlength entries.
- * Returns 0, or -1 when PNevolution fails. */
-int oracle_waveform(double *t, double *hI, double *hII, double timestep, int vlength, int nmodes, double zeta,
-                    const double *par, const double *e_traj, const double *v_map, double M_phys, const double *M_map,
-                    double S_phys, const double *S_map, const double *dt_map, int steps, int backint, int mich,
-                    int *i_plunge_out, int *i_buffer_out) {
-  const double lam = par[4], qS = par[7], phiS = par[8], qK = par[9], phiK = par[10];
+/* Host threads for the per-sample harmonic sums of oracle_waveform (each
+ * sample depends only on the dense PNevolution arrays, so the samples split
+ * into independent ranges; the arithmetic of a sample does not change).
+ * Default 1. */
+static int o_threads = 1;
+void oracle_set_threads(int n) { o_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+
+typedef struct {
+  double *t, *hI, *hII;
+  const double *tv, *ev, *vv, *Mv, *Sv, *gv, *Pv, *av, *nv, *gdv;
+  int nmodes, mich;
+  double zeta, M_phys, lam, qS, phiS, qK, phiK;
+  int lo, hi; /* sample range [lo, hi) */
+} o_wave_job;
+
+/* AAK.cc:409-532 for the samples [lo, hi) of one job. */
+static void o_wave_range(const o_wave_job *jb) {
+  const double lam = jb->lam, qS = jb->qS, phiS = jb->phiS, qK = jb->qK, phiK = jb->phiK;
   const double coslam = cos(lam), sinlam = sin(lam), cosqS = cos(qS), sinqS = sin(qS);
   const double cosqK = cos(qK), sinqK = sin(qK), cosphiK = cos(phiK), sinphiK = sin(phiK);
   const double halfsqrt3 = sqrt(3.) / 2.;
-  size_t nn = (size_t)vlength + 1;
-  double *tv = malloc(nn * 8), *ev = malloc(nn * 8), *vv = malloc(nn * 8), *Mv = malloc(nn * 8), *Sv = malloc(nn * 8);
-  double *gv = malloc(nn * 8), *Pv = malloc(nn * 8), *av = malloc(nn * 8), *nv = malloc(nn * 8), *gdv = malloc(nn * 8);
-  int ip, ib;
-  int rc = oracle_pnevolution(tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, timestep, vlength, par, e_traj, v_map, M_phys,
-                              M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint);
-  if (rc != 0) {
-    free(tv); free(ev); free(vv); free(Mv); free(Sv); free(gv); free(Pv); free(av); free(nv); free(gdv);
-    return rc;
-  }
-  if (i_plunge_out) *i_plunge_out = ip;
-  if (i_buffer_out) *i_buffer_out = ib;
-  int nJ = nmodes + 3;
-  double *J = malloc(sizeof(double) * 8);
-  (void)nJ;
-  for (int i = 0; i < vlength; ++i) {
-    t[i] = tv[i];
+  const int nmodes = jb->nmodes, mich = jb->mich;
+  double J[8];
+  for (int i = jb->lo; i < jb->hi; ++i) {
+    double *t = jb->t, *hI = jb->hI, *hII = jb->hII;
+    t[i] = jb->tv[i];
     hI[i] = 0.;
     hII[i] = 0.;
-    const double e = ev[i], v = vv[i], M = Mv[i], S = Sv[i], gim = gv[i], Phi = Pv[i], alp = av[i], nu = nv[i];
-    const double gimdot = gdv[i];
+    const double e = jb->ev[i], v = jb->vv[i], M = jb->Mv[i], S = jb->Sv[i], gim = jb->gv[i], Phi = jb->Pv[i];
+    const double alp = jb->av[i], nu = jb->nv[i];
+    const double gimdot = jb->gdv[i];
     const double cosalp = cos(alp), sinalp = sin(alp);
     const double cosqL = cosqK * coslam + sinqK * sinlam * cosalp;
     const double sinqL = sqrt(1. - cosqL * cosqL);
@@ -866,7 +867,7 @@ int oracle_waveform(double *t, double *hI, double *hII, double timestep, int vle
       FplusII = s2;
       FcrosII = c2;
     }
-    const double Amp = pow(oracle_omega_phi(v, e, coslam, S, M) * M_phys * O_MSUN_SEC, 2. / 3.) * zeta;
+    const double Amp = pow(oracle_omega_phi(v, e, coslam, S, M) * jb->M_phys * O_MSUN_SEC, 2. / 3.) * jb->zeta;
     double rot[4];
     oracle_rotcoeff(rot, lam, qS, phiS, qK, phiK, alp);
     for (int n = 1; n <= nmodes; ++n) {
@@ -909,7 +910,53 @@ int oracle_waveform(double *t, double *hI, double *hII, double timestep, int vle
       hI[i] += hnI;
       hII[i] += hnII;
     }
-    if (i == ip + ib) break;
+  }
+}
+
+static void *o_wave_thread(void *arg) {
+  o_wave_range((const o_wave_job *)arg);
+  return NULL;
+}
+
+/* AAK.cc:321-562 (traj == false).  t, hI, hII hold vlength entries.
+ * Returns 0, or -1 when PNevolution fails. */
+int oracle_waveform(double *t, double *hI, double *hII, double timestep, int vlength, int nmodes, double zeta,
+                    const double *par, const double *e_traj, const double *v_map, double M_phys, const double *M_map,
+                    double S_phys, const double *S_map, const double *dt_map, int steps, int backint, int mich,
+                    int *i_plunge_out, int *i_buffer_out) {
+  size_t nn = (size_t)vlength + 1;
+  double *tv = malloc(nn * 8), *ev = malloc(nn * 8), *vv = malloc(nn * 8), *Mv = malloc(nn * 8), *Sv = malloc(nn * 8);
+  double *gv = malloc(nn * 8), *Pv = malloc(nn * 8), *av = malloc(nn * 8), *nv = malloc(nn * 8), *gdv = malloc(nn * 8);
+  int ip, ib;
+  int rc = oracle_pnevolution(tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, timestep, vlength, par, e_traj, v_map, M_phys,
+                              M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint);
+  if (rc != 0) {
+    free(tv); free(ev); free(vv); free(Mv); free(Sv); free(gv); free(Pv); free(av); free(nv); free(gdv);
+    return rc;
+  }
+  if (i_plunge_out) *i_plunge_out = ip;
+  if (i_buffer_out) *i_buffer_out = ib;
+  /* the harmonic sum runs through sample ip + ib (AAK.cc:530-532 stops there) */
+  long long last = (long long)ip + ib;
+  int nsum = (int)(last + 1 < vlength ? last + 1 : vlength);
+  o_wave_job base = {t, hI, hII, tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, nmodes, mich, zeta, M_phys,
+                     par[4], par[7], par[8], par[9], par[10], 0, nsum};
+  int nt = o_threads;
+  if (nt > 1 && nsum >= 4096 * nt) {
+    o_wave_job jobs[256];
+    pthread_t th[256];
+    int started[256];
+    for (int k = 0; k < nt; ++k) {
+      jobs[k] = base;
+      jobs[k].lo = (int)((long long)nsum * k / nt);
+      jobs[k].hi = (int)((long long)nsum * (k + 1) / nt);
+      started[k] = pthread_create(&th[k], NULL, o_wave_thread, &jobs[k]) == 0;
+      if (!started[k]) o_wave_range(&jobs[k]);
+    }
+    for (int k = 0; k < nt; ++k)
+      if (started[k]) pthread_join(th[k], NULL);
+  } else {
+    o_wave_range(&base);
   }
   double t_plunge = t[ip], t_zero = t_plunge + timestep * ib;
   for (int i = ip + 1; i < vlength; ++i) {
@@ -923,7 +970,6 @@ int oracle_waveform(double *t, double *hI, double *hII, double timestep, int vle
       hII[i] = 0.;
     }
   }
-  free(J);
   free(tv); free(ev); free(vv); free(Mv); free(Sv); free(gv); free(Pv); free(av); free(nv); free(gdv);
   return 0;
 }
@@ -953,6 +999,58 @@ int oracle_genwave(double *t, double *hI, double *hII, double timestep, int vlen
   double zeta = par[0] / dist / O_GPC;
   return oracle_waveform(t, hI, hII, timestep, vlength, nmodes, zeta, par, e_traj, v_map, M_phys, M_map, S_phys, S_map,
                          dt_map, steps, backint, mich, i_plunge, i_buffer);
+}
+
+/* The GenWave call above evaluated at a list of sample indices only: the
+ * full PNevolution (the phases are a sequential sum over every sample), then
+ * the harmonic sum and the taper of AAK.cc:409-547 at idx[0..nidx) (each in
+ * [0, vlength)).  hI_out, hII_out receive nidx values; the values are those of
+ * oracle_genwave at the same samples. */
+int oracle_genwave_at(double timestep, int vlength, const double *e_traj, const double *v_map, double M_phys,
+                      const double *M_map, double mu, double S_phys, const double *S_map, double dist, double inc,
+                      double gim0, double Phi0, double qS, double phiS, double alp0, double qK, double phiK,
+                      const double *dt_map, int steps, int backint, int mich, int nmodes_override, const int64_t *idx,
+                      int nidx, double *hI_out, double *hII_out) {
+  double par[12] = {mu * O_MSUN_SEC, M_map[0] * O_MSUN_SEC, S_map[0], e_traj[0], inc, gim0, Phi0, qS, phiS, qK, phiK,
+                    alp0};
+  int nmodes = (int)(30 * par[3]);
+  if (par[3] < 0.135) nmodes = 4;
+  if (nmodes_override > 0) nmodes = nmodes_override;
+  const double zeta = par[0] / dist / O_GPC;
+  size_t nn = (size_t)vlength + 1;
+  double *tv = malloc(nn * 8), *ev = malloc(nn * 8), *vv = malloc(nn * 8), *Mv = malloc(nn * 8), *Sv = malloc(nn * 8);
+  double *gv = malloc(nn * 8), *Pv = malloc(nn * 8), *av = malloc(nn * 8), *nv = malloc(nn * 8), *gdv = malloc(nn * 8);
+  double *tt = malloc(nn * 8), *hI = malloc(nn * 8), *hII = malloc(nn * 8);
+  int ip, ib;
+  int rc = oracle_pnevolution(tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, timestep, vlength, par, e_traj, v_map, M_phys,
+                              M_map, S_phys, S_map, dt_map, steps, &ip, &ib, backint);
+  if (rc == 0) {
+    const long long last = (long long)ip + ib;
+    const double t_plunge = tv[ip], t_zero = t_plunge + timestep * ib;
+    for (int k = 0; k < nidx; ++k) {
+      const int i = (int)idx[k];
+      hI_out[k] = hII_out[k] = 0.0;
+      if (i < 0 || i >= vlength || i > last) continue;
+      o_wave_job jb = {tt, hI, hII, tv, ev, vv, Mv, Sv, gv, Pv, av, nv, gdv, nmodes, mich, zeta, M_phys,
+                       par[4], par[7], par[8], par[9], par[10], i, i + 1};
+      o_wave_range(&jb);
+      double a = hI[i], b = hII[i];
+      if (i > ip) {
+        if (i < ip + ib) {
+          const double w = exp((t_plunge - t_zero) / (tv[i] - t_plunge) + (t_plunge - t_zero) / (tv[i] - t_zero)) + 1.;
+          a /= w;
+          b /= w;
+        } else {
+          a = b = 0.0;
+        }
+      }
+      hI_out[k] = a;
+      hII_out[k] = b;
+    }
+  }
+  free(tv); free(ev); free(vv); free(Mv); free(Sv); free(gv); free(Pv); free(av); free(nv); free(gdv);
+  free(tt); free(hI); free(hII);
+  return rc;
 }
 
 /* ------------------------------------------------------------------ phases */

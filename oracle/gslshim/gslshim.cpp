@@ -132,8 +132,24 @@ double gsl_sf_bessel_Jn(int n, double x) {
   }
   return sign * std::cyl_bessel_j((double)n, x);
 }
+// GSL documents this routine as computed "using recurrence relations for
+// efficiency": the two highest orders directly, then the three-term
+// recurrence J_{n-1}(x) = (2n / x) J_n(x) - J_{n+1}(x) downwards (the stable
+// direction for J_n, DLMF 10.6.1), so that an array of five orders costs two
+// direct evaluations and three recurrence steps.
 int gsl_sf_bessel_Jn_array(int nmin, int nmax, double x, double *r) {
-  for (int n = nmin; n <= nmax; ++n) r[n - nmin] = gsl_sf_bessel_Jn(n, x);
+  if (nmax < nmin) return GSL_SUCCESS;
+  if (x == 0.0) {
+    for (int n = nmin; n <= nmax; ++n) r[n - nmin] = (n == 0) ? 1.0 : 0.0;
+    return GSL_SUCCESS;
+  }
+  double jp1 = gsl_sf_bessel_Jn(nmax + 1, x), j = gsl_sf_bessel_Jn(nmax, x);
+  for (int n = nmax; n >= nmin; --n) {
+    r[n - nmin] = j;
+    const double jm1 = (2.0 * n / x) * j - jp1;
+    jp1 = j;
+    j = jm1;
+  }
   return GSL_SUCCESS;
 }
 

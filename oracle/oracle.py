@@ -46,12 +46,26 @@ _oracle = None
 _ref = None
 
 
+def reference_src() -> str | None:
+    """The reference checkout to compile oracle/_ref from: $AAK_REFERENCE_SRC,
+    else the build container's read-only checkout when it exists."""
+    for cand in (os.environ.get("AAK_REFERENCE_SRC"), "/root/reference"):
+        if cand and os.path.exists(os.path.join(cand, "src", "suite", "AAK.cc")):
+            return cand
+    return None
+
+
 def build(force: bool = False) -> None:
     """Compile liboracle.so (and the reference build when its sources exist)."""
     import subprocess
 
-    target = "all"
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    ref = reference_src()
+    subprocess.run(["make", "-s", "-C", HERE, "all"] + ([f"REF={ref}"] if ref else []), check=True)
+
+
+def set_threads(n: int) -> None:
+    """Host threads of the oracle's per-sample harmonic sums (default 1)."""
+    oracle_lib().oracle_set_threads(int(n))
 
 
 def oracle_lib():
@@ -194,6 +208,19 @@ def oracle_genwave(pars: dict, mt: MappedTrajectory, nmodes: int = 0):
     if rc != 0:
         raise ValueError("oracle: fitting error, t_0 too close to plunge")
     return t, hI, hII, ip.value, ib.value
+
+
+def oracle_genwave_at(pars: dict, mt: MappedTrajectory, idx: np.ndarray, nmodes: int = 0):
+    """oracle_genwave at the sample indices idx only (full PNevolution, harmonic
+    sums at those samples); returns (hI[idx], hII[idx])."""
+    L = oracle_lib()
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    a, b = np.zeros(len(idx)), np.zeros(len(idx))
+    rc = L.oracle_genwave_at(*_genwave_args(pars, mt), ctypes.c_int(nmodes),
+                             idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ctypes.c_int(len(idx)), _ptr(a), _ptr(b))
+    if rc != 0:
+        raise ValueError("oracle: fitting error, t_0 too close to plunge")
+    return a, b
 
 
 def _pnevo(L, fn, pars, mt):

@@ -61,6 +61,26 @@ def mismatch(a1, a2, b1, b2):
     return 1.0 - np.dot(a, b) / np.sqrt(na * nb)
 
 
+def psd_mismatch(a1, a2, b1, b2, dt, dur=1):
+    """1 - <a|b>/sqrt(<a|a><b|b>) with the noise-weighted inner product
+    4 Re sum_k a~_k conj(b~_k) / S_n(f_k) over both channels (k >= 1; the PSD
+    is the oracle's LISA_Noise restatement, pinned to the reference's)."""
+    from oracle import oracle as O
+
+    n = len(a1)
+    f = np.fft.rfftfreq(n, dt)[1:]
+    w = 1.0 / O.lisa_noise(f, dur=dur)
+    ab = aa = bb = 0.0
+    for x, y in ((a1, b1), (a2, b2)):
+        X, Y = np.fft.rfft(x)[1:], np.fft.rfft(y)[1:]
+        ab += float(np.sum(w * (X * np.conj(Y)).real))
+        aa += float(np.sum(w * np.abs(X) ** 2))
+        bb += float(np.sum(w * np.abs(Y) ** 2))
+    if aa == 0.0 and bb == 0.0:
+        return 0.0
+    return 1.0 - ab / np.sqrt(aa * bb)
+
+
 def cuda_available():
     try:
         import torch

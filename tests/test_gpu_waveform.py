@@ -74,7 +74,11 @@ def test_dense_trajectory_matches_reference(name):
         assert rel < 1e-13, (k, rel)
     for row, k in zip((4, 5, 6), ("gim", "Phi", "alp")):
         ref = g["dense_" + k][:n_out]
-        assert np.max(np.abs(tr[row, :n_out] - ref)) < 1e-9 * max(1.0, np.abs(ref).max()), k
+        # the trajectory bar, 1e-10 relative to the phase's largest value
+        # (the sums are regrouped: tile scans with double-double carries)
+        rel = np.max(np.abs(tr[row, :n_out] - ref)) / max(1.0, np.abs(ref).max())
+        print(name, k, "max|dPhase|/max|Phase|", rel)
+        assert rel < 1e-10, (k, rel)
     for row, k in zip((7, 8), ("nu", "gimdot")):
         ref = g["dense_" + k][:n_out]
         assert np.max(np.abs(tr[row, :n_out] - ref) / np.abs(ref)) < 1e-12, k
