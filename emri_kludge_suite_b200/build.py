@@ -33,6 +33,7 @@ SOURCES = [
     "host/inspiral.cpp",
     "host/pipeline.cpp",
     "host/parmap_data.cpp",
+    "host/shard.cpp",
     "kernels/aak_dense.cu",
     "kernels/likelihood.cu",
     "kernels/parmap_mlp.cu",

@@ -93,6 +93,8 @@ struct aak_ctx {
   DevBuf<TileLink> d_link;                // look-back records, one per tile
   DevBuf<int32_t> d_flag;                 // look-back flags, one per tile
   DevBuf<unsigned long long> d_counter;   // [0] work-queue head, [1] device status word
+  DevBuf<TilePrep> d_tile_prep;           // tile pre-pass: per-tile parameters
+  DevBuf<unsigned char> d_tile_tab;       //   and per-tile Taylor tables
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
   // batched device solve of the Kerr -> AK map (opt-in: parmap_device)
   bool parmap_device = false;
@@ -624,6 +626,25 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
 
 BatchView batch_view(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride);
 
+// The tile pre-pass buffers of a waveform launch in `precision` (one
+// TilePrep and one Taylor-table slot per tile), grown as needed, set in bv.
+void drop_graph(aak_ctx *ctx);
+
+int tile_tables(aak_ctx *ctx, int precision, BatchView &bv) {
+  const int64_t tiles = std::max<int64_t>(ctx->total_tiles, 1);
+  const int64_t slot = tile_table_slot_bytes(ctx->max_nmodes, precision == 1);
+  const void *p0 = ctx->d_tile_prep.ptr, *t0 = ctx->d_tile_tab.ptr;
+  int r;
+  if ((r = ctx->d_tile_prep.reserve(tiles)) != AAK_OK || (r = ctx->d_tile_tab.reserve(tiles * slot)) != AAK_OK)
+    return r;
+  // a captured dense graph holds the old buffers: recapture on its next use
+  if (ctx->d_tile_prep.ptr != p0 || ctx->d_tile_tab.ptr != t0) drop_graph(ctx);
+  bv.tile_prep = ctx->d_tile_prep.ptr;
+  bv.tile_tab = ctx->d_tile_tab.ptr;
+  bv.tab_slot = slot;
+  return AAK_OK;
+}
+
 int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t traj_stride, int precision,
         cudaStream_t st) {
   if (!ctx->uploaded) return AAK_ERR_INVALID_PARAM;
@@ -632,11 +653,12 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   if (precision != 0 && precision != 1) return AAK_ERR_INVALID_PARAM;
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
-  const BatchView bv = batch_view(ctx, hI, hII, t, traj, traj_stride);
+  BatchView bv = batch_view(ctx, hI, hII, t, traj, traj_stride);
+  if (!traj && (r = tile_tables(ctx, precision, bv)) != AAK_OK) return r;
   if (ctx->profile && !ctx->ev[0])
     for (auto &e : ctx->ev) cudaEventCreate(&e);
   launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
-  ctx->last_launches = 1;
+  ctx->last_launches = bv.tile_prep ? 3 : 1;
   return cuda_ok(cudaGetLastError());
 }
 
@@ -659,7 +681,8 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
     if (!ctx->cap_stream && (r = cuda_ok(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking))) != AAK_OK)
       return r;
     prepare_dense_launch();
-    const BatchView bv = batch_view(ctx, hI, hII, nullptr, nullptr, 0);
+    BatchView bv = batch_view(ctx, hI, hII, nullptr, nullptr, 0);
+    if ((r = tile_tables(ctx, precision, bv)) != AAK_OK) return r;
     if ((r = cuda_ok(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal))) != AAK_OK) return r;
     // the whole dense stage: natural-spline solve of every source's knots
     // (idempotent: the same knots give the same coefficients), then the clears
@@ -684,7 +707,7 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
     ctx->g_prec = precision;
     ctx->g_gen = ctx->upload_gen;
   }
-  ctx->last_launches = 2;
+  ctx->last_launches = 4;  // spline solve, tile parameters, tile tables, waveform kernel
   return cuda_ok(cudaGraphLaunch(ctx->gexec, st));
 }
 
@@ -1951,6 +1974,7 @@ int aak_gpu_input_data(aak_gpu *g, const double *hI_f, const double *hII_f, cons
   if (!g || !hI_f || !hII_f || !ASDinv1 || !ASDinv2) return AAK_ERR_INVALID_PARAM;
   if (len != g->nbins) return AAK_ERR_INVALID_PARAM;  // the reference asserts len == fft_length
   int r;
+  if ((r = select_device(g->ctx->device)) != AAK_OK) return r;  // callers may drive several devices from one thread
   if ((r = cuda_ok(cudaMemcpy(g->d_D[0].ptr, hI_f, 2 * (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
       (r = cuda_ok(cudaMemcpy(g->d_D[1].ptr, hII_f, 2 * (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
       (r = cuda_ok(cudaMemcpy(g->d_w[0].ptr, ASDinv1, (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
@@ -1963,7 +1987,9 @@ int aak_gpu_gen(aak_gpu *g, const double *pars14) {
   if (!g || !pars14) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(g->ctx->mu);
   int32_t st = 0;
-  int r = gpu_generate(g, pars14, 1, 1, &st, true);
+  int r = select_device(g->ctx->device);
+  if (r != AAK_OK) return r;
+  r = gpu_generate(g, pars14, 1, 1, &st, true);
   if (r != AAK_OK) return r;
   return st;
 }
@@ -1974,6 +2000,7 @@ int aak_gpu_get_waveform(aak_gpu *g, double *t, double *hI, double *hII) {
   std::vector<double> buf(n, 0.0);
   int r;
   const size_t m = std::min(n, (size_t)g->row);
+  if ((r = select_device(g->ctx->device)) != AAK_OK) return r;
   if ((r = cuda_ok(cudaStreamSynchronize(g->stream))) != AAK_OK) return r;  // the template's generation
   double *dst[3] = {t, hI, hII};
   const double *src[3] = {g->d_t.ptr, g->d_H[0].ptr, g->d_H[1].ptr};
@@ -1989,6 +2016,8 @@ int aak_gpu_likelihood(aak_gpu *g, double *out2) {
   if (!g || !out2) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(g->ctx->mu);
   if (g->count != 1) return AAK_ERR_INVALID_PARAM;
+  const int r = select_device(g->ctx->device);
+  if (r != AAK_OK) return r;
   return gpu_likelihood(g, out2);
 }
 
@@ -1998,6 +2027,7 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   std::lock_guard<std::mutex> lk(g->ctx->mu);
   if (max_batch <= 0) max_batch = 256;
   double tot[4] = {0, 0, 0, 0};
+  if (select_device(g->ctx->device) != AAK_OK) return AAK_ERR_CUDA;
   // batch k + 1 is planned on the host while the device generates,
   // transforms and reduces batch k (its upload has finished by then, so the
   // plan arrays are free)
@@ -2027,6 +2057,8 @@ int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, i
                    int32_t *status) {
   if (!g) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(g->ctx->mu);
+  const int r = select_device(g->ctx->device);
+  if (r != AAK_OK) return r;
   return gpu_fisher(g, params, nd, scale, nthreads, gram, status);
 }
 

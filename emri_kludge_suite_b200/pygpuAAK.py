@@ -26,8 +26,16 @@ class pyGPUAAK:
         for prop, default in prop_defaults.items():
             setattr(self, prop, kwargs.get(prop, default))
             kwargs[prop] = kwargs.get(prop, default)
-        self.generator = GPUAAK(self.T_fit, self.init_length, self.length, self.init_dt, self.dt, self.LISA,
-                                self.backint)
+        if int(self.ndevices) > 1:
+            # the reference accepts ndevices but uses one device; here the
+            # templates of a batch are split over the devices (LPT)
+            from .shard import MultiDeviceGPUAAK
+
+            self.generator = MultiDeviceGPUAAK(range(int(self.ndevices)), self.T_fit, self.init_length, self.length,
+                                               self.init_dt, self.dt, self.LISA, self.backint)
+        else:
+            self.generator = GPUAAK(self.T_fit, self.init_length, self.length, self.init_dt, self.dt, self.LISA,
+                                    self.backint)
         self.determine_freqs_noise(**kwargs)
         self.data_info = data_info
         self.create_input_data(**kwargs)

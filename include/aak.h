@@ -427,6 +427,18 @@ int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m);
 int aak_ctx_set_parmap_device(aak_ctx *ctx, int32_t on);
 int aak_gpu_set_parmap_device(aak_gpu *g, int32_t on);
 
+/* ---------------------------------------------------------------- several devices
+ * Split of one batch over `parts` devices (or ranks): the reference's
+ * pyGPUAAK accepts an ndevices argument and evaluates every template on one
+ * device in a serial loop (pygpuAAK/pygpuAAK.py:31, 204-232).  Here a batch of
+ * n units with costs cost[i] (samples x harmonics for waveforms; equal for the
+ * templates of one likelihood batch) is divided by greedy LPT: units in
+ * decreasing cost, each to the part with the least cost so far, ties to the
+ * lowest index (the split depends on the costs alone, so every rank computes
+ * the same one).  assign[i] receives the part of unit i; load (optional,
+ * `parts` entries) the summed cost per part.  Host only. */
+int aak_lpt_partition(const double *cost, int64_t n, int32_t parts, int32_t *assign, double *load);
+
 #ifdef __cplusplus
 }
 #endif
