@@ -111,19 +111,9 @@ __device__ __forceinline__ Traj4 spline4w(const BatchView &bv, const SourceDesc 
   return eval_piece(bv.knot_y[o], bv.knot_y[o + 1], bv.knot_c[o], bv.knot_c[o + 1], kt[k], kt[k + 1], t);
 }
 
-// Stage the knots of tile g (bracket precomputed on the host, tile_knot).
-__device__ __forceinline__ void load_window(const BatchView &bv, const SourceDesc &d, int64_t g, KnotWin &w) {
-  w.k0 = bv.tile_knot[2 * g];
-  w.n = bv.tile_knot[2 * g + 1];
-  w.staged = w.n <= kWin;
-  if (w.staged)
-    for (int k = threadIdx.x; k < w.n; k += blockDim.x) {
-      const int64_t o = d.knot_offset + w.k0 + k;
-      w.t[k] = bv.knot_t[o];
-      w.y[k] = bv.knot_y[o];
-      w.c[k] = bv.knot_c[o];
-    }
-  __syncthreads();
+// Knots per unit time of the window and, for a staged window, the piece
+// coefficients (the knots are in shared memory and visible to every thread).
+__device__ __forceinline__ void finish_window(const BatchView &bv, const SourceDesc &d, KnotWin &w) {
   if (!w.staged) {
     const double *kt = bv.knot_t + d.knot_offset;
     const double span = kt[w.k0 + w.n - 1] - kt[w.k0];
@@ -144,6 +134,22 @@ __device__ __forceinline__ void load_window(const BatchView &bv, const SourceDes
     }
     __syncthreads();
   }
+}
+
+// Stage the knots of tile g (bracket precomputed on the host, tile_knot).
+__device__ __forceinline__ void load_window(const BatchView &bv, const SourceDesc &d, int64_t g, KnotWin &w) {
+  w.k0 = bv.tile_knot[2 * g];
+  w.n = bv.tile_knot[2 * g + 1];
+  w.staged = w.n <= kWin;
+  if (w.staged)
+    for (int k = threadIdx.x; k < w.n; k += blockDim.x) {
+      const int64_t o = d.knot_offset + w.k0 + k;
+      w.t[k] = bv.knot_t[o];
+      w.y[k] = bv.knot_y[o];
+      w.c[k] = bv.knot_c[o];
+    }
+  __syncthreads();
+  finish_window(bv, d, w);
 }
 
 // gamma~dot, Phidot, alphadot (AAK.cc:251-253)
@@ -401,9 +407,51 @@ __device__ void look_back_warp(const BatchView &bv, const TileCtx &c, int dir, d
   }
 }
 
+// ------------------------------------------------------------------ bulk copies into shared memory
+// One-dimensional TMA bulk copies (cp.async.bulk, global -> this CTA's
+// shared memory; no multicast: the source is this GPU's own memory) that
+// complete on an mbarrier with a byte count.  Addresses 16-byte aligned,
+// sizes multiples of 16.  Every wait is bounded.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// order this thread's earlier generic-proxy accesses of shared memory before
+// later async-proxy (bulk copy) writes to it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Wait for phase `parity` of the barrier: at most 2^25 polls (seconds), false if it did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 25); ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (it >= 32) __nanosleep(64);
+  }
+  return false;
+}
+
 // Taylor-table term counts (defined with the harmonic sums); sources with
 // more modes than kTabModes evaluate Bessel functions per sample
-constexpr int kTabModes = 128;
 __device__ __forceinline__ int taylor_terms_fp64(double q, int nmodes);
 __device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes);
 
@@ -493,10 +541,13 @@ __device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double
 // with the J values of one row from a Miller backward recurrence (or the
 // power series below x = 1), and the 2e factors of A_n expanded exactly.
 // Row n holds [A_0 .. A_K | B_0 .. B_K | C_0 .. C_K].
-constexpr int kTaylorMax64 = 10;                          // FP64 terms at most
-constexpr int kTaylorMax32 = 6;                           // FP32 terms at most
-constexpr int kRowD = (3 * (kTaylorMax64 + 1) + 1) / 2 * 2;  // doubles per FP64 row (34)
-constexpr int kRowF = (3 * (kTaylorMax32 + 1) + 3) / 4 * 4;  // floats per FP32 row (24)
+// (kTaylorMax64, kTaylorMax32, kRowD, kRowF: aak_dense.cuh)
+// Row stride of a tile with K terms: 3 (K + 1) coefficients padded to 16 bytes.
+template <typename T>
+__host__ __device__ __forceinline__ int row_stride(int K) {
+  const int per = 16 / (int)sizeof(T);
+  return (3 * (K + 1) + per - 1) / per * per;
+}
 
 // J_m(x) for m = mlo .. mhi (x >= 0) into J[m - mlo]: Miller's backward
 // recurrence from order max(start, mhi + 8), normalised by
@@ -946,6 +997,90 @@ __device__ __forceinline__ void finish(const SamplePrep<T> &P, T Sa, T Sb, T Sc,
 
 
 
+// ------------------------------------------------------------------ tile pre-pass
+// The per-tile work of the waveform kernel that does not depend on the phase
+// scan, done for every tile of the batch before it: (1) k_tile_params, one
+// thread per tile: e at the tile's first, middle and last output samples
+// (the Taylor-table centre e_c and term count K), and the raw rates of the
+// samples just before and after the tile; (2) k_tile_table, one thread per
+// (tile, harmonic): the tile's Taylor row of that harmonic.  Both evaluate
+// the spline with the same window, search and arithmetic as the waveform
+// kernel, so the values equal the ones it would compute itself.
+template <bool kSplit>
+__global__ void __launch_bounds__(128) k_tile_params(BatchView bv) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= bv.total_tiles) return;
+  const int s = find_source(bv.tile_start, bv.nsrc, g);
+  const SourceDesc &d = bv.src[s];
+  TilePrep P;
+  P.ec = 0.0;
+  P.K = -1;
+  P.stride = 0;
+  P.src = s;
+  for (int q = 0; q < 3; ++q) P.rb[q] = P.ra[q] = 0.0;
+  P.rb[1] = -1.0;
+  const int lt = (int)(g - bv.tile_start[s]);
+  const int start = lt * kTileSamples, end = min(start + kTileSamples, d.vlength);
+  const int lim = min(end, n_eff(d));
+  if (d.status == 0 && lim > start) {
+    KnotWin w{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0};
+    w.k0 = bv.tile_knot[2 * g];
+    w.n = bv.tile_knot[2 * g + 1];
+    const double *kt = bv.knot_t + d.knot_offset;
+    const double span = kt[w.k0 + w.n - 1] - kt[w.k0];
+    w.inv_h = (span > 0.0) ? (double)(w.n - 1) / span : 0.0;
+    const double e0 = spline4w(bv, d, sample_time(d, start), w).e;
+    const double em = spline4w(bv, d, sample_time(d, (start + lim - 1) / 2), w).e;
+    const double e1 = spline4w(bv, d, sample_time(d, lim - 1), w).e;
+    {
+      double r[3] = {0, 0, 0};
+      const int i = start - 1;
+      const bool ok = i >= 0 && i < d.vlength;
+      if (ok) phase_rates(d, spline4w(bv, d, sample_time(d, i), w), r);
+      P.rb[0] = r[0];
+      P.rb[1] = ok ? r[1] : -1.0;
+      P.rb[2] = r[2];
+    }
+    if (end - 1 < d.i0 && end < d.vlength) {
+      double r[3] = {0, 0, 0};
+      phase_rates(d, spline4w(bv, d, sample_time(d, end), w), r);
+      P.ra[0] = r[0];
+      P.ra[1] = r[1];
+      P.ra[2] = r[2];
+    }
+    int K = 0;
+    double ec = 0.0;
+    if (d.nmodes <= kTabModes) {
+      ec = em;
+      const double de = fmax(fabs(e0 - ec), fabs(e1 - ec));
+      if (ec > 1e-6) {
+        const double q = d.nmodes * (1.25 * de + 1e-15);  // bounds n |e - e_c| over the tile
+        K = kSplit ? taylor_terms_fp32(q, d.nmodes) : taylor_terms_fp64(q, d.nmodes);
+      }
+    }
+    P.ec = ec;
+    P.K = (int16_t)K;
+    P.stride = (int16_t)(K > 0 ? (kSplit ? row_stride<float>(K) : row_stride<double>(K)) : 0);
+  }
+  bv.tile_prep[g] = P;
+}
+
+template <bool kSplit>
+__global__ void __launch_bounds__(128) k_tile_table(BatchView bv, int rows) {
+  using T = typename std::conditional<kSplit, float, double>::type;
+  const int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t g = id / rows;
+  if (g >= bv.total_tiles) return;
+  const int n = (int)(id - g * rows) + 1;
+  const TilePrep &P = bv.tile_prep[g];
+  const int K = P.K;
+  if (K <= 0) return;
+  const SourceDesc &d = bv.src[P.src];
+  if (n > d.nmodes) return;
+  T *row = reinterpret_cast<T *>(static_cast<unsigned char *>(bv.tile_tab) + g * bv.tab_slot) + (n - 1) * P.stride;
+  build_taylor_row<T>(row, n, P.ec, K, bv.bessel_start[d.bessel_offset + n - 1]);
+}
+
 // ------------------------------------------------------------------ waveform kernel
 // Samples per thread whose harmonic sums run side by side (divides kTileChunks).
 // 1: build the Taylor table after phase 1, on warps 1-7 while warp 0 looks
@@ -976,23 +1111,41 @@ constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double)
 // after the plunge buffer are frozen afterwards by k_phase_freeze.
 // kMode 2, the phase grid of the frequency-domain TDI (PNevolutionTDI,
 // AAKTDI.cc:311-469): the same pass writes kTdiRows rows (TdiRow order).
-template <bool kSplit, int kMode = 0>
+// kPre (waveform mode with the tile pre-pass): each tile's source record,
+// TilePrep, knot window and Taylor table arrive in shared memory by bulk
+// copies that thread 0 issues at the start of the tile (the table's on a
+// second mbarrier, waited for only before phase 2); no table is built here.
+static_assert(sizeof(SourceDesc) % 16 == 0, "SourceDesc lands in shared memory with one bulk copy");
+template <bool kSplit, int kMode = 0, bool kPre = false>
 __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
   constexpr bool kPhase = kMode != 0, kTdi = kMode == 2;
+  static_assert(!kPre || kMode == 0, "the pre-pass serves the waveform mode");
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
   __shared__ double s_par[3], s_rb[3], s_ra[3], s_cy[7], s_lastP;  // tile parameters, chain carry
   __shared__ __align__(16) SourceDesc s_desc;           // this tile's source
+  __shared__ __align__(16) TilePrep s_prep;             // kPre: this tile's parameters
+  __shared__ __align__(8) uint64_t s_mbar[2];           // kPre: bulk-copy barriers (record + window, table)
+  __shared__ int s_win[4];                              // kPre: window first knot, knots, offset in s_wt, table
   __shared__ Geom<typename std::conditional<kSplit, float, double>::type> s_geom;
-  __shared__ double s_wt[kWin];
-  __shared__ double4 s_wy[kWin], s_wc[kWin], s_wb[kWin], s_wd[kWin];
+  __shared__ __align__(16) double s_wt[kWin + 2];
+  __shared__ __align__(16) double4 s_wy[kWin], s_wc[kWin], s_wb[kWin], s_wd[kWin];
   double *sv_e = s_dyn, *sv_om = s_dyn + kTileSamples, *sv_gim = s_dyn + 2 * kTileSamples;
   double *sv_Phi = s_dyn + 3 * kTileSamples, *sv_alp = s_dyn + 4 * kTileSamples, *sv_nu = s_dyn + 5 * kTileSamples;
   double *sv_gd = s_dyn + 6 * kTileSamples;
   double *tabD = s_dyn + kDynVals * kTileSamples;  // Taylor table after the per-sample values
   float *tabF = reinterpret_cast<float *>(tabD);
   const int tid = threadIdx.x;
+  uint32_t ph0 = 0u, ph1 = 0u;  // kPre: phase parity of the two barriers
+  if constexpr (kPre) {
+    if (tid == 0) {
+      mbar_init(&s_mbar[0], 1);
+      mbar_init(&s_mbar[1], 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
   for (;;) {
     if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
     __syncthreads();
@@ -1026,22 +1179,80 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
       continue;
     }
-    // stage the source record and its response constants (the window's barrier publishes them)
-    {
-      const uint4 *src4 = reinterpret_cast<const uint4 *>(dp);
-      uint4 *dst4 = reinterpret_cast<uint4 *>(&s_desc);
-      for (int k = tid; k < (int)(sizeof(SourceDesc) / 16); k += kTileThreads) dst4[k] = src4[k];
-      if (tid == kTileThreads - 1) make_geom(*dp, s_geom);
-    }
     KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
-    load_window(bv, *dp, g, w);
+    if constexpr (kPre) {
+      using TT = typename std::conditional<kSplit, float, double>::type;
+      if (tid == 0) {
+        // every thread's reads of the previous tile's shared memory are
+        // ordered before these copies by the loop's barriers
+        fence_proxy_async_smem();
+        const int k0 = bv.tile_knot[2 * g], nk = bv.tile_knot[2 * g + 1];
+        const bool staged = nk > 0 && nk <= kWin;
+        const int64_t off = dp->knot_offset + k0;
+        const int64_t a = off & ~(int64_t)1;  // knot times from a 16-byte boundary
+        const int toff = (int)(off - a);
+        const int cnt = (nk + toff + 1) & ~1;
+        const TilePrep *pg = bv.tile_prep + g;
+        const int Kt = pg->K, st = pg->stride, nm = dp->nmodes;
+        const uint32_t b0 = (uint32_t)(sizeof(SourceDesc) + sizeof(TilePrep)) +
+                            (staged ? (uint32_t)(cnt * sizeof(double) + 2 * nk * sizeof(double4)) : 0u);
+        mbar_arrive_expect_tx(&s_mbar[0], b0);
+        bulk_copy_g2s(&s_desc, dp, (uint32_t)sizeof(SourceDesc), &s_mbar[0]);
+        bulk_copy_g2s(&s_prep, pg, (uint32_t)sizeof(TilePrep), &s_mbar[0]);
+        if (staged) {
+          bulk_copy_g2s(s_wt, bv.knot_t + a, (uint32_t)(cnt * sizeof(double)), &s_mbar[0]);
+          bulk_copy_g2s(s_wy, bv.knot_y + off, (uint32_t)(nk * sizeof(double4)), &s_mbar[0]);
+          bulk_copy_g2s(s_wc, bv.knot_c + off, (uint32_t)(nk * sizeof(double4)), &s_mbar[0]);
+        }
+        const bool tab = Kt > 0 && nm <= kTabModes;
+        if (tab) {
+          const uint32_t b1 = (uint32_t)nm * (uint32_t)st * (uint32_t)sizeof(TT);
+          mbar_arrive_expect_tx(&s_mbar[1], b1);
+          bulk_copy_g2s(tabD, static_cast<const unsigned char *>(bv.tile_tab) + g * bv.tab_slot, b1, &s_mbar[1]);
+        }
+        s_win[0] = k0;
+        s_win[1] = nk;
+        s_win[2] = toff;
+        s_win[3] = tab ? 1 : 0;
+      }
+      if (tid == kTileThreads - 1) make_geom(*dp, s_geom);
+      const bool ok = mbar_wait_bounded(&s_mbar[0], ph0);
+      ph0 ^= 1u;
+      if (__syncthreads_or(!ok)) {  // a copy did not land: report it and stop this CTA
+        if (tid == 0) {
+          atomicExch(bv.device_status, 1u);
+          if (bv.status_report) atomicExch(bv.status_report, 1u);
+        }
+        return;
+      }
+      w.k0 = s_win[0];
+      w.n = s_win[1];
+      w.staged = w.n > 0 && w.n <= kWin;
+      w.t = s_wt + s_win[2];
+      finish_window(bv, *dp, w);
+    } else {
+      // stage the source record and its response constants (the window's barrier publishes them)
+      {
+        const uint4 *src4 = reinterpret_cast<const uint4 *>(dp);
+        uint4 *dst4 = reinterpret_cast<uint4 *>(&s_desc);
+        for (int k = tid; k < (int)(sizeof(SourceDesc) / 16); k += kTileThreads) dst4[k] = src4[k];
+        if (tid == kTileThreads - 1) make_geom(*dp, s_geom);
+      }
+      load_window(bv, *dp, g, w);
+    }
     const SourceDesc &d = s_desc;
     const int32_t *bstart = bv.bessel_start + d.bessel_offset;
     const double X0[3] = {d.gim0, d.Phi0, d.alp0};
     // tile parameters from the staged window: e at the first, middle and last
     // output samples (Bessel-table centre and term count), and the raw rates
-    // of the sample just before the tile (Phi: -1 if there is none)
-    if (tid < 3) {
+    // of the sample just before the tile (Phi: -1 if there is none); kPre:
+    // from the pre-pass
+    if (kPre) {
+      if (tid < 3) {
+        s_rb[tid] = s_prep.rb[tid];
+        s_ra[tid] = s_prep.ra[tid];
+      }
+    } else if (tid < 3) {
       const int i = (tid == 0) ? c.start : (tid == 1) ? (c.start + lim - 1) / 2 : lim - 1;
       s_par[tid] = spline4w(bv, d, sample_time(d, i), w).e;
     } else if (tid == 32) {
@@ -1066,7 +1277,10 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     __syncthreads();
     double ec = 0.0;
     int K = 0;
-    if (d.nmodes <= kTabModes) {
+    if (kPre) {
+      ec = s_prep.ec;
+      K = max((int)s_prep.K, 0);
+    } else if (d.nmodes <= kTabModes) {
       ec = s_par[1];
       const double de = fmax(fabs(s_par[0] - ec), fabs(s_par[2] - ec));
       if (ec > 1e-6) {
@@ -1095,7 +1309,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const double Cin = needC ? s_cy[6] : 0.0;
 #if !AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread per harmonic); its barrier is the first one of phase 1
-    if (!kPhase && K > 0 && !bv.trajectory_only)
+    if (!kPhase && !kPre && K > 0 && !bv.trajectory_only)
       for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
         if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
@@ -1302,7 +1516,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     }
 #if AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread of warps 1-7 per harmonic) while warp 0 looks back
-    else if (!kPhase && K > 0 && !bv.trajectory_only)
+    else if (!kPhase && !kPre && K > 0 && !bv.trajectory_only)
       for (int n = tid - 31; n <= d.nmodes; n += kTileThreads - 32) {
         if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
@@ -1362,11 +1576,25 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     // ---------------- phase 2: harmonic sums of this thread's own samples,
     // kJoint of them at a time (shared table loads, independent recurrences)
     if (kPhase || bv.trajectory_only) continue;
+    if constexpr (kPre) {
+      if (s_win[3]) {  // the tile's table (uniform)
+        const bool ok = mbar_wait_bounded(&s_mbar[1], ph1);
+        ph1 ^= 1u;
+        if (__syncthreads_or(!ok)) {
+          if (tid == 0) {
+            atomicExch(bv.device_status, 1u);
+            if (bv.status_report) atomicExch(bv.status_report, 1u);
+          }
+          return;
+        }
+      }
+    }
     const double t_plunge = sample_time(d, d.i_plunge);
     const double t_zero = t_plunge + d.dt * d.i_buffer;
     using T = typename std::conditional<kSplit, float, double>::type;
     constexpr int kJoint = kSplit ? AAK_JOINT_SPLIT : AAK_JOINT_FP64;
     const T *tab = kSplit ? reinterpret_cast<const T *>(tabF) : reinterpret_cast<const T *>(tabD);
+    const int rs = kPre ? (int)s_prep.stride : (kSplit ? kRowF : kRowD);  // table row stride
 #pragma unroll 1
     for (int g0 = 0; g0 < kTileChunks; g0 += kJoint) {
       SamplePrep<T> P[kJoint];
@@ -1394,19 +1622,19 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
       if constexpr (kSplit) {
         switch (K) {
-          case 2: mode_sums_taylor_multi<2, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 3: mode_sums_taylor_multi<3, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, kRowF, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 2: mode_sums_taylor_multi<2, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 3: mode_sums_taylor_multi<3, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
           default: break;
         }
       } else {
         switch (K) {
-          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 5: mode_sums_taylor_multi<5, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 8: mode_sums_taylor_multi<8, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 10: mode_sums_taylor_multi<10, T, kJoint>(tab, d.nmodes, kRowD, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 5: mode_sums_taylor_multi<5, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 8: mode_sums_taylor_multi<8, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 10: mode_sums_taylor_multi<10, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
           default: break;
         }
       }
@@ -1641,34 +1869,47 @@ void prepare_dense_launch() {
     const int most = (int)(kWaveDynSmem + (size_t)kTabModes * kRowD * sizeof(double));
     cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    cudaFuncSetAttribute(k_waveform<true, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    cudaFuncSetAttribute(k_waveform<false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     cudaFuncSetAttribute(k_waveform<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     cudaFuncSetAttribute(k_waveform<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     attrs_set.fetch_or(bit);
   }
 }
 
-void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision) {
-  if (bv.total_tiles <= 0) return;
+template <bool kSplit>
+void launch_dense_t(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[0], stream);
   cudaMemsetAsync(bv.work_counter, 0, sizeof(unsigned long long), stream);
   cudaMemsetAsync(bv.link_flag, 0, (size_t)bv.total_tiles * sizeof(int32_t), stream);
-  if (ev) {
-    cudaEventRecord(ev[1], stream);
-    cudaEventRecord(ev[2], stream);
-  }
+  if (ev) cudaEventRecord(ev[1], stream);
   // per-sample values, then the Taylor table sized for the batch's harmonic count
   const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
-  const size_t dyn = kWaveDynSmem + (size_t)rows * (precision == 1 ? kRowF * sizeof(float) : kRowD * sizeof(double));
+  const size_t dyn = kWaveDynSmem + (size_t)rows * (kSplit ? kRowF * sizeof(float) : kRowD * sizeof(double));
+  const bool pre =
+      bv.tile_prep && bv.tile_tab && !bv.trajectory_only && bv.tab_slot >= tile_table_slot_bytes(rows, kSplit);
   prepare_dense_launch();
+  if (pre) {
+    const int64_t tiles = bv.total_tiles;
+    k_tile_params<kSplit><<<(unsigned)((tiles + 127) / 128), 128, 0, stream>>>(bv);
+    k_tile_table<kSplit><<<(unsigned)((tiles * rows + 127) / 128), 128, 0, stream>>>(bv, rows);
+  }
+  if (ev) cudaEventRecord(ev[2], stream);
   // persistent grid: every CTA that fits on the device at once
   int resident = 0;
-  if (precision == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<true>, kTileThreads, dyn);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false>, kTileThreads, dyn);
+  if (pre) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<kSplit, 0, true>, kTileThreads, dyn);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<kSplit>, kTileThreads, dyn);
   resident = std::max(resident, 1);
   const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
-  if (precision == 1) k_waveform<true><<<grid2, kTileThreads, dyn, stream>>>(bv);
-  else k_waveform<false><<<grid2, kTileThreads, dyn, stream>>>(bv);
+  if (pre) k_waveform<kSplit, 0, true><<<grid2, kTileThreads, dyn, stream>>>(bv);
+  else k_waveform<kSplit><<<grid2, kTileThreads, dyn, stream>>>(bv);
   if (ev) cudaEventRecord(ev[3], stream);
+}
+
+void launch_dense(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev, int precision) {
+  if (bv.total_tiles <= 0) return;
+  if (precision == 1) launch_dense_t<true>(bv, num_sms, stream, ev);
+  else launch_dense_t<false>(bv, num_sms, stream, ev);
 }
 
 // The phases of the samples after the plunge buffer hold their values at

@@ -37,6 +37,36 @@ struct TileLink {
   double inc_C;             // clamped Phidot after the tile (0 before the first forward sample)
 };
 
+// Per-tile values the waveform kernel needs before its phase pass, computed
+// for every tile of a batch by the tile pre-pass (k_tile_params): the centre
+// e_c and term count K of the tile's Bessel table, and the raw AB2 rates of
+// the samples just before and just after the tile.  64 bytes, so that it
+// lands in shared memory with one bulk copy.
+struct alignas(16) TilePrep {
+  double ec;
+  int16_t K;        // Taylor terms (0: per-sample Miller recurrence; -1: no harmonic sums in the tile)
+  int16_t stride;   // elements per table row of the tile
+  int32_t src;      // source of the tile
+  double rb[3];     // rates of sample start - 1 (rb[1] = -1: there is none)
+  double ra[3];     // rates of sample end (for the backward AB2 step of the tile's last sample)
+};
+static_assert(sizeof(TilePrep) == 64, "TilePrep is one 64-byte bulk copy");
+
+// Taylor-table rows: FP64 terms at most (K <= 10) and FP32 terms at most
+// (K <= 6); a tile's rows hold 3 (K + 1) coefficients, padded to 16 bytes.
+constexpr int kTaylorMax64 = 10;
+constexpr int kTaylorMax32 = 6;
+constexpr int kRowD = (3 * (kTaylorMax64 + 1) + 1) / 2 * 2;  // doubles per FP64 row at most (34)
+constexpr int kRowF = (3 * (kTaylorMax32 + 1) + 3) / 4 * 4;  // floats per FP32 row at most (24)
+// Harmonic counts up to kTabModes use the tables (more: per-sample Bessel recurrences).
+constexpr int kTabModes = 128;
+// Bytes of one tile's slot in the pre-built table array for `rows` harmonics
+// (largest harmonic count of the batch) in FP64 (split = false) or FP32 rows.
+inline int64_t tile_table_slot_bytes(int rows, bool split) {
+  const int r = (rows > 0 && rows < kTabModes) ? rows : kTabModes;
+  return split ? (int64_t)r * kRowF * (int64_t)sizeof(float) : (int64_t)r * kRowD * (int64_t)sizeof(double);
+}
+
 // Everything the kernels read about a batch.
 struct BatchView {
   const SourceDesc *src;
@@ -63,11 +93,22 @@ struct BatchView {
   long long lookback_cycles = 0;     // bound of one look-back wait in SM clocks (<= 0: about 2 s)
   double *phase_out = nullptr;       // launch_phase: 8 x phase_stride (t, phase_r, phase_theta, phase_phi,
   int64_t phase_stride = 0;          //   omega_r, omega_theta, omega_phi, e), indexed by src.out_offset + i
+  // optional tile pre-pass buffers (launch_dense): one TilePrep per tile and
+  // one table slot of tab_slot bytes per tile; without them the waveform
+  // kernel computes both inside each tile
+  TilePrep *tile_prep = nullptr;
+  void *tile_tab = nullptr;
+  int64_t tab_slot = 0;
 };
 
 // Clear the work queue and the look-back flags, then launch the waveform
-// kernel, on `stream`.  ev (optional, 4 events): ev[0]..ev[1] bracket the
-// clears, ev[2]..ev[3] the kernel.
+// kernel, on `stream`.  With bv.tile_prep and bv.tile_tab set (and no
+// trajectory output), the tile pre-pass (tile parameters, then every tile's
+// Taylor table, harmonics in parallel) runs first and the waveform kernel
+// stages each tile's source record, parameters, knot window and table in
+// shared memory with bulk copies.  ev (optional, 4 events): ev[0]..ev[1]
+// bracket the clears, ev[1]..ev[2] the pre-pass (empty without it),
+// ev[2]..ev[3] the waveform kernel.
 void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEvent_t *ev);
 // precision 0: FP64 throughout; 1: split (FP64 phases and reductions, FP32
 // geometry, response, Bessel evaluation and harmonic recurrence).
