@@ -16,9 +16,11 @@ A step is one pass of the dense AAK path over the whole batch.
   --impl reference : the reference's own CPU AAK (oracle/_ref, compiled from
           its sources) on all host cores, same workload, bounded sample.
 
-Multi-GPU (torchrun, one rank per GPU): every rank generates its own
-512-source batch (seed + rank); no collective on the data path; value is the
-total over ranks divided by the max-over-ranks device time ("weak" scaling).
+Multi-GPU (torchrun, one rank per GPU): one caller batch of 512 x N sources
+(and 4096 x N likelihood templates) is split over the ranks by greedy LPT on
+samples x harmonics; no collective on the data path, one all-gather of the
+per-template (4<h|d>, 4<h|h>) rows; value is the total over ranks divided by
+the max-over-ranks device time ("weak" scaling: 512 sources per GPU).
 """
 from __future__ import annotations
 
@@ -41,6 +43,29 @@ from emri_kludge_suite_b200.workloads import DT, MSUN_SEC, NMODES, SEED, YEAR, c
 
 
 # ----------------------------------------------------------------------------- workload
+# Algorithmic work of the harmonic sum, in the convention of the FP32/FP64 FMA
+# probes (every multiply and every add one flop, an FMA two): per harmonic the
+# reference's algebra of src/suite/AAK.cc:484-526 (Doppler phase, the a, b, c
+# combinations, A+, Ax, the NK-frame rotation and the two responses: 24
+# FMA-equivalents = 48 flops) and three Bessel recurrence steps (2 flops each);
+# 60 flops per sample outside the harmonic loop.  Transcendentals (sin/cos of
+# n Phi, the Bessel seeds) are SFU work and not counted.
+FLOPS_PER_SAMPLE_BASE = 60.0
+FLOPS_PER_HARMONIC = 48.0 + 6.0
+
+
+def flops_per_sample(nmodes: float) -> float:
+    return FLOPS_PER_SAMPLE_BASE + FLOPS_PER_HARMONIC * nmodes
+
+
+def bench_config(nsrc: int, world: int) -> dict:
+    """The workload description both arms print (same keys and values)."""
+    return {"workload": f"config1: {nsrc} AAK sources/GPU, T~U(0.1,1) yr, dt=10 s, n=1..30, LISA response",
+            "nsrc_per_gpu": nsrc, "nmodes": NMODES, "seed": SEED, "dt_s": DT,
+            "l2": "outputs 16 B/sample x ~8.7e8 samples per GPU exceed the 126 MB L2",
+            "parallelism": f"sources sharded, {world} rank(s)"}
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -115,8 +140,15 @@ def _ref_worker(args):
     return samples, busy, done
 
 
-def cpu_reference(sources, budget_s: float = 15.0, sample_len: int = 20000, procs: int = 0) -> dict:
-    """Reference CPU AAK throughput on the host cores (spawn pool; the reference is not thread-safe)."""
+def cpu_reference(sources, budget_s: float = 15.0, sample_len: int = 20000, procs: int = 0,
+                  untruncated: bool = False) -> dict:
+    """Reference CPU AAK throughput on the host cores (spawn pool; the reference is not thread-safe).
+
+    The bounded sample truncates the configuration-1 sources to sample_len
+    samples, which spreads each source's fixed front-end cost (LSO search,
+    Kerr constants, the map solve) over fewer samples than at full length.
+    untruncated=True also times the procs shortest sources at their full
+    length (one per process) as a check on that bias."""
     import multiprocessing as mp
 
     from oracle import oracle as O
@@ -136,14 +168,84 @@ def cpu_reference(sources, budget_s: float = 15.0, sample_len: int = 20000, proc
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
         res = pool.map(_ref_worker, [(t, budget_s) for t in per])
+        full = None
+        if untruncated:
+            short = sorted(sources, key=lambda p: int(p["length"]))[:procs]
+            rf = pool.map(_ref_worker, [([p], 1e9) for p in short])
+            fs, fb = sum(r[0] for r in rf), max(r[1] for r in rf)
+            full = {"value": fs / fb if fb > 0 else 0.0, "unit": "samples/s", "sources": sum(r[2] for r in rf),
+                    "samples": fs, "sample": f"the {procs} shortest config-1 sources at full length "
+                                              f"({min(int(p['length']) for p in short)}-"
+                                              f"{max(int(p['length']) for p in short)} samples), one per process"}
     wall = time.perf_counter() - t0
     samples = sum(r[0] for r in res)
     busy = max(r[1] for r in res)
     done = sum(r[2] for r in res)
-    return {"value": samples / busy if busy > 0 else 0.0, "unit": "samples/s", "cores": procs, "kind": "reference",
-            "sample": f"{done} config-1 sources truncated to {sample_len} samples, front end + waveform() with "
-                      f"n=1..{NMODES} (reference AAK, GSL shim), {procs} processes, {budget_s:.0f} s budget each",
-            "wall_s": wall}
+    out = {"value": samples / busy if busy > 0 else 0.0, "unit": "samples/s", "cores": procs, "kind": "reference",
+           "sample": f"{done} config-1 sources truncated to {sample_len} samples, front end + waveform() with "
+                     f"n=1..{NMODES} (reference AAK, GSL shim with Jn_array as a downward recurrence), "
+                     f"{procs} processes, {budget_s:.0f} s budget each",
+           "wall_s": wall}
+    if full is not None:
+        out["untruncated"] = full
+    return out
+
+
+def _ref_like_worker(args):
+    """One process: the reference AAKwave on the configuration-4 fiducial source
+    truncated to sample_len samples, then one full-length FP64 rFFT inner
+    product of both channels with the data (pyGPUAAK.NLL's host work per
+    template, pygpuAAK.py:204-232)."""
+    sample_len, length = args
+    sys.path.insert(0, REPO)
+    from oracle import oracle as O
+
+    iota, s_, p, e, M, mu, gamma, psi, alph, thS, phS, thK, phK, D = FIDUCIAL
+    pars = dict(backint=False, LISA=True, length=sample_len, dt=DT, p=p, T=sample_len * DT / YEAR, f=0.0, T_fit=1.0,
+                mu=mu, M=M, s=s_, e=e, iota=iota, gamma=gamma, psi=psi, theta_S=thS, phi_S=phS, theta_K=thK,
+                phi_K=phK, alpha=alph, D=D)
+    O.ref_aakwave(pars)  # warm-up
+    t0 = time.perf_counter()
+    O.ref_aakwave(pars)
+    rate = sample_len / (time.perf_counter() - t0)
+    rng = np.random.default_rng(1)
+    hI, hII = rng.standard_normal(length), rng.standard_normal(length)
+    nb = length // 2 + 1
+    dI, dII = rng.standard_normal(nb) + 1j * rng.standard_normal(nb), rng.standard_normal(nb) + 1j * rng.standard_normal(nb)
+    w = rng.random(nb)
+    t0 = time.perf_counter()
+    fI, fII = np.fft.rfft(hI) * w, np.fft.rfft(hII) * w
+    d_h = 4.0 * float(np.real(np.vdot(fI, dI) + np.vdot(fII, dII)))
+    h_h = 4.0 * float(np.real(np.vdot(fI, fI) + np.vdot(fII, fII)))
+    t_ip = time.perf_counter() - t0
+    assert np.isfinite(d_h + h_h)
+    return rate, t_ip
+
+
+def cpu_likelihood_reference(procs: int = 0, sample_len: int = 200000) -> dict:
+    """likelihoods/s of the reference's CPU path on the host cores: per
+    template its own AAKwave (timed on a sample_len-sample truncation of the
+    fiducial source, scaled to LIKE_LENGTH samples) plus a full-length numpy
+    rFFT inner product, one template at a time per process."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return {"value": None, "unit": "likelihoods/s", "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/libaakref.so is not built"}
+    procs = procs or (os.cpu_count() or 1)
+    with mp.get_context("spawn").Pool(procs) as pool:
+        res = pool.map(_ref_like_worker, [(sample_len, LIKE_LENGTH)] * procs)
+    per_template = [LIKE_LENGTH / r + t for r, t in res]
+    value = sum(1.0 / x for x in per_template)
+    return {"value": value, "unit": "likelihoods/s", "cores": procs, "kind": "reference",
+            "seconds_per_likelihood": float(np.mean(per_template)),
+            "waveform_samples_per_s_per_core": float(np.mean([r for r, _ in res])),
+            "fft_inner_product_s": float(np.mean([t for _, t in res])),
+            "sample": f"reference AAKwave on the fiducial config-4 source truncated to {sample_len} samples (scaled to "
+                      f"{LIKE_LENGTH}), plus a {LIKE_LENGTH}-sample numpy rFFT inner product of both channels; "
+                      f"{procs} processes, one template each"}
 
 
 # ----------------------------------------------------------------------------- likelihood (config 4)
@@ -293,7 +395,8 @@ def ref_fisher_seconds(sample_len: int = 200000) -> dict:
                                           f"{rate:.3g} samples/s, scaled to 28 x {LIKE_LENGTH} samples"}
 
 
-def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int = 0) -> dict:
+def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int = 0, with_cpu: bool = False,
+                   rank: int = 0, world: int = 1) -> dict:
     """likelihoods/s of the batched path: host planning + waveforms + FFT + reduction, end to end per call."""
     from emri_kludge_suite_b200.gpuAAK import GPUAAK
     from emri_kludge_suite_b200.LISAnoise import LISA_Noise, generate_noise_frequencies, generate_noise_single_channel
@@ -318,7 +421,17 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
     n2 = generate_noise_single_channel(LISA_Noise, [], {"dur": 1}, df, freqs, rng)
     dI, dII = w * (hI_f + n1), w * (hII_f + n2)
     g.input_data(dI, dII, w, w)
-    X = config4_templates(n_templates)
+    # one caller batch of n_templates x world templates, split over the ranks
+    # (equal costs: LPT balances the counts); per-template (4<h|d>, 4<h|h>)
+    # rows are gathered back with one all-gather
+    X_all = config4_templates(n_templates * world)
+    mine = np.arange(len(X_all))
+    if world > 1:
+        from emri_kludge_suite_b200.shard import rank_indices
+
+        mine = rank_indices(np.ones(len(X_all)), rank, world)
+    X = X_all[mine]
+    n_templates = len(X)
     d_d = 4.0 * float(np.sum(np.abs(dI) ** 2) + np.sum(np.abs(dII) ** 2))  # pygpuAAK.py:67
 
     def timed():
@@ -332,6 +445,13 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
                        "failed": int(np.sum(st != 0)), "ms": ms}
 
     out64, st64, plain = timed()
+    if world > 1:
+        from emri_kludge_suite_b200.shard import gather_rows
+
+        t0 = time.perf_counter()
+        gathered = gather_rows(out64, mine, len(X_all))
+        plain["gather"] = {"templates": len(X_all), "seconds": time.perf_counter() - t0,
+                           "finite": bool(np.all(np.isfinite(gathered)))}
     res = {"workload": "config4: fiducial config-0 source, 3.2e6 samples (1.014 yr, dt=10 s), LISA-coloured noise, "
                        "templates perturbed 1e-5 rel (M, mu, p0) / 1e-3 rad (angles), reference harmonic rule",
            "templates": n_templates, "samples_per_template": LIKE_LENGTH, "fp64_plain": plain}
@@ -351,6 +471,8 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
     fast["max_abs_logL"] = float(np.max(np.abs(logl64[ok]))) if ok.any() else None
     fast["warm_start"] = model is not None
     res["split_warm"] = fast
+    if with_cpu:
+        res["cpu_baseline"] = cpu_likelihood_reference()
     return res
 
 
@@ -513,7 +635,15 @@ def run_gpu(args, rank, world, local_rank):
     if world > 1:
         import torch.distributed as dist
 
-    sources, rng = config1(SEED + rank, args.nsrc)
+    # one caller batch of nsrc x world sources, split over the ranks by LPT on
+    # samples x harmonics (world = 1: the seeded 512-source draw itself)
+    from emri_kludge_suite_b200.shard import rank_indices, source_costs
+
+    all_sources, rng = config1(SEED, args.nsrc * world)
+    mine = rank_indices(source_costs(all_sources, NMODES), rank, world) if world > 1 else np.arange(len(all_sources))
+    sources = [all_sources[i] for i in mine]
+    if world > 1:
+        rng = np.random.default_rng([SEED, rank])  # redraws (rare) stay on their rank
     wb = E.WaveBatch(local_rank)
     nthreads = os.cpu_count() or 1
     t_plan0 = time.perf_counter()
@@ -610,7 +740,7 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
     clk = clocks.stop()
     ms = reduce_max(ev0.elapsed_time(ev1))
-    launches = 1 * args.steps  # k_waveform<split>; the clears are memset nodes
+    launches = 2 * args.steps  # k_spline_coeffs and k_waveform<split>; the clears are memset nodes
     value = N_all * args.steps / (ms * 1e-3)
     # accuracy of every source against the FP64 outputs of the same batch
     worst_mm, worst_rel, mms = 0.0, 0.0, []
@@ -628,8 +758,8 @@ def run_gpu(args, rank, world, local_rank):
         worst_mm, worst_rel = max(worst_mm, mm), max(worst_rel, rel)
     accuracy = {"max_mismatch": worst_mm, "median_mismatch": float(np.median(mms)), "max_rel_dh": worst_rel,
                 "sources": len(sources), "bar": 1e-6}
-    flops_per_sample = 60.0 + NMODES * 33.0  # algorithmic flops per sample: 60 per sample + 33 per harmonic
-    ach64 = flops_per_sample * N / (kern[2] * 1e-3) / 1e12
+    fps = flops_per_sample(NMODES)
+    ach64 = fps * N / (kern[2] * 1e-3) / 1e12
     fp64 = {"value": value64, "unit": "samples/s", "ms_per_step": ms64 / args.steps,
             "kernel_ms": {"clears": kern[0], "waveform_fp64": kern[2]},
             "roofline": {"kernel": "k_waveform<fp64>", "bound": "fp64", "achieved": ach64, "peak": fp64_peak,
@@ -677,9 +807,12 @@ def run_gpu(args, rank, world, local_rank):
         del pI, pII, traj
         wp.close()
 
-    # ---- configuration 2: split precision vs FP64 per source at high eccentricity
+    # ---- configuration 2: split precision vs FP64 per source at high eccentricity,
+    #      mismatch flat and weighted by the LISA noise PSD
     cfg2 = None
     if args.config2_sources > 0:
+        from emri_kludge_suite_b200.LISAnoise import LISA_Noise
+
         src2, nm2 = config2(SEED + 2 + rank, args.config2_sources)
         w2 = E.WaveBatch(local_rank)
         w2.plan(src2, nmodes=nm2, nthreads=nthreads)
@@ -695,8 +828,19 @@ def run_gpu(args, rank, world, local_rank):
         ev1.record(stream)
         torch.cuda.synchronize()
         ms2 = ev0.elapsed_time(ev1)
+        # the PSD (dur = 1 yr) on a log grid of 2e5 points, interpolated in log f on the device
+        lf0, lf1, ng = math.log(1e-9), math.log(0.06), 200_000
+        logS = torch.tensor(np.log(LISA_Noise(np.exp(np.linspace(lf0, lf1, ng)), dur=1)), device="cuda")
+
+        def inv_psd(n, dt):
+            f = torch.fft.rfftfreq(n, dt, dtype=torch.float64, device="cuda")[1:]
+            x = (torch.log(f) - lf0) / (lf1 - lf0) * (ng - 1)
+            k = x.floor().clamp(0, ng - 2).long()
+            fr = x - k
+            return torch.exp(-(logS[k] * (1 - fr) + logS[k + 1] * fr))
+
         o2 = w2.offsets
-        mm2, rel2 = [], []
+        mm2, rel2, psd2 = [], [], []
         for s_ in range(len(src2)):
             if w2.status[s_] != 0:
                 continue
@@ -706,13 +850,25 @@ def run_gpu(args, rank, world, local_rank):
             mm2.append(1.0 - ab / math.sqrt(aa * bb) if aa > 0 and bb > 0 else 0.0)
             rel2.append(float(torch.maximum((x1 - y1).abs().max(), (x2 - y2).abs().max()) /
                               torch.maximum(x1.abs().max(), x2.abs().max())))
+            w = inv_psd(len(x1), DT)
+            paa = pbb = pab = 0.0
+            for u, v in ((x1, y1), (x2, y2)):
+                U, V = torch.fft.rfft(u)[1:], torch.fft.rfft(v)[1:]
+                pab += float((w * (U * V.conj()).real).sum())
+                paa += float((w * U.abs() ** 2).sum())
+                pbb += float((w * V.abs() ** 2).sum())
+            psd2.append(1.0 - pab / math.sqrt(paa * pbb) if paa > 0 and pbb > 0 else 0.0)
         cfg2 = {"workload": "config2: e0~U(0.05,0.7), n_max=min(100,ceil(10/(1-e0)^1.5)), otherwise config1",
                 "sources": len(src2), "ok_sources": int(np.sum(w2.status == 0)), "samples": int(N2),
                 "nmodes_min_max": [int(min(nm2)), int(max(nm2))], "split_samples_per_s": N2 / (ms2 * 1e-3),
                 "max_mismatch": float(max(mm2)), "median_mismatch": float(np.median(mm2)),
-                "max_rel_dh": float(max(rel2)), "median_rel_dh": float(np.median(rel2)), "bar": 1e-6}
-        del a64, a32
+                "max_mismatch_psd": float(max(psd2)), "median_mismatch_psd": float(np.median(psd2)),
+                "psd": "LISA_Noise(dur=1), f > 0, interpolated from a 2e5-point log grid",
+                "max_rel_dh": float(max(rel2)), "median_rel_dh": float(np.median(rel2)), "bar": 1e-6,
+                "reference": "the FP64 path of the same batch (each source is pinned to the FP64 oracle in the tests)"}
+        del a64, a32, logS
         w2.close()
+        torch.cuda.empty_cache()
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
@@ -748,14 +904,17 @@ def run_gpu(args, rank, world, local_rank):
 
     # ---- roofline of the dominant kernel (split harmonic sum: FP32 mode sums, FP64 phases)
     wave_ms = kern_s[2]
-    achieved = flops_per_sample * N / (wave_ms * 1e-3) / 1e12
+    achieved = fps * N / (wave_ms * 1e-3) / 1e12
     roofline = {"kernel": "k_waveform<split>", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak > 0 else None,
                 "traffic": TRAFFIC_BYTES_PER_SAMPLE * N,
                 "traffic_source": "dram read+write per sample of one ncu capture of the same kernel on 16 sources "
                                   "of this draw (28,332,971 samples), scaled to this launch",
                 "peak_source": "measured FP32 FMA rate on this GPU (aak_probe_fp32_tflops)",
-                "flops_per_sample": flops_per_sample, "kernel_ms": wave_ms}
+                "flops_per_sample": fps, "flop_convention": "multiplies and adds one flop each (an FMA two), as the "
+                "FMA-rate probe; per sample 60 + 54 n: 24 FMA-equivalents (48 flops) of the reference's per-harmonic "
+                "algebra and 3 Bessel recurrence steps of 2 flops per harmonic; SFU work not counted",
+                "kernel_ms": wave_ms}
     out = {
         "metric": "AAK samples/s & likelihoods/s on 1 B200 at mismatch<=1e-6 vs plain FP64 path",
         "value": value,
@@ -769,11 +928,9 @@ def run_gpu(args, rank, world, local_rank):
         "vs_baseline": None,
         "dtype": "f64+f32 (FP64 phases and reductions, FP32 harmonic sums)",
         "data": "synthetic (seeded configuration-1 draw)",
-        "config": {"workload": f"config1: {len(sources)} AAK sources/GPU, T~U(0.1,1) yr, dt=10 s, n=1..30, LISA, "
-                               "split precision checked against the FP64 path of the same batch",
-                   "nsrc_per_gpu": len(sources), "samples_per_gpu": int(N), "nmodes": NMODES, "seed": SEED,
-                   "l2": "outputs 16 B/sample x samples_per_gpu exceed the 126 MB L2",
-                   "parallelism": f"sources sharded, {world} rank(s)", "launch": "one CUDA graph replay per step"},
+        "config": bench_config(len(sources), world),
+        "samples_per_gpu": int(N),
+        "launch": "one CUDA graph replay per step: the spline solve, two clears and the split waveform kernel",
         "accuracy_vs_fp64": accuracy,
         "config2_split_vs_fp64": cfg2,
         "kernel_ms": split["kernel_ms"],
@@ -794,8 +951,109 @@ def run_gpu(args, rank, world, local_rank):
         del hI, hII, hIh, hIIh
         wb.close()
         torch.cuda.empty_cache()
-        out["likelihood"] = run_likelihood(args.likelihood, local_rank, model, args.fisher)
+        out["likelihood"] = run_likelihood(args.likelihood, local_rank, model, args.fisher,
+                                           with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline,
+                                           rank=rank, world=world)
     return out
+
+
+# ----------------------------------------------------------------------------- profiling workloads
+# Small cases of the same kernels for ncu captures (one GPU):
+#   python bench.py --profile waveform   # 16 of the 512 sources, FP64 and split, twice each
+#   python bench.py --profile phase      # the phase product of the same 16 sources, twice
+#   python bench.py --profile fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
+#   python bench.py --profile tdi        # frequency-domain TDI of the waveform workload's 16 sources, twice
+#   python bench.py --profile mlp        # warm-start network: forward on 2^20 points, a training step
+def profile_waveform():
+    import torch
+
+    from emri_kludge_suite_b200.aak import WaveBatch
+
+    src, _ = config1(SEED, 512)
+    wb = WaveBatch(0)
+    wb.plan(src[::32][:16], nmodes=NMODES)
+    wb.upload()
+    n = wb.total_samples
+    hI = torch.empty(n, dtype=torch.float64, device="cuda")
+    hII = torch.empty_like(hI)
+    for precision in (0, 1):
+        for _ in range(2):
+            wb.run(hI.data_ptr(), hII.data_ptr(), precision=precision)
+    torch.cuda.synchronize()
+    print("waveform workload:", n, "samples")
+
+
+def profile_phase():
+    """The phase product of the same 16 sources as the waveform workload, twice
+    (64 B/sample of outputs: 1.8 GB, above the 126 MB L2)."""
+    import torch
+
+    from emri_kludge_suite_b200.aak import WaveBatch
+
+    src, _ = config1(SEED, 512)
+    wb = WaveBatch(0)
+    wb.plan(src[::32][:16], nmodes=NMODES)
+    wb.upload()
+    n = wb.total_samples
+    out = torch.empty(8 * n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        wb.run_phase(out.data_ptr(), n)
+    torch.cuda.synchronize()
+    assert wb.device_status() == 0
+    print("phase workload:", n, "samples")
+
+
+def profile_fisher():
+    """Two Fisher-matrix calls at the configuration-4 fiducial point: 28
+    templates of 3.2e6 samples (1.43 GB of spectra, above the 126 MB L2)."""
+    from emri_kludge_suite_b200.gpuAAK import GPUAAK
+
+    length, dt = 3_200_000, 10.0
+    x0 = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])
+    g = GPUAAK(1.0, 100, length, 100.0, dt, True, False)
+    X = np.tile(x0, (28, 1))
+    for i in range(14):
+        X[2 * i, i] += 1e-6 * max(abs(x0[i]), 1.0)
+        X[2 * i + 1, i] -= 1e-6 * max(abs(x0[i]), 1.0)
+    for _ in range(2):
+        G, st = g.fisher_gram(X, 1.0, return_status=True)
+        assert np.all(st == 0) and np.all(np.isfinite(G))
+    print("fisher workload: 28 x", length, "samples")
+
+
+def profile_tdi():
+    """The frequency-domain TDI of the same 16 sources as the waveform workload, twice."""
+    from emri_kludge_suite_b200.aak import WaveBatch
+
+    src, _ = config1(SEED, 512)
+    wb = WaveBatch(0)
+    for _ in range(2):
+        rows, offs, st = wb.tdi_host(src[::32][:16])
+    assert np.all(st == 0) and np.all(np.isfinite(rows))
+    print("tdi workload:", int(offs[-1]), "bins")
+
+
+def profile_mlp():
+    import torch
+
+    from emri_kludge_suite_b200 import parmap_mlp as P
+
+    d = P.make_dataset(1 << 16, 5)
+    m = P.ParMapMLP(0, seed=1)
+    m.fit_norm(d["x"][d["valid"]], d["y"][d["valid"]])
+    n = 1 << 20
+    x = torch.tensor(np.tile(d["x"], (16, 1)).astype(np.float32), device="cuda")
+    y = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    yt = torch.tensor(np.tile(np.nan_to_num(d["y"]), (16, 1)).astype(np.float32), device="cuda")
+    for _ in range(2):
+        m.forward_device(x.data_ptr(), y.data_ptr(), n)
+        m.train_step_device(x.data_ptr(), yt.data_ptr(), 16384, 1e-3)
+    torch.cuda.synchronize()
+    print("mlp workload done")
+
+
+PROFILES = {"waveform": profile_waveform, "phase": profile_phase, "fisher": profile_fisher,
+            "tdi": profile_tdi, "mlp": profile_mlp}
 
 
 def main():
@@ -808,8 +1066,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--likelihood", type=int, default=1024, help="config-4 templates to time (0: skip)")
-    ap.add_argument("--config2-sources", type=int, default=128,
+    ap.add_argument("--likelihood", type=int, default=4096, help="config-4 templates to time (0: skip)")
+    ap.add_argument("--config2-sources", type=int, default=512,
                     help="sources of the configuration-2 accuracy check (0: skip)")
     ap.add_argument("--plain-sources", type=int, default=16,
                     help="sources of the plain FP64 per-source baseline (0: skip)")
@@ -818,7 +1076,12 @@ def main():
     ap.add_argument("--phases", type=int, default=1, help="time the AAK phase product of the batch (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,
                     help="config-3 training points of the warm-start network (0: skip)")
+    ap.add_argument("--profile", default=None, choices=sorted(PROFILES),
+                    help="run one small profiling workload instead of the benchmark")
     args = ap.parse_args()
+    if args.profile:
+        PROFILES[args.profile]()
+        return 0
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -831,9 +1094,10 @@ def main():
         samples_per_step = []
         t_all = time.perf_counter()
         res = None
-        for _ in range(args.warmup + args.steps):
+        for k in range(args.warmup + args.steps):
             res = cpu_reference(sources, budget_s=args.cpu_budget / max(1, args.steps))
             samples_per_step.append(res["value"])
+        full = cpu_reference(sources, budget_s=1.0, untruncated=True).get("untruncated")
         vals = samples_per_step[args.warmup:] or samples_per_step
         v = float(np.mean(vals))
         line = {"metric": "AAK samples/s & likelihoods/s on 1 B200 at mismatch<=1e-6 vs plain FP64 path", "value": v,
@@ -841,10 +1105,10 @@ def main():
                 "ms_per_step": (time.perf_counter() - t_all) * 1e3 / (args.warmup + args.steps),
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded configuration-1 draw)", "impl": "reference",
-                "config": {"workload": f"config1: {len(sources)} AAK sources, T~U(0.1,1) yr, dt=10 s, n=1..30, LISA, FP64",
-                           "nsrc": len(sources), "nmodes": NMODES, "seed": SEED},
+                "config": bench_config(len(sources), world),
                 "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
-                "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                "e2e": {"value": v, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "untruncated_check": full}
         print(json.dumps(line), flush=True)
         return 0
 
@@ -860,14 +1124,16 @@ def main():
         # before any CUDA call: the pool is spawned from a process without a CUDA context
         try:
             sources, _ = config1(SEED, args.nsrc)
-            cpu = cpu_reference(sources, budget_s=args.cpu_budget)
+            cpu = cpu_reference(sources, budget_s=args.cpu_budget, untruncated=True)
         except Exception as ex:  # reported, never fatal for the GPU arm
             cpu = {"value": None, "unit": "samples/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {ex}"}
     out = run_gpu(args, rank, world, local_rank)
     if rank == 0:
         if cpu is not None:
-            out["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            out["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample") if k in cpu}
+            if cpu.get("untruncated"):
+                out["cpu_baseline"]["untruncated_check"] = cpu["untruncated"]
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist

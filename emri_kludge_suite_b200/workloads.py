@@ -8,18 +8,11 @@
   dt = 10 s, and p0 set so that the plunge falls after T (leading-order
   time to plunge from p_end = 10 + 3 e0, clipped to [9, 80]).
 
-Profiling workloads (run from the repository root on one GPU)::
-
-    python -m emri_kludge_suite_b200.workloads waveform   # 16 of the 512 sources, FP64 and split, twice each
-    python -m emri_kludge_suite_b200.workloads phase      # the phase product of the same 16 sources, twice
-    python -m emri_kludge_suite_b200.workloads fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
-    python -m emri_kludge_suite_b200.workloads tdi        # frequency-domain TDI of the waveform workload's 16 sources, twice
-    python -m emri_kludge_suite_b200.workloads mlp        # warm-start network: forward on 2^20 points, a training step
+The small profiling workloads that use these draws are ``bench.py --profile``.
 """
 from __future__ import annotations
 
 import math
-import sys
 
 import numpy as np
 
@@ -67,96 +60,3 @@ def config2(seed: int, nsrc: int = 512):
     rng = np.random.default_rng(seed)
     src = [draw_source(rng, e_max=0.7) for _ in range(nsrc)]
     return src, [min(100, math.ceil(10.0 / (1.0 - p["e"]) ** 1.5)) for p in src]
-
-
-def profile_waveform():
-    import torch
-
-    from .aak import WaveBatch
-
-    src, _ = config1(SEED, 512)
-    wb = WaveBatch(0)
-    wb.plan(src[::32][:16], nmodes=NMODES)
-    wb.upload()
-    n = wb.total_samples
-    hI = torch.empty(n, dtype=torch.float64, device="cuda")
-    hII = torch.empty_like(hI)
-    for precision in (0, 1):
-        for _ in range(2):
-            wb.run(hI.data_ptr(), hII.data_ptr(), precision=precision)
-    torch.cuda.synchronize()
-    print("waveform workload:", n, "samples")
-
-
-def profile_phase():
-    """The phase product of the same 16 sources as the waveform workload, twice
-    (64 B/sample of outputs: 1.8 GB, above the 126 MB L2)."""
-    import torch
-
-    from .aak import WaveBatch
-
-    src, _ = config1(SEED, 512)
-    wb = WaveBatch(0)
-    wb.plan(src[::32][:16], nmodes=NMODES)
-    wb.upload()
-    n = wb.total_samples
-    out = torch.empty(8 * n, dtype=torch.float64, device="cuda")
-    for _ in range(2):
-        wb.run_phase(out.data_ptr(), n)
-    torch.cuda.synchronize()
-    assert wb.device_status() == 0
-    print("phase workload:", n, "samples")
-
-
-def profile_fisher():
-    """Two Fisher-matrix calls at the configuration-4 fiducial point: 28
-    templates of 3.2e6 samples (1.43 GB of spectra, above the 126 MB L2)."""
-    from .gpuAAK import GPUAAK
-
-    length, dt = 3_200_000, 10.0
-    x0 = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])
-    g = GPUAAK(1.0, 100, length, 100.0, dt, True, False)
-    X = np.tile(x0, (28, 1))
-    for i in range(14):
-        X[2 * i, i] += 1e-6 * max(abs(x0[i]), 1.0)
-        X[2 * i + 1, i] -= 1e-6 * max(abs(x0[i]), 1.0)
-    for _ in range(2):
-        G, st = g.fisher_gram(X, 1.0, return_status=True)
-        assert np.all(st == 0) and np.all(np.isfinite(G))
-    print("fisher workload: 28 x", length, "samples")
-
-
-def profile_tdi():
-    """The frequency-domain TDI of the same 16 sources as the waveform workload, twice."""
-    from .aak import WaveBatch
-
-    src, _ = config1(SEED, 512)
-    wb = WaveBatch(0)
-    for _ in range(2):
-        rows, offs, st = wb.tdi_host(src[::32][:16])
-    assert np.all(st == 0) and np.all(np.isfinite(rows))
-    print("tdi workload:", int(offs[-1]), "bins")
-
-
-def profile_mlp():
-    import torch
-
-    from . import parmap_mlp as P
-
-    d = P.make_dataset(1 << 16, 5)
-    m = P.ParMapMLP(0, seed=1)
-    m.fit_norm(d["x"][d["valid"]], d["y"][d["valid"]])
-    n = 1 << 20
-    x = torch.tensor(np.tile(d["x"], (16, 1)).astype(np.float32), device="cuda")
-    y = torch.empty((n, 3), dtype=torch.float32, device="cuda")
-    yt = torch.tensor(np.tile(np.nan_to_num(d["y"]), (16, 1)).astype(np.float32), device="cuda")
-    for _ in range(2):
-        m.forward_device(x.data_ptr(), y.data_ptr(), n)
-        m.train_step_device(x.data_ptr(), yt.data_ptr(), 16384, 1e-3)
-    torch.cuda.synchronize()
-    print("mlp workload done")
-
-
-if __name__ == "__main__":
-    {"waveform": profile_waveform, "phase": profile_phase, "fisher": profile_fisher,
-     "tdi": profile_tdi, "mlp": profile_mlp}[sys.argv[1] if len(sys.argv) > 1 else "waveform"]()
