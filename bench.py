@@ -370,7 +370,7 @@ def run_fisher(g, n_points: int) -> dict:
                               "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
                               "bytes": gram_bytes, "peak_source": "measured copy bandwidth (MEASURED_PEAKS.json)"
                               if peaks.get("hbm_gbs") else "fallback"},
-            "gpu_launches_per_matrix": 4,  # k_spline_coeffs, k_waveform, k_fisher_partial, k_fisher_final (+ cuFFT)
+            "gpu_launches_per_matrix": 6,  # spline solve, tile pre-pass (2), k_waveform, Fisher Gram (2) (+ cuFFT)
             "cpu_baseline": ref_fisher_seconds()}
 
 
@@ -471,6 +471,35 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
     fast["max_abs_logL"] = float(np.max(np.abs(logl64[ok]))) if ok.any() else None
     fast["warm_start"] = model is not None
     res["split_warm"] = fast
+    # split templates with the FP32 transform and compensated FP32 inner products
+    g.set_precision(2)
+    g.set_warm_start(model)
+    out32, st32, f32 = timed()
+    g.set_precision(0)
+    g.set_warm_start(None)
+    ok32 = (st64 == 0) & (st32 == 0)
+    logl32 = -0.5 * (d_d + out32[:, 1] - 2.0 * out32[:, 0])
+    f32["max_abs_dlogL_vs_fp64"] = float(np.max(np.abs(logl32 - logl64)[ok32])) if ok32.any() else None
+    f32["median_abs_dlogL_vs_fp64"] = float(np.median(np.abs(logl32 - logl64)[ok32])) if ok32.any() else None
+    res["split_fp32_fft"] = f32
+    # HBM roofline of the inner-product kernel: template spectra of both
+    # channels, the data of both channels and one weight array per bin
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    nb = LIKE_LENGTH // 2 + 1
+    for key, run_, per_bin in (("fp64_plain", plain, 2 * (16 + 16) + 8), ("split_fp32_fft", f32, 2 * (8 + 8) + 4)):
+        ms_red = run_["ms"]["reduce"]
+        gbs = per_bin * nb * n_templates / (ms_red * 1e-3) / 1e9 if ms_red > 0 else None
+        res[key]["reduce_roofline"] = {
+            "kernel": "k_inner_partial" + ("_f32" if per_bin < 60 else "") + " + k_inner_final", "bound": "hbm",
+            "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if gbs else None,
+            "bytes_per_template": per_bin * nb,
+            "bytes_formula": "2 channels x nbins x (template + data complex) + nbins x weight",
+            "peak_source": "measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback"}
     if with_cpu:
         res["cpu_baseline"] = cpu_likelihood_reference()
     return res
@@ -688,6 +717,16 @@ def run_gpu(args, rank, world, local_rank):
     else:
         N_all = float(N)
 
+    # ---- autotuner: every launch shape of the waveform stage timed on this
+    #      batch, the fastest kept per precision (no cache file: all timed)
+    tune = {}
+    for prec, name in ((0, "fp64"), (1, "split")):
+        v, ms_v = wb.autotune(hI.data_ptr(), hII.data_ptr(), precision=prec)
+        tune[name] = {"choice": v, "ms_per_variant": ms_v}
+    tune["variants"] = ["pre-pass, joint 2 (split) / 1 (FP64), 2 CTAs/SM", "tables inside the tiles, 2 CTAs/SM",
+                        "pre-pass, joint 1 / 2, 2 CTAs/SM", "pre-pass, joint 4, 2 CTAs/SM",
+                        "pre-pass, joint 2 / 1, 3 CTAs/SM", "pre-pass, joint 1 / 2, 3 CTAs/SM"]
+
     # ---- plain FP64 batched path (precision 0): per-kernel times
     for _ in range(args.warmup):
         wb.run(hI.data_ptr(), hII.data_ptr(), stream=sptr)
@@ -740,7 +779,9 @@ def run_gpu(args, rank, world, local_rank):
         dist.barrier()
     clk = clocks.stop()
     ms = reduce_max(ev0.elapsed_time(ev1))
-    launches = 2 * args.steps  # k_spline_coeffs and k_waveform<split>; the clears are memset nodes
+    # k_spline_coeffs, the tile pre-pass (two kernels, when the tuned shape uses
+    # it) and k_waveform<split> per replay; the clears are memset nodes
+    launches = wb.launches() * args.steps
     value = N_all * args.steps / (ms * 1e-3)
     # accuracy of every source against the FP64 outputs of the same batch
     worst_mm, worst_rel, mms = 0.0, 0.0, []
@@ -759,15 +800,16 @@ def run_gpu(args, rank, world, local_rank):
     accuracy = {"max_mismatch": worst_mm, "median_mismatch": float(np.median(mms)), "max_rel_dh": worst_rel,
                 "sources": len(sources), "bar": 1e-6}
     fps = flops_per_sample(NMODES)
-    ach64 = fps * N / (kern[2] * 1e-3) / 1e12
+    ach64 = fps * N / ((kern[1] + kern[2]) * 1e-3) / 1e12
     fp64 = {"value": value64, "unit": "samples/s", "ms_per_step": ms64 / args.steps,
-            "kernel_ms": {"clears": kern[0], "waveform_fp64": kern[2]},
-            "roofline": {"kernel": "k_waveform<fp64>", "bound": "fp64", "achieved": ach64, "peak": fp64_peak,
+            "kernel_ms": {"clears": kern[0], "tile_prepass": kern[1], "waveform_fp64": kern[2]},
+            "roofline": {"kernel": "k_tile_params + k_tile_table + k_waveform<fp64>", "bound": "fp64",
+                         "achieved": ach64, "peak": fp64_peak,
                          "unit": "TFLOP/s", "frac": ach64 / fp64_peak if fp64_peak > 0 else None,
                          "peak_source": "measured FP64 FMA rate on this GPU (aak_probe_fp64_tflops)"},
             "split_speedup": ms64 / ms}
     del hI2, hII2
-    split = {"value": value, "kernel_ms": {"clears": kern_s[0], "waveform_split": kern_s[2]}}
+    split = {"value": value, "kernel_ms": {"clears": kern_s[0], "tile_prepass": kern_s[1], "waveform_split": kern_s[2]}}
 
     # ---- frequency-domain TDI of a subset of the batch
     tdi = run_tdi(sources, local_rank, nthreads) if args.tdi and rank == 0 else None
@@ -903,9 +945,10 @@ def run_gpu(args, rank, world, local_rank):
            "d2h_bytes_per_step": int(16 * N), "seconds_per_step": e2e_s, "host_threads": nthreads}
 
     # ---- roofline of the dominant kernel (split harmonic sum: FP32 mode sums, FP64 phases)
-    wave_ms = kern_s[2]
+    wave_ms = kern_s[1] + kern_s[2]  # the harmonic sums' Bessel tables are built in the pre-pass
     achieved = fps * N / (wave_ms * 1e-3) / 1e12
-    roofline = {"kernel": "k_waveform<split>", "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+    roofline = {"kernel": "k_waveform<split> (with its tile pre-pass k_tile_params + k_tile_table)", "bound": "fp32",
+                "achieved": achieved, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak > 0 else None,
                 "traffic": TRAFFIC_BYTES_PER_SAMPLE * N,
                 "traffic_source": "dram read+write per sample of one ncu capture of the same kernel on 16 sources "
@@ -931,6 +974,7 @@ def run_gpu(args, rank, world, local_rank):
         "config": bench_config(len(sources), world),
         "samples_per_gpu": int(N),
         "launch": "one CUDA graph replay per step: the spline solve, two clears and the split waveform kernel",
+        "autotune": tune,
         "accuracy_vs_fp64": accuracy,
         "config2_split_vs_fp64": cfg2,
         "kernel_ms": split["kernel_ms"],
@@ -951,9 +995,19 @@ def run_gpu(args, rank, world, local_rank):
         del hI, hII, hIh, hIIh
         wb.close()
         torch.cuda.empty_cache()
-        out["likelihood"] = run_likelihood(args.likelihood, local_rank, model, args.fisher,
-                                           with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline,
-                                           rank=rank, world=world)
+        free_b, total_b = torch.cuda.mem_get_info()
+        try:
+            out["likelihood"] = run_likelihood(args.likelihood, local_rank, model, args.fisher,
+                                               with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline,
+                                               rank=rank, world=world)
+        except Exception as ex:  # one rank alone: report the failure, keep the waveform line
+            if world > 1:
+                raise
+            from emri_kludge_suite_b200 import _lib
+
+            out["likelihood"] = {"error": f"{type(ex).__name__}: {ex}",
+                                 "detail": (_lib.lib().aak_last_error_detail() or b"").decode(errors="replace")}
+        out["likelihood"]["device_free_gb_before"] = free_b / 1e9
     return out
 
 
@@ -964,6 +1018,7 @@ def run_gpu(args, rank, world, local_rank):
 #   python bench.py --profile fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
 #   python bench.py --profile tdi        # frequency-domain TDI of the waveform workload's 16 sources, twice
 #   python bench.py --profile mlp        # warm-start network: forward on 2^20 points, a training step
+#   python bench.py --profile likelihood # 32 config-4 templates, FP64 and FP32 transform + products
 def profile_waveform():
     import torch
 
@@ -1052,8 +1107,27 @@ def profile_mlp():
     print("mlp workload done")
 
 
+def profile_likelihood():
+    """32 configuration-4 templates (3.2e6 samples each) through the batched
+    likelihood, FP64 then FP32 transform + compensated FP32 products (one batch
+    of 32 each; 0.8 GB of FP64 spectra, above the 126 MB L2)."""
+    from emri_kludge_suite_b200.gpuAAK import GPUAAK
+
+    g = GPUAAK(1.0, 100, LIKE_LENGTH, 100.0, DT, True, False)
+    nb = LIKE_LENGTH // 2 + 1
+    rng = np.random.default_rng(3)
+    d = rng.standard_normal(nb) + 1j * rng.standard_normal(nb)
+    g.input_data(d, d, np.ones(nb), np.ones(nb))
+    X = config4_templates(32)
+    for prec in (0, 2):
+        g.set_precision(prec)
+        out, st = g.likelihood_batch(X, max_batch=32, return_status=True)
+        assert np.all(st == 0) and np.all(np.isfinite(out))
+    print("likelihood workload: 32 x", LIKE_LENGTH, "samples, FP64 and FP32 transforms")
+
+
 PROFILES = {"waveform": profile_waveform, "phase": profile_phase, "fisher": profile_fisher,
-            "tdi": profile_tdi, "mlp": profile_mlp}
+            "tdi": profile_tdi, "mlp": profile_mlp, "likelihood": profile_likelihood}
 
 
 def main():

@@ -144,6 +144,8 @@ def lib():
     L.aak_batch_run_graph.argtypes = [_vp, _vp, _vp, _i32, _vp]
     L.aak_ctx_set_precision.argtypes = [_vp, _i32]
     L.aak_ctx_set_lookback_bound.argtypes = [_vp, _i64]
+    L.aak_ctx_autotune.argtypes = [_vp, _vp, _vp, _i32, ctypes.c_char_p, _i32p, ctypes.POINTER(ctypes.c_float)]
+    L.aak_ctx_set_variant.argtypes = [_vp, _i32, _i32]
     L.aak_wave_batch_host.argtypes = [_vp, ctypes.POINTER(AAKParams), _i32, _i32p, _i32, _dp, _dp, _i64p, _i32p]
     # learned ParMap warm start
     _fp = ctypes.POINTER(ctypes.c_float)

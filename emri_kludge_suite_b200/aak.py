@@ -284,6 +284,22 @@ class WaveBatch:
         check(lib().aak_batch_run_graph(self._ctx, ctypes.c_void_p(hI_ptr), ctypes.c_void_p(hII_ptr), int(precision),
                                         ctypes.c_void_p(stream)), "aak_batch_run_graph")
 
+    def autotune(self, hI_ptr: int, hII_ptr: int, precision: int = 1, cache_path: str | None = None):
+        """Time every launch shape of the waveform stage on the uploaded batch
+        (outputs into the given device buffers) and keep the fastest for
+        ``precision``; with ``cache_path``, reuse or append a tuning-cache
+        entry.  Returns (variant, ms per variant; -1 where not timed)."""
+        v = ctypes.c_int32()
+        ms = (ctypes.c_float * 6)()
+        path = cache_path.encode() if cache_path else None
+        check(lib().aak_ctx_autotune(self._ctx, ctypes.c_void_p(hI_ptr), ctypes.c_void_p(hII_ptr), int(precision), path,
+                                     ctypes.byref(v), ms), "aak_ctx_autotune")
+        return int(v.value), [float(x) for x in ms]
+
+    def set_variant(self, precision: int, variant: int):
+        """Launch shape of the waveform stage for ``precision`` (0: default)."""
+        check(lib().aak_ctx_set_variant(self._ctx, int(precision), int(variant)), "aak_ctx_set_variant")
+
     def set_precision(self, precision: int):
         """Precision of :meth:`generate_host` (0: FP64, 1: split)."""
         check(lib().aak_ctx_set_precision(self._ctx, int(precision)), "aak_ctx_set_precision")

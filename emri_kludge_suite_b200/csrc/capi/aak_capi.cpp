@@ -10,8 +10,11 @@
 #include <thread>
 #include <atomic>
 #include <chrono>
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
+#include <string>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -121,6 +124,8 @@ struct aak_ctx {
   double *g_hI = nullptr, *g_hII = nullptr;
   int g_prec = -1;
   uint64_t g_gen = ~0ull;
+  int g_variant = -1;
+  int variant[2] = {0, 0};  // launch shape of the waveform stage per precision (autotuner; 0: default)
   int64_t newton_points = 0, newton_iters = 0, newton_fallbacks = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::mutex mu;
@@ -583,7 +588,9 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   if ((r = ctx->d_src.reserve(n)) || (r = ctx->d_tile_start.reserve(n + 1)) ||
       (r = ctx->d_tile_knot.reserve(ctx->tile_knot.size())) || (r = ctx->d_tile_pairs.reserve(ctx->tile_pairs.size())) ||
       (r = ctx->d_queue.reserve(ctx->queue.size())) || (r = ctx->d_spl_blk.reserve(ctx->spl_blk.size())) ||
-      (r = ctx->d_knot_t.reserve(std::max<int64_t>(ctx->total_knots, 1))) ||
+      // knot times: two entries of slack past the last knot (a window's bulk
+      // copy starts on a 16-byte boundary and may read one element beyond it)
+      (r = ctx->d_knot_t.reserve(std::max<int64_t>(ctx->total_knots, 1) + 2)) ||
       (r = ctx->d_knot_y.reserve(std::max<int64_t>(ctx->total_knots, 1))) ||
       (r = ctx->d_knot_c.reserve(std::max<int64_t>(ctx->total_knots, 1))) || (r = ctx->d_bessel.reserve(ctx->bessel.size())) ||
       (r = ctx->d_link.reserve(std::max<int64_t>(ctx->total_tiles, 1))) ||
@@ -654,11 +661,27 @@ int run(aak_ctx *ctx, double *hI, double *hII, double *t, double *traj, int64_t 
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
   BatchView bv = batch_view(ctx, hI, hII, t, traj, traj_stride);
+  bv.variant = ctx->variant[precision];
   if (!traj && (r = tile_tables(ctx, precision, bv)) != AAK_OK) return r;
   if (ctx->profile && !ctx->ev[0])
     for (auto &e : ctx->ev) cudaEventCreate(&e);
   launch_dense(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr, precision);
-  ctx->last_launches = bv.tile_prep ? 3 : 1;
+  ctx->last_launches = (bv.tile_prep && wave_variant(precision == 1, bv.variant).pre) ? 3 : 1;
+  return cuda_ok(cudaGetLastError());
+}
+
+// The waveform kernel into FP32 rows (hI32, hII32 indexed as the FP64 outputs).
+int run_rows32(aak_ctx *ctx, float *hI32, float *hII32, int precision, cudaStream_t st) {
+  if (!ctx->uploaded || !hI32 || !hII32 || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  BatchView bv = batch_view(ctx, nullptr, nullptr, nullptr, nullptr, 0);
+  bv.hI_f32 = hI32;
+  bv.hII_f32 = hII32;
+  bv.variant = ctx->variant[precision];
+  if ((r = tile_tables(ctx, precision, bv)) != AAK_OK) return r;
+  launch_dense(bv, ctx->num_sms, st, nullptr, precision);
+  ctx->last_launches = 3;
   return cuda_ok(cudaGetLastError());
 }
 
@@ -675,13 +698,15 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
   if (!ctx->uploaded || !hI || !hII || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
-  if (ctx->gexec && (ctx->g_hI != hI || ctx->g_hII != hII || ctx->g_prec != precision || ctx->g_gen != ctx->upload_gen))
+  if (ctx->gexec && (ctx->g_hI != hI || ctx->g_hII != hII || ctx->g_prec != precision || ctx->g_gen != ctx->upload_gen ||
+                     ctx->g_variant != ctx->variant[precision]))
     drop_graph(ctx);
   if (!ctx->gexec) {
     if (!ctx->cap_stream && (r = cuda_ok(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking))) != AAK_OK)
       return r;
     prepare_dense_launch();
     BatchView bv = batch_view(ctx, hI, hII, nullptr, nullptr, 0);
+    bv.variant = ctx->variant[precision];
     if ((r = tile_tables(ctx, precision, bv)) != AAK_OK) return r;
     if ((r = cuda_ok(cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeThreadLocal))) != AAK_OK) return r;
     // the whole dense stage: natural-spline solve of every source's knots
@@ -706,8 +731,10 @@ int run_graph(aak_ctx *ctx, double *hI, double *hII, int precision, cudaStream_t
     ctx->g_hII = hII;
     ctx->g_prec = precision;
     ctx->g_gen = ctx->upload_gen;
+    ctx->g_variant = ctx->variant[precision];
   }
-  ctx->last_launches = 4;  // spline solve, tile parameters, tile tables, waveform kernel
+  // spline solve, tile parameters and tables (with the pre-pass), waveform kernel
+  ctx->last_launches = wave_variant(precision == 1, ctx->variant[precision]).pre ? 4 : 2;
   return cuda_ok(cudaGraphLaunch(ctx->gexec, st));
 }
 
@@ -1091,6 +1118,8 @@ int wave_batch_streamed(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const i
         return r;
     }
     ctx->aux[k]->precision = ctx->precision;
+    ctx->aux[k]->variant[0] = ctx->variant[0];
+    ctx->aux[k]->variant[1] = ctx->variant[1];
   }
   std::vector<int64_t> pre(nsrc + 1, 0);  // sample offsets of the sources in the host outputs
   for (int s = 0; s < nsrc; ++s) pre[s + 1] = pre[s] + Pv[s].length;
@@ -1277,6 +1306,8 @@ void aak_ctx_destroy(aak_ctx *c) {
     c->d_link.release();
     c->d_flag.release();
     c->d_counter.release();
+    c->d_tile_prep.release();
+    c->d_tile_tab.release();
     c->d_out.release();
     c->d_tdi.release();
     c->d_tdi_work.release();
@@ -1487,6 +1518,125 @@ int aak_ctx_set_precision(aak_ctx *ctx, int32_t precision) {
   return AAK_OK;
 }
 
+// ---------------------------------------------------------------- autotuner
+// The launch shape of the waveform stage (wave_variant: tile pre-pass or
+// tables inside the tiles, samples per thread in the harmonic loop, resident
+// CTAs per SM) is chosen per (device, precision, largest harmonic count,
+// sources and median length in powers of two) by timing every candidate on
+// the uploaded batch; the choice and the timings are appended to a tuning
+// cache file, and a later call with the same key reads the choice from there.
+static_assert(AAK_NUM_VARIANTS == kNumVariants, "the header states the number of launch shapes");
+
+namespace {
+
+std::string tune_key(aak_ctx *ctx, int precision) {
+  cudaDeviceProp prop;
+  std::memset(&prop, 0, sizeof(prop));
+  cudaGetDeviceProperties(&prop, ctx->device);
+  std::string name(prop.name);
+  for (auto &c : name)
+    if (c == ' ' || c == '|') c = '_';
+  std::vector<int32_t> len;
+  for (const auto &d : ctx->descs) len.push_back(d.vlength);
+  std::sort(len.begin(), len.end());
+  const int32_t med = len.empty() ? 0 : len[len.size() / 2];
+  auto lg = [](double x) { return x > 0 ? (int)std::lround(std::log2(x)) : 0; };
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%s|sm%d|p%d|nm%d|src2^%d|len2^%d", name.c_str(), prop.multiProcessorCount, precision,
+                ctx->max_nmodes, lg((double)ctx->nsrc), lg((double)med));
+  return buf;
+}
+
+int tune_lookup(const char *path, const std::string &key, int *variant) {
+  if (!path) return 0;
+  FILE *f = std::fopen(path, "r");
+  if (!f) return 0;
+  char line[1024];
+  int found = 0;
+  while (std::fgets(line, sizeof(line), f)) {
+    char k[512];
+    int v = -1;
+    if (std::sscanf(line, "%511s %d", k, &v) == 2 && key == k && v >= 0 && v < kNumVariants) {
+      *variant = v;  // the last entry for a key wins
+      found = 1;
+    }
+  }
+  std::fclose(f);
+  return found;
+}
+
+}  // namespace
+
+int aak_ctx_autotune(aak_ctx *ctx, double *d_hI, double *d_hII, int32_t precision, const char *cache_path,
+                     int32_t *variant, float *ms_per_variant) {
+  if (!ctx || !d_hI || !d_hII || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (!ctx->uploaded) return AAK_ERR_INVALID_PARAM;
+  int r;
+  if ((r = select_device(ctx->device)) != AAK_OK) return r;
+  const std::string key = tune_key(ctx, precision);
+  if (ms_per_variant)
+    for (int v = 0; v < kNumVariants; ++v) ms_per_variant[v] = -1.0f;
+  int best = 0;
+  if (tune_lookup(cache_path, key, &best)) {
+    ctx->variant[precision] = best;
+    if (variant) *variant = best;
+    return AAK_OK;
+  }
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if ((r = cuda_ok(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) != AAK_OK) return r;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float ms[kNumVariants];
+  float best_ms = 0.0f;
+  for (int v = 0; v < kNumVariants && r == AAK_OK; ++v) {
+    BatchView bv = batch_view(ctx, d_hI, d_hII, nullptr, nullptr, 0);
+    bv.variant = v;
+    if ((r = tile_tables(ctx, precision, bv)) != AAK_OK) break;
+    ms[v] = 0.0f;
+    for (int rep = 0; rep < 3 && r == AAK_OK; ++rep) {  // one warm-up, then the faster of two
+      cudaEventRecord(e0, st);
+      launch_dense(bv, ctx->num_sms, st, nullptr, precision);
+      cudaEventRecord(e1, st);
+      if ((r = cuda_ok(cudaEventSynchronize(e1))) != AAK_OK) break;
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep == 1 || (rep == 2 && t < ms[v])) ms[v] = t;
+    }
+    if (r != AAK_OK) break;
+    if (ms_per_variant) ms_per_variant[v] = ms[v];
+    if (v == 0 || ms[v] < best_ms) {
+      best = v;
+      best_ms = ms[v];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(st);
+  if (r != AAK_OK) return r;
+  if ((r = device_status(ctx)) != AAK_OK) return r;  // a timing run must not have given up a wait
+  ctx->variant[precision] = best;
+  if (variant) *variant = best;
+  if (cache_path) {
+    FILE *f = std::fopen(cache_path, "a");
+    if (f) {
+      std::fprintf(f, "%s %d", key.c_str(), best);
+      for (int v = 0; v < kNumVariants; ++v) std::fprintf(f, " %.4f", ms[v]);
+      std::fprintf(f, "\n");
+      std::fclose(f);
+    }
+  }
+  return AAK_OK;
+}
+
+int aak_ctx_set_variant(aak_ctx *ctx, int32_t precision, int32_t variant) {
+  if (!ctx || (precision != 0 && precision != 1) || variant < 0 || variant >= kNumVariants) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->variant[precision] = variant;
+  return AAK_OK;
+}
+
 int aak_ctx_set_lookback_bound(aak_ctx *ctx, int64_t cycles) {
   if (!ctx) return AAK_ERR_INVALID_PARAM;
   std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1692,6 +1842,12 @@ struct aak_gpu {
   DevBuf<double> d_fisher;  // Fisher Gram partial sums and the 2 x nd x nd result
   cufftHandle plan = 0;
   int plan_batch = 0;
+  // precision 2: FP32 template rows, an FP32 R2C transform and the FP32 copies
+  // of the data and weights (the compensated FP32 inner products)
+  DevBuf<float> d_H32[2], d_D32[2], d_w32[2];
+  cufftHandle plan32 = 0;
+  int plan32_batch = 0;
+  bool rows32 = false;   // the rows of the last generation are the FP32 ones
   int32_t count = 0;     // templates currently in the rows
   bool spectral = false; // rows hold spectra (after a likelihood)
   std::vector<double> like;
@@ -1721,6 +1877,27 @@ int gpu_capacity(aak_gpu *g, int B) {
       return AAK_ERR_CUDA;
     }
     g->plan_batch = B;
+  }
+  return AAK_OK;
+}
+
+int gpu_capacity32(aak_gpu *g, int B) {
+  int r;
+  if ((r = g->d_H32[0].reserve((size_t)B * g->row)) || (r = g->d_H32[1].reserve((size_t)B * g->row)) ||
+      (r = g->d_partial.reserve((size_t)B * kIpBlocksPerTemplate * 2)) || (r = g->d_out.reserve((size_t)B * 2)))
+    return r;
+  if (g->plan32_batch != B) {  // an exact-size plan: a larger one would transform stale rows
+    if (g->plan32) cufftDestroy(g->plan32);
+    g->plan32 = 0;
+    g->plan32_batch = 0;
+    int n = g->length;
+    int inembed = (int)g->row, onembed = (int)(g->row / 2);
+    if (cufftPlanMany(&g->plan32, 1, &n, &inembed, 1, (int)g->row, &onembed, 1, (int)(g->row / 2), CUFFT_R2C, B) !=
+        CUFFT_SUCCESS) {
+      g->plan32 = 0;
+      return AAK_ERR_CUDA;
+    }
+    g->plan32_batch = B;
   }
   return AAK_OK;
 }
@@ -1770,8 +1947,22 @@ int gpu_plan(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status) 
 
 // Device half: upload the planned batch and generate it into the rows
 // (asynchronous after the upload, on the legacy default stream).
-int gpu_launch(aak_gpu *g, int B, bool with_t) {
+int gpu_launch(aak_gpu *g, int B, bool with_t, bool rows32 = false) {
   int r;
+  if (rows32 && !with_t) {  // precision 2 (likelihood batches): split templates into FP32 rows
+    if ((r = gpu_capacity32(g, B)) != AAK_OK) return r;
+    if ((r = upload(g->ctx, g->stream)) != AAK_OK) return r;
+    if (!g->ev[0])
+      for (auto &e : g->ev) cudaEventCreate(&e);
+    cudaEventRecord(g->ev[0], g->stream);
+    if ((r = run_rows32(g->ctx, g->d_H32[0].ptr, g->d_H32[1].ptr, 1, g->stream)) != AAK_OK) return r;
+    cudaEventRecord(g->ev[1], g->stream);
+    g->count = B;
+    g->spectral = false;
+    g->rows32 = true;
+    return AAK_OK;
+  }
+  g->rows32 = false;
   if ((r = gpu_capacity(g, B)) != AAK_OK) return r;
   if ((r = upload(g->ctx, g->stream)) != AAK_OK) return r;
   double *dt = nullptr;
@@ -1783,7 +1974,9 @@ int gpu_launch(aak_gpu *g, int B, bool with_t) {
   if (!g->ev[0])
     for (auto &e : g->ev) cudaEventCreate(&e);
   cudaEventRecord(g->ev[0], g->stream);
-  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, g->precision, g->stream)) != AAK_OK) return r;
+  if ((r = run(g->ctx, g->d_H[0].ptr, g->d_H[1].ptr, dt, nullptr, 0, g->precision == 0 ? 0 : 1, g->stream)) !=
+      AAK_OK)
+    return r;
   cudaEventRecord(g->ev[1], g->stream);
   g->count = B;
   g->spectral = false;
@@ -1797,6 +1990,16 @@ int gpu_generate(aak_gpu *g, const double *x, int B, int nthreads, int32_t *stat
 
 // In-place D2Z transforms of the rows of both channels (once per generation).
 int gpu_fft_rows(aak_gpu *g) {
+  if (!g->spectral && g->rows32) {
+    int r = gpu_capacity32(g, g->count);
+    if (r != AAK_OK) return r;
+    if (cufftSetStream(g->plan32, g->stream) != CUFFT_SUCCESS) return AAK_ERR_CUDA;
+    if (cufftExecR2C(g->plan32, g->d_H32[0].ptr, reinterpret_cast<cufftComplex *>(g->d_H32[0].ptr)) != CUFFT_SUCCESS ||
+        cufftExecR2C(g->plan32, g->d_H32[1].ptr, reinterpret_cast<cufftComplex *>(g->d_H32[1].ptr)) != CUFFT_SUCCESS)
+      return AAK_ERR_CUDA;
+    g->spectral = true;
+    return AAK_OK;
+  }
   if (!g->spectral) {
     if (g->plan_batch != g->count) {
       // a plan of a larger batch would transform stale rows: make one of this size
@@ -1824,6 +2027,22 @@ int gpu_likelihood_launch(aak_gpu *g) {
   int r0 = gpu_fft_rows(g);
   if (r0 != AAK_OK) return r0;
   cudaEventRecord(g->ev[2], g->stream);
+  if (g->rows32) {
+    InnerProductArgs32 a;
+    for (int ch = 0; ch < 2; ++ch) {
+      a.H[ch] = g->d_H32[ch].ptr;
+      a.D[ch] = g->d_D32[ch].ptr;
+      a.w[ch] = g->d_w32[ch].ptr;
+    }
+    a.row_floats = g->row;
+    a.nbins = g->nbins;
+    a.ntemplates = g->count;
+    a.partial = g->d_partial.ptr;
+    a.out = g->d_out.ptr;
+    launch_inner_products_f32(a, g->stream);
+    cudaEventRecord(g->ev[3], g->stream);
+    return cuda_ok(cudaGetLastError());
+  }
   InnerProductArgs a;
   a.H[0] = g->d_H[0].ptr;
   a.H[1] = g->d_H[1].ptr;
@@ -1955,7 +2174,11 @@ void aak_gpu_destroy(aak_gpu *g) {
     cudaStreamDestroy(g->stream);
   }
   if (g->plan) cufftDestroy(g->plan);
+  if (g->plan32) cufftDestroy(g->plan32);
   for (int ch = 0; ch < 2; ++ch) {
+    g->d_H32[ch].release();
+    g->d_D32[ch].release();
+    g->d_w32[ch].release();
     g->d_H[ch].release();
     g->d_D[ch].release();
     g->d_w[ch].release();
@@ -1980,6 +2203,18 @@ int aak_gpu_input_data(aak_gpu *g, const double *hI_f, const double *hII_f, cons
       (r = cuda_ok(cudaMemcpy(g->d_w[0].ptr, ASDinv1, (size_t)len * sizeof(double), cudaMemcpyHostToDevice))) ||
       (r = cuda_ok(cudaMemcpy(g->d_w[1].ptr, ASDinv2, (size_t)len * sizeof(double), cudaMemcpyHostToDevice))))
     return r;
+  // FP32 copies for precision 2 (rounded once, on the host)
+  const double *hd[2] = {hI_f, hII_f}, *hw[2] = {ASDinv1, ASDinv2};
+  std::vector<float> f(2 * (size_t)len);
+  for (int ch = 0; ch < 2; ++ch) {
+    if ((r = g->d_D32[ch].reserve(2 * (size_t)len)) || (r = g->d_w32[ch].reserve((size_t)len))) return r;
+    for (size_t j = 0; j < 2 * (size_t)len; ++j) f[j] = (float)hd[ch][j];
+    if ((r = cuda_ok(cudaMemcpy(g->d_D32[ch].ptr, f.data(), 2 * (size_t)len * sizeof(float), cudaMemcpyHostToDevice))))
+      return r;
+    for (size_t j = 0; j < (size_t)len; ++j) f[j] = (float)hw[ch][j];
+    if ((r = cuda_ok(cudaMemcpy(g->d_w32[ch].ptr, f.data(), (size_t)len * sizeof(float), cudaMemcpyHostToDevice))))
+      return r;
+  }
   return AAK_OK;
 }
 
@@ -2036,7 +2271,8 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   for (int32_t k0 = 0; k0 < nsrc; k0 += max_batch) {
     const int B = std::min<int32_t>(max_batch, nsrc - k0);
     tot[0] += g->ms[0];
-    if ((r = gpu_launch(g, B, false)) != AAK_OK || (r = gpu_likelihood_launch(g)) != AAK_OK) {
+    if ((r = gpu_launch(g, B, false, g->precision == 2 && g->d_D32[0].ptr)) != AAK_OK ||
+        (r = gpu_likelihood_launch(g)) != AAK_OK) {
       cudaDeviceSynchronize();
       return r;
     }
@@ -2080,7 +2316,7 @@ int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m) {
 }
 
 int aak_gpu_set_precision(aak_gpu *g, int32_t precision) {
-  if (!g || (precision != 0 && precision != 1)) return AAK_ERR_INVALID_PARAM;
+  if (!g || precision < 0 || precision > 2) return AAK_ERR_INVALID_PARAM;
   g->precision = precision;
   return AAK_OK;
 }

@@ -15,8 +15,9 @@
 #include <math.h>
 
 #include <atomic>
-#include <type_traits>
 #include <mutex>
+#include <type_traits>
+#include <utility>
 
 #include "aak_dense.cuh"
 
@@ -32,6 +33,14 @@ constexpr double kHalfSqrt3 = 0.86602540378443864676;
 #endif
 
 // ------------------------------------------------------------------ small helpers
+// x mod 2pi in [-pi, pi], two-term Cody-Waite reduction in FP64
+__device__ __forceinline__ double reduce_2pi_d(double x) {
+  const double k = rint(x * (1.0 / kTwoPi));
+  return fma(-k, 2.4492935982947064e-16, fma(-k, 6.283185307179586, x));
+}
+// the same, returned as float
+__device__ __forceinline__ float reduce_2pi_f(double x) { return (float)reduce_2pi_d(x); }
+
 __device__ __forceinline__ int find_source(const int64_t *tile_start, int nsrc, int64_t g) {
   int lo = 0, hi = nsrc;
   while (hi - lo > 1) {
@@ -166,6 +175,17 @@ __device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q,
   r[1] = sr * inv;
   r[2] = (sph - sth) * inv;
   if (om) *om = (d.coslam > 0) ? sph * inv : omega_phi(q.v, q.e, d.coslam, q.S, q.M);
+}
+
+// h_I, h_II of one sample: FP64 outputs, or FP32 ones (rows of an FP32 FFT)
+__device__ __forceinline__ void store_h(const BatchView &bv, int64_t o, double hI, double hII) {
+  if (bv.hI_f32) {
+    bv.hI_f32[o] = (float)hI;
+    bv.hII_f32[o] = (float)hII;
+  } else {
+    bv.hI[o] = hI;
+    bv.hII[o] = hII;
+  }
 }
 
 __device__ __forceinline__ double sample_time(const SourceDesc &d, int i) {
@@ -689,9 +709,16 @@ __device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes) {
 // w_n = z_1^n z_D: one complex product per harmonic), for M samples of one
 // tile at once: each table row is loaded once for all of them and the M
 // recurrences run side by side.
+// Split precision (T = float): every kAnchorEvery-th harmonic the rotor is
+// re-anchored at exp(i (n Phi' + D0)) with n Phi' + D0 reduced in FP64, so
+// the FP32 recurrence carries at most kAnchorEvery - 1 steps of rounding and
+// of the error of z_1, whatever n: the n Phi argument reduction stays FP64.
+constexpr int kAnchorEvery = 8;
 template <int K, typename T, int M>
 __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes, int stride, const T *dl, const T *c1,
-                                                       const T *s1, const T *cD, const T *sD, T *Sa, T *Sb, T *Sc) {
+                                                       const T *s1, const T *cD, const T *sD, const double *ph,
+                                                       const T *d0, T *Sa, T *Sb, T *Sc) {
+  constexpr bool kAnchor = sizeof(T) == 4;
   constexpr int NV = 3 * (K + 1);
   T zr[M], zi[M], sa[M], sb[M], sc[M];
 #pragma unroll
@@ -731,9 +758,16 @@ __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes,
         B = fma(B, dl[m], v[K + 1 + k]);
         C = fma(C, dl[m], v[2 * (K + 1) + k]);
       }
-      const T tr = zr[m] * c1[m] - zi[m] * s1[m];
-      zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
-      zr[m] = tr;
+      if (kAnchor && (n & (kAnchorEvery - 1)) == 0) {
+        float sn, cn;
+        __sincosf(reduce_2pi_f(fma((double)n, ph[m], (double)d0[m])), &sn, &cn);
+        zr[m] = (T)cn;
+        zi[m] = (T)sn;
+      } else {
+        const T tr = zr[m] * c1[m] - zi[m] * s1[m];
+        zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
+        zr[m] = tr;
+      }
       sa[m] = fma(A, zr[m], sa[m]);
       sb[m] = fma(B, zi[m], sb[m]);
       sc[m] = fma(C, zr[m], sc[m]);
@@ -920,12 +954,6 @@ __device__ __forceinline__ Resp<T> response(const Geom<T> &d, T ca, T sa, T c2g,
   return R;
 }
 
-// x mod 2pi in [-pi, pi], two-term Cody-Waite reduction in FP64, returned as float
-__device__ __forceinline__ float reduce_2pi_f(double x) {
-  const double k = rint(x * (1.0 / kTwoPi));
-  const double r = fma(-k, 2.4492935982947064e-16, fma(-k, 6.283185307179586, x));
-  return (float)r;
-}
 
 // Everything of one sample's harmonic sum except the mode sums: response
 // coefficients, amplitude and the harmonic phase rotors.
@@ -934,6 +962,8 @@ struct SamplePrep {
   Resp<T> R;
   T Amp, se;            // amplitude, sqrt(1 - e^2)
   T c1, s1, cD, sD;     // harmonic n: (c1 + i s1)^n (cD + i sD)
+  double ph;            // split: Phi + Doppler term reduced to [-pi, pi] in FP64 (the rotor's anchors)
+  T d0;                 // split: the harmonic-independent phase D0 (cD + i sD = exp(i D0))
   T dl;                 // e - e_c
 };
 
@@ -954,6 +984,8 @@ __device__ __forceinline__ SamplePrep<double> prep_fp64(const SourceDesc &d, con
   }
   sincos(Phi + D1, &P.s1, &P.c1);
   sincos(D0, &P.sD, &P.cD);
+  P.ph = 0.0;  // the FP64 rotor needs no anchors
+  P.d0 = 0.0;
   P.se = sqrt(1. - e * e);
   P.dl = e - ec;
   return P;
@@ -975,7 +1007,11 @@ __device__ __forceinline__ SamplePrep<float> prep_split(const SourceDesc &d, con
     D1 = kTwoPi * nu * kAUsec * d.sinqS * (double)P.R.cosorb_S;
     D0 = (float)(2.0 * gimdot * kAUsec * d.sinqS) * P.R.cosorb_S;
   }
-  __sincosf(reduce_2pi_f(Phi + D1), &P.s1, &P.c1);
+  // the rotor z_1 from the FP64 reduction, with the accurate sincosf: its
+  // phase error is multiplied by the harmonic number between two anchors
+  P.ph = reduce_2pi_d(Phi + D1);
+  sincosf((float)P.ph, &P.s1, &P.c1);
+  P.d0 = D0;
   __sincosf(D0, &P.sD, &P.cD);
   const float e = (float)e_d;
   P.se = sqrtf(1.f - e * e);
@@ -1115,9 +1151,12 @@ constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double)
 // TilePrep, knot window and Taylor table arrive in shared memory by bulk
 // copies that thread 0 issues at the start of the tile (the table's on a
 // second mbarrier, waited for only before phase 2); no table is built here.
+// kJointT: samples per thread whose harmonic sums run side by side (0: the
+// default of the precision); kMinB: resident CTAs per SM the register budget
+// is sized for.  Both are launch-shape choices of the autotuner.
 static_assert(sizeof(SourceDesc) % 16 == 0, "SourceDesc lands in shared memory with one bulk copy");
-template <bool kSplit, int kMode = 0, bool kPre = false>
-__global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(BatchView bv) {
+template <bool kSplit, int kMode = 0, bool kPre = false, int kJointT = 0, int kMinB = AAK_WAVE_MIN_BLOCKS>
+__global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) {
   constexpr bool kPhase = kMode != 0, kTdi = kMode == 2;
   static_assert(!kPre || kMode == 0, "the pre-pass serves the waveform mode");
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
@@ -1167,8 +1206,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           if constexpr (kPhase) {
             for (int r = 0; r < (kTdi ? kTdiRows : 8); ++r) bv.phase_out[r * bv.phase_stride + dz.out_offset + i] = 0.0;
           } else {
-            bv.hI[dz.out_offset + i] = 0.0;
-            bv.hII[dz.out_offset + i] = 0.0;
+            store_h(bv, dz.out_offset + i, 0.0, 0.0);
             if (bv.t_out) bv.t_out[dz.out_offset + i] = (dz.status != 0) ? 0.0 : sample_time(dz, i);
           }
         }
@@ -1592,13 +1630,15 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
     const double t_plunge = sample_time(d, d.i_plunge);
     const double t_zero = t_plunge + d.dt * d.i_buffer;
     using T = typename std::conditional<kSplit, float, double>::type;
-    constexpr int kJoint = kSplit ? AAK_JOINT_SPLIT : AAK_JOINT_FP64;
+    constexpr int kJoint = kJointT > 0 ? kJointT : (kSplit ? AAK_JOINT_SPLIT : AAK_JOINT_FP64);
+    static_assert(kTileChunks % kJoint == 0, "joint samples must divide the chunks");
     const T *tab = kSplit ? reinterpret_cast<const T *>(tabF) : reinterpret_cast<const T *>(tabD);
     const int rs = kPre ? (int)s_prep.stride : (kSplit ? kRowF : kRowD);  // table row stride
 #pragma unroll 1
     for (int g0 = 0; g0 < kTileChunks; g0 += kJoint) {
       SamplePrep<T> P[kJoint];
-      T dl[kJoint], c1[kJoint], s1[kJoint], cD[kJoint], sD[kJoint], Sa[kJoint], Sb[kJoint], Sc[kJoint];
+      T dl[kJoint], c1[kJoint], s1[kJoint], cD[kJoint], sD[kJoint], Sa[kJoint], Sb[kJoint], Sc[kJoint], d0[kJoint];
+      double ph[kJoint];
 #pragma unroll
       for (int m = 0; m < kJoint; ++m) {
         const int i = c.start + (g0 + m) * kTileThreads + tid;
@@ -1615,6 +1655,8 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
           P[m].c1 = P[m].cD = T(1);
         }
         dl[m] = P[m].dl;
+        ph[m] = P[m].ph;
+        d0[m] = P[m].d0;
         c1[m] = P[m].c1;
         s1[m] = P[m].s1;
         cD[m] = P[m].cD;
@@ -1622,19 +1664,19 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
       }
       if constexpr (kSplit) {
         switch (K) {
-          case 2: mode_sums_taylor_multi<2, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 3: mode_sums_taylor_multi<3, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 2: mode_sums_taylor_multi<2, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 3: mode_sums_taylor_multi<3, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
           default: break;
         }
       } else {
         switch (K) {
-          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 5: mode_sums_taylor_multi<5, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 8: mode_sums_taylor_multi<8, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
-          case 10: mode_sums_taylor_multi<10, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 5: mode_sums_taylor_multi<5, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 8: mode_sums_taylor_multi<8, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 10: mode_sums_taylor_multi<10, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
           default: break;
         }
       }
@@ -1661,8 +1703,7 @@ __global__ void __launch_bounds__(kTileThreads, AAK_WAVE_MIN_BLOCKS) k_waveform(
             hII = hII / wgt;
           }
         }
-        bv.hI[d.out_offset + i] = hI;
-        bv.hII[d.out_offset + i] = hII;
+        store_h(bv, d.out_offset + i, hI, hII);
         if (bv.t_out) bv.t_out[d.out_offset + i] = t;
       }
     }
@@ -1860,6 +1901,14 @@ void launch_dense_fp64(const BatchView &bv, int num_sms, cudaStream_t stream, cu
   launch_dense(bv, num_sms, stream, ev, 0);
 }
 
+template <bool kSplit, size_t... I>
+void set_variant_smem(int bytes, std::index_sequence<I...>) {
+  (cudaFuncSetAttribute(k_waveform<kSplit, 0, wave_variant(kSplit, (int)I).pre, wave_variant(kSplit, (int)I).joint,
+                                   wave_variant(kSplit, (int)I).min_blocks>,
+                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+   ...);
+}
+
 void prepare_dense_launch() {
   static std::atomic<unsigned long long> attrs_set{0};  // opt in to > 48 KB of shared memory once per device
   int dev = 0;
@@ -1869,12 +1918,35 @@ void prepare_dense_launch() {
     const int most = (int)(kWaveDynSmem + (size_t)kTabModes * kRowD * sizeof(double));
     cudaFuncSetAttribute(k_waveform<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     cudaFuncSetAttribute(k_waveform<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
-    cudaFuncSetAttribute(k_waveform<true, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
-    cudaFuncSetAttribute(k_waveform<false, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
+    set_variant_smem<true>(most, std::make_index_sequence<kNumVariants>{});
+    set_variant_smem<false>(most, std::make_index_sequence<kNumVariants>{});
     cudaFuncSetAttribute(k_waveform<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     cudaFuncSetAttribute(k_waveform<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     attrs_set.fetch_or(bit);
   }
+}
+
+// Launch one waveform-kernel instantiation as a persistent grid: every CTA
+// that fits on the device at once.
+template <typename K>
+void launch_persistent(K kernel, const BatchView &bv, int num_sms, size_t dyn, cudaStream_t stream) {
+  int resident = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kTileThreads, dyn);
+  resident = std::max(resident, 1);
+  const int grid = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
+  kernel<<<grid, kTileThreads, dyn, stream>>>(bv);
+}
+
+template <bool kSplit, int v>
+void launch_variant(const BatchView &bv, int num_sms, size_t dyn, cudaStream_t stream) {
+  constexpr WaveVariant w = wave_variant(kSplit, v);
+  launch_persistent(k_waveform<kSplit, 0, w.pre, w.joint, w.min_blocks>, bv, num_sms, dyn, stream);
+}
+
+template <bool kSplit, size_t... I>
+void launch_variant_index(int v, const BatchView &bv, int num_sms, size_t dyn, cudaStream_t stream,
+                          std::index_sequence<I...>) {
+  ((v == (int)I ? launch_variant<kSplit, (int)I>(bv, num_sms, dyn, stream) : void()), ...);
 }
 
 template <bool kSplit>
@@ -1886,8 +1958,9 @@ void launch_dense_t(const BatchView &bv, int num_sms, cudaStream_t stream, cudaE
   // per-sample values, then the Taylor table sized for the batch's harmonic count
   const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
   const size_t dyn = kWaveDynSmem + (size_t)rows * (kSplit ? kRowF * sizeof(float) : kRowD * sizeof(double));
-  const bool pre =
-      bv.tile_prep && bv.tile_tab && !bv.trajectory_only && bv.tab_slot >= tile_table_slot_bytes(rows, kSplit);
+  const int v = (bv.variant >= 0 && bv.variant < kNumVariants) ? bv.variant : 0;
+  const bool pre = wave_variant(kSplit, v).pre && bv.tile_prep && bv.tile_tab && !bv.trajectory_only &&
+                   bv.tab_slot >= tile_table_slot_bytes(rows, kSplit);
   prepare_dense_launch();
   if (pre) {
     const int64_t tiles = bv.total_tiles;
@@ -1895,14 +1968,8 @@ void launch_dense_t(const BatchView &bv, int num_sms, cudaStream_t stream, cudaE
     k_tile_table<kSplit><<<(unsigned)((tiles * rows + 127) / 128), 128, 0, stream>>>(bv, rows);
   }
   if (ev) cudaEventRecord(ev[2], stream);
-  // persistent grid: every CTA that fits on the device at once
-  int resident = 0;
-  if (pre) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<kSplit, 0, true>, kTileThreads, dyn);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<kSplit>, kTileThreads, dyn);
-  resident = std::max(resident, 1);
-  const int grid2 = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
-  if (pre) k_waveform<kSplit, 0, true><<<grid2, kTileThreads, dyn, stream>>>(bv);
-  else k_waveform<kSplit><<<grid2, kTileThreads, dyn, stream>>>(bv);
+  if (pre) launch_variant_index<kSplit>(v, bv, num_sms, dyn, stream, std::make_index_sequence<kNumVariants>{});
+  else launch_persistent(k_waveform<kSplit>, bv, num_sms, dyn, stream);
   if (ev) cudaEventRecord(ev[3], stream);
 }
 

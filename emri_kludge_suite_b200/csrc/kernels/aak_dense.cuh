@@ -67,6 +67,23 @@ inline int64_t tile_table_slot_bytes(int rows, bool split) {
   return split ? (int64_t)r * kRowF * (int64_t)sizeof(float) : (int64_t)r * kRowD * (int64_t)sizeof(double);
 }
 
+// Launch shapes of the waveform stage, the autotuner's candidates: with the
+// tile pre-pass or tables built inside the tiles, samples per thread whose
+// harmonic sums run side by side, and resident CTAs per SM the register
+// budget is sized for.  Variant 0 is the default of each precision.
+struct WaveVariant {
+  bool pre;
+  int joint;
+  int min_blocks;
+};
+constexpr int kNumVariants = 6;
+constexpr WaveVariant wave_variant(bool split, int v) {
+  return split ? (v == 1 ? WaveVariant{false, 0, 2} : v == 2 ? WaveVariant{true, 1, 2} : v == 3 ? WaveVariant{true, 4, 2}
+                  : v == 4 ? WaveVariant{true, 2, 3} : v == 5 ? WaveVariant{true, 1, 3} : WaveVariant{true, 2, 2})
+               : (v == 1 ? WaveVariant{false, 0, 2} : v == 2 ? WaveVariant{true, 2, 2} : v == 3 ? WaveVariant{true, 4, 2}
+                  : v == 4 ? WaveVariant{true, 1, 3} : v == 5 ? WaveVariant{true, 2, 3} : WaveVariant{true, 1, 2});
+}
+
 // Everything the kernels read about a batch.
 struct BatchView {
   const SourceDesc *src;
@@ -82,6 +99,7 @@ struct BatchView {
   TileLink *link;               // one per tile
   int32_t *link_flag;           // one per tile, cleared before every launch
   double *hI, *hII;             // outputs, indexed by src.out_offset + i
+  float *hI_f32 = nullptr, *hII_f32 = nullptr;  // FP32 outputs instead (same indexing), when set
   double *t_out;                // optional
   double *traj_out;             // optional dense trajectory, 9 x total samples (e,v,M,S,gim,Phi,alp,nu,gimdot)
   int64_t traj_stride;
@@ -99,6 +117,7 @@ struct BatchView {
   TilePrep *tile_prep = nullptr;
   void *tile_tab = nullptr;
   int64_t tab_slot = 0;
+  int32_t variant = 0;  // launch shape of the waveform stage (wave_variant), chosen by the autotuner
 };
 
 // Clear the work queue and the look-back flags, then launch the waveform

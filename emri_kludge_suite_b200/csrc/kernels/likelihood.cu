@@ -8,7 +8,9 @@
 // and shared-memory reduction to one partial per CTA, then a second tiny
 // kernel adds the partials of each template in a fixed order (deterministic,
 // no atomics).  Data and weights (77 MB for N = 3.2e6) stay L2-resident
-// across templates; the template spectra stream from HBM once.
+// across templates; the template spectra stream from HBM once.  An FP32
+// variant reads FP32 spectra, data and weights and accumulates with Kahan
+// compensation.
 #include "likelihood.cuh"
 
 #include <algorithm>
@@ -44,6 +46,59 @@ __global__ void __launch_bounds__(kIpThreads) k_inner_partial(InnerProductArgs a
   if (l == 0) {
     s[0][w] = dh;
     s[1][w] = hh;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int i = 0; i < kIpThreads / 32; ++i) {
+      a0 += s[0][i];
+      a1 += s[1][i];
+    }
+    a.partial[((int64_t)k * gridDim.x + blockIdx.x) * 2 + 0] = a0;
+    a.partial[((int64_t)k * gridDim.x + blockIdx.x) * 2 + 1] = a1;
+  }
+}
+
+// FP32 spectra: per-thread Kahan sums (the compensation c carries the low
+// part each addition loses), then the warp's pairwise shuffle tree in FP32
+// and the warps of the CTA in FP64.
+__device__ __forceinline__ void kahan_add(float &sum, float &c, float x) {
+  const float y = x - c;
+  const float t = sum + y;
+  c = (t - sum) - y;
+  sum = t;
+}
+
+__global__ void __launch_bounds__(kIpThreads) k_inner_partial_f32(InnerProductArgs32 a) {
+  const int k = blockIdx.y;
+  const int tid = threadIdx.x;
+  float dh = 0.f, hh = 0.f, cdh = 0.f, chh = 0.f;
+  const int64_t stride = (int64_t)gridDim.x * kIpThreads;
+  for (int ch = 0; ch < 2; ++ch) {
+    const float2 *H = reinterpret_cast<const float2 *>(a.H[ch] + (int64_t)k * a.row_floats);
+    const float2 *D = reinterpret_cast<const float2 *>(a.D[ch]);
+    const float *w = a.w[ch];
+    for (int64_t j = (int64_t)blockIdx.x * kIpThreads + tid; j < a.nbins; j += stride) {
+      const float2 h = H[j];
+      const float2 d = __ldg(&D[j]);
+      const float wj = __ldg(&w[j]);
+      const float hr = wj * h.x, hi = wj * h.y;
+      kahan_add(dh, cdh, fmaf(hr, d.x, hi * d.y));
+      kahan_add(hh, chh, fmaf(hr, hr, hi * hi));
+    }
+  }
+  dh -= cdh;
+  hh -= chh;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    dh += __shfl_xor_sync(0xffffffffu, dh, o);
+    hh += __shfl_xor_sync(0xffffffffu, hh, o);
+  }
+  __shared__ double s[2][kIpThreads / 32];
+  const int w = tid >> 5, l = tid & 31;
+  if (l == 0) {
+    s[0][w] = (double)dh;
+    s[1][w] = (double)hh;
   }
   __syncthreads();
   if (tid == 0) {
@@ -170,6 +225,13 @@ void launch_fisher_gram(const FisherArgs &a, int num_sms, cudaStream_t stream) {
   k_fisher_partial<<<grid, kFisherThreads, 0, stream>>>(a);
   const int ncombo = a.nd * (a.nd + 1), warps = kFisherThreads / 32;
   k_fisher_final<<<(ncombo + warps - 1) / warps, kFisherThreads, 0, stream>>>(a, grid);
+}
+
+void launch_inner_products_f32(const InnerProductArgs32 &a, cudaStream_t stream) {
+  if (a.ntemplates <= 0) return;
+  dim3 grid(kIpBlocksPerTemplate, a.ntemplates);
+  k_inner_partial_f32<<<grid, kIpThreads, 0, stream>>>(a);
+  k_inner_final<<<(a.ntemplates + 127) / 128, 128, 0, stream>>>(a.partial, kIpBlocksPerTemplate, a.ntemplates, a.out);
 }
 
 void launch_inner_products(const InnerProductArgs &a, cudaStream_t stream) {

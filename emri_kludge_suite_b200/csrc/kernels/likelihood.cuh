@@ -28,6 +28,23 @@ constexpr int kIpBlocksPerTemplate = 64;
 
 void launch_inner_products(const InnerProductArgs &a, cudaStream_t stream);
 
+// The same products from FP32 spectra (an FP32 R2C transform of FP32
+// template rows, row stride `row_floats` floats) and FP32 copies of the data
+// and weights.  Each thread accumulates its bins in FP32 with Kahan
+// compensation, a warp combines its lanes by a pairwise shuffle tree, and the
+// warps' and CTAs' partial sums are added in FP64 in a fixed order.
+struct InnerProductArgs32 {
+  const float *H[2];   // channel I, II template spectra (ntemplates rows)
+  int64_t row_floats;  // distance between template rows, in floats
+  const float *D[2];   // data spectra (nbins complex, interleaved)
+  const float *w[2];   // weights (nbins)
+  int64_t nbins;
+  int32_t ntemplates;
+  double *partial;     // scratch: ntemplates x blocks_per_template x 2
+  double *out;         // ntemplates x 2
+};
+void launch_inner_products_f32(const InnerProductArgs32 &a, cudaStream_t stream);
+
 // Fisher-matrix Gram sums of finite-difference template spectra
 // (pygpuAAK/pygpuAAK.py:269-300): rows 2i and 2i+1 of each channel hold the
 // two evaluations of derivative i, D_i = scale w (H[2i+1] - H[2i]), and

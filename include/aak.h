@@ -229,6 +229,29 @@ int aak_batch_last_launches(aak_ctx *ctx);
  * reference counterpart (the reference's kernels do not wait on one another). */
 int aak_batch_device_status(aak_ctx *ctx);
 
+/* Autotuner of the waveform stage's launch shape.  The candidates
+ * (AAK_NUM_VARIANTS of them, per precision) are the tile pre-pass with bulk
+ * copies or tables built inside the tiles, 1, 2 or 4 samples per thread in the
+ * harmonic loop, and 2 or 3 resident CTAs per SM; tiles are 1024 samples in
+ * every candidate (the host plan is laid out per tile).  On the context's
+ * uploaded batch, with the caller's output buffers d_hI, d_hII, every
+ * candidate runs once as a warm-up and twice timed (CUDA events); the fastest
+ * becomes the context's choice for `precision`, used by aak_batch_run,
+ * aak_batch_run_graph and the host-buffer entry points.  Key: device name and
+ * SM count, precision, largest harmonic count, and the numbers of sources and
+ * of samples of the median source in powers of two.  cache_path (optional): a
+ * text file of "key variant ms_0 .. ms_5" lines; an entry for the key is used
+ * without timing, a new choice is appended.  variant (optional) receives the
+ * choice, ms_per_variant (optional, AAK_NUM_VARIANTS entries) the timings in
+ * ms (-1 when read from the cache).  No reference counterpart: the
+ * reference's launch shape is fixed (src/cuda/AAK_manager.cu:233, 245). */
+#define AAK_NUM_VARIANTS 6
+int aak_ctx_autotune(aak_ctx *ctx, double *d_hI, double *d_hII, int32_t precision, const char *cache_path,
+                     int32_t *variant, float *ms_per_variant);
+/* Set the launch shape of `precision` directly (0 .. AAK_NUM_VARIANTS - 1;
+ * 0 is the default). */
+int aak_ctx_set_variant(aak_ctx *ctx, int32_t precision, int32_t variant);
+
 /* Bound of one look-back wait of this context's batch launches, in SM clocks
  * (<= 0: the default, about 2 s).  A wait that reaches it gives up, the tile
  * takes a zero carry and aak_batch_device_status reports
@@ -244,8 +267,8 @@ int aak_selftest_lookback_timeout(int64_t cycles);
 
 /* Per-kernel timing of aak_batch_run with CUDA events on its stream: after
  * aak_batch_set_profiling(ctx, 1), aak_batch_kernel_ms returns the durations
- * of (work-queue and look-back flag clears, 0 -- no separate phase-sum kernel,
- * waveform kernel) of the last run in ms. */
+ * of (work-queue and look-back flag clears, the tile pre-pass -- 0 without
+ * it --, the waveform kernel) of the last run in ms. */
 int aak_batch_set_profiling(aak_ctx *ctx, int32_t on);
 int aak_batch_kernel_ms(aak_ctx *ctx, float *ms3);
 
@@ -340,7 +363,10 @@ int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, i
                    int32_t *status);
 
 /* Template precision: 0 = FP64 throughout (default), 1 = split (FP64 phases
- * and angle reductions, FP32 geometry, response, Bessel evaluation). */
+ * and angle reductions, FP32 geometry, response, Bessel evaluation), 2 =
+ * split templates written as FP32 rows, an FP32 R2C transform and FP32 inner
+ * products with Kahan-compensated sums (aak_gpu_likelihood_batch only; the
+ * other calls run as precision 1). */
 int aak_gpu_set_precision(aak_gpu *g, int32_t precision);
 
 /* Milliseconds of the last batch: host planning, waveform kernels, FFT, reduction. */

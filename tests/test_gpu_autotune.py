@@ -1,0 +1,64 @@
+"""The autotuner of the waveform stage's launch shape (aak_ctx_autotune):
+every candidate gives the same waveforms, the fastest is kept, and the
+tuning-cache file is written and read back."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_mapped, golden_names, load_golden
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+import emri_kludge_suite_b200 as E  # noqa: E402
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _batch():
+    gs = [load_golden(n) for n in golden_names()]
+    wb = E.WaveBatch(0)
+    wb.plan([g["pars"] for g in gs], nmodes=[int(g["nmodes"]) for g in gs], mapped=[golden_mapped(g) for g in gs])
+    wb.upload()
+    return wb
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_every_launch_shape_gives_the_same_waveforms(precision):
+    wb = _batch()
+    N = wb.total_samples
+    ref = None
+    for v in range(6):
+        a = torch.zeros(N, dtype=torch.float64, device="cuda")
+        b = torch.zeros_like(a)
+        wb.set_variant(precision, v)
+        wb.run(a.data_ptr(), b.data_ptr(), precision=precision)
+        torch.cuda.synchronize()
+        x = np.concatenate([a.cpu().numpy(), b.cpu().numpy()])
+        if ref is None:
+            ref = x
+        else:
+            # the same arithmetic per sample in every shape (tables from the same builder)
+            assert np.abs(x - ref).max() <= 1e-14 * np.abs(ref).max(), v
+    assert wb.device_status() == 0
+
+
+def test_autotune_keeps_the_fastest_and_uses_its_cache(tmp_path):
+    wb = _batch()
+    N = wb.total_samples
+    a = torch.zeros(N, dtype=torch.float64, device="cuda")
+    b = torch.zeros_like(a)
+    cache = str(tmp_path / "tune.txt")
+    v, ms = wb.autotune(a.data_ptr(), b.data_ptr(), precision=1, cache_path=cache)
+    assert all(m > 0 for m in ms) and ms[v] == min(ms)
+    lines = open(cache).read().splitlines()
+    assert len(lines) == 1 and int(lines[0].split()[1]) == v
+    v2, ms2 = wb.autotune(a.data_ptr(), b.data_ptr(), precision=1, cache_path=cache)
+    assert v2 == v and all(m == -1.0 for m in ms2)  # read from the cache, nothing timed
+    assert len(open(cache).read().splitlines()) == 1
+    assert os.path.getsize(cache) > 0

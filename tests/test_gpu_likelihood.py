@@ -98,3 +98,35 @@ def test_pygpuaak_nll_is_zero_at_injection_without_noise():
     # the injected SNR^2 equals <h|h>
     snr_d, snr_h = like.NLL(*INJ, return_snr=True)
     assert snr_h[0] ** 2 == pytest.approx(like.d_d, rel=1e-9)
+
+
+def test_fp32_transform_and_compensated_products_against_fp64_oracle():
+    """Precision 2: split templates in FP32 rows, an FP32 R2C transform and the
+    Kahan-compensated FP32 inner products, against the FP64 oracle's inner
+    products of the FP64 oracle waveforms.  Bar: 2e-5 relative on <h|d> and
+    <h|h>, and |dlogL| <= 2e-5 (d_d + h_h) (the FP32 transform's rounding)."""
+    w1, w2 = _weights()
+    dI, dII = _oracle_wave(INJ * np.r_[1, 1, 1.0001, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1, 1])
+    D1, D2 = np.fft.rfft(dI) * w1, np.fft.rfft(dII) * w2
+    d_d = 4.0 * float(np.sum(np.abs(D1) ** 2) + np.sum(np.abs(D2) ** 2))
+    g = GPUAAK(1.0, 100, LENGTH, 100.0, DT, True, False)
+    g.input_data(D1, D2, w1, w2)
+    rng = np.random.default_rng(11)
+    X = np.tile(INJ, (5, 1))
+    X[:, 2] *= 1 + 1e-5 * rng.standard_normal(5)
+    X[:, 6:11] += 1e-3 * rng.standard_normal((5, 5))
+    g.set_precision(2)
+    out32, st = g.likelihood_batch(X, max_batch=4, return_status=True)
+    g.set_precision(0)
+    out64 = g.likelihood_batch(X, max_batch=4)
+    assert np.all(st == 0)
+    worst = 0.0
+    for k in range(len(X)):
+        oI, oII = _oracle_wave(X[k])
+        ref = O.inner_products(oI, oII, D1, D2, w1, w2)
+        np.testing.assert_allclose(out64[k], ref, rtol=1e-8)
+        np.testing.assert_allclose(out32[k], ref, rtol=2e-5)
+        dl = 0.5 * abs((out32[k, 1] - 2 * out32[k, 0]) - (ref[1] - 2 * ref[0]))
+        worst = max(worst, dl / (d_d + ref[1]))
+    print("fp32 likelihood: max |dlogL| / (d_d + h_h) =", worst)
+    assert worst <= 2e-5
