@@ -252,7 +252,7 @@ def cpu_likelihood_reference(procs: int = 0, sample_len: int = 200000) -> dict:
 FIDUCIAL = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])  # gpu_gen_AAK order
 # DRAM bytes (read + write) per sample of the split waveform kernel, from an ncu
 # capture of that kernel on 16 sources of the configuration-1 draw
-TRAFFIC_BYTES_PER_SAMPLE = (238.248192e6 + 413.877248e6) / 28_332_971
+TRAFFIC_BYTES_PER_SAMPLE = (281.245184e6 + 413.069056e6) / 28_332_971
 LIKE_LENGTH = 3_200_000  # 1 yr at dt = 10 s rounded up to the 5-smooth FFT length 2^10 * 5^5
 
 
@@ -482,8 +482,11 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
     f32["max_abs_dlogL_vs_fp64"] = float(np.max(np.abs(logl32 - logl64)[ok32])) if ok32.any() else None
     f32["median_abs_dlogL_vs_fp64"] = float(np.median(np.abs(logl32 - logl64)[ok32])) if ok32.any() else None
     res["split_fp32_fft"] = f32
-    # HBM roofline of the inner-product kernel: template spectra of both
-    # channels, the data of both channels and one weight array per bin
+    # HBM roofline of the inner-product kernel.  Each template's spectra of
+    # both channels stream from HBM once; the data and weights (77 MB in FP64,
+    # 38 MB in FP32) stay in the 126 MB L2 across the templates of a batch, so
+    # the HBM-bound bytes per template are the spectra.  The byte count of the
+    # formula with the data and weights is reported beside it.
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
@@ -491,14 +494,16 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
         pass
     hbm = peaks.get("hbm_gbs") or 6650.0
     nb = LIKE_LENGTH // 2 + 1
-    for key, run_, per_bin in (("fp64_plain", plain, 2 * (16 + 16) + 8), ("split_fp32_fft", f32, 2 * (8 + 8) + 4)):
+    for key, run_, stream_bin, formula_bin, kern in (("fp64_plain", plain, 2 * 16, 2 * (16 + 16) + 8, "k_inner_partial"),
+                                                     ("split_fp32_fft", f32, 2 * 8, 2 * (8 + 8) + 4, "k_inner_partial_f32")):
         ms_red = run_["ms"]["reduce"]
-        gbs = per_bin * nb * n_templates / (ms_red * 1e-3) / 1e9 if ms_red > 0 else None
+        gbs = stream_bin * nb * n_templates / (ms_red * 1e-3) / 1e9 if ms_red > 0 else None
         res[key]["reduce_roofline"] = {
-            "kernel": "k_inner_partial" + ("_f32" if per_bin < 60 else "") + " + k_inner_final", "bound": "hbm",
-            "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm if gbs else None,
-            "bytes_per_template": per_bin * nb,
-            "bytes_formula": "2 channels x nbins x (template + data complex) + nbins x weight",
+            "kernel": kern + " + k_inner_final", "bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+            "frac": gbs / hbm if gbs else None, "bytes_per_template": stream_bin * nb,
+            "bytes_rule": "template spectra of both channels (HBM); data and weights are L2-resident",
+            "formula_bytes_per_template": formula_bin * nb,
+            "formula_gbs": formula_bin * nb * n_templates / (ms_red * 1e-3) / 1e9 if ms_red > 0 else None,
             "peak_source": "measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)" if peaks.get("hbm_gbs") else "fallback"}
     if with_cpu:
         res["cpu_baseline"] = cpu_likelihood_reference()
@@ -1013,13 +1018,18 @@ def run_gpu(args, rank, world, local_rank):
 
 # ----------------------------------------------------------------------------- profiling workloads
 # Small cases of the same kernels for ncu captures (one GPU):
-#   python bench.py --profile waveform   # 16 of the 512 sources, FP64 and split, twice each
+#   python bench.py --profile waveform   # 16 of the 512 sources, FP64 and split, default and tuned shapes
 #   python bench.py --profile phase      # the phase product of the same 16 sources, twice
 #   python bench.py --profile fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
 #   python bench.py --profile tdi        # frequency-domain TDI of the waveform workload's 16 sources, twice
 #   python bench.py --profile mlp        # warm-start network: forward on 2^20 points, a training step
 #   python bench.py --profile likelihood # 32 config-4 templates, FP64 and FP32 transform + products
 def profile_waveform():
+    """16 of the 512 configuration-1 sources (every 32nd; 28,332,971 samples,
+    n = 1..30): per precision the default launch shape and the one the
+    autotuner picks on the full batch (FP64: 3 CTAs/SM; split: 1 sample per
+    thread, 3 CTAs/SM), twice each, in the order FP64 v0, FP64 v4, split v0,
+    split v5 (16 B/sample of outputs: 453 MB, above the 126 MB L2)."""
     import torch
 
     from emri_kludge_suite_b200.aak import WaveBatch
@@ -1031,10 +1041,12 @@ def profile_waveform():
     n = wb.total_samples
     hI = torch.empty(n, dtype=torch.float64, device="cuda")
     hII = torch.empty_like(hI)
-    for precision in (0, 1):
+    for precision, variant in ((0, 0), (0, 4), (1, 0), (1, 5)):
+        wb.set_variant(precision, variant)
         for _ in range(2):
             wb.run(hI.data_ptr(), hII.data_ptr(), precision=precision)
     torch.cuda.synchronize()
+    assert wb.device_status() == 0
     print("waveform workload:", n, "samples")
 
 

@@ -43,8 +43,11 @@ def test_every_launch_shape_gives_the_same_waveforms(precision):
         if ref is None:
             ref = x
         else:
-            # the same arithmetic per sample in every shape (tables from the same builder)
-            assert np.abs(x - ref).max() <= 1e-14 * np.abs(ref).max(), v
+            # the same algorithm and tables in every shape; the instantiations
+            # may contract multiply-adds differently, so they agree to the
+            # rounding of their arithmetic: FP64, or the FP32 harmonic sums
+            tol = 1e-10 if precision == 0 else 1e-5
+            assert np.abs(x - ref).max() <= tol * np.abs(ref).max(), (v, np.abs(x - ref).max() / np.abs(ref).max())
     assert wb.device_status() == 0
 
 
