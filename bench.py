@@ -395,6 +395,42 @@ def ref_fisher_seconds(sample_len: int = 200000) -> dict:
                                           f"{rate:.3g} samples/s, scaled to 28 x {LIKE_LENGTH} samples"}
 
 
+def template_pars(x) -> dict:
+    """gpu_gen_AAK-order parameters -> an AAKwrapper pars dict over the configuration-4 span."""
+    iota, s_, p, e, M, mu, gamma, psi, alph, thS, phS, thK, phK, D = x
+    return dict(backint=False, LISA=True, length=LIKE_LENGTH, dt=DT, p=p, T=LIKE_LENGTH * DT / YEAR, f=0.0, T_fit=1.0,
+                mu=mu, M=M, s=s_, e=e, iota=iota, gamma=gamma, psi=psi, theta_S=thS, phi_S=phS, theta_K=thK, phi_K=phK,
+                alpha=alph, D=D)
+
+
+def run_evolve_compare(sources, local_rank: int, nthreads: int, n_templates: int = 4096) -> dict:
+    """Batch planning with the coarse AK recurrences on the host threads (AVX2
+    lane groups, the default) against one GPU thread per source
+    (aak_ctx_set_evolve_device), on the configuration-1 sources and on
+    configuration-4 likelihood templates: wall time of one plan each way."""
+    import emri_kludge_suite_b200 as E
+
+    out = {}
+    for name, plist, nm in (("config1_512_sources", sources, NMODES),
+                            (f"config4_{n_templates}_templates", [template_pars(x) for x in config4_templates(n_templates)],
+                             None)):
+        res = {}
+        for mode in ("host", "device"):
+            wb = E.WaveBatch(local_rank)
+            wb.set_evolve_device(mode == "device")
+            wb.plan(plist[: min(8, len(plist))], nmodes=nm, nthreads=nthreads)  # warm-up (threads, pinned buffers)
+            t0 = time.perf_counter()
+            wb.plan(plist, nmodes=nm, nthreads=nthreads)
+            res[mode] = {"plan_s": time.perf_counter() - t0, "failed": int(np.sum(wb.status != 0))}
+            if mode == "device":
+                res[mode]["passes_ms"] = wb.plan_ms()
+            wb.close()
+        res["device_over_host"] = res["device"]["plan_s"] / res["host"]["plan_s"]
+        out[name] = res
+    out["host_threads"] = nthreads
+    return out
+
+
 def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int = 0, with_cpu: bool = False,
                    rank: int = 0, world: int = 1) -> dict:
     """likelihoods/s of the batched path: host planning + waveforms + FFT + reduction, end to end per call."""
@@ -917,6 +953,9 @@ def run_gpu(args, rank, world, local_rank):
         w2.close()
         torch.cuda.empty_cache()
 
+    # ---- batch planning: host recurrences against the device evolution
+    evolve_cmp = run_evolve_compare(sources, local_rank, nthreads) if args.evolve_compare and rank == 0 else None
+
     # ---- end to end through the C ABI with pinned host buffers
     e2e_steps = max(1, min(args.steps, args.e2e_steps))
     hIh = torch.empty(N, dtype=torch.float64, pin_memory=True)
@@ -987,6 +1026,7 @@ def run_gpu(args, rank, world, local_rank):
         "plain_fp64_per_source": plain,
         "phase_product": phases,
         "tdi": tdi,
+        "front_end_device_evolution": evolve_cmp,
         "roofline": roofline,
         "clocks": clk,
         "e2e": e2e,
@@ -1160,6 +1200,8 @@ def main():
     ap.add_argument("--fisher", type=int, default=8, help="Fisher matrices to time at config-4 points (0: skip)")
     ap.add_argument("--tdi", type=int, default=1, help="time the frequency-domain TDI of 16 sources (0: skip)")
     ap.add_argument("--phases", type=int, default=1, help="time the AAK phase product of the batch (0: skip)")
+    ap.add_argument("--evolve-compare", type=int, default=1,
+                    help="time batch planning with the host and the device AK evolution (0: skip)")
     ap.add_argument("--parmap-points", type=int, default=1 << 20,
                     help="config-3 training points of the warm-start network (0: skip)")
     ap.add_argument("--profile", default=None, choices=sorted(PROFILES),

@@ -170,6 +170,9 @@ def lib():
     L.aak_batch_newton_stats.argtypes = [_vp, _i64p, _i64p, _i64p]
     L.aak_gpu_set_parmap_model.argtypes = [_vp, _vp]
     L.aak_ctx_set_parmap_device.argtypes = [_vp, _i32]
+    L.aak_ctx_set_evolve_device.argtypes = [_vp, _i32]
+    L.aak_batch_plan_ms.argtypes = [_vp, _dp]
+    L.aak_lpt_partition.argtypes = [_dp, _i64, _i32, _i32p, _dp]
     L.aak_gpu_set_parmap_device.argtypes = [_vp, _i32]
     _lib = L
     return L

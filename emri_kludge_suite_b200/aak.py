@@ -197,6 +197,18 @@ class WaveBatch:
         launch) instead of on the planning threads; results are bit-identical."""
         check(lib().aak_ctx_set_parmap_device(self._ctx, int(bool(on))), "aak_ctx_set_parmap_device")
 
+    def set_evolve_device(self, on: bool = True):
+        """Run every source's coarse AK recurrence on the GPU (one thread per
+        source) between two host planning passes, instead of on the planning
+        threads; knots agree with the host's to about 1e-15 relative."""
+        check(lib().aak_ctx_set_evolve_device(self._ctx, int(bool(on))), "aak_ctx_set_evolve_device")
+
+    def plan_ms(self) -> dict:
+        """Wall times (ms) of the last plan's passes with the device evolution."""
+        ms = np.zeros(4)
+        check(lib().aak_batch_plan_ms(self._ctx, ptr(ms)), "aak_batch_plan_ms")
+        return dict(zip(("host_before", "device_evolution", "host_after", "total"), ms.tolist()))
+
     def newton_stats(self) -> dict:
         """Map statistics of the last plan: points, Newton iterations, fallbacks."""
         a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

@@ -25,8 +25,8 @@ LIB = os.path.join(PKG, "libaak_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-I", os.path.join(REPO, "include")]
 
-# per-file flags: the device map solve must round as the host does (no FMA contraction)
-FILE_FLAGS = {"kernels/parmap_newton.cu": ["-fmad=false"]}
+# per-file flags: the device map solve and the device AK evolution round as the host does (no FMA contraction)
+FILE_FLAGS = {"kernels/parmap_newton.cu": ["-fmad=false"], "kernels/ak_evolve.cu": ["-fmad=false"]}
 
 SOURCES = [
     "host/kerr.cpp",
@@ -38,6 +38,7 @@ SOURCES = [
     "kernels/likelihood.cu",
     "kernels/parmap_mlp.cu",
     "kernels/parmap_newton.cu",
+    "kernels/ak_evolve.cu",
     "capi/aak_capi.cpp",
     "capi/mlp_capi.cpp",
 ]

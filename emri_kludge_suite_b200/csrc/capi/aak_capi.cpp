@@ -25,6 +25,7 @@
 #include "../host/parmap_data.hpp"
 #include "../host/pipeline.hpp"
 #include "../kernels/aak_dense.cuh"
+#include "../kernels/ak_evolve.cuh"
 #include "../kernels/likelihood.cuh"
 #include "../kernels/parmap_newton.cuh"
 #include "errors.hpp"
@@ -101,6 +102,8 @@ struct aak_ctx {
   DevBuf<double> d_out;  // outputs for the host-buffer entry points
   // batched device solve of the Kerr -> AK map (opt-in: parmap_device)
   bool parmap_device = false;
+  bool evolve_device = false;      // coarse AK evolution of a batch on the GPU (one thread per source)
+  double plan_ms[4] = {0, 0, 0, 0};  // last plan: before / on the device / after the evolution, total
   DevBuf<ParmapJob> d_pm_jobs;
   DevBuf<double> d_pm_warm, d_pm_map;
   DevBuf<int32_t> d_pm_it;
@@ -546,6 +549,105 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     }
     return st;
   };
+  if (ctx->evolve_device && dev >= 0) {
+    // Planning in three passes around a device evolution: (a) front end, map
+    // and the fit window of every source on host threads; (b) every source's
+    // AK recurrence beyond the fit window in one launch, one GPU thread per
+    // source; (c) fitted knots, plunge search and descriptors on host threads.
+    using clk = std::chrono::steady_clock;
+    const auto t_a = clk::now();
+    std::vector<MappedTrajectory> mts(nsrc);
+    std::vector<WaveInputs> ws(nsrc);
+    std::vector<PlanCarryPtr> carry(nsrc);
+    std::vector<EvolveJob> jobs(nsrc);
+    parallel_for(nsrc, nthreads, [&](int64_t t) {
+      on_device();
+      const int s = order[t];
+      const Params Pp = to_params(Pv[s]);
+      int st = map_one(s, Pp, &mts[s]);
+      if (st == kOk) {
+        genwave_inputs(Pp, mts[s], nm ? nm[s] : 0, &ws[s]);
+        if (ws[s].nmodes > 4096) st = kErrCapacity;
+        else st = plan_source_begin(ws[s], &ctx->plans[s], &carry[s], &jobs[s]);
+      }
+      ctx->status[s] = st;
+    });
+    const auto t_b = clk::now();
+    // the jobs of the sources still in play, their segments one after another
+    std::vector<int> live;
+    int64_t total = 0;
+    for (int s = 0; s < nsrc; ++s)
+      if (ctx->status[s] == kOk) {
+        jobs[s].off = total;
+        total += jobs[s].j_end + 1;
+        live.push_back(s);
+      }
+    std::vector<EvolveJob> lj(live.size());
+    for (size_t k = 0; k < live.size(); ++k) lj[k] = jobs[live[k]];
+    std::vector<double> ev(2 * (size_t)std::max<int64_t>(total, 1));
+    double *eh = ev.data(), *vh = eh + std::max<int64_t>(total, 1);
+    parallel_for((int64_t)live.size(), nthreads, [&](int64_t k) {
+      const int s = live[k];
+      plan_carry_prefix(*carry[s], jobs[s], eh + jobs[s].off, vh + jobs[s].off);
+    });
+    if (!live.empty()) {
+      on_device();
+      int r;
+      if (!ctx->pm_stream &&
+          (r = cuda_ok(cudaStreamCreateWithFlags(&ctx->pm_stream, cudaStreamNonBlocking))) != AAK_OK)
+        return r;
+      DevBuf<double> d_ev;
+      DevBuf<EvolveJob> d_jobs;
+      if ((r = d_ev.reserve(2 * (size_t)total)) || (r = d_jobs.reserve(live.size()))) return r;
+      cudaStream_t st = ctx->pm_stream;
+      // every entry goes up (the recurrence's part is overwritten): one copy each way
+      r = cuda_ok(cudaMemcpyAsync(d_ev.ptr, eh, (size_t)total * sizeof(double), cudaMemcpyHostToDevice, st));
+      if (r == AAK_OK)
+        r = cuda_ok(cudaMemcpyAsync(d_ev.ptr + total, vh, (size_t)total * sizeof(double), cudaMemcpyHostToDevice, st));
+      if (r == AAK_OK)
+        r = cuda_ok(cudaMemcpyAsync(d_jobs.ptr, lj.data(), lj.size() * sizeof(EvolveJob), cudaMemcpyHostToDevice, st));
+      if (r == AAK_OK) {
+        launch_ak_evolve(d_jobs.ptr, (int)lj.size(), d_ev.ptr, d_ev.ptr + total, st);
+        r = cuda_ok(cudaGetLastError());
+      }
+      if (r == AAK_OK)
+        r = cuda_ok(cudaMemcpyAsync(eh, d_ev.ptr, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, st));
+      if (r == AAK_OK)
+        r = cuda_ok(cudaMemcpyAsync(vh, d_ev.ptr + total, (size_t)total * sizeof(double), cudaMemcpyDeviceToHost, st));
+      if (r == AAK_OK)
+        r = cuda_ok(cudaMemcpyAsync(lj.data(), d_jobs.ptr, lj.size() * sizeof(EvolveJob), cudaMemcpyDeviceToHost, st));
+      if (r == AAK_OK) r = cuda_ok(cudaStreamSynchronize(st));
+      d_ev.release();
+      d_jobs.release();
+      if (r != AAK_OK) return r;
+      for (size_t k = 0; k < live.size(); ++k) jobs[live[k]] = lj[k];
+    }
+    const auto t_c = clk::now();
+    parallel_for((int64_t)live.size(), nthreads, [&](int64_t k) {
+      on_device();
+      const int s = live[k];
+      const int st = plan_source_end(*carry[s], jobs[s], eh + jobs[s].off, vh + jobs[s].off);
+      carry[s].reset();
+      ctx->status[s] = st;
+    });
+    for (int s = 0; s < nsrc; ++s)
+      if (ctx->status[s] != kOk) {
+        ctx->plans[s].knot_t.clear();
+        ctx->plans[s].knot_y.clear();
+      }
+    if (on_done)
+      for (int s = 0; s < nsrc; ++s) on_done(s);
+    const auto t_d = clk::now();
+    auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    ctx->plan_ms[0] = ms(t_a, t_b);
+    ctx->plan_ms[1] = ms(t_b, t_c);
+    ctx->plan_ms[2] = ms(t_c, t_d);
+    ctx->plan_ms[3] = ms(t_a, t_d);
+    ctx->newton_points = points;
+    ctx->newton_iters = iters;
+    ctx->newton_fallbacks = fallbacks;
+    return AAK_OK;
+  }
   parallel_for(ntasks, nthreads, [&](int64_t t) {
     on_device();
     const int64_t k = (t < nbig) ? t : nbig + kPlanGroup * (t - nbig);
@@ -2296,6 +2398,20 @@ int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, i
   const int r = select_device(g->ctx->device);
   if (r != AAK_OK) return r;
   return gpu_fisher(g, params, nd, scale, nthreads, gram, status);
+}
+
+int aak_ctx_set_evolve_device(aak_ctx *ctx, int32_t on) {
+  if (!ctx || (on && ctx->device < 0)) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->evolve_device = on != 0;
+  return AAK_OK;
+}
+
+int aak_batch_plan_ms(aak_ctx *ctx, double *ms4) {
+  if (!ctx || !ms4) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (int k = 0; k < 4; ++k) ms4[k] = ctx->plan_ms[k];
+  return AAK_OK;
 }
 
 int aak_ctx_set_parmap_device(aak_ctx *ctx, int32_t on) {

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <memory>
 #include <vector>
 
 #include "../aak_common.hpp"
@@ -211,6 +212,35 @@ static_assert(kPlanGroup % 4 == 0, "whole AVX2 vectors");
 void plan_source_group(const WaveInputs *const w[], SourcePlan *const p[], int n);
 // Per-source geometry constants of the waveform (orientation fields set).
 void fill_geometry(SourceDesc *d);
+
+// plan_source split at the coarse AK evolution beyond the fit window, so
+// that the recurrence can run elsewhere (one GPU thread per source,
+// ak_evolve.cu).  Indices are relative to j0, the first knot of the fit
+// window: a source's AK (e, v) occupy entries 0 .. j_end of a segment at
+// `off` in the batch's arrays; the fit window fills entries 0 .. j_first and
+// the recurrence entries j_first + 1 .. j_end, with evolve()'s freezing.
+struct EvolveJob {
+  int64_t off;                // the source's first entry in the batch's e, v arrays
+  int32_t j_first, j_end;     // the recurrence computes entries j_first + 1 .. j_end
+  int32_t j_max, j_max_temp;  // freeze indices: in, after the fit window; out, after the recurrence
+  double edot, vdot;          // AK rates of the step before j_first (out: of the last step)
+  double coslam, mu, M0, S0, dt_large;
+};
+struct PlanCarry;  // a source's planning state between the two halves
+struct PlanCarryDelete {
+  void operator()(PlanCarry *c) const;
+};
+using PlanCarryPtr = std::unique_ptr<PlanCarry, PlanCarryDelete>;
+// The first half (the fit window and its corrections).  Returns plan->status;
+// on success *carry holds the state (w and plan must outlive it) and *job the
+// recurrence (off left to the caller).
+int plan_source_begin(const WaveInputs &w, SourcePlan *plan, PlanCarryPtr *carry, EvolveJob *job);
+// e, v of the fit window: entries 0 .. job.j_first.
+void plan_carry_prefix(const PlanCarry &c, const EvolveJob &job, double *e, double *v);
+// The second half, with e, v holding entries 0 .. job.j_end and the job's
+// outputs: the fitted knots, the plunge search and the descriptor, as
+// plan_source.  Returns plan->status.
+int plan_source_end(PlanCarry &c, const EvolveJob &job, const double *e, const double *v);
 
 // (e, v, M, S) of the natural spline through the n knots (x, y[4 n]) at xv,
 // with the coefficients of its piece from the windowed solve the device

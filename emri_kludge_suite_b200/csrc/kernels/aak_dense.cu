@@ -174,7 +174,11 @@ __device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q,
   r[0] = (sth - sr) * inv;
   r[1] = sr * inv;
   r[2] = (sph - sth) * inv;
-  if (om) *om = (d.coslam > 0) ? sph * inv : omega_phi(q.v, q.e, d.coslam, q.S, q.M);
+  // Omega_phi: the ratio for phi with (Y, q) on prograde orbits and (-Y, -q)
+  // on retrograde ones (AAK.cc:15-23).  The t numerator depends on q only
+  // through q Y, q^2 and Y^2, so it is the same number for (-Y, -q): only the
+  // phi numerator is evaluated again.
+  if (om) *om = ((d.coslam > 0) ? sph : pn_dphidm_num(q.v, q.e, -d.coslam, -q.S)) * inv;
 }
 
 // h_I, h_II of one sample: FP64 outputs, or FP32 ones (rows of an FP32 FFT)

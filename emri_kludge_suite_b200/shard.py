@@ -27,10 +27,7 @@ from ._lib import check, lib, params_array, ptr  # noqa: F401
 
 
 def _bind():
-    L = lib()
-    L.aak_lpt_partition.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int64, ctypes.c_int32,
-                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double)]
-    return L
+    return lib()
 
 
 def source_costs(params, nmodes=None) -> np.ndarray:

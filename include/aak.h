@@ -453,6 +453,20 @@ int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m);
 int aak_ctx_set_parmap_device(aak_ctx *ctx, int32_t on);
 int aak_gpu_set_parmap_device(aak_gpu *g, int32_t on);
 
+/* Coarse AK evolution of a batch on the GPU: planning runs in three passes
+ * (front end, map and fit window on host threads; every source's AK
+ * recurrence beyond the fit window in one launch, one GPU thread per source;
+ * fitted knots and plunge search on host threads) instead of the host's
+ * grouped recurrences (AAK.cc:62-144 is the reference's serial loop).  The
+ * device rounds as the host does except in log(), so knots agree to about
+ * 1e-15 relative rather than bit for bit.  on = 0 (default): host.  Not for
+ * host-only contexts.  No reference counterpart. */
+int aak_ctx_set_evolve_device(aak_ctx *ctx, int32_t on);
+/* Wall times of the last plan with the device evolution, in ms: the host
+ * pass before it, the device pass (copies included), the host pass after it,
+ * and the total.  Zero for plans without it. */
+int aak_batch_plan_ms(aak_ctx *ctx, double *ms4);
+
 /* ---------------------------------------------------------------- several devices
  * Split of one batch over `parts` devices (or ranks): the reference's
  * pyGPUAAK accepts an ndevices argument and evaluates every template on one
