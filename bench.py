@@ -1195,8 +1195,8 @@ def main():
     ap.add_argument("--likelihood", type=int, default=4096, help="config-4 templates to time (0: skip)")
     ap.add_argument("--config2-sources", type=int, default=512,
                     help="sources of the configuration-2 accuracy check (0: skip)")
-    ap.add_argument("--plain-sources", type=int, default=16,
-                    help="sources of the plain FP64 per-source baseline (0: skip)")
+    ap.add_argument("--plain-sources", type=int, default=512,
+                    help="sources of the plain FP64 per-source baseline (0: skip; default: the whole batch)")
     ap.add_argument("--fisher", type=int, default=8, help="Fisher matrices to time at config-4 points (0: skip)")
     ap.add_argument("--tdi", type=int, default=1, help="time the frequency-domain TDI of 16 sources (0: skip)")
     ap.add_argument("--phases", type=int, default=1, help="time the AAK phase product of the batch (0: skip)")
