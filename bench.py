@@ -518,6 +518,16 @@ def run_likelihood(n_templates: int, local_rank: int, model=None, n_fisher: int 
     f32["max_abs_dlogL_vs_fp64"] = float(np.max(np.abs(logl32 - logl64)[ok32])) if ok32.any() else None
     f32["median_abs_dlogL_vs_fp64"] = float(np.median(np.abs(logl32 - logl64)[ok32])) if ok32.any() else None
     res["split_fp32_fft"] = f32
+    # the same without the warm start: the start's tensor-core inference waits
+    # for the persistent waveform kernel of the previous batch, which holds
+    # every SM, so the warm start lengthens the pipelined host planning
+    g.set_precision(2)
+    o32n, s32n, f32n = timed()
+    g.set_precision(0)
+    okn = (st64 == 0) & (s32n == 0)
+    f32n["max_abs_dlogL_vs_fp64"] = float(np.max(np.abs(-0.5 * (d_d + o32n[:, 1] - 2.0 * o32n[:, 0]) - logl64)[okn])) \
+        if okn.any() else None
+    res["split_fp32_fft_no_warm_start"] = f32n
     # HBM roofline of the inner-product kernel.  Each template's spectra of
     # both channels stream from HBM once; the data and weights (77 MB in FP64,
     # 38 MB in FP32) stay in the 126 MB L2 across the templates of a batch, so
@@ -715,7 +725,8 @@ def run_gpu(args, rank, world, local_rank):
     if world > 1:
         rng = np.random.default_rng([SEED, rank])  # redraws (rare) stay on their rank
     wb = E.WaveBatch(local_rank)
-    nthreads = os.cpu_count() or 1
+    # the host cores are shared by the ranks of one node
+    nthreads = max(1, (os.cpu_count() or 1) // world)
     t_plan0 = time.perf_counter()
     for _ in range(8):  # redraw sources that fail or plunge inside T
         wb.plan(sources, nmodes=NMODES, nthreads=nthreads)
@@ -889,6 +900,7 @@ def run_gpu(args, rank, world, local_rank):
                  "speedup_batched_split": value / sps}
         del pI, pII, traj
         wp.close()
+        torch.cuda.empty_cache()  # the plain path's 77 GB of buffers go back before configuration 2
 
     # ---- configuration 2: split precision vs FP64 per source at high eccentricity,
     #      mismatch flat and weighted by the LISA noise PSD
@@ -1210,6 +1222,13 @@ def main():
     if args.profile:
         PROFILES[args.profile]()
         return 0
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        # several ranks share one node's host cores: the multi-GPU line keeps the
+        # headline, the end-to-end step and the likelihoods; the single-GPU
+        # extras (plain path, configuration 2, phase product, TDI, Fisher,
+        # planning comparison) run at N = 1
+        args.plain_sources = args.config2_sources = args.fisher = args.tdi = args.phases = 0
+        args.evolve_compare = 0
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -320,14 +320,14 @@ __device__ __forceinline__ void dd_add_dd(double &hi, double &lo, double bh, dou
 }
 
 // Publish tile g's aggregate or inclusive record (one thread): the fields go
-// to L2 (st.cg) before the flag is released.
+// to L2 (st.cg), then the flag's st.release.gpu orders them before it (a reader
+// loads the flag with ld.acquire.gpu before the fields), so no separate fence.
 __device__ __forceinline__ void publish_aggregate(const BatchView &bv, int64_t g, const double x[3], double C, bool hasC) {
   TileLink *L = bv.link + g;
 #pragma unroll
   for (int q = 0; q < 3; ++q) __stcg(&L->agg[q], x[q]);
   __stcg(&L->agg_C, C);
   __stcg(&L->agg_hasC, hasC ? 1 : 0);
-  __threadfence();
   st_release(bv.link_flag + g, 1);
 }
 __device__ __forceinline__ void publish_inclusive(const BatchView &bv, int64_t g, const double fh[3], const double fl[3],
@@ -341,7 +341,6 @@ __device__ __forceinline__ void publish_inclusive(const BatchView &bv, int64_t g
     __stcg(&L->inc_b_lo[q], bl[q]);
   }
   __stcg(&L->inc_C, C);
-  __threadfence();
   st_release(bv.link_flag + g, 2);
 }
 
@@ -829,7 +828,9 @@ template <typename T>
 __device__ __forceinline__ void double_angle(T y, T x, T &c2, T &s2) {
   const T r2 = x * x + y * y;
   if (r2 > T(0)) {
-    const T inv = T(1) / r2;
+    T inv;  // FP32: the correctly rounded reciprocal, cheaper than a division
+    if constexpr (sizeof(T) == 4) inv = __frcp_rn(r2);
+    else inv = T(1) / r2;
     c2 = (x * x - y * y) * inv;
     s2 = T(2) * x * y * inv;
   } else {
@@ -941,8 +942,15 @@ __device__ __forceinline__ Resp<T> response(const Geom<T> &d, T ca, T sa, T c2g,
   const T S0 = (T)d.Sv[0], S1 = (T)d.Sv[1], S2 = (T)d.Sv[2];
   const T nS0 = (T)d.nxS[0], nS1 = (T)d.nxS[1], nS2 = (T)d.nxS[2];
   const T norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * (T)d.nxS_norm;
-  const T cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
-  const T sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
+  T cosrot, sinrot;
+  if constexpr (sizeof(T) == 4) {
+    const T rn = __frcp_rn(norm);
+    cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) * rn;
+    sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) * rn;
+  } else {
+    cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
+    sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
+  }
   const T r0 = T(2) * cosrot * cosrot - T(1), r1 = cosrot * sinrot;
   const T uI = FplusI * r0 - FcrosI * r1, wI = FplusI * r1 + FcrosI * r0;
   const T uII = FplusII * r0 - FcrosII * r1, wII = FplusII * r1 + FcrosII * r0;
@@ -1002,7 +1010,7 @@ __device__ __forceinline__ SamplePrep<float> prep_split(const SourceDesc &d, con
   float sa, ca, s2g, c2g, so = 0.f, co = 1.f;
   __sincosf(reduce_2pi_f(alp), &sa, &ca);
   __sincosf(reduce_2pi_f(2.0 * gim), &s2g, &c2g);
-  if (d.mich) __sincosf(reduce_2pi_f(kTwoPi * t / kYear), &so, &co);
+  if (d.mich) __sincosf(reduce_2pi_f(t * (kTwoPi / kYear)), &so, &co);  // a product, not a division, in FP64
   P.R = response<float>(g, ca, sa, c2g, s2g, co, so);
   P.Amp = exp2f((2.f / 3.f) * __log2f((float)om_M)) * g.zeta;
   double D1 = 0.0;
@@ -1189,9 +1197,12 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     }
     __syncthreads();
   }
+  // Work queue: the first tile is fetched here, every later one during the
+  // tile before it (before that tile's last barrier), so that the atomic's
+  // round trip overlaps the tile's work.
+  if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
+  __syncthreads();
   for (;;) {
-    if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
-    __syncthreads();
     const long long j = s_tile;
     __syncthreads();
     if (j >= bv.total_tiles) break;
@@ -1218,7 +1229,9 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
       if (tid == 0) {
         const double zero[3] = {0.0, 0.0, 0.0};
         publish_aggregate(bv, g, zero, 0.0, false);
+        s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
       }
+      __syncthreads();
       continue;
     }
     KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
@@ -1363,7 +1376,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     //     phase slots until (C)
     const double Pin = (s_rb[1] > 0.0) ? s_rb[1] : Cin;  // clamped Phidot just before the tile
     int nonpos = 0;                                      // a forward sample whose raw Phidot is not positive
-#pragma unroll 2
+#pragma unroll 1
     for (int ch = 0; ch < kTileChunks; ++ch) {
       const int sl = ch * kTileThreads + tid;
       const int i = c.start + sl;
@@ -1564,6 +1577,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
       }
 #endif
+    if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);  // the next tile, read after the loop's barrier
     __syncthreads();
     // the phases of this thread's own samples: X0 + carry + local part
     // (forward), X0 - (carry + increments after the sample) (backward)
