@@ -694,13 +694,13 @@ def run_phases(args, wb, sources, sptr, stream, N, N_all, reduce_max, local_rank
                     "of the configuration-1 batch",
         "value": N_all / (ms * 1e-3), "unit": "samples/s", "ms_per_step": ms,
         "kernel_ms": {"clears": kern[0], "phase_and_freeze": kern[2]},
-        "roofline": {"kernel": "k_waveform<fp64, phase> + k_phase_freeze", "bound": "hbm", "achieved": gbs,
+        "roofline": {"kernel": "k_tile_params + k_waveform<fp64, phase> + k_phase_freeze", "bound": "hbm", "achieved": gbs,
                      "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "peak_source": hbm_src,
                      "bytes_per_sample": bytes_per_sample},
         "e2e": {"value": Np / e2e_s, "unit": "samples/s", "seconds_per_step": e2e_s, "sources": len(sub),
                 "samples": Np, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": 64 * Np, "host_threads": nthreads},
-        "gpu_launches_per_step": 2,
+        "gpu_launches_per_step": 3,  # k_tile_params, k_waveform<fp64, phase>, k_phase_freeze
     }
 
 

@@ -877,10 +877,15 @@ int run_phase(aak_ctx *ctx, double *out, int64_t stride, cudaStream_t st) {
   bv.phase_out = out;
   bv.phase_stride = stride;
   bv.trajectory_only = 1;
+  // the tile pre-pass's parameters (no tables in the phase product)
+  const void *p0 = ctx->d_tile_prep.ptr;
+  if ((r = ctx->d_tile_prep.reserve(std::max<int64_t>(ctx->total_tiles, 1))) != AAK_OK) return r;
+  if (ctx->d_tile_prep.ptr != p0) drop_graph(ctx);
+  bv.tile_prep = ctx->d_tile_prep.ptr;
   if (ctx->profile && !ctx->ev[0])
     for (auto &e : ctx->ev) cudaEventCreate(&e);
   launch_phase(bv, ctx->num_sms, st, ctx->profile ? ctx->ev : nullptr);
-  ctx->last_launches = 2;
+  ctx->last_launches = 3;
   return cuda_ok(cudaGetLastError());
 }
 

@@ -1070,16 +1070,15 @@ __global__ void __launch_bounds__(128) k_tile_params(BatchView bv) {
   const int lt = (int)(g - bv.tile_start[s]);
   const int start = lt * kTileSamples, end = min(start + kTileSamples, d.vlength);
   const int lim = min(end, n_eff(d));
-  if (d.status == 0 && lim > start) {
-    KnotWin w{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0};
+  // the rates either side of every tile (the phase product uses the tiles
+  // after the taper as well); the table parameters of tiles with output
+  KnotWin w{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0, 0};
+  if (d.status == 0 && end > start) {
     w.k0 = bv.tile_knot[2 * g];
     w.n = bv.tile_knot[2 * g + 1];
     const double *kt = bv.knot_t + d.knot_offset;
     const double span = kt[w.k0 + w.n - 1] - kt[w.k0];
     w.inv_h = (span > 0.0) ? (double)(w.n - 1) / span : 0.0;
-    const double e0 = spline4w(bv, d, sample_time(d, start), w).e;
-    const double em = spline4w(bv, d, sample_time(d, (start + lim - 1) / 2), w).e;
-    const double e1 = spline4w(bv, d, sample_time(d, lim - 1), w).e;
     {
       double r[3] = {0, 0, 0};
       const int i = start - 1;
@@ -1096,6 +1095,11 @@ __global__ void __launch_bounds__(128) k_tile_params(BatchView bv) {
       P.ra[1] = r[1];
       P.ra[2] = r[2];
     }
+  }
+  if (d.status == 0 && lim > start) {  // lim <= end: the window above is set
+    const double e0 = spline4w(bv, d, sample_time(d, start), w).e;
+    const double em = spline4w(bv, d, sample_time(d, (start + lim - 1) / 2), w).e;
+    const double e1 = spline4w(bv, d, sample_time(d, lim - 1), w).e;
     int K = 0;
     double ec = 0.0;
     if (d.nmodes <= kTabModes) {
@@ -1170,7 +1174,7 @@ static_assert(sizeof(SourceDesc) % 16 == 0, "SourceDesc lands in shared memory w
 template <bool kSplit, int kMode = 0, bool kPre = false, int kJointT = 0, int kMinB = AAK_WAVE_MIN_BLOCKS>
 __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) {
   constexpr bool kPhase = kMode != 0, kTdi = kMode == 2;
-  static_assert(!kPre || kMode == 0, "the pre-pass serves the waveform mode");
+  static_assert(!kPre || kMode != 2, "the pre-pass serves the waveform and phase modes");
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
   __shared__ double red[3][kTileThreads / 32];
   __shared__ long long s_tile;
@@ -1259,7 +1263,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
           bulk_copy_g2s(s_wy, bv.knot_y + off, (uint32_t)(nk * sizeof(double4)), &s_mbar[0]);
           bulk_copy_g2s(s_wc, bv.knot_c + off, (uint32_t)(nk * sizeof(double4)), &s_mbar[0]);
         }
-        const bool tab = Kt > 0 && nm <= kTabModes;
+        const bool tab = !kPhase && Kt > 0 && nm <= kTabModes;
         if (tab) {
           const uint32_t b1 = (uint32_t)nm * (uint32_t)st * (uint32_t)sizeof(TT);
           mbar_arrive_expect_tx(&s_mbar[1], b1);
@@ -1939,6 +1943,8 @@ void prepare_dense_launch() {
     set_variant_smem<true>(most, std::make_index_sequence<kNumVariants>{});
     set_variant_smem<false>(most, std::make_index_sequence<kNumVariants>{});
     cudaFuncSetAttribute(k_waveform<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
+    cudaFuncSetAttribute(k_waveform<false, 1, true, 0, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kWaveDynSmem);
     cudaFuncSetAttribute(k_waveform<false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWaveDynSmem);
     attrs_set.fetch_or(bit);
   }
@@ -2032,11 +2038,13 @@ void launch_phase(const BatchView &bv, int num_sms, cudaStream_t stream, cudaEve
     cudaEventRecord(ev[2], stream);
   }
   prepare_dense_launch();
-  int resident = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_waveform<false, 1>, kTileThreads, kWaveDynSmem);
-  resident = std::max(resident, 1);
-  const int grid = (int)std::min<int64_t>(bv.total_tiles, (int64_t)num_sms * resident);
-  k_waveform<false, 1><<<grid, kTileThreads, kWaveDynSmem, stream>>>(bv);
+  if (bv.tile_prep) {
+    // the tile parameters from the pre-pass, each tile's inputs staged by bulk copies
+    k_tile_params<false><<<(unsigned)((bv.total_tiles + 127) / 128), 128, 0, stream>>>(bv);
+    launch_persistent(k_waveform<false, 1, true, 0, 3>, bv, num_sms, kWaveDynSmem, stream);
+  } else {
+    launch_persistent(k_waveform<false, 1>, bv, num_sms, kWaveDynSmem, stream);
+  }
   const dim3 fgrid(64, (unsigned)std::min(std::max(bv.nsrc, 1), 1024));
   k_phase_freeze<<<fgrid, 256, 0, stream>>>(bv.src, bv.nsrc, bv.phase_out, bv.phase_stride);
   if (ev) cudaEventRecord(ev[3], stream);

@@ -177,7 +177,8 @@ int aak_batch_run(aak_ctx *ctx, double *d_hI, double *d_hII, double *d_t, double
  * into caller device memory: 8 rows of `stride` doubles (stride >= the
  * batch's total samples) -- t, phase_r, phase_theta, phase_phi, omega_r,
  * omega_theta, omega_phi, eccentricity -- each indexed by the batch offsets.
- * Batched counterpart of AAKphase (src/suite/AAKpy.cc:53-88); two kernels. */
+ * Batched counterpart of AAKphase (src/suite/AAKpy.cc:53-88); three kernels
+ * (per-tile parameters, the phase pass, the post-plunge freeze). */
 int aak_batch_run_phase(aak_ctx *ctx, double *d_out, int64_t stride, void *stream);
 
 /* Plan + upload + phase product + copy back for nsrc sources: h_out holds
@@ -207,7 +208,9 @@ int aak_tdi_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t 
  * 4,849,920 bytes (about 4.9 MB) held by every GPU that loads the library
  * until exit; batches above 32768 tiles of 1024 samples (33,554,432 samples)
  * are rejected with AAK_ERR_CAPACITY.  The first call on a device looks the
- * array's address up; make that call before any stream capture.  Every call
+ * array's address up; make that call before any stream capture.  The address
+ * is kept for the life of the process: after a cudaDeviceReset of that device
+ * it is stale, so do not call this entry point after resetting the device.  Every call
  * shares the array: calls that overlap on the GPU race.  Each call clears its
  * own look-back status word before its kernel, so a wait that gave up in an
  * earlier call does not affect it; a give-up is kept in a report word that
@@ -218,7 +221,8 @@ int aak_tdi_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t 
 int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_t *required_bytes, double *d_hI,
                           double *d_hII, void *stream);
 
-/* Number of CUDA kernels the last aak_batch_run launched. */
+/* Number of CUDA kernels the last aak_batch_run (or aak_batch_run_phase)
+ * launched. */
 int aak_batch_last_launches(aak_ctx *ctx);
 
 /* Waits for the device, then reports whether a bounded device-side wait of

@@ -34,7 +34,7 @@ def _run_phase(params, mapped=None):
     wb.upload()
     wb.run_phase(out.data_ptr(), N)
     torch.cuda.synchronize()
-    assert wb.launches() == 2
+    assert wb.launches() == 3  # tile parameters, phase pass, freeze
     assert wb.device_status() == 0
     return out.cpu().numpy(), wb
 
