@@ -15,7 +15,6 @@
 #include <math.h>
 
 #include <atomic>
-#include <mutex>
 #include <type_traits>
 #include <utility>
 
@@ -2439,8 +2438,21 @@ static __device__ __align__(256) unsigned char g_tile_scratch[kStaticScratchByte
 constexpr size_t kStaticStatusOffset = kStaticCounterOffset + sizeof(unsigned long long);
 constexpr size_t kStaticReportOffset = kStaticStatusOffset + sizeof(unsigned int);
 
-std::mutex g_scratch_mu;
-void *g_scratch_addr[kMaxStaticDevices] = {nullptr};
+// devices on which an allocation-free launch has run (their report word is live)
+std::atomic<bool> g_scratch_used[kMaxStaticDevices];
+
+// The array's device address in the current context (the caller has made the
+// device current).  Looked up on every call: the lookup allocates nothing,
+// and a cached address would be stale after a cudaDeviceReset or in another
+// context of the same device.
+void *static_scratch_base() {
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_tile_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
 }  // namespace
 
 namespace {
@@ -2480,12 +2492,9 @@ int lookback_timeout_selftest(long long cycles, cudaStream_t stream) {
 
 int static_scratch_status(int device, bool clear) {
   if (device < 0 || device >= kMaxStaticDevices) return 0;
-  void *base = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    base = g_scratch_addr[device];
-  }
-  if (!base) return 0;  // no allocation-free launch on this device yet
+  if (!g_scratch_used[device].load()) return 0;  // no allocation-free launch on this device yet
+  void *base = static_scratch_base();
+  if (!base) return -1;
   unsigned int *word = reinterpret_cast<unsigned int *>(static_cast<unsigned char *>(base) + kStaticReportOffset);
   unsigned int v = 0;
   if (cudaMemcpy(&v, word, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
@@ -2496,21 +2505,9 @@ int static_scratch_status(int device, bool clear) {
 int launch_dense_static_scratch(BatchView bv, int device, int num_sms, cudaStream_t stream, int precision) {
   if (bv.total_tiles > kStaticScratchTiles) return 8;  // AAK_ERR_CAPACITY
   if (device < 0 || device >= kMaxStaticDevices || (precision != 0 && precision != 1)) return 1;
-  void *base = nullptr;
-  {
-    // host code needs the device address of the array: look it up once per
-    // device, with that device current (the caller has selected it)
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_addr[device]) {
-      void *p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_tile_scratch) != cudaSuccess || !p) {
-        cudaGetLastError();
-        return 5;  // AAK_ERR_CUDA
-      }
-      g_scratch_addr[device] = p;
-    }
-    base = g_scratch_addr[device];
-  }
+  void *base = static_scratch_base();
+  if (!base) return 5;  // AAK_ERR_CUDA
+  g_scratch_used[device].store(true);
   unsigned char *b = static_cast<unsigned char *>(base);
   bv.link = reinterpret_cast<TileLink *>(b);
   bv.link_flag = reinterpret_cast<int32_t *>(b + kStaticFlagOffset);
