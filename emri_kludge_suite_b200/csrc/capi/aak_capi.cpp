@@ -263,18 +263,25 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
     d.n_tiles = (int32_t)(ctx->tile_start[s + 1] - ctx->tile_start[s]);
     ctx->descs[s] = d;
     if (ctx->status[s] != AAK_OK) return;
-    // knot window of every tile: knots bracketing samples start-1 .. start+1024
+    // knot window of every tile: knots bracketing samples start-1 .. start+1024.
+    // k0 is the last knot in [k0, nk - 2] with kt[k0] <= ta (kept at least at
+    // its previous value), k1 the same for tb; found by binary search, so the
+    // cost follows the tiles, not the knots (sources may have thousands of
+    // knots per tile)
     const double *kt = pl.knot_t.data();
     const int nk = d.n_knots;
     auto tsample = [&](int i) { return (i == 0) ? d.t_first : (double)(i - d.i0) * d.dt; };
+    auto last_le = [&](int lo, double x) {  // largest k in [lo, nk - 2] with kt[k] <= x, else lo
+      if (lo + 1 > nk - 2) return lo;
+      return (int)(std::upper_bound(kt + lo + 1, kt + nk - 1, x) - kt) - 1;
+    };
     int k0 = 0, k1 = 0;
     for (int64_t t = 0; t < d.n_tiles; ++t) {
       const int start = (int)(t * kTileSamples);
       const double ta = tsample(std::max(start - 1, 0));
       const double tb = tsample(std::min(start + kTileSamples, d.vlength - 1));
-      while (k0 + 1 <= nk - 2 && kt[k0 + 1] <= ta) ++k0;
-      k1 = std::max(k1, k0);
-      while (k1 + 1 <= nk - 2 && kt[k1 + 1] <= tb) ++k1;
+      k0 = last_le(k0, ta);
+      k1 = last_le(std::max(k1, k0), tb);
       ctx->tile_knot[2 * (d.tile_offset + t)] = k0;
       ctx->tile_knot[2 * (d.tile_offset + t) + 1] = k1 + 2 - k0;
     }
@@ -351,7 +358,7 @@ void finish_source(aak_ctx *ctx, int s, const Params &Pp, const MappedTrajectory
 // on_done(s), if set, is called on the worker thread right after source s is
 // planned (its plan and status final from then on).
 int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapped *maps, const int32_t *nm,
-                 int32_t nthreads, const std::function<void(int)> &on_done, bool early_small = false) {
+                 int32_t nthreads, const std::function<void(int)> &on_done, bool stream_order = false) {
   const int32_t nsrc = (int32_t)Pv.size();
   // worker threads page-lock knot arrays: make this context's device theirs
   // (a new thread starts on device 0, where it would otherwise open a context)
@@ -477,6 +484,9 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
   // behind one long source at the end.
   std::vector<int> order(nsrc);
   int nbig = 0;  // the leading sources of order that run alone (the rest in groups)
+  int64_t ntasks = 0;
+  std::vector<int64_t> task_order;  // the order in which threads take the tasks
+  const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
   {
     std::vector<double> cost(nsrc, 0.0);
     for (int s = 0; s < nsrc; ++s) {
@@ -491,17 +501,52 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     // the shortest latency per step.  The others are planned kPlanGroup at a
     // time, neighbours in cost, their recurrences run together in vector
     // lanes (the same results, at a fraction of the cost per source).
-    // Streaming takes the others smallest first, so that finished sources
-    // start flowing to the device early while the long ones are being planned.
     double total = 0.0;
     for (double c : cost) total += c;
-    const int threads = nthreads > 0 ? nthreads : (int)std::max(1u, std::thread::hardware_concurrency());
     const double big = total / threads / 4.0;
     const auto split = std::find_if(order.begin(), order.end(), [&](int s) { return cost[s] <= big; });
     nbig = (int)(split - order.begin());
-    if (early_small) std::reverse(split, order.end());
+    ntasks = nbig + (nsrc - nbig + kPlanGroup - 1) / kPlanGroup;
+    task_order.resize(ntasks);
+    for (int64_t t = 0; t < ntasks; ++t) task_order[t] = t;
+    if (stream_order && ntasks > threads) {
+      // Streaming: cheap tasks, whose sources carry many samples per unit
+      // of planning time, should finish early (their waveforms start the
+      // device work and the copies back) without the long tasks ending
+      // late.  The order comes from list scheduling simulated on estimated
+      // task times: a free thread takes the costliest task left when it is
+      // a big source or would otherwise end after kSlack of the makespan
+      // bound (total / threads), else the cheapest task left.  Estimated
+      // time of a task, in cost units: its sources' costs (x kLaneShare in
+      // vector lanes) plus kSourceFixed per source for the front end; both
+      // constants were fitted to measured task times on a 16-core host, and
+      // kSlack = 0.75 was the most robust to 15 % estimate errors in
+      // simulation of the 512-source benchmark batch.
+      constexpr double kSlack = 0.75, kLaneShare = 0.54, kSourceFixed = 270.0;
+      std::vector<double> est(ntasks);
+      for (int64_t t = 0; t < ntasks; ++t) {
+        const int64_t k = (t < nbig) ? t : nbig + kPlanGroup * (t - nbig);
+        const int n = (t < nbig) ? 1 : (int)std::min<int64_t>(kPlanGroup, nsrc - k);
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += cost[order[k + i]];
+        est[t] = (t < nbig ? c : kLaneShare * c) + kSourceFixed * n;
+      }
+      std::vector<int64_t> desc(ntasks);
+      for (int64_t t = 0; t < ntasks; ++t) desc[t] = t;
+      std::stable_sort(desc.begin(), desc.end(), [&](int64_t a, int64_t b) { return est[a] > est[b]; });
+      double sum = 0.0;
+      for (double x : est) sum += x;
+      const double bound = kSlack * sum / threads;
+      std::vector<double> busy(threads, 0.0);
+      int64_t hi = 0, lo = ntasks - 1, q = 0;
+      while (hi <= lo) {
+        const int p = (int)(std::min_element(busy.begin(), busy.end()) - busy.begin());
+        const int64_t t = (desc[hi] < nbig || busy[p] + est[desc[hi]] >= bound) ? desc[hi++] : desc[lo--];
+        task_order[q++] = t;
+        busy[p] += est[t];
+      }
+    }
   }
-  const int64_t ntasks = nbig + (nsrc - nbig + kPlanGroup - 1) / kPlanGroup;
   std::atomic<int64_t> points(0), iters(0), fallbacks(0);
   auto map_one = [&](int s, const Params &Pp, MappedTrajectory *mt) {
     if (fused) {
@@ -648,8 +693,9 @@ int plan_sources(aak_ctx *ctx, const std::vector<aak_params> &Pv, const aak_mapp
     ctx->newton_fallbacks = fallbacks;
     return AAK_OK;
   }
-  parallel_for(ntasks, nthreads, [&](int64_t t) {
+  parallel_for(ntasks, nthreads, [&](int64_t q) {
     on_device();
+    const int64_t t = task_order[q];
     const int64_t k = (t < nbig) ? t : nbig + kPlanGroup * (t - nbig);
     const int n = (t < nbig) ? 1 : (int)std::min<int64_t>(kPlanGroup, nsrc - k);
     int idx[kPlanGroup], st[kPlanGroup];
@@ -683,7 +729,10 @@ int plan_common(aak_ctx *ctx, const aak_params *P, const aak_mapped *maps, int32
   return pack(ctx, Pv, nthreads);
 }
 
-int upload(aak_ctx *ctx, cudaStream_t st) {
+// wait_pinned: finish the copies from page-locked plan arrays before
+// returning (callers whose next plan may refill those arrays); a caller that
+// keeps the plans untouched until it synchronises the stream passes false.
+int upload(aak_ctx *ctx, cudaStream_t st, bool wait_pinned = true) {
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
   const int n = ctx->nsrc;
@@ -727,7 +776,7 @@ int upload(aak_ctx *ctx, cudaStream_t st) {
   if ((r = cuda_ok(cudaGetLastError())) != AAK_OK) return r;
   // copies from page-locked memory run asynchronously: finish them before the
   // host arrays can be refilled by the next plan
-  if (ctx->want_pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
+  if (wait_pinned && ctx->want_pinned && (r = cuda_ok(cudaStreamSynchronize(st))) != AAK_OK) return r;
   ctx->uploaded = true;
   ++ctx->upload_gen;
   return AAK_OK;
@@ -1198,8 +1247,8 @@ int tdi_batch(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t nthreads,
 }
 
 // aak_wave_batch_host for batches worth streaming.  Host threads plan the
-// sources (the few that bound the planning time first, then the rest smallest
-// first); as they finish, the calling thread gathers them in groups of about
+// sources (the few that bound the planning time first, the cheap ones early
+// wherever the long ones can wait: plan_sources' streaming order); as they finish, the calling thread gathers them in groups of about
 // nsrc / kStreamGroups (or takes what has finished when 10 ms pass without a
 // full group) and, on one of two auxiliary
 // contexts in turn, packs, uploads, generates and copies back each group on
@@ -1291,7 +1340,9 @@ int wave_batch_streamed(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const i
       Pg[i] = Pv[grp[i]];
     }
     rc = pack(A, Pg, 2);
-    if (rc == AAK_OK) rc = upload(A, A->pipe_stream);  // waits for its own copies
+    // the knot copies read the plans' page-locked arrays, which nothing
+    // refills before this call's streams are drained: no wait here
+    if (rc == AAK_OK) rc = upload(A, A->pipe_stream, false);
     for (int i = 0; i < k; ++i) std::swap(A->plans[i], ctx->plans[grp[i]]);
     if (rc != AAK_OK) break;
     const int64_t N = A->total_samples;
@@ -1310,6 +1361,9 @@ int wave_batch_streamed(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const i
     slot ^= 1;
   }
   planner.join();
+  // the whole batch's plan in this context (every plan is back), packed while
+  // the last groups' kernels and copies run
+  if (rc == AAK_OK) rc = pack(ctx, Pv, nthreads);
   for (int k = 0; k < 2; ++k)  // drain both streams whatever happened
     if (pending[k]) {
       const int e = cuda_ok(cudaStreamSynchronize(ctx->aux[k]->pipe_stream));
@@ -1318,7 +1372,7 @@ int wave_batch_streamed(aak_ctx *ctx, const aak_params *P, int32_t nsrc, const i
   if (rc != AAK_OK) return rc;
   for (int k = 0; k < 2; ++k)
     if ((r = device_status(ctx->aux[k])) != AAK_OK) return r;
-  return pack(ctx, Pv, nthreads);  // the whole batch's plan in this context
+  return AAK_OK;
 }
 
 }  // namespace
