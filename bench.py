@@ -32,6 +32,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import resource
 import time
 
 import numpy as np
@@ -704,6 +705,18 @@ def run_phases(args, wb, sources, sptr, stream, N, N_all, reduce_max, local_rank
     }
 
 
+def _mem_available_gb():
+    """MemAvailable of the host (Linux), in GB; None elsewhere."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return round(int(line.split()[1]) / 1e6, 1)
+    except OSError:
+        pass
+    return None
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
 
@@ -977,11 +990,12 @@ def run_gpu(args, rank, world, local_rank):
     st = np.zeros(len(sources), dtype=np.int32)
     nm = np.full(len(sources), NMODES, dtype=np.int32)
     h2d = 0
-    e2e_times = []
+    e2e_times, e2e_faults = [], []
     wb.set_precision(1)  # the headline path, through the host-buffer entry point
     for k in range(e2e_steps + 1):  # first call warms the host buffers
         if dist:
             dist.barrier()
+        f0 = resource.getrusage(resource.RUSAGE_SELF).ru_minflt
         t0 = time.perf_counter()
         _lib.check(L.aak_wave_batch_host(wb._ctx, P, len(sources), _lib.ptr(nm), nthreads,
                                          ctypes.cast(hIh.data_ptr(), ctypes.POINTER(ctypes.c_double)),
@@ -990,6 +1004,7 @@ def run_gpu(args, rank, world, local_rank):
         dt_e2e = time.perf_counter() - t0
         if k > 0:
             e2e_times.append(dt_e2e)
+            e2e_faults.append(resource.getrusage(resource.RUSAGE_SELF).ru_minflt - f0)
     e2e_s = float(np.mean(e2e_times))
     if dist:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
@@ -998,7 +1013,9 @@ def run_gpu(args, rank, world, local_rank):
     # plan bytes copied to the device per call (descriptors, knots, Bessel table)
     h2d = int(wb.plan_bytes())
     e2e = {"value": N_all / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": int(16 * N), "seconds_per_step": e2e_s, "host_threads": nthreads}
+           "d2h_bytes_per_step": int(16 * N), "seconds_per_step": e2e_s, "host_threads": nthreads,
+           "seconds_each": [round(x, 4) for x in e2e_times], "host_mem_available_gb": _mem_available_gb(),
+           "minor_page_faults_each": e2e_faults}
 
     # ---- roofline of the dominant kernel (split harmonic sum: FP32 mode sums, FP64 phases)
     wave_ms = kern_s[1] + kern_s[2]  # the harmonic sums' Bessel tables are built in the pre-pass
@@ -1201,7 +1218,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nsrc", type=int, default=512)
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--likelihood", type=int, default=4096, help="config-4 templates to time (0: skip)")

@@ -2024,6 +2024,15 @@ struct aak_gpu {
   // device work of the templates: its own non-blocking stream, so that host
   // planning (and the warm-start model's copies) can overlap it
   cudaStream_t stream = nullptr;
+  // likelihood batches in chunks, double-buffered: chunk c is planned into
+  // ctxs()[c & 1] and uploaded on up_stream while the chunk before it runs
+  aak_ctx *ctx2 = nullptr;
+  cudaStream_t up_stream = nullptr;
+  // per parity: upload done, generation done, generation start, transform
+  // done, reduction done, results copied
+  cudaEvent_t pev[2][6] = {{nullptr}};
+  double *h_stage = nullptr;  // page-locked results of the two chunks in flight (2 x 2 x stage_cap)
+  int stage_cap = 0;
 };
 
 namespace {
@@ -2099,18 +2108,23 @@ aak_params gpu_params(const aak_gpu *g, const double *x) {
 }
 
 // Host half of a batch of templates: plan them into the context's rows.
-int gpu_plan(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status) {
+// Plan B templates into context C (rows of g->row doubles); *ms: host time.
+int gpu_plan_into(aak_gpu *g, aak_ctx *C, const double *x, int B, int nthreads, int32_t *status, double *ms) {
   std::vector<aak_params> P(B);
   for (int k = 0; k < B; ++k) P[k] = gpu_params(g, x + 14 * (size_t)k);
   const auto t0 = std::chrono::steady_clock::now();
-  g->ctx->out_stride = g->row;
-  const int r = plan_common(g->ctx, P.data(), nullptr, B, nullptr, nthreads);
-  g->ctx->out_stride = 0;
-  g->ms[0] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  C->out_stride = g->row;
+  const int r = plan_common(C, P.data(), nullptr, B, nullptr, nthreads);
+  C->out_stride = 0;
+  *ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (r != AAK_OK) return r;
   for (int k = 0; k < B; ++k)
-    if (status) status[k] = g->ctx->status[k];
+    if (status) status[k] = C->status[k];
   return AAK_OK;
+}
+
+int gpu_plan(aak_gpu *g, const double *x, int B, int nthreads, int32_t *status) {
+  return gpu_plan_into(g, g->ctx, x, B, nthreads, status, &g->ms[0]);
 }
 
 // Device half: upload the planned batch and generate it into the rows
@@ -2186,15 +2200,9 @@ int gpu_fft_rows(aak_gpu *g) {
   return AAK_OK;
 }
 
-// FFT of the rows and the weighted inner products, queued on the
-// likelihood's stream; gpu_likelihood_finish copies the results back.
-int gpu_likelihood_launch(aak_gpu *g) {
-  if (g->count <= 0) return AAK_ERR_INVALID_PARAM;
-  if (!g->ev[0])
-    for (auto &e : g->ev) cudaEventCreate(&e);
-  int r0 = gpu_fft_rows(g);
-  if (r0 != AAK_OK) return r0;
-  cudaEventRecord(g->ev[2], g->stream);
+// The weighted inner products of the transformed rows into d_out, on the
+// likelihood's stream.
+int gpu_inner_products(aak_gpu *g) {
   if (g->rows32) {
     InnerProductArgs32 a;
     for (int ch = 0; ch < 2; ++ch) {
@@ -2208,7 +2216,6 @@ int gpu_likelihood_launch(aak_gpu *g) {
     a.partial = g->d_partial.ptr;
     a.out = g->d_out.ptr;
     launch_inner_products_f32(a, g->stream);
-    cudaEventRecord(g->ev[3], g->stream);
     return cuda_ok(cudaGetLastError());
   }
   InnerProductArgs a;
@@ -2224,8 +2231,101 @@ int gpu_likelihood_launch(aak_gpu *g) {
   a.partial = g->d_partial.ptr;
   a.out = g->d_out.ptr;
   launch_inner_products(a, g->stream);
-  cudaEventRecord(g->ev[3], g->stream);
   return cuda_ok(cudaGetLastError());
+}
+
+// FFT of the rows and the weighted inner products, queued on the
+// likelihood's stream; gpu_likelihood_finish copies the results back.
+int gpu_likelihood_launch(aak_gpu *g) {
+  if (g->count <= 0) return AAK_ERR_INVALID_PARAM;
+  if (!g->ev[0])
+    for (auto &e : g->ev) cudaEventCreate(&e);
+  int r0 = gpu_fft_rows(g);
+  if (r0 != AAK_OK) return r0;
+  cudaEventRecord(g->ev[2], g->stream);
+  if ((r0 = gpu_inner_products(g)) != AAK_OK) return r0;
+  cudaEventRecord(g->ev[3], g->stream);
+  return AAK_OK;
+}
+
+// ------------------------------------------------------------ pipelined likelihood batches
+// The second planning context, the upload stream, the events and the
+// page-locked result slots of aak_gpu_likelihood_batch (created on first use,
+// grown with max_batch); the second context takes the first one's settings.
+int gpu_pipeline_ready(aak_gpu *g, int max_batch) {
+  int r;
+  if (!g->ctx2 && (r = aak_ctx_create(g->ctx->device, &g->ctx2)) != AAK_OK) return r;
+  aak_ctx *a = g->ctx, *b = g->ctx2;
+  b->want_pinned = a->want_pinned;
+  b->parmap_device = a->parmap_device;
+  b->evolve_device = a->evolve_device;
+  b->model = a->model;
+  b->precision = a->precision;
+  b->lookback_cycles = a->lookback_cycles;
+  b->variant[0] = a->variant[0];
+  b->variant[1] = a->variant[1];
+  if (!g->up_stream && (r = cuda_ok(cudaStreamCreateWithFlags(&g->up_stream, cudaStreamNonBlocking))) != AAK_OK)
+    return r;
+  for (auto &row : g->pev)
+    for (auto &e : row)
+      if (!e && (r = cuda_ok(cudaEventCreate(&e))) != AAK_OK) return r;
+  if (g->stage_cap < max_batch) {
+    if (g->h_stage) cudaFreeHost(g->h_stage);
+    g->h_stage = nullptr;
+    g->stage_cap = 0;
+    if ((r = cuda_ok(cudaHostAlloc(reinterpret_cast<void **>(&g->h_stage), 4 * (size_t)max_batch * sizeof(double),
+                                   cudaHostAllocDefault))) != AAK_OK)
+      return r;
+    g->stage_cap = max_batch;
+  }
+  return AAK_OK;
+}
+
+// Chunk of B templates planned in C, result slot p: C's plan is uploaded on
+// up_stream (after the generation of the chunk two back, the last reader of
+// C's device buffers), then on the likelihood's stream the rows are
+// generated, transformed and reduced, and the results copied to slot p.
+int gpu_chunk_launch(aak_gpu *g, aak_ctx *C, int p, int B) {
+  cudaEvent_t *E = g->pev[p];
+  const bool r32 = g->precision == 2 && g->d_D32[0].ptr;
+  int r;
+  if ((r = r32 ? gpu_capacity32(g, B) : gpu_capacity(g, B)) != AAK_OK) return r;
+  if ((r = cuda_ok(cudaStreamWaitEvent(g->up_stream, E[1], 0))) != AAK_OK) return r;
+  if ((r = upload(C, g->up_stream, false)) != AAK_OK) return r;
+  if ((r = cuda_ok(cudaEventRecord(E[0], g->up_stream))) != AAK_OK ||
+      (r = cuda_ok(cudaStreamWaitEvent(g->stream, E[0], 0))) != AAK_OK)
+    return r;
+  cudaEventRecord(E[2], g->stream);
+  if (r32) r = run_rows32(C, g->d_H32[0].ptr, g->d_H32[1].ptr, 1, g->stream);
+  else r = run(C, g->d_H[0].ptr, g->d_H[1].ptr, nullptr, nullptr, 0, g->precision == 0 ? 0 : 1, g->stream);
+  if (r != AAK_OK) return r;
+  cudaEventRecord(E[1], g->stream);
+  g->count = B;
+  g->spectral = false;
+  g->rows32 = r32;
+  if ((r = gpu_fft_rows(g)) != AAK_OK) return r;
+  cudaEventRecord(E[3], g->stream);
+  if ((r = gpu_inner_products(g)) != AAK_OK) return r;
+  cudaEventRecord(E[4], g->stream);
+  if ((r = cuda_ok(cudaMemcpyAsync(g->h_stage + 2 * (size_t)g->stage_cap * p, g->d_out.ptr,
+                                   2 * (size_t)B * sizeof(double), cudaMemcpyDeviceToHost, g->stream))) != AAK_OK)
+    return r;
+  return cuda_ok(cudaEventRecord(E[5], g->stream));
+}
+
+// Wait for the chunk in slot p, copy its B results to out and add its device
+// times (generate, FFT, reduce) to ms[1..3].
+int gpu_chunk_collect(aak_gpu *g, int p, int B, double *out, double *ms) {
+  cudaEvent_t *E = g->pev[p];
+  const int r = cuda_ok(cudaEventSynchronize(E[5]));
+  if (r != AAK_OK) return r;
+  std::memcpy(out, g->h_stage + 2 * (size_t)g->stage_cap * p, 2 * (size_t)B * sizeof(double));
+  float f;
+  if (cudaEventElapsedTime(&f, E[2], E[1]) == cudaSuccess) ms[1] += f;
+  if (cudaEventElapsedTime(&f, E[1], E[3]) == cudaSuccess) ms[2] += f;
+  if (cudaEventElapsedTime(&f, E[3], E[4]) == cudaSuccess) ms[3] += f;
+  cudaGetLastError();
+  return AAK_OK;
 }
 
 int gpu_likelihood_finish(aak_gpu *g, double *out) {
@@ -2356,6 +2456,15 @@ void aak_gpu_destroy(aak_gpu *g) {
   g->d_t.release();
   for (auto &e : g->ev)
     if (e) cudaEventDestroy(e);
+  if (g->up_stream) {
+    cudaStreamSynchronize(g->up_stream);
+    cudaStreamDestroy(g->up_stream);
+  }
+  for (auto &row : g->pev)
+    for (auto &e : row)
+      if (e) cudaEventDestroy(e);
+  if (g->h_stage) cudaFreeHost(g->h_stage);
+  aak_ctx_destroy(g->ctx2);
   aak_ctx_destroy(g->ctx);
   delete g;
 }
@@ -2431,28 +2540,43 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   if (max_batch <= 0) max_batch = 256;
   double tot[4] = {0, 0, 0, 0};
   if (select_device(g->ctx->device) != AAK_OK) return AAK_ERR_CUDA;
-  // batch k + 1 is planned on the host while the device generates,
-  // transforms and reduces batch k (its upload has finished by then, so the
-  // plan arrays are free)
-  int r = gpu_plan(g, params, std::min<int32_t>(max_batch, nsrc), nthreads, status);
-  if (r != AAK_OK) return r;
-  for (int32_t k0 = 0; k0 < nsrc; k0 += max_batch) {
-    const int B = std::min<int32_t>(max_batch, nsrc - k0);
-    tot[0] += g->ms[0];
-    if ((r = gpu_launch(g, B, false, g->precision == 2 && g->d_D32[0].ptr)) != AAK_OK ||
-        (r = gpu_likelihood_launch(g)) != AAK_OK) {
-      cudaDeviceSynchronize();
-      return r;
+  int r;
+  if ((r = gpu_pipeline_ready(g, max_batch)) != AAK_OK) return r;
+  // Chunk c is planned into ctxs[c & 1]: while the device generates,
+  // transforms and reduces chunk c, the host plans chunk c + 1 into the other
+  // context (whose upload, of chunk c - 1, has finished reading its plan
+  // arrays) and then queues it, so that the device goes from one chunk to the
+  // next without waiting for the host; chunk c - 1's results are collected
+  // after that.
+  aak_ctx *ctxs[2] = {g->ctx, g->ctx2};
+  const int32_t nch = (nsrc + max_batch - 1) / max_batch;
+  auto chunk_size = [&](int32_t c) { return std::min<int32_t>(max_batch, nsrc - c * max_batch); };
+  auto fail = [&](int e) {
+    cudaStreamSynchronize(g->up_stream);
+    cudaStreamSynchronize(g->stream);
+    return e;
+  };
+  double ms = 0.0;
+  if ((r = gpu_plan_into(g, ctxs[0], params, chunk_size(0), nthreads, status, &ms)) != AAK_OK) return r;
+  tot[0] += ms;
+  for (int32_t c = 0; c < nch; ++c) {
+    const int p = c & 1;
+    if ((r = gpu_chunk_launch(g, ctxs[p], p, chunk_size(c))) != AAK_OK) return fail(r);
+    if (c + 1 < nch) {
+      const int64_t k1 = (int64_t)(c + 1) * max_batch;
+      if ((r = cuda_ok(cudaEventSynchronize(g->pev[1 - p][0]))) != AAK_OK) return fail(r);
+      if ((r = gpu_plan_into(g, ctxs[1 - p], params + 14 * k1, chunk_size(c + 1), nthreads,
+                             status ? status + k1 : nullptr, &ms)) != AAK_OK)
+        return fail(r);
+      tot[0] += ms;
     }
-    const int32_t k1 = k0 + max_batch;
-    int rp = AAK_OK;
-    if (k1 < nsrc)
-      rp = gpu_plan(g, params + 14 * (size_t)k1, std::min<int32_t>(max_batch, nsrc - k1), nthreads,
-                    status ? status + k1 : nullptr);
-    if ((r = gpu_likelihood_finish(g, out + 2 * (size_t)k0)) != AAK_OK) return r;
-    if (rp != AAK_OK) return rp;
-    for (int q = 1; q < 4; ++q) tot[q] += g->ms[q];
+    if (c > 0 && (r = gpu_chunk_collect(g, 1 - p, chunk_size(c - 1), out + 2 * (int64_t)(c - 1) * max_batch, tot)) !=
+                     AAK_OK)
+      return fail(r);
   }
+  if ((r = gpu_chunk_collect(g, (nch - 1) & 1, chunk_size(nch - 1), out + 2 * (int64_t)(nch - 1) * max_batch, tot)) !=
+      AAK_OK)
+    return fail(r);
   for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
   return AAK_OK;
 }
