@@ -788,9 +788,10 @@ def run_gpu(args, rank, world, local_rank):
     for prec, name in ((0, "fp64"), (1, "split")):
         v, ms_v = wb.autotune(hI.data_ptr(), hII.data_ptr(), precision=prec)
         tune[name] = {"choice": v, "ms_per_variant": ms_v}
-    tune["variants"] = ["pre-pass, joint 2 (split) / 1 (FP64), 2 CTAs/SM", "tables inside the tiles, 2 CTAs/SM",
-                        "pre-pass, joint 1 / 2, 2 CTAs/SM", "pre-pass, joint 4, 2 CTAs/SM",
-                        "pre-pass, joint 2 / 1, 3 CTAs/SM", "pre-pass, joint 1 / 2, 3 CTAs/SM"]
+    tune["variants"] = ["pre-pass, joint 1, 3 CTAs/SM", "tables inside the tiles, 2 CTAs/SM",
+                        "pre-pass, joint 1 (split) / 2 (FP64), 2 CTAs/SM", "pre-pass, joint 4, 2 CTAs/SM",
+                        "pre-pass, joint 2 / 1, 3 CTAs/SM (split) / 2 CTAs/SM (FP64)",
+                        "pre-pass, joint 2, 2 CTAs/SM (split) / 3 CTAs/SM (FP64)"]
 
     # ---- plain FP64 batched path (precision 0): per-kernel times
     for _ in range(args.warmup):
@@ -1095,10 +1096,11 @@ def run_gpu(args, rank, world, local_rank):
 #   python bench.py --profile likelihood # 32 config-4 templates, FP64 and FP32 transform + products
 def profile_waveform():
     """16 of the 512 configuration-1 sources (every 32nd; 28,332,971 samples,
-    n = 1..30): per precision the default launch shape and the one the
-    autotuner picks on the full batch (FP64: 3 CTAs/SM; split: 1 sample per
-    thread, 3 CTAs/SM), twice each, in the order FP64 v0, FP64 v4, split v0,
-    split v5 (16 B/sample of outputs: 453 MB, above the 126 MB L2)."""
+    n = 1..30): per precision the earlier default launch shape (FP64: 2
+    CTAs/SM; split: 2 samples per thread, 2 CTAs/SM) and the autotuner's
+    choice on the full batch (pre-pass, 1 sample per thread, 3 CTAs/SM: shape
+    0, the default now), twice each, in the order FP64 v4, FP64 v0, split v5,
+    split v0 (16 B/sample of outputs: 453 MB, above the 126 MB L2)."""
     import torch
 
     from emri_kludge_suite_b200.aak import WaveBatch
@@ -1110,7 +1112,7 @@ def profile_waveform():
     n = wb.total_samples
     hI = torch.empty(n, dtype=torch.float64, device="cuda")
     hII = torch.empty_like(hI)
-    for precision, variant in ((0, 0), (0, 4), (1, 0), (1, 5)):
+    for precision, variant in ((0, 4), (0, 0), (1, 5), (1, 0)):
         wb.set_variant(precision, variant)
         for _ in range(2):
             wb.run(hI.data_ptr(), hII.data_ptr(), precision=precision)

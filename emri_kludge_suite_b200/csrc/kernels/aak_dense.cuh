@@ -70,7 +70,9 @@ inline int64_t tile_table_slot_bytes(int rows, bool split) {
 // Launch shapes of the waveform stage, the autotuner's candidates: with the
 // tile pre-pass or tables built inside the tiles, samples per thread whose
 // harmonic sums run side by side, and resident CTAs per SM the register
-// budget is sized for.  Variant 0 is the default of each precision.
+// budget is sized for.  Variant 0 is the default of each precision: the
+// autotuner's choice on both the 512-source configuration-1 batch and a
+// 256-template configuration-4 chunk, in both precisions.
 struct WaveVariant {
   bool pre;
   int joint;
@@ -79,9 +81,9 @@ struct WaveVariant {
 constexpr int kNumVariants = 6;
 constexpr WaveVariant wave_variant(bool split, int v) {
   return split ? (v == 1 ? WaveVariant{false, 0, 2} : v == 2 ? WaveVariant{true, 1, 2} : v == 3 ? WaveVariant{true, 4, 2}
-                  : v == 4 ? WaveVariant{true, 2, 3} : v == 5 ? WaveVariant{true, 1, 3} : WaveVariant{true, 2, 2})
+                  : v == 4 ? WaveVariant{true, 2, 3} : v == 5 ? WaveVariant{true, 2, 2} : WaveVariant{true, 1, 3})
                : (v == 1 ? WaveVariant{false, 0, 2} : v == 2 ? WaveVariant{true, 2, 2} : v == 3 ? WaveVariant{true, 4, 2}
-                  : v == 4 ? WaveVariant{true, 1, 3} : v == 5 ? WaveVariant{true, 2, 3} : WaveVariant{true, 1, 2});
+                  : v == 4 ? WaveVariant{true, 1, 2} : v == 5 ? WaveVariant{true, 2, 3} : WaveVariant{true, 1, 3});
 }
 
 // Everything the kernels read about a batch.
