@@ -562,7 +562,11 @@ __device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double
 //   J_nu^(k)(x) = 2^-k sum_j (-1)^j C(k, j) J_{nu-k+2j}(x)     (DLMF 10.6.7),
 // with the J values of one row from a Miller backward recurrence (or the
 // power series below x = 1), and the 2e factors of A_n expanded exactly.
-// Row n holds [A_0 .. A_K | B_0 .. B_K | C_0 .. C_K].
+// Row n holds [A_0 .. A_K | B_0 .. B_K | C_0 .. C_K] in FP64 and
+// [A_0 B_0 A_1 B_1 .. A_K B_K | C_0 .. C_K] in FP32, where the A and B
+// polynomials of a sample are evaluated as one packed FP32x2 Horner chain
+// (__ffma2_rn, sm_100: each component rounds as fmaf, so the results are
+// those of two scalar chains with one instruction per step).
 // (kTaylorMax64, kTaylorMax32, kRowD, kRowF: aak_dense.cuh)
 // Row stride of a tile with K terms: 3 (K + 1) coefficients padded to 16 bytes.
 template <typename T>
@@ -655,8 +659,13 @@ __device__ __forceinline__ void build_taylor_row_k(T *row, int n, double ec, int
     const double c0 = fac * D[K], c1 = fac * D[K + 1], c2 = fac * D[K + 2], c3 = fac * D[K + 3], c4 = fac * D[K + 4];
     const double A = dn * (c0 - te * c1 - 2.0 * p1 + tn * c2 + te * c3 + 2.0 * p3 - c4);
     const double B = dn * (c0 - 2.0 * c2 + c4);
-    row[k] = (T)A;
-    row[K + 1 + k] = (T)B;
+    if constexpr (sizeof(T) == 4) {
+      row[2 * k] = (T)A;
+      row[2 * k + 1] = (T)B;
+    } else {
+      row[k] = (T)A;
+      row[K + 1 + k] = (T)B;
+    }
     row[2 * (K + 1) + k] = (T)c2;
     p1 = c1;
     p3 = c3;
@@ -753,12 +762,27 @@ __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes,
     }
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-      T A = v[K], B = v[2 * K + 1], C = v[3 * K + 2];
+      T A, B, C = v[3 * K + 2];
+      if constexpr (sizeof(T) == 4) {
+        // A and B of the split rows as one packed FP32x2 Horner chain
+        const float2 dd = make_float2(dl[m], dl[m]);
+        float2 AB = make_float2(v[2 * K], v[2 * K + 1]);
 #pragma unroll
-      for (int k = K - 1; k >= 0; --k) {
-        A = fma(A, dl[m], v[k]);
-        B = fma(B, dl[m], v[K + 1 + k]);
-        C = fma(C, dl[m], v[2 * (K + 1) + k]);
+        for (int k = K - 1; k >= 0; --k) {
+          AB = __ffma2_rn(AB, dd, make_float2(v[2 * k], v[2 * k + 1]));
+          C = fma(C, dl[m], v[2 * (K + 1) + k]);
+        }
+        A = AB.x;
+        B = AB.y;
+      } else {
+        A = v[K];
+        B = v[2 * K + 1];
+#pragma unroll
+        for (int k = K - 1; k >= 0; --k) {
+          A = fma(A, dl[m], v[k]);
+          B = fma(B, dl[m], v[K + 1 + k]);
+          C = fma(C, dl[m], v[2 * (K + 1) + k]);
+        }
       }
       if (kAnchor && (n & (kAnchorEvery - 1)) == 0) {
         float sn, cn;
@@ -770,8 +794,14 @@ __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes,
         zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
         zr[m] = tr;
       }
-      sa[m] = fma(A, zr[m], sa[m]);
-      sb[m] = fma(B, zi[m], sb[m]);
+      if constexpr (sizeof(T) == 4) {
+        const float2 s2 = __ffma2_rn(make_float2(A, B), make_float2(zr[m], zi[m]), make_float2(sa[m], sb[m]));
+        sa[m] = s2.x;
+        sb[m] = s2.y;
+      } else {
+        sa[m] = fma(A, zr[m], sa[m]);
+        sb[m] = fma(B, zi[m], sb[m]);
+      }
       sc[m] = fma(C, zr[m], sc[m]);
     }
   }
