@@ -54,9 +54,21 @@ struct Traj4 {
   double e, v, M, S;
 };
 
-__device__ __forceinline__ double piece(double y0, double y1, double c0, double c1, double h, double dx) {
-  const double b = (y1 - y0) / h - h * (c1 + 2.0 * c0) / 3.0;
-  const double d = (c1 - c0) / (3.0 * h);
+// Coefficients b, d of the natural-spline piece y0 + dx (b + dx (c0 + dx d))
+// on [x0, x0 + h] (the GSL cspline form, KSParMap.cc:487-498), from the
+// piece's reciprocal length rh = 1 / h and rh3 = rh / 3: one division per
+// piece instead of three per component.  Against the divided form the
+// coefficients differ by an ulp or two; the pre-pass and the waveform kernel
+// both evaluate the spline through here, so their values stay equal.
+__device__ __forceinline__ void piece_bd(double y0, double y1, double c0, double c1, double h, double rh, double rh3,
+                                         double &b, double &d) {
+  b = (y1 - y0) * rh - h * (c1 + 2.0 * c0) * (1.0 / 3.0);
+  d = (c1 - c0) * rh3;
+}
+__device__ __forceinline__ double piece(double y0, double y1, double c0, double c1, double h, double rh, double rh3,
+                                        double dx) {
+  double b, d;
+  piece_bd(y0, y1, c0, c1, h, rh, rh3, b, d);
   return y0 + dx * (b + dx * (c0 + dx * d));
 }
 
@@ -82,12 +94,12 @@ struct KnotWin {
 
 __device__ __forceinline__ Traj4 eval_piece(const double4 &y0, const double4 &y1, const double4 &c0, const double4 &c1,
                                             double x0, double x1, double t) {
-  const double h = x1 - x0, dx = t - x0;
+  const double h = x1 - x0, dx = t - x0, rh = 1.0 / h, rh3 = rh * (1.0 / 3.0);
   Traj4 q;
-  q.e = piece(y0.x, y1.x, c0.x, c1.x, h, dx);
-  q.v = piece(y0.y, y1.y, c0.y, c1.y, h, dx);
-  q.M = piece(y0.z, y1.z, c0.z, c1.z, h, dx);
-  q.S = piece(y0.w, y1.w, c0.w, c1.w, h, dx);
+  q.e = piece(y0.x, y1.x, c0.x, c1.x, h, rh, rh3, dx);
+  q.v = piece(y0.y, y1.y, c0.y, c1.y, h, rh, rh3, dx);
+  q.M = piece(y0.z, y1.z, c0.z, c1.z, h, rh, rh3, dx);
+  q.S = piece(y0.w, y1.w, c0.w, c1.w, h, rh, rh3, dx);
   return q;
 }
 
@@ -131,14 +143,15 @@ __device__ __forceinline__ void finish_window(const BatchView &bv, const SourceD
     w.inv_h = (span > 0.0) ? (double)(w.n - 1) / span : 0.0;
     // piece coefficients y + dx (b + dx (c + dx d)) of the natural spline, once per window
     for (int k = threadIdx.x; k < w.n - 1; k += blockDim.x) {
-      const double h = w.t[k + 1] - w.t[k];
+      const double h = w.t[k + 1] - w.t[k], rh = 1.0 / h, rh3 = rh * (1.0 / 3.0);
       const double4 y0 = w.y[k], y1 = w.y[k + 1], c0 = w.c[k], c1 = w.c[k + 1];
-      w.b[k] = make_double4((y1.x - y0.x) / h - h * (c1.x + 2.0 * c0.x) / 3.0,
-                            (y1.y - y0.y) / h - h * (c1.y + 2.0 * c0.y) / 3.0,
-                            (y1.z - y0.z) / h - h * (c1.z + 2.0 * c0.z) / 3.0,
-                            (y1.w - y0.w) / h - h * (c1.w + 2.0 * c0.w) / 3.0);
-      w.d[k] = make_double4((c1.x - c0.x) / (3.0 * h), (c1.y - c0.y) / (3.0 * h), (c1.z - c0.z) / (3.0 * h),
-                            (c1.w - c0.w) / (3.0 * h));
+      double4 b, d;
+      piece_bd(y0.x, y1.x, c0.x, c1.x, h, rh, rh3, b.x, d.x);
+      piece_bd(y0.y, y1.y, c0.y, c1.y, h, rh, rh3, b.y, d.y);
+      piece_bd(y0.z, y1.z, c0.z, c1.z, h, rh, rh3, b.z, d.z);
+      piece_bd(y0.w, y1.w, c0.w, c1.w, h, rh, rh3, b.w, d.w);
+      w.b[k] = b;
+      w.d[k] = d;
     }
     __syncthreads();
   }
@@ -343,6 +356,14 @@ __device__ __forceinline__ void publish_inclusive(const BatchView &bv, int64_t g
   st_release(bv.link_flag + g, 2);
 }
 
+// This tile's aggregate, published by the look-back only when it has to wait.
+struct TileAgg {
+  double x[3];  // the tile's own sums of the chain's direction
+  double C;     // the clamped Phidot of its last forward output sample
+  bool hasC;
+  bool publish;  // false: nothing to publish (the tile looks back before its phases are known)
+};
+
 // Exclusive prefix of tile c.lt along its chain (dir +1: forward, -1:
 // backward), computed by one whole warp.  Each round looks at the 32 nearest
 // predecessors not yet summed (lane k: k + 1 tiles further towards the head),
@@ -350,13 +371,18 @@ __device__ __forceinline__ void publish_inclusive(const BatchView &bv, int64_t g
 // than the head tile) is written, and sums their aggregates and that
 // inclusive record in double-double.  C (forward chains): the clamped Phidot
 // of the nearest record that sets one, else 0.  Every lane returns the sums.
-__device__ void look_back_warp(const BatchView &bv, const TileCtx &c, int dir, double hi[3], double lo[3], double &C) {
+// agg: the tile's aggregate, published before the first wait or
+// second round, and not at all when the first round finds the prefix ready
+// (the tile's inclusive record follows at once): successors never wait on a
+// tile that waits itself without its aggregate out.
+__device__ void look_back_warp(const BatchView &bv, const TileCtx &c, int dir, double hi[3], double lo[3], double &C,
+                               TileAgg agg = TileAgg{{0.0, 0.0, 0.0}, 0.0, false, false}) {
   const unsigned kAll = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int64_t t0 = c.g - c.lt;
   const long long bound = (bv.lookback_cycles > 0) ? bv.lookback_cycles : kLookBackCycles;
   const long long start = clock64();
-  bool haveC = false;
+  bool haveC = false, published = !agg.publish;
   C = 0.0;
 #pragma unroll
   for (int q = 0; q < 3; ++q) hi[q] = lo[q] = 0.0;
@@ -371,7 +397,12 @@ __device__ void look_back_warp(const BatchView &bv, const TileCtx &c, int dir, d
       const unsigned vmask = __ballot_sync(kAll, valid);
       const unsigned ready = __ballot_sync(kAll, valid && f != 0);
       need = stop_mask ? ((stop_mask & (0u - stop_mask)) << 1) - 1u : vmask;  // lanes up to the first stop
-      if ((ready & need) == need) break;
+      const bool done = (ready & need) == need;
+      if (!published && !(done && stop_mask)) {  // a wait or a further round follows
+        if (lane == 0) publish_aggregate(bv, c.g, agg.x, agg.C, agg.hasC);
+        published = true;
+      }
+      if (done) break;
       int give_up = 0;
       if (lane == 0)
         give_up = (*(volatile unsigned int *)bv.device_status != 0u || clock64() - start > bound) ? 1 : 0;
@@ -1230,15 +1261,20 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     }
     __syncthreads();
   }
-  // Work queue: the first tile is fetched here, every later one during the
-  // tile before it (before that tile's last barrier), so that the atomic's
-  // round trip overlaps the tile's work.
+  // Work queue: the first tile is fetched here, every later one by a thread
+  // of warp 1 at the start of the tile before it, so that the atomic's round
+  // trip overlaps that tile's work and stays off warp 0's look-back.  Items
+  // leave the queue in chain order, and a CTA's next item always comes after
+  // its current one, so the earliest unfinished item is always being worked
+  // on and its predecessors are done: holding one item ahead cannot stall the
+  // chains.
   if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
   __syncthreads();
   for (;;) {
     const long long j = s_tile;
     __syncthreads();
     if (j >= bv.total_tiles) break;
+    if (tid == 32) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);  // read after this tile's last barrier
     const SourceDesc *dp;
     const TileCtx c = tile_ctx(bv, j, dp);
     const int64_t g = c.g;
@@ -1262,7 +1298,6 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
       if (tid == 0) {
         const double zero[3] = {0.0, 0.0, 0.0};
         publish_aggregate(bv, g, zero, 0.0, false);
-        s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
       }
       __syncthreads();
       continue;
@@ -1580,8 +1615,9 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
         }
         C = s_cy[6];
       } else if (dir != 0) {
-        if (tid == 0) publish_aggregate(bv, g, (dir > 0) ? runF : runB, hasF ? s_lastP : 0.0, hasF);
-        look_back_warp(bv, c, dir, hi, lo, C);
+        const TileAgg agg{{(dir > 0) ? runF[0] : runB[0], (dir > 0) ? runF[1] : runB[1], (dir > 0) ? runF[2] : runB[2]},
+                          hasF ? s_lastP : 0.0, hasF, true};
+        look_back_warp(bv, c, dir, hi, lo, C, agg);
       }
       if (tid == 0) {
         double fh[3] = {0, 0, 0}, fl[3] = {0, 0, 0}, bh[3] = {0, 0, 0}, bl[3] = {0, 0, 0};
@@ -1610,7 +1646,6 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
         else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
       }
 #endif
-    if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);  // the next tile, read after the loop's barrier
     __syncthreads();
     // the phases of this thread's own samples: X0 + carry + local part
     // (forward), X0 - (carry + increments after the sample) (backward)
