@@ -593,17 +593,28 @@ __device__ __forceinline__ void bessel5_fp64(int lo, double x, int start, double
 //   J_nu^(k)(x) = 2^-k sum_j (-1)^j C(k, j) J_{nu-k+2j}(x)     (DLMF 10.6.7),
 // with the J values of one row from a Miller backward recurrence (or the
 // power series below x = 1), and the 2e factors of A_n expanded exactly.
-// Row n holds [A_0 .. A_K | B_0 .. B_K | C_0 .. C_K] in FP64 and
-// [A_0 B_0 A_1 B_1 .. A_K B_K | C_0 .. C_K] in FP32, where the A and B
-// polynomials of a sample are evaluated as one packed FP32x2 Horner chain
-// (__ffma2_rn, sm_100: each component rounds as fmaf, so the results are
-// those of two scalar chains with one instruction per step).
+// FP64 tables: row n holds [A_0 .. A_K | B_0 .. B_K | C_0 .. C_K].  FP32
+// tables hold the harmonics in pairs (2p+1, 2p+2): pair row p is
+// [A_0 B_0 .. A_K B_K of 2p+1 | the same of 2p+2 | C_0 of both, C_1 of both,
+// .. C_K of both], so that a sample evaluates the A and B polynomials of one
+// harmonic, and the C polynomials of the two harmonics of a pair, as packed
+// FP32x2 Horner chains (__ffma2_rn, sm_100: each component rounds as fmaf,
+// so the results are those of scalar chains with one instruction per step
+// for two).  A pair row past an odd harmonic count holds zeros for the
+// missing harmonic.
 // (kTaylorMax64, kTaylorMax32, kRowD, kRowF: aak_dense.cuh)
-// Row stride of a tile with K terms: 3 (K + 1) coefficients padded to 16 bytes.
+// Stride of a tile with K terms, padded to 16 bytes: FP64, 3 (K + 1) doubles
+// per harmonic; FP32, 6 (K + 1) floats per pair of harmonics.
 template <typename T>
 __host__ __device__ __forceinline__ int row_stride(int K) {
   const int per = 16 / (int)sizeof(T);
-  return (3 * (K + 1) + per - 1) / per * per;
+  const int vals = (sizeof(T) == 4) ? 6 * (K + 1) : 3 * (K + 1);
+  return (vals + per - 1) / per * per;
+}
+// Harmonic rows a launch provides for `rows` harmonics: FP32 tables hold whole pairs.
+template <typename T>
+__host__ __device__ __forceinline__ int table_rows(int rows) {
+  return (sizeof(T) == 4) ? (rows + 1) & ~1 : rows;
 }
 
 // J_m(x) for m = mlo .. mhi (x >= 0) into J[m - mlo]: Miller's backward
@@ -662,7 +673,7 @@ __device__ void bessel_window(double x, int mlo, int mhi, int start, double *J) 
 // narrows the valid window by one order on each side and leaves orders
 // n-2 .. n+2 at positions K .. K+4.
 template <int K, typename T>
-__device__ __forceinline__ void build_taylor_row_k(T *row, int n, double ec, int start) {
+__device__ __forceinline__ void build_taylor_row_k(T *tab, int stride, int n, double ec, int start) {
   constexpr int W = 2 * K + 5;
   const int lo = n - 2 - K, mlo = max(0, lo);
   double Jw[W];
@@ -691,34 +702,63 @@ __device__ __forceinline__ void build_taylor_row_k(T *row, int n, double ec, int
     const double A = dn * (c0 - te * c1 - 2.0 * p1 + tn * c2 + te * c3 + 2.0 * p3 - c4);
     const double B = dn * (c0 - 2.0 * c2 + c4);
     if constexpr (sizeof(T) == 4) {
-      row[2 * k] = (T)A;
-      row[2 * k + 1] = (T)B;
+      T *pr = tab + ((n - 1) >> 1) * stride;
+      const int h = (n - 1) & 1;
+      pr[2 * (K + 1) * h + 2 * k] = (T)A;
+      pr[2 * (K + 1) * h + 2 * k + 1] = (T)B;
+      pr[4 * (K + 1) + 2 * k + h] = (T)c2;
     } else {
+      T *row = tab + (n - 1) * stride;
       row[k] = (T)A;
       row[K + 1 + k] = (T)B;
+      row[2 * (K + 1) + k] = (T)c2;
     }
-    row[2 * (K + 1) + k] = (T)c2;
     p1 = c1;
     p3 = c3;
   }
 }
 
+// Zero coefficients for harmonic n of an FP32 pair row (the harmonic past an odd count).
+template <int K>
+__device__ __forceinline__ void zero_taylor_row_k(float *tab, int stride, int n) {
+  float *pr = tab + ((n - 1) >> 1) * stride;
+  const int h = (n - 1) & 1;
+#pragma unroll
+  for (int k = 0; k <= K; ++k) {
+    pr[2 * (K + 1) * h + 2 * k] = 0.f;
+    pr[2 * (K + 1) * h + 2 * k + 1] = 0.f;
+    pr[4 * (K + 1) + 2 * k + h] = 0.f;
+  }
+}
+
+// Table row of harmonic n (tab: the tile's table, stride: row_stride of the
+// tile, or larger); n = nmodes + 1 of an FP32 table writes the zero half of
+// the last pair.
 template <typename T>
-__device__ void build_taylor_row(T *row, int n, double ec, int K, int start) {
+__device__ void build_taylor_row(T *tab, int stride, int n, int nmodes, double ec, int K, int start) {
   if constexpr (sizeof(T) == 4) {
+    if (n > nmodes) {
+      switch (K) {
+        case 2: zero_taylor_row_k<2>(tab, stride, n); break;
+        case 3: zero_taylor_row_k<3>(tab, stride, n); break;
+        case 4: zero_taylor_row_k<4>(tab, stride, n); break;
+        default: zero_taylor_row_k<6>(tab, stride, n); break;
+      }
+      return;
+    }
     switch (K) {
-      case 2: build_taylor_row_k<2, T>(row, n, ec, start); break;
-      case 3: build_taylor_row_k<3, T>(row, n, ec, start); break;
-      case 4: build_taylor_row_k<4, T>(row, n, ec, start); break;
-      default: build_taylor_row_k<6, T>(row, n, ec, start); break;
+      case 2: build_taylor_row_k<2, T>(tab, stride, n, ec, start); break;
+      case 3: build_taylor_row_k<3, T>(tab, stride, n, ec, start); break;
+      case 4: build_taylor_row_k<4, T>(tab, stride, n, ec, start); break;
+      default: build_taylor_row_k<6, T>(tab, stride, n, ec, start); break;
     }
   } else {
     switch (K) {
-      case 4: build_taylor_row_k<4, T>(row, n, ec, start); break;
-      case 5: build_taylor_row_k<5, T>(row, n, ec, start); break;
-      case 6: build_taylor_row_k<6, T>(row, n, ec, start); break;
-      case 8: build_taylor_row_k<8, T>(row, n, ec, start); break;
-      default: build_taylor_row_k<10, T>(row, n, ec, start); break;
+      case 4: build_taylor_row_k<4, T>(tab, stride, n, ec, start); break;
+      case 5: build_taylor_row_k<5, T>(tab, stride, n, ec, start); break;
+      case 6: build_taylor_row_k<6, T>(tab, stride, n, ec, start); break;
+      case 8: build_taylor_row_k<8, T>(tab, stride, n, ec, start); break;
+      default: build_taylor_row_k<10, T>(tab, stride, n, ec, start); break;
     }
   }
 }
@@ -750,89 +790,43 @@ __device__ __forceinline__ int taylor_terms_fp32(double q, int nmodes) {
 // phases from the rotation recurrence w_n = w_{n-1} z_1, w_0 = z_D (so
 // w_n = z_1^n z_D: one complex product per harmonic), for M samples of one
 // tile at once: each table row is loaded once for all of them and the M
-// recurrences run side by side.
-// Split precision (T = float): every kAnchorEvery-th harmonic the rotor is
-// re-anchored at exp(i (n Phi' + D0)) with n Phi' + D0 reduced in FP64, so
-// the FP32 recurrence carries at most kAnchorEvery - 1 steps of rounding and
-// of the error of z_1, whatever n: the n Phi argument reduction stays FP64.
-constexpr int kAnchorEvery = 8;
-template <int K, typename T, int M>
-__device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes, int stride, const T *dl, const T *c1,
-                                                       const T *s1, const T *cD, const T *sD, const double *ph,
-                                                       const T *d0, T *Sa, T *Sb, T *Sc) {
-  constexpr bool kAnchor = sizeof(T) == 4;
+// recurrences run side by side.  FP64 tables.
+template <int K, int M>
+__device__ __forceinline__ void mode_sums_fp64(const double *tab, int nmodes, int stride, const double *dl,
+                                               const double *c1, const double *s1, const double *cD, const double *sD,
+                                               double *Sa, double *Sb, double *Sc) {
   constexpr int NV = 3 * (K + 1);
-  T zr[M], zi[M], sa[M], sb[M], sc[M];
+  double zr[M], zi[M], sa[M], sb[M], sc[M];
 #pragma unroll
   for (int m = 0; m < M; ++m) {
     zr[m] = cD[m];  // w_0 = z_D; w_n = w_{n-1} z_1 = z_1^n z_D
     zi[m] = sD[m];
-    sa[m] = sb[m] = sc[m] = T(0);
+    sa[m] = sb[m] = sc[m] = 0.0;
   }
 #pragma unroll 1
   for (int n = 1; n <= nmodes; ++n) {
-    T v[(sizeof(T) == 4) ? (NV + 3) / 4 * 4 : (NV + 1) / 2 * 2];
-    if constexpr (sizeof(T) == 4) {
-      const float4 *r4 = reinterpret_cast<const float4 *>(tab + (n - 1) * stride);
+    double v[(NV + 1) / 2 * 2];
+    const double2 *r2 = reinterpret_cast<const double2 *>(tab + (n - 1) * stride);
 #pragma unroll
-      for (int i = 0; i < (NV + 3) / 4; ++i) {
-        const float4 q = r4[i];
-        v[4 * i] = q.x;
-        v[4 * i + 1] = q.y;
-        v[4 * i + 2] = q.z;
-        v[4 * i + 3] = q.w;
-      }
-    } else {
-      const double2 *r2 = reinterpret_cast<const double2 *>(tab + (n - 1) * stride);
-#pragma unroll
-      for (int i = 0; i < (NV + 1) / 2; ++i) {
-        const double2 q = r2[i];
-        v[2 * i] = q.x;
-        v[2 * i + 1] = q.y;
-      }
+    for (int i = 0; i < (NV + 1) / 2; ++i) {
+      const double2 q = r2[i];
+      v[2 * i] = q.x;
+      v[2 * i + 1] = q.y;
     }
 #pragma unroll
     for (int m = 0; m < M; ++m) {
-      T A, B, C = v[3 * K + 2];
-      if constexpr (sizeof(T) == 4) {
-        // A and B of the split rows as one packed FP32x2 Horner chain
-        const float2 dd = make_float2(dl[m], dl[m]);
-        float2 AB = make_float2(v[2 * K], v[2 * K + 1]);
+      double A = v[K], B = v[2 * K + 1], C = v[3 * K + 2];
 #pragma unroll
-        for (int k = K - 1; k >= 0; --k) {
-          AB = __ffma2_rn(AB, dd, make_float2(v[2 * k], v[2 * k + 1]));
-          C = fma(C, dl[m], v[2 * (K + 1) + k]);
-        }
-        A = AB.x;
-        B = AB.y;
-      } else {
-        A = v[K];
-        B = v[2 * K + 1];
-#pragma unroll
-        for (int k = K - 1; k >= 0; --k) {
-          A = fma(A, dl[m], v[k]);
-          B = fma(B, dl[m], v[K + 1 + k]);
-          C = fma(C, dl[m], v[2 * (K + 1) + k]);
-        }
+      for (int k = K - 1; k >= 0; --k) {
+        A = fma(A, dl[m], v[k]);
+        B = fma(B, dl[m], v[K + 1 + k]);
+        C = fma(C, dl[m], v[2 * (K + 1) + k]);
       }
-      if (kAnchor && (n & (kAnchorEvery - 1)) == 0) {
-        float sn, cn;
-        __sincosf(reduce_2pi_f(fma((double)n, ph[m], (double)d0[m])), &sn, &cn);
-        zr[m] = (T)cn;
-        zi[m] = (T)sn;
-      } else {
-        const T tr = zr[m] * c1[m] - zi[m] * s1[m];
-        zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
-        zr[m] = tr;
-      }
-      if constexpr (sizeof(T) == 4) {
-        const float2 s2 = __ffma2_rn(make_float2(A, B), make_float2(zr[m], zi[m]), make_float2(sa[m], sb[m]));
-        sa[m] = s2.x;
-        sb[m] = s2.y;
-      } else {
-        sa[m] = fma(A, zr[m], sa[m]);
-        sb[m] = fma(B, zi[m], sb[m]);
-      }
+      const double tr = zr[m] * c1[m] - zi[m] * s1[m];
+      zi[m] = fma(zr[m], s1[m], zi[m] * c1[m]);
+      zr[m] = tr;
+      sa[m] = fma(A, zr[m], sa[m]);
+      sb[m] = fma(B, zi[m], sb[m]);
       sc[m] = fma(C, zr[m], sc[m]);
     }
   }
@@ -841,6 +835,96 @@ __device__ __forceinline__ void mode_sums_taylor_multi(const T *tab, int nmodes,
     Sa[m] = sa[m];
     Sb[m] = sb[m];
     Sc[m] = sc[m];
+  }
+}
+
+// The same sums from an FP32 pair table (split precision).  Per pair of
+// harmonics (2p+1, 2p+2): the A, B polynomials of each harmonic and the C
+// polynomials of both as packed FP32x2 Horner chains, two rotor steps, and
+// (Sa, Sb) += (A, B) (Re w, Im w) and (Sc_odd, Sc_even) += (C_odd, C_even)
+// (Re w_odd, Re w_even) as packed FMAs.  The rotor is re-anchored at every
+// harmonic n = 8j: exp(i (n Phi' + D0)) with n Phi' + D0 reduced in FP64, so
+// the FP32 recurrence carries at most 7 steps (w_1 .. w_7 from z_D, w_{8j+1}
+// .. w_{8j+7} from an anchor) of rounding and of the error of z_1, whatever n:
+// the n Phi argument reduction stays FP64.  Pairs run in blocks of four
+// (harmonics 8b+1 .. 8b+8, the last one the anchor), then the remaining
+// fewer than four pairs, which hold no anchor.
+constexpr int kAnchorEvery = 8;
+template <int K, int M, bool kAnchorLast>
+__device__ __forceinline__ void pair_step(const float *pr, int nlast, const float *dl, const float *c1, const float *s1,
+                                          const double *ph, const float *d0, float *zr, float *zi, float2 *sab,
+                                          float2 *sc2) {
+  constexpr int PV = 6 * (K + 1), PV4 = (PV + 3) / 4;
+  float v[PV4 * 4];
+  const float4 *r4 = reinterpret_cast<const float4 *>(pr);
+#pragma unroll
+  for (int i = 0; i < PV4; ++i) {
+    const float4 q = r4[i];
+    v[4 * i] = q.x;
+    v[4 * i + 1] = q.y;
+    v[4 * i + 2] = q.z;
+    v[4 * i + 3] = q.w;
+  }
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    const float2 dd = make_float2(dl[m], dl[m]);
+    float2 ABo = make_float2(v[2 * K], v[2 * K + 1]);
+    float2 ABe = make_float2(v[2 * (K + 1) + 2 * K], v[2 * (K + 1) + 2 * K + 1]);
+    float2 Cp = make_float2(v[4 * (K + 1) + 2 * K], v[4 * (K + 1) + 2 * K + 1]);
+#pragma unroll
+    for (int k = K - 1; k >= 0; --k) {
+      ABo = __ffma2_rn(ABo, dd, make_float2(v[2 * k], v[2 * k + 1]));
+      ABe = __ffma2_rn(ABe, dd, make_float2(v[2 * (K + 1) + 2 * k], v[2 * (K + 1) + 2 * k + 1]));
+      Cp = __ffma2_rn(Cp, dd, make_float2(v[4 * (K + 1) + 2 * k], v[4 * (K + 1) + 2 * k + 1]));
+    }
+    // w of the odd harmonic, then of the even one (the anchor at the end of a block)
+    const float ro = zr[m] * c1[m] - zi[m] * s1[m];
+    const float io = fmaf(zr[m], s1[m], zi[m] * c1[m]);
+    float re, ie;
+    if constexpr (kAnchorLast) {
+      __sincosf(reduce_2pi_f(fma((double)nlast, ph[m], (double)d0[m])), &ie, &re);
+    } else {
+      re = ro * c1[m] - io * s1[m];
+      ie = fmaf(ro, s1[m], io * c1[m]);
+    }
+    sab[m] = __ffma2_rn(ABo, make_float2(ro, io), sab[m]);
+    sab[m] = __ffma2_rn(ABe, make_float2(re, ie), sab[m]);
+    sc2[m] = __ffma2_rn(Cp, make_float2(ro, re), sc2[m]);
+    zr[m] = re;
+    zi[m] = ie;
+  }
+}
+
+template <int K, int M>
+__device__ __forceinline__ void mode_sums_split(const float *tab, int nmodes, int stride, const float *dl,
+                                                const float *c1, const float *s1, const float *cD, const float *sD,
+                                                const double *ph, const float *d0, float *Sa, float *Sb, float *Sc) {
+  static_assert(kAnchorEvery == 8, "a block of four pairs ends at the anchor");
+  float zr[M], zi[M];
+  float2 sab[M], sc2[M];
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    zr[m] = cD[m];  // w_0 = z_D
+    zi[m] = sD[m];
+    sab[m] = sc2[m] = make_float2(0.f, 0.f);
+  }
+  const int npairs = (nmodes + 1) >> 1;
+  int p = 0;
+#pragma unroll 1
+  for (; p + 4 <= npairs; p += 4) {
+    const float *pr = tab + p * stride;
+    pair_step<K, M, false>(pr, 0, dl, c1, s1, ph, d0, zr, zi, sab, sc2);
+    pair_step<K, M, false>(pr + stride, 0, dl, c1, s1, ph, d0, zr, zi, sab, sc2);
+    pair_step<K, M, false>(pr + 2 * stride, 0, dl, c1, s1, ph, d0, zr, zi, sab, sc2);
+    pair_step<K, M, true>(pr + 3 * stride, 2 * p + 8, dl, c1, s1, ph, d0, zr, zi, sab, sc2);
+  }
+#pragma unroll 1
+  for (; p < npairs; ++p) pair_step<K, M, false>(tab + p * stride, 0, dl, c1, s1, ph, d0, zr, zi, sab, sc2);
+#pragma unroll
+  for (int m = 0; m < M; ++m) {
+    Sa[m] = sab[m].x;
+    Sb[m] = sab[m].y;
+    Sc[m] = sc2[m].x + sc2[m].y;
   }
 }
 
@@ -1188,9 +1272,9 @@ __global__ void __launch_bounds__(128) k_tile_table(BatchView bv, int rows) {
   const int K = P.K;
   if (K <= 0) return;
   const SourceDesc &d = bv.src[P.src];
-  if (n > d.nmodes) return;
-  T *row = reinterpret_cast<T *>(static_cast<unsigned char *>(bv.tile_tab) + g * bv.tab_slot) + (n - 1) * P.stride;
-  build_taylor_row<T>(row, n, P.ec, K, bv.bessel_start[d.bessel_offset + n - 1]);
+  if (n > table_rows<T>(d.nmodes)) return;
+  T *tab = reinterpret_cast<T *>(static_cast<unsigned char *>(bv.tile_tab) + g * bv.tab_slot);
+  build_taylor_row<T>(tab, P.stride, n, d.nmodes, P.ec, K, (n <= d.nmodes) ? bv.bessel_start[d.bessel_offset + n - 1] : 0);
 }
 
 // ------------------------------------------------------------------ waveform kernel
@@ -1329,7 +1413,8 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
         }
         const bool tab = !kPhase && Kt > 0 && nm <= kTabModes;
         if (tab) {
-          const uint32_t b1 = (uint32_t)nm * (uint32_t)st * (uint32_t)sizeof(TT);
+          // FP64: one row per harmonic; FP32: one row per pair of harmonics
+          const uint32_t b1 = (uint32_t)(kSplit ? (nm + 1) >> 1 : nm) * (uint32_t)st * (uint32_t)sizeof(TT);
           mbar_arrive_expect_tx(&s_mbar[1], b1);
           bulk_copy_g2s(tabD, static_cast<const unsigned char *>(bv.tile_tab) + g * bv.tab_slot, b1, &s_mbar[1]);
         }
@@ -1433,9 +1518,10 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
 #if !AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread per harmonic); its barrier is the first one of phase 1
     if (!kPhase && !kPre && K > 0 && !bv.trajectory_only)
-      for (int n = tid + 1; n <= d.nmodes; n += kTileThreads) {
-        if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
-        else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
+      for (int n = tid + 1; n <= (kSplit ? table_rows<float>(d.nmodes) : d.nmodes); n += kTileThreads) {
+        const int st = (n <= d.nmodes) ? bstart[n - 1] : 0;
+        if (kSplit) build_taylor_row<float>(tabF, 2 * kRowF, n, d.nmodes, ec, K, st);
+        else build_taylor_row<double>(tabD, kRowD, n, d.nmodes, ec, K, st);
       }
 #endif
     // ---------------- phase 1: phases of the tile's samples, relative to the tile
@@ -1641,9 +1727,10 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
 #if AAK_TABLE_AFTER_SCAN
     // Taylor table rows (one thread of warps 1-7 per harmonic) while warp 0 looks back
     else if (!kPhase && !kPre && K > 0 && !bv.trajectory_only)
-      for (int n = tid - 31; n <= d.nmodes; n += kTileThreads - 32) {
-        if (kSplit) build_taylor_row<float>(tabF + (n - 1) * kRowF, n, ec, K, bstart[n - 1]);
-        else build_taylor_row<double>(tabD + (n - 1) * kRowD, n, ec, K, bstart[n - 1]);
+      for (int n = tid - 31; n <= (kSplit ? table_rows<float>(d.nmodes) : d.nmodes); n += kTileThreads - 32) {
+        const int st = (n <= d.nmodes) ? bstart[n - 1] : 0;
+        if (kSplit) build_taylor_row<float>(tabF, 2 * kRowF, n, d.nmodes, ec, K, st);
+        else build_taylor_row<double>(tabD, kRowD, n, d.nmodes, ec, K, st);
       }
 #endif
     __syncthreads();
@@ -1719,7 +1806,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     constexpr int kJoint = kJointT > 0 ? kJointT : (kSplit ? AAK_JOINT_SPLIT : AAK_JOINT_FP64);
     static_assert(kTileChunks % kJoint == 0, "joint samples must divide the chunks");
     const T *tab = kSplit ? reinterpret_cast<const T *>(tabF) : reinterpret_cast<const T *>(tabD);
-    const int rs = kPre ? (int)s_prep.stride : (kSplit ? kRowF : kRowD);  // table row stride
+    const int rs = kPre ? (int)s_prep.stride : (kSplit ? 2 * kRowF : kRowD);  // table row (FP32: pair row) stride
 #pragma unroll 1
     for (int g0 = 0; g0 < kTileChunks; g0 += kJoint) {
       SamplePrep<T> P[kJoint];
@@ -1750,19 +1837,19 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
       }
       if constexpr (kSplit) {
         switch (K) {
-          case 2: mode_sums_taylor_multi<2, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 3: mode_sums_taylor_multi<3, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 2: mode_sums_split<2, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 3: mode_sums_split<3, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 4: mode_sums_split<4, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 6: mode_sums_split<6, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
           default: break;
         }
       } else {
         switch (K) {
-          case 4: mode_sums_taylor_multi<4, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 5: mode_sums_taylor_multi<5, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 6: mode_sums_taylor_multi<6, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 8: mode_sums_taylor_multi<8, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
-          case 10: mode_sums_taylor_multi<10, T, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, ph, d0, Sa, Sb, Sc); break;
+          case 4: mode_sums_fp64<4, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 5: mode_sums_fp64<5, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 6: mode_sums_fp64<6, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 8: mode_sums_fp64<8, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
+          case 10: mode_sums_fp64<10, kJoint>(tab, d.nmodes, rs, dl, c1, s1, cD, sD, Sa, Sb, Sc); break;
           default: break;
         }
       }
@@ -2044,7 +2131,8 @@ void launch_dense_t(const BatchView &bv, int num_sms, cudaStream_t stream, cudaE
   cudaMemsetAsync(bv.link_flag, 0, (size_t)bv.total_tiles * sizeof(int32_t), stream);
   if (ev) cudaEventRecord(ev[1], stream);
   // per-sample values, then the Taylor table sized for the batch's harmonic count
-  const int rows = (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes;
+  const int rows = table_rows<typename std::conditional<kSplit, float, double>::type>(
+      (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes);
   const size_t dyn = kWaveDynSmem + (size_t)rows * (kSplit ? kRowF * sizeof(float) : kRowD * sizeof(double));
   const int v = (bv.variant >= 0 && bv.variant < kNumVariants) ? bv.variant : 0;
   const bool pre = wave_variant(kSplit, v).pre && bv.tile_prep && bv.tile_tab && !bv.trajectory_only &&

@@ -53,7 +53,8 @@ struct alignas(16) TilePrep {
 static_assert(sizeof(TilePrep) == 64, "TilePrep is one 64-byte bulk copy");
 
 // Taylor-table rows: FP64 terms at most (K <= 10) and FP32 terms at most
-// (K <= 6); a tile's rows hold 3 (K + 1) coefficients, padded to 16 bytes.
+// (K <= 6); a tile's FP64 rows hold 3 (K + 1) coefficients of one harmonic,
+// its FP32 rows 6 (K + 1) of a pair of harmonics, padded to 16 bytes.
 constexpr int kTaylorMax64 = 10;
 constexpr int kTaylorMax32 = 6;
 constexpr int kRowD = (3 * (kTaylorMax64 + 1) + 1) / 2 * 2;  // doubles per FP64 row at most (34)
@@ -64,7 +65,9 @@ constexpr int kTabModes = 128;
 // (largest harmonic count of the batch) in FP64 (split = false) or FP32 rows.
 inline int64_t tile_table_slot_bytes(int rows, bool split) {
   const int r = (rows > 0 && rows < kTabModes) ? rows : kTabModes;
-  return split ? (int64_t)r * kRowF * (int64_t)sizeof(float) : (int64_t)r * kRowD * (int64_t)sizeof(double);
+  // FP32 tables hold pairs of harmonics (a pair row is at most 2 kRowF floats)
+  return split ? (int64_t)((r + 1) & ~1) * kRowF * (int64_t)sizeof(float)
+               : (int64_t)r * kRowD * (int64_t)sizeof(double);
 }
 
 // Launch shapes of the waveform stage, the autotuner's candidates: with the
