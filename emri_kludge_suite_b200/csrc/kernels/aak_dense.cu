@@ -1346,19 +1346,20 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     __syncthreads();
   }
   // Work queue: the first tile is fetched here, every later one by a thread
-  // of warp 1 at the start of the tile before it, so that the atomic's round
-  // trip overlaps that tile's work and stays off warp 0's look-back.  Items
-  // leave the queue in chain order, and a CTA's next item always comes after
-  // its current one, so the earliest unfinished item is always being worked
-  // on and its predecessors are done: holding one item ahead cannot stall the
-  // chains.
+  // of warp 1 while warp 0 looks back in the tile before it (an empty tile:
+  // by thread 0 at its end), so that the atomic's round trip overlaps the
+  // look-back.  Items leave the queue in chain order, and a CTA's next item
+  // always comes after its current one, so the earliest unfinished item is
+  // always being worked on and its predecessors are done: holding one item
+  // ahead cannot stall the chains.  (Fetching at the start of the tile was
+  // slower: the CTAs then hold twice as many items, and more of them start
+  // while their chain predecessors are still running.)
   if (tid == 0) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
   __syncthreads();
   for (;;) {
     const long long j = s_tile;
     __syncthreads();
     if (j >= bv.total_tiles) break;
-    if (tid == 32) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);  // read after this tile's last barrier
     const SourceDesc *dp;
     const TileCtx c = tile_ctx(bv, j, dp);
     const int64_t g = c.g;
@@ -1382,6 +1383,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
       if (tid == 0) {
         const double zero[3] = {0.0, 0.0, 0.0};
         publish_aggregate(bv, g, zero, 0.0, false);
+        s_tile = (long long)atomicAdd(bv.work_counter, 1ull);
       }
       __syncthreads();
       continue;
@@ -1689,6 +1691,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
       if (bv.traj_out) bv.traj_out[7 * bv.traj_stride + d.out_offset + i] = nuv[k];
     }
     __syncthreads();
+    if (tid == 32) s_tile = (long long)atomicAdd(bv.work_counter, 1ull);  // the next tile, read after the loop's barrier
     // ---------------- chain carries: warp 0 publishes this tile's aggregate,
     // looks back for the exclusive prefix and publishes the inclusive record
     if (tid < 32) {
