@@ -77,7 +77,7 @@ struct aak_ctx {
   std::vector<SourceDesc> descs;
   std::vector<int64_t> tile_start;
   std::vector<int64_t> tile_pairs;  // per source {0, its tiles}: the tile prefix of a one-source view
-  std::vector<int64_t> queue;       // work-queue order of the tiles (global tile indices)
+  std::vector<QueueItem> queue;     // work-queue order of the tiles, with what staging each needs
   std::vector<int32_t> tile_knot;  // 2 per tile: first knot of the tile window, knots in it
   std::vector<int64_t> kofs;       // nsrc + 1 prefix of knots (the sources' knots stay in their plans)
   std::vector<int64_t> spl_blk;    // nsrc + 1 prefix of the device spline solve's blocks
@@ -89,7 +89,8 @@ struct aak_ctx {
   bool uploaded = false;
   // device buffers
   DevBuf<SourceDesc> d_src;
-  DevBuf<int64_t> d_tile_start, d_tile_pairs, d_queue, d_spl_blk;
+  DevBuf<int64_t> d_tile_start, d_tile_pairs, d_spl_blk;
+  DevBuf<QueueItem> d_queue;
   DevBuf<int32_t> d_tile_knot;
   DevBuf<double> d_knot_t;
   DevBuf<double4> d_knot_y, d_knot_c;
@@ -300,11 +301,28 @@ int pack(aak_ctx *ctx, const std::vector<aak_params> &P, int nthreads) {
     head[s] = (i0 <= 0 || T[s] == 0) ? 0 : std::min(i0 / kTileSamples, T[s] - 1);
     maxT = std::max(maxT, T[s]);
   }
-  ctx->queue.resize(std::max<int64_t>(ctx->total_tiles, 1));
+  // Each item also carries the tile's knot window and whether it has output
+  // (the waveform kernel's test: a failed source, or a tile that starts at or
+  // after the taper's end, min(vlength, i_plunge + i_buffer)).
+  ctx->queue.assign(std::max<int64_t>(ctx->total_tiles, 1), QueueItem{});
   int64_t q = 0;
   for (int k = 0; k < maxT; ++k)
     for (int s = 0; s < n; ++s)
-      if (k < T[s]) ctx->queue[q++] = ctx->tile_start[s] + ((k < T[s] - head[s]) ? head[s] + k : T[s] - 1 - k);
+      if (k < T[s]) {
+        const SourceDesc &d = ctx->descs[s];
+        const int lt = (k < T[s] - head[s]) ? head[s] + k : T[s] - 1 - k;
+        const int64_t g = ctx->tile_start[s] + lt;
+        const long long neff = std::min<long long>(d.vlength, (long long)d.i_plunge + (long long)d.i_buffer);
+        QueueItem &it = ctx->queue[q++];
+        it.g = (int32_t)g;
+        it.s = s;
+        it.lt = lt;
+        it.k0 = ctx->tile_knot[2 * g];
+        it.nk = ctx->tile_knot[2 * g + 1];
+        it.knot = d.knot_offset + it.k0;
+        it.flags = (d.status != 0 ? kQueueFailed | kQueueNoWave : 0) |
+                   ((long long)lt * kTileSamples >= neff ? kQueueNoWave : 0);
+      }
   ctx->uploaded = false;
   return AAK_OK;
 }
@@ -756,7 +774,7 @@ int upload(aak_ctx *ctx, cudaStream_t st, bool wait_pinned = true) {
       (r = cp(ctx->d_tile_start.ptr, ctx->tile_start.data(), (n + 1) * sizeof(int64_t))) ||
       (r = cp(ctx->d_tile_knot.ptr, ctx->tile_knot.data(), ctx->tile_knot.size() * sizeof(int32_t))) ||
       (r = cp(ctx->d_tile_pairs.ptr, ctx->tile_pairs.data(), ctx->tile_pairs.size() * sizeof(int64_t))) ||
-      (r = cp(ctx->d_queue.ptr, ctx->queue.data(), ctx->queue.size() * sizeof(int64_t))) ||
+      (r = cp(ctx->d_queue.ptr, ctx->queue.data(), ctx->queue.size() * sizeof(QueueItem))) ||
       (r = cp(ctx->d_spl_blk.ptr, ctx->spl_blk.data(), ctx->spl_blk.size() * sizeof(int64_t))) ||
       (r = cp(ctx->d_bessel.ptr, ctx->bessel.data(), ctx->bessel.size() * sizeof(int32_t))))
     return r;
@@ -1539,7 +1557,7 @@ int aak_batch_plan_bytes(aak_ctx *ctx, int64_t *bytes) {
   // start orders and the spline-block prefix
   *bytes = (int64_t)(ctx->descs.size() * sizeof(SourceDesc) + ctx->tile_start.size() * sizeof(int64_t) +
                      ctx->tile_knot.size() * sizeof(int32_t) + ctx->tile_pairs.size() * sizeof(int64_t) +
-                     ctx->queue.size() * sizeof(int64_t) + ctx->total_knots * (sizeof(double) + sizeof(double4)) +
+                     ctx->queue.size() * sizeof(QueueItem) + ctx->total_knots * (sizeof(double) + sizeof(double4)) +
                      ctx->bessel.size() * sizeof(int32_t) + ctx->spl_blk.size() * sizeof(int64_t));
   return AAK_OK;
 }

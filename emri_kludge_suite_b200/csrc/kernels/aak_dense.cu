@@ -287,20 +287,27 @@ struct TileCtx {
 // orders interleaved across sources.
 __device__ __forceinline__ TileCtx tile_ctx(const BatchView &bv, int64_t j, const SourceDesc *&dp) {
   TileCtx c;
-  const int64_t g = bv.queue ? bv.queue[j] : j;
-  c.s = find_source(bv.tile_start, bv.nsrc, g);
-  dp = bv.src + c.s;
-  const int64_t t0 = bv.tile_start[c.s];
-  const int T = (int)(bv.tile_start[c.s + 1] - t0);
-  const int i0 = dp->i0;
-  c.head = (i0 <= 0) ? 0 : min(i0 / kTileSamples, T - 1);
+  int T;
   if (bv.queue) {
-    c.lt = (int)(g - t0);
+    const QueueItem &q = bv.queue[j];
+    c.s = q.s;
+    c.lt = q.lt;
+    c.g = q.g;
+    dp = bv.src + c.s;
+    T = dp->n_tiles;
+    const int i0 = dp->i0;
+    c.head = (i0 <= 0) ? 0 : min(i0 / kTileSamples, T - 1);
   } else {
-    const int jj = (int)(g - t0);
+    c.s = find_source(bv.tile_start, bv.nsrc, j);
+    dp = bv.src + c.s;
+    const int64_t t0 = bv.tile_start[c.s];
+    T = (int)(bv.tile_start[c.s + 1] - t0);
+    const int i0 = dp->i0;
+    c.head = (i0 <= 0) ? 0 : min(i0 / kTileSamples, T - 1);
+    const int jj = (int)(j - t0);
     c.lt = (jj < T - c.head) ? c.head + jj : T - 1 - jj;
+    c.g = t0 + c.lt;
   }
-  c.g = t0 + c.lt;
   c.start = c.lt * kTileSamples;
   c.end = min(c.start + kTileSamples, dp->vlength);
   c.neff = n_eff(*dp);
@@ -1315,6 +1322,37 @@ constexpr size_t kWaveDynSmem = (size_t)kDynVals * kTileSamples * sizeof(double)
 // default of the precision); kMinB: resident CTAs per SM the register budget
 // is sized for.  Both are launch-shape choices of the autotuner.
 static_assert(sizeof(SourceDesc) % 16 == 0, "SourceDesc lands in shared memory with one bulk copy");
+
+// kPre: one thread issues the bulk copies of queue item q's source record,
+// its TilePrep and, when its knot window has at most kWin knots, the window's
+// knot times (from a 16-byte boundary: one element of slack is allocated past
+// the last knot), values and spline coefficients, all completing on bar; win
+// gets the window's first knot, knot count and offset of the first time in
+// wt.  The caller orders every earlier read of the destinations before it.
+__device__ __forceinline__ void issue_stage(const BatchView &bv, const QueueItem &q, SourceDesc *desc, TilePrep *prep,
+                                            int *win, double *wt, double4 *wy, double4 *wc, uint64_t *bar) {
+  fence_proxy_async_smem();
+  const int nk = q.nk;
+  const bool staged = nk > 0 && nk <= kWin;
+  const int64_t off = q.knot;
+  const int64_t a = off & ~(int64_t)1;  // knot times from a 16-byte boundary
+  const int toff = (int)(off - a);
+  const int cnt = (nk + toff + 1) & ~1;
+  const uint32_t b0 = (uint32_t)(sizeof(SourceDesc) + sizeof(TilePrep)) +
+                      (staged ? (uint32_t)(cnt * sizeof(double) + 2 * nk * sizeof(double4)) : 0u);
+  mbar_arrive_expect_tx(bar, b0);
+  bulk_copy_g2s(desc, bv.src + q.s, (uint32_t)sizeof(SourceDesc), bar);
+  bulk_copy_g2s(prep, bv.tile_prep + q.g, (uint32_t)sizeof(TilePrep), bar);
+  if (staged) {
+    bulk_copy_g2s(wt, bv.knot_t + a, (uint32_t)(cnt * sizeof(double)), bar);
+    bulk_copy_g2s(wy, bv.knot_y + off, (uint32_t)(nk * sizeof(double4)), bar);
+    bulk_copy_g2s(wc, bv.knot_c + off, (uint32_t)(nk * sizeof(double4)), bar);
+  }
+  win[0] = q.k0;
+  win[1] = nk;
+  win[2] = toff;
+}
+
 template <bool kSplit, int kMode = 0, bool kPre = false, int kJointT = 0, int kMinB = AAK_WAVE_MIN_BLOCKS>
 __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) {
   constexpr bool kPhase = kMode != 0, kTdi = kMode == 2;
@@ -1360,12 +1398,22 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     const long long j = s_tile;
     __syncthreads();
     if (j >= bv.total_tiles) break;
+    // kPre (batches, which have queue items): the tile's record, parameters
+    // and knot window are requested first thing, straight from its item
+    bool empty = false;
+    if constexpr (kPre) {
+      const QueueItem &q = bv.queue[j];
+      empty = (q.flags & (kPhase ? kQueueFailed : kQueueNoWave)) != 0;
+      if (tid == 0 && !empty) issue_stage(bv, q, &s_desc, &s_prep, s_win, s_wt, s_wy, s_wc, &s_mbar[0]);
+    }
     const SourceDesc *dp;
     const TileCtx c = tile_ctx(bv, j, dp);
     const int64_t g = c.g;
-    // samples [start, lim) feed the output (the phase product: every sample)
+    // samples [start, lim) feed the output (the phase product: every sample);
+    // kPre: the item's flags say the same (failed source, or lim <= start)
     const int lim = kPhase ? c.end : min(c.end, c.neff);
-    if (dp->status != 0 || lim <= c.start) {
+    if (!kPre) empty = dp->status != 0 || lim <= c.start;
+    if (empty) {
       // failed source, or a tile entirely after the taper: zeros, and an
       // empty aggregate for the chain
       const SourceDesc &dz = *dp;
@@ -1391,43 +1439,24 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
     KnotWin w{s_wt, s_wy, s_wc, s_wb, s_wd, 0, 0, 0};
     if constexpr (kPre) {
       using TT = typename std::conditional<kSplit, float, double>::type;
-      if (tid == 0) {
-        // every thread's reads of the previous tile's shared memory are
-        // ordered before these copies by the loop's barriers
-        fence_proxy_async_smem();
-        const int k0 = bv.tile_knot[2 * g], nk = bv.tile_knot[2 * g + 1];
-        const bool staged = nk > 0 && nk <= kWin;
-        const int64_t off = dp->knot_offset + k0;
-        const int64_t a = off & ~(int64_t)1;  // knot times from a 16-byte boundary
-        const int toff = (int)(off - a);
-        const int cnt = (nk + toff + 1) & ~1;
-        const TilePrep *pg = bv.tile_prep + g;
-        const int Kt = pg->K, st = pg->stride, nm = dp->nmodes;
-        const uint32_t b0 = (uint32_t)(sizeof(SourceDesc) + sizeof(TilePrep)) +
-                            (staged ? (uint32_t)(cnt * sizeof(double) + 2 * nk * sizeof(double4)) : 0u);
-        mbar_arrive_expect_tx(&s_mbar[0], b0);
-        bulk_copy_g2s(&s_desc, dp, (uint32_t)sizeof(SourceDesc), &s_mbar[0]);
-        bulk_copy_g2s(&s_prep, pg, (uint32_t)sizeof(TilePrep), &s_mbar[0]);
-        if (staged) {
-          bulk_copy_g2s(s_wt, bv.knot_t + a, (uint32_t)(cnt * sizeof(double)), &s_mbar[0]);
-          bulk_copy_g2s(s_wy, bv.knot_y + off, (uint32_t)(nk * sizeof(double4)), &s_mbar[0]);
-          bulk_copy_g2s(s_wc, bv.knot_c + off, (uint32_t)(nk * sizeof(double4)), &s_mbar[0]);
-        }
-        const bool tab = !kPhase && Kt > 0 && nm <= kTabModes;
-        if (tab) {
-          // FP64: one row per harmonic; FP32: one row per pair of harmonics
-          const uint32_t b1 = (uint32_t)(kSplit ? (nm + 1) >> 1 : nm) * (uint32_t)st * (uint32_t)sizeof(TT);
-          mbar_arrive_expect_tx(&s_mbar[1], b1);
-          bulk_copy_g2s(tabD, static_cast<const unsigned char *>(bv.tile_tab) + g * bv.tab_slot, b1, &s_mbar[1]);
-        }
-        s_win[0] = k0;
-        s_win[1] = nk;
-        s_win[2] = toff;
-        s_win[3] = tab ? 1 : 0;
-      }
       if (tid == kTileThreads - 1) make_geom(*dp, s_geom);
       const bool ok = mbar_wait_bounded(&s_mbar[0], ph0);
       ph0 ^= 1u;
+      if (tid == 0 && ok) {
+        // the tile's Taylor table (its term count and row stride came with
+        // the record; the previous tile's reads of it are ordered before this
+        // by the loop's barriers)
+        const int nm = s_desc.nmodes;
+        const bool tab = !kPhase && s_prep.K > 0 && nm <= kTabModes;
+        if (tab) {
+          fence_proxy_async_smem();
+          // FP64: one row per harmonic; FP32: one row per pair of harmonics
+          const uint32_t b1 = (uint32_t)(kSplit ? (nm + 1) >> 1 : nm) * (uint32_t)s_prep.stride * (uint32_t)sizeof(TT);
+          mbar_arrive_expect_tx(&s_mbar[1], b1);
+          bulk_copy_g2s(tabD, static_cast<const unsigned char *>(bv.tile_tab) + g * bv.tab_slot, b1, &s_mbar[1]);
+        }
+        s_win[3] = tab ? 1 : 0;
+      }
       if (__syncthreads_or(!ok)) {  // a copy did not land: report it and stop this CTA
         if (tid == 0) {
           atomicExch(bv.device_status, 1u);
@@ -2138,7 +2167,7 @@ void launch_dense_t(const BatchView &bv, int num_sms, cudaStream_t stream, cudaE
       (bv.max_nmodes > 0 && bv.max_nmodes < kTabModes) ? bv.max_nmodes : kTabModes);
   const size_t dyn = kWaveDynSmem + (size_t)rows * (kSplit ? kRowF * sizeof(float) : kRowD * sizeof(double));
   const int v = (bv.variant >= 0 && bv.variant < kNumVariants) ? bv.variant : 0;
-  const bool pre = wave_variant(kSplit, v).pre && bv.tile_prep && bv.tile_tab && !bv.trajectory_only &&
+  const bool pre = wave_variant(kSplit, v).pre && bv.tile_prep && bv.tile_tab && bv.queue && !bv.trajectory_only &&
                    bv.tab_slot >= tile_table_slot_bytes(rows, kSplit);
   prepare_dense_launch();
   if (pre) {

@@ -89,13 +89,29 @@ constexpr WaveVariant wave_variant(bool split, int v) {
                   : v == 4 ? WaveVariant{true, 1, 2} : v == 5 ? WaveVariant{true, 2, 3} : WaveVariant{true, 1, 3});
 }
 
+// One work-queue item: a tile, its place in its source, and what staging it
+// needs, so that a CTA can issue the tile's bulk copies and find its source
+// with one load (no search over the tile prefix, no dependent lookups).
+struct alignas(16) QueueItem {
+  int64_t knot;   // absolute index (in the knot arrays) of the first knot of the tile's window
+  int32_t g;      // global tile index
+  int32_t s;      // source
+  int32_t lt;     // tile index inside the source
+  int32_t k0;     // first knot of the window, source-relative
+  int32_t nk;     // knots in the window
+  int32_t flags;  // kQueueNoWave, kQueueFailed
+};
+static_assert(sizeof(QueueItem) == 32, "a queue item is two 16-byte loads");
+constexpr int32_t kQueueNoWave = 1;  // no waveform output: failed source, or a tile entirely after the taper
+constexpr int32_t kQueueFailed = 2;  // failed source (the phase passes have no output either)
+
 // Everything the kernels read about a batch.
 struct BatchView {
   const SourceDesc *src;
   int32_t nsrc;
   int64_t total_tiles;
   const int64_t *tile_start;    // nsrc + 1 prefix of tiles (device)
-  const int64_t *queue = nullptr;  // work-queue order (global tile indices); null: source by source, each in chain order
+  const QueueItem *queue = nullptr;  // work-queue order; null: source by source, each in chain order
   const int32_t *tile_knot;     // 2 per tile: first knot of the tile's window, knots in it
   const double *knot_t;         // knots
   const double4 *knot_y;        // (e, v, M, S) at the knots
