@@ -173,24 +173,55 @@ __device__ __forceinline__ void load_window(const BatchView &bv, const SourceDes
   finish_window(bv, d, w);
 }
 
-// gamma~dot, Phidot, alphadot (AAK.cc:251-253)
-// with one division: d(x)/dm / dt/dm / M = 16 v^3 num_x / (num_t M) for the
-// PN numerators of aak_common.hpp.  om (optional) receives Omega_phi, the
-// same ratio for phi on prograde orbits (omega_phi, AAK.cc:15-23).
+// gamma~dot, Phidot, alphadot (AAK.cc:251-253) with one division:
+// d(x)/dm / dt/dm / M = 16 v^3 num_x / (num_t M) for the 3PN numerators of
+// aak_common.hpp (KSParMap.cc:86-144).  Here they are regrouped, exactly, as
+// polynomials in x = v^2, w = q v, wy = w Y and E = e^2 (Y = cos iota is the
+// source's; every coefficient below is an integer, so the regrouping holds
+// term for term), and the rates are formed from
+//   T = num_t,  A = num_theta - num_r,  B = num_r,  C = num_phi - num_theta,
+// so that the differences are evaluated without cancellation: gamma~dot = A,
+// Phidot = B, alphadot = C (times 16 v^3 / (T M)).  om (optional) receives
+// Omega_phi, the ratio for phi with (Y, q) on prograde orbits and (-Y, -q) on
+// retrograde ones (AAK.cc:15-23): num_phi(Y, q) = A + B + C and num_phi(-Y,
+// -q) = A + B - C (the t numerator is even in (Y, q)).  Against the
+// reference's evaluation order the rates differ by rounding only.
 __device__ __forceinline__ void phase_rates(const SourceDesc &d, const Traj4 &q, double r[3], double *om = nullptr) {
-  const double st = pn_dtdm_num(q.v, q.e, d.coslam, q.S);
-  const double sr = pn_drdm_num(q.v, q.e, d.coslam, q.S);
-  const double sth = pn_dthetadm_num(q.v, q.e, d.coslam, q.S);
-  const double sph = pn_dphidm_num(q.v, q.e, d.coslam, q.S);
-  const double inv = 16. * (q.v * q.v * q.v) / (st * q.M);
-  r[0] = (sth - sr) * inv;
-  r[1] = sr * inv;
-  r[2] = (sph - sth) * inv;
-  // Omega_phi: the ratio for phi with (Y, q) on prograde orbits and (-Y, -q)
-  // on retrograde ones (AAK.cc:15-23).  The t numerator depends on q only
-  // through q Y, q^2 and Y^2, so it is the same number for (-Y, -q): only the
-  // phi numerator is evaluated again.
-  if (om) *om = ((d.coslam > 0) ? sph : pn_dphidm_num(q.v, q.e, -d.coslam, -q.S)) * inv;
+  const double Y = d.coslam;
+  const double E = q.e * q.e, x = q.v * q.v, w = q.S * q.v, wy = w * Y, w2 = w * w, wy2 = wy * wy;
+  // T: coefficients of x^k w^a wy^b as cubics in E
+  const double c00 = fma(fma(fma(560., E, 480.), E, 384.), E, 256.);
+  const double c20 = fma(fma(fma(-360., E, -240.), E, -64.), E, 384.);
+  const double t31 = E * fma(fma(960., E, 768.), E, 512.);
+  const double t42a = fma(fma(fma(400., E, 336.), E, 256.), E, 128.);
+  const double t42b = fma(fma(fma(-880., E, -720.), E, -512.), E, -128.);
+  const double c40 = fma(fma(fma(-2742., E, -2268.), E, -1584.), E, 864.);
+  const double t51 = fma(fma(fma(8816., E, 7392.), E, 5504.), E, -768.);
+  const double t62a = fma(fma(fma(4800., E, 3992.), E, 3008.), E, -64.);
+  const double t62b = fma(fma(fma(-15096., E, -12616.), E, -9600.), E, 192.);
+  const double c60 = fma(fma(fma(-15565., E, -13134.), E, -9864.), E, 2160.);
+  const double T4 = fma(x, c60, fma(wy2, t62b, fma(w2, t62a, fma(wy, t51, c40))));
+  const double T2 = fma(x, T4, fma(wy2, t42b, fma(w2, t42a, fma(wy, t31, c20))));
+  const double T = fma(x, T2, c00);
+  // A = num_theta - num_r
+  const double A6 = fma(fma(24., E, 270.), E, 486.);
+  const double A4 = fma(x, A6, fma(-fma(90., E, 186.), w2, fma(fma(258., E, 522.), wy2,
+                                                               fma(-fma(144., E, 384.), wy, fma(36., E, 144.)))));
+  const double A = x * fma(x, A4, fma(-12., w2, fma(60., wy2, fma(-96., wy, 48.))));
+  // B = num_r
+  const double B6 = fma(fma(fma(5., E, 21.), E, -135.), E, -351.);
+  const double B4 = fma(x, B6, fma(fma(fma(2., E, 14.), E, 132.), w2,
+                                   fma(fma(fma(26., E, -78.), E, -408.), wy2,
+                                       fma(fma(fma(-24., E, 32.), E, 264.), wy, fma(6., E * E, -90.)))));
+  const double B2 = fma(x, B4, fma(fma(4., E, 8.), w2, fma(fma(4., E, -32.), wy2, fma(fma(-16., E, 48.), wy, fma(8., E, -24.)))));
+  const double B = fma(x, B2, 16.);
+  // C = num_phi - num_theta
+  const double C = (x * w) * fma(x, fma(-fma(140., E, 36.), wy, fma(64., E, 48.)), fma(-24., wy, 32.));
+  const double inv = 16. * (x * q.v) / (T * q.M);
+  r[0] = A * inv;
+  r[1] = B * inv;
+  r[2] = C * inv;
+  if (om) *om = ((Y > 0) ? (A + B) + C : (A + B) - C) * inv;
 }
 
 // h_I, h_II of one sample: FP64 outputs, or FP32 ones (rows of an FP32 FFT)
@@ -979,8 +1010,8 @@ template <typename T>
 __device__ __forceinline__ void double_angle(T y, T x, T &c2, T &s2) {
   const T r2 = x * x + y * y;
   if (r2 > T(0)) {
-    T inv;  // FP32: the correctly rounded reciprocal, cheaper than a division
-    if constexpr (sizeof(T) == 4) inv = __frcp_rn(r2);
+    T inv;  // FP32: the approximate reciprocal (2 ulp), below the FP32 response's own rounding
+    if constexpr (sizeof(T) == 4) inv = __fdividef(T(1), r2);
     else inv = T(1) / r2;
     c2 = (x * x - y * y) * inv;
     s2 = T(2) * x * y * inv;
@@ -1008,7 +1039,7 @@ struct Resp {
 template <typename T>
 struct Geom {
   T Lc[3], Ls[3], Lq[3], nv[3], Sv[3], nxS[3];
-  T nxS_norm, Sdotn, coslam, beta_c, beta_s, cphiS, sphiS, cosphiK, sinphiK;
+  T nxS_norm, inv_nxS_norm, Sdotn, coslam, beta_c, beta_s, cphiS, sphiS, cosphiK, sinphiK;
   T cosqS, sinqS, cosqK, sinqK, psd0, psd1, psd2, F0[4], zeta;
   int mich;
 };
@@ -1024,6 +1055,7 @@ __device__ void make_geom(const SourceDesc &d, Geom<T> &g) {
     g.nxS[i] = (T)d.nxS[i];
   }
   g.nxS_norm = (T)d.nxS_norm;
+  g.inv_nxS_norm = (T)(1.0 / d.nxS_norm);
   g.Sdotn = (T)d.Sdotn;
   g.coslam = (T)d.coslam;
   g.beta_c = (T)d.beta_c;
@@ -1092,13 +1124,14 @@ __device__ __forceinline__ Resp<T> response(const Geom<T> &d, T ca, T sa, T c2g,
   const T nL0 = n1 * L2 - n2 * L1, nL1 = n2 * L0 - n0 * L2, nL2 = n0 * L1 - n1 * L0;
   const T S0 = (T)d.Sv[0], S1 = (T)d.Sv[1], S2 = (T)d.Sv[2];
   const T nS0 = (T)d.nxS[0], nS1 = (T)d.nxS[1], nS2 = (T)d.nxS[2];
-  const T norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * (T)d.nxS_norm;
   T cosrot, sinrot;
   if constexpr (sizeof(T) == 4) {
-    const T rn = __frcp_rn(norm);
+    // 1 / (|n x L| |n x S|) from the approximate reciprocal square root (2 ulp)
+    const T rn = rsqrtf(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * d.inv_nxS_norm;
     cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) * rn;
     sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) * rn;
   } else {
+    const T norm = sqrt(nL0 * nL0 + nL1 * nL1 + nL2 * nL2) * (T)d.nxS_norm;
     cosrot = (nL0 * nS0 + nL1 * nS1 + nL2 * nS2) / norm;
     sinrot = ((L0 * nS0 + L1 * nS1 + L2 * nS2) - (S0 * nL0 + S1 * nL1 + S2 * nL2)) / norm;
   }
