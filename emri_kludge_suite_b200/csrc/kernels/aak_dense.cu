@@ -259,11 +259,9 @@ __device__ __forceinline__ void dd_add(double &hi, double &lo, double x) {
   lo = e - (hi - s);
 }
 
-// block-wide exclusive scan of three values; every thread also gets the totals
-__device__ __forceinline__ void block_exscan3(const double v[3], double (*red)[kTileThreads / 32], double ex[3],
-                                              double tot[3]) {
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  double in[3] = {v[0], v[1], v[2]};
+// Warp-wide scan of three values: in[] becomes the inclusive prefix, ex[] the exclusive one.
+__device__ __forceinline__ void warp_scan3(double in[3], double ex[3]) {
+  const int l = threadIdx.x & 31;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
@@ -277,11 +275,26 @@ __device__ __forceinline__ void block_exscan3(const double v[3], double (*red)[k
     const double e = __shfl_up_sync(0xffffffffu, in[q], 1);
     ex[q] = (l == 0) ? 0.0 : e;
   }
-  __syncthreads();
+}
+
+// Block-wide exclusive scans of three values, the forward ones and (both, a
+// block-uniform flag) the backward ones, with one barrier for the two: each
+// warp's totals go to red[direction], and every thread adds the totals of the
+// warps before it; every thread also gets the block totals.  The barrier also
+// orders every shared-memory read before the call before any write after it.
+__device__ __forceinline__ void block_exscan3x2(const double vf[3], const double vb[3], bool both,
+                                                double (*red)[3][kTileThreads / 32], double exf[3], double totf[3],
+                                                double exb[3], double totb[3]) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  double inf[3] = {vf[0], vf[1], vf[2]}, inb[3] = {vb[0], vb[1], vb[2]};
+  warp_scan3(inf, exf);
+  if (both) warp_scan3(inb, exb);
   if (l == 31) {
-    red[0][w] = in[0];
-    red[1][w] = in[1];
-    red[2][w] = in[2];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      red[0][q][w] = inf[q];
+      if (both) red[1][q][w] = inb[q];
+    }
   }
   __syncthreads();
 #pragma unroll
@@ -289,12 +302,26 @@ __device__ __forceinline__ void block_exscan3(const double v[3], double (*red)[k
     double pre = 0.0, t = 0.0;
 #pragma unroll
     for (int k = 0; k < kTileThreads / 32; ++k) {
-      const double r = red[q][k];
+      const double r = red[0][q][k];
       if (k < w) pre += r;
       t += r;
     }
-    ex[q] += pre;
-    tot[q] = t;
+    exf[q] += pre;
+    totf[q] = t;
+  }
+  if (both) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      double pre = 0.0, t = 0.0;
+#pragma unroll
+      for (int k = 0; k < kTileThreads / 32; ++k) {
+        const double r = red[1][q][k];
+        if (k < w) pre += r;
+        t += r;
+      }
+      exb[q] += pre;
+      totb[q] = t;
+    }
   }
 }
 
@@ -1391,7 +1418,7 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
   constexpr bool kPhase = kMode != 0, kTdi = kMode == 2;
   static_assert(!kPre || kMode != 2, "the pre-pass serves the waveform and phase modes");
   extern __shared__ double s_dyn[];  // [kDynVals][kTileSamples]
-  __shared__ double red[3][kTileThreads / 32];
+  __shared__ double red[2][3][kTileThreads / 32];  // warp totals of the forward and backward scans
   __shared__ long long s_tile;
   __shared__ double s_par[3], s_rb[3], s_ra[3], s_cy[7], s_lastP;  // tile parameters, chain carry
   __shared__ __align__(16) SourceDesc s_desc;           // this tile's source
@@ -1728,8 +1755,9 @@ __global__ void __launch_bounds__(kTileThreads, kMinB) k_waveform(BatchView bv) 
         tB[qq] += incB[k][qq];
       }
     double runF[3], runB[3] = {0.0, 0.0, 0.0}, eF[3], eB[3] = {0.0, 0.0, 0.0};
-    block_exscan3(tF, red, eF, runF);  // its barriers order every read of (C) before the writes of (D)
-    if (d.i0 > 0 && c.start <= d.i0) block_exscan3(tB, red, eB, runB);  // backward region present (tile-uniform)
+    // (the backward scan only where the tile has a backward region; its
+    // barrier orders every read of (C) before the writes of (D))
+    block_exscan3x2(tF, tB, d.i0 > 0 && c.start <= d.i0, red, eF, runF, eB, runB);
     // (D) tile-local phases: forward, the increments of the tile's samples
     //     before i; backward, those of its samples up to i; the chain's carry
     //     is added after the look-back
