@@ -252,8 +252,9 @@ def cpu_likelihood_reference(procs: int = 0, sample_len: int = 200000) -> dict:
 # ----------------------------------------------------------------------------- likelihood (config 4)
 FIDUCIAL = np.array([0.785, 0.5, 8.0, 0.2, 1e6, 10.0, 0.0, 0.0, 0.0, 0.5, 1.0, 0.8, 2.0, 1.0])  # gpu_gen_AAK order
 # DRAM bytes (read + write) per sample of the split waveform kernel, from an ncu
-# capture of that kernel on 16 sources of the configuration-1 draw
-TRAFFIC_BYTES_PER_SAMPLE = (281.245184e6 + 413.069056e6) / 28_332_971
+# capture of that kernel on all 512 sources of the configuration-1 draw cut to
+# an eighth of their length (bench.py --profile waveform512)
+TRAFFIC_BYTES_PER_SAMPLE = (923.200768e6 + 1849.097e6) / 108_999_922
 LIKE_LENGTH = 3_200_000  # 1 yr at dt = 10 s rounded up to the 5-smooth FFT length 2^10 * 5^5
 
 
@@ -1025,8 +1026,9 @@ def run_gpu(args, rank, world, local_rank):
                 "achieved": achieved, "peak": fp32_peak,
                 "unit": "TFLOP/s", "frac": achieved / fp32_peak if fp32_peak > 0 else None,
                 "traffic": TRAFFIC_BYTES_PER_SAMPLE * N,
-                "traffic_source": "dram read+write per sample of one ncu capture of the same kernel on 16 sources "
-                                  "of this draw (28,332,971 samples), scaled to this launch",
+                "traffic_source": "dram read+write per sample of one ncu capture of the same kernel on the 512 "
+                                  "sources of this draw cut to an eighth of their length (108,999,922 samples), "
+                                  "scaled to this launch",
                 "peak_source": "measured FP32 FMA rate on this GPU (aak_probe_fp32_tflops)",
                 "flops_per_sample": fps, "flop_convention": "multiplies and adds one flop each (an FMA two), as the "
                 "FMA-rate probe; per sample 60 + 54 n: 24 FMA-equivalents (48 flops) of the reference's per-harmonic "
@@ -1089,6 +1091,7 @@ def run_gpu(args, rank, world, local_rank):
 # ----------------------------------------------------------------------------- profiling workloads
 # Small cases of the same kernels for ncu captures (one GPU):
 #   python bench.py --profile waveform   # 16 of the 512 sources, FP64 and split, default and tuned shapes
+#   python bench.py --profile waveform512  # all 512 sources at an eighth of their length, split default shape, twice
 #   python bench.py --profile phase      # the phase product of the same 16 sources, twice
 #   python bench.py --profile fisher     # two 14-parameter Fisher matrices, 28 x 3.2e6-sample templates
 #   python bench.py --profile tdi        # frequency-domain TDI of the waveform workload's 16 sources, twice
@@ -1119,6 +1122,33 @@ def profile_waveform():
     torch.cuda.synchronize()
     assert wb.device_status() == 0
     print("waveform workload:", n, "samples")
+
+
+def profile_waveform512():
+    """All 512 configuration-1 sources with their observation times cut to an
+    eighth (about 1.1e8 samples, 1.7 GB of FP64 outputs: above the 126 MB L2),
+    so that, as on the full batch, a tile's phase-chain predecessor is a whole
+    batch row earlier in the work queue; the split default launch shape, twice."""
+    import torch
+
+    from emri_kludge_suite_b200.aak import WaveBatch
+
+    src, _ = config1(SEED, 512)
+    for p in src:
+        p["T"] = p["T"] / 8.0
+        p["length"] = p["length"] // 8
+    wb = WaveBatch(0)
+    wb.plan(src, nmodes=NMODES)
+    wb.upload()
+    n = wb.total_samples
+    hI = torch.empty(n, dtype=torch.float64, device="cuda")
+    hII = torch.empty_like(hI)
+    wb.set_variant(1, 0)
+    for _ in range(2):
+        wb.run(hI.data_ptr(), hII.data_ptr(), precision=1)
+    torch.cuda.synchronize()
+    assert wb.device_status() == 0
+    print("waveform512 workload:", n, "samples")
 
 
 def profile_phase():
@@ -1209,7 +1239,7 @@ def profile_likelihood():
     print("likelihood workload: 32 x", LIKE_LENGTH, "samples, FP64 and FP32 transforms")
 
 
-PROFILES = {"waveform": profile_waveform, "phase": profile_phase, "fisher": profile_fisher,
+PROFILES = {"waveform": profile_waveform, "waveform512": profile_waveform512, "phase": profile_phase, "fisher": profile_fisher,
             "tdi": profile_tdi, "mlp": profile_mlp, "likelihood": profile_likelihood}
 
 
