@@ -344,17 +344,128 @@ void KerrGeodesic::frequencies(double Om[3]) const {
 // CKG with USING_cosiota: equatorial cases directly, inclined orbits by
 // bisection of E between the prograde and retrograde equatorial energies
 // until the implied cos(iota) matches to 1e-9 (src/circ/CKG.cc:86-127).
-void CircularConstants::set(double r, double cosi, double a) {
-  const double Delta = r * r - 2. * r + a * a;
-  auto Lz_of_E = [&](double En) {
+//
+// The bisection's result is the midpoint of the first step whose cos(iota)
+// is within 1e-9, so it carries the bisection's own error (up to ~1e-9 in
+// cos iota); the inspiral rates depend on it, and the trajectory must agree
+// with the reference's to 1e-10.  Each step costs two square roots and two
+// divisions and about 30 steps are needed, which made this 75 % of an
+// inspiral rate evaluation.  The fast path below reaches the same bits with a
+// few evaluations: cos(iota)(E) falls monotonically from +1 at the prograde
+// to -1 at the retrograde equatorial energy, so a bisection step whose
+// |cos iota - c| exceeds 1e-9 turns exactly as the side of the root E* its
+// midpoint lies on.  E* is found by a safeguarded Newton iteration with the
+// analytic derivative, and a half-width d is found around it outside which
+// |cos iota - c| > 2e-9 (checked by evaluating both ends).  The bisection is
+// then replayed: a midpoint farther than d from E* turns by comparison with
+// E*, one within d is evaluated exactly as the plain bisection evaluates it,
+// which also decides where it stops.  Where any of this fails (|c| close to
+// 1, where cos iota(E) saturates, or Newton does not settle) the plain
+// bisection runs.
+namespace {
+struct CircFns {
+  double r, a, Delta;
+  double Lz_of_E(double En) const {
     const double t1 = r * (1. + r * (En * En - 1.));
     return (En * (r * r - a * a) - Delta * std::sqrt(t1)) / (a * (r - 1.));
-  };
-  auto Q_of = [&](double En, double L) {
+  }
+  double Q_of(double En, double L) const {
     const double q1 = (En * (a * a + r * r) - a * L) * (En * (a * a + r * r) - a * L) / Delta;
     const double q2 = r * r + a * En * (a * En - 2. * L) + L * L;
     return (std::fabs(q1 - q2) < 1.e-9) ? 0.0 : q1 - q2;
-  };
+  }
+  // cos(iota) at energy En, as the bisection evaluates it
+  double cosi_of(double En) const {
+    const double L = Lz_of_E(En);
+    const double q = Q_of(En, L);
+    return L / std::sqrt(L * L + q);
+  }
+  // cos(iota) and its derivative in E (no clamp on Q: used only to find the root)
+  void cosi_and_slope(double En, double &cg, double &dcg) const {
+    const double t1 = r * (1. + r * (En * En - 1.));
+    const double st = std::sqrt(t1);
+    const double den = a * (r - 1.);
+    const double L = (En * (r * r - a * a) - Delta * st) / den;
+    const double dL = ((r * r - a * a) - Delta * r * r * En / st) / den;
+    const double u = En * (a * a + r * r) - a * L, du = (a * a + r * r) - a * dL;
+    const double q = u * u / Delta - (r * r + a * En * (a * En - 2. * L) + L * L);
+    const double dq = 2. * u * du / Delta - (2. * a * a * En - 2. * a * (L + En * dL) + 2. * L * dL);
+    const double n2 = L * L + q;
+    cg = L / std::sqrt(n2);
+    dcg = (dL * q - 0.5 * L * dq) / (n2 * std::sqrt(n2));
+  }
+};
+
+// The bisection of CKG: returns the energy it stops at.
+double circ_bisect(const CircFns &F, double c, double Elo, double Ehi) {
+  double En = 0.5 * (Ehi + Elo);
+  for (int it = 0; it < 400; ++it) {
+    En = 0.5 * (Ehi + Elo);
+    const double cg = F.cosi_of(En);
+    if (cg > c) Elo = En;
+    else Ehi = En;
+    if (std::fabs(cg - c) < 1.e-9) break;
+  }
+  return En;
+}
+
+// The same result by root, zone and replay; false where the fast path does not apply.
+bool circ_fast(const CircFns &F, double c, double Elo, double Ehi, double &E_out) {
+  if (!(std::fabs(c) < 0.999) || !(Ehi > Elo)) return false;
+  // safeguarded Newton for cos iota(E) = c on [Elo, Ehi], from this thread's
+  // previous root when it lies in the bracket (the inspiral's rate
+  // evaluations come in close succession); the result does not depend on the
+  // start, since any E* accurate to far below d gives the same replay
+  thread_local double last_root = 0.0;
+  double lo = Elo, hi = Ehi, E = (last_root > Elo && last_root < Ehi) ? last_root : 0.5 * (Elo + Ehi), slope = 0.0;
+  bool done = false;
+  for (int it = 0; it < 60; ++it) {
+    double cg, dcg;
+    F.cosi_and_slope(E, cg, dcg);
+    if (!std::isfinite(cg) || !std::isfinite(dcg)) return false;
+    const double f = cg - c;
+    if (f > 0) lo = E;
+    else hi = E;
+    slope = dcg;
+    if (dcg < 0.0 && std::fabs(f) <= -dcg * 4e-16 * std::fabs(E)) {  // the Newton step is below an ulp or two
+      done = true;
+      break;
+    }
+    double En = (dcg < 0.0) ? E - f / dcg : 0.5 * (lo + hi);
+    if (!(En >= lo && En <= hi)) En = 0.5 * (lo + hi);
+    E = En;
+  }
+  if (!done || !(slope < 0.0)) return false;
+  last_root = E;
+  // the zone around E* outside which |cos iota - c| > 2e-9
+  double d = 4e-9 / -slope;
+  for (int k = 0;; ++k) {
+    if (k == 20) return false;
+    if (F.cosi_of(E - d) - c > 2e-9 && F.cosi_of(E + d) - c < -2e-9) break;
+    d *= 2.0;
+  }
+  // replay the bisection
+  double a_ = Elo, b_ = Ehi, En = 0.5 * (b_ + a_);
+  for (int it = 0; it < 400; ++it) {
+    En = 0.5 * (b_ + a_);
+    if (std::fabs(En - E) >= d) {  // decided by the side of the root; cannot stop here
+      if (En < E) a_ = En;
+      else b_ = En;
+      continue;
+    }
+    const double cg = F.cosi_of(En);
+    if (cg > c) a_ = En;
+    else b_ = En;
+    if (std::fabs(cg - c) < 1.e-9) break;
+  }
+  E_out = En;
+  return true;
+}
+}  // namespace
+
+void CircularConstants::set(double r, double cosi, double a, bool bisection_only) {
+  const double Delta = r * r - 2. * r + a * a;
+  const CircFns F{r, a, Delta};
   double En;
   double c = cosi;
   if (c == 1.) {
@@ -369,25 +480,16 @@ void CircularConstants::set(double r, double cosi, double a) {
     den = Delta * std::sqrt(r * den);
     E = numer / den;
     Lz = 0.;
-    Q = Q_of(E, 0.);
+    Q = F.Q_of(E, 0.);
     L_over_cosi = std::sqrt(Q);
     return;
   } else {
-    double Elo = kerr_e_eq_pro(r, a);
-    double Ehi = (r >= kerr_isco_ret(a)) ? kerr_e_eq_ret(r, a) : 1.;
-    En = 0.5 * (Ehi + Elo);
-    for (int it = 0; it < 400; ++it) {
-      En = 0.5 * (Ehi + Elo);
-      const double L = Lz_of_E(En);
-      const double q = Q_of(En, L);
-      const double cg = L / std::sqrt(L * L + q);
-      if (cg > c) Elo = En;
-      else Ehi = En;
-      if (std::fabs(cg - c) < 1.e-9) break;
-    }
+    const double Elo = kerr_e_eq_pro(r, a);
+    const double Ehi = (r >= kerr_isco_ret(a)) ? kerr_e_eq_ret(r, a) : 1.;
+    if (bisection_only || !circ_fast(F, c, Elo, Ehi, En)) En = circ_bisect(F, c, Elo, Ehi);
   }
   E = En;
-  Lz = Lz_of_E(En);
+  Lz = F.Lz_of_E(En);
   Q = Lz * Lz * (1. - c * c) / (c * c);
   L_over_cosi = std::sqrt(Lz * Lz + Q);
 }

@@ -49,7 +49,9 @@ struct KerrGeodesic {
 // reference CKG constructor with the USING_cosiota flag (src/circ/CKG.cc:63-128).
 struct CircularConstants {
   double E = 0, Lz = 0, Q = 0, L_over_cosi = 0;
-  void set(double r, double cosi, double a);
+  // bisection_only: run every bisection step as written (the check of the
+  // fast path, which must give the same bits)
+  void set(double r, double cosi, double a, bool bisection_only = false);
 };
 
 // Radiation-reaction rates dp/dt, de/dt, d(cos iota)/dt in radiation-reaction
