@@ -91,6 +91,35 @@ AAK_HD T pn_dphidm_num(T v, T e, T Y, T q) {
 }
 AAK_HD double pn_dphidm(double v, double e, double Y, double q) { return pn_dphidm_num(v, e, Y, q) / (16. * v); }
 
+// The same four numerators regrouped, exactly (every coefficient is an
+// integer, so the regrouping holds term for term), as polynomials in
+// x = v^2, w = q v, wy = q v Y and E = e^2, and combined as
+//   T = num_t,  A = num_theta - num_r,  B = num_r,  C = num_phi - num_theta,
+// so that the rate differences come without cancellation; num_phi(-Y, -q)
+// = A + B - C (T, A and B are even in (Y, q), C is odd).  Plain products and
+// sums, no fused multiply-adds, so that host and device evaluate it alike.
+AAK_HD void pn_numerators_TABC(double v, double e, double Y, double q, double &T, double &A, double &B, double &C) {
+  const double E = e * e, x = v * v, w = q * v, wy = w * Y, w2 = w * w, wy2 = wy * wy;
+  const double c00 = ((560. * E + 480.) * E + 384.) * E + 256.;
+  const double c20 = ((-360. * E - 240.) * E - 64.) * E + 384.;
+  const double t31 = E * ((960. * E + 768.) * E + 512.);
+  const double t42a = ((400. * E + 336.) * E + 256.) * E + 128.;
+  const double t42b = ((-880. * E - 720.) * E - 512.) * E - 128.;
+  const double c40 = ((-2742. * E - 2268.) * E - 1584.) * E + 864.;
+  const double t51 = ((8816. * E + 7392.) * E + 5504.) * E - 768.;
+  const double t62a = ((4800. * E + 3992.) * E + 3008.) * E - 64.;
+  const double t62b = ((-15096. * E - 12616.) * E - 9600.) * E + 192.;
+  const double c60 = ((-15565. * E - 13134.) * E - 9864.) * E + 2160.;
+  T = c00 + x * ((c20 + wy * t31 + w2 * t42a + wy2 * t42b) + x * ((c40 + wy * t51 + w2 * t62a + wy2 * t62b) + x * c60));
+  A = x * ((48. - 96. * wy + 60. * wy2 - 12. * w2) +
+           x * ((144. + 36. * E) - (384. + 144. * E) * wy + (522. + 258. * E) * wy2 - (186. + 90. * E) * w2 +
+                x * ((24. * E + 270.) * E + 486.)));
+  B = 16. + x * ((8. * E - 24.) + (48. - 16. * E) * wy + (4. * E - 32.) * wy2 + (4. * E + 8.) * w2 +
+                 x * ((6. * E * E - 90.) + ((-24. * E + 32.) * E + 264.) * wy + ((26. * E - 78.) * E - 408.) * wy2 +
+                      ((2. * E + 14.) * E + 132.) * w2 + x * (((5. * E + 21.) * E - 135.) * E - 351.)));
+  C = (x * w) * ((32. - 24. * wy) + x * ((64. * E + 48.) - (140. * E + 36.) * wy));
+}
+
 // Azimuthal frequency magnitude for pro/retrograde orbits (src/suite/AAK.cc:15-23).
 AAK_HD double omega_phi(double v, double e, double cosiota, double s, double M) {
   if (cosiota > 0) return pn_dphidm(v, e, cosiota, s) / pn_dtdm(v, e, cosiota, s) / M;

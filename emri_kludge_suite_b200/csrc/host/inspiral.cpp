@@ -25,6 +25,14 @@ constexpr int kMaxCol = 8;
 }  // namespace
 
 KerrInspiral::KerrInspiral(double cosi0, double spin) : cosi0_(cosi0), a_(spin) {
+  // The table depends on the spin alone: this thread's last one is reused
+  // for the same spin (the templates of a likelihood batch share theirs).
+  thread_local double last_spin = 2.0, last_table[2][2];
+  if (spin == last_spin) {
+    for (int j = 0; j < 2; ++j)
+      for (int i = 0; i < 2; ++i) p_lso_[j][i] = last_table[j][i];
+    return;
+  }
   const double csi[2] = {1.0, -1.0};
   const double ecc[2] = {0.0, kEccOne};
   double p_g = 0.0;
@@ -54,6 +62,9 @@ KerrInspiral::KerrInspiral(double cosi0, double spin) : cosi0_(cosi0), a_(spin) 
       p_lso_[j][i] = p_g;
     }
   }
+  last_spin = spin;
+  for (int j = 0; j < 2; ++j)
+    for (int i = 0; i < 2; ++i) last_table[j][i] = p_lso_[j][i];
 }
 
 double KerrInspiral::p_lso(double csi, double e) const {

@@ -22,21 +22,17 @@ constexpr double kWarmAcceptance = 0.05;
 AAK_HD bool pm_finite(double a) { return a - a == 0.0; }
 AAK_HD double pm_norm1(const double f[3]) { return fabs(f[0]) + fabs(f[1]) + fabs(f[2]); }
 
-// Kerr->AK residual: Omega_k M_map - Omega_k^PN(v_map, s_map) M  (KSParMap.cc:323-358)
+// Kerr->AK residual: Omega_k M_map - Omega_k^PN(v_map, s_map) M  (KSParMap.cc:323-358).
+// The PN frequencies d(x)/dm / dt/dm / (2 pi) = 16 v^3 num_x / (num_t 2 pi),
+// from the regrouped numerators (pn_numerators_TABC) at (Y, s), or at (-Y, -s)
+// with Omega_phi negated on retrograde orbits, as the reference evaluates them.
 AAK_HD void pm_residual(const double Om[3], double M, double e, double Y, const double x[3], double f[3]) {
   const double v = x[0], Mm = x[1], s = x[2];
-  double Or, Ot, Op;
-  if (Y > 0) {
-    const double tm = pn_dtdm(v, e, Y, s);
-    Or = pn_drdm(v, e, Y, s) / tm / 2. / kPi;
-    Ot = pn_dthetadm(v, e, Y, s) / tm / 2. / kPi;
-    Op = pn_dphidm(v, e, Y, s) / tm / 2. / kPi;
-  } else {
-    const double tm = pn_dtdm(v, e, -Y, -s);
-    Or = pn_drdm(v, e, -Y, -s) / tm / 2. / kPi;
-    Ot = pn_dthetadm(v, e, -Y, -s) / tm / 2. / kPi;
-    Op = -pn_dphidm(v, e, -Y, -s) / tm / 2. / kPi;
-  }
+  double T, A, B, C;
+  const bool pro = Y > 0;
+  pn_numerators_TABC(v, e, pro ? Y : -Y, pro ? s : -s, T, A, B, C);
+  const double k = 16. * (v * v * v) / (T * (2. * kPi));
+  const double Or = B * k, Ot = (A + B) * k, Op = (pro ? 1.0 : -1.0) * ((A + B) + C) * k;
   f[0] = Om[0] * Mm - Or * M;
   f[1] = Om[1] * Mm - Ot * M;
   f[2] = Om[2] * Mm - Op * M;
