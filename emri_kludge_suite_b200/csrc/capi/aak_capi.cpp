@@ -2127,15 +2127,75 @@ aak_params gpu_params(const aak_gpu *g, const double *x) {
 
 // Host half of a batch of templates: plan them into the context's rows.
 // Plan B templates into context C (rows of g->row doubles); *ms: host time.
-int gpu_plan_into(aak_gpu *g, aak_ctx *C, const double *x, int B, int nthreads, int32_t *status, double *ms) {
+// The front end of a chunk of templates with the learned warm start, done
+// ahead of the chunk's planning: coarse Kerr inspirals on host threads, one
+// prediction launch for every coarse point of the chunk, then the map solves
+// from the predictions (the planner's own warm-started front end, step for
+// step).  fe[k]: the front end's status of template k, maps[k] its mapped
+// trajectory where that is AAK_OK.
+struct WarmFrontEnd {
+  std::vector<aak_mapped> maps;
+  std::vector<int32_t> fe;
+};
+
+int front_end_warm(aak_ctx *ctx, const aak_params *P, int B, int nthreads, WarmFrontEnd *out) {
+  out->maps.resize(B);
+  out->fe.assign(B, AAK_OK);
+  std::vector<CoarseKerr> ck(B);
+  parallel_for(B, nthreads, [&](int64_t s) {
+    const Params Pp = to_params(P[s]);
+    int st = validate(Pp);
+    if (st == kOk) st = coarse_kerr(Pp, &ck[s]);
+    out->fe[s] = st;
+  });
+  std::vector<int64_t> first(B + 1, 0);
+  for (int s = 0; s < B; ++s) first[s + 1] = first[s] + (out->fe[s] == kOk ? ck[s].steps : 0);
+  const int64_t np = first[B];
+  std::vector<double> xs(4 * np), ys(3 * np), warm(3 * np);
+  for (int s = 0; s < B; ++s)
+    for (int64_t i = 0; i < first[s + 1] - first[s]; ++i) {
+      double *x = &xs[4 * (first[s] + i)];
+      x[0] = ck[s].p[i];
+      x[1] = ck[s].e[i];
+      x[2] = P[s].iota;
+      x[3] = P[s].s;
+    }
+  if (np > 0) {
+    const int r = mlp_predict_host(ctx->model, xs.data(), ys.data(), np);
+    if (r != AAK_OK) return r;
+  }
+  for (int s = 0; s < B; ++s)
+    for (int64_t i = first[s]; i < first[s + 1]; ++i) parmap_from_coords(&xs[4 * i], P[s].M, &ys[3 * i], &warm[3 * i]);
+  parallel_for(B, nthreads, [&](int64_t s) {
+    if (out->fe[s] != kOk) return;
+    MappedTrajectory mt;
+    int fb = 0;
+    const int st = map_coarse(to_params(P[s]), ck[s], &mt, &warm[3 * first[s]], &fb);
+    out->fe[s] = st;
+    if (st == kOk) to_mapped(mt, &out->maps[s]);
+  });
+  return AAK_OK;
+}
+
+// Plan a chunk of templates into C.  With fe (a warm front end done ahead),
+// the planner starts from its mapped trajectories; templates whose front end
+// failed are planned as invalid and reported with the front end's status.
+int gpu_plan_into(aak_gpu *g, aak_ctx *C, const double *x, int B, int nthreads, int32_t *status, double *ms,
+                  const WarmFrontEnd *fe = nullptr) {
   std::vector<aak_params> P(B);
   for (int k = 0; k < B; ++k) P[k] = gpu_params(g, x + 14 * (size_t)k);
+  if (fe)
+    for (int k = 0; k < B; ++k)
+      if (fe->fe[k] != AAK_OK) P[k].e = 0.0;  // rejected by the per-source validation, not planned
   const auto t0 = std::chrono::steady_clock::now();
   C->out_stride = g->row;
-  const int r = plan_common(C, P.data(), nullptr, B, nullptr, nthreads);
+  const int r = plan_common(C, P.data(), fe ? fe->maps.data() : nullptr, B, nullptr, nthreads);
   C->out_stride = 0;
   *ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (r != AAK_OK) return r;
+  if (fe)
+    for (int k = 0; k < B; ++k)
+      if (fe->fe[k] != AAK_OK) C->status[k] = fe->fe[k];
   for (int k = 0; k < B; ++k)
     if (status) status[k] = C->status[k];
   return AAK_OK;
@@ -2565,8 +2625,14 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
   // context (whose upload, of chunk c - 1, has finished reading its plan
   // arrays) and then queues it, so that the device goes from one chunk to the
   // next without waiting for the host; chunk c - 1's results are collected
-  // after that.
+  // after that.  With a learned warm start, its prediction needs the device,
+  // which is busy with the persistent waveform kernel of the chunk in flight:
+  // the front end of chunk c + 2 (coarse inspirals, prediction, maps) is then
+  // done after chunk c + 1 is planned, so that its prediction runs between
+  // chunk c's kernels and the planning of a chunk never waits for the device.
   aak_ctx *ctxs[2] = {g->ctx, g->ctx2};
+  const bool ahead = g->ctx->model != nullptr;
+  WarmFrontEnd fe[3];
   const int32_t nch = (nsrc + max_batch - 1) / max_batch;
   auto chunk_size = [&](int32_t c) { return std::min<int32_t>(max_batch, nsrc - c * max_batch); };
   auto fail = [&](int e) {
@@ -2575,7 +2641,19 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
     return e;
   };
   double ms = 0.0;
-  if ((r = gpu_plan_into(g, ctxs[0], params, chunk_size(0), nthreads, status, &ms)) != AAK_OK) return r;
+  // the warm front end of chunk c (ahead only), timed with the planning
+  auto front = [&](int32_t c) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<aak_params> P(chunk_size(c));
+    for (int k = 0; k < chunk_size(c); ++k) P[k] = gpu_params(g, params + 14 * ((int64_t)c * max_batch + k));
+    const int e = front_end_warm(g->ctx, P.data(), chunk_size(c), nthreads, &fe[c % 3]);
+    tot[0] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return e;
+  };
+  if (ahead && ((r = front(0)) != AAK_OK || (nch > 1 && (r = front(1)) != AAK_OK))) return r;
+  if ((r = gpu_plan_into(g, ctxs[0], params, chunk_size(0), nthreads, status, &ms, ahead ? &fe[0] : nullptr)) !=
+      AAK_OK)
+    return r;
   tot[0] += ms;
   for (int32_t c = 0; c < nch; ++c) {
     const int p = c & 1;
@@ -2584,10 +2662,11 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
       const int64_t k1 = (int64_t)(c + 1) * max_batch;
       if ((r = cuda_ok(cudaEventSynchronize(g->pev[1 - p][0]))) != AAK_OK) return fail(r);
       if ((r = gpu_plan_into(g, ctxs[1 - p], params + 14 * k1, chunk_size(c + 1), nthreads,
-                             status ? status + k1 : nullptr, &ms)) != AAK_OK)
+                             status ? status + k1 : nullptr, &ms, ahead ? &fe[(c + 1) % 3] : nullptr)) != AAK_OK)
         return fail(r);
       tot[0] += ms;
     }
+    if (ahead && c + 2 < nch && (r = front(c + 2)) != AAK_OK) return fail(r);
     if (c > 0 && (r = gpu_chunk_collect(g, 1 - p, chunk_size(c - 1), out + 2 * (int64_t)(c - 1) * max_batch, tot)) !=
                      AAK_OK)
       return fail(r);

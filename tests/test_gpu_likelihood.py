@@ -130,3 +130,34 @@ def test_fp32_transform_and_compensated_products_against_fp64_oracle():
         worst = max(worst, dl / (d_d + ref[1]))
     print("fp32 likelihood: max |dlogL| / (d_d + h_h) =", worst)
     assert worst <= 2e-5
+
+
+def test_warm_started_batch_equals_single_template_calls():
+    """With a learned warm start, a likelihood batch does each chunk's front end
+    (coarse inspirals, one prediction launch, map solves) two chunks ahead of
+    its planning; the templates must come out as single-template calls, whose
+    planner runs the warm-started front end itself."""
+    from emri_kludge_suite_b200 import parmap_mlp as PM
+
+    train = PM.make_dataset(1 << 14, seed=41)
+    m = PM.ParMapMLP(0, seed=2)
+    m.train(train["x"][train["valid"]], train["y"][train["valid"]], epochs=10, batch=4096, lr=1e-2)
+    w1, w2 = _weights()
+    dI, dII = _oracle_wave(INJ)
+    D1, D2 = np.fft.rfft(dI) * w1, np.fft.rfft(dII) * w2
+    g = GPUAAK(1.0, 100, LENGTH, 100.0, DT, True, False)
+    g.input_data(D1, D2, w1, w2)
+    g.set_warm_start(m)
+    rng = np.random.default_rng(5)
+    X = np.tile(INJ, (9, 1))
+    X[:, 2] *= 1 + 1e-4 * rng.standard_normal(9)
+    X[:, 6:11] += 1e-2 * rng.standard_normal((9, 5))
+    X[4, 3] = -0.5  # invalid eccentricity: zero template, status reported
+    out, st = g.likelihood_batch(X, max_batch=2, return_status=True)  # five chunks: the front ends run ahead
+    assert st[4] != 0 and np.all(out[4] == 0.0)
+    for k in range(9):
+        if k == 4:
+            continue
+        assert st[k] == 0
+        g.gpu_gen_AAK(*X[k])
+        np.testing.assert_allclose(out[k], g.Likelihood(), rtol=1e-13)
