@@ -47,7 +47,8 @@ AAK_HD_FI T dvdt_core(T v, T e, T Y, T m, T M, T q, T lv, T ome15) {
               1044921875. * l5 * (1. / 96768.));
   c6 -= 107. * (256. + 1832. * e2 + 1308. * e4 + 69. * e6) * lv * (1. / 1680.);
   s += v6 * c6;
-  return 32. * ome15 * m * v6 * v3 * s / (5. * M * M);
+  // the source's constant factor first and no division: the step's critical path is a serial recurrence
+  return (32. / 5.) * (m / (M * M)) * ome15 * v6 * v3 * s;
 }
 
 template <class T>
@@ -72,7 +73,7 @@ AAK_HD_FI T dedt_core(T v, T e, T Y, T m, T M, T q, T lv, T ome15) {
               1022385321. * l3 * (1. / 340480.) - 1044921875. * l5 * (1. / 204228.));
   c6 -= 107. * (6152. + 22256. * e2 + 10721. * e4) * lv * (1. / 15960.);
   s += 2451456. * v6 * c6;
-  return -(e * ome15 * m * v6 * v2 * s) / (120960. * M * M);
+  return -((1. / 120960.) * (m / (M * M)) * e * ome15 * v6 * v2 * s);
 }
 
 // Inlined into the evolution loops, so that the compiler keeps the terms that
