@@ -4,7 +4,7 @@ The split kernel forms the harmonic phases exp(i (n Phi' + D0)) in FP32 by the
 recurrence w_n = w_{n-1} z_1 from z_1 = exp(i Phi'), where Phi' (the orbital
 phase plus the Doppler term) is reduced to [-pi, pi] in FP64 and rounded to
 FP32, and re-anchors the rotor every 8th harmonic at exp(i (n Phi' + D0))
-with n Phi' + D0 reduced in FP64 (aak_dense.cu: mode_sums_taylor_multi).
+with n Phi' + D0 reduced in FP64 (aak_dense.cu: mode_sums_split, pair_step).
 This test emulates that arithmetic in numpy float32 (IEEE rounding of every
 product and sum; sin/cos of the FP32 argument rounded once, standing in for
 sincosf, plus the documented 2^-21.41 absolute error of __sincosf on the
