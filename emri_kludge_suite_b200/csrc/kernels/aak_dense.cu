@@ -868,7 +868,7 @@ __device__ __forceinline__ void mode_sums_fp64(const double *tab, int nmodes, in
     zi[m] = sD[m];
     sa[m] = sb[m] = sc[m] = 0.0;
   }
-#pragma unroll 1
+#pragma unroll 2  // two harmonics' Horner chains side by side (unrolling by four was slower)
   for (int n = 1; n <= nmodes; ++n) {
     double v[(NV + 1) / 2 * 2];
     const double2 *r2 = reinterpret_cast<const double2 *>(tab + (n - 1) * stride);
