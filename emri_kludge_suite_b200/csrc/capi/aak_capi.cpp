@@ -2465,6 +2465,106 @@ int gpu_fisher(aak_gpu *g, const double *x, int nd, double scale, int nthreads, 
   return device_status(g->ctx);
 }
 
+// The device half of one Fisher point planned in C, slot p: C's plan is
+// uploaded on up_stream (after the generation of the point two back, the
+// last reader of C's device buffers), then on the likelihood's stream the 2 nd
+// rows are generated, transformed and reduced to the Gram matrices, which are
+// copied to page-locked slot p.  Events as gpu_chunk_launch's.
+int gpu_fisher_point_launch(aak_gpu *g, aak_ctx *C, int p, int nd, double scale, int grid) {
+  cudaEvent_t *E = g->pev[p];
+  int r;
+  if ((r = cuda_ok(cudaStreamWaitEvent(g->up_stream, E[1], 0))) != AAK_OK) return r;
+  if ((r = upload(C, g->up_stream, false)) != AAK_OK) return r;
+  if ((r = cuda_ok(cudaEventRecord(E[0], g->up_stream))) != AAK_OK ||
+      (r = cuda_ok(cudaStreamWaitEvent(g->stream, E[0], 0))) != AAK_OK)
+    return r;
+  cudaEventRecord(E[2], g->stream);
+  if ((r = run(C, g->d_H[0].ptr, g->d_H[1].ptr, nullptr, nullptr, 0, g->precision == 0 ? 0 : 1, g->stream)) != AAK_OK)
+    return r;
+  cudaEventRecord(E[1], g->stream);
+  g->count = 2 * nd;
+  g->spectral = false;
+  g->rows32 = false;
+  if ((r = gpu_fft_rows(g)) != AAK_OK) return r;
+  cudaEventRecord(E[3], g->stream);
+  FisherArgs a;
+  a.H[0] = g->d_H[0].ptr;
+  a.H[1] = g->d_H[1].ptr;
+  a.row_doubles = g->row;
+  a.w[0] = g->d_w[0].ptr;
+  a.w[1] = g->d_w[1].ptr;
+  a.nbins = g->nbins;
+  a.nd = nd;
+  a.scale = scale;
+  a.partial = g->d_fisher.ptr;
+  a.out = g->d_fisher.ptr + fisher_partial_doubles(nd, grid);
+  launch_fisher_gram(a, g->ctx->num_sms, g->stream);
+  if ((r = cuda_ok(cudaGetLastError())) != AAK_OK) return r;
+  cudaEventRecord(E[4], g->stream);
+  if ((r = cuda_ok(cudaMemcpyAsync(g->h_stage + 2 * (size_t)g->stage_cap * p, a.out, 2 * (size_t)nd * nd * sizeof(double),
+                                   cudaMemcpyDeviceToHost, g->stream))) != AAK_OK)
+    return r;
+  return cuda_ok(cudaEventRecord(E[5], g->stream));
+}
+
+// Fisher matrices of npts points, pipelined as the likelihood batches are:
+// point k + 1 is planned on host threads into the other planning context while
+// the device generates, transforms and reduces point k.
+int gpu_fisher_batch(aak_gpu *g, const double *x, int npts, int nd, double scale, int nthreads, double *gram,
+                     int32_t *status) {
+  if (npts < 1 || nd < 1 || nd > kFisherMaxDim || !x || !gram || !std::isfinite(scale)) return AAK_ERR_INVALID_PARAM;
+  if (!g->d_w[0].ptr || !g->d_w[1].ptr) return AAK_ERR_INVALID_PARAM;  // input_data first: the weights
+  const int B = 2 * nd;
+  int r;
+  // result slots of 2 nd^2 doubles (the page-locked stage holds two of 2 x stage_cap)
+  if ((r = gpu_pipeline_ready(g, std::max(B, nd * nd))) != AAK_OK) return r;
+  if (g->plan_batch != B) {  // an exact-size transform plan of the rows, made once before the loop
+    if (g->plan) cufftDestroy(g->plan);
+    g->plan = 0;
+    g->plan_batch = 0;
+  }
+  if ((r = gpu_capacity(g, B)) != AAK_OK) return r;
+  const int grid = fisher_grid(g->ctx->num_sms, g->nbins);
+  if ((r = g->d_fisher.reserve((size_t)(fisher_partial_doubles(nd, grid) + 2 * (int64_t)nd * nd))) != AAK_OK) return r;
+  aak_ctx *ctxs[2] = {g->ctx, g->ctx2};
+  auto fail = [&](int e) {
+    cudaStreamSynchronize(g->up_stream);
+    cudaStreamSynchronize(g->stream);
+    return e;
+  };
+  auto collect = [&](int p, int k, double *tot) -> int {
+    cudaEvent_t *E = g->pev[p];
+    const int e = cuda_ok(cudaEventSynchronize(E[5]));
+    if (e != AAK_OK) return e;
+    std::memcpy(gram + 2 * (int64_t)nd * nd * k, g->h_stage + 2 * (size_t)g->stage_cap * p, 2 * (size_t)nd * nd * sizeof(double));
+    float f;
+    if (cudaEventElapsedTime(&f, E[2], E[1]) == cudaSuccess) tot[1] += f;
+    if (cudaEventElapsedTime(&f, E[1], E[3]) == cudaSuccess) tot[2] += f;
+    if (cudaEventElapsedTime(&f, E[3], E[4]) == cudaSuccess) tot[3] += f;
+    cudaGetLastError();
+    return AAK_OK;
+  };
+  double tot[4] = {0, 0, 0, 0}, ms = 0.0;
+  if ((r = gpu_plan_into(g, ctxs[0], x, B, nthreads, status, &ms)) != AAK_OK) return r;
+  tot[0] += ms;
+  for (int c = 0; c < npts; ++c) {
+    const int p = c & 1;
+    if ((r = gpu_fisher_point_launch(g, ctxs[p], p, nd, scale, grid)) != AAK_OK) return fail(r);
+    if (c + 1 < npts) {
+      const int64_t k1 = (int64_t)(c + 1) * B;
+      if ((r = cuda_ok(cudaEventSynchronize(g->pev[1 - p][0]))) != AAK_OK) return fail(r);
+      if ((r = gpu_plan_into(g, ctxs[1 - p], x + 14 * k1, B, nthreads, status ? status + k1 : nullptr, &ms)) != AAK_OK)
+        return fail(r);
+      tot[0] += ms;
+    }
+    if (c > 0 && (r = collect(1 - p, c - 1, tot)) != AAK_OK) return fail(r);
+  }
+  if ((r = collect((npts - 1) & 1, npts - 1, tot)) != AAK_OK) return fail(r);
+  for (int q = 0; q < 4; ++q) g->ms[q] = tot[q];
+  const int s1 = device_status(g->ctx), s2 = device_status(g->ctx2);
+  return s1 != AAK_OK ? s1 : s2;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2685,6 +2785,15 @@ int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, i
   const int r = select_device(g->ctx->device);
   if (r != AAK_OK) return r;
   return gpu_fisher(g, params, nd, scale, nthreads, gram, status);
+}
+
+int aak_gpu_fisher_batch(aak_gpu *g, const double *params, int32_t npts, int32_t nd, double scale, int32_t nthreads,
+                         double *gram, int32_t *status) {
+  if (!g) return AAK_ERR_INVALID_PARAM;
+  std::lock_guard<std::mutex> lk(g->ctx->mu);
+  const int r = select_device(g->ctx->device);
+  if (r != AAK_OK) return r;
+  return gpu_fisher_batch(g, params, npts, nd, scale, nthreads, gram, status);
 }
 
 int aak_ctx_set_evolve_device(aak_ctx *ctx, int32_t on) {

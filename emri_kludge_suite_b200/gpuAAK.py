@@ -35,6 +35,8 @@ def _bind():
     L.aak_gpu_last_timing.argtypes = [v, _dp]
     L.aak_gpu_set_precision.argtypes = [v, ctypes.c_int32]
     L.aak_gpu_fisher.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _dp, _i32p]
+    L.aak_gpu_fisher_batch.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _dp,
+                                       _i32p]
     L._gpu_bound = True
     return L
 
@@ -129,6 +131,25 @@ class GPUAAK:
         G = np.zeros((2, nd, nd))
         st = np.zeros(2 * nd, dtype=np.int32)
         check(lib().aak_gpu_fisher(self._g, ptr(x), nd, float(scale), int(nthreads), ptr(G), ptr(st)), "fisher")
+        self._spectral = True
+        return (G, st) if return_status else G
+
+    def fisher_gram_batch(self, params, scale, nthreads=0, return_status=False):
+        """fisher_gram of several points in one call.
+
+        params: (npts, 2 nd, 14), each block laid out as for fisher_gram;
+        returns G of shape (npts, 2, nd, nd), G[k] = fisher_gram(params[k]).
+        The next point is planned on host threads while the device generates,
+        transforms and reduces the current one.
+        """
+        x = np.ascontiguousarray(params, dtype=np.float64)
+        if x.ndim != 3 or x.shape[2] != 14 or x.shape[1] % 2:
+            raise ValueError("params must be (npts, 2 nd, 14) in gpu_gen_AAK order")
+        npts, nd = x.shape[0], x.shape[1] // 2
+        G = np.zeros((npts, 2, nd, nd))
+        st = np.zeros((npts, 2 * nd), dtype=np.int32)
+        check(lib().aak_gpu_fisher_batch(self._g, ptr(x), npts, nd, float(scale), int(nthreads), ptr(G), ptr(st)),
+              "fisher_batch")
         self._spectral = True
         return (G, st) if return_status else G
 

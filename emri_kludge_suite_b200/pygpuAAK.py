@@ -125,16 +125,33 @@ class pyGPUAAK:
         <d_i h_II, d_j h_II>) for i <= j, mirrored.  form="full" is the
         two-channel Fisher matrix 4 Re(<d_i h_I, d_j h_I> + <d_i h_II, d_j h_II>).
         """
+        if form not in ("reference", "full"):
+            raise ValueError("form must be 'reference' or 'full'")
+        G = self.generator.fisher_gram(self._fisher_rows(x), 1.0 / (2 * self.eps))
+        return self._fisher_matrix(G, form).astype(x.dtype)
+
+    def get_Fisher_batch(self, X, form="reference"):
+        """get_Fisher at each row of X (npts, ndim) in one device call
+        (GPUAAK.fisher_gram_batch: the next point is planned while the device
+        works on the current one); returns (npts, ndim, ndim)."""
+        if form not in ("reference", "full"):
+            raise ValueError("form must be 'reference' or 'full'")
+        X = np.atleast_2d(X)
+        rows = np.stack([self._fisher_rows(x) for x in X])
+        G = self.generator.fisher_gram_batch(rows, 1.0 / (2 * self.eps))
+        return np.stack([self._fisher_matrix(g, form) for g in G]).astype(X.dtype)
+
+    def _fisher_rows(self, x):
+        """The 2 ndim central-difference templates of x, (2 ndim, 14) physical."""
         x_in = np.tile(x, (2 * self.ndim, 1))
         for i in range(self.ndim):
             x_in[2 * i, i] += self.eps
             x_in[2 * i + 1, i] -= self.eps
-        G = self.generator.fisher_gram(self._physical(x_in.T), 1.0 / (2 * self.eps))
+        return self._physical(x_in.T)
+
+    @staticmethod
+    def _fisher_matrix(G, form):
         if form == "reference":
             A = G[0].diagonal()[None, :] + G[1]
-            M = np.triu(A) + np.triu(A, 1).T
-        elif form == "full":
-            M = G[0] + G[1]
-        else:
-            raise ValueError("form must be 'reference' or 'full'")
-        return M.astype(x.dtype)
+            return np.triu(A) + np.triu(A, 1).T
+        return G[0] + G[1]

@@ -367,6 +367,17 @@ int aak_gpu_likelihood_batch(aak_gpu *g, const double *params, int32_t nsrc, int
 int aak_gpu_fisher(aak_gpu *g, const double *params, int32_t nd, double scale, int32_t nthreads, double *gram,
                    int32_t *status);
 
+/* Fisher-matrix Gram sums of npts points in one call (the reference computes
+ * one point per get_Fisher call, pygpuAAK/pygpuAAK.py:269-300; this is its
+ * loop over points): params holds npts blocks of 2 nd rows x 14, each laid
+ * out as for aak_gpu_fisher, and gram npts blocks of 2 x nd x nd, block k
+ * equal to aak_gpu_fisher of block k of params.  Point k + 1 is planned on
+ * host threads into a second planning context while the device generates,
+ * transforms and reduces point k.  status (optional, npts x 2 nd) per
+ * template. */
+int aak_gpu_fisher_batch(aak_gpu *g, const double *params, int32_t npts, int32_t nd, double scale, int32_t nthreads,
+                         double *gram, int32_t *status);
+
 /* Template precision: 0 = FP64 throughout (default), 1 = split (FP64 phases
  * and angle reductions, FP32 geometry, response, Bessel evaluation), 2 =
  * split templates written as FP32 rows, an FP32 R2C transform and FP32 inner

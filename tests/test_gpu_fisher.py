@@ -137,3 +137,35 @@ def test_fisher_reports_failed_templates():
     G, st = g.fisher_gram(X, 1.0, return_status=True)
     assert st[4] != 0 and np.all(np.delete(st, 4) == 0)
     assert np.all(np.isfinite(G))
+
+
+def test_fisher_batch_equals_single_point_calls():
+    """GPUAAK.fisher_gram_batch (aak_gpu_fisher_batch: the next point planned
+    while the device reduces the current one, two planning contexts in turn)
+    against one fisher_gram call per point; five points, so both result slots
+    are reused, and one invalid template in the third point."""
+    g, _ = _generator()
+    rng = np.random.default_rng(17)
+    pts = np.tile(INJ, (5, 1))
+    pts[:, 2] *= 1 + 1e-3 * rng.standard_normal(5)
+    pts[:, 6:11] += 1e-2 * rng.standard_normal((5, 5))
+    rows = np.stack([_rows(14, p) for p in pts])
+    rows[2, 7, 3] = -0.5  # invalid eccentricity: that template reported, the others unaffected
+    G, st = g.fisher_gram_batch(rows, 0.5, return_status=True)
+    assert G.shape == (5, 2, 14, 14) and st.shape == (5, 28)
+    assert st[2, 7] != 0 and np.count_nonzero(st) == 1
+    for k in range(5):
+        Gk, sk = g.fisher_gram(rows[k], 0.5, return_status=True)
+        assert np.array_equal(sk, st[k])
+        assert np.abs(G[k] - Gk).max() <= 1e-12 * np.abs(Gk).max(), k
+    # pyGPUAAK.get_Fisher_batch: the same matrices as get_Fisher point by point
+    x = INJ.copy()
+    x[4:6] = np.log(x[4:6])
+    like = pyGPUAAK({"injection_params": dict(zip(KEYS, x))}, LENGTH, DT, 100.0, KEYS, backint=False, eps=1e-4)
+    X = np.tile(x, (3, 1))
+    X[:, 6:9] += 1e-2 * rng.standard_normal((3, 3))
+    for form in ("reference", "full"):
+        M = like.get_Fisher_batch(X, form=form)
+        for k in range(3):
+            Mk = like.get_Fisher(X[k], form=form)
+            assert np.abs(M[k] - Mk).max() <= 1e-12 * np.abs(Mk).max(), (form, k)
