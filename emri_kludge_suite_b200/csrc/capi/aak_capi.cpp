@@ -2827,6 +2827,11 @@ int aak_gpu_set_parmap_model(aak_gpu *g, aak_mlp *m) {
   return aak_ctx_set_parmap_model(g->ctx, m);
 }
 
+int aak_gpu_set_variant(aak_gpu *g, int32_t precision, int32_t variant) {
+  if (!g) return AAK_ERR_INVALID_PARAM;
+  return aak_ctx_set_variant(g->ctx, precision, variant);  // the second planning context copies it per batch
+}
+
 int aak_gpu_set_precision(aak_gpu *g, int32_t precision) {
   if (!g || precision < 0 || precision > 2) return AAK_ERR_INVALID_PARAM;
   g->precision = precision;

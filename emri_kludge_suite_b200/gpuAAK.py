@@ -34,6 +34,7 @@ def _bind():
     L.aak_gpu_likelihood_batch.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp, _i32p]
     L.aak_gpu_last_timing.argtypes = [v, _dp]
     L.aak_gpu_set_precision.argtypes = [v, ctypes.c_int32]
+    L.aak_gpu_set_variant.argtypes = [v, ctypes.c_int32, ctypes.c_int32]
     L.aak_gpu_fisher.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _dp, _i32p]
     L.aak_gpu_fisher_batch.argtypes = [v, _dp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, _dp,
                                        _i32p]
@@ -45,6 +46,7 @@ class GPUAAK:
     def __init__(self, T_fit, init_length, length, init_dt, dt, LISA, backint):
         L = _bind()
         self.length = int(length)
+        self._precision = 0
         self.fft_length = self.length // 2 + 1
         self._g = ctypes.c_void_p()
         check(L.aak_gpu_create(float(T_fit), int(init_length), int(length), float(init_dt), float(dt), int(bool(LISA)),
@@ -159,8 +161,34 @@ class GPUAAK:
         check(lib().aak_gpu_set_parmap_device(self._g, int(bool(on))), "set_parmap_device")
 
     def set_precision(self, precision: int):
-        """0: FP64 throughout (default); 1: split precision."""
+        """0: FP64 throughout (default); 1: split precision; 2: split templates,
+        FP32 transform and compensated FP32 products (likelihood batches)."""
         check(lib().aak_gpu_set_precision(self._g, int(precision)), "set_precision")
+        self._precision = int(precision)
+
+    NUM_VARIANTS = 6  # AAK_NUM_VARIANTS: launch shapes of the waveform stage
+
+    def set_variant(self, precision: int, variant: int):
+        """Launch shape of the template waveform stage for kernel precision 0
+        (FP64) or 1 (split, also precision 2)."""
+        check(lib().aak_gpu_set_variant(self._g, int(precision), int(variant)), "set_variant")
+
+    def autotune(self, params, max_batch=256, nthreads=0):
+        """Pick the waveform stage's launch shape for the current precision on
+        a representative sample of templates (params: (n, 14)): each candidate
+        runs likelihood_batch(params) once to warm up and once timed (device
+        time of the waveform stage); the fastest is kept.  Returns (choice,
+        ms per candidate)."""
+        kp = 0 if self._precision == 0 else 1
+        ms = []
+        for v in range(self.NUM_VARIANTS):
+            self.set_variant(kp, v)
+            self.likelihood_batch(params, max_batch=max_batch, nthreads=nthreads)
+            self.likelihood_batch(params, max_batch=max_batch, nthreads=nthreads)
+            ms.append(self.last_timing_ms()["waveform"])
+        best = int(np.argmin(ms))
+        self.set_variant(kp, best)
+        return best, ms
 
     def set_warm_start(self, model=None):
         """Seed every Kerr->AK map solve of the template batches with a trained

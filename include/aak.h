@@ -385,6 +385,13 @@ int aak_gpu_fisher_batch(aak_gpu *g, const double *params, int32_t npts, int32_t
  * other calls run as precision 1). */
 int aak_gpu_set_precision(aak_gpu *g, int32_t precision);
 
+/* Launch shape of the template waveform stage for `precision` (0 FP64, 1
+ * split, also used by precision 2): one of the AAK_NUM_VARIANTS candidates of
+ * aak_ctx_autotune, applied to both planning contexts of the batches.  No
+ * reference counterpart (the reference's launch shape is fixed,
+ * src/cuda/AAK_manager.cu:233,245). */
+int aak_gpu_set_variant(aak_gpu *g, int32_t precision, int32_t variant);
+
 /* Milliseconds of the last batch: host planning, waveform kernels, FFT, reduction. */
 int aak_gpu_last_timing(aak_gpu *g, double *ms4);
 

@@ -65,3 +65,36 @@ def test_autotune_keeps_the_fastest_and_uses_its_cache(tmp_path):
     assert v2 == v and all(m == -1.0 for m in ms2)  # read from the cache, nothing timed
     assert len(open(cache).read().splitlines()) == 1
     assert os.path.getsize(cache) > 0
+
+
+def test_template_batches_take_every_launch_shape():
+    """GPUAAK.set_variant / autotune (aak_gpu_set_variant): likelihood batches
+    give the same inner products with every launch shape of the template
+    waveform stage (FP64 to 1e-9, split with the FP32 transform to 1e-5 of
+    <h|h>), and autotune keeps the fastest candidate."""
+    from emri_kludge_suite_b200.gpuAAK import GPUAAK
+    from test_gpu_likelihood import DT, INJ, LENGTH, _oracle_wave, _weights
+
+    w1, w2 = _weights()
+    dI, dII = _oracle_wave(INJ)  # data: the injection's oracle waveform, no noise
+    g = GPUAAK(1.0, 100, LENGTH, 100.0, DT, True, False)
+    g.input_data(np.fft.rfft(dI) * w1, np.fft.rfft(dII) * w2, w1, w2)
+    rng = np.random.default_rng(3)
+    X = np.tile(INJ, (6, 1))
+    X[:, 2] *= 1 + 1e-4 * rng.standard_normal(6)
+    X[:, 6:11] += 1e-2 * rng.standard_normal((6, 5))
+    for precision, tol in ((0, 1e-9), (2, 1e-5)):
+        g.set_precision(precision)
+        kp = 0 if precision == 0 else 1
+        ref = None
+        for v in range(GPUAAK.NUM_VARIANTS):
+            g.set_variant(kp, v)
+            out = g.likelihood_batch(X, max_batch=4)
+            if ref is None:
+                ref = out
+            assert np.abs(out - ref).max() <= tol * ref[:, 1].max(), (precision, v)
+        best, ms = g.autotune(X, max_batch=4)
+        assert len(ms) == GPUAAK.NUM_VARIANTS and 0 <= best < GPUAAK.NUM_VARIANTS
+        assert ms[best] == min(ms)
+        assert np.abs(g.likelihood_batch(X, max_batch=4) - ref).max() <= tol * ref[:, 1].max()
+    g.set_precision(0)
