@@ -187,3 +187,29 @@ class MultiDeviceGPUAAK:
             if r is not None:
                 out[parts[k]], st[parts[k]] = r
         return (out, st) if return_status else out
+
+    def fisher_gram_batch(self, params, scale, nthreads=0, return_status=False):
+        """GPUAAK.fisher_gram_batch with the points split over the devices
+        (equal costs: a balanced split of the counts); the Gram matrices are
+        reassembled in the caller's order."""
+        x = np.ascontiguousarray(params, dtype=np.float64)
+        if x.ndim != 3 or x.shape[2] != 14 or x.shape[1] % 2:
+            raise ValueError("params must be (npts, 2 nd, 14) in gpu_gen_AAK order")
+        n, nd = x.shape[0], x.shape[1] // 2
+        assign, _ = lpt_partition(np.ones(n), len(self.gens))
+        parts = [np.flatnonzero(assign == k) for k in range(len(self.gens))]
+        per = max(1, int(nthreads) // len(self.gens)) if nthreads else 0
+
+        def work(k):
+            if len(parts[k]) == 0:
+                return None
+            return self.gens[k].fisher_gram_batch(x[parts[k]], scale, nthreads=per, return_status=True)
+
+        with ThreadPoolExecutor(len(self.gens)) as ex:
+            res = list(ex.map(work, range(len(self.gens))))
+        G = np.zeros((n, 2, nd, nd))
+        st = np.zeros((n, 2 * nd), dtype=np.int32)
+        for k, r in enumerate(res):
+            if r is not None:
+                G[parts[k]], st[parts[k]] = r
+        return (G, st) if return_status else G
