@@ -1607,13 +1607,6 @@ int aak_batch_run_noalloc(aak_ctx *ctx, void *d_plan, int64_t plan_bytes, int64_
   int r;
   if ((r = select_device(ctx->device)) != AAK_OK) return r;
   cudaStream_t st = (cudaStream_t)stream;
-  // the call copies from host arrays (and may wait for those copies), which a
-  // stream capture cannot record: refuse rather than invalidate the capture
-  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
-    cudaGetLastError();
-    return AAK_ERR_INVALID_PARAM;
-  }
   unsigned char *base = static_cast<unsigned char *>(d_plan);
   auto cp = [&](size_t off, const void *src, size_t bytes) {
     return cuda_ok(cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st));

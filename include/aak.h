@@ -209,10 +209,9 @@ int aak_tdi_batch_host(aak_ctx *ctx, const aak_params *P, int32_t nsrc, int32_t 
  * until exit; batches above 32768 tiles of 1024 samples (33,554,432 samples)
  * are rejected with AAK_ERR_CAPACITY.  Each call looks the array's address
  * up in the current context (no allocation), so the entry point stays usable
- * after a cudaDeviceReset.  The call copies the plan from host memory, so it
- * cannot be recorded in a CUDA graph: on a capturing stream it returns
- * AAK_ERR_INVALID_PARAM and leaves the capture intact.  Every call
- * shares the array: calls that overlap on the GPU race.  Each call clears its
+ * after a cudaDeviceReset.  Each call copies the plan from host memory into
+ * d_plan on `stream`.  Every call shares the array: calls that overlap on the
+ * GPU race.  Each call clears its
  * own look-back status word before its kernel, so a wait that gave up in an
  * earlier call does not affect it; a give-up is kept in a report word that
  * aak_batch_device_status of a context that made such a call reads and
